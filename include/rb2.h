@@ -1,0 +1,155 @@
+/*
+ * rb2.h -- C ABI of librb2, the B200 (sm_100a) ray-query engine that drops in
+ * for renderbox2's acceleration-structure build, tracer and integrator path.
+ *
+ * Conventions
+ *  - Every function returns an rb2_status (0 = RB2_OK); rb2_last_error() gives
+ *    the thread-local text of the last failure.  Nothing asserts or aborts.
+ *  - Pointers named d_* are device pointers on the tracer's device; h_* are
+ *    host pointers.  Caller buffers are borrowed, never freed by the library.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *  - Rays use the reference's Ray layout (core/primitives.h:145-208):
+ *    two float4 per ray, (origin.xyz, tmin) then (direction.xyz, tmax).
+ */
+#ifndef RB2_H
+#define RB2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    RB2_OK = 0,
+    RB2_EINVAL = 1,      /* bad argument */
+    RB2_ENOMEM = 2,      /* host or device allocation failed */
+    RB2_ECUDA = 3,       /* CUDA runtime error */
+    RB2_EIO = 4,         /* file could not be read or written */
+    RB2_EFORMAT = 5,     /* corrupt or unsupported BVH / cache contents */
+    RB2_ETIMEOUT = 6,    /* a bounded device wait ran out */
+    RB2_EDEVICE = 7,     /* device-side check failed (status word set) */
+    RB2_ENOTSUP = 8      /* feature not available on this device / build */
+} rb2_status;
+
+/* Node layouts (accelerators/sbvh/cudatracerkernels.h:85-90).  Only Compact2
+ * (child index = float4 offset, the layout the reference's Kepler kernel
+ * reads) is produced and traced. */
+enum { RB2_LAYOUT_COMPACT = 0, RB2_LAYOUT_COMPACT2 = 1 };
+
+const char* rb2_last_error(void);
+const char* rb2_version(void);
+
+/* ------------------------------------------------------------------ build --
+ * Replaces BVH(Scene*, const Platform&, const BuildParams&)
+ * (accelerators/sbvh/bvh.h:115) + CudaBvh(const BVH&, BVHLayout)
+ * (accelerators/sbvh/cudabvh.h:80).  Defaults equal the reference's Platform
+ * (accelerators/sbvh/platform.h:78-90) and BuildParams (bvh.h:104-112) and the
+ * SplitBVHBuilder constants (splitbvhbuilder.h:135-140), except that the
+ * number of spatial bins and the object-split binning threshold are tunable. */
+typedef struct {
+    float sah_node_cost;        /* 1.0 */
+    float sah_triangle_cost;    /* 1.0 */
+    uint32_t min_leaf_size;     /* 1 */
+    uint32_t max_leaf_size;     /* 0x7FFFFFF */
+    float split_alpha;          /* 1e-5: spatial split if child overlap >= alpha * root area */
+    uint32_t max_depth;         /* 64 */
+    uint32_t max_spatial_depth; /* 48 */
+    uint32_t spatial_bins;      /* 64 (reference: 128) */
+    uint32_t object_bins;       /* 64; nodes with <= exact_sweep_max refs use a full sorted sweep */
+    uint32_t exact_sweep_max;   /* 512 */
+    int32_t num_threads;        /* <= 0: all hardware threads */
+    uint32_t layout;            /* RB2_LAYOUT_COMPACT2 */
+} rb2_build_params;
+
+typedef struct {
+    uint64_t n_nodes_u4;        /* node buffer size in uint4 (4 per inner node) */
+    uint64_t n_woop_u4;         /* Woop buffer size in uint4 (3 per tri ref + 1 per leaf) */
+    uint64_t n_triidx;          /* == n_woop_u4 */
+    uint32_t n_inner, n_leaves, n_tri_refs, n_tris;
+    uint32_t max_depth;
+    uint32_t layout;
+    float sah;                  /* top-down SAH cost (bvnode.cpp:85-100 definition) */
+    double build_ms;
+} rb2_bvh_counts;
+
+typedef struct rb2_host_bvh rb2_host_bvh;
+
+int rb2_build_params_default(rb2_build_params* p);
+
+/* v_xyz: nv vertices (float x,y,z); idx3: ntri triangles (3 vertex indices). */
+int rb2_bvh_build(const float* v_xyz, uint32_t nv, const uint32_t* idx3, uint32_t ntri,
+                  const rb2_build_params* params, rb2_host_bvh** out);
+
+/* Wraps existing Compact2 buffers (e.g. from the reference's CudaBvh getters,
+ * cudabvh.h:95-97).  The buffers are copied and validated. */
+int rb2_bvh_from_buffers(const uint32_t* nodes, uint64_t n_nodes_u4, const uint32_t* woop,
+                         uint64_t n_woop_u4, const uint32_t* triidx, uint64_t n_triidx,
+                         rb2_host_bvh** out);
+
+int rb2_bvh_counts_get(const rb2_host_bvh* b, rb2_bvh_counts* out);
+/* Getters (cudabvh.h:95-97): pointers stay valid until rb2_host_bvh_free. */
+const uint32_t* rb2_bvh_nodes(const rb2_host_bvh* b);
+const uint32_t* rb2_bvh_woop(const rb2_host_bvh* b);
+const uint32_t* rb2_bvh_triidx(const rb2_host_bvh* b);
+void rb2_host_bvh_free(rb2_host_bvh* b);
+
+/* BVH cache.  rb2_bvh_save writes the versioned binary format (magic "RB2BVH\0\1",
+ * version, layout, counts, FNV-1a checksum).  rb2_bvh_load reads that format
+ * or the reference's text cache (cudabvh.cpp:108-214, magic 0x76543210). */
+int rb2_bvh_save(const rb2_host_bvh* b, const char* path);
+int rb2_bvh_save_text(const rb2_host_bvh* b, const char* path);
+int rb2_bvh_load(const char* path, rb2_host_bvh** out);
+
+/* --------------------------------------------------------------- tracer --
+ * Replaces CudaTracer(const CudaBvh&, MemoryAllocator&) (cudatracer.h:67) and
+ * float trace(const RayBuffer&, IntersectionBuffer&, SceneBuffer&, uint8_t*
+ * stencil, bool any_hit) (cudatracer.h:87). */
+typedef struct rb2_tracer rb2_tracer;
+
+typedef struct {
+    int32_t prim;   /* original triangle index, -1 = miss */
+    float t;        /* hit distance (tmax of the ray on a miss) */
+    float u, v;     /* Woop barycentrics of the accepted triangle */
+} rb2_hit;
+
+/* Launch configuration of the persistent traversal kernel.  Zero fields mean
+ * "use the tuned default". */
+typedef struct {
+    uint32_t block_threads;     /* threads per CTA (multiple of 32) */
+    uint32_t ctas_per_sm;       /* resident CTAs per SM */
+    uint32_t fetch_threshold;   /* refill a warp when fewer lanes stay busy */
+    uint32_t reserved;
+} rb2_launch_config;
+
+/* Uploads the BVH to the current CUDA device.  The tracer owns that memory. */
+int rb2_tracer_create(const rb2_host_bvh* bvh, rb2_tracer** out);
+int rb2_tracer_destroy(rb2_tracer* t);
+int rb2_tracer_set_launch(rb2_tracer* t, const rb2_launch_config* cfg);
+int rb2_tracer_device_bytes(const rb2_tracer* t, uint64_t* bytes);
+
+/* Bulk trace of n rays (device buffers).  any_hit != 0 stops at the first
+ * accepted triangle.  d_mask (nullable) is the reference's stencil: rays with
+ * mask 0 are skipped and reported as misses.  Asynchronous on `stream`. */
+int rb2_trace(rb2_tracer* t, const float* d_rays, uint32_t n, int any_hit, const uint8_t* d_mask,
+              rb2_hit* d_hits, void* stream);
+
+/* Same from/to host memory: copies rays in, traces, copies hits out, and
+ * synchronises `stream`.  Scratch device buffers are grown on demand and
+ * reused across calls. */
+int rb2_trace_host(rb2_tracer* t, const float* h_rays, uint32_t n, int any_hit, const uint8_t* h_mask,
+                   rb2_hit* h_hits, void* stream);
+
+/* Occlusion-only any-hit: writes 1 byte per ray (1 = occluded). */
+int rb2_trace_occlusion(rb2_tracer* t, const float* d_rays, uint32_t n, const uint8_t* d_mask,
+                        uint8_t* d_occluded, void* stream);
+
+/* Device-side status word of the tracer (0 = clean).  Non-zero means a kernel
+ * hit a guard (stack overflow on a corrupt tree, bad index) and skipped work. */
+int rb2_tracer_status(rb2_tracer* t, uint32_t* status, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RB2_H */

@@ -1,0 +1,215 @@
+"""TEST INFRASTRUCTURE ONLY: the oracle.
+
+Two checkers, both CPU-only, used by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py -- never by the product library:
+
+* ``ref_*``: the reference's own host code (SBVH builder, Compact2 packer,
+  text BVH cache, perspective camera, Moller-Trumbore test) compiled in place
+  from the reference sources into oracle/_ref/librb2ref.so (oracle/Makefile).
+* ``trace`` / ``woop_test`` / ``bruteforce``: the CPU restatement of the
+  reference's traversal (oracle/rb2_oracle.c), plus the integrator
+  restatements in oracle/shading.py.
+
+Parity is pinned by comparing the restatement with the reference's own
+compiled code and against fixtures in tests/golden/ generated from it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_SO = HERE / "_ref" / "librb2ref.so"
+ORACLE_SO = HERE / "liboracle.so"
+REF_SRC = Path(os.environ.get("RB2_REF_SRC", "/root/reference/renderbox2/src"))
+
+_ref = None
+_orc = None
+
+
+class RefBvh(C.Structure):
+    _fields_ = [
+        ("n_nodes", C.c_uint32), ("n_woop", C.c_uint32), ("n_triidx", C.c_uint32), ("layout", C.c_uint32),
+        ("nodes", C.POINTER(C.c_uint32)), ("woop", C.POINTER(C.c_uint32)), ("triidx", C.POINTER(C.c_uint32)),
+        ("sah", C.c_float), ("n_inner", C.c_uint32), ("n_leaves", C.c_uint32), ("n_tri_refs", C.c_uint32),
+        ("build_ms", C.c_double),
+    ]
+
+
+class Hit(C.Structure):
+    _fields_ = [("prim", C.c_int32), ("t", C.c_float), ("u", C.c_float), ("v", C.c_float)]
+
+
+HIT_DTYPE = np.dtype([("prim", np.int32), ("t", np.float32), ("u", np.float32), ("v", np.float32)])
+COUNT_DTYPE = np.dtype([("nodes", np.uint32), ("tris", np.uint32), ("leafterms", np.uint32), ("pad", np.uint32)])
+
+
+def build(ref: bool = True) -> None:
+    """Builds liboracle.so, and librb2ref.so when the reference sources exist."""
+    targets = ["oracle"]
+    if ref and REF_SRC.exists():
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets, f"REF_SRC={REF_SRC}"], check=True)
+
+
+def have_ref() -> bool:
+    return REF_SO.exists()
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise RuntimeError(f"{REF_SO} not built (make -C oracle ref)")
+        L = C.CDLL(str(REF_SO))
+        L.rb2ref_build.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_int, C.c_char_p,
+                                   C.POINTER(RefBvh)]
+        L.rb2ref_build.restype = C.c_int
+        L.rb2ref_load.argtypes = [C.c_char_p, C.POINTER(RefBvh)]
+        L.rb2ref_load.restype = C.c_int
+        L.rb2ref_free.argtypes = [C.POINTER(RefBvh)]
+        L.rb2ref_free.restype = None
+        L.rb2ref_camera_rays.argtypes = [C.c_void_p] * 3 + [C.c_float] * 3 + [C.c_void_p, C.c_uint32, C.c_void_p]
+        L.rb2ref_camera_rays.restype = C.c_int
+        L.rb2ref_intersect_triangle.argtypes = [C.c_void_p] * 5
+        L.rb2ref_intersect_triangle.restype = C.c_int
+        _ref = L
+    return _ref
+
+
+def orc_lib():
+    global _orc
+    if _orc is None:
+        if not ORACLE_SO.exists():
+            raise RuntimeError(f"{ORACLE_SO} not built (make -C oracle oracle)")
+        L = C.CDLL(str(ORACLE_SO))
+        L.rb2o_trace.argtypes = [C.c_void_p] * 4 + [C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.rb2o_trace.restype = None
+        L.rb2o_woop_test.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p]
+        L.rb2o_woop_test.restype = C.c_int
+        L.rb2o_bruteforce.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
+        L.rb2o_bruteforce.restype = None
+        _orc = L
+    return _orc
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _copy_ref(b: RefBvh) -> dict:
+    nodes = np.ctypeslib.as_array(b.nodes, shape=(b.n_nodes * 4,)).copy().reshape(-1, 4)
+    woop = np.ctypeslib.as_array(b.woop, shape=(b.n_woop * 4,)).copy().reshape(-1, 4)
+    triidx = np.ctypeslib.as_array(b.triidx, shape=(b.n_triidx,)).copy()
+    return dict(nodes=nodes, woop=woop, triidx=triidx, sah=float(b.sah), n_inner=int(b.n_inner),
+                n_leaves=int(b.n_leaves), n_tri_refs=int(b.n_tri_refs), build_ms=float(b.build_ms),
+                layout=int(b.layout))
+
+
+def ref_build(vertices, indices, cache_path: str | None = None) -> dict:
+    """The reference SBVH + Compact2 buffers for a triangle soup."""
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+    i = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
+    b = RefBvh()
+    rc = ref_lib().rb2ref_build(_p(v), v.shape[0], _p(i), i.shape[0], 1,
+                                cache_path.encode() if cache_path else None, C.byref(b))
+    if rc != 0:
+        raise RuntimeError(f"reference build failed ({rc})")
+    try:
+        return _copy_ref(b)
+    finally:
+        ref_lib().rb2ref_free(C.byref(b))
+
+
+def ref_load(path: str) -> dict:
+    b = RefBvh()
+    rc = ref_lib().rb2ref_load(str(path).encode(), C.byref(b))
+    if rc != 0:
+        raise RuntimeError(f"reference cache load failed ({rc})")
+    try:
+        return _copy_ref(b)
+    finally:
+        ref_lib().rb2ref_free(C.byref(b))
+
+
+def ref_camera_rays(eye, lookat, up, width, height, fov, raster_xy) -> np.ndarray:
+    xy = np.ascontiguousarray(raster_xy, np.float32).reshape(-1, 2)
+    out = np.empty((xy.shape[0], 8), np.float32)
+    e, l_, u = (np.asarray(x, np.float32) for x in (eye, lookat, up))
+    ref_lib().rb2ref_camera_rays(_p(e), _p(l_), _p(u), float(width), float(height), float(fov), _p(xy),
+                                 xy.shape[0], _p(out))
+    return out
+
+
+def ref_intersect_triangle(v0, v1, v2, ray8):
+    a = [np.ascontiguousarray(x, np.float32) for x in (v0, v1, v2, ray8)]
+    uvt = np.zeros(3, np.float32)
+    hit = ref_lib().rb2ref_intersect_triangle(_p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]), _p(uvt))
+    return bool(hit), uvt
+
+
+def trace(nodes, woop, triidx, rays, any_hit=False, mask=None, counts=False, nthreads=0):
+    """CPU restatement of the reference traversal.  Returns a structured hit
+    array (prim, t, u, v) and, with counts=True, per-ray visit counts."""
+    nodes = np.ascontiguousarray(nodes, np.uint32)
+    woop = np.ascontiguousarray(woop, np.uint32)
+    triidx = np.ascontiguousarray(triidx, np.uint32)
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = rays.shape[0]
+    hits = np.empty(n, HIT_DTYPE)
+    cnt = np.empty(n, COUNT_DTYPE) if counts else None
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+    orc_lib().rb2o_trace(_p(nodes), _p(woop), _p(triidx), _p(rays), n, 1 if any_hit else 0, _p(m), _p(hits),
+                         _p(cnt), int(nthreads))
+    return (hits, cnt) if counts else hits
+
+
+def woop_test(woop_row3, ray8, tmax):
+    w = np.ascontiguousarray(woop_row3, np.uint32).reshape(12)
+    r = np.ascontiguousarray(ray8, np.float32).reshape(8)
+    tuv = np.zeros(3, np.float32)
+    ok = orc_lib().rb2o_woop_test(_p(w), _p(r), float(tmax), _p(tuv))
+    return bool(ok), tuv
+
+
+def bruteforce(woop, triidx, rays, nthreads=0):
+    woop = np.ascontiguousarray(woop, np.uint32)
+    triidx = np.ascontiguousarray(triidx, np.uint32)
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    hits = np.empty(rays.shape[0], HIT_DTYPE)
+    orc_lib().rb2o_bruteforce(_p(woop), _p(triidx), woop.reshape(-1, 4).shape[0], _p(rays), rays.shape[0],
+                              _p(hits), int(nthreads))
+    return hits
+
+
+def woop_slots_of(woop, triidx):
+    """Map from triangle id to its first Woop slot (for tie checks)."""
+    w = np.asarray(woop, np.uint32).reshape(-1, 4)
+    slots = {}
+    s = 0
+    n = w.shape[0]
+    while s < n:
+        if w[s, 0] == 0x80000000:
+            s += 1
+            continue
+        slots.setdefault(int(triidx[s]), s)
+        s += 3
+    return slots
+
+
+def is_tie(woop, triidx, slots, ray8, prim_a, prim_b) -> bool:
+    """True when both triangles accept the ray at the same t (an edge/vertex tie)."""
+    w = np.asarray(woop, np.uint32).reshape(-1, 4)
+    if prim_a < 0 or prim_b < 0:
+        return False
+    sa, sb = slots.get(int(prim_a)), slots.get(int(prim_b))
+    if sa is None or sb is None:
+        return False
+    big = np.float32(3.4028235e38)
+    oka, tuva = woop_test(w[sa:sa + 3], ray8, big)
+    okb, tuvb = woop_test(w[sb:sb + 3], ray8, big)
+    return oka and okb and tuva[0] == tuvb[0]

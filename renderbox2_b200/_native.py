@@ -1,0 +1,112 @@
+"""ctypes bindings for librb2.so (the C ABI declared in include/rb2*.h).
+
+The library is loaded from this package's _lib/ directory.  There is no
+fallback: if the shared object is missing, loading raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_LIB_PATH = Path(__file__).resolve().parent / "_lib" / "librb2.so"
+_lib = None
+
+
+class BuildParams(C.Structure):
+    """rb2_build_params; field meanings follow Platform / BuildParams of the
+    reference (accelerators/sbvh/platform.h:78-90, bvh.h:104-112)."""
+    _fields_ = [
+        ("sah_node_cost", C.c_float), ("sah_triangle_cost", C.c_float),
+        ("min_leaf_size", C.c_uint32), ("max_leaf_size", C.c_uint32),
+        ("split_alpha", C.c_float), ("max_depth", C.c_uint32), ("max_spatial_depth", C.c_uint32),
+        ("spatial_bins", C.c_uint32), ("object_bins", C.c_uint32), ("exact_sweep_max", C.c_uint32),
+        ("num_threads", C.c_int32), ("layout", C.c_uint32),
+    ]
+
+
+class BvhCounts(C.Structure):
+    _fields_ = [
+        ("n_nodes_u4", C.c_uint64), ("n_woop_u4", C.c_uint64), ("n_triidx", C.c_uint64),
+        ("n_inner", C.c_uint32), ("n_leaves", C.c_uint32), ("n_tri_refs", C.c_uint32), ("n_tris", C.c_uint32),
+        ("max_depth", C.c_uint32), ("layout", C.c_uint32), ("sah", C.c_float), ("build_ms", C.c_double),
+    ]
+
+
+class LaunchConfig(C.Structure):
+    _fields_ = [("block_threads", C.c_uint32), ("ctas_per_sm", C.c_uint32),
+                ("fetch_threshold", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class Camera(C.Structure):
+    _fields_ = [
+        ("raster_to_camera", C.c_float * 16), ("camera_to_world", C.c_float * 16),
+        ("width", C.c_uint32), ("height", C.c_uint32),
+        ("eye", C.c_float * 3), ("lookat", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float),
+    ]
+
+
+P = C.c_void_p
+U32 = C.c_uint32
+U64 = C.c_uint64
+I32 = C.c_int
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "rb2_last_error": (C.c_char_p, []),
+    "rb2_version": (C.c_char_p, []),
+    "rb2_build_params_default": (C.c_int, [C.POINTER(BuildParams)]),
+    "rb2_bvh_build": (C.c_int, [P, U32, P, U32, C.POINTER(BuildParams), C.POINTER(P)]),
+    "rb2_bvh_from_buffers": (C.c_int, [P, U64, P, U64, P, U64, C.POINTER(P)]),
+    "rb2_bvh_counts_get": (C.c_int, [P, C.POINTER(BvhCounts)]),
+    "rb2_bvh_nodes": (P, [P]),
+    "rb2_bvh_woop": (P, [P]),
+    "rb2_bvh_triidx": (P, [P]),
+    "rb2_host_bvh_free": (None, [P]),
+    "rb2_bvh_save": (C.c_int, [P, C.c_char_p]),
+    "rb2_bvh_save_text": (C.c_int, [P, C.c_char_p]),
+    "rb2_bvh_load": (C.c_int, [C.c_char_p, C.POINTER(P)]),
+    "rb2_tracer_create": (C.c_int, [P, C.POINTER(P)]),
+    "rb2_tracer_destroy": (C.c_int, [P]),
+    "rb2_tracer_set_launch": (C.c_int, [P, C.POINTER(LaunchConfig)]),
+    "rb2_tracer_device_bytes": (C.c_int, [P, C.POINTER(U64)]),
+    "rb2_trace": (C.c_int, [P, P, U32, I32, P, P, P]),
+    "rb2_trace_host": (C.c_int, [P, P, U32, I32, P, P, P]),
+    "rb2_trace_occlusion": (C.c_int, [P, P, U32, P, P, P]),
+    "rb2_tracer_status": (C.c_int, [P, C.POINTER(U32), P]),
+    "rb2_camera_init": (C.c_int, [C.POINTER(Camera), P, P, P, U32, U32, C.c_float]),
+    "rb2_camera_rays": (C.c_int, [C.POINTER(Camera), U32, U64, I32, P, P]),
+    "rb2_camera_rays_at": (C.c_int, [C.POINTER(Camera), P, U32, P, P]),
+    "rb2_gen_heightfield_counts": (C.c_int, [U32, U32, C.POINTER(U32), C.POINTER(U32)]),
+    "rb2_gen_heightfield": (C.c_int, [U64, U32, C.c_float, U32, C.c_float, C.c_float, P, P]),
+    "rb2_gen_room_counts": (C.c_int, [U32, U32, U32, U32, C.POINTER(U32), C.POINTER(U32)]),
+    "rb2_gen_room": (C.c_int, [U64, U32, U32, U32, C.c_float, C.c_float, U32, P, P, P]),
+    "rb2_gen_surface_rays": (C.c_int, [P, U32, P, U32, U64, U64, C.c_float, C.c_float, P, P]),
+    "rb2_pcg32_fill": (C.c_int, [U64, U64, U32, P]),
+}
+
+
+class Rb2Error(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rb2 error {code}: {msg}")
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    """Returns the loaded librb2 (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise RuntimeError(f"librb2.so not built at {_LIB_PATH}; run `python -m renderbox2_b200.build`")
+        L = C.CDLL(str(_LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        msg = lib().rb2_last_error()
+        raise Rb2Error(rc, msg.decode() if msg else "")

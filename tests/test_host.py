@@ -1,0 +1,190 @@
+"""CPU tests of librb2's host side: C-ABI exports, error behaviour, builder
+edge cases, layout validation and the BVH cache formats."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from parity import golden
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _declared_functions():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(rb2_\w+)\s*\(", text, re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol(rb):
+    names = _declared_functions()
+    assert len(names) > 20
+    out = subprocess.run(["nm", "-D", "--defined-only", str(ROOT / "renderbox2_b200/_lib/librb2.so")],
+                         capture_output=True, text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = sorted(n for n in names if n not in exported)
+    assert not missing, f"declared but not exported: {missing}"
+    L = rb.lib()
+    for n in names:
+        getattr(L, n)
+
+
+def test_errors_are_status_codes(rb):
+    L = rb.lib()
+    h = C.c_void_p()
+    rc = L.rb2_bvh_build(None, 0, None, 5, None, C.byref(h))
+    assert rc == 1 and b"null" in L.rb2_last_error()
+    rc = L.rb2_bvh_load(b"/nonexistent/file.bvh", C.byref(h))
+    assert rc == 4
+    v = np.zeros((3, 3), np.float32)
+    i = np.array([[0, 1, 7]], np.uint32)
+    rc = L.rb2_bvh_build(v.ctypes.data, 3, i.ctypes.data, 1, None, C.byref(h))
+    assert rc == 1 and b"out of range" in L.rb2_last_error()
+
+
+@pytest.mark.parametrize("ntri", [0, 1, 2, 5])
+def test_build_tiny_inputs(rb, orc, ntri):
+    rng = np.random.Generator(np.random.PCG64(ntri))
+    v = rng.uniform(0, 1, size=(3 * ntri, 3)).astype(np.float32)
+    i = np.arange(3 * ntri, dtype=np.uint32).reshape(-1, 3)
+    b = rb.BVH(rb.Scene().add_mesh(v, i))
+    st = b.stats()
+    assert st["n_inner"] >= 1 and st["n_nodes_u4"] % 4 == 0
+    rays = np.zeros((64, 8), np.float32)
+    rays[:, 0:3] = rng.uniform(-1, 2, size=(64, 3))
+    d = rng.normal(size=(64, 3))
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 7] = 1e30
+    h = orc.trace(b.get_node_buffer(), b.get_tri_woop_buffer(), b.get_tri_index_buffer(), rays)
+    bf = orc.bruteforce(b.get_tri_woop_buffer(), b.get_tri_index_buffer(), rays)
+    assert np.array_equal(h["prim"], bf["prim"])
+
+
+def test_degenerate_and_duplicate_triangles(rb, orc):
+    s = rb.heightfield_scene(seed=5, grid_n=8, n_boxes=2)
+    v = np.concatenate([s.vertices, np.array([[0.3, 0.5, 0.3], [0.3, 0.5, 0.3], [0.3, 0.5, 0.3]], np.float32)])
+    n0 = s.vertices.shape[0]
+    extra = np.array([[n0, n0 + 1, n0 + 2], [0, 1, 2]], np.uint32)  # a point triangle and a duplicate
+    i = np.concatenate([s.indices, extra])
+    b = rb.BVH(rb.Scene().add_mesh(v, i))
+    tri = set(b.get_tri_index_buffer()[b.get_tri_woop_buffer()[:, 0] != 0x80000000].tolist())
+    assert (i.shape[0] - 2) not in tri  # degenerate (point) triangle removed, as the reference does
+    rays, _ = rb.surface_rays(s, seed=6, n=4000)
+    h = orc.trace(b.get_node_buffer(), b.get_tri_woop_buffer(), b.get_tri_index_buffer(), rays)
+    bf = orc.bruteforce(b.get_tri_woop_buffer(), b.get_tri_index_buffer(), rays)
+    assert np.array_equal(h["t"].view(np.uint32), bf["t"].view(np.uint32))
+
+
+def test_builder_deterministic_across_thread_counts(rb):
+    s = rb.heightfield_scene(seed=8, grid_n=200, n_boxes=32)
+    b1 = rb.BVH(s, params=rb.BuildParams(num_threads=1))
+    b8 = rb.BVH(s, params=rb.BuildParams(num_threads=8))
+    assert np.array_equal(b1.get_node_buffer(), b8.get_node_buffer())
+    assert np.array_equal(b1.get_tri_woop_buffer(), b8.get_tri_woop_buffer())
+
+
+def test_spatial_splits_duplicate_long_triangles(rb, orc):
+    # Long thin diagonal triangles overlap heavily: the SBVH should split some.
+    rng = np.random.Generator(np.random.PCG64(3))
+    n = 400
+    a = rng.uniform(0, 1, size=(n, 3)).astype(np.float32)
+    b_ = (a + rng.normal(scale=0.5, size=(n, 3))).astype(np.float32)
+    c = (a + rng.normal(scale=0.01, size=(n, 3))).astype(np.float32)
+    v = np.stack([a, b_, c], 1).reshape(-1, 3)
+    i = np.arange(3 * n, dtype=np.uint32).reshape(-1, 3)
+    bvh = rb.BVH(rb.Scene().add_mesh(v, i))
+    assert bvh.stats()["n_tri_refs"] > n
+    rays = np.zeros((5000, 8), np.float32)
+    rays[:, 0:3] = rng.uniform(-0.5, 1.5, size=(5000, 3))
+    d = rng.normal(size=(5000, 3))
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 7] = 1e30
+    h = orc.trace(bvh.get_node_buffer(), bvh.get_tri_woop_buffer(), bvh.get_tri_index_buffer(), rays)
+    bf = orc.bruteforce(bvh.get_tri_woop_buffer(), bvh.get_tri_index_buffer(), rays)
+    assert np.array_equal(h["t"].view(np.uint32), bf["t"].view(np.uint32))
+
+
+def test_validation_rejects_corrupt_layouts(rb):
+    g = golden()
+    nodes, woop, tri = g["ref_nodes"].copy(), g["ref_woop"].copy(), g["ref_triidx"].copy()
+    rb.BVH.from_buffers(nodes, woop, tri)  # valid
+    bad = nodes.copy()
+    bad[3, 0] = 4 * (nodes.shape[0] // 4 + 10)  # child index past the end
+    with pytest.raises(rb.Rb2Error):
+        rb.BVH.from_buffers(bad, woop, tri)
+    cyc = nodes.copy()
+    cyc[3, 0] = 0  # root as its own child
+    with pytest.raises(rb.Rb2Error):
+        rb.BVH.from_buffers(cyc, woop, tri)
+    unterminated = woop.copy()
+    unterminated[unterminated[:, 0] == 0x80000000] = 0
+    with pytest.raises(rb.Rb2Error):
+        rb.BVH.from_buffers(nodes, unterminated, tri)
+    with pytest.raises(rb.Rb2Error):
+        rb.BVH.from_buffers(nodes[:5], woop, tri)
+
+
+def test_binary_cache_round_trip(rb, tmp_path):
+    s = rb.heightfield_scene(seed=9, grid_n=24, n_boxes=4)
+    b = rb.BVH(s)
+    p = tmp_path / "a.rb2bvh"
+    b.serialize(str(p))
+    c = rb.BVH.load(str(p))
+    assert np.array_equal(b.get_node_buffer(), c.get_node_buffer())
+    assert np.array_equal(b.get_tri_woop_buffer(), c.get_tri_woop_buffer())
+    assert np.array_equal(b.get_tri_index_buffer(), c.get_tri_index_buffer())
+    assert c.stats()["sah"] == b.stats()["sah"]
+    raw = bytearray(p.read_bytes())
+    raw[-5] ^= 0xFF
+    p.write_bytes(bytes(raw))
+    with pytest.raises(rb.Rb2Error) as e:
+        rb.BVH.load(str(p))
+    assert e.value.code == 5
+    p.write_bytes(bytes(raw[:100]))
+    with pytest.raises(rb.Rb2Error):
+        rb.BVH.load(str(p))
+
+
+def test_reads_reference_text_cache(rb):
+    """The reference's own serialize() output (fixture) loads into rb2."""
+    g = golden()
+    c = rb.BVH.load(str(ROOT / "tests/golden/ref_cache_small.txt"))
+    assert np.array_equal(c.get_node_buffer(), g["ref_nodes"])
+    assert np.array_equal(c.get_tri_woop_buffer(), g["ref_woop"])
+    assert np.array_equal(c.get_tri_index_buffer(), g["ref_triidx"])
+
+
+def test_reference_reads_rb2_text_cache(rb, orc, tmp_path):
+    if not orc.have_ref():
+        pytest.skip("reference sources not compiled here")
+    s = rb.heightfield_scene(seed=10, grid_n=12, n_boxes=2)
+    b = rb.BVH(s)
+    p = tmp_path / "x.txt"
+    b.serialize_text(str(p))
+    r = orc.ref_load(str(p))
+    assert np.array_equal(r["nodes"], b.get_node_buffer())
+    assert np.array_equal(r["woop"], b.get_tri_woop_buffer())
+    assert np.array_equal(r["triidx"], b.get_tri_index_buffer())
+
+
+def test_generators_are_seeded(rb):
+    a = rb.heightfield_scene(seed=3, grid_n=16, n_boxes=4)
+    b = rb.heightfield_scene(seed=3, grid_n=16, n_boxes=4)
+    c = rb.heightfield_scene(seed=4, grid_n=16, n_boxes=4)
+    assert np.array_equal(a.vertices, b.vertices) and not np.array_equal(a.vertices, c.vertices)
+    assert a.num_triangles == 2 * 16 * 16 + 12 * 4
+    r1, f1 = rb.surface_rays(a, seed=1, n=1000)
+    r2, f2 = rb.surface_rays(a, seed=1, n=1000)
+    assert np.array_equal(r1, r2) and np.array_equal(f1, f2)
+    assert 0.4 < f1.mean() < 0.6
+    d = r1[:, 4:7]
+    assert np.allclose(np.linalg.norm(d, axis=1), 1.0, atol=1e-5)
+    room = rb.RoomScene(seed=2, n_boxes=3, n_spheres=5, sphere_subdiv=2, n_lights=2)
+    assert room.num_lights == 4
+    assert room.emission[room.material_ids[room.light_ids_to_primitive_ids]].min() == 10.0

@@ -1,0 +1,153 @@
+"""CPU tests of the oracle against the reference's own compiled code and the
+golden fixtures, and of the rb2 builder/packer against the reference's."""
+import numpy as np
+import pytest
+
+from parity import golden
+
+
+def test_oracle_reproduces_golden_hits(orc):
+    g = golden()
+    ch, cnt = orc.trace(g["ref_nodes"], g["ref_woop"], g["ref_triidx"], g["rays"], counts=True, nthreads=1)
+    assert np.array_equal(ch["prim"], g["ch_prim"])
+    for k in ("t", "u", "v"):
+        assert np.array_equal(ch[k].view(np.uint32), g["ch_" + k].view(np.uint32))
+    assert np.array_equal(cnt["nodes"], g["ch_nodes"])
+    assert np.array_equal(cnt["tris"], g["ch_tris"])
+    assert np.array_equal(cnt["leafterms"], g["ch_terms"])
+    ah = orc.trace(g["ref_nodes"], g["ref_woop"], g["ref_triidx"], g["rays"], any_hit=True, nthreads=1)
+    assert np.array_equal(ah["prim"] >= 0, g["ah_prim"] >= 0)
+    assert int((g["ch_prim"] >= 0).sum()) > 300  # fixture exercises real hits
+
+
+def test_oracle_equals_bruteforce(orc):
+    g = golden()
+    ch = orc.trace(g["ref_nodes"], g["ref_woop"], g["ref_triidx"], g["rays"])
+    bf = orc.bruteforce(g["ref_woop"], g["ref_triidx"], g["rays"])
+    assert np.array_equal(ch["prim"], bf["prim"])
+    assert np.array_equal(ch["t"].view(np.uint32), bf["t"].view(np.uint32))
+
+
+def test_oracle_agrees_with_reference_moller_trumbore():
+    g = golden()
+    hit = g["ch_prim"] >= 0
+    # The reference's own host triangle test (core/primitives.cu:51-70) accepts
+    # every triangle the traversal reports.  Moller-Trumbore and the Woop
+    # transform are different fp32 formulas for the same distance, so they
+    # agree to a few ulps of the scene scale (1.0), not bit for bit.
+    assert g["mt_hit"][hit].all()
+    t_mt = g["mt_uvt"][hit, 2]
+    t_tr = g["ch_t"][hit]
+    assert np.all(np.abs(t_mt - t_tr) <= 1e-5 * np.abs(t_tr) + 4e-6)
+
+
+def test_anyhit_iff_closest_hit(orc):
+    g = golden()
+    assert np.array_equal(g["ah_prim"] >= 0, g["ch_prim"] >= 0)
+
+
+def test_reference_build_is_reproducible(orc):
+    if not orc.have_ref():
+        pytest.skip("reference sources not compiled here")
+    g = golden()
+    ref = orc.ref_build(g["vertices"], g["indices"])
+    assert np.array_equal(ref["nodes"], g["ref_nodes"])
+    assert np.array_equal(ref["woop"], g["ref_woop"])
+    assert np.array_equal(ref["triidx"], g["ref_triidx"])
+
+
+def _woop_by_tri(woop, triidx):
+    w = np.asarray(woop, np.uint32).reshape(-1, 4)
+    out, s = {}, 0
+    while s < w.shape[0]:
+        if w[s, 0] == 0x80000000:
+            s += 1
+            continue
+        out.setdefault(int(triidx[s]), w[s:s + 3].copy())
+        s += 3
+    return out
+
+
+def test_rb2_woop_rows_bit_equal_reference_fixture(rb):
+    g = golden()
+    sc = rb.Scene().add_mesh(g["vertices"], g["indices"])
+    b = rb.BVH(sc)
+    mine = _woop_by_tri(b.get_tri_woop_buffer(), b.get_tri_index_buffer())
+    ref = _woop_by_tri(g["ref_woop"], g["ref_triidx"])
+    assert set(mine) == set(ref)
+    assert all(np.array_equal(mine[k], ref[k]) for k in ref)
+
+
+@pytest.mark.parametrize("kind", ["heightfield", "room"])
+def test_rb2_woop_rows_bit_equal_reference_builder(rb, orc, kind):
+    if not orc.have_ref():
+        pytest.skip("reference sources not compiled here")
+    if kind == "heightfield":
+        sc = rb.heightfield_scene(seed=21, grid_n=40, n_boxes=12)
+    else:
+        sc = rb.RoomScene(seed=22, n_boxes=6, n_spheres=12, sphere_subdiv=1)
+    ref = orc.ref_build(sc.vertices, sc.indices)
+    b = rb.BVH(sc)
+    mine = _woop_by_tri(b.get_tri_woop_buffer(), b.get_tri_index_buffer())
+    theirs = _woop_by_tri(ref["woop"], ref["triidx"])
+    assert set(mine) == set(theirs)
+    assert all(np.array_equal(mine[k], theirs[k]) for k in theirs)
+    # SAH quality at least on par with the reference's builder.
+    assert b.stats()["sah"] <= ref["sah"] * 1.05
+
+
+def test_rb2_tree_gives_reference_hits(rb, orc):
+    from parity import compare_closest
+    g = golden()
+    sc = rb.Scene().add_mesh(g["vertices"], g["indices"])
+    b = rb.BVH(sc)
+    mine = orc.trace(b.get_node_buffer(), b.get_tri_woop_buffer(), b.get_tri_index_buffer(), g["rays"])
+    ref = {"prim": g["ch_prim"], "t": g["ch_t"], "u": g["ch_u"], "v": g["ch_v"]}
+    as_dev = np.stack([mine["prim"], mine["t"].view(np.int32), mine["u"].view(np.int32), mine["v"].view(np.int32)], 1)
+    ties, bad, first = compare_closest(orc, as_dev, ref, g["ref_woop"], g["ref_triidx"], g["rays"])
+    assert bad == 0, f"ray {first} differs beyond a tie"
+
+
+def test_camera_matrices_reproduce_reference_rays(rb):
+    """Host camera set-up: applying rb2's matrices with IEEE single ops in the
+    device kernel's order reproduces the reference camera's rays bit-exactly."""
+    from renderbox2_b200.configs import CONFIG1 as C1
+    g = golden()
+    cam = rb.PerspectiveCamera(C1["eye"], C1["lookat"], C1["up"], (C1["width"], C1["height"]), C1["fov"])
+    r2c = np.array(cam.c.raster_to_camera, np.float32).reshape(4, 4)
+    c2w = np.array(cam.c.camera_to_world, np.float32).reshape(4, 4)
+    f = np.float32
+
+    def row(m, i, x, y, z, w):
+        return ((m[i, 0] * x + m[i, 1] * y) + m[i, 2] * z) + m[i, 3] * w
+
+    xy = g["cam_xy"]
+    x, y = xy[:, 0].astype(f), xy[:, 1].astype(f)
+    z0, one = np.zeros_like(x), np.ones_like(x)
+    px, py, pz, pw = (row(r2c, i, x, y, z0, one) for i in range(4))
+    px, py, pz = px / pw, py / pw, pz / pw
+    inv = f(1.0) / np.sqrt((px * px + py * py) + pz * pz)
+    dx, dy, dz = px * inv, py * inv, pz * inv
+    ow = row(c2w, 3, z0, z0, z0, one)
+    o = [row(c2w, i, z0, z0, z0, one) / ow for i in range(3)]
+    d = [row(c2w, i, dx, dy, dz, z0) for i in range(3)]
+    mine = np.stack([o[0], o[1], o[2], z0, d[0], d[1], d[2], np.full_like(x, np.finfo(f).max)], 1)
+    assert np.array_equal(mine.view(np.uint32), g["cam_rays"].view(np.uint32))
+
+
+def test_pcg32_matches_oracle_restatement(rb, orc):
+    import ctypes as C
+    L = orc.orc_lib()
+
+    class Pcg(C.Structure):
+        _fields_ = [("state", C.c_uint64), ("inc", C.c_uint64)]
+
+    L.rb2o_pcg32_seed.argtypes = [C.POINTER(Pcg), C.c_uint64, C.c_uint64]
+    L.rb2o_pcg32_next.restype = C.c_uint32
+    L.rb2o_pcg32_next.argtypes = [C.POINTER(Pcg)]
+    r = Pcg()
+    L.rb2o_pcg32_seed(C.byref(r), 42, 54)
+    ref = np.array([L.rb2o_pcg32_next(C.byref(r)) for _ in range(6)], np.uint32)
+    assert np.array_equal(rb.pcg32(42, 54, 6), ref)
+    # O'Neill's published demo sequence for seed 42, stream 54.
+    assert ref[0] == 0xA15C02B7 and ref[1] == 0x7B47F409
