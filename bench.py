@@ -1,0 +1,400 @@
+"""Benchmark: incoherent ray-query throughput on one B200 (config 4 workload).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl rb2|reference]
+                  [--mode plain|batched] [--rays-per-scene R] [--scenes S]
+
+One step = every scene's ray batch traced once: 64 heightfield scenes with
+log-uniform 1k..2M triangles, 1M incoherent diffuse-bounce rays per scene,
+50 % closest-hit and 50 % any-hit (occlusion).  Inputs are resident in HBM
+when the timed region starts; L2 is flushed (256 MB write) between timed
+steps.  `e2e` repeats the step through the host-buffer C-ABI call
+(rb2_trace_host), copies included.  Under torchrun each rank runs the same
+workload on its own GPU (replicas, no collective); `value` = all ranks' rays
+/ max-over-ranks time.
+
+--impl reference times the CPU restatement of the reference traversal (the
+reference has no host traversal of its own) on all host cores over a bounded
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s incoherent closest-hit; served-job p50/p99 vs plain launches, 1 B200"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------------------- workload
+def build_workload(n_scenes: int, rays_per_scene: int, seed_base: int = 4):
+    import renderbox2_b200 as rb
+    from renderbox2_b200.configs import CONFIG4, config4_triangle_counts
+    counts = config4_triangle_counts(dict(CONFIG4, n_scenes=64))[:n_scenes]
+    scenes = []
+    t0 = time.time()
+    build_s = 0.0
+    for k, tris in enumerate(counts):
+        sc = rb.heightfield_for_triangles(seed=seed_base * 1000 + k, n_tris=tris)
+        tb = time.time()
+        bvh = rb.BVH(sc)
+        build_s += time.time() - tb
+        rays, flags = rb.surface_rays(sc, seed=seed_base * 1000 + 500 + k, n=rays_per_scene,
+                                      offset_scale=CONFIG4["offset_scale"],
+                                      anyhit_fraction=CONFIG4["anyhit_fraction"])
+        order = np.argsort(flags, kind="stable")  # closest-hit rays first, then any-hit
+        rays = np.ascontiguousarray(rays[order])
+        n_ch = int((flags == 0).sum())
+        scenes.append(dict(scene=sc, bvh=bvh, rays=rays, n_ch=n_ch, tris=sc.num_triangles))
+    log(f"workload: {n_scenes} scenes, {sum(s['tris'] for s in scenes):,} triangles, "
+        f"{n_scenes * rays_per_scene:,} rays; build {build_s:.1f}s, total setup {time.time() - t0:.1f}s")
+    return scenes, build_s
+
+
+def oracle_bytes_sample(scenes, per_scene: int, nthreads: int = 0):
+    """Canonical single-lane visit counts of the oracle on a sample of each
+    scene's rays -> mean algorithmic bytes per ray, per mode and scene."""
+    import oracle
+    out = []
+    t_cpu = 0.0
+    n_cpu = 0
+    for s in scenes:
+        nodes, woop, tri = s["bvh"].buffers_view()
+        res = {}
+        for mode, sl in (("ch", slice(0, s["n_ch"])), ("ah", slice(s["n_ch"], None))):
+            r = s["rays"][sl]
+            idx = np.linspace(0, r.shape[0] - 1, min(per_scene, r.shape[0])).astype(np.int64)
+            t0 = time.perf_counter()
+            _, cnt = oracle.trace(nodes, woop, tri, r[idx], any_hit=(mode == "ah"), counts=True, nthreads=nthreads)
+            t_cpu += time.perf_counter() - t0
+            n_cpu += idx.size
+            out_b = 16 if mode == "ch" else 1
+            bpr = 32 + 64 * cnt["nodes"].astype(np.float64) + 48 * cnt["tris"] + 16 * cnt["leafterms"] + out_b
+            res[mode] = dict(bytes_per_ray=float(bpr.mean()), nodes=float(cnt["nodes"].mean()),
+                             tris=float(cnt["tris"].mean()))
+        out.append(res)
+    return out, (n_cpu / t_cpu / 1e6 if t_cpu > 0 else 0.0), n_cpu, t_cpu
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = [r.split(",") for r in self.path.read_text().splitlines() if r.strip()]
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------- GPU arm
+def run_rb2(args, rank, world, local_rank):
+    import torch
+    import renderbox2_b200 as rb
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    scenes, build_s = build_workload(args.scenes, args.rays_per_scene)
+    total_rays = sum(s["rays"].shape[0] for s in scenes)
+    tracers, d_rays, d_hits, d_occ = [], [], [], []
+    for s in scenes:
+        tracers.append(rb.CudaTracer(s["bvh"]))
+        d_rays.append(torch.from_numpy(s["rays"]).to(dev))
+        d_hits.append(torch.empty((s["n_ch"], 4), dtype=torch.int32, device=dev))
+        d_occ.append(torch.empty((s["rays"].shape[0] - s["n_ch"],), dtype=torch.uint8, device=dev))
+    bvh_bytes = sum(t.device_bytes() for t in tracers)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(2)]
+          for _ in scenes]
+
+    def step(record: bool):
+        with torch.cuda.stream(stream):
+            for k, s in enumerate(scenes):
+                tr, r = tracers[k], d_rays[k]
+                if record:
+                    ev[k][0][0].record(stream)
+                tr.trace(r[: s["n_ch"]], any_hit=False, out=d_hits[k], stream=stream)
+                if record:
+                    ev[k][0][1].record(stream)
+                    ev[k][1][0].record(stream)
+                tr.trace_occlusion(r[s["n_ch"]:], out=d_occ[k], stream=stream)
+                if record:
+                    ev[k][1][1].record(stream)
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize(dev)
+    launches_per_step = 2 * len(scenes)
+
+    barrier(world)
+    step_ms, ch_ms, ah_ms = [], np.zeros(len(scenes)), np.zeros(len(scenes))
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        for it in range(args.steps):
+            flush.fill_(float(it))  # evict L2 between timed steps (outside the timed region)
+            torch.cuda.synchronize(dev)
+            t_start.record(stream)
+            step(True)
+            t_end.record(stream)
+            torch.cuda.synchronize(dev)
+            step_ms.append(t_start.elapsed_time(t_end))
+            for k in range(len(scenes)):
+                ch_ms[k] += ev[k][0][0].elapsed_time(ev[k][0][1])
+                ah_ms[k] += ev[k][1][0].elapsed_time(ev[k][1][1])
+    clocks = clk.summary()
+    total_ms = float(sum(step_ms))
+    total_ms = max_over_ranks(total_ms, world, dev)
+    for t in tracers:
+        assert t.status() == 0, "device status word set"
+
+    # ---- e2e through the host-buffer C-ABI call (pinned host memory).
+    h_rays = [torch.from_numpy(s["rays"]).pin_memory() for s in scenes]
+    h_hits = [torch.empty((s["rays"].shape[0], 4), dtype=torch.int32).pin_memory() for s in scenes]
+    import ctypes as C
+    from renderbox2_b200._native import check, lib
+    L = lib()
+    sh = stream.cuda_stream
+
+    def e2e_step():
+        for k, s in enumerate(scenes):
+            n_ch = s["n_ch"]
+            hr, hh = h_rays[k], h_hits[k]
+            check(L.rb2_trace_host(tracers[k].handle, hr.data_ptr(), n_ch, 0, None, hh.data_ptr(), sh))
+            check(L.rb2_trace_host(tracers[k].handle, hr.data_ptr() + 32 * n_ch, s["rays"].shape[0] - n_ch, 1, None,
+                                   hh.data_ptr() + 16 * n_ch, sh))
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    e2e_steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    e2e_ms = max_over_ranks(e2e_ms, world, dev)
+
+    # ---- roofline inputs: oracle counts on a sample (CPU), dominant kernel = closest hit.
+    per_scene_sample = 4096
+    bytes_info, cpu_mrays, n_cpu, t_cpu = oracle_bytes_sample(scenes, per_scene_sample)
+    ch_bytes = sum(bi["ch"]["bytes_per_ray"] * s["n_ch"] for bi, s in zip(bytes_info, scenes))
+    ah_bytes = sum(bi["ah"]["bytes_per_ray"] * (s["rays"].shape[0] - s["n_ch"]) for bi, s in zip(bytes_info, scenes))
+    ch_time_s = ch_ms.sum() / 1e3 / args.steps
+    ah_time_s = ah_ms.sum() / 1e3 / args.steps
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = ch_bytes / ch_time_s / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "trace_ch_traffic.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get("traffic_per_launch_bytes")
+        except (ValueError, OSError):
+            traffic = None
+
+    # ---- CPU baseline: oracle on host cores over a bounded sample (rank 0, N=1 only).
+    cpu_baseline = None
+    if rank == 0 and world == 1:
+        cpu_baseline = cpu_baseline_run(scenes, args.cpu_sample_s)
+
+    value = world * total_rays * args.steps / (total_ms / 1e3) / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG32 scenes and rays)",
+        "config": {
+            "workload": "config 4: 64 heightfield scenes, log-uniform 1k..2M triangles, 1M incoherent "
+                        "diffuse-bounce rays per scene, 50% closest-hit / 50% any-hit (occlusion)",
+            "mode": "plain per-scene launches (2 per scene)",
+            "scenes": len(scenes), "triangles": int(sum(s["tris"] for s in scenes)),
+            "rays_per_step": int(total_rays), "l2": "flushed (256 MB write) between timed steps",
+            "bvh_device_bytes": int(bvh_bytes), "build_s_host": round(build_s, 2), "parallelism": "replicas",
+        },
+        "closest_hit_mrays": round(sum(s["n_ch"] for s in scenes) / ch_time_s / 1e6, 2),
+        "any_hit_mrays": round(sum(s["rays"].shape[0] - s["n_ch"] for s in scenes) / ah_time_s / 1e6, 2),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
+                     "kernel": "k_trace<closest>", "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
+                     "alg_bytes_per_ray": round(ch_bytes / sum(s["n_ch"] for s in scenes), 1)},
+        "e2e": {"value": round(world * total_rays * e2e_steps / (e2e_ms / 1e3) / 1e6, 2), "unit": "Mrays/s",
+                "h2d_bytes_per_step": int(total_rays * 32), "d2h_bytes_per_step": int(total_rays * 16)},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks,
+    }
+    if cpu_baseline is not None:
+        line["cpu_baseline"] = cpu_baseline
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_run(scenes, budget_s: float):
+    """Oracle traversal on all host cores over a bounded sample: equal share of
+    each scene's closest-hit and any-hit rays, sized to ~budget_s seconds."""
+    import oracle
+    cores = os.cpu_count() or 1
+    # Calibrate on a small sample, then size the measured sample to the budget.
+    per = 512
+    for _ in range(2):
+        t0 = time.perf_counter()
+        n = trace_sample(oracle, scenes, per)
+        dt = time.perf_counter() - t0
+        if dt > 0.5:
+            break
+        per *= 4
+    rate = n / dt
+    per = int(max(256, min(scenes[0]["rays"].shape[0] // 2, per * budget_s / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    n = trace_sample(oracle, scenes, per)
+    dt = time.perf_counter() - t0
+    return {"value": round(n / dt / 1e6, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
+            "sample": f"{per} closest-hit + {per} any-hit rays from each of {len(scenes)} scenes "
+                      f"({n:,} rays, {dt:.1f}s), oracle C restatement, OpenMP over {cores} threads"}
+
+
+def trace_sample(oracle, scenes, per):
+    n = 0
+    for s in scenes:
+        nodes, woop, tri = s["bvh"].buffers_view()
+        ch = s["rays"][: min(per, s["n_ch"])]
+        ah = s["rays"][s["n_ch"]: s["n_ch"] + per]
+        oracle.trace(nodes, woop, tri, ch, any_hit=False)
+        oracle.trace(nodes, woop, tri, ah, any_hit=True)
+        n += ch.shape[0] + ah.shape[0]
+    return n
+
+
+# ------------------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    scenes, _ = build_workload(args.scenes, args.rays_per_scene)
+    import oracle
+    cores = os.cpu_count() or 1
+    per = max(256, args.ref_rays_per_scene)
+    for _ in range(args.warmup):
+        trace_sample(oracle, scenes, min(per, 256))
+    times, n = [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        n = trace_sample(oracle, scenes, per)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = n * args.steps / tot / 1e6
+    sample = (f"{per} closest-hit + {per} any-hit rays from each of {len(scenes)} scenes per step "
+              f"({n:,} rays), CPU restatement of the reference traversal (the reference has no host "
+              f"traversal), OpenMP over {cores} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "config 4: 64 heightfield scenes, log-uniform 1k..2M triangles, incoherent "
+                               "diffuse-bounce rays, 50% closest-hit / 50% any-hit", "parallelism": "host cores"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------- dist glue
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world, dev) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["rb2", "reference"], default="rb2")
+    ap.add_argument("--scenes", type=int, default=64)
+    ap.add_argument("--rays-per-scene", type=int, default=1 << 20)
+    ap.add_argument("--ref-rays-per-scene", type=int, default=2048)
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        if args.impl == "rb2":
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl" if args.impl == "rb2" else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_rb2(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

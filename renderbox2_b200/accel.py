@@ -164,12 +164,21 @@ class BVH:
         c = self.counts()
         return {k: getattr(c, k) for k, _ in BvhCounts._fields_}
 
-    def _buf(self, getter, n, cols):
+    def _buf(self, getter, n, cols, copy=True):
         ptr = getter(self._h)
         if n == 0:
             return np.zeros((0, cols) if cols > 1 else (0,), np.uint32)
-        arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint32)), shape=(n * cols,)).copy()
+        arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint32)), shape=(n * cols,))
+        if copy:
+            arr = arr.copy()
         return arr.reshape(-1, cols) if cols > 1 else arr
+
+    def buffers_view(self):
+        """Zero-copy (nodes, woop, triidx) views; valid while this BVH lives."""
+        c = self.counts()
+        L = lib()
+        return (self._buf(L.rb2_bvh_nodes, c.n_nodes_u4, 4, False), self._buf(L.rb2_bvh_woop, c.n_woop_u4, 4, False),
+                self._buf(L.rb2_bvh_triidx, c.n_triidx, 1, False))
 
     # CudaBvh getters (cudabvh.h:95-97)
     def get_node_buffer(self) -> np.ndarray:
