@@ -117,11 +117,18 @@ typedef struct {
 /* Launch configuration of the persistent traversal kernel.  Zero fields mean
  * "use the tuned default". */
 typedef struct {
-    uint32_t block_threads;     /* threads per CTA (multiple of 32) */
-    uint32_t ctas_per_sm;       /* resident CTAs per SM */
-    uint32_t fetch_threshold;   /* refill a warp when fewer lanes stay busy */
+    uint32_t block_threads;     /* threads per CTA: 64, 128 or 256 */
+    uint32_t ctas_per_sm;       /* resident CTAs per SM (0 = occupancy maximum) */
+    uint32_t fetch_threshold;   /* refill a warp when fewer lanes stay busy (reference: 20) */
     uint32_t reserved;
 } rb2_launch_config;
+
+/* Inner-node order of the uploaded Compact2 buffer: the reference's DFS
+ * order (cudabvh.cpp:234-288) or breadth-first (top levels contiguous). */
+enum { RB2_NODE_ORDER_DFS = 0, RB2_NODE_ORDER_BFS = 1 };
+
+/* Ray-query modes. */
+enum { RB2_MODE_CLOSEST = 0, RB2_MODE_ANY = 1, RB2_MODE_OCCLUSION = 2 };
 
 /* Uploads the BVH to the current CUDA device.  The tracer owns that memory. */
 int rb2_tracer_create(const rb2_host_bvh* bvh, rb2_tracer** out);
@@ -148,6 +155,53 @@ int rb2_trace_occlusion(rb2_tracer* t, const float* d_rays, uint32_t n, const ui
 /* Device-side status word of the tracer (0 = clean).  Non-zero means a kernel
  * hit a guard (stack overflow on a corrupt tree, bad index) and skipped work. */
 int rb2_tracer_status(rb2_tracer* t, uint32_t* status, void* stream);
+
+/* Re-uploads the tracer's nodes in another order (RB2_NODE_ORDER_*); results
+ * are unchanged, only memory locality differs.  Synchronises the device. */
+int rb2_tracer_set_node_order(rb2_tracer* t, uint32_t order);
+
+/* -------------------------------------------------------------- batching --
+ * Many scenes and ray batches of uneven size in ONE persistent launch: every
+ * job's rays are served from a single global queue, so warps move between
+ * scenes without a kernel boundary.  No reference counterpart (the reference
+ * traces one RayBuffer per CudaTracer::trace call, cudatracer.cu:134-183). */
+typedef struct {
+    rb2_tracer* tracer;       /* scene (its device BVH) */
+    const float* d_rays;      /* 2 float4 per ray, 16-byte aligned */
+    uint64_t n;
+    uint32_t mode;            /* RB2_MODE_* */
+    uint32_t reserved;
+    const uint8_t* d_mask;    /* nullable stencil */
+    void* d_out;              /* rb2_hit[n] (closest/any) or uint8_t[n] (occlusion) */
+} rb2_trace_job;
+
+typedef struct {
+    uint32_t block_threads;   /* 64, 128, 256 (0 = 128) */
+    uint32_t ctas_per_sm;     /* 0 = occupancy maximum */
+    uint32_t fetch_threshold; /* 0 = 20 */
+    uint32_t chunk;           /* queue chunk: a warp reserves chunk*32 rays per atomic (0/1 = exact) */
+    uint32_t node_order;      /* RB2_NODE_ORDER_*; applied to every tracer in the batch */
+    uint32_t reserved;
+} rb2_batch_config;
+
+typedef struct rb2_batch rb2_batch;
+
+/* Uploads the job table; buffers are borrowed and must outlive the batch. */
+int rb2_batch_create(const rb2_trace_job* jobs, uint32_t n_jobs, rb2_batch** out);
+int rb2_batch_destroy(rb2_batch* b);
+int rb2_batch_set_config(rb2_batch* b, const rb2_batch_config* cfg);
+int rb2_batch_get_config(const rb2_batch* b, rb2_batch_config* cfg);
+/* Queue reset + one persistent kernel; replays the captured graph if any. */
+int rb2_batch_launch(rb2_batch* b, void* stream);
+/* Captures the launch (queue reset + kernel) into a CUDA graph on `stream`
+ * (must be a non-default stream); later rb2_batch_launch calls replay it.
+ * Changing the config drops the graph. */
+int rb2_batch_capture(rb2_batch* b, void* stream);
+int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream);
+/* Times candidate configs (coordinate descent over node order, block shape,
+ * CTAs per SM, fetch threshold and queue chunk; median of `reps` launches
+ * each), applies and returns the fastest. */
+int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best, double* best_ms);
 
 #ifdef __cplusplus
 }

@@ -37,6 +37,16 @@ class LaunchConfig(C.Structure):
                 ("fetch_threshold", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class TraceJob(C.Structure):
+    _fields_ = [("tracer", C.c_void_p), ("d_rays", C.c_void_p), ("n", C.c_uint64), ("mode", C.c_uint32),
+                ("reserved", C.c_uint32), ("d_mask", C.c_void_p), ("d_out", C.c_void_p)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("block_threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("fetch_threshold", C.c_uint32),
+                ("chunk", C.c_uint32), ("node_order", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class Camera(C.Structure):
     _fields_ = [
         ("raster_to_camera", C.c_float * 16), ("camera_to_world", C.c_float * 16),
@@ -73,6 +83,15 @@ SIGNATURES = {
     "rb2_trace_host": (C.c_int, [P, P, U32, I32, P, P, P]),
     "rb2_trace_occlusion": (C.c_int, [P, P, U32, P, P, P]),
     "rb2_tracer_status": (C.c_int, [P, C.POINTER(U32), P]),
+    "rb2_tracer_set_node_order": (C.c_int, [P, U32]),
+    "rb2_batch_create": (C.c_int, [C.POINTER(TraceJob), U32, C.POINTER(P)]),
+    "rb2_batch_destroy": (C.c_int, [P]),
+    "rb2_batch_set_config": (C.c_int, [P, C.POINTER(BatchConfig)]),
+    "rb2_batch_get_config": (C.c_int, [P, C.POINTER(BatchConfig)]),
+    "rb2_batch_launch": (C.c_int, [P, P]),
+    "rb2_batch_capture": (C.c_int, [P, P]),
+    "rb2_batch_status": (C.c_int, [P, C.POINTER(U32), P]),
+    "rb2_batch_autotune": (C.c_int, [P, P, U32, C.POINTER(BatchConfig), C.POINTER(C.c_double)]),
     "rb2_camera_init": (C.c_int, [C.POINTER(Camera), P, P, P, U32, U32, C.c_float]),
     "rb2_camera_rays": (C.c_int, [C.POINTER(Camera), U32, U64, I32, P, P]),
     "rb2_camera_rays_at": (C.c_int, [C.POINTER(Camera), P, U32, P, P]),

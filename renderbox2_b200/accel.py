@@ -271,3 +271,67 @@ def hits_view(hits):
     import torch
     f = hits.view(torch.float32)
     return hits[:, 0], f[:, 1], f[:, 2], f[:, 3]
+
+
+MODE_CLOSEST, MODE_ANY, MODE_OCCLUSION = 0, 1, 2
+
+
+class TraceBatch:
+    """Many (scene, ray batch, mode) jobs served by ONE persistent launch.
+
+    jobs: iterable of (tracer, rays tensor (n,8), mode, out tensor, mask or None).
+    Buffers are borrowed: keep them alive while the batch exists."""
+
+    def __init__(self, jobs):
+        from ._native import TraceJob
+        jobs = list(jobs)
+        arr = (TraceJob * max(1, len(jobs)))()
+        self._keep = []
+        for k, (tr, rays, mode, out, mask) in enumerate(jobs):
+            arr[k].tracer = tr.handle.value
+            arr[k].d_rays = _ptr(rays)
+            arr[k].n = int(rays.shape[0])
+            arr[k].mode = int(mode)
+            arr[k].d_mask = _ptr(mask)
+            arr[k].d_out = _ptr(out)
+            self._keep.append((tr, rays, out, mask))
+        self._b = C.c_void_p()
+        check(lib().rb2_batch_create(arr, len(jobs), C.byref(self._b)))
+
+    def __del__(self):
+        b = getattr(self, "_b", None)
+        if b and b.value:
+            lib().rb2_batch_destroy(b)
+            self._b = C.c_void_p()
+
+    def config(self) -> dict:
+        from ._native import BatchConfig
+        c = BatchConfig()
+        check(lib().rb2_batch_get_config(self._b, C.byref(c)))
+        return {k: getattr(c, k) for k, _ in BatchConfig._fields_ if k != "reserved"}
+
+    def set_config(self, **kw):
+        from ._native import BatchConfig
+        c = BatchConfig()
+        check(lib().rb2_batch_get_config(self._b, C.byref(c)))
+        for k, v in kw.items():
+            setattr(c, k, v)
+        check(lib().rb2_batch_set_config(self._b, C.byref(c)))
+
+    def launch(self, stream=None):
+        check(lib().rb2_batch_launch(self._b, _stream_handle(stream)))
+
+    def capture(self, stream):
+        check(lib().rb2_batch_capture(self._b, _stream_handle(stream)))
+
+    def autotune(self, stream=None, reps=3):
+        from ._native import BatchConfig
+        c = BatchConfig()
+        ms = C.c_double()
+        check(lib().rb2_batch_autotune(self._b, _stream_handle(stream), reps, C.byref(c), C.byref(ms)))
+        return {k: getattr(c, k) for k, _ in BatchConfig._fields_ if k != "reserved"}, ms.value
+
+    def status(self, stream=None) -> int:
+        v = C.c_uint32()
+        check(lib().rb2_batch_status(self._b, C.byref(v), _stream_handle(stream)))
+        return v.value

@@ -1,28 +1,24 @@
-// Tracer: device BVH upload and the persistent while-while traversal kernel
-// for sm_100a, plus camera-ray generation.
+// Tracer (device BVH) and the bulk / batched traversal entry points, plus
+// camera-ray generation.
 //
-// Traversal follows the reference's Aila-Laine persistent kernel
-// (accelerators/sbvh/kepler_dynamic_fetch.h:67-363) and single-ray trace_ray
-// (accelerators/sbvh/cuda_tracer_functions.cu:42-279): Compact2 nodes (64 B,
-// two child boxes), Woop triangles (48 B) with a -0.0 terminator per leaf, a
-// 64-entry stack, near child first, at most one postponed leaf, a warp vote
-// that stops node traversal once every busy lane holds a leaf, and warps that
-// refill from a global ray queue when fewer than `fetch_threshold` lanes are
-// still busy.  B200 specifics: plain global loads through the non-coherent
-// path (LDG.128) instead of texture objects, full-warp *_sync votes
-// (independent thread scheduling), one queue counter per launch slot so
-// traces on different streams do not share a counter, and a stack guard that
-// records a status bit instead of writing out of bounds.
-//
-// Arithmetic is pinned: __fmaf_rn / __fmul_rn / __fdiv_rn in the exact order
-// the CPU oracle uses, so hits, t, u and v are bit-identical to it.
+// Every traversal launch runs k_trace_jobs<BLOCK> (rb2_sources.cuh), the
+// persistent while-while kernel of rb2_traverse.cuh: a single-scene trace is a
+// one-entry job table passed inline; a batch serves many (scene, ray batch,
+// mode) jobs from one queue in one launch, optionally replayed from a CUDA
+// graph.  B200 specifics: LDG.128 non-coherent loads instead of texture
+// objects, full-warp *_sync votes, a queue counter per launch slot (so traces
+// on different streams never share a counter; the reference's global
+// g_warpCounter made trace() non-reentrant, kepler_dynamic_fetch.h:65), and a
+// stack guard that records a status bit instead of writing out of bounds.
 #include "rb2.h"
 #include "rb2_internal.h"
 #include "rb2_render.h"
+#include "rb2_sources.cuh"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <mutex>
 
 namespace rb2 {
@@ -30,216 +26,6 @@ const HostBvh& host_of(const rb2_host_bvh* b);
 }
 
 namespace rb2dev {
-
-constexpr int kSentinel = 0x76543210;
-constexpr int kStackSize = 64;
-constexpr unsigned kFull = 0xffffffffu;
-constexpr int kBlock = 128;
-constexpr uint32_t kStatusStack = 1u;
-
-enum Mode { kClosest = 0, kAny = 1, kOcclusion = 2 };
-
-struct TraceArgs {
-    const float4* __restrict__ nodes;
-    const float4* __restrict__ woop;
-    const uint32_t* __restrict__ triidx;
-    const float4* __restrict__ rays;
-    const uint8_t* __restrict__ mask;
-    int4* __restrict__ hits;
-    uint8_t* __restrict__ occl;
-    unsigned int* counter;
-    unsigned int* status;
-    uint32_t n;
-    uint32_t fetch_threshold;
-};
-
-__device__ __forceinline__ float fmin_s(float a, float b) { return a < b ? a : b; }
-__device__ __forceinline__ float fmax_s(float a, float b) { return a > b ? a : b; }
-__device__ __forceinline__ float imin_f(float a, float b) { return __int_as_float(min(__float_as_int(a), __float_as_int(b))); }
-__device__ __forceinline__ float imax_f(float a, float b) { return __int_as_float(max(__float_as_int(a), __float_as_int(b))); }
-
-__device__ __forceinline__ float span_begin(float a0, float a1, float b0, float b1, float c0, float c1, float d)
-{
-    return imax_f(imax_f(fmin_s(a0, a1), fmin_s(b0, b1)), imax_f(imin_f(c0, c1), d));
-}
-__device__ __forceinline__ float span_end(float a0, float a1, float b0, float b1, float c0, float c1, float d)
-{
-    return imin_f(imin_f(fmax_s(a0, a1), fmax_s(b0, b1)), imin_f(imax_f(c0, c1), d));
-}
-
-__device__ __forceinline__ float safe_rcp(float d)
-{
-    const float ooeps = 0x1p-80f;
-    return __fdiv_rn(1.0f, fabsf(d) > ooeps ? d : copysignf(ooeps, d));
-}
-
-template <int MODE>
-__device__ __forceinline__ void write_result(const TraceArgs& a, uint32_t ray, int hitIndex, float t, float u, float v)
-{
-    if (MODE == kOcclusion) {
-        a.occl[ray] = hitIndex >= 0 ? 1 : 0;
-    } else {
-        int prim = hitIndex >= 0 ? (int)__ldg(a.triidx + hitIndex) : -1;
-        a.hits[ray] = make_int4(prim, __float_as_int(t), __float_as_int(hitIndex >= 0 ? u : 0.0f),
-                                __float_as_int(hitIndex >= 0 ? v : 0.0f));
-    }
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(kBlock, 8) k_trace(TraceArgs a)
-{
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned lt_mask = (1u << lane) - 1u;
-
-    int stack[kStackSize + 2];
-    int sp = 0;
-    int nodeAddr = kSentinel, leafAddr = 0, hitIndex = -1;
-    float ox = 0, oy = 0, oz = 0, dx = 0, dy = 0, dz = 0;
-    float idx = 0, idy = 0, idz = 0, oodx = 0, oody = 0, oodz = 0;
-    float tmin = 0, hitT = 0, hu = 0, hv = 0;
-    uint32_t rayidx = 0;
-    bool has_ray = false, retired = false;
-
-    for (;;) {
-        // ---- refill: lanes without a ray take the next indices from the queue.
-        const bool need = !has_ray && !retired;
-        const unsigned needm = __ballot_sync(kFull, need);
-        if (needm) {
-            const int leader = __ffs(needm) - 1;
-            unsigned base = 0;
-            if ((int)lane == leader) base = atomicAdd(a.counter, (unsigned)__popc(needm));
-            base = __shfl_sync(kFull, base, leader);
-            if (need) {
-                rayidx = base + (unsigned)__popc(needm & lt_mask);
-                if (rayidx >= a.n) {
-                    retired = true;
-                } else if (a.mask != nullptr && a.mask[rayidx] == 0) {
-                    const float4 d4 = __ldg(a.rays + 2 * (size_t)rayidx + 1);
-                    write_result<MODE>(a, rayidx, -1, d4.w, 0.0f, 0.0f);
-                } else {
-                    const float4 o4 = __ldg(a.rays + 2 * (size_t)rayidx + 0);
-                    const float4 d4 = __ldg(a.rays + 2 * (size_t)rayidx + 1);
-                    ox = o4.x; oy = o4.y; oz = o4.z; tmin = o4.w;
-                    dx = d4.x; dy = d4.y; dz = d4.z; hitT = d4.w;
-                    idx = safe_rcp(dx); idy = safe_rcp(dy); idz = safe_rcp(dz);
-                    oodx = __fmul_rn(ox, idx); oody = __fmul_rn(oy, idy); oodz = __fmul_rn(oz, idz);
-                    stack[0] = kSentinel;
-                    sp = 0;
-                    leafAddr = 0;
-                    nodeAddr = 0;
-                    hitIndex = -1;
-                    hu = hv = 0.0f;
-                    has_ray = true;
-                }
-            }
-        }
-        if (__all_sync(kFull, retired)) break;
-
-        // ---- traversal until too few lanes are busy.
-        while (__any_sync(kFull, has_ray)) {
-            // Inner nodes until every busy lane has postponed a leaf.
-            for (;;) {
-                const bool in = has_ray && (unsigned)nodeAddr < (unsigned)kSentinel;
-                if (!__any_sync(kFull, in)) break;
-                if (in) {
-                    const float4* np = a.nodes + nodeAddr;
-                    const float4 n0xy = __ldg(np + 0);
-                    const float4 n1xy = __ldg(np + 1);
-                    const float4 nz = __ldg(np + 2);
-                    const float4 cn = __ldg(np + 3);
-                    int c0 = __float_as_int(cn.x), c1 = __float_as_int(cn.y);
-
-                    const float c0lox = __fmaf_rn(n0xy.x, idx, -oodx);
-                    const float c0hix = __fmaf_rn(n0xy.y, idx, -oodx);
-                    const float c0loy = __fmaf_rn(n0xy.z, idy, -oody);
-                    const float c0hiy = __fmaf_rn(n0xy.w, idy, -oody);
-                    const float c0loz = __fmaf_rn(nz.x, idz, -oodz);
-                    const float c0hiz = __fmaf_rn(nz.y, idz, -oodz);
-                    const float c1loz = __fmaf_rn(nz.z, idz, -oodz);
-                    const float c1hiz = __fmaf_rn(nz.w, idz, -oodz);
-                    const float c0min = span_begin(c0lox, c0hix, c0loy, c0hiy, c0loz, c0hiz, tmin);
-                    const float c0max = span_end(c0lox, c0hix, c0loy, c0hiy, c0loz, c0hiz, hitT);
-                    const float c1lox = __fmaf_rn(n1xy.x, idx, -oodx);
-                    const float c1hix = __fmaf_rn(n1xy.y, idx, -oodx);
-                    const float c1loy = __fmaf_rn(n1xy.z, idy, -oody);
-                    const float c1hiy = __fmaf_rn(n1xy.w, idy, -oody);
-                    const float c1min = span_begin(c1lox, c1hix, c1loy, c1hiy, c1loz, c1hiz, tmin);
-                    const float c1max = span_end(c1lox, c1hix, c1loy, c1hiy, c1loz, c1hiz, hitT);
-
-                    const bool swp = c1min < c0min;
-                    const bool t0 = c0max >= c0min;
-                    const bool t1 = c1max >= c1min;
-                    if (!t0 && !t1) {
-                        nodeAddr = stack[sp--];
-                    } else {
-                        nodeAddr = t0 ? c0 : c1;
-                        if (t0 && t1) {
-                            if (swp) { const int tmp = nodeAddr; nodeAddr = c1; c1 = tmp; }
-                            if (sp >= kStackSize) {
-                                atomicOr(a.status, kStatusStack);
-                                nodeAddr = kSentinel;  // abandon this ray; reported as a miss
-                                leafAddr = 0;
-                                hitIndex = -1;
-                            } else {
-                                stack[++sp] = c1;
-                            }
-                        }
-                    }
-                    if (nodeAddr < 0 && leafAddr >= 0) {
-                        leafAddr = nodeAddr;
-                        nodeAddr = stack[sp--];
-                    }
-                }
-                if (!__any_sync(kFull, in && leafAddr >= 0)) break;
-            }
-
-            // Postponed leaves.
-            if (has_ray) {
-                while (leafAddr < 0) {
-                    for (int triAddr = ~leafAddr;; triAddr += 3) {
-                        const float4* wp = a.woop + triAddr;
-                        const float4 v00 = __ldg(wp + 0);
-                        const float4 v11 = __ldg(wp + 1);
-                        const float4 v22 = __ldg(wp + 2);
-                        if (__float_as_int(v00.x) == (int)0x80000000) break;
-
-                        const float Oz = __fmaf_rn(-oz, v00.z, __fmaf_rn(-oy, v00.y, __fmaf_rn(-ox, v00.x, v00.w)));
-                        const float Dz = __fmaf_rn(dz, v00.z, __fmaf_rn(dy, v00.y, __fmul_rn(dx, v00.x)));
-                        const float t = __fmul_rn(Oz, __fdiv_rn(1.0f, Dz));
-                        if (t > tmin && t < hitT) {
-                            const float Ox = __fmaf_rn(oz, v11.z, __fmaf_rn(oy, v11.y, __fmaf_rn(ox, v11.x, v11.w)));
-                            const float Dx = __fmaf_rn(dz, v11.z, __fmaf_rn(dy, v11.y, __fmul_rn(dx, v11.x)));
-                            const float u = __fmaf_rn(t, Dx, Ox);
-                            if (u >= 0.0f) {
-                                const float Oy = __fmaf_rn(oz, v22.z, __fmaf_rn(oy, v22.y, __fmaf_rn(ox, v22.x, v22.w)));
-                                const float Dy = __fmaf_rn(dz, v22.z, __fmaf_rn(dy, v22.y, __fmul_rn(dx, v22.x)));
-                                const float v = __fmaf_rn(t, Dy, Oy);
-                                if (v >= 0.0f && __fadd_rn(u, v) <= 1.0f) {
-                                    hitT = t;
-                                    hu = u;
-                                    hv = v;
-                                    hitIndex = triAddr;
-                                    if (MODE != kClosest) {
-                                        nodeAddr = kSentinel;
-                                        break;
-                                    }
-                                }
-                            }
-                        }
-                    }
-                    leafAddr = nodeAddr;
-                    if (nodeAddr < 0) nodeAddr = stack[sp--];
-                }
-                if (nodeAddr == kSentinel) {
-                    write_result<MODE>(a, rayidx, hitIndex, hitT, hu, hv);
-                    has_ray = false;
-                }
-            }
-            // Dynamic fetch (kepler_dynamic_fetch.h:308-310).
-            if ((unsigned)__popc(__ballot_sync(kFull, has_ray)) < a.fetch_threshold) break;
-        }
-    }
-}
 
 // ---- camera rays ------------------------------------------------------------------
 struct CamArgs {
@@ -258,7 +44,7 @@ __device__ __forceinline__ float row_dot(const float* r, float x, float y, float
 
 __device__ __forceinline__ void camera_ray(const float* r2c, const float* c2w, float x, float y, float4& o4, float4& d4)
 {
-    // p_camera = raster_to_camera(point (x, y, 0)), divided by w.
+    // p_camera = raster_to_camera(point (x, y, 0)), divided by w (core/camera.cu:91-98).
     float px = row_dot(r2c + 0, x, y, 0.0f, 1.0f);
     float py = row_dot(r2c + 4, x, y, 0.0f, 1.0f);
     float pz = row_dot(r2c + 8, x, y, 0.0f, 1.0f);
@@ -322,17 +108,105 @@ __global__ void k_camera_rays_at(CamArgs c, const float2* xy, uint32_t n, float4
 // ======================================================================= host side
 using namespace rb2;
 
+namespace {
+
+constexpr uint32_t kSlots = 256;
+constexpr uint32_t kDefaultBlock = 128;
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+    return fail(RB2_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define RB2_CUDA(call, what)                                \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what);  \
+    } while (0)
+
+struct Occupancy {
+    int sms = 0;
+    int per_sm[3] = {0, 0, 0};  // block 64, 128, 256
+};
+
+int block_index(uint32_t block) { return block == 64 ? 0 : (block == 256 ? 2 : 1); }
+
+int occupancy(Occupancy& o)
+{
+    int dev = 0;
+    RB2_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    RB2_CUDA(cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    const size_t smem = rb2dev::job_smem_bytes(rb2dev::kMaxSmemJobs, false);
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm[0], rb2dev::k_trace_jobs<64>, 64, smem), "occupancy");
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm[1], rb2dev::k_trace_jobs<128>, 128, smem), "occupancy");
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm[2], rb2dev::k_trace_jobs<256>, 256, smem), "occupancy");
+    return RB2_OK;
+}
+
+// Launches the persistent kernel: grid = SMs x resident CTAs per SM, capped
+// by the work available.
+int launch_jobs(const rb2dev::KernelArgs& a, uint64_t total_rays, uint32_t block, uint32_t ctas_per_sm,
+                const Occupancy& occ, cudaStream_t s)
+{
+    const int bi = block_index(block);
+    const uint32_t per_sm = ctas_per_sm ? std::min<uint32_t>(ctas_per_sm, (uint32_t)std::max(1, occ.per_sm[bi]))
+                                        : (uint32_t)std::max(1, occ.per_sm[bi]);
+    uint64_t blocks = (uint64_t)occ.sms * per_sm;
+    const uint64_t warps_needed = (total_rays + 31) / 32;
+    blocks = std::min<uint64_t>(blocks, (warps_needed + block / 32 - 1) / (block / 32));
+    blocks = std::max<uint64_t>(blocks, 1);
+    const size_t smem = rb2dev::job_smem_bytes(a.n_jobs, a.jobs == nullptr);
+    switch (block) {
+    case 64: rb2dev::k_trace_jobs<64><<<(unsigned)blocks, 64, smem, s>>>(a); break;
+    case 256: rb2dev::k_trace_jobs<256><<<(unsigned)blocks, 256, smem, s>>>(a); break;
+    default: rb2dev::k_trace_jobs<128><<<(unsigned)blocks, 128, smem, s>>>(a); break;
+    }
+    RB2_CUDA(cudaGetLastError(), "trace launch");
+    return RB2_OK;
+}
+
+// Inner-node order of the Compact2 buffer: the reference's DFS order, or
+// breadth-first so the top of the tree is contiguous.
+void reorder_nodes(const std::vector<uint32_t>& in, uint32_t order, std::vector<uint32_t>& out)
+{
+    if (order == RB2_NODE_ORDER_DFS) { out = in; return; }
+    const uint32_t n_inner = (uint32_t)(in.size() / 16);
+    std::vector<uint32_t> new_of(n_inner, 0), bfs;
+    bfs.reserve(n_inner);
+    bfs.push_back(0);
+    for (size_t h = 0; h < bfs.size(); h++) {
+        const uint32_t* nd = &in[(size_t)bfs[h] * 16];
+        for (int k = 0; k < 2; k++) {
+            int32_t c = (int32_t)nd[12 + k];
+            if (c >= 0) bfs.push_back((uint32_t)c / 4);
+        }
+    }
+    for (uint32_t i = 0; i < (uint32_t)bfs.size(); i++) new_of[bfs[i]] = i;
+    out.assign(in.size(), 0u);
+    for (uint32_t i = 0; i < (uint32_t)bfs.size(); i++) {
+        std::memcpy(&out[(size_t)i * 16], &in[(size_t)bfs[i] * 16], 64);
+        for (int k = 0; k < 2; k++) {
+            int32_t c = (int32_t)out[(size_t)i * 16 + 12 + k];
+            if (c >= 0) out[(size_t)i * 16 + 12 + k] = new_of[(uint32_t)c / 4] * 4;
+        }
+    }
+}
+
+}  // namespace
+
 struct rb2_tracer {
     int device = 0;
-    int num_sms = 0;
+    Occupancy occ;
     float4* d_nodes = nullptr;
     float4* d_woop = nullptr;
     uint32_t* d_triidx = nullptr;
     uint64_t n_nodes_u4 = 0, n_woop_u4 = 0;
-    unsigned int* d_words = nullptr;  // [0, kSlots) queue heads, [kSlots] status
+    std::vector<uint32_t> host_nodes;  // DFS order, kept for re-layout
+    uint32_t node_order = RB2_NODE_ORDER_DFS;
+    unsigned long long* d_counters = nullptr;  // kSlots queue heads
+    unsigned int* d_status = nullptr;
     uint32_t slot = 0;
     rb2_launch_config cfg{};
-    int occ[3] = {0, 0, 0};
     // scratch for the host-buffer path
     float4* d_rays = nullptr;
     int4* d_hits = nullptr;
@@ -340,54 +214,47 @@ struct rb2_tracer {
     uint64_t scratch_cap = 0;
     uint64_t device_bytes = 0;
     std::mutex mu;
+
+    unsigned long long* next_counter()
+    {
+        std::lock_guard<std::mutex> g(mu);
+        return d_counters + (slot++ % kSlots);
+    }
 };
 
 namespace {
 
-constexpr uint32_t kSlots = 256;
-
-int cuda_fail(cudaError_t e, const char* what)
+rb2dev::JobDesc job_of(const rb2_tracer* t, const float* rays, uint64_t n, uint32_t mode, const uint8_t* mask, void* out)
 {
-    return fail(RB2_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    rb2dev::JobDesc d{};
+    d.nodes = t->d_nodes;
+    d.woop = t->d_woop;
+    d.triidx = t->d_triidx;
+    d.rays = reinterpret_cast<const float4*>(rays);
+    d.mask = mask;
+    d.out = out;
+    d.n = n;
+    d.mode = mode;
+    return d;
 }
 
-#define RB2_CUDA(call, what)                         \
-    do {                                             \
-        cudaError_t e_ = (call);                     \
-        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
-    } while (0)
-
-template <int MODE>
-int launch_trace(rb2_tracer* t, const float* d_rays, uint32_t n, const uint8_t* d_mask, int4* d_hits, uint8_t* d_occ,
+int trace_single(rb2_tracer* t, const float* d_rays, uint64_t n, uint32_t mode, const uint8_t* d_mask, void* d_out,
                  cudaStream_t s)
 {
     if (n == 0) return RB2_OK;
-    uint32_t slot;
-    {
-        std::lock_guard<std::mutex> g(t->mu);
-        slot = t->slot++ % kSlots;
-    }
-    RB2_CUDA(cudaMemsetAsync(t->d_words + slot, 0, sizeof(unsigned int), s), "queue reset");
-    rb2dev::TraceArgs a;
-    a.nodes = t->d_nodes;
-    a.woop = t->d_woop;
-    a.triidx = t->d_triidx;
-    a.rays = reinterpret_cast<const float4*>(d_rays);
-    a.mask = d_mask;
-    a.hits = d_hits;
-    a.occl = d_occ;
-    a.counter = t->d_words + slot;
-    a.status = t->d_words + kSlots;
-    a.n = n;
+    unsigned long long* counter = t->next_counter();
+    RB2_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s), "queue reset");
+    rb2dev::KernelArgs a{};
+    a.jobs = nullptr;
+    a.start = nullptr;
+    a.inline_job = job_of(t, d_rays, n, mode, d_mask, d_out);
+    a.n_jobs = 1;
     a.fetch_threshold = t->cfg.fetch_threshold ? t->cfg.fetch_threshold : 20u;
-    int per_sm = t->cfg.ctas_per_sm ? (int)t->cfg.ctas_per_sm : t->occ[MODE];
-    uint64_t warps_needed = ((uint64_t)n + 31) / 32;
-    uint64_t blocks = (uint64_t)t->num_sms * (uint64_t)std::max(1, per_sm);
-    blocks = std::min<uint64_t>(blocks, (warps_needed + rb2dev::kBlock / 32 - 1) / (rb2dev::kBlock / 32));
-    blocks = std::max<uint64_t>(blocks, 1);
-    rb2dev::k_trace<MODE><<<(unsigned)blocks, rb2dev::kBlock, 0, s>>>(a);
-    RB2_CUDA(cudaGetLastError(), "trace launch");
-    return RB2_OK;
+    a.chunk = 1;
+    a.counter = counter;
+    a.status = t->d_status;
+    const uint32_t block = t->cfg.block_threads ? t->cfg.block_threads : kDefaultBlock;
+    return launch_jobs(a, n, block, t->cfg.ctas_per_sm, t->occ, s);
 }
 
 }  // namespace
@@ -405,19 +272,22 @@ int rb2_tracer_create(const rb2_host_bvh* bvh, rb2_tracer** out)
     if (rc) return rc;
     std::unique_ptr<rb2_tracer> t(new rb2_tracer());
     RB2_CUDA(cudaGetDevice(&t->device), "cudaGetDevice");
-    RB2_CUDA(cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, t->device), "SM count");
+    rc = occupancy(t->occ);
+    if (rc) return rc;
     t->n_nodes_u4 = h.nodes.size() / 4;
     t->n_woop_u4 = h.woop.size() / 4;
+    t->host_nodes = h.nodes;
     // Two spare uint4 after the Woop buffer: the kernel fetches a triangle's
     // three rows before testing the first for the terminator.
     const size_t nb = h.nodes.size() * 4, wb = (h.woop.size() + 8) * 4, ib = h.triidx.size() * 4 + 16;
     auto cleanup = [&]() {
-        cudaFree(t->d_nodes); cudaFree(t->d_woop); cudaFree(t->d_triidx); cudaFree(t->d_words);
+        cudaFree(t->d_nodes); cudaFree(t->d_woop); cudaFree(t->d_triidx); cudaFree(t->d_counters); cudaFree(t->d_status);
     };
     cudaError_t e;
     if ((e = cudaMalloc(&t->d_nodes, nb)) != cudaSuccess || (e = cudaMalloc(&t->d_woop, wb)) != cudaSuccess ||
         (e = cudaMalloc(&t->d_triidx, ib)) != cudaSuccess ||
-        (e = cudaMalloc(&t->d_words, (kSlots + 1) * sizeof(unsigned int))) != cudaSuccess) {
+        (e = cudaMalloc(&t->d_counters, kSlots * sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMalloc(&t->d_status, sizeof(unsigned int))) != cudaSuccess) {
         cleanup();
         return fail(RB2_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
     }
@@ -426,14 +296,12 @@ int rb2_tracer_create(const rb2_host_bvh* bvh, rb2_tracer** out)
         (e = cudaMemcpy(t->d_woop, h.woop.data(), h.woop.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemset(t->d_triidx, 0, ib)) != cudaSuccess ||
         (e = cudaMemcpy(t->d_triidx, h.triidx.data(), h.triidx.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemset(t->d_words, 0, (kSlots + 1) * sizeof(unsigned int))) != cudaSuccess) {
+        (e = cudaMemset(t->d_counters, 0, kSlots * sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMemset(t->d_status, 0, sizeof(unsigned int))) != cudaSuccess) {
         cleanup();
         return cuda_fail(e, "BVH upload");
     }
-    t->device_bytes = nb + wb + ib + (kSlots + 1) * sizeof(unsigned int);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&t->occ[0], rb2dev::k_trace<0>, rb2dev::kBlock, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&t->occ[1], rb2dev::k_trace<1>, rb2dev::kBlock, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&t->occ[2], rb2dev::k_trace<2>, rb2dev::kBlock, 0);
+    t->device_bytes = nb + wb + ib + kSlots * sizeof(unsigned long long) + sizeof(unsigned int);
     *out = t.release();
     return RB2_OK;
 }
@@ -444,7 +312,8 @@ int rb2_tracer_destroy(rb2_tracer* t)
     cudaFree(t->d_nodes);
     cudaFree(t->d_woop);
     cudaFree(t->d_triidx);
-    cudaFree(t->d_words);
+    cudaFree(t->d_counters);
+    cudaFree(t->d_status);
     cudaFree(t->d_rays);
     cudaFree(t->d_hits);
     cudaFree(t->d_mask);
@@ -455,10 +324,23 @@ int rb2_tracer_destroy(rb2_tracer* t)
 int rb2_tracer_set_launch(rb2_tracer* t, const rb2_launch_config* cfg)
 {
     if (!t || !cfg) return fail(RB2_EINVAL, "null argument");
-    if (cfg->block_threads && cfg->block_threads != (uint32_t)rb2dev::kBlock)
-        return fail(RB2_ENOTSUP, "the traversal kernel is compiled for 128-thread CTAs");
+    if (cfg->block_threads && cfg->block_threads != 64 && cfg->block_threads != 128 && cfg->block_threads != 256)
+        return fail(RB2_ENOTSUP, "block_threads must be 64, 128 or 256");
     if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
     t->cfg = *cfg;
+    return RB2_OK;
+}
+
+int rb2_tracer_set_node_order(rb2_tracer* t, uint32_t order)
+{
+    if (!t) return fail(RB2_EINVAL, "null argument");
+    if (order != RB2_NODE_ORDER_DFS && order != RB2_NODE_ORDER_BFS) return fail(RB2_EINVAL, "unknown node order");
+    if (order == t->node_order) return RB2_OK;
+    std::vector<uint32_t> nodes;
+    reorder_nodes(t->host_nodes, order, nodes);
+    RB2_CUDA(cudaDeviceSynchronize(), "sync before re-layout");
+    RB2_CUDA(cudaMemcpy(t->d_nodes, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice), "node upload");
+    t->node_order = order;
     return RB2_OK;
 }
 
@@ -474,10 +356,7 @@ int rb2_trace(rb2_tracer* t, const float* d_rays, uint32_t n, int any_hit, const
 {
     if (!t || (n && (!d_rays || !d_hits))) return fail(RB2_EINVAL, "null argument");
     if (((uintptr_t)d_rays | (uintptr_t)d_hits) & 15u) return fail(RB2_EINVAL, "rays and hits must be 16-byte aligned");
-    cudaStream_t s = (cudaStream_t)stream;
-    int4* hits = reinterpret_cast<int4*>(d_hits);
-    return any_hit ? launch_trace<rb2dev::kAny>(t, d_rays, n, d_mask, hits, nullptr, s)
-                   : launch_trace<rb2dev::kClosest>(t, d_rays, n, d_mask, hits, nullptr, s);
+    return trace_single(t, d_rays, n, any_hit ? rb2dev::kAny : rb2dev::kClosest, d_mask, d_hits, (cudaStream_t)stream);
 }
 
 int rb2_trace_occlusion(rb2_tracer* t, const float* d_rays, uint32_t n, const uint8_t* d_mask, uint8_t* d_occluded,
@@ -485,7 +364,7 @@ int rb2_trace_occlusion(rb2_tracer* t, const float* d_rays, uint32_t n, const ui
 {
     if (!t || (n && (!d_rays || !d_occluded))) return fail(RB2_EINVAL, "null argument");
     if ((uintptr_t)d_rays & 15u) return fail(RB2_EINVAL, "rays must be 16-byte aligned");
-    return launch_trace<rb2dev::kOcclusion>(t, d_rays, n, d_mask, nullptr, d_occluded, (cudaStream_t)stream);
+    return trace_single(t, d_rays, n, rb2dev::kOcclusion, d_mask, d_occluded, (cudaStream_t)stream);
 }
 
 int rb2_trace_host(rb2_tracer* t, const float* h_rays, uint32_t n, int any_hit, const uint8_t* h_mask, rb2_hit* h_hits,
@@ -494,21 +373,25 @@ int rb2_trace_host(rb2_tracer* t, const float* h_rays, uint32_t n, int any_hit, 
     if (!t || (n && (!h_rays || !h_hits))) return fail(RB2_EINVAL, "null argument");
     if (n == 0) return RB2_OK;
     cudaStream_t s = (cudaStream_t)stream;
+    std::unique_lock<std::mutex> g(t->mu);
     if (n > t->scratch_cap) {
         RB2_CUDA(cudaStreamSynchronize(s), "stream sync");
         cudaFree(t->d_rays); cudaFree(t->d_hits); cudaFree(t->d_mask);
         t->d_rays = nullptr; t->d_hits = nullptr; t->d_mask = nullptr;
         t->scratch_cap = 0;
         cudaError_t e;
-        if ((e = cudaMalloc(&t->d_rays, (size_t)n * 32)) != cudaSuccess || (e = cudaMalloc(&t->d_hits, (size_t)n * 16)) != cudaSuccess ||
+        if ((e = cudaMalloc(&t->d_rays, (size_t)n * 32)) != cudaSuccess ||
+            (e = cudaMalloc(&t->d_hits, (size_t)n * 16)) != cudaSuccess ||
             (e = cudaMalloc(&t->d_mask, (size_t)n)) != cudaSuccess)
             return fail(RB2_ENOMEM, std::string("scratch allocation: ") + cudaGetErrorString(e));
         t->scratch_cap = n;
     }
     RB2_CUDA(cudaMemcpyAsync(t->d_rays, h_rays, (size_t)n * 32, cudaMemcpyHostToDevice, s), "ray upload");
     if (h_mask) RB2_CUDA(cudaMemcpyAsync(t->d_mask, h_mask, n, cudaMemcpyHostToDevice, s), "mask upload");
-    int rc = rb2_trace(t, reinterpret_cast<const float*>(t->d_rays), n, any_hit, h_mask ? t->d_mask : nullptr,
-                       reinterpret_cast<rb2_hit*>(t->d_hits), stream);
+    // trace_single takes the tracer mutex for the counter slot; release ours first.
+    g.unlock();
+    int rc = trace_single(t, reinterpret_cast<const float*>(t->d_rays), n, any_hit ? rb2dev::kAny : rb2dev::kClosest,
+                          h_mask ? t->d_mask : nullptr, t->d_hits, s);
     if (rc) return rc;
     RB2_CUDA(cudaMemcpyAsync(h_hits, t->d_hits, (size_t)n * 16, cudaMemcpyDeviceToHost, s), "hit download");
     RB2_CUDA(cudaStreamSynchronize(s), "stream sync");
@@ -519,11 +402,247 @@ int rb2_tracer_status(rb2_tracer* t, uint32_t* status, void* stream)
 {
     if (!t || !status) return fail(RB2_EINVAL, "null argument");
     cudaStream_t s = (cudaStream_t)stream;
-    RB2_CUDA(cudaMemcpyAsync(status, t->d_words + kSlots, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "status read");
+    RB2_CUDA(cudaMemcpyAsync(status, t->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "status read");
     RB2_CUDA(cudaStreamSynchronize(s), "stream sync");
     return RB2_OK;
 }
 
+// ------------------------------------------------------------------------ batching
+}  // extern "C"
+
+struct rb2_batch {
+    std::vector<rb2_trace_job> jobs;
+    std::vector<rb2_tracer*> tracers;
+    rb2dev::JobDesc* d_jobs = nullptr;
+    unsigned long long* d_start = nullptr;
+    unsigned long long* d_counter = nullptr;
+    unsigned int* d_status = nullptr;
+    uint64_t total = 0;
+    rb2_batch_config cfg{};
+    Occupancy occ;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+
+    void drop_graph()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+};
+
+namespace {
+
+int batch_enqueue(rb2_batch* b, cudaStream_t s)
+{
+    RB2_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), s), "queue reset");
+    rb2dev::KernelArgs a{};
+    a.jobs = b->d_jobs;
+    a.start = b->d_start;
+    a.n_jobs = (uint32_t)b->jobs.size();
+    a.fetch_threshold = b->cfg.fetch_threshold ? b->cfg.fetch_threshold : 20u;
+    a.chunk = b->cfg.chunk ? b->cfg.chunk : 1u;
+    a.counter = b->d_counter;
+    a.status = b->d_status;
+    return launch_jobs(a, b->total, b->cfg.block_threads ? b->cfg.block_threads : kDefaultBlock, b->cfg.ctas_per_sm,
+                       b->occ, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rb2_batch_create(const rb2_trace_job* jobs, uint32_t n_jobs, rb2_batch** out)
+{
+    if (!out || (n_jobs && !jobs)) return fail(RB2_EINVAL, "null argument");
+    *out = nullptr;
+    std::unique_ptr<rb2_batch> b(new rb2_batch());
+    std::vector<rb2dev::JobDesc> descs(n_jobs);
+    std::vector<unsigned long long> start(n_jobs + 1, 0);
+    for (uint32_t i = 0; i < n_jobs; i++) {
+        const rb2_trace_job& j = jobs[i];
+        if (!j.tracer || (j.n && (!j.d_rays || !j.d_out))) return fail(RB2_EINVAL, "job with null tracer or buffer");
+        if (j.mode > RB2_MODE_OCCLUSION) return fail(RB2_EINVAL, "unknown job mode");
+        if ((uintptr_t)j.d_rays & 15u) return fail(RB2_EINVAL, "job rays must be 16-byte aligned");
+        if (j.mode != RB2_MODE_OCCLUSION && ((uintptr_t)j.d_out & 15u)) return fail(RB2_EINVAL, "job hits must be 16-byte aligned");
+        descs[i] = job_of(j.tracer, j.d_rays, j.n, j.mode, j.d_mask, j.d_out);
+        start[i + 1] = start[i] + j.n;
+    }
+    b->jobs.assign(jobs, jobs + n_jobs);
+    b->total = start[n_jobs];
+    int rc = occupancy(b->occ);
+    if (rc) return rc;
+    cudaError_t e;
+    if ((e = cudaMalloc(&b->d_jobs, sizeof(rb2dev::JobDesc) * std::max<uint32_t>(1, n_jobs))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_start, sizeof(unsigned long long) * (n_jobs + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_counter, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_status, sizeof(unsigned int))) != cudaSuccess) {
+        cudaFree(b->d_jobs); cudaFree(b->d_start); cudaFree(b->d_counter); cudaFree(b->d_status);
+        return fail(RB2_ENOMEM, std::string("batch allocation: ") + cudaGetErrorString(e));
+    }
+    if (n_jobs) RB2_CUDA(cudaMemcpy(b->d_jobs, descs.data(), sizeof(rb2dev::JobDesc) * n_jobs, cudaMemcpyHostToDevice), "job upload");
+    RB2_CUDA(cudaMemcpy(b->d_start, start.data(), sizeof(unsigned long long) * (n_jobs + 1), cudaMemcpyHostToDevice), "job upload");
+    RB2_CUDA(cudaMemset(b->d_status, 0, sizeof(unsigned int)), "status reset");
+    *out = b.release();
+    return RB2_OK;
+}
+
+int rb2_batch_destroy(rb2_batch* b)
+{
+    if (!b) return RB2_OK;
+    b->drop_graph();
+    cudaFree(b->d_jobs);
+    cudaFree(b->d_start);
+    cudaFree(b->d_counter);
+    cudaFree(b->d_status);
+    delete b;
+    return RB2_OK;
+}
+
+int rb2_batch_set_config(rb2_batch* b, const rb2_batch_config* cfg)
+{
+    if (!b || !cfg) return fail(RB2_EINVAL, "null argument");
+    if (cfg->block_threads && cfg->block_threads != 64 && cfg->block_threads != 128 && cfg->block_threads != 256)
+        return fail(RB2_ENOTSUP, "block_threads must be 64, 128 or 256");
+    if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
+    if (cfg->node_order > RB2_NODE_ORDER_BFS) return fail(RB2_EINVAL, "unknown node order");
+    b->drop_graph();
+    b->cfg = *cfg;
+    std::vector<rb2_tracer*> seen;
+    for (const auto& j : b->jobs) {
+        if (std::find(seen.begin(), seen.end(), j.tracer) != seen.end()) continue;
+        seen.push_back(j.tracer);
+        int rc = rb2_tracer_set_node_order(j.tracer, cfg->node_order);
+        if (rc) return rc;
+    }
+    return RB2_OK;
+}
+
+int rb2_batch_get_config(const rb2_batch* b, rb2_batch_config* cfg)
+{
+    if (!b || !cfg) return fail(RB2_EINVAL, "null argument");
+    *cfg = b->cfg;
+    return RB2_OK;
+}
+
+int rb2_batch_capture(rb2_batch* b, void* stream)
+{
+    if (!b) return fail(RB2_EINVAL, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!s) return fail(RB2_EINVAL, "graph capture needs a non-default stream");
+    b->drop_graph();
+    RB2_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int rc = batch_enqueue(b, s);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return cuda_fail(e, "end capture");
+    b->graph = g;
+    RB2_CUDA(cudaGraphInstantiate(&b->exec, g, 0), "graph instantiate");
+    return RB2_OK;
+}
+
+int rb2_batch_launch(rb2_batch* b, void* stream)
+{
+    if (!b) return fail(RB2_EINVAL, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b->total == 0) return RB2_OK;
+    if (b->exec) {
+        RB2_CUDA(cudaGraphLaunch(b->exec, s), "graph launch");
+        return RB2_OK;
+    }
+    return batch_enqueue(b, s);
+}
+
+int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream)
+{
+    if (!b || !status) return fail(RB2_EINVAL, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    RB2_CUDA(cudaMemcpyAsync(status, b->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "status read");
+    RB2_CUDA(cudaStreamSynchronize(s), "stream sync");
+    return RB2_OK;
+}
+
+// Coordinate-descent autotuner over node order, block shape, resident CTAs
+// per SM, fetch threshold and queue chunk: each candidate is timed with CUDA
+// events (median of `reps` launches after one warm-up) and the fastest kept.
+int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best_out, double* best_ms_out)
+{
+    if (!b) return fail(RB2_EINVAL, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (reps == 0) reps = 3;
+    cudaEvent_t e0, e1;
+    RB2_CUDA(cudaEventCreate(&e0), "event");
+    RB2_CUDA(cudaEventCreate(&e1), "event");
+    auto time_cfg = [&](const rb2_batch_config& c, double& ms) -> int {
+        int rc = rb2_batch_set_config(b, &c);
+        if (rc) return rc;
+        rc = batch_enqueue(b, s);
+        if (rc) return rc;
+        std::vector<float> t(reps);
+        for (uint32_t r = 0; r < reps; r++) {
+            RB2_CUDA(cudaEventRecord(e0, s), "event");
+            rc = batch_enqueue(b, s);
+            if (rc) return rc;
+            RB2_CUDA(cudaEventRecord(e1, s), "event");
+            RB2_CUDA(cudaEventSynchronize(e1), "event sync");
+            RB2_CUDA(cudaEventElapsedTime(&t[r], e0, e1), "event time");
+        }
+        std::sort(t.begin(), t.end());
+        ms = t[reps / 2];
+        return RB2_OK;
+    };
+    rb2_batch_config best{};
+    best.block_threads = kDefaultBlock;
+    best.fetch_threshold = 20;
+    best.chunk = 1;
+    best.node_order = RB2_NODE_ORDER_DFS;
+    double best_ms = 0;
+    int rc = time_cfg(best, best_ms);
+    if (rc) return rc;
+    const uint32_t orders[] = {RB2_NODE_ORDER_DFS, RB2_NODE_ORDER_BFS};
+    const uint32_t blocks[] = {64, 128, 256};
+    const uint32_t thresholds[] = {8, 16, 20, 24, 28};
+    const uint32_t chunks[] = {1, 2, 4, 8};
+    for (int pass = 0; pass < 2; pass++) {
+        for (uint32_t o : orders) {
+            rb2_batch_config c = best; c.node_order = o; double ms;
+            if ((rc = time_cfg(c, ms))) return rc;
+            if (ms < best_ms) { best = c; best_ms = ms; }
+        }
+        for (uint32_t bl : blocks) {
+            rb2_batch_config c = best; c.block_threads = bl; c.ctas_per_sm = 0; double ms;
+            if ((rc = time_cfg(c, ms))) return rc;
+            if (ms < best_ms) { best = c; best_ms = ms; }
+        }
+        const int maxc = std::max(1, b->occ.per_sm[block_index(best.block_threads)]);
+        for (int k : {maxc, std::max(1, maxc * 3 / 4), std::max(1, maxc / 2)}) {
+            rb2_batch_config c = best; c.ctas_per_sm = (uint32_t)k; double ms;
+            if ((rc = time_cfg(c, ms))) return rc;
+            if (ms < best_ms) { best = c; best_ms = ms; }
+        }
+        for (uint32_t th : thresholds) {
+            rb2_batch_config c = best; c.fetch_threshold = th; double ms;
+            if ((rc = time_cfg(c, ms))) return rc;
+            if (ms < best_ms) { best = c; best_ms = ms; }
+        }
+        for (uint32_t ch : chunks) {
+            rb2_batch_config c = best; c.chunk = ch; double ms;
+            if ((rc = time_cfg(c, ms))) return rc;
+            if (ms < best_ms) { best = c; best_ms = ms; }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rc = rb2_batch_set_config(b, &best);
+    if (rc) return rc;
+    if (best_out) *best_out = best;
+    if (best_ms_out) *best_ms_out = best_ms;
+    return RB2_OK;
+}
+
+// ------------------------------------------------------------------ camera entry points
 int rb2_camera_rays(const rb2_camera* cam, uint32_t spp, uint64_t seed, int jitter, float* d_rays, void* stream)
 {
     if (!cam || !d_rays || spp == 0) return fail(RB2_EINVAL, "bad camera-ray arguments");

@@ -1,0 +1,236 @@
+// Persistent while-while traversal body shared by every launch flavour
+// (single tracer, batched job table, integrator queues).
+//
+// Semantics follow the reference's Aila-Laine persistent kernel
+// (accelerators/sbvh/kepler_dynamic_fetch.h:67-363) and single-ray trace_ray
+// (accelerators/sbvh/cuda_tracer_functions.cu:42-279); arithmetic is pinned
+// to the CPU oracle's (oracle/rb2_oracle.c) with __fmaf_rn / __fmul_rn /
+// __fdiv_rn so results are bit-identical.
+//
+// A RaySource policy supplies rays and consumes results:
+//   void claim(unsigned count, u64& b1, unsigned& n1, u64& b2)
+//        warp leader reserves `count` slots: ranks [0, n1) get b1 + rank,
+//        ranks [n1, count) get b2 + (rank - n1)
+//   int fetch(u64 slot, Lane& L)   1: ray loaded; 0: slot past the end (lane
+//                                  retires); -1: ray consumed by the source
+//                                  (masked ray, result already written)
+//   void finish(const Lane& L)     write the result of a finished ray
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rb2dev {
+
+constexpr int kSentinel = 0x76543210;
+constexpr int kStackSize = 64;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kStatusStack = 1u;
+
+enum Mode : uint32_t { kClosest = 0, kAny = 1, kOcclusion = 2 };
+
+struct Lane {
+    // BVH of the ray's scene
+    const float4* nodes;
+    const float4* woop;
+    const uint32_t* triidx;
+    // ray
+    float ox, oy, oz, dx, dy, dz, idx, idy, idz, oodx, oody, oodz, tmin;
+    // state
+    float hitT, hu, hv;
+    int nodeAddr, leafAddr, hitIndex;
+    uint32_t mode;      // Mode
+    uint32_t job;       // source-defined tag (job index)
+    uint64_t ray;       // source-defined index of the ray within its job
+};
+
+__device__ __forceinline__ float fmin_s(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float fmax_s(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float imin_f(float a, float b) { return __int_as_float(min(__float_as_int(a), __float_as_int(b))); }
+__device__ __forceinline__ float imax_f(float a, float b) { return __int_as_float(max(__float_as_int(a), __float_as_int(b))); }
+
+__device__ __forceinline__ float span_begin(float a0, float a1, float b0, float b1, float c0, float c1, float d)
+{
+    return imax_f(imax_f(fmin_s(a0, a1), fmin_s(b0, b1)), imax_f(imin_f(c0, c1), d));
+}
+__device__ __forceinline__ float span_end(float a0, float a1, float b0, float b1, float c0, float c1, float d)
+{
+    return imin_f(imin_f(fmax_s(a0, a1), fmax_s(b0, b1)), imin_f(imax_f(c0, c1), d));
+}
+
+__device__ __forceinline__ float safe_rcp(float d)
+{
+    const float ooeps = 0x1p-80f;
+    return __fdiv_rn(1.0f, fabsf(d) > ooeps ? d : copysignf(ooeps, d));
+}
+
+// Ray set-up (cuda_tracer_functions.cu:68-89).
+__device__ __forceinline__ void setup_ray(Lane& L, float4 o4, float4 d4)
+{
+    L.ox = o4.x; L.oy = o4.y; L.oz = o4.z; L.tmin = o4.w;
+    L.dx = d4.x; L.dy = d4.y; L.dz = d4.z; L.hitT = d4.w;
+    L.idx = safe_rcp(L.dx); L.idy = safe_rcp(L.dy); L.idz = safe_rcp(L.dz);
+    L.oodx = __fmul_rn(L.ox, L.idx); L.oody = __fmul_rn(L.oy, L.idy); L.oodz = __fmul_rn(L.oz, L.idz);
+    L.leafAddr = 0;
+    L.nodeAddr = 0;
+    L.hitIndex = -1;
+    L.hu = L.hv = 0.0f;
+}
+
+template <class Source>
+__device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_threshold, unsigned int* status)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    int stack[kStackSize + 2];
+    int sp = 0;
+    Lane L;
+    L.nodeAddr = kSentinel;
+    L.leafAddr = 0;
+    L.hitIndex = -1;
+    bool has_ray = false, retired = false;
+
+    for (;;) {
+        // ---- refill: lanes without a ray claim the next slots from the queue.
+        const bool need = !has_ray && !retired;
+        const unsigned needm = __ballot_sync(kFull, need);
+        if (needm) {
+            const int leader = __ffs(needm) - 1;
+            unsigned long long b1 = 0, b2 = 0;
+            unsigned n1 = 0;
+            if ((int)lane == leader) src.claim((unsigned)__popc(needm), b1, n1, b2);
+            b1 = __shfl_sync(kFull, b1, leader);
+            b2 = __shfl_sync(kFull, b2, leader);
+            n1 = __shfl_sync(kFull, n1, leader);
+            if (need) {
+                const unsigned rank = (unsigned)__popc(needm & lt_mask);
+                const unsigned long long slot = rank < n1 ? b1 + rank : b2 + (rank - n1);
+                const int r = src.fetch(slot, L);
+                if (r == 0) {
+                    retired = true;
+                } else if (r > 0) {
+                    stack[0] = kSentinel;
+                    sp = 0;
+                    has_ray = true;
+                }
+            }
+        }
+        if (__all_sync(kFull, retired)) break;
+
+        // ---- traversal until too few lanes are busy.
+        while (__any_sync(kFull, has_ray)) {
+            // Inner nodes until every busy lane has postponed a leaf.
+            for (;;) {
+                const bool in = has_ray && (unsigned)L.nodeAddr < (unsigned)kSentinel;
+                if (!__any_sync(kFull, in)) break;
+                if (in) {
+                    const float4* np = L.nodes + L.nodeAddr;
+                    const float4 n0xy = __ldg(np + 0);
+                    const float4 n1xy = __ldg(np + 1);
+                    const float4 nz = __ldg(np + 2);
+                    const float4 cn = __ldg(np + 3);
+                    int c0 = __float_as_int(cn.x), c1 = __float_as_int(cn.y);
+
+                    const float c0lox = __fmaf_rn(n0xy.x, L.idx, -L.oodx);
+                    const float c0hix = __fmaf_rn(n0xy.y, L.idx, -L.oodx);
+                    const float c0loy = __fmaf_rn(n0xy.z, L.idy, -L.oody);
+                    const float c0hiy = __fmaf_rn(n0xy.w, L.idy, -L.oody);
+                    const float c0loz = __fmaf_rn(nz.x, L.idz, -L.oodz);
+                    const float c0hiz = __fmaf_rn(nz.y, L.idz, -L.oodz);
+                    const float c1loz = __fmaf_rn(nz.z, L.idz, -L.oodz);
+                    const float c1hiz = __fmaf_rn(nz.w, L.idz, -L.oodz);
+                    const float c0min = span_begin(c0lox, c0hix, c0loy, c0hiy, c0loz, c0hiz, L.tmin);
+                    const float c0max = span_end(c0lox, c0hix, c0loy, c0hiy, c0loz, c0hiz, L.hitT);
+                    const float c1lox = __fmaf_rn(n1xy.x, L.idx, -L.oodx);
+                    const float c1hix = __fmaf_rn(n1xy.y, L.idx, -L.oodx);
+                    const float c1loy = __fmaf_rn(n1xy.z, L.idy, -L.oody);
+                    const float c1hiy = __fmaf_rn(n1xy.w, L.idy, -L.oody);
+                    const float c1min = span_begin(c1lox, c1hix, c1loy, c1hiy, c1loz, c1hiz, L.tmin);
+                    const float c1max = span_end(c1lox, c1hix, c1loy, c1hiy, c1loz, c1hiz, L.hitT);
+
+                    const bool swp = c1min < c0min;
+                    const bool t0 = c0max >= c0min;
+                    const bool t1 = c1max >= c1min;
+                    if (!t0 && !t1) {
+                        L.nodeAddr = stack[sp--];
+                    } else {
+                        L.nodeAddr = t0 ? c0 : c1;
+                        if (t0 && t1) {
+                            if (swp) { const int tmp = L.nodeAddr; L.nodeAddr = c1; c1 = tmp; }
+                            if (sp >= kStackSize) {
+                                // Unreachable for validated trees (depth <= 64); a
+                                // corrupt tree abandons the ray and reports it.
+                                atomicOr(status, kStatusStack);
+                                L.nodeAddr = kSentinel;
+                                L.leafAddr = 0;
+                                L.hitIndex = -1;
+                            } else {
+                                stack[++sp] = c1;
+                            }
+                        }
+                    }
+                    if (L.nodeAddr < 0 && L.leafAddr >= 0) {
+                        L.leafAddr = L.nodeAddr;
+                        L.nodeAddr = stack[sp--];
+                    }
+                }
+                if (!__any_sync(kFull, in && L.leafAddr >= 0)) break;
+            }
+
+            // Postponed leaves.
+            if (has_ray) {
+                while (L.leafAddr < 0) {
+                    for (int triAddr = ~L.leafAddr;; triAddr += 3) {
+                        const float4* wp = L.woop + triAddr;
+                        const float4 v00 = __ldg(wp + 0);
+                        const float4 v11 = __ldg(wp + 1);
+                        const float4 v22 = __ldg(wp + 2);
+                        if (__float_as_int(v00.x) == (int)0x80000000) break;
+
+                        const float Oz = __fmaf_rn(-L.oz, v00.z, __fmaf_rn(-L.oy, v00.y, __fmaf_rn(-L.ox, v00.x, v00.w)));
+                        const float Dz = __fmaf_rn(L.dz, v00.z, __fmaf_rn(L.dy, v00.y, __fmul_rn(L.dx, v00.x)));
+                        const float t = __fmul_rn(Oz, __fdiv_rn(1.0f, Dz));
+                        if (t > L.tmin && t < L.hitT) {
+                            const float Ox = __fmaf_rn(L.oz, v11.z, __fmaf_rn(L.oy, v11.y, __fmaf_rn(L.ox, v11.x, v11.w)));
+                            const float Dx = __fmaf_rn(L.dz, v11.z, __fmaf_rn(L.dy, v11.y, __fmul_rn(L.dx, v11.x)));
+                            const float u = __fmaf_rn(t, Dx, Ox);
+                            if (u >= 0.0f) {
+                                const float Oy = __fmaf_rn(L.oz, v22.z, __fmaf_rn(L.oy, v22.y, __fmaf_rn(L.ox, v22.x, v22.w)));
+                                const float Dy = __fmaf_rn(L.dz, v22.z, __fmaf_rn(L.dy, v22.y, __fmul_rn(L.dx, v22.x)));
+                                const float v = __fmaf_rn(t, Dy, Oy);
+                                if (v >= 0.0f && __fadd_rn(u, v) <= 1.0f) {
+                                    L.hitT = t;
+                                    L.hu = u;
+                                    L.hv = v;
+                                    L.hitIndex = triAddr;
+                                    if (L.mode != kClosest) {
+                                        L.nodeAddr = kSentinel;
+                                        break;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    L.leafAddr = L.nodeAddr;
+                    if (L.nodeAddr < 0) L.nodeAddr = stack[sp--];
+                }
+                if (L.nodeAddr == kSentinel) {
+                    src.finish(L);
+                    has_ray = false;
+                }
+            }
+            // Dynamic fetch (kepler_dynamic_fetch.h:308-310).
+            if ((unsigned)__popc(__ballot_sync(kFull, has_ray)) < fetch_threshold) break;
+        }
+    }
+}
+
+// Result record shared by all sources: prim (original triangle id, -1 miss), t, u, v.
+__device__ __forceinline__ int4 hit_record(const Lane& L)
+{
+    const bool hit = L.hitIndex >= 0;
+    const int prim = hit ? (int)__ldg(L.triidx + L.hitIndex) : -1;
+    return make_int4(prim, __float_as_int(L.hitT), __float_as_int(hit ? L.hu : 0.0f), __float_as_int(hit ? L.hv : 0.0f));
+}
+
+}  // namespace rb2dev
