@@ -203,6 +203,44 @@ int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream);
  * each), applies and returns the fastest. */
 int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best, double* best_ms);
 
+/* --------------------------------------------------- allocation-free batch --
+ * No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory: hosts that own all device memory through their own
+ * arena or admit work against a fixed memory budget, and loops in which
+ * cudaMalloc/cudaFree, which can synchronise the device, must not appear.
+ * The caller passes every input and output (BVH buffers, rays, results) in
+ * memory it owns; the only scratch (job table, ray-count prefix, queue head,
+ * status word) lives in a fixed file-scope device array of the library sized
+ * for RB2_NOALLOC_MAX_JOBS jobs (about 18.5 KB, held on every GPU that loads
+ * the library until the process exits).  This entry point calls no
+ * cudaMalloc, cudaFree or other allocating routine.
+ *  - More than RB2_NOALLOC_MAX_JOBS jobs: returns RB2_EINVAL, nothing runs.
+ *  - Every call reuses the same array (it keeps the last call's contents;
+ *    the queue head and status are cleared at the start of each call), so
+ *    calls whose work overlaps on the GPU race and corrupt each other:
+ *    issue them one after another on one stream.
+ *  - The first call on a device resolves the array's device address and the
+ *    launch shape for that device (with that device current); make that first
+ *    call before any stream capture on the device.
+ *  - Buffers: d_nodes/d_woop/d_triidx are a Compact2 layout as produced by
+ *    rb2_bvh_build or accepted by rb2_bvh_from_buffers, 16-byte aligned, and
+ *    d_woop must stay readable for two uint4 past its last row. */
+#define RB2_NOALLOC_MAX_JOBS 256
+
+typedef struct {
+    const float* d_nodes;     /* Compact2 nodes (uint4 words) */
+    const float* d_woop;      /* Woop rows + 2 spare uint4 */
+    const uint32_t* d_triidx; /* parallel to the Woop rows */
+    const float* d_rays;      /* 2 float4 per ray */
+    uint64_t n;
+    uint32_t mode;            /* RB2_MODE_* */
+    uint32_t reserved;
+    const uint8_t* d_mask;    /* nullable stencil */
+    void* d_out;              /* rb2_hit[n] (closest/any) or uint8_t[n] (occlusion) */
+} rb2_noalloc_job;
+
+int rb2_trace_batch_noalloc(const rb2_noalloc_job* jobs, uint32_t n_jobs, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
