@@ -36,6 +36,90 @@ int rb2_camera_rays(const rb2_camera* cam, uint32_t spp, uint64_t seed, int jitt
 /* Same for an explicit list of raster positions (2 floats each). */
 int rb2_camera_rays_at(const rb2_camera* cam, const float* d_raster_xy, uint32_t n, float* d_rays, void* stream);
 
+/* ------------------------------------------------------------- device scene --
+ * Replaces Scene::gpu_prepare / SceneBuffer + MaterialBuffer
+ * (core/scene.cpp:166-339, core/buffer.h:322-360) for the Lambertian +
+ * diffuse-area-light subset the integrators use: per-material albedo and
+ * emission (RGB); every triangle whose material emits is a light
+ * (core/scene.cpp:105-113); lights are chosen uniformly per triangle. */
+typedef struct rb2_scene_dev rb2_scene_dev;
+int rb2_scene_create(const float* v_xyz, uint32_t nv, const uint32_t* idx3, uint32_t ntri,
+                     const uint32_t* tri_material /* nullable: all 0 */, uint32_t n_materials,
+                     const float* albedo_rgb /* nullable: 0.5 */, const float* emission_rgb /* nullable: 0 */,
+                     rb2_scene_dev** out);
+int rb2_scene_destroy(rb2_scene_dev* s);
+int rb2_scene_device_bytes(const rb2_scene_dev* s, uint64_t* bytes);
+
+/* An integrator binds a tracer (BVH) and a device scene and owns the
+ * wavefront scratch (grown on demand, reused across renders).  Replaces
+ * Integrator::render(Scene*, CudaTracer*, void**, uint32_t) (core/integrator.h:59). */
+typedef struct rb2_integrator rb2_integrator;
+int rb2_integrator_create(rb2_tracer* tracer, const rb2_scene_dev* scene, rb2_integrator** out);
+int rb2_integrator_destroy(rb2_integrator* it);
+int rb2_integrator_device_bytes(const rb2_integrator* it, uint64_t* bytes);
+
+/* Ambient occlusion (AmbientOcclusionIntegratorParams, core/params.h:126-131;
+ * integrators/integrator_ao.cu:42-110): one primary ray per pixel centre,
+ * `samples` any-hit rays per hit from the hit point (tmin = 1e-3 t, tmax =
+ * radius), cosine-distributed about the geometric normal facing the viewer.
+ * d_ao[pixel] = unoccluded fraction (0 for pixels whose primary ray misses). */
+typedef struct {
+    uint32_t samples;
+    float radius;
+    uint64_t seed;
+} rb2_ao_params;
+int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params* p, float* d_ao, void* stream);
+
+/* Wavefront path tracing (PathIntegratorParams, core/params.h:88-94;
+ * integrators/integrator_path.cu:43-283, the reference's declared
+ * MODE_MULTI_KERNEL3).  Lambertian surfaces, next-event estimation to a
+ * uniformly chosen emissive triangle combined with BSDF sampling by the
+ * balance heuristic, Russian roulette from bounce rr_start with continue
+ * probability min(rr_prob, luminance(throughput)) and division by it.
+ * Vertices 0..max_depth get NEE; extension rays are traced from vertices
+ * below max_depth.  d_rgb[3*pixel] = mean radiance over spp jittered samples. */
+typedef struct {
+    uint32_t spp;
+    uint32_t max_depth;
+    uint32_t rr_start;
+    float rr_prob;
+    uint64_t seed;
+    uint32_t spp_per_wave;   /* samples per pixel in flight at once (0 = auto) */
+    uint32_t reserved;
+} rb2_pt_params;
+int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, float* d_rgb, void* stream);
+
+/* Bidirectional path tracing with a light-vertex cache
+ * (BidirectionalPathIntegratorLvcParams, core/params.h:103-118;
+ * integrators/integrator_bdpt_lvc_sk.cu:47-514).  Per iteration (one camera
+ * sample per pixel): num_light_paths light subpaths are traced and every
+ * surface vertex is stored in the cache (slots assigned by a prefix scan over
+ * (path, depth), so the cache is deterministic); each camera vertex then adds
+ * emission (s = 0), next-event estimation (s = 1) and `connections`
+ * connections to uniformly chosen cached vertices (s >= 2, scaled by
+ * cached vertices / light paths).  Every strategy of a path of k segments
+ * (k <= max_path_length) is weighted 1/k: all k strategies are sampled, so the
+ * estimator is unbiased.  (The reference weights connections by
+ * 1/((bounce+1)+depth) but gives NEE full weight and omits the cache-size
+ * factor.)  d_rgb[3*pixel] = mean radiance over spp iterations. */
+typedef struct {
+    uint32_t spp;
+    uint32_t max_path_length;   /* segments, camera to light (config 3: 6) */
+    uint32_t num_light_paths;   /* per iteration (0 = one per pixel) */
+    uint32_t connections;       /* cached vertices per camera vertex (1..8) */
+    uint32_t rr_start;
+    float rr_prob;
+    uint64_t seed;
+} rb2_bdpt_params;
+int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_params* p, float* d_rgb, void* stream);
+
+/* Statistics of the last render on this integrator (rays traced per kind). */
+typedef struct {
+    uint64_t primary_rays, extension_rays, shadow_rays, connection_rays, light_rays;
+    uint64_t lvc_vertices;
+} rb2_render_stats;
+int rb2_integrator_stats(rb2_integrator* it, rb2_render_stats* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -213,3 +213,78 @@ def is_tie(woop, triidx, slots, ray8, prim_a, prim_b) -> bool:
     oka, tuva = woop_test(w[sa:sa + 3], ray8, big)
     okb, tuvb = woop_test(w[sb:sb + 3], ray8, big)
     return oka and okb and tuva[0] == tuvb[0]
+
+
+# ---------------------------------------------------------------- shading references
+class _Scene(C.Structure):
+    _fields_ = [("verts", C.c_void_p), ("tris", C.c_void_p), ("tri_mat", C.c_void_p), ("albedo", C.c_void_p),
+                ("emission", C.c_void_p), ("lights", C.c_void_p), ("n_lights", C.c_uint32)]
+
+
+class _Bvh(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("woop", C.c_void_p), ("triidx", C.c_void_p)]
+
+
+def _scene_struct(vertices, indices, tri_mat, albedo, emission, lights):
+    keep = [np.ascontiguousarray(vertices, np.float32), np.ascontiguousarray(indices, np.uint32),
+            np.ascontiguousarray(tri_mat, np.uint32), np.ascontiguousarray(albedo, np.float32),
+            np.ascontiguousarray(emission, np.float32), np.ascontiguousarray(lights, np.uint32)]
+    s = _Scene(*[_p(k) for k in keep[:6]], keep[5].shape[0])
+    return s, keep
+
+
+def _bvh_struct(nodes, woop, triidx):
+    keep = [np.ascontiguousarray(nodes, np.uint32), np.ascontiguousarray(woop, np.uint32),
+            np.ascontiguousarray(triidx, np.uint32)]
+    return _Bvh(*[_p(k) for k in keep]), keep
+
+
+def ao(bvh_buffers, vertices, indices, prim_rays, samples, radius, seed=1, nthreads=0):
+    """FP64 ambient occlusion per primary ray (see rb2_oracle.h)."""
+    L = orc_lib()
+    L.rb2o_ao.argtypes = [C.POINTER(_Bvh), C.POINTER(_Scene), C.c_void_p, C.c_uint32, C.c_uint32, C.c_float,
+                          C.c_uint64, C.c_void_p, C.c_int]
+    L.rb2o_ao.restype = None
+    n_tri = np.asarray(indices).reshape(-1, 3).shape[0]
+    s, ks = _scene_struct(vertices, indices, np.zeros(n_tri, np.uint32), np.zeros((1, 3), np.float32),
+                          np.zeros((1, 3), np.float32), np.zeros(1, np.uint32))
+    b, kb = _bvh_struct(*bvh_buffers)
+    r = np.ascontiguousarray(prim_rays, np.float32).reshape(-1, 8)
+    out = np.empty(r.shape[0], np.float64)
+    L.rb2o_ao(C.byref(b), C.byref(s), _p(r), r.shape[0], samples, radius, seed, _p(out), nthreads)
+    return out
+
+
+def pt(bvh_buffers, vertices, indices, tri_mat, albedo, emission, lights, rays, max_depth, rr_start, rr_prob,
+       seed=1, nthreads=0):
+    """One FP64 path-traced sample per camera ray; returns (n, 3) radiance."""
+    L = orc_lib()
+    L.rb2o_pt.argtypes = [C.POINTER(_Bvh), C.POINTER(_Scene), C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                          C.c_float, C.c_uint64, C.c_void_p, C.c_int]
+    L.rb2o_pt.restype = None
+    s, ks = _scene_struct(vertices, indices, tri_mat, albedo, emission, lights)
+    b, kb = _bvh_struct(*bvh_buffers)
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    out = np.empty((r.shape[0], 3), np.float64)
+    L.rb2o_pt(C.byref(b), C.byref(s), _p(r), r.shape[0], max_depth, rr_start, rr_prob, seed, _p(out), nthreads)
+    return out
+
+
+def bdpt(bvh_buffers, vertices, indices, tri_mat, albedo, emission, lights, cam_rays, n_cam, n_iter, n_light_paths,
+         K, C, rr_start, rr_prob, seed=1, nthreads=0):
+    """FP64 BDPT-LVC mean radiance per camera pixel over n_iter iterations."""
+    L = orc_lib()
+    L.rb2o_bdpt.argtypes = [C_.POINTER(_Bvh), C_.POINTER(_Scene), C_.c_void_p, C_.c_uint32, C_.c_uint32, C_.c_uint32,
+                            C_.c_uint32, C_.c_uint32, C_.c_uint32, C_.c_float, C_.c_uint64, C_.c_void_p, C_.c_int]
+    L.rb2o_bdpt.restype = None
+    s, ks = _scene_struct(vertices, indices, tri_mat, albedo, emission, lights)
+    b, kb = _bvh_struct(*bvh_buffers)
+    r = np.ascontiguousarray(cam_rays, np.float32).reshape(-1, 8)
+    assert r.shape[0] == n_cam * n_iter
+    out = np.empty((n_cam, 3), np.float64)
+    L.rb2o_bdpt(C_.byref(b), C_.byref(s), _p(r), n_cam, n_iter, n_light_paths, K, C, rr_start, rr_prob, seed, _p(out),
+                nthreads)
+    return out
+
+
+C_ = C

@@ -32,6 +32,7 @@
 #include "rb2_oracle.h"
 
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
 #include <omp.h>
@@ -39,6 +40,7 @@
 
 #define RB2O_SENTINEL 0x76543210
 #define RB2O_STACK 64
+#define RB2O_PI 3.14159265358979323846
 
 static inline float as_f(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
 static inline int32_t as_i(float f) { int32_t i; memcpy(&i, &f, 4); return i; }
@@ -261,4 +263,382 @@ uint32_t rb2o_pcg32_next(rb2o_pcg32* r)
     uint32_t xorshifted = (uint32_t)(((old >> 18u) ^ old) >> 27u);
     uint32_t rot = (uint32_t)(old >> 59u);
     return (xorshifted >> rot) | (xorshifted << ((-rot) & 31));
+}
+
+/* ======================================================================= shading
+ * Reference estimators for the integrator tests.  Shading math in double;
+ * rays handed to the traversal restatement are rounded to float. */
+
+typedef struct { double x, y, z; } d3;
+static inline d3 D3(double x, double y, double z) { d3 r = {x, y, z}; return r; }
+static inline d3 dadd(d3 a, d3 b) { return D3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline d3 dsub(d3 a, d3 b) { return D3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline d3 dmul(d3 a, double s) { return D3(a.x * s, a.y * s, a.z * s); }
+static inline double ddot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline d3 dcross(d3 a, d3 b) { return D3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static inline d3 dnorm(d3 v) { return dmul(v, 1.0 / sqrt(ddot(v, v))); }
+static inline d3 vtx(const rb2o_scene* s, uint32_t i) { return D3(s->verts[3 * i], s->verts[3 * i + 1], s->verts[3 * i + 2]); }
+
+/* splitmix64 (Steele, Lea & Flood 2014) keyed draws in [0, 1). */
+static inline uint64_t smix(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static inline double u01(uint64_t seed, uint64_t key, uint32_t dim)
+{
+    return (double)(smix(seed ^ smix(key * 0x100000001B3ull + dim)) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* Orthonormal frame about n (z axis). */
+static void frame(d3 n, d3* x, d3* y)
+{
+    d3 t = fabs(n.x) > 0.99 ? D3(0, 1, 0) : D3(1, 0, 0);
+    *y = dnorm(dcross(n, t));
+    *x = dcross(*y, n);
+}
+
+/* Malley's method over Shirley-Chiu's concentric disk (core/montecarlo.cu:59-106,153-158). */
+static d3 cos_hemi(double u1, double u2)
+{
+    double sx = 1.0 - 2.0 * u1, sy = 1.0 - 2.0 * u2, r, th;
+    if (sx == 0.0 && sy == 0.0) return D3(0, 0, 1);
+    if (sx >= -sy) {
+        if (sx > sy) { r = sx; th = sy > 0.0 ? sy / r : 8.0 + sy / r; }
+        else { r = sy; th = 2.0 - sx / r; }
+    } else {
+        if (sx <= sy) { r = -sx; th = 4.0 - sy / r; }
+        else { r = -sy; th = 6.0 + sx / r; }
+    }
+    th *= RB2O_PI / 4.0;
+    double x = r * cos(th), y = r * sin(th);
+    double z = 1.0 - x * x - y * y;
+    return D3(x, y, z > 0.0 ? sqrt(z) : 0.0);
+}
+
+static inline void mkray(float* r8, d3 o, double tmin, d3 d, double tmax)
+{
+    r8[0] = (float)o.x; r8[1] = (float)o.y; r8[2] = (float)o.z; r8[3] = (float)tmin;
+    r8[4] = (float)d.x; r8[5] = (float)d.y; r8[6] = (float)d.z; r8[7] = (float)tmax;
+}
+
+static inline int occluded(const rb2o_bvh* b, const float* r8)
+{
+    rb2o_hit h;
+    trace_one(b->nodes, b->woop, b->triidx, r8, 1, &h, NULL);
+    return h.prim >= 0;
+}
+
+void rb2o_ao(const rb2o_bvh* b, const rb2o_scene* s, const float* prim_rays, uint32_t n, uint32_t samples,
+             float radius, uint64_t seed, double* out, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        const float* r = prim_rays + 8 * i;
+        rb2o_hit h;
+        trace_one(b->nodes, b->woop, b->triidx, r, 0, &h, NULL);
+        if (h.prim < 0) { out[i] = 0.0; continue; }
+        const uint32_t* t = s->tris + 3 * (size_t)h.prim;
+        d3 v0 = vtx(s, t[0]), v1 = vtx(s, t[1]), v2 = vtx(s, t[2]);
+        d3 ng = dnorm(dcross(dsub(v1, v0), dsub(v2, v0)));
+        d3 d = D3(r[4], r[5], r[6]);
+        if (ddot(ng, d) > 0.0) ng = dmul(ng, -1.0);
+        d3 pos = dadd(D3(r[0], r[1], r[2]), dmul(d, h.t));
+        d3 fx, fy;
+        frame(ng, &fx, &fy);
+        uint64_t open = 0;
+        for (uint32_t k = 0; k < samples; k++) {
+            uint64_t key = (uint64_t)i * samples + k;
+            d3 l = cos_hemi(u01(seed, key, 0), u01(seed, key, 1));
+            d3 w = dadd(dadd(dmul(fx, l.x), dmul(fy, l.y)), dmul(ng, l.z));
+            float r8[8];
+            mkray(r8, pos, 1.0e-3 * (double)h.t, w, radius);
+            if (!occluded(b, r8)) open++;
+        }
+        out[i] = (double)open / (double)samples;
+    }
+    (void)nthreads;
+}
+
+static double tri_area_d(d3 a, d3 b_, d3 c)
+{
+    d3 cr = dcross(dsub(b_, a), dsub(c, a));
+    return 0.5 * sqrt(ddot(cr, cr));
+}
+
+void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t n, uint32_t max_depth,
+             uint32_t rr_start, float rr_prob, uint64_t seed, double* out_rgb, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        double L[3] = {0, 0, 0}, T[3] = {1, 1, 1}, pdf_prev = 0.0;
+        float ray[8];
+        for (int k = 0; k < 8; k++) ray[k] = rays[8 * i + k];
+        const double inv_nl = s->n_lights ? 1.0 / (double)s->n_lights : 0.0;
+        for (uint32_t bnc = 0;; bnc++) {
+            rb2o_hit h;
+            trace_one(b->nodes, b->woop, b->triidx, ray, 0, &h, NULL);
+            if (h.prim < 0) break;
+            const uint32_t* t = s->tris + 3 * (size_t)h.prim;
+            const uint32_t m = s->tri_mat[h.prim];
+            d3 v0 = vtx(s, t[0]), v1 = vtx(s, t[1]), v2 = vtx(s, t[2]);
+            d3 ng = dnorm(dcross(dsub(v1, v0), dsub(v2, v0)));
+            d3 d = D3(ray[4], ray[5], ray[6]);
+            d3 wo = dmul(d, -1.0);
+            d3 pos = dadd(D3(ray[0], ray[1], ray[2]), dmul(d, h.t));
+            const double eps = 1.0e-3 * (double)h.t;
+            const float* E = s->emission + 3 * (size_t)m;
+            if (E[0] > 0.0f || E[1] > 0.0f || E[2] > 0.0f) {
+                double cosl = ddot(ng, wo);
+                if (cosl > 0.0) {
+                    double w = 1.0;
+                    if (bnc > 0) {
+                        double pdf_l = inv_nl * (double)h.t * (double)h.t / (tri_area_d(v0, v1, v2) * cosl);
+                        w = pdf_prev / (pdf_prev + pdf_l);
+                    }
+                    for (int c = 0; c < 3; c++) L[c] += T[c] * E[c] * w;
+                }
+                break;
+            }
+            d3 nrm = ddot(ng, wo) < 0.0 ? dmul(ng, -1.0) : ng;
+            const float* A = s->albedo + 3 * (size_t)m;
+            uint64_t key = (uint64_t)i * 64 + bnc;
+            if (s->n_lights) {
+                uint32_t j = (uint32_t)(u01(seed, key, 0) * s->n_lights);
+                if (j >= s->n_lights) j = s->n_lights - 1;
+                const uint32_t lt = s->lights[j];
+                const uint32_t* lv = s->tris + 3 * (size_t)lt;
+                d3 l0 = vtx(s, lv[0]), l1 = vtx(s, lv[1]), l2 = vtx(s, lv[2]);
+                double su = sqrt(u01(seed, key, 1)), u2 = u01(seed, key, 2);
+                double b0 = 1.0 - su, b1 = u2 * su;
+                d3 lp = dadd(dadd(dmul(l0, b0), dmul(l1, b1)), dmul(l2, 1.0 - b0 - b1));
+                d3 ln = dnorm(dcross(dsub(l1, l0), dsub(l2, l0)));
+                d3 dv = dsub(lp, pos);
+                double dist2 = ddot(dv, dv), dist = sqrt(dist2);
+                d3 wi = dmul(dv, 1.0 / dist);
+                double cos_l = -ddot(ln, wi), cos_s = ddot(nrm, wi);
+                const float* Le = s->emission + 3 * (size_t)s->tri_mat[lt];
+                if (cos_l > 0.0 && cos_s > 0.0 && dist > 0.0) {
+                    double pdf_l = inv_nl * dist2 / (tri_area_d(l0, l1, l2) * cos_l);
+                    double pdf_b = cos_s / RB2O_PI;
+                    double w = (bnc == max_depth) ? 1.0 : pdf_l / (pdf_l + pdf_b);
+                    float sr[8];
+                    mkray(sr, pos, eps, wi, dist * (1.0 - 1.0e-3));
+                    if (!occluded(b, sr))
+                        for (int c = 0; c < 3; c++) L[c] += T[c] * (A[c] / RB2O_PI) * Le[c] * cos_s * w / pdf_l;
+                }
+            }
+            if (bnc >= max_depth) break;
+            d3 fx, fy;
+            frame(nrm, &fx, &fy);
+            d3 l = cos_hemi(u01(seed, key, 3), u01(seed, key, 4));
+            double pdf = l.z / RB2O_PI;
+            if (!(pdf > 0.0)) break;
+            d3 wi = dnorm(dadd(dadd(dmul(fx, l.x), dmul(fy, l.y)), dmul(nrm, l.z)));
+            for (int c = 0; c < 3; c++) T[c] *= A[c];
+            pdf_prev = pdf;
+            if (T[0] <= 0.0 && T[1] <= 0.0 && T[2] <= 0.0) break;
+            if (bnc >= rr_start) {
+                double lum = 0.212671 * T[0] + 0.715160 * T[1] + 0.072169 * T[2];
+                double q = lum < rr_prob ? lum : rr_prob;
+                if (!(u01(seed, key, 5) < q)) break;
+                for (int c = 0; c < 3; c++) T[c] /= q;
+            }
+            mkray(ray, pos, eps, wi, 3.402823466e+38);
+        }
+        for (int c = 0; c < 3; c++) out_rgb[3 * i + c] = L[c];
+    }
+    (void)nthreads;
+}
+
+/* ---- BDPT with a light-vertex cache ------------------------------------------------
+ * Per iteration: n_light_paths light subpaths (uniform emissive triangle,
+ * uniform point, cosine direction), every non-emitter surface vertex y1..y_Dl
+ * cached (Dl = K - 2); then one camera path per camera ray with emission
+ * (s = 0), NEE (s = 1) and C uniform cache connections (s >= 2, scaled by
+ * cache size / light paths), each strategy of a k-segment path weighted 1/k. */
+typedef struct { d3 pos, nrm, beta; uint32_t s, mat; } lvc_vertex;
+
+void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, uint32_t n_cam, uint32_t n_iter,
+               uint32_t n_light_paths, uint32_t K, uint32_t C, uint32_t rr_start, float rr_prob, uint64_t seed,
+               double* out_rgb, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#endif
+    const uint32_t Dl = K >= 2 ? K - 2 : 0;
+    const double inv_nl = s->n_lights ? 1.0 / (double)s->n_lights : 0.0;
+    lvc_vertex* sparse = (lvc_vertex*)calloc((size_t)n_light_paths * (Dl ? Dl : 1), sizeof(lvc_vertex));
+    uint8_t* valid = (uint8_t*)calloc((size_t)n_light_paths * (Dl ? Dl : 1), 1);
+    lvc_vertex* dense = (lvc_vertex*)calloc((size_t)n_light_paths * (Dl ? Dl : 1), sizeof(lvc_vertex));
+    for (size_t i = 0; i < (size_t)n_cam * 3; i++) out_rgb[i] = 0.0;
+    for (uint32_t it = 0; it < n_iter; it++) {
+        memset(valid, 0, (size_t)n_light_paths * (Dl ? Dl : 1));
+        const uint64_t ls = seed ^ 0xA24BAED4963EE407ull;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+#endif
+        for (int64_t p = 0; p < (int64_t)n_light_paths; p++) {
+            if (!s->n_lights || Dl == 0) continue;
+            const uint64_t key = (uint64_t)it * n_light_paths + (uint64_t)p;
+            uint32_t j = (uint32_t)(u01(ls, key, 0) * s->n_lights);
+            if (j >= s->n_lights) j = s->n_lights - 1;
+            const uint32_t lt = s->lights[j];
+            const uint32_t* lv = s->tris + 3 * (size_t)lt;
+            d3 l0 = vtx(s, lv[0]), l1 = vtx(s, lv[1]), l2 = vtx(s, lv[2]);
+            double su = sqrt(u01(ls, key, 1)), u2 = u01(ls, key, 2);
+            double b0 = 1.0 - su, b1 = u2 * su;
+            d3 y0 = dadd(dadd(dmul(l0, b0), dmul(l1, b1)), dmul(l2, 1.0 - b0 - b1));
+            d3 ln = dnorm(dcross(dsub(l1, l0), dsub(l2, l0)));
+            d3 fx, fy;
+            frame(ln, &fx, &fy);
+            d3 l = cos_hemi(u01(ls, key, 3), u01(ls, key, 4));
+            d3 dir = dnorm(dadd(dadd(dmul(fx, l.x), dmul(fy, l.y)), dmul(ln, l.z)));
+            const float* Le = s->emission + 3 * (size_t)s->tri_mat[lt];
+            double kk = (double)s->n_lights * tri_area_d(l0, l1, l2) * RB2O_PI;
+            double beta[3] = {Le[0] * kk, Le[1] * kk, Le[2] * kk};
+            float ray[8];
+            mkray(ray, y0, 1.0e-4, dir, 3.402823466e+38);
+            for (uint32_t d = 1; d <= Dl; d++) {
+                rb2o_hit h;
+                trace_one(b->nodes, b->woop, b->triidx, ray, 0, &h, NULL);
+                if (h.prim < 0) break;
+                const uint32_t* t = s->tris + 3 * (size_t)h.prim;
+                const uint32_t m = s->tri_mat[h.prim];
+                const float* E = s->emission + 3 * (size_t)m;
+                if (E[0] > 0.0f || E[1] > 0.0f || E[2] > 0.0f) break;
+                d3 v0 = vtx(s, t[0]), v1 = vtx(s, t[1]), v2 = vtx(s, t[2]);
+                d3 ng = dnorm(dcross(dsub(v1, v0), dsub(v2, v0)));
+                d3 dd = D3(ray[4], ray[5], ray[6]);
+                d3 wo = dmul(dd, -1.0);
+                d3 nrm = ddot(ng, wo) < 0.0 ? dmul(ng, -1.0) : ng;
+                d3 pos = dadd(D3(ray[0], ray[1], ray[2]), dmul(dd, h.t));
+                size_t slot = (size_t)p * Dl + (d - 1);
+                sparse[slot].pos = pos; sparse[slot].nrm = nrm;
+                sparse[slot].beta = D3(beta[0], beta[1], beta[2]);
+                sparse[slot].s = d + 1; sparse[slot].mat = m;
+                valid[slot] = 1;
+                if (d >= Dl) break;
+                const float* A = s->albedo + 3 * (size_t)m;
+                d3 lc = cos_hemi(u01(ls, key, 8 + 8 * d), u01(ls, key, 9 + 8 * d));
+                if (!(lc.z > 0.0)) break;
+                frame(nrm, &fx, &fy);
+                d3 wi = dnorm(dadd(dadd(dmul(fx, lc.x), dmul(fy, lc.y)), dmul(nrm, lc.z)));
+                double lum = 0.212671 * A[0] + 0.715160 * A[1] + 0.072169 * A[2];
+                double q = lum < 1.0 ? lum : 1.0;
+                if (d < rr_start) q = 1.0; else if (q > rr_prob) q = rr_prob;
+                if (!(q > 0.0 && u01(ls, key, 10 + 8 * d) < q)) break;
+                for (int c = 0; c < 3; c++) beta[c] *= A[c] / q;
+                mkray(ray, pos, 1.0e-3 * (double)h.t, wi, 3.402823466e+38);
+            }
+        }
+        uint32_t M = 0;
+        for (size_t i = 0; i < (size_t)n_light_paths * Dl; i++)
+            if (valid[i]) dense[M++] = sparse[i];
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+#endif
+        for (int64_t ci = 0; ci < (int64_t)n_cam; ci++) {
+            double L[3] = {0, 0, 0}, T[3] = {1, 1, 1};
+            float ray[8];
+            for (int k = 0; k < 8; k++) ray[k] = cam_rays[8 * ((size_t)it * n_cam + ci) + k];
+            const uint64_t key = (uint64_t)it * n_cam + (uint64_t)ci;
+            for (uint32_t i = 1; i <= K; i++) {
+                rb2o_hit h;
+                trace_one(b->nodes, b->woop, b->triidx, ray, 0, &h, NULL);
+                if (h.prim < 0) break;
+                const uint32_t* t = s->tris + 3 * (size_t)h.prim;
+                const uint32_t m = s->tri_mat[h.prim];
+                d3 v0 = vtx(s, t[0]), v1 = vtx(s, t[1]), v2 = vtx(s, t[2]);
+                d3 ng = dnorm(dcross(dsub(v1, v0), dsub(v2, v0)));
+                d3 dd = D3(ray[4], ray[5], ray[6]);
+                d3 wo = dmul(dd, -1.0);
+                d3 pos = dadd(D3(ray[0], ray[1], ray[2]), dmul(dd, h.t));
+                const double eps = 1.0e-3 * (double)h.t;
+                const float* E = s->emission + 3 * (size_t)m;
+                if (E[0] > 0.0f || E[1] > 0.0f || E[2] > 0.0f) {
+                    if (ddot(ng, wo) > 0.0)
+                        for (int c = 0; c < 3; c++) L[c] += T[c] * E[c] / (double)i;
+                    break;
+                }
+                d3 nrm = ddot(ng, wo) < 0.0 ? dmul(ng, -1.0) : ng;
+                const float* A = s->albedo + 3 * (size_t)m;
+                uint64_t vkey = key * 64 + i;
+                if (s->n_lights && i + 1 <= K) {
+                    uint32_t j = (uint32_t)(u01(seed, vkey, 0) * s->n_lights);
+                    if (j >= s->n_lights) j = s->n_lights - 1;
+                    const uint32_t lt = s->lights[j];
+                    const uint32_t* lv = s->tris + 3 * (size_t)lt;
+                    d3 l0 = vtx(s, lv[0]), l1 = vtx(s, lv[1]), l2 = vtx(s, lv[2]);
+                    double su = sqrt(u01(seed, vkey, 1)), u2 = u01(seed, vkey, 2);
+                    double b0 = 1.0 - su, b1 = u2 * su;
+                    d3 lp = dadd(dadd(dmul(l0, b0), dmul(l1, b1)), dmul(l2, 1.0 - b0 - b1));
+                    d3 ln = dnorm(dcross(dsub(l1, l0), dsub(l2, l0)));
+                    d3 dv = dsub(lp, pos);
+                    double dist2 = ddot(dv, dv), dist = sqrt(dist2);
+                    d3 wi = dmul(dv, 1.0 / dist);
+                    double cos_l = -ddot(ln, wi), cos_s = ddot(nrm, wi);
+                    const float* Le = s->emission + 3 * (size_t)s->tri_mat[lt];
+                    if (cos_l > 0.0 && cos_s > 0.0 && dist > 0.0) {
+                        double pdf_l = inv_nl * dist2 / (tri_area_d(l0, l1, l2) * cos_l);
+                        float sr[8];
+                        mkray(sr, pos, eps, wi, dist * (1.0 - 1.0e-3));
+                        if (!occluded(b, sr))
+                            for (int c = 0; c < 3; c++)
+                                L[c] += T[c] * (A[c] / RB2O_PI) * Le[c] * cos_s / pdf_l / (double)(i + 1);
+                    }
+                }
+                if (M > 0 && i + 2 <= K) {
+                    for (uint32_t cidx = 0; cidx < C; cidx++) {
+                        uint32_t v = (uint32_t)(u01(seed, vkey, 16 + cidx) * M);
+                        if (v >= M) v = M - 1;
+                        const lvc_vertex* V = &dense[v];
+                        if (V->s + i > K) continue;
+                        d3 dv = dsub(V->pos, pos);
+                        double dist2 = ddot(dv, dv), dist = sqrt(dist2);
+                        if (!(dist > 0.0)) continue;
+                        d3 dir = dmul(dv, 1.0 / dist);
+                        double cos_c = ddot(nrm, dir), cos_v = -ddot(V->nrm, dir);
+                        if (!(cos_c > 0.0 && cos_v > 0.0)) continue;
+                        float cr[8];
+                        mkray(cr, pos, eps, dir, dist * (1.0 - 1.0e-3));
+                        if (occluded(b, cr)) continue;
+                        const float* Av = s->albedo + 3 * (size_t)V->mat;
+                        double g = cos_c * cos_v / dist2 / (RB2O_PI * RB2O_PI) * ((double)M / (double)n_light_paths) /
+                                   ((double)(V->s + i) * (double)C);
+                        double bv[3] = {V->beta.x, V->beta.y, V->beta.z};
+                        for (int c = 0; c < 3; c++) L[c] += T[c] * A[c] * Av[c] * bv[c] * g;
+                    }
+                }
+                if (i >= K) break;
+                d3 fx, fy;
+                frame(nrm, &fx, &fy);
+                d3 lc = cos_hemi(u01(seed, vkey, 3), u01(seed, vkey, 4));
+                if (!(lc.z > 0.0)) break;
+                d3 wi = dnorm(dadd(dadd(dmul(fx, lc.x), dmul(fy, lc.y)), dmul(nrm, lc.z)));
+                for (int c = 0; c < 3; c++) T[c] *= A[c];
+                if (T[0] <= 0.0 && T[1] <= 0.0 && T[2] <= 0.0) break;
+                if (i - 1 >= rr_start) {
+                    double lum = 0.212671 * T[0] + 0.715160 * T[1] + 0.072169 * T[2];
+                    double q = lum < rr_prob ? lum : rr_prob;
+                    if (!(u01(seed, vkey, 5) < q)) break;
+                    for (int c = 0; c < 3; c++) T[c] /= q;
+                }
+                mkray(ray, pos, eps, wi, 3.402823466e+38);
+            }
+            for (int c = 0; c < 3; c++) out_rgb[3 * ci + c] += L[c] / (double)n_iter;
+        }
+    }
+    free(sparse);
+    free(valid);
+    free(dense);
+    (void)nthreads;
 }

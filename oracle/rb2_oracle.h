@@ -40,6 +40,48 @@ int rb2o_woop_test(const uint32_t* woop12, const float* ray8, float tmax, float*
 void rb2o_bruteforce(const uint32_t* woop, const uint32_t* triidx, uint32_t n_woop_u4,
                      const float* rays, uint32_t n, rb2o_hit* out, int nthreads);
 
+/* ---- shading references (FP64 accumulation) ---------------------------------
+ * Scene for the integrator references: vertices (xyz), triangles (3 indices),
+ * per-triangle material, per-material albedo/emission (rgb), emissive
+ * triangle list (uniform light choice, integrators/integrator_path.cu:122). */
+typedef struct {
+    const float* verts;
+    const uint32_t* tris;
+    const uint32_t* tri_mat;
+    const float* albedo;
+    const float* emission;
+    const uint32_t* lights;
+    uint32_t n_lights;
+} rb2o_scene;
+
+typedef struct {
+    const uint32_t* nodes;
+    const uint32_t* woop;
+    const uint32_t* triidx;
+} rb2o_bvh;
+
+/* Ambient occlusion (integrators/integrator_ao.cu:51-84): per primary ray, the
+ * unoccluded fraction of `samples` cosine-distributed rays about the
+ * viewer-facing geometric normal, tmin 1e-3 t, tmax radius; 0 on a miss. */
+void rb2o_ao(const rb2o_bvh* b, const rb2o_scene* s, const float* prim_rays, uint32_t n, uint32_t samples,
+             float radius, uint64_t seed, double* out, int nthreads);
+
+/* One path-traced sample per camera ray (integrators/integrator_path.cu:56-260
+ * with unbiased Russian roulette): NEE to a uniformly chosen emissive triangle
+ * and BSDF sampling combined by the balance heuristic; out_rgb: 3 per ray. */
+void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t n, uint32_t max_depth,
+             uint32_t rr_start, float rr_prob, uint64_t seed, double* out_rgb, int nthreads);
+
+/* BDPT with a light-vertex cache (integrators/integrator_bdpt_lvc_sk.cu:47-514,
+ * with uniform 1/k weights over all k strategies of a k-segment path and the
+ * cache-size factor): n_iter iterations, each tracing n_light_paths light
+ * subpaths into the cache and one camera path per camera ray
+ * (cam_rays: n_iter x n_cam rays, iteration-major).  out_rgb: mean over
+ * iterations, 3 per camera pixel. */
+void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, uint32_t n_cam, uint32_t n_iter,
+               uint32_t n_light_paths, uint32_t K, uint32_t C, uint32_t rr_start, float rr_prob, uint64_t seed,
+               double* out_rgb, int nthreads);
+
 /* PCG32 (O'Neill 2014, pcg32_srandom_r / pcg32_random_r), the generator the
  * product uses for every seeded stream. */
 typedef struct { uint64_t state, inc; } rb2o_pcg32;

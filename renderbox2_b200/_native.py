@@ -47,6 +47,25 @@ class BatchConfig(C.Structure):
                 ("chunk", C.c_uint32), ("node_order", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class AoParams(C.Structure):
+    _fields_ = [("samples", C.c_uint32), ("radius", C.c_float), ("seed", C.c_uint64)]
+
+
+class PtParams(C.Structure):
+    _fields_ = [("spp", C.c_uint32), ("max_depth", C.c_uint32), ("rr_start", C.c_uint32), ("rr_prob", C.c_float),
+                ("seed", C.c_uint64), ("spp_per_wave", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class BdptParams(C.Structure):
+    _fields_ = [("spp", C.c_uint32), ("max_path_length", C.c_uint32), ("num_light_paths", C.c_uint32),
+                ("connections", C.c_uint32), ("rr_start", C.c_uint32), ("rr_prob", C.c_float), ("seed", C.c_uint64)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("primary_rays", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("connection_rays", C.c_uint64), ("light_rays", C.c_uint64), ("lvc_vertices", C.c_uint64)]
+
+
 class Camera(C.Structure):
     _fields_ = [
         ("raster_to_camera", C.c_float * 16), ("camera_to_world", C.c_float * 16),
@@ -92,6 +111,16 @@ SIGNATURES = {
     "rb2_batch_capture": (C.c_int, [P, P]),
     "rb2_batch_status": (C.c_int, [P, C.POINTER(U32), P]),
     "rb2_batch_autotune": (C.c_int, [P, P, U32, C.POINTER(BatchConfig), C.POINTER(C.c_double)]),
+    "rb2_scene_create": (C.c_int, [P, U32, P, U32, P, U32, P, P, C.POINTER(P)]),
+    "rb2_scene_destroy": (C.c_int, [P]),
+    "rb2_scene_device_bytes": (C.c_int, [P, C.POINTER(U64)]),
+    "rb2_integrator_create": (C.c_int, [P, P, C.POINTER(P)]),
+    "rb2_integrator_destroy": (C.c_int, [P]),
+    "rb2_integrator_device_bytes": (C.c_int, [P, C.POINTER(U64)]),
+    "rb2_integrator_stats": (C.c_int, [P, C.POINTER(RenderStats), P]),
+    "rb2_render_ao": (C.c_int, [P, C.POINTER(Camera), C.POINTER(AoParams), P, P]),
+    "rb2_render_pt": (C.c_int, [P, C.POINTER(Camera), C.POINTER(PtParams), P, P]),
+    "rb2_render_bdpt": (C.c_int, [P, C.POINTER(Camera), C.POINTER(BdptParams), P, P]),
     "rb2_camera_init": (C.c_int, [C.POINTER(Camera), P, P, P, U32, U32, C.c_float]),
     "rb2_camera_rays": (C.c_int, [C.POINTER(Camera), U32, U64, I32, P, P]),
     "rb2_camera_rays_at": (C.c_int, [C.POINTER(Camera), P, U32, P, P]),

@@ -112,6 +112,15 @@ int build_tree(const float* v, uint32_t nv, const uint32_t* idx, uint32_t ntri, 
 int validate_compact2(const uint32_t* nodes, uint64_t n_nodes_u4, const uint32_t* woop, uint64_t n_woop_u4,
                       const uint32_t* triidx, uint64_t n_triidx, uint32_t n_tris_hint, uint32_t* max_depth_out);
 
+// Device view of a tracer's BVH (defined in rb2_trace.cu) for integrator kernels.
+struct DeviceBvhView {
+    const void* nodes;    // float4*
+    const void* woop;     // float4*
+    const uint32_t* triidx;
+    unsigned int* status;
+};
+DeviceBvhView device_bvh(const rb2_tracer* t);
+
 inline uint32_t f2u(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
 inline float u2f(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
 

@@ -1,0 +1,1210 @@
+// Device scene, integrator scratch and the wavefront integrators (AO, path
+// tracing, BDPT with a light-vertex cache).
+//
+// Every ray query goes through persistent_trace (rb2_traverse.cuh) with an
+// integrator-specific ray source: rays are generated inside the traversal
+// kernel's fetch() from path state and consumed in finish(), so secondary-ray
+// buffers never round-trip through HBM.
+#include "rb2.h"
+#include "rb2_internal.h"
+#include "rb2_render.h"
+#include "rb2_camera.cuh"
+#include "rb2_shading.cuh"
+#include "rb2_traverse.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+using namespace rb2;
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char* what) { return fail(RB2_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)); }
+
+#define RB2_CUDA(call, what)                               \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+template <class T>
+int grow(T*& p, uint64_t& cap, uint64_t n)
+{
+    if (n <= cap) return RB2_OK;
+    cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, sizeof(T) * std::max<uint64_t>(n, 1));
+    if (e != cudaSuccess) return fail(RB2_ENOMEM, std::string("integrator scratch: ") + cudaGetErrorString(e));
+    cap = n;
+    return RB2_OK;
+}
+
+}  // namespace
+
+struct rb2_scene_dev {
+    float4* d_verts = nullptr;     // xyz, w unused
+    uint4* d_tris = nullptr;       // vertex indices + material id
+    float4* d_albedo = nullptr;    // per material
+    float4* d_emission = nullptr;  // per material
+    uint32_t* d_lights = nullptr;  // emissive triangle ids
+    uint32_t nv = 0, ntri = 0, n_mat = 0, n_lights = 0;
+    uint64_t bytes = 0;
+};
+
+// Wavefront path state, one entry per path of the wave (SoA).
+struct PathState {
+    float4* T = nullptr;        // throughput rgb, w = solid-angle pdf of the last BSDF sample
+    float4* L = nullptr;        // radiance gathered by the path
+    float4* ray = nullptr;      // current extension ray (2 per path)
+    int4* hit = nullptr;        // extension hit
+    float4* sray = nullptr;     // pending shadow / connection ray (2 per path)
+    float4* sc = nullptr;       // its contribution when unoccluded
+    uint32_t* q[2] = {nullptr, nullptr};  // active-path queues (ping-pong)
+    uint32_t* qs = nullptr;     // shadow queue
+    uint64_t cap = 0;
+};
+
+// Device-side counters of one wave.
+struct WaveCounters {
+    uint32_t n_ext[2];
+    uint32_t n_shadow;
+    uint32_t n_conn;
+    unsigned long long head_ext;     // traversal queue heads
+    unsigned long long head_shadow;
+    unsigned long long head_conn;
+    unsigned long long stats[6];     // rb2_render_stats order
+    uint32_t lvc_count;              // dense light-vertex-cache size of this iteration
+    uint32_t pad;
+};
+
+// Light-vertex cache and light-path state of the BDPT integrator.
+struct BdptState {
+    // light subpaths
+    float4* lray = nullptr;     // 2 per light path
+    float4* lbeta = nullptr;    // throughput arriving at the next vertex
+    int4* lhit = nullptr;
+    uint32_t* lq[2] = {nullptr, nullptr};
+    uint64_t cap_paths = 0;
+    // cache, sparse (path, depth) slots and dense compacted copy
+    float4* s_pos = nullptr;    // xyz, w = light-subpath vertex count s (as float)
+    float4* s_nrm = nullptr;    // normal facing the arriving light, w = material id bits
+    float4* s_beta = nullptr;
+    uint8_t* s_valid = nullptr;
+    float4* d_pos = nullptr;
+    float4* d_nrm = nullptr;
+    float4* d_beta = nullptr;
+    uint32_t* block_sums = nullptr;
+    uint64_t cap_slots = 0;
+    // connection rays of camera vertices (connections per path)
+    float4* cray = nullptr;
+    float4* cc = nullptr;
+    uint32_t* cq = nullptr;
+    uint64_t cap_conn = 0;
+};
+
+struct rb2_integrator {
+    rb2_tracer* tracer = nullptr;
+    const rb2_scene_dev* scene = nullptr;
+    int sms = 0;
+    // generic scratch
+    float4* d_rays = nullptr; uint64_t cap_rays = 0;        // 2 per ray
+    int4* d_hits = nullptr; uint64_t cap_hits = 0;
+    uint32_t* d_count = nullptr; uint64_t cap_count = 0;
+    unsigned long long* d_counters = nullptr;                // queue heads (16)
+    float4* d_accum = nullptr; uint64_t cap_accum = 0;
+    PathState ps;
+    BdptState bd;
+    WaveCounters* d_wave = nullptr;
+    uint64_t bytes() const
+    {
+        return cap_rays * 32 + cap_hits * 16 + cap_count * 4 + 16 * 8 + cap_accum * 16 + ps.cap * (16 * 8 + 12) +
+               sizeof(WaveCounters) + bd.cap_paths * (32 + 16 + 16 + 8) + bd.cap_slots * (6 * 16 + 1) +
+               bd.cap_conn * (32 + 16 + 4);
+    }
+};
+
+namespace rb2dev {
+
+using WaveCountersDev = ::WaveCounters;
+
+// ---- AO ray source ------------------------------------------------------------------
+// Slot = pixel * samples + k.  fetch() builds AO ray k of the pixel from its
+// primary hit (integrators/integrator_ao.cu:51-84): origin = hit point,
+// tmin = 1e-3 * t (the reference's epsilon), tmax = radius, direction
+// cosine-distributed about the geometric normal facing the viewer.
+struct AoSource {
+    const float4* nodes;
+    const float4* woop;
+    const uint32_t* triidx;
+    const float4* prim_rays;
+    const int4* hits;
+    const float4* verts;
+    const uint4* tris;
+    uint32_t* counts;
+    unsigned long long* counter;
+    uint64_t n_slots;
+    uint32_t samples;
+    float radius;
+    uint64_t seed;
+
+    __device__ __forceinline__ void claim(unsigned count, unsigned long long& b1, unsigned& n1, unsigned long long& b2)
+    {
+        b1 = atomicAdd(counter, (unsigned long long)count);
+        n1 = count;
+        b2 = 0;
+    }
+
+    __device__ __forceinline__ int fetch(unsigned long long slot, Lane& L) const
+    {
+        if (slot >= n_slots) return 0;
+        const uint64_t pix = slot / samples;
+        const int4 h = hits[pix];
+        if (h.x < 0) return -1;
+        const float t = __int_as_float(h.y);
+        const float4 o4 = prim_rays[2 * pix], d4 = prim_rays[2 * pix + 1];
+        const float3 pos = f3(fmaf(d4.x, t, o4.x), fmaf(d4.y, t, o4.y), fmaf(d4.z, t, o4.z));
+        const uint4 tri = tris[h.x];
+        const float3 v0 = xyz(verts[tri.x]), v1 = xyz(verts[tri.y]), v2 = xyz(verts[tri.z]);
+        float3 ng = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
+        if (dot3(ng, xyz(d4)) > 0.0f) ng = mul(ng, -1.0f);
+        const Frame fr = frame_from_z(ng);
+        const float3 dir = to_world(fr, cosine_hemisphere(rng_u01(seed, slot, 0), rng_u01(seed, slot, 1)));
+        L.nodes = nodes;
+        L.woop = woop;
+        L.triidx = triidx;
+        L.mode = kOcclusion;
+        L.job = 0;
+        L.ray = pix;
+        setup_ray(L, make_float4(pos.x, pos.y, pos.z, 1.0e-3f * t), make_float4(dir.x, dir.y, dir.z, radius));
+        return 1;
+    }
+
+    __device__ __forceinline__ void finish(const Lane& L) const
+    {
+        if (L.hitIndex < 0) atomicAdd(&counts[L.ray], 1u);
+    }
+};
+
+template <int BLOCK, class Src>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_persistent(Src src, uint32_t fetch_threshold, unsigned int* status)
+{
+    persistent_trace(src, fetch_threshold, status);
+}
+
+__global__ void k_ao_finalize(const int4* hits, const uint32_t* counts, uint32_t npix, uint32_t samples, float* out)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x)
+        out[i] = hits[i].x >= 0 ? (float)counts[i] / (float)samples : 0.0f;
+}
+
+// ---- path tracing -----------------------------------------------------------------
+// Random dimensions per (sample key, vertex b): camera jitter uses dims 0-1,
+// vertex b uses 8 dims from 2 + 8b.
+enum : uint32_t { kDimLight = 0, kDimLightU = 1, kDimLightV = 2, kDimBsdfU = 3, kDimBsdfV = 4, kDimRR = 5 };
+__device__ __forceinline__ uint32_t vdim(uint32_t b, uint32_t d) { return 2u + 8u * b + d; }
+
+struct SceneView {
+    const float4* verts;
+    const uint4* tris;
+    const float4* albedo;
+    const float4* emission;
+    const uint32_t* lights;
+    uint32_t n_lights;
+};
+
+// Queue-driven ray source: the i-th entry of `queue` names a path whose ray
+// is in `rays`; `n` (device) is the queue length written by the previous
+// kernel, so no host round trip is needed between stages.
+struct QueueSource {
+    const float4* nodes;
+    const float4* woop;
+    const uint32_t* triidx;
+    const uint32_t* queue;
+    const uint32_t* n;
+    const float4* rays;
+    unsigned long long* head;
+    uint32_t mode;
+    // closest hit: store the hit record; occlusion: add the pending contribution
+    // to L when unoccluded, or (L == nullptr) clear `contrib` when occluded
+    int4* hits;
+    float4* L;
+    float4* contrib;
+
+    __device__ __forceinline__ void claim(unsigned count, unsigned long long& b1, unsigned& n1, unsigned long long& b2)
+    {
+        b1 = atomicAdd(head, (unsigned long long)count);
+        n1 = count;
+        b2 = 0;
+    }
+
+    __device__ __forceinline__ int fetch(unsigned long long slot, Lane& L_) const
+    {
+        if (slot >= (unsigned long long)__ldg(n)) return 0;
+        const uint32_t path = __ldg(queue + slot);
+        L_.nodes = nodes;
+        L_.woop = woop;
+        L_.triidx = triidx;
+        L_.mode = mode;
+        L_.job = 0;
+        L_.ray = path;
+        setup_ray(L_, rays[2 * (size_t)path], rays[2 * (size_t)path + 1]);
+        return 1;
+    }
+
+    __device__ __forceinline__ void finish(const Lane& L_) const
+    {
+        if (mode == kClosest) {
+            hits[L_.ray] = hit_record(L_);
+        } else if (L == nullptr) {
+            if (L_.hitIndex >= 0) contrib[L_.ray] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        } else if (L_.hitIndex < 0) {
+            const float4 c = contrib[L_.ray];
+            float4 a = L[L_.ray];
+            L[L_.ray] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w);
+        }
+    }
+};
+
+// Warp-aggregated append: returns this lane's slot (valid only when pred).
+__device__ __forceinline__ uint32_t warp_append(uint32_t* count, bool pred)
+{
+    const unsigned act = __activemask();
+    const unsigned m = __ballot_sync(act, pred);
+    if (!m) return 0;
+    const int leader = __ffs(m) - 1;
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+    base = __shfl_sync(act, base, leader);
+    return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+}
+
+__global__ void k_pt_camera(CamArgs cam, uint64_t seed, uint32_t npix, uint32_t paths, uint32_t sample0,
+                            float4* rays, float4* T, float4* L, uint32_t* q0, WaveCountersDev* wc)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) wc->n_ext[0] = paths;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < paths; p += gridDim.x * blockDim.x) {
+        const uint32_t pix = p % npix;
+        const uint64_t key = (uint64_t)(sample0 + p / npix) * npix + pix;
+        const float jx = rng_u01(seed, key, 0), jy = rng_u01(seed, key, 1);
+        float4 o, d;
+        camera_ray(cam.r2c, cam.c2w, (float)(pix % cam.width) + jx, (float)(pix / cam.width) + jy, o, d);
+        rays[2 * (size_t)p] = o;
+        rays[2 * (size_t)p + 1] = d;
+        T[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        L[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        q0[p] = p;
+    }
+}
+
+__global__ void k_pt_bounce_reset(WaveCountersDev* wc, uint32_t next)
+{
+    wc->n_ext[next] = 0;
+    wc->n_shadow = 0;
+    wc->n_conn = 0;
+    wc->head_ext = 0;
+    wc->head_shadow = 0;
+    wc->head_conn = 0;
+}
+
+__device__ __forceinline__ float tri_area(float3 v0, float3 v1, float3 v2)
+{
+    return 0.5f * sqrtf(dot3(cross3(sub(v1, v0), sub(v2, v0)), cross3(sub(v1, v0), sub(v2, v0))));
+}
+
+// Shade every path of the current queue at vertex b (integrator_path.cu:84-254):
+// emission (MIS-weighted after the first vertex), next-event estimation with
+// a shadow ray, BSDF sampling of the continuation, Russian roulette.
+__global__ void k_pt_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t sample0, uint32_t b, uint32_t max_depth,
+                           uint32_t rr_start, float rr_prob, const uint32_t* q_in, uint32_t* q_out, float4* rays,
+                           const int4* hits, float4* T, float4* L, float4* srays, float4* sc_out, uint32_t* qs,
+                           WaveCountersDev* wc, uint32_t cur)
+{
+    const uint32_t n = wc->n_ext[cur];
+    const uint32_t next = cur ^ 1u;
+    const float inv_nl = sc.n_lights ? 1.0f / (float)sc.n_lights : 0.0f;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        bool cont = false, shadow = false;
+        uint32_t path = 0;
+        float4 new_o, new_d, so, sd, scv;
+        if (i < n) {
+            path = q_in[i];
+            const int4 h = hits[path];
+            if (h.x >= 0) {
+                const uint32_t pix = path % npix;
+                const uint64_t key = (uint64_t)(sample0 + path / npix) * npix + pix;
+                const float4 o4 = rays[2 * (size_t)path], d4 = rays[2 * (size_t)path + 1];
+                const float t = __int_as_float(h.y);
+                const float3 d = xyz(d4);
+                const float3 pos = f3(fmaf(d.x, t, o4.x), fmaf(d.y, t, o4.y), fmaf(d.z, t, o4.z));
+                const float eps = 1.0e-3f * t;
+                const uint4 tri = sc.tris[h.x];
+                const float3 v0 = xyz(sc.verts[tri.x]), v1 = xyz(sc.verts[tri.y]), v2 = xyz(sc.verts[tri.z]);
+                const float3 ng = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
+                const float3 wo = mul(d, -1.0f);
+                float4 Tp = T[path];
+                float4 Lp = L[path];
+                const float4 E = sc.emission[tri.w];
+                if (E.x > 0.0f || E.y > 0.0f || E.z > 0.0f) {
+                    // DiffuseAreaLight::L (core/lights.cu:70-78): one-sided emitter.
+                    const float cosl = dot3(ng, wo);
+                    if (cosl > 0.0f) {
+                        float w = 1.0f;
+                        if (b > 0) {
+                            const float pdf_l = inv_nl * t * t / (tri_area(v0, v1, v2) * cosl);
+                            w = Tp.w / (Tp.w + pdf_l);
+                        }
+                        Lp.x += Tp.x * E.x * w; Lp.y += Tp.y * E.y * w; Lp.z += Tp.z * E.z * w;
+                        L[path] = Lp;
+                    }
+                    // Emitters end the path (integrator_path.cu:94-107).
+                } else {
+                    const float3 nrm = dot3(ng, wo) < 0.0f ? mul(ng, -1.0f) : ng;
+                    const float4 A = sc.albedo[tri.w];
+                    // Next-event estimation to one uniformly chosen emissive triangle.
+                    if (sc.n_lights) {
+                        uint32_t j = (uint32_t)(rng_u01(seed, key, vdim(b, kDimLight)) * (float)sc.n_lights);
+                        j = min(j, sc.n_lights - 1);
+                        const uint4 lt = sc.tris[sc.lights[j]];
+                        const float3 l0 = xyz(sc.verts[lt.x]), l1 = xyz(sc.verts[lt.y]), l2 = xyz(sc.verts[lt.z]);
+                        const float3 lp = sample_triangle(l0, l1, l2, rng_u01(seed, key, vdim(b, kDimLightU)),
+                                                          rng_u01(seed, key, vdim(b, kDimLightV)));
+                        const float3 ln = normalize3(cross3(sub(l1, l0), sub(l2, l0)));
+                        const float3 dv = sub(lp, pos);
+                        const float dist2 = dot3(dv, dv);
+                        const float dist = sqrtf(dist2);
+                        const float3 wi = mul(dv, 1.0f / dist);
+                        const float cos_l = -dot3(ln, wi);
+                        const float cos_s = dot3(nrm, wi);
+                        const float4 Le = sc.emission[lt.w];
+                        if (cos_l > 0.0f && cos_s > 0.0f && dist > 0.0f) {
+                            const float pdf_l = inv_nl * dist2 / (tri_area(l0, l1, l2) * cos_l);
+                            const float pdf_b = cos_s * kInvPi;
+                            const float w = (b == max_depth) ? 1.0f : pdf_l / (pdf_l + pdf_b);
+                            const float k = cos_s * w / pdf_l * kInvPi;
+                            scv = make_float4(Tp.x * A.x * Le.x * k, Tp.y * A.y * Le.y * k, Tp.z * A.z * Le.z * k, 0.0f);
+                            // VisibilityTesterElement::set_segment (core/util.h:186-195).
+                            so = make_float4(pos.x, pos.y, pos.z, eps);
+                            sd = make_float4(wi.x, wi.y, wi.z, dist * (1.0f - 1.0e-3f));
+                            shadow = scv.x > 0.0f || scv.y > 0.0f || scv.z > 0.0f;
+                        }
+                    }
+                    if (b < max_depth) {
+                        // Lambertian sample (core/reflection.cu:42-69): f cos / pdf = albedo.
+                        const float3 loc = cosine_hemisphere(rng_u01(seed, key, vdim(b, kDimBsdfU)),
+                                                             rng_u01(seed, key, vdim(b, kDimBsdfV)));
+                        const float pdf = loc.z * kInvPi;
+                        if (pdf > 0.0f) {
+                            const float3 wi = normalize3(to_world(frame_from_z(nrm), loc));
+                            Tp.x *= A.x; Tp.y *= A.y; Tp.z *= A.z; Tp.w = pdf;
+                            cont = Tp.x > 0.0f || Tp.y > 0.0f || Tp.z > 0.0f;
+                            if (cont && b >= rr_start) {
+                                // Unbiased Russian roulette (the reference divides by 1 - q,
+                                // integrator_path.cu:232-244).
+                                const float q = fminf(rr_prob, luminance(xyz(Tp)));
+                                if (!(rng_u01(seed, key, vdim(b, kDimRR)) < q)) cont = false;
+                                else { Tp.x /= q; Tp.y /= q; Tp.z /= q; }
+                            }
+                            if (cont) {
+                                T[path] = Tp;
+                                new_o = make_float4(pos.x, pos.y, pos.z, eps);
+                                new_d = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        const uint32_t so_slot = warp_append(&wc->n_shadow, shadow);
+        if (shadow) {
+            srays[2 * (size_t)path] = so;
+            srays[2 * (size_t)path + 1] = sd;
+            sc_out[path] = scv;
+            qs[so_slot] = path;
+        }
+        const uint32_t ext_slot = warp_append(&wc->n_ext[next], cont);
+        if (cont) {
+            rays[2 * (size_t)path] = new_o;
+            rays[2 * (size_t)path + 1] = new_d;
+            q_out[ext_slot] = path;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&wc->stats[b == 0 ? 0 : 1], (unsigned long long)n);
+    }
+}
+
+__global__ void k_pt_stats_shadow(WaveCountersDev* wc)
+{
+    wc->stats[2] += wc->n_shadow;
+}
+
+__global__ void k_pt_accumulate(const float4* L, uint32_t npix, uint32_t per_pixel, float4* accum)
+{
+    for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < npix; pix += gridDim.x * blockDim.x) {
+        float4 a = accum[pix];
+        for (uint32_t j = 0; j < per_pixel; j++) {
+            const float4 l = L[(size_t)j * npix + pix];
+            a.x += l.x; a.y += l.y; a.z += l.z;
+        }
+        accum[pix] = a;
+    }
+}
+
+// ---- BDPT with a light-vertex cache -----------------------------------------------
+constexpr uint32_t kMaxConnections = 8;
+constexpr uint64_t kLightSalt = 0xA24BAED4963EE407ull;
+constexpr float kLightRayTmin = 1.0e-4f;
+
+// Light subpath start (integrators/integrator_bdpt_lvc_sk.cu:61-83): uniform
+// emissive triangle, uniform point, cosine-distributed direction about its
+// normal (one-sided emitter).  Throughput Le cos / (pdf_A pdf_w) = Le NL A pi.
+__global__ void k_bd_light_init(SceneView sc, uint64_t seed, uint64_t key0, uint32_t n_paths, float4* lray,
+                                float4* lbeta, uint32_t* lq0, WaveCountersDev* wc)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) wc->n_ext[0] = sc.n_lights ? n_paths : 0u;
+    if (!sc.n_lights) return;
+    const uint64_t ls = seed ^ kLightSalt;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
+        const uint64_t key = key0 + p;
+        uint32_t j = min((uint32_t)(rng_u01(ls, key, 0) * (float)sc.n_lights), sc.n_lights - 1);
+        const uint4 lt = sc.tris[sc.lights[j]];
+        const float3 l0 = xyz(sc.verts[lt.x]), l1 = xyz(sc.verts[lt.y]), l2 = xyz(sc.verts[lt.z]);
+        const float3 y0 = sample_triangle(l0, l1, l2, rng_u01(ls, key, 1), rng_u01(ls, key, 2));
+        const float3 ln = normalize3(cross3(sub(l1, l0), sub(l2, l0)));
+        const float3 dir = normalize3(to_world(frame_from_z(ln), cosine_hemisphere(rng_u01(ls, key, 3), rng_u01(ls, key, 4))));
+        const float4 Le = sc.emission[lt.w];
+        const float k = (float)sc.n_lights * tri_area(l0, l1, l2) * 3.14159265358979f;
+        lbeta[p] = make_float4(Le.x * k, Le.y * k, Le.z * k, 0.0f);
+        lray[2 * (size_t)p] = make_float4(y0.x, y0.y, y0.z, kLightRayTmin);
+        lray[2 * (size_t)p + 1] = make_float4(dir.x, dir.y, dir.z, 3.402823466e+38f);
+        lq0[p] = p;
+    }
+}
+
+// Light vertex d (1-based surface vertex): store it in the sparse cache slot
+// (path, d) and continue the subpath by BSDF sampling with Russian roulette on
+// the per-bounce factor (integrator_bdpt_lvc_sk.cu:93-166).
+__global__ void k_bd_light_shade(SceneView sc, uint64_t seed, uint64_t key0, uint32_t d, uint32_t Dl, uint32_t rr_start,
+                                 float rr_prob, const uint32_t* q_in, uint32_t* q_out, float4* lray, const int4* lhit,
+                                 float4* lbeta, float4* s_pos, float4* s_nrm, float4* s_beta, uint8_t* s_valid,
+                                 WaveCountersDev* wc, uint32_t cur)
+{
+    const uint32_t n = wc->n_ext[cur];
+    const uint64_t ls = seed ^ kLightSalt;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        bool cont = false;
+        uint32_t path = 0;
+        float4 no, nd;
+        if (i < n) {
+            path = q_in[i];
+            const int4 h = lhit[path];
+            if (h.x >= 0) {
+                const float4 o4 = lray[2 * (size_t)path], d4 = lray[2 * (size_t)path + 1];
+                const float t = __int_as_float(h.y);
+                const float3 dd = xyz(d4);
+                const float3 pos = f3(fmaf(dd.x, t, o4.x), fmaf(dd.y, t, o4.y), fmaf(dd.z, t, o4.z));
+                const uint4 tri = sc.tris[h.x];
+                const float4 E = sc.emission[tri.w];
+                if (!(E.x > 0.0f || E.y > 0.0f || E.z > 0.0f)) {
+                    const float3 v0 = xyz(sc.verts[tri.x]), v1 = xyz(sc.verts[tri.y]), v2 = xyz(sc.verts[tri.z]);
+                    const float3 ng = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
+                    const float3 wo = mul(dd, -1.0f);
+                    const float3 nrm = dot3(ng, wo) < 0.0f ? mul(ng, -1.0f) : ng;
+                    float4 beta = lbeta[path];
+                    const size_t slot = (size_t)path * Dl + (d - 1);
+                    s_pos[slot] = make_float4(pos.x, pos.y, pos.z, (float)(d + 1));
+                    s_nrm[slot] = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(tri.w));
+                    s_beta[slot] = beta;
+                    s_valid[slot] = 1;
+                    if (d < Dl) {
+                        const uint64_t key = key0 + path;
+                        const float4 A = sc.albedo[tri.w];
+                        const float3 loc = cosine_hemisphere(rng_u01(ls, key, 8 + 8 * d), rng_u01(ls, key, 9 + 8 * d));
+                        if (loc.z > 0.0f) {
+                            const float3 wi = normalize3(to_world(frame_from_z(nrm), loc));
+                            float q = fminf(1.0f, luminance(xyz(A)));
+                            if (d < rr_start) q = 1.0f;
+                            else q = fminf(q, rr_prob);
+                            cont = q > 0.0f && rng_u01(ls, key, 10 + 8 * d) < q;
+                            if (cont) {
+                                beta.x *= A.x / q; beta.y *= A.y / q; beta.z *= A.z / q;
+                                lbeta[path] = beta;
+                                no = make_float4(pos.x, pos.y, pos.z, 1.0e-3f * t);
+                                nd = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        const uint32_t slot_out = warp_append(&wc->n_ext[cur ^ 1u], cont);
+        if (cont) {
+            lray[2 * (size_t)path] = no;
+            lray[2 * (size_t)path + 1] = nd;
+            q_out[slot_out] = path;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&wc->stats[4], (unsigned long long)n);
+}
+
+// Deterministic cache compaction: chunks of kScanChunk sparse slots.
+constexpr uint32_t kScanChunk = 2048;
+constexpr uint32_t kScanThreads = 256;
+
+__global__ void k_lvc_count(const uint8_t* valid, uint64_t n_slots, uint32_t* block_sums)
+{
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    const uint64_t base = (uint64_t)blockIdx.x * kScanChunk;
+    uint32_t c = 0;
+    for (uint32_t k = threadIdx.x; k < kScanChunk; k += kScanThreads) {
+        const uint64_t i = base + k;
+        if (i < n_slots) c += valid[i];
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (uint32_t w = 0; w < kScanThreads / 32; w++) t += s_warp[w];
+        block_sums[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of the per-chunk counts in one block; total -> lvc_count.
+__global__ void k_lvc_scan_top(uint32_t* block_sums, uint32_t n_blocks, WaveCountersDev* wc)
+{
+    __shared__ uint32_t s[1024];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n_blocks; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < n_blocks ? block_sums[i] : 0u;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (uint32_t off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scan
+            const uint32_t add = threadIdx.x >= off ? s[threadIdx.x - off] : 0u;
+            __syncthreads();
+            s[threadIdx.x] += add;
+            __syncthreads();
+        }
+        if (i < n_blocks) block_sums[i] = carry + s[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += s[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        wc->lvc_count = carry;
+        wc->stats[5] += carry;
+    }
+}
+
+// Scatter valid slots in slot order: thread t of a chunk owns 8 consecutive slots.
+__global__ void k_lvc_scatter(const uint8_t* valid, uint64_t n_slots, const uint32_t* block_offsets, const float4* s_pos,
+                              const float4* s_nrm, const float4* s_beta, float4* d_pos, float4* d_nrm, float4* d_beta)
+{
+    constexpr uint32_t kPer = kScanChunk / kScanThreads;
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    const uint64_t base = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)threadIdx.x * kPer;
+    uint32_t c = 0;
+    for (uint32_t k = 0; k < kPer; k++) c += (base + k < n_slots) ? valid[base + k] : 0u;
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t incl = c;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, incl, o);
+        if ((int)lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t warp_off = 0;
+    for (uint32_t w = 0; w < warp; w++) warp_off += s_warp[w];
+    uint32_t out = block_offsets[blockIdx.x] + warp_off + incl - c;
+    for (uint32_t k = 0; k < kPer; k++) {
+        const uint64_t i = base + k;
+        if (i < n_slots && valid[i]) {
+            d_pos[out] = s_pos[i];
+            d_nrm[out] = s_nrm[i];
+            d_beta[out] = s_beta[i];
+            out++;
+        }
+    }
+}
+
+// Camera vertex i (1-based): emission (s = 0), next-event estimation (s = 1),
+// connections to cached light vertices (s >= 2), continuation.  Every
+// strategy of a k-segment path is weighted 1/k.
+__global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t iter, uint32_t i, uint32_t Kmax,
+                               uint32_t C, uint32_t rr_start, float rr_prob, float n_light_paths, const uint32_t* q_in,
+                               uint32_t* q_out, float4* rays, const int4* hits, float4* T, float4* L, float4* srays,
+                               float4* sc_out, uint32_t* qs, float4* cray, float4* cc, uint32_t* cq,
+                               const float4* lvc_pos, const float4* lvc_nrm, const float4* lvc_beta,
+                               WaveCountersDev* wc, uint32_t cur)
+{
+    const uint32_t n = wc->n_ext[cur];
+    const uint32_t M = wc->lvc_count;
+    const float inv_nl = sc.n_lights ? 1.0f / (float)sc.n_lights : 0.0f;
+    const uint32_t b = i - 1;  // random-dimension block of this vertex
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t qi = base + threadIdx.x;
+        bool cont = false, shadow = false;
+        bool conn[kMaxConnections];
+        float4 cro[kMaxConnections], crd[kMaxConnections];
+        for (uint32_t c = 0; c < kMaxConnections; c++) conn[c] = false;
+        uint32_t path = 0;
+        float4 new_o, new_d, so, sd, scv;
+        if (qi < n) {
+            path = q_in[qi];
+            for (uint32_t c = 0; c < C; c++) cc[(size_t)path * C + c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const int4 h = hits[path];
+            if (h.x >= 0) {
+                const uint64_t key = (uint64_t)iter * npix + (path % npix);
+                const float4 o4 = rays[2 * (size_t)path], d4 = rays[2 * (size_t)path + 1];
+                const float t = __int_as_float(h.y);
+                const float3 d = xyz(d4);
+                const float3 pos = f3(fmaf(d.x, t, o4.x), fmaf(d.y, t, o4.y), fmaf(d.z, t, o4.z));
+                const float eps = 1.0e-3f * t;
+                const uint4 tri = sc.tris[h.x];
+                const float3 v0 = xyz(sc.verts[tri.x]), v1 = xyz(sc.verts[tri.y]), v2 = xyz(sc.verts[tri.z]);
+                const float3 ng = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
+                const float3 wo = mul(d, -1.0f);
+                float4 Tp = T[path];
+                const float4 E = sc.emission[tri.w];
+                if (E.x > 0.0f || E.y > 0.0f || E.z > 0.0f) {
+                    if (dot3(ng, wo) > 0.0f) {  // s = 0, k = i
+                        float4 Lp = L[path];
+                        const float w = 1.0f / (float)i;
+                        Lp.x += Tp.x * E.x * w; Lp.y += Tp.y * E.y * w; Lp.z += Tp.z * E.z * w;
+                        L[path] = Lp;
+                    }
+                } else {
+                    const float3 nrm = dot3(ng, wo) < 0.0f ? mul(ng, -1.0f) : ng;
+                    const float4 A = sc.albedo[tri.w];
+                    if (sc.n_lights && i + 1 <= Kmax) {  // s = 1, k = i + 1
+                        uint32_t j = min((uint32_t)(rng_u01(seed, key, vdim(b, kDimLight)) * (float)sc.n_lights),
+                                         sc.n_lights - 1);
+                        const uint4 lt = sc.tris[sc.lights[j]];
+                        const float3 l0 = xyz(sc.verts[lt.x]), l1 = xyz(sc.verts[lt.y]), l2 = xyz(sc.verts[lt.z]);
+                        const float3 lp = sample_triangle(l0, l1, l2, rng_u01(seed, key, vdim(b, kDimLightU)),
+                                                          rng_u01(seed, key, vdim(b, kDimLightV)));
+                        const float3 ln = normalize3(cross3(sub(l1, l0), sub(l2, l0)));
+                        const float3 dv = sub(lp, pos);
+                        const float dist2 = dot3(dv, dv), dist = sqrtf(dist2);
+                        const float3 wi = mul(dv, 1.0f / dist);
+                        const float cos_l = -dot3(ln, wi), cos_s = dot3(nrm, wi);
+                        const float4 Le = sc.emission[lt.w];
+                        if (cos_l > 0.0f && cos_s > 0.0f && dist > 0.0f) {
+                            const float pdf_l = inv_nl * dist2 / (tri_area(l0, l1, l2) * cos_l);
+                            const float k = cos_s * kInvPi / (pdf_l * (float)(i + 1));
+                            scv = make_float4(Tp.x * A.x * Le.x * k, Tp.y * A.y * Le.y * k, Tp.z * A.z * Le.z * k, 0.0f);
+                            so = make_float4(pos.x, pos.y, pos.z, eps);
+                            sd = make_float4(wi.x, wi.y, wi.z, dist * (1.0f - 1.0e-3f));
+                            shadow = scv.x > 0.0f || scv.y > 0.0f || scv.z > 0.0f;
+                        }
+                    }
+                    if (M > 0 && i + 2 <= Kmax) {  // s >= 2
+                        for (uint32_t c = 0; c < C; c++) {
+                            const uint32_t v = min((uint32_t)(rng_u01(seed, key, vdim(b, 6) + 520u * (c + 1)) * (float)M), M - 1);
+                            const float4 vp4 = lvc_pos[v];
+                            const uint32_t s = (uint32_t)vp4.w;
+                            if (s + i > Kmax) continue;
+                            const float4 vn4 = lvc_nrm[v];
+                            const float3 dv = sub(xyz(vp4), pos);
+                            const float dist2 = dot3(dv, dv), dist = sqrtf(dist2);
+                            if (!(dist > 0.0f)) continue;
+                            const float3 dir = mul(dv, 1.0f / dist);
+                            const float cos_c = dot3(nrm, dir), cos_v = -dot3(xyz(vn4), dir);
+                            if (!(cos_c > 0.0f && cos_v > 0.0f)) continue;
+                            const float4 Av = sc.albedo[__float_as_uint(vn4.w)];
+                            const float4 bv = lvc_beta[v];
+                            const float g = cos_c * cos_v / dist2 * kInvPi * kInvPi * ((float)M / n_light_paths) /
+                                            ((float)(s + i) * (float)C);
+                            const float4 cv = make_float4(Tp.x * A.x * Av.x * bv.x * g, Tp.y * A.y * Av.y * bv.y * g,
+                                                          Tp.z * A.z * Av.z * bv.z * g, 0.0f);
+                            if (!(cv.x > 0.0f || cv.y > 0.0f || cv.z > 0.0f)) continue;
+                            cc[(size_t)path * C + c] = cv;
+                            cro[c] = make_float4(pos.x, pos.y, pos.z, eps);
+                            crd[c] = make_float4(dir.x, dir.y, dir.z, dist * (1.0f - 1.0e-3f));
+                            conn[c] = true;
+                        }
+                    }
+                    if (i < Kmax) {
+                        const float3 loc = cosine_hemisphere(rng_u01(seed, key, vdim(b, kDimBsdfU)),
+                                                             rng_u01(seed, key, vdim(b, kDimBsdfV)));
+                        if (loc.z > 0.0f) {
+                            const float3 wi = normalize3(to_world(frame_from_z(nrm), loc));
+                            Tp.x *= A.x; Tp.y *= A.y; Tp.z *= A.z; Tp.w = loc.z * kInvPi;
+                            cont = Tp.x > 0.0f || Tp.y > 0.0f || Tp.z > 0.0f;
+                            if (cont && b >= rr_start) {
+                                const float q = fminf(rr_prob, luminance(xyz(Tp)));
+                                if (!(rng_u01(seed, key, vdim(b, kDimRR)) < q)) cont = false;
+                                else { Tp.x /= q; Tp.y /= q; Tp.z /= q; }
+                            }
+                            if (cont) {
+                                T[path] = Tp;
+                                new_o = make_float4(pos.x, pos.y, pos.z, eps);
+                                new_d = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        const uint32_t s_slot = warp_append(&wc->n_shadow, shadow);
+        if (shadow) {
+            srays[2 * (size_t)path] = so;
+            srays[2 * (size_t)path + 1] = sd;
+            sc_out[path] = scv;
+            qs[s_slot] = path;
+        }
+        for (uint32_t c = 0; c < C; c++) {
+            const uint32_t c_slot = warp_append(&wc->n_conn, conn[c]);
+            if (conn[c]) {
+                const size_t cs = (size_t)path * C + c;
+                cray[2 * cs] = cro[c];
+                cray[2 * cs + 1] = crd[c];
+                cq[c_slot] = (uint32_t)cs;
+            }
+        }
+        const uint32_t e_slot = warp_append(&wc->n_ext[cur ^ 1u], cont);
+        if (cont) {
+            rays[2 * (size_t)path] = new_o;
+            rays[2 * (size_t)path + 1] = new_d;
+            q_out[e_slot] = path;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&wc->stats[i == 1 ? 0 : 1], (unsigned long long)n);
+}
+
+__global__ void k_bd_stats(WaveCountersDev* wc)
+{
+    wc->stats[2] += wc->n_shadow;
+    wc->stats[3] += wc->n_conn;
+}
+
+// Adds the surviving connection contributions of each shaded path, in
+// connection order (deterministic).
+__global__ void k_bd_conn_reduce(const uint32_t* q_in, const WaveCountersDev* wc, uint32_t cur, uint32_t C,
+                                 const float4* cc, float4* L)
+{
+    const uint32_t n = wc->n_ext[cur];
+    for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n; qi += gridDim.x * blockDim.x) {
+        const uint32_t path = q_in[qi];
+        float4 a = L[path];
+        for (uint32_t c = 0; c < C; c++) {
+            const float4 v = cc[(size_t)path * C + c];
+            a.x += v.x; a.y += v.y; a.z += v.z;
+        }
+        L[path] = a;
+    }
+}
+
+__global__ void k_pt_finalize(const float4* accum, uint32_t npix, float inv_spp, float* rgb)
+{
+    for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < npix; pix += gridDim.x * blockDim.x) {
+        const float4 a = accum[pix];
+        rgb[3 * (size_t)pix + 0] = a.x * inv_spp;
+        rgb[3 * (size_t)pix + 1] = a.y * inv_spp;
+        rgb[3 * (size_t)pix + 2] = a.z * inv_spp;
+    }
+}
+
+}  // namespace rb2dev
+
+namespace {
+
+template <class Src>
+int launch_persistent(const Src& src, uint64_t work, int sms, unsigned int* status, cudaStream_t s)
+{
+    int per_sm = 0;
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb2dev::k_persistent<128, Src>, 128, 0), "occupancy");
+    uint64_t blocks = (uint64_t)sms * (uint64_t)std::max(1, per_sm);
+    blocks = std::min<uint64_t>(blocks, (work + 127) / 128);
+    blocks = std::max<uint64_t>(blocks, 1);
+    rb2dev::k_persistent<128, Src><<<(unsigned)blocks, 128, 0, s>>>(src, 20u, status);
+    RB2_CUDA(cudaGetLastError(), "persistent launch");
+    return RB2_OK;
+}
+
+unsigned grid_for(uint64_t n, int sms) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 8)); }
+
+int ensure_path_state(PathState& ps, uint64_t P)
+{
+    if (P <= ps.cap) return RB2_OK;
+    cudaFree(ps.T); cudaFree(ps.L); cudaFree(ps.ray); cudaFree(ps.hit); cudaFree(ps.sray); cudaFree(ps.sc);
+    cudaFree(ps.q[0]); cudaFree(ps.q[1]); cudaFree(ps.qs);
+    ps = PathState();
+    cudaError_t e;
+    if ((e = cudaMalloc(&ps.T, P * 16)) != cudaSuccess || (e = cudaMalloc(&ps.L, P * 16)) != cudaSuccess ||
+        (e = cudaMalloc(&ps.ray, P * 32)) != cudaSuccess || (e = cudaMalloc(&ps.hit, P * 16)) != cudaSuccess ||
+        (e = cudaMalloc(&ps.sray, P * 32)) != cudaSuccess || (e = cudaMalloc(&ps.sc, P * 16)) != cudaSuccess ||
+        (e = cudaMalloc(&ps.q[0], P * 4)) != cudaSuccess || (e = cudaMalloc(&ps.q[1], P * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&ps.qs, P * 4)) != cudaSuccess)
+        return fail(RB2_ENOMEM, std::string("path state: ") + cudaGetErrorString(e));
+    ps.cap = P;
+    return RB2_OK;
+}
+
+int ensure_bdpt_state(BdptState& bd, uint64_t n_paths, uint64_t n_slots, uint64_t n_conn)
+{
+    cudaError_t e = cudaSuccess;
+    if (n_paths > bd.cap_paths) {
+        for (void* p : {(void*)bd.lray, (void*)bd.lbeta, (void*)bd.lhit, (void*)bd.lq[0], (void*)bd.lq[1]}) cudaFree(p);
+        bd.lray = bd.lbeta = nullptr; bd.lhit = nullptr; bd.lq[0] = bd.lq[1] = nullptr; bd.cap_paths = 0;
+        if ((e = cudaMalloc(&bd.lray, n_paths * 32)) != cudaSuccess || (e = cudaMalloc(&bd.lbeta, n_paths * 16)) != cudaSuccess ||
+            (e = cudaMalloc(&bd.lhit, n_paths * 16)) != cudaSuccess || (e = cudaMalloc(&bd.lq[0], n_paths * 4)) != cudaSuccess ||
+            (e = cudaMalloc(&bd.lq[1], n_paths * 4)) != cudaSuccess)
+            return fail(RB2_ENOMEM, std::string("light paths: ") + cudaGetErrorString(e));
+        bd.cap_paths = n_paths;
+    }
+    if (n_slots > bd.cap_slots) {
+        for (void* p : {(void*)bd.s_pos, (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_valid, (void*)bd.d_pos,
+                        (void*)bd.d_nrm, (void*)bd.d_beta, (void*)bd.block_sums})
+            cudaFree(p);
+        bd.s_pos = bd.s_nrm = bd.s_beta = bd.d_pos = bd.d_nrm = bd.d_beta = nullptr;
+        bd.s_valid = nullptr; bd.block_sums = nullptr; bd.cap_slots = 0;
+        const uint64_t nb = (n_slots + rb2dev::kScanChunk - 1) / rb2dev::kScanChunk;
+        if ((e = cudaMalloc(&bd.s_pos, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.s_nrm, n_slots * 16)) != cudaSuccess ||
+            (e = cudaMalloc(&bd.s_beta, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.s_valid, n_slots)) != cudaSuccess ||
+            (e = cudaMalloc(&bd.d_pos, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.d_nrm, n_slots * 16)) != cudaSuccess ||
+            (e = cudaMalloc(&bd.d_beta, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.block_sums, nb * 4)) != cudaSuccess)
+            return fail(RB2_ENOMEM, std::string("light vertex cache: ") + cudaGetErrorString(e));
+        bd.cap_slots = n_slots;
+    }
+    if (n_conn > bd.cap_conn) {
+        for (void* p : {(void*)bd.cray, (void*)bd.cc, (void*)bd.cq}) cudaFree(p);
+        bd.cray = bd.cc = nullptr; bd.cq = nullptr; bd.cap_conn = 0;
+        if ((e = cudaMalloc(&bd.cray, n_conn * 32)) != cudaSuccess || (e = cudaMalloc(&bd.cc, n_conn * 16)) != cudaSuccess ||
+            (e = cudaMalloc(&bd.cq, n_conn * 4)) != cudaSuccess)
+            return fail(RB2_ENOMEM, std::string("connection rays: ") + cudaGetErrorString(e));
+        bd.cap_conn = n_conn;
+    }
+    return RB2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rb2_scene_create(const float* v_xyz, uint32_t nv, const uint32_t* idx3, uint32_t ntri, const uint32_t* tri_material,
+                     uint32_t n_materials, const float* albedo_rgb, const float* emission_rgb, rb2_scene_dev** out)
+{
+    if (!out || (nv && !v_xyz) || (ntri && !idx3)) return fail(RB2_EINVAL, "null scene argument");
+    *out = nullptr;
+    for (uint64_t i = 0; i < 3ull * ntri; i++)
+        if (idx3[i] >= nv) return fail(RB2_EINVAL, "scene triangle index out of range");
+    const uint32_t nm = std::max<uint32_t>(1, n_materials);
+    if (tri_material)
+        for (uint32_t i = 0; i < ntri; i++)
+            if (tri_material[i] >= nm) return fail(RB2_EINVAL, "material id out of range");
+    std::vector<float4> v(std::max<uint32_t>(1, nv));
+    for (uint32_t i = 0; i < nv; i++) v[i] = make_float4(v_xyz[3 * i], v_xyz[3 * i + 1], v_xyz[3 * i + 2], 0.0f);
+    std::vector<uint4> t(std::max<uint32_t>(1, ntri));
+    std::vector<float4> alb(nm), emi(nm);
+    for (uint32_t m = 0; m < nm; m++) {
+        alb[m] = albedo_rgb ? make_float4(albedo_rgb[3 * m], albedo_rgb[3 * m + 1], albedo_rgb[3 * m + 2], 0.0f)
+                            : make_float4(0.5f, 0.5f, 0.5f, 0.0f);
+        emi[m] = emission_rgb ? make_float4(emission_rgb[3 * m], emission_rgb[3 * m + 1], emission_rgb[3 * m + 2], 0.0f)
+                              : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    std::vector<uint32_t> lights;
+    for (uint32_t i = 0; i < ntri; i++) {
+        uint32_t m = tri_material ? tri_material[i] : 0;
+        t[i] = make_uint4(idx3[3 * i], idx3[3 * i + 1], idx3[3 * i + 2], m);
+        const float4& e = emi[m];
+        if (e.x > 0.0f || e.y > 0.0f || e.z > 0.0f) lights.push_back(i);  // core/scene.cpp:105-113
+    }
+    std::unique_ptr<rb2_scene_dev> s(new rb2_scene_dev());
+    s->nv = nv; s->ntri = ntri; s->n_mat = nm; s->n_lights = (uint32_t)lights.size();
+    if (lights.empty()) lights.push_back(0);
+    cudaError_t e;
+    if ((e = cudaMalloc(&s->d_verts, v.size() * sizeof(float4))) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_tris, t.size() * sizeof(uint4))) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_albedo, nm * sizeof(float4))) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_emission, nm * sizeof(float4))) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_lights, lights.size() * sizeof(uint32_t))) != cudaSuccess) {
+        cudaFree(s->d_verts); cudaFree(s->d_tris); cudaFree(s->d_albedo); cudaFree(s->d_emission); cudaFree(s->d_lights);
+        return fail(RB2_ENOMEM, std::string("scene allocation: ") + cudaGetErrorString(e));
+    }
+    RB2_CUDA(cudaMemcpy(s->d_verts, v.data(), v.size() * sizeof(float4), cudaMemcpyHostToDevice), "scene upload");
+    RB2_CUDA(cudaMemcpy(s->d_tris, t.data(), t.size() * sizeof(uint4), cudaMemcpyHostToDevice), "scene upload");
+    RB2_CUDA(cudaMemcpy(s->d_albedo, alb.data(), nm * sizeof(float4), cudaMemcpyHostToDevice), "scene upload");
+    RB2_CUDA(cudaMemcpy(s->d_emission, emi.data(), nm * sizeof(float4), cudaMemcpyHostToDevice), "scene upload");
+    RB2_CUDA(cudaMemcpy(s->d_lights, lights.data(), lights.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "scene upload");
+    s->bytes = v.size() * 16 + t.size() * 16 + nm * 32 + lights.size() * 4;
+    *out = s.release();
+    return RB2_OK;
+}
+
+int rb2_scene_destroy(rb2_scene_dev* s)
+{
+    if (!s) return RB2_OK;
+    cudaFree(s->d_verts); cudaFree(s->d_tris); cudaFree(s->d_albedo); cudaFree(s->d_emission); cudaFree(s->d_lights);
+    delete s;
+    return RB2_OK;
+}
+
+int rb2_scene_device_bytes(const rb2_scene_dev* s, uint64_t* bytes)
+{
+    if (!s || !bytes) return fail(RB2_EINVAL, "null argument");
+    *bytes = s->bytes;
+    return RB2_OK;
+}
+
+int rb2_integrator_create(rb2_tracer* tracer, const rb2_scene_dev* scene, rb2_integrator** out)
+{
+    if (!tracer || !scene || !out) return fail(RB2_EINVAL, "null argument");
+    *out = nullptr;
+    std::unique_ptr<rb2_integrator> it(new rb2_integrator());
+    it->tracer = tracer;
+    it->scene = scene;
+    int dev = 0;
+    RB2_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    RB2_CUDA(cudaDeviceGetAttribute(&it->sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    RB2_CUDA(cudaMalloc(&it->d_counters, 16 * sizeof(unsigned long long)), "integrator counters");
+    *out = it.release();
+    return RB2_OK;
+}
+
+int rb2_integrator_destroy(rb2_integrator* it)
+{
+    if (!it) return RB2_OK;
+    cudaFree(it->d_rays); cudaFree(it->d_hits); cudaFree(it->d_count); cudaFree(it->d_counters);
+    cudaFree(it->d_accum); cudaFree(it->d_wave);
+    PathState& ps = it->ps;
+    cudaFree(ps.T); cudaFree(ps.L); cudaFree(ps.ray); cudaFree(ps.hit); cudaFree(ps.sray); cudaFree(ps.sc);
+    cudaFree(ps.q[0]); cudaFree(ps.q[1]); cudaFree(ps.qs);
+    BdptState& bd = it->bd;
+    for (void* p : {(void*)bd.lray, (void*)bd.lbeta, (void*)bd.lhit, (void*)bd.lq[0], (void*)bd.lq[1], (void*)bd.s_pos,
+                    (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_valid, (void*)bd.d_pos, (void*)bd.d_nrm,
+                    (void*)bd.d_beta, (void*)bd.block_sums, (void*)bd.cray, (void*)bd.cc, (void*)bd.cq})
+        cudaFree(p);
+    delete it;
+    return RB2_OK;
+}
+
+int rb2_integrator_device_bytes(const rb2_integrator* it, uint64_t* bytes)
+{
+    if (!it || !bytes) return fail(RB2_EINVAL, "null argument");
+    *bytes = it->bytes();
+    return RB2_OK;
+}
+
+int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params* p, float* d_ao, void* stream)
+{
+    if (!it || !cam || !p || !d_ao) return fail(RB2_EINVAL, "null argument");
+    if (p->samples == 0 || !(p->radius > 0.0f)) return fail(RB2_EINVAL, "AO needs samples > 0 and radius > 0");
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t npix = (uint64_t)cam->width * cam->height;
+    if (npix > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image too large");
+    int rc;
+    if ((rc = grow(it->d_rays, it->cap_rays, 2 * npix)) || (rc = grow(it->d_hits, it->cap_hits, npix)) ||
+        (rc = grow(it->d_count, it->cap_count, npix)))
+        return rc;
+    // 1. Primary rays through pixel centres, 2. closest hit (IntegratorAO::compute, integrator_ao.cu:92-101).
+    if ((rc = rb2_camera_rays(cam, 1, 0, 0, reinterpret_cast<float*>(it->d_rays), stream))) return rc;
+    if ((rc = rb2_trace(it->tracer, reinterpret_cast<const float*>(it->d_rays), (uint32_t)npix, 0, nullptr,
+                        reinterpret_cast<rb2_hit*>(it->d_hits), stream)))
+        return rc;
+    // 3. AO rays generated and traced in one persistent launch, unoccluded counts per pixel.
+    RB2_CUDA(cudaMemsetAsync(it->d_count, 0, npix * sizeof(uint32_t), s), "AO count reset");
+    RB2_CUDA(cudaMemsetAsync(it->d_counters, 0, sizeof(unsigned long long), s), "queue reset");
+    const DeviceBvhView bv = device_bvh(it->tracer);
+    rb2dev::AoSource src;
+    src.nodes = static_cast<const float4*>(bv.nodes);
+    src.woop = static_cast<const float4*>(bv.woop);
+    src.triidx = bv.triidx;
+    src.prim_rays = it->d_rays;
+    src.hits = it->d_hits;
+    src.verts = it->scene->d_verts;
+    src.tris = it->scene->d_tris;
+    src.counts = it->d_count;
+    src.counter = it->d_counters;
+    src.n_slots = npix * p->samples;
+    src.samples = p->samples;
+    src.radius = p->radius;
+    src.seed = p->seed;
+    if ((rc = launch_persistent(src, src.n_slots, it->sms, bv.status, s))) return rc;
+    // 4. AO = unoccluded fraction (misses contribute 0, integrator_ao.cu:56-84).
+    rb2dev::k_ao_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_hits, it->d_count, (uint32_t)npix, p->samples, d_ao);
+    RB2_CUDA(cudaGetLastError(), "AO finalize");
+    return RB2_OK;
+}
+
+int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, float* d_rgb, void* stream)
+{
+    if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
+    if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
+    if (p->max_depth > 64) return fail(RB2_EINVAL, "max_depth must be <= 64");
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t npix = (uint64_t)cam->width * cam->height;
+    if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");
+    // Samples per pixel in flight: about 8M paths per wave by default.
+    uint32_t spw = p->spp_per_wave ? p->spp_per_wave : (uint32_t)std::max<uint64_t>(1, (8ull << 20) / npix);
+    spw = std::min(spw, p->spp);
+    const uint64_t P = npix * spw;
+    PathState& ps = it->ps;
+    int rc;
+    if ((rc = ensure_path_state(ps, P))) return rc;
+    if ((rc = grow(it->d_accum, it->cap_accum, npix))) return rc;
+    if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
+    RB2_CUDA(cudaMemsetAsync(it->d_accum, 0, npix * 16, s), "accumulator reset");
+    RB2_CUDA(cudaMemsetAsync(it->d_wave, 0, sizeof(WaveCounters), s), "counter reset");
+
+    rb2dev::CamArgs ca;
+    std::memcpy(ca.r2c, cam->raster_to_camera, sizeof(ca.r2c));
+    std::memcpy(ca.c2w, cam->camera_to_world, sizeof(ca.c2w));
+    ca.width = cam->width; ca.height = cam->height; ca.spp = 1; ca.jitter = 1; ca.seed = p->seed;
+    const rb2_scene_dev* sd = it->scene;
+    rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights};
+    const DeviceBvhView bv = device_bvh(it->tracer);
+    WaveCounters* wc = it->d_wave;
+    const unsigned g = grid_for(P, it->sms);
+    for (uint32_t s0 = 0; s0 < p->spp; s0 += spw) {
+        const uint32_t cur_spw = std::min(spw, p->spp - s0);
+        const uint32_t paths = (uint32_t)(npix * cur_spw);
+        rb2dev::k_pt_camera<<<g, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, paths, s0, ps.ray, ps.T, ps.L, ps.q[0], wc);
+        RB2_CUDA(cudaGetLastError(), "PT camera");
+        uint32_t cur = 0;
+        for (uint32_t b = 0; b <= p->max_depth; b++) {
+            rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
+            rb2dev::QueueSource ext{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop), bv.triidx,
+                                    ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext, rb2dev::kClosest,
+                                    ps.hit, nullptr, nullptr};
+            if ((rc = launch_persistent(ext, paths, it->sms, bv.status, s))) return rc;
+            rb2dev::k_pt_shade<<<g, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, s0, b, p->max_depth, p->rr_start, p->rr_prob,
+                                                ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L, ps.sray, ps.sc,
+                                                ps.qs, wc, cur);
+            RB2_CUDA(cudaGetLastError(), "PT shade");
+            rb2dev::k_pt_stats_shadow<<<1, 1, 0, s>>>(wc);
+            rb2dev::QueueSource shadow{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop),
+                                       bv.triidx, ps.qs, &wc->n_shadow, ps.sray, &wc->head_shadow,
+                                       rb2dev::kOcclusion, nullptr, ps.L, ps.sc};
+            if ((rc = launch_persistent(shadow, paths, it->sms, bv.status, s))) return rc;
+            cur ^= 1u;
+        }
+        rb2dev::k_pt_accumulate<<<grid_for(npix, it->sms), 256, 0, s>>>(ps.L, (uint32_t)npix, cur_spw, it->d_accum);
+        RB2_CUDA(cudaGetLastError(), "PT accumulate");
+    }
+    rb2dev::k_pt_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp, d_rgb);
+    RB2_CUDA(cudaGetLastError(), "PT finalize");
+    return RB2_OK;
+}
+
+int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_params* p, float* d_rgb, void* stream)
+{
+    if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
+    if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
+    if (p->max_path_length < 1 || p->max_path_length > 16) return fail(RB2_EINVAL, "max_path_length must be in [1, 16]");
+    if (p->connections < 1 || p->connections > rb2dev::kMaxConnections) return fail(RB2_EINVAL, "connections must be in [1, 8]");
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t npix = (uint64_t)cam->width * cam->height;
+    if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");
+    const uint32_t K = p->max_path_length, C = p->connections;
+    const uint32_t Dl = K >= 2 ? K - 2 : 0;  // cached light vertices y1..y_{K-2} suffice for k <= K
+    const uint64_t NL = p->num_light_paths ? p->num_light_paths : npix;
+    const uint64_t n_slots = std::max<uint64_t>(1, NL * std::max<uint32_t>(Dl, 1));
+    int rc;
+    if ((rc = ensure_path_state(it->ps, npix))) return rc;
+    if ((rc = ensure_bdpt_state(it->bd, NL, n_slots, npix * C))) return rc;
+    if ((rc = grow(it->d_accum, it->cap_accum, npix))) return rc;
+    if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
+    RB2_CUDA(cudaMemsetAsync(it->d_accum, 0, npix * 16, s), "accumulator reset");
+    RB2_CUDA(cudaMemsetAsync(it->d_wave, 0, sizeof(WaveCounters), s), "counter reset");
+
+    rb2dev::CamArgs ca;
+    std::memcpy(ca.r2c, cam->raster_to_camera, sizeof(ca.r2c));
+    std::memcpy(ca.c2w, cam->camera_to_world, sizeof(ca.c2w));
+    ca.width = cam->width; ca.height = cam->height; ca.spp = 1; ca.jitter = 1; ca.seed = p->seed;
+    const rb2_scene_dev* sd = it->scene;
+    rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights};
+    const DeviceBvhView bv = device_bvh(it->tracer);
+    const float4* bn = static_cast<const float4*>(bv.nodes);
+    const float4* bw = static_cast<const float4*>(bv.woop);
+    WaveCounters* wc = it->d_wave;
+    PathState& ps = it->ps;
+    BdptState& bd = it->bd;
+    const unsigned gl = grid_for(NL, it->sms), gc = grid_for(npix, it->sms);
+    const uint64_t n_chunks = (n_slots + rb2dev::kScanChunk - 1) / rb2dev::kScanChunk;
+    for (uint32_t iter = 0; iter < p->spp; iter++) {
+        // ---- light pass: subpaths into the sparse cache, then compaction.
+        RB2_CUDA(cudaMemsetAsync(bd.s_valid, 0, n_slots, s), "cache reset");
+        rb2dev::k_bd_light_init<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)iter * NL, (uint32_t)NL, bd.lray, bd.lbeta,
+                                                   bd.lq[0], wc);
+        RB2_CUDA(cudaGetLastError(), "BDPT light init");
+        uint32_t cur = 0;
+        for (uint32_t d = 1; d <= Dl; d++) {
+            rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
+            rb2dev::QueueSource lsrc{bn, bw, bv.triidx, bd.lq[cur], &wc->n_ext[cur], bd.lray, &wc->head_ext,
+                                     rb2dev::kClosest, bd.lhit, nullptr, nullptr};
+            if ((rc = launch_persistent(lsrc, NL, it->sms, bv.status, s))) return rc;
+            rb2dev::k_bd_light_shade<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)iter * NL, d, Dl, p->rr_start, p->rr_prob,
+                                                        bd.lq[cur], bd.lq[cur ^ 1u], bd.lray, bd.lhit, bd.lbeta, bd.s_pos,
+                                                        bd.s_nrm, bd.s_beta, bd.s_valid, wc, cur);
+            RB2_CUDA(cudaGetLastError(), "BDPT light shade");
+            cur ^= 1u;
+        }
+        rb2dev::k_lvc_count<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(bd.s_valid, n_slots, bd.block_sums);
+        rb2dev::k_lvc_scan_top<<<1, 1024, 0, s>>>(bd.block_sums, (uint32_t)n_chunks, wc);
+        rb2dev::k_lvc_scatter<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(
+            bd.s_valid, n_slots, bd.block_sums, bd.s_pos, bd.s_nrm, bd.s_beta, bd.d_pos, bd.d_nrm, bd.d_beta);
+        RB2_CUDA(cudaGetLastError(), "cache compaction");
+        // ---- camera pass.
+        rb2dev::k_pt_camera<<<gc, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, (uint32_t)npix, iter, ps.ray, ps.T, ps.L,
+                                               ps.q[0], wc);
+        RB2_CUDA(cudaGetLastError(), "BDPT camera");
+        cur = 0;
+        for (uint32_t i = 1; i <= K; i++) {
+            rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
+            rb2dev::QueueSource ext{bn, bw, bv.triidx, ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext,
+                                    rb2dev::kClosest, ps.hit, nullptr, nullptr};
+            if ((rc = launch_persistent(ext, npix, it->sms, bv.status, s))) return rc;
+            rb2dev::k_bd_cam_shade<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, iter, i, K, C, p->rr_start, p->rr_prob,
+                                                      (float)NL, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L,
+                                                      ps.sray, ps.sc, ps.qs, bd.cray, bd.cc, bd.cq, bd.d_pos, bd.d_nrm,
+                                                      bd.d_beta, wc, cur);
+            RB2_CUDA(cudaGetLastError(), "BDPT camera shade");
+            rb2dev::k_bd_stats<<<1, 1, 0, s>>>(wc);
+            rb2dev::QueueSource nee{bn, bw, bv.triidx, ps.qs, &wc->n_shadow, ps.sray, &wc->head_shadow,
+                                    rb2dev::kOcclusion, nullptr, ps.L, ps.sc};
+            if ((rc = launch_persistent(nee, npix, it->sms, bv.status, s))) return rc;
+            rb2dev::QueueSource con{bn, bw, bv.triidx, bd.cq, &wc->n_conn, bd.cray, &wc->head_conn,
+                                    rb2dev::kOcclusion, nullptr, nullptr, bd.cc};
+            if ((rc = launch_persistent(con, npix * C, it->sms, bv.status, s))) return rc;
+            rb2dev::k_bd_conn_reduce<<<gc, 256, 0, s>>>(ps.q[cur], wc, cur, C, bd.cc, ps.L);
+            RB2_CUDA(cudaGetLastError(), "BDPT connection reduce");
+            cur ^= 1u;
+        }
+        rb2dev::k_pt_accumulate<<<gc, 256, 0, s>>>(ps.L, (uint32_t)npix, 1u, it->d_accum);
+        RB2_CUDA(cudaGetLastError(), "BDPT accumulate");
+    }
+    rb2dev::k_pt_finalize<<<gc, 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp, d_rgb);
+    RB2_CUDA(cudaGetLastError(), "BDPT finalize");
+    return RB2_OK;
+}
+
+int rb2_integrator_stats(rb2_integrator* it, rb2_render_stats* out, void* stream)
+{
+    if (!it || !out) return fail(RB2_EINVAL, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    if (!it->d_wave) return RB2_OK;
+    WaveCounters w;
+    cudaStream_t s = (cudaStream_t)stream;
+    RB2_CUDA(cudaMemcpyAsync(&w, it->d_wave, sizeof(w), cudaMemcpyDeviceToHost, s), "stats read");
+    RB2_CUDA(cudaStreamSynchronize(s), "stream sync");
+    out->primary_rays = w.stats[0];
+    out->extension_rays = w.stats[1];
+    out->shadow_rays = w.stats[2];
+    out->connection_rays = w.stats[3];
+    out->light_rays = w.stats[4];
+    out->lvc_vertices = w.stats[5];
+    return RB2_OK;
+}
+
+}  // extern "C"
