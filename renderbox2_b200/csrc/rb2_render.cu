@@ -45,87 +45,8 @@ int grow(T*& p, uint64_t& cap, uint64_t n)
 
 }  // namespace
 
-struct rb2_scene_dev {
-    float4* d_verts = nullptr;     // xyz, w unused
-    uint4* d_tris = nullptr;       // vertex indices + material id
-    float4* d_albedo = nullptr;    // per material
-    float4* d_emission = nullptr;  // per material
-    uint32_t* d_lights = nullptr;  // emissive triangle ids
-    uint32_t nv = 0, ntri = 0, n_mat = 0, n_lights = 0;
-    uint64_t bytes = 0;
-};
+#include "rb2_render_internal.h"
 
-// Wavefront path state, one entry per path of the wave (SoA).
-struct PathState {
-    float4* T = nullptr;        // throughput rgb, w = solid-angle pdf of the last BSDF sample
-    float4* L = nullptr;        // radiance gathered by the path
-    float4* ray = nullptr;      // current extension ray (2 per path)
-    int4* hit = nullptr;        // extension hit
-    float4* sray = nullptr;     // pending shadow / connection ray (2 per path)
-    float4* sc = nullptr;       // its contribution when unoccluded
-    uint32_t* q[2] = {nullptr, nullptr};  // active-path queues (ping-pong)
-    uint32_t* qs = nullptr;     // shadow queue
-    uint64_t cap = 0;
-};
-
-// Device-side counters of one wave.
-struct WaveCounters {
-    uint32_t n_ext[2];
-    uint32_t n_shadow;
-    uint32_t n_conn;
-    unsigned long long head_ext;     // traversal queue heads
-    unsigned long long head_shadow;
-    unsigned long long head_conn;
-    unsigned long long stats[6];     // rb2_render_stats order
-    uint32_t lvc_count;              // dense light-vertex-cache size of this iteration
-    uint32_t pad;
-};
-
-// Light-vertex cache and light-path state of the BDPT integrator.
-struct BdptState {
-    // light subpaths
-    float4* lray = nullptr;     // 2 per light path
-    float4* lbeta = nullptr;    // throughput arriving at the next vertex
-    int4* lhit = nullptr;
-    uint32_t* lq[2] = {nullptr, nullptr};
-    uint64_t cap_paths = 0;
-    // cache, sparse (path, depth) slots and dense compacted copy
-    float4* s_pos = nullptr;    // xyz, w = light-subpath vertex count s (as float)
-    float4* s_nrm = nullptr;    // normal facing the arriving light, w = material id bits
-    float4* s_beta = nullptr;
-    uint8_t* s_valid = nullptr;
-    float4* d_pos = nullptr;
-    float4* d_nrm = nullptr;
-    float4* d_beta = nullptr;
-    uint32_t* block_sums = nullptr;
-    uint64_t cap_slots = 0;
-    // connection rays of camera vertices (connections per path)
-    float4* cray = nullptr;
-    float4* cc = nullptr;
-    uint32_t* cq = nullptr;
-    uint64_t cap_conn = 0;
-};
-
-struct rb2_integrator {
-    rb2_tracer* tracer = nullptr;
-    const rb2_scene_dev* scene = nullptr;
-    int sms = 0;
-    // generic scratch
-    float4* d_rays = nullptr; uint64_t cap_rays = 0;        // 2 per ray
-    int4* d_hits = nullptr; uint64_t cap_hits = 0;
-    uint32_t* d_count = nullptr; uint64_t cap_count = 0;
-    unsigned long long* d_counters = nullptr;                // queue heads (16)
-    float4* d_accum = nullptr; uint64_t cap_accum = 0;
-    PathState ps;
-    BdptState bd;
-    WaveCounters* d_wave = nullptr;
-    uint64_t bytes() const
-    {
-        return cap_rays * 32 + cap_hits * 16 + cap_count * 4 + 16 * 8 + cap_accum * 16 + ps.cap * (16 * 8 + 12) +
-               sizeof(WaveCounters) + bd.cap_paths * (32 + 16 + 16 + 8) + bd.cap_slots * (6 * 16 + 1) +
-               bd.cap_conn * (32 + 16 + 4);
-    }
-};
 
 namespace rb2dev {
 
@@ -834,6 +755,10 @@ int launch_persistent(const Src& src, uint64_t work, int sms, unsigned int* stat
 
 unsigned grid_for(uint64_t n, int sms) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 8)); }
 
+}  // namespace
+
+namespace rb2 {
+
 int ensure_path_state(PathState& ps, uint64_t P)
 {
     if (P <= ps.cap) return RB2_OK;
@@ -888,7 +813,23 @@ int ensure_bdpt_state(BdptState& bd, uint64_t n_paths, uint64_t n_slots, uint64_
     return RB2_OK;
 }
 
-}  // namespace
+uint64_t pt_paths_in_flight(uint64_t npix, uint32_t spp, uint32_t spp_per_wave)
+{
+    uint32_t spw = spp_per_wave ? spp_per_wave : (uint32_t)std::max<uint64_t>(1, (8ull << 20) / std::max<uint64_t>(1, npix));
+    spw = std::min(spw, std::max<uint32_t>(1, spp));
+    return npix * spw;
+}
+
+int integrator_reserve_pt(rb2_integrator* it, uint64_t paths, uint64_t npix)
+{
+    int rc;
+    if ((rc = ensure_path_state(it->ps, paths))) return rc;
+    if ((rc = grow(it->d_accum, it->cap_accum, npix))) return rc;
+    if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
+    return RB2_OK;
+}
+
+}  // namespace rb2
 
 extern "C" {
 
@@ -1046,9 +987,8 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
     const uint64_t npix = (uint64_t)cam->width * cam->height;
     if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");
     // Samples per pixel in flight: about 8M paths per wave by default.
-    uint32_t spw = p->spp_per_wave ? p->spp_per_wave : (uint32_t)std::max<uint64_t>(1, (8ull << 20) / npix);
-    spw = std::min(spw, p->spp);
-    const uint64_t P = npix * spw;
+    const uint64_t P = pt_paths_in_flight(npix, p->spp, p->spp_per_wave);
+    const uint32_t spw = (uint32_t)(P / npix);
     PathState& ps = it->ps;
     int rc;
     if ((rc = ensure_path_state(ps, P))) return rc;

@@ -1,0 +1,213 @@
+"""Serving: resident BVH pool, config-5 job mix, continuous-batching runs.
+
+The request loop itself is native (librb2's rb2_server_run, include/rb2_serve.h);
+this module builds pools and job lists and reads results.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._native import check, lib
+from .accel import BVH, CudaTracer, Scene
+from .render import DeviceScene
+from .scenes import heightfield_for_triangles, surface_rays
+
+
+class Job(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("bvh", C.c_uint32), ("arrival_s", C.c_double), ("h_rays", C.c_void_p),
+                ("n_rays", C.c_uint64), ("mode", C.c_uint32), ("tile", C.c_uint32), ("spp", C.c_uint32),
+                ("max_depth", C.c_uint32), ("rr_start", C.c_uint32), ("rr_prob", C.c_float), ("seed", C.c_uint64),
+                ("eye", C.c_float * 3), ("lookat", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float),
+                ("h_out", C.c_void_p)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("admit_s", C.c_double), ("end_s", C.c_double), ("latency_s", C.c_double),
+                ("footprint_bytes", C.c_uint64), ("rays", C.c_uint64), ("slot", C.c_uint32), ("status", C.c_int32)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("fifo", C.c_uint32), ("hbm_budget", C.c_uint64), ("max_tile", C.c_uint32),
+                ("reserved", C.c_uint32), ("max_rays", C.c_uint64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("wall_s", C.c_double), ("rays", C.c_uint64), ("mrays_per_s", C.c_double), ("p50_s", C.c_double),
+                ("p99_s", C.c_double), ("mean_s", C.c_double), ("max_s", C.c_double), ("max_concurrent", C.c_uint32),
+                ("jobs", C.c_uint32), ("peak_admitted_bytes", C.c_uint64), ("resident_bytes", C.c_uint64)]
+
+
+_SIGS = {
+    "rb2_server_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
+    "rb2_server_destroy": (C.c_int, [C.c_void_p]),
+    "rb2_server_run": (C.c_int, [C.c_void_p, C.POINTER(Job), C.c_uint32, C.POINTER(JobResult), C.POINTER(ServerStats)]),
+    "rb2_job_footprint": (C.c_uint64, [C.POINTER(Job)]),
+}
+
+
+def _lib():
+    L = lib()
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(L, name)
+        fn.restype, fn.argtypes = res, args
+    return L
+
+
+def lit_heightfield(seed: int, n_tris: int, emission: float = 4.0) -> Scene:
+    """Config-1 generator sized to about n_tris triangles plus one emissive
+    panel (two triangles, facing down) above the field, so path-traced tiles
+    of the pool scenes receive light."""
+    s = heightfield_for_triangles(seed=seed, n_tris=max(n_tris - 2, 20))
+    rng = np.random.Generator(np.random.PCG64(seed))
+    s.material_ids = np.zeros(s.num_triangles, np.uint32)
+    quad = np.array([[-0.5, 1.5, -0.5], [1.5, 1.5, -0.5], [1.5, 1.5, 1.5], [-0.5, 1.5, 1.5]], np.float32)
+    s.add_mesh(quad, [[0, 1, 3], [1, 2, 3]], material_ids=1, is_emissive=True)  # (+x) x (+z) = -y: faces down
+    s.albedo = np.array([rng.uniform(0.3, 0.8, 3), [0.0, 0.0, 0.0]], np.float32)
+    s.emission = np.array([[0.0, 0.0, 0.0], [emission] * 3], np.float32)
+    return s
+
+
+@dataclass
+class Pool:
+    scenes: list
+    bvhs: list
+    tracers: list
+    dscenes: list
+
+
+def build_pool(tri_counts, seed: int = 5) -> Pool:
+    scenes, bvhs, tracers, dscenes = [], [], [], []
+    for k, t in enumerate(tri_counts):
+        sc = lit_heightfield(seed * 1000 + k, int(t))
+        bvh = BVH(sc)
+        scenes.append(sc)
+        bvhs.append(bvh)
+        tracers.append(CudaTracer(bvh))
+        dscenes.append(DeviceScene(sc))
+    return Pool(scenes, bvhs, tracers, dscenes)
+
+
+def pool_triangle_counts(n: int, lo: float, hi: float, seed: int) -> list[int]:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return [int(x) for x in np.exp(rng.uniform(np.log(lo), np.log(hi), n))]
+
+
+class Server:
+    def __init__(self, pool: Pool, slots=8, fifo=False, hbm_budget=8 << 30, max_tile=1024, max_rays=4 << 20):
+        L = _lib()
+        self.pool = pool
+        n = len(pool.tracers)
+        self._tr = (C.c_void_p * n)(*[t.handle.value for t in pool.tracers])
+        self._sc = (C.c_void_p * n)(*[d.handle.value for d in pool.dscenes])
+        cfg = ServerConfig(slots, 1 if fifo else 0, hbm_budget, max_tile, 0, max_rays)
+        self._s = C.c_void_p()
+        check(L.rb2_server_create(self._tr, self._sc, n, C.byref(cfg), C.byref(self._s)))
+
+    def __del__(self):
+        s = getattr(self, "_s", None)
+        if s and s.value:
+            _lib().rb2_server_destroy(s)
+            self._s = C.c_void_p()
+
+    def run(self, jobs: "JobList"):
+        n = len(jobs.jobs)
+        res = (JobResult * max(1, n))()
+        st = ServerStats()
+        check(_lib().rb2_server_run(self._s, jobs.array, n, res, C.byref(st)))
+        return [res[i] for i in range(n)], {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+
+class JobList:
+    """Jobs plus the pinned host buffers they read and write."""
+
+    def __init__(self):
+        self.jobs, self.inputs, self.outputs = [], [], []
+        self._arr = None
+
+    def add_rays(self, bvh: int, rays: np.ndarray, mode: int, arrival: float = 0.0):
+        import torch
+        r = torch.from_numpy(np.ascontiguousarray(rays, np.float32)).pin_memory()
+        out = torch.empty((rays.shape[0], 4) if mode != 2 else (rays.shape[0],),
+                          dtype=torch.int32 if mode != 2 else torch.uint8).pin_memory()
+        j = Job()
+        j.kind, j.bvh, j.arrival_s, j.h_rays, j.n_rays, j.mode = 0, bvh, arrival, r.data_ptr(), rays.shape[0], mode
+        j.h_out = out.data_ptr()
+        self.jobs.append(j)
+        self.inputs.append(r)
+        self.outputs.append(out)
+        self._arr = None
+        return len(self.jobs) - 1
+
+    def add_tile(self, bvh: int, tile: int, spp: int, seed: int, eye, lookat, up=(0.0, 1.0, 0.0), fov=60.0,
+                 max_depth=8, rr_start=3, rr_prob=0.95, arrival: float = 0.0):
+        import torch
+        out = torch.empty((tile * tile, 3), dtype=torch.float32).pin_memory()
+        j = Job()
+        j.kind, j.bvh, j.arrival_s, j.tile, j.spp = 1, bvh, arrival, tile, spp
+        j.max_depth, j.rr_start, j.rr_prob, j.seed, j.fov_deg = max_depth, rr_start, rr_prob, seed, fov
+        j.eye[:], j.lookat[:], j.up[:] = list(eye), list(lookat), list(up)
+        j.h_out = out.data_ptr()
+        self.jobs.append(j)
+        self.inputs.append(None)
+        self.outputs.append(out)
+        self._arr = None
+        return len(self.jobs) - 1
+
+    def subset(self, idx, arrival: float = 0.0) -> "JobList":
+        """A job list sharing inputs with this one, with fresh outputs."""
+        import torch
+        out = JobList()
+        for i in idx:
+            j = Job.from_buffer_copy(self.jobs[i])
+            j.arrival_s = arrival
+            o = torch.empty_like(self.outputs[i]).pin_memory()
+            j.h_out = o.data_ptr()
+            out.jobs.append(j)
+            out.inputs.append(self.inputs[i])
+            out.outputs.append(o)
+        return out
+
+    def with_arrivals(self, arrivals) -> "JobList":
+        out = self.subset(range(len(self.jobs)))
+        for j, a in zip(out.jobs, arrivals):
+            j.arrival_s = float(a)
+        return out
+
+    @property
+    def array(self):
+        if self._arr is None:
+            self._arr = (Job * max(1, len(self.jobs)))(*self.jobs)
+        return self._arr
+
+    def footprint(self, i) -> int:
+        return int(_lib().rb2_job_footprint(C.byref(self.jobs[i])))
+
+
+def config5_jobs(pool: Pool, n_jobs: int, seed: int = 5, tile_fraction=0.7, tile_min=64, tile_max=1024,
+                 spp_choices=(1, 4, 16, 64), rays_min=64 * 1024, rays_max=4 * 1024 * 1024) -> JobList:
+    """The config-5 mix: tile renders (square side uniform in [tile_min,
+    tile_max], spp from spp_choices, depth 8) and incoherent ray batches
+    (log-uniform size, half closest-hit, half occlusion)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    jl = JobList()
+    for k in range(n_jobs):
+        b = int(rng.integers(0, len(pool.tracers)))
+        if rng.uniform() < tile_fraction:
+            tile = int(rng.integers(tile_min, tile_max + 1))
+            spp = int(rng.choice(spp_choices))
+            ex, ez = rng.uniform(0.2, 0.8, 2)
+            jl.add_tile(b, tile, spp, seed=int(rng.integers(1 << 31)), eye=(-ex, 0.9, ez - 0.9),
+                        lookat=(-ex, 0.0, ez), fov=60.0)
+        else:
+            n = int(np.exp(rng.uniform(np.log(rays_min), np.log(rays_max))))
+            rays, _ = surface_rays(pool.scenes[b], seed=int(rng.integers(1 << 31)), n=n)
+            jl.add_rays(b, rays, mode=0 if rng.uniform() < 0.5 else 2)
+    return jl
+
+
+def poisson_arrivals(n: int, rate: float, seed: int = 7) -> np.ndarray:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.cumsum(rng.exponential(1.0 / rate, n))

@@ -1,0 +1,94 @@
+"""GPU tests of the serving runtime (config 5 pattern): jobs admitted while
+others run overlap on the device, and every job's result is identical alone
+and in the mix (bit for bit: traversal and counter-keyed sampling do not
+depend on scheduling)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pool(rb, cuda):
+    from renderbox2_b200.serve import build_pool
+    return build_pool([5_000, 20_000, 60_000], seed=9)
+
+
+def _mixed_jobs(pool):
+    from renderbox2_b200.serve import JobList
+    rng = np.random.Generator(np.random.PCG64(3))
+    jl = JobList()
+    import renderbox2_b200 as rb
+    for k in range(6):
+        b = k % 3
+        n = int(rng.integers(10_000, 200_000))
+        rays, _ = rb.surface_rays(pool.scenes[b], seed=100 + k, n=n)
+        rays[::2, 4:7] *= -1.0
+        jl.add_rays(b, rays, mode=0 if k % 2 == 0 else 2)
+    for k in range(6):
+        b = (k + 1) % 3
+        tile = int(rng.integers(32, 97))
+        jl.add_tile(b, tile, spp=int(rng.choice([2, 4, 8])), seed=200 + k, eye=(-0.5, 0.9, -0.3),
+                    lookat=(-0.5, 0.0, 0.5))
+    return jl
+
+
+def _outputs_equal(a, b):
+    import torch
+    return all(torch.equal(x, y) for x, y in zip(a.outputs, b.outputs))
+
+
+def test_results_identical_alone_and_in_the_mix(pool, cuda):
+    from renderbox2_b200.serve import Server
+    jobs = _mixed_jobs(pool)
+    srv = Server(pool, slots=4, hbm_budget=8 << 30, max_tile=128, max_rays=256 * 1024)
+    mix = jobs.subset(range(len(jobs.jobs)))
+    res, st = srv.run(mix)
+    assert all(r.status == 0 for r in res)
+    assert st["max_concurrent"] > 1, st  # work of several jobs was in flight together
+    for i in range(len(jobs.jobs)):
+        alone = jobs.subset([i])
+        r1, _ = srv.run(alone)
+        assert r1[0].status == 0
+        assert cuda.equal(alone.outputs[0], mix.outputs[i]), f"job {i} differs alone vs in the mix"
+    fifo = Server(pool, fifo=True, max_tile=128, max_rays=256 * 1024)
+    seq = jobs.subset(range(len(jobs.jobs)))
+    rf, sf = fifo.run(seq)
+    assert sf["max_concurrent"] == 1
+    assert _outputs_equal(seq, mix)
+    # tile images carry light (the pool scenes have an emissive panel)
+    assert float(mix.outputs[-1].mean()) > 0.0
+
+
+def test_ray_jobs_equal_direct_traces(pool, cuda):
+    from renderbox2_b200.serve import JobList, Server
+    import renderbox2_b200 as rb
+    rays, _ = rb.surface_rays(pool.scenes[2], seed=55, n=50_000)
+    rays[::3, 4:7] *= -1.0
+    jl = JobList()
+    jl.add_rays(2, rays, mode=0)
+    jl.add_rays(2, rays, mode=2)
+    srv = Server(pool, slots=2, max_tile=64, max_rays=64 * 1024)
+    res, _ = srv.run(jl)
+    d = cuda.from_numpy(rays).cuda()
+    direct = pool.tracers[2].trace(d).cpu()
+    occ = pool.tracers[2].trace_occlusion(d).cpu()
+    assert cuda.equal(jl.outputs[0], direct)
+    assert cuda.equal(jl.outputs[1], occ)
+
+
+def test_admission_by_hbm_footprint(pool, cuda):
+    from renderbox2_b200.serve import Server
+    jobs = _mixed_jobs(pool)
+    fps = [jobs.footprint(i) for i in range(len(jobs.jobs))]
+    budget = max(fps) + min(fps) // 2
+    srv = Server(pool, slots=8, hbm_budget=budget, max_tile=128, max_rays=256 * 1024)
+    res, st = srv.run(jobs.subset(range(len(jobs.jobs))))
+    assert all(r.status == 0 for r in res)
+    assert st["peak_admitted_bytes"] <= budget
+    # Poisson arrivals: latency is measured from arrival, never negative.
+    from renderbox2_b200.serve import poisson_arrivals
+    arr = poisson_arrivals(len(jobs.jobs), rate=200.0)
+    res2, st2 = srv.run(jobs.with_arrivals(arr))
+    assert all(r.latency_s > 0 and r.admit_s >= a - 1e-6 for r, a in zip(res2, arr))
+    assert st2["p99_s"] >= st2["p50_s"] > 0

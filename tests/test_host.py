@@ -188,3 +188,22 @@ def test_generators_are_seeded(rb):
     room = rb.RoomScene(seed=2, n_boxes=3, n_spheres=5, sphere_subdiv=2, n_lights=2)
     assert room.num_lights == 4
     assert room.emission[room.material_ids[room.light_ids_to_primitive_ids]].min() == 10.0
+
+
+def test_job_footprints_and_arrivals(rb):
+    import ctypes as C_
+    from renderbox2_b200.serve import Job, _lib, poisson_arrivals
+    L = _lib()
+    j = Job()
+    j.kind, j.n_rays, j.mode = 0, 1000, 0
+    assert L.rb2_job_footprint(C_.byref(j)) == 1000 * 48
+    j.mode = 2
+    assert L.rb2_job_footprint(C_.byref(j)) == 1000 * 33
+    t = Job()
+    t.kind, t.tile, t.spp = 1, 256, 4
+    small = L.rb2_job_footprint(C_.byref(t))
+    t.tile = 1024
+    big = L.rb2_job_footprint(C_.byref(t))
+    assert big > 10 * small > 0
+    a = poisson_arrivals(5000, rate=100.0, seed=1)
+    assert np.all(np.diff(a) > 0) and abs(5000 / a[-1] - 100.0) < 5.0
