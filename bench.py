@@ -273,6 +273,14 @@ def run_rb2(args, rank, world, local_rank):
     if rank == 0 and world == 1:
         cpu_baseline = cpu_baseline_run(scenes, args.cpu_sample_s)
 
+    # ---- config 5: served jobs (continuous batching) vs plain one-at-a-time launches.
+    serving = None
+    if args.serve_jobs > 0:
+        del batch
+        batch = None
+        from renderbox2_b200.workloads import serving as serving_run
+        serving = serving_run(n_jobs=args.serve_jobs)
+
     value = world * total_rays * args.steps / (batch_total / 1e3) / 1e6
     plain_value = world * total_rays * args.steps / (plain_total / 1e3) / 1e6
     line = {
@@ -306,10 +314,25 @@ def run_rb2(args, rank, world, local_rank):
     }
     if cpu_baseline is not None:
         line["cpu_baseline"] = cpu_baseline
+    if serving is not None:
+        line["serving"] = serving
     if rank == 0:
         print(json.dumps(line), flush=True)
     del batch
     torch.cuda.synchronize(dev)
+
+
+def run_workload(args, rank, local_rank):
+    """Configs 1-3 at full size (one JSON line, not the headline)."""
+    import torch
+
+    from renderbox2_b200.workloads import integrator
+    torch.cuda.set_device(local_rank)
+    r = integrator(args.workload)
+    if rank == 0:
+        names = {"ao": "config 1: ambient occlusion", "pt": "config 2: wavefront path tracing",
+                 "bdpt": "config 3: BDPT with light-vertex cache"}
+        print(json.dumps({"metric": "samples/s and Mrays/s", "workload": names[args.workload], **r}), flush=True)
 
 
 def cpu_baseline_run(scenes, budget_s: float):
@@ -408,6 +431,9 @@ def main():
     ap.add_argument("--rays-per-scene", type=int, default=1 << 20)
     ap.add_argument("--ref-rays-per-scene", type=int, default=2048)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--serve-jobs", type=int, default=300, help="config-5 jobs in the serving measurement (0: skip)")
+    ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt"], default="trace",
+                    help="trace: the headline config-4 line; ao/pt/bdpt: configs 1-3 at full size")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -424,6 +450,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload != "trace":
+            run_workload(args, rank, local_rank)
         else:
             run_rb2(args, rank, world, local_rank)
     finally:

@@ -120,7 +120,7 @@ typedef struct {
     uint32_t block_threads;     /* threads per CTA: 64, 128 or 256 */
     uint32_t ctas_per_sm;       /* resident CTAs per SM (0 = occupancy maximum) */
     uint32_t fetch_threshold;   /* refill a warp when fewer lanes stay busy (reference: 20) */
-    uint32_t reserved;
+    uint32_t regs;              /* register budget of the kernel variant: 64, 48 or 40 (0 = 64) */
 } rb2_launch_config;
 
 /* Inner-node order of the uploaded Compact2 buffer: the reference's DFS
@@ -181,7 +181,8 @@ typedef struct {
     uint32_t fetch_threshold; /* 0 = 20 */
     uint32_t chunk;           /* queue chunk: a warp reserves chunk*32 rays per atomic (0/1 = exact) */
     uint32_t node_order;      /* RB2_NODE_ORDER_*; applied to every tracer in the batch */
-    uint32_t reserved;
+    uint32_t regs;            /* register budget of the kernel variant: 64, 48 or 40 (0 = 64);
+                                 lower budgets keep more warps resident and spill a little to L1 */
 } rb2_batch_config;
 
 typedef struct rb2_batch rb2_batch;
@@ -198,9 +199,9 @@ int rb2_batch_launch(rb2_batch* b, void* stream);
  * Changing the config drops the graph. */
 int rb2_batch_capture(rb2_batch* b, void* stream);
 int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream);
-/* Times candidate configs (coordinate descent over node order, block shape,
- * CTAs per SM, fetch threshold and queue chunk; median of `reps` launches
- * each), applies and returns the fastest. */
+/* Times candidate configs (coordinate descent over node order, block shape x
+ * register budget, CTAs per SM, fetch threshold and queue chunk; median of
+ * `reps` launches each), applies and returns the fastest. */
 int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best, double* best_ms);
 
 /* --------------------------------------------------- allocation-free batch --

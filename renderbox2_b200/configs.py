@@ -22,14 +22,19 @@ CONFIG1 = dict(
 # 2000 spheres at subdivision 3 would be 2.56M triangles, not the stated 1M
 # total; the 1M total is kept: 2000 icospheres at subdivision 2 (320 triangles
 # each, 640k) plus tessellated walls and 100 boxes fill the rest.
+# The room of configs 2 and 3 is 10 units on a side (room_size) so that 2000
+# (4000) spheres of radius up to 0.2 leave it open; camera poses are given in
+# room-relative units (multiplied by room_size when used).
 CONFIG2 = dict(
     seed=2, n_boxes=100, n_spheres=2000, sphere_subdiv=2, rmin=0.01, rmax=0.2, n_lights=1, emission=10.0,
+    room_size=10.0,
     eye=(-0.5, 0.5, 0.02), lookat=(-0.5, 0.45, 1.0), up=(0.0, 1.0, 0.0), width=1920, height=1080, fov=60.0,
     spp=64, max_depth=8, rr_start=3, rr_prob=0.95,
 )
 
 CONFIG3 = dict(
     seed=3, n_boxes=100, n_spheres=4000, sphere_subdiv=2, rmin=0.01, rmax=0.2, n_lights=2, emission=10.0,
+    room_size=10.0,
     eye=(-0.5, 0.5, 0.02), lookat=(-0.5, 0.45, 1.0), up=(0.0, 1.0, 0.0), width=1280, height=720, fov=60.0,
     spp=16, max_path_length=6, lvc_connections=1,
 )

@@ -117,8 +117,11 @@ __host__ __device__ constexpr size_t job_smem_bytes(uint32_t n_jobs, bool inline
                       : (n_jobs <= kMaxSmemJobs ? (n_jobs + 1) * sizeof(unsigned long long) : 0);
 }
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_trace_jobs(const __grid_constant__ KernelArgs a)
+// REGS is the register budget per thread the variant is compiled for (64:
+// 32 resident warps per SM, 48: 40 warps, 40: 48 warps; lower budgets spill a
+// little state to L1).  The autotuner picks the variant by measurement.
+template <int BLOCK, int REGS = 64>
+__global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK) k_trace_jobs(const __grid_constant__ KernelArgs a)
 {
     extern __shared__ unsigned long long s_start[];
     __shared__ unsigned long long s_rem[2 * (BLOCK / 32)];

@@ -79,12 +79,21 @@ int cuda_fail(cudaError_t e, const char* what)
         if (e_ != cudaSuccess) return cuda_fail(e_, what);  \
     } while (0)
 
+// Kernel variants: block shape {64, 128, 256} x register budget {64, 48, 40}.
 struct Occupancy {
     int sms = 0;
-    int per_sm[3] = {0, 0, 0};  // block 64, 128, 256
+    int per_sm[3][3] = {};  // [block index][register-budget index]
 };
 
 int block_index(uint32_t block) { return block == 64 ? 0 : (block == 256 ? 2 : 1); }
+int regs_index(uint32_t regs) { return regs == 48 ? 1 : (regs == 40 ? 2 : 0); }
+
+template <int B, int R>
+int occ_of(int& out, size_t smem)
+{
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&out, rb2dev::k_trace_jobs<B, R>, B, smem), "occupancy");
+    return RB2_OK;
+}
 
 int occupancy(Occupancy& o)
 {
@@ -92,29 +101,44 @@ int occupancy(Occupancy& o)
     RB2_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
     RB2_CUDA(cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
     const size_t smem = rb2dev::job_smem_bytes(rb2dev::kMaxSmemJobs, false);
-    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm[0], rb2dev::k_trace_jobs<64>, 64, smem), "occupancy");
-    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm[1], rb2dev::k_trace_jobs<128>, 128, smem), "occupancy");
-    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm[2], rb2dev::k_trace_jobs<256>, 256, smem), "occupancy");
-    return RB2_OK;
+    int rc = 0;
+    rc |= occ_of<64, 64>(o.per_sm[0][0], smem) | occ_of<64, 48>(o.per_sm[0][1], smem) | occ_of<64, 40>(o.per_sm[0][2], smem);
+    rc |= occ_of<128, 64>(o.per_sm[1][0], smem) | occ_of<128, 48>(o.per_sm[1][1], smem) | occ_of<128, 40>(o.per_sm[1][2], smem);
+    rc |= occ_of<256, 64>(o.per_sm[2][0], smem) | occ_of<256, 48>(o.per_sm[2][1], smem) | occ_of<256, 40>(o.per_sm[2][2], smem);
+    return rc ? RB2_ECUDA : RB2_OK;
+}
+
+template <int B, int R>
+void launch_variant(const rb2dev::KernelArgs& a, unsigned blocks, size_t smem, cudaStream_t s)
+{
+    rb2dev::k_trace_jobs<B, R><<<blocks, B, smem, s>>>(a);
 }
 
 // Launches the persistent kernel: grid = SMs x resident CTAs per SM, capped
 // by the work available.
-int launch_jobs(const rb2dev::KernelArgs& a, uint64_t total_rays, uint32_t block, uint32_t ctas_per_sm,
+int launch_jobs(const rb2dev::KernelArgs& a, uint64_t total_rays, uint32_t block, uint32_t ctas_per_sm, uint32_t regs,
                 const Occupancy& occ, cudaStream_t s)
 {
-    const int bi = block_index(block);
-    const uint32_t per_sm = ctas_per_sm ? std::min<uint32_t>(ctas_per_sm, (uint32_t)std::max(1, occ.per_sm[bi]))
-                                        : (uint32_t)std::max(1, occ.per_sm[bi]);
+    const int bi = block_index(block), ri = regs_index(regs);
+    const int max_per_sm = std::max(1, occ.per_sm[bi][ri]);
+    const uint32_t per_sm = ctas_per_sm ? std::min<uint32_t>(ctas_per_sm, (uint32_t)max_per_sm) : (uint32_t)max_per_sm;
     uint64_t blocks = (uint64_t)occ.sms * per_sm;
     const uint64_t warps_needed = (total_rays + 31) / 32;
-    blocks = std::min<uint64_t>(blocks, (warps_needed + block / 32 - 1) / (block / 32));
+    const uint32_t bthreads = bi == 0 ? 64 : (bi == 2 ? 256 : 128);
+    blocks = std::min<uint64_t>(blocks, (warps_needed + bthreads / 32 - 1) / (bthreads / 32));
     blocks = std::max<uint64_t>(blocks, 1);
     const size_t smem = rb2dev::job_smem_bytes(a.n_jobs, a.jobs == nullptr);
-    switch (block) {
-    case 64: rb2dev::k_trace_jobs<64><<<(unsigned)blocks, 64, smem, s>>>(a); break;
-    case 256: rb2dev::k_trace_jobs<256><<<(unsigned)blocks, 256, smem, s>>>(a); break;
-    default: rb2dev::k_trace_jobs<128><<<(unsigned)blocks, 128, smem, s>>>(a); break;
+    const unsigned g = (unsigned)blocks;
+    switch (bi * 3 + ri) {
+    case 0: launch_variant<64, 64>(a, g, smem, s); break;
+    case 1: launch_variant<64, 48>(a, g, smem, s); break;
+    case 2: launch_variant<64, 40>(a, g, smem, s); break;
+    case 4: launch_variant<128, 48>(a, g, smem, s); break;
+    case 5: launch_variant<128, 40>(a, g, smem, s); break;
+    case 6: launch_variant<256, 64>(a, g, smem, s); break;
+    case 7: launch_variant<256, 48>(a, g, smem, s); break;
+    case 8: launch_variant<256, 40>(a, g, smem, s); break;
+    default: launch_variant<128, 64>(a, g, smem, s); break;
     }
     RB2_CUDA(cudaGetLastError(), "trace launch");
     return RB2_OK;
@@ -209,8 +233,10 @@ int trace_single(rb2_tracer* t, const float* d_rays, uint64_t n, uint32_t mode, 
     a.counter = counter;
     a.status = t->d_status;
     const uint32_t block = t->cfg.block_threads ? t->cfg.block_threads : kDefaultBlock;
-    return launch_jobs(a, n, block, t->cfg.ctas_per_sm, t->occ, s);
+    return launch_jobs(a, n, block, t->cfg.ctas_per_sm, t->cfg.regs, t->occ, s);
 }
+
+bool valid_regs(uint32_t r) { return r == 0 || r == 64 || r == 48 || r == 40; }
 
 }  // namespace
 
@@ -282,6 +308,7 @@ int rb2_tracer_set_launch(rb2_tracer* t, const rb2_launch_config* cfg)
     if (cfg->block_threads && cfg->block_threads != 64 && cfg->block_threads != 128 && cfg->block_threads != 256)
         return fail(RB2_ENOTSUP, "block_threads must be 64, 128 or 256");
     if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
+    if (!valid_regs(cfg->regs)) return fail(RB2_ENOTSUP, "regs must be 64, 48 or 40");
     t->cfg = *cfg;
     return RB2_OK;
 }
@@ -401,7 +428,7 @@ int batch_enqueue(rb2_batch* b, cudaStream_t s)
     a.counter = b->d_counter;
     a.status = b->d_status;
     return launch_jobs(a, b->total, b->cfg.block_threads ? b->cfg.block_threads : kDefaultBlock, b->cfg.ctas_per_sm,
-                       b->occ, s);
+                       b->cfg.regs, b->occ, s);
 }
 
 }  // namespace
@@ -462,6 +489,7 @@ int rb2_batch_set_config(rb2_batch* b, const rb2_batch_config* cfg)
         return fail(RB2_ENOTSUP, "block_threads must be 64, 128 or 256");
     if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
     if (cfg->node_order > RB2_NODE_ORDER_BFS) return fail(RB2_EINVAL, "unknown node order");
+    if (!valid_regs(cfg->regs)) return fail(RB2_ENOTSUP, "regs must be 64, 48 or 40");
     b->drop_graph();
     b->cfg = *cfg;
     std::vector<rb2_tracer*> seen;
@@ -553,11 +581,13 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     best.fetch_threshold = 20;
     best.chunk = 1;
     best.node_order = RB2_NODE_ORDER_DFS;
+    best.regs = 64;
     double best_ms = 0;
     int rc = time_cfg(best, best_ms);
     if (rc) return rc;
     const uint32_t orders[] = {RB2_NODE_ORDER_DFS, RB2_NODE_ORDER_BFS};
     const uint32_t blocks[] = {64, 128, 256};
+    const uint32_t regs[] = {64, 48, 40};
     const uint32_t thresholds[] = {8, 16, 20, 24, 28};
     const uint32_t chunks[] = {1, 2, 4, 8};
     for (int pass = 0; pass < 2; pass++) {
@@ -567,11 +597,13 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
             if (ms < best_ms) { best = c; best_ms = ms; }
         }
         for (uint32_t bl : blocks) {
-            rb2_batch_config c = best; c.block_threads = bl; c.ctas_per_sm = 0; double ms;
-            if ((rc = time_cfg(c, ms))) return rc;
-            if (ms < best_ms) { best = c; best_ms = ms; }
+            for (uint32_t rg : regs) {
+                rb2_batch_config c = best; c.block_threads = bl; c.regs = rg; c.ctas_per_sm = 0; double ms;
+                if ((rc = time_cfg(c, ms))) return rc;
+                if (ms < best_ms) { best = c; best_ms = ms; }
+            }
         }
-        const int maxc = std::max(1, b->occ.per_sm[block_index(best.block_threads)]);
+        const int maxc = std::max(1, b->occ.per_sm[block_index(best.block_threads)][regs_index(best.regs)]);
         for (int k : {maxc, std::max(1, maxc * 3 / 4), std::max(1, maxc / 2)}) {
             rb2_batch_config c = best; c.ctas_per_sm = (uint32_t)k; double ms;
             if ((rc = time_cfg(c, ms))) return rc;

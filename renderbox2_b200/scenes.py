@@ -39,7 +39,10 @@ class RoomScene(Scene):
     triangles (two per quad)."""
 
     def __init__(self, seed=1, n_boxes=100, n_spheres=2000, sphere_subdiv=2, rmin=0.01, rmax=0.2, n_lights=1,
-                 emission=10.0):
+                 emission=10.0, room_size=1.0):
+        """room_size scales the whole room (walls, boxes, lights); sphere
+        radii rmin..rmax are absolute, so a 10-unit room holds 2000 spheres
+        of radius up to 0.2 with space between them."""
         super().__init__()
         L = lib()
         nv, nt = C.c_uint32(), C.c_uint32()
@@ -47,7 +50,10 @@ class RoomScene(Scene):
         v = np.empty((nv.value, 3), np.float32)
         i = np.empty((nt.value, 3), np.uint32)
         m = np.empty((nt.value,), np.uint32)
-        check(L.rb2_gen_room(seed, n_boxes, n_spheres, sphere_subdiv, rmin, rmax, n_lights, _ptr(v), _ptr(i), _ptr(m)))
+        check(L.rb2_gen_room(seed, n_boxes, n_spheres, sphere_subdiv, rmin / room_size, rmax / room_size, n_lights,
+                             _ptr(v), _ptr(i), _ptr(m)))
+        if room_size != 1.0:
+            v *= np.float32(room_size)
         self.vertices, self.indices, self.material_ids = v, i, m
         n_mat = 6 + n_boxes + n_spheres + n_lights
         rng = np.random.Generator(np.random.PCG64(seed))

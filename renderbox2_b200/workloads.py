@@ -1,0 +1,116 @@
+"""Full-size workloads of configs 1-3 and 5, used by bench.py.
+
+Each function builds its seeded synthetic scene (renderbox2_b200.configs),
+runs on the current CUDA device and returns a dict of measurements.  Times
+are CUDA-event times on the launching stream unless marked wall-clock.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+
+def _event_ms(fn, stream, reps=1):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def integrator(kind: str, warmup: int = 1):
+    """Config 1 (AO), 2 (PT) or 3 (BDPT) at full size: samples/s and Mrays/s."""
+    import torch
+
+    import renderbox2_b200 as rb
+    from renderbox2_b200 import configs
+    from renderbox2_b200.render import (AmbientOcclusionIntegratorParams, BidirectionalPathIntegratorLvcParams,
+                                        DeviceScene, Integrator, PathIntegratorParams)
+    t0 = time.time()
+    if kind == "ao":
+        c = configs.CONFIG1
+        scene = rb.heightfield_scene(seed=c["seed"], grid_n=c["grid_n"], amplitude=c["amplitude"],
+                                     n_boxes=c["n_boxes"], box_min=c["box_min"], box_max=c["box_max"])
+    else:
+        c = configs.CONFIG2 if kind == "pt" else configs.CONFIG3
+        scene = rb.RoomScene(seed=c["seed"], n_boxes=c["n_boxes"], n_spheres=c["n_spheres"],
+                             sphere_subdiv=c["sphere_subdiv"], rmin=c["rmin"], rmax=c["rmax"],
+                             n_lights=c["n_lights"], emission=c["emission"], room_size=c["room_size"])
+    bvh = rb.BVH(scene)
+    build_s = time.time() - t0
+    it = Integrator(rb.CudaTracer(bvh), DeviceScene(scene))
+    scale = c.get("room_size", 1.0)
+    eye = [x * scale for x in c["eye"]]
+    look = [x * scale for x in c["lookat"]]
+    cam = rb.PerspectiveCamera(eye, look, c["up"], (c["width"], c["height"]), c["fov"])
+    stream = torch.cuda.Stream()
+    npix = c["width"] * c["height"]
+    with torch.cuda.stream(stream):
+        if kind == "ao":
+            p = AmbientOcclusionIntegratorParams(samples=c["ao_samples"], radius=c["ao_radius"], seed=c["ao_seed"])
+            out = torch.empty((npix,), dtype=torch.float32, device="cuda")
+            run = lambda: it.render_ao(cam, p, out=out, stream=stream)  # noqa: E731
+            samples = npix * c["ao_samples"]
+        elif kind == "pt":
+            p = PathIntegratorParams(spp=c["spp"], max_depth=c["max_depth"], rr_start=c["rr_start"],
+                                     rr_prob=c["rr_prob"], seed=1)
+            out = torch.empty((npix, 3), dtype=torch.float32, device="cuda")
+            run = lambda: it.render_pt(cam, p, out=out, stream=stream)  # noqa: E731
+            samples = npix * c["spp"]
+        else:
+            p = BidirectionalPathIntegratorLvcParams(spp=c["spp"], max_path_length=c["max_path_length"],
+                                                     connections=c["lvc_connections"], seed=1)
+            out = torch.empty((npix, 3), dtype=torch.float32, device="cuda")
+            run = lambda: it.render_bdpt(cam, p, out=out, stream=stream)  # noqa: E731
+            samples = npix * c["spp"]
+        for _ in range(warmup):
+            run()
+        torch.cuda.synchronize()
+        ms = _event_ms(run, stream)
+    st = it.stats(stream)
+    rays = (npix if kind == "ao" else 0) + sum(st[k] for k in ("primary_rays", "extension_rays", "shadow_rays",
+                                                              "connection_rays", "light_rays"))
+    if kind == "ao":
+        rays = npix + npix * c["ao_samples"]
+    return {"workload": kind, "triangles": scene.num_triangles, "width": c["width"], "height": c["height"],
+            "samples": int(samples), "ms": round(ms, 3), "samples_per_s": round(samples / (ms / 1e3), 1),
+            "mrays_per_s": round(rays / (ms / 1e3) / 1e6, 2), "rays": int(rays), "build_s": round(build_s, 2),
+            "stats": st, "image_mean": float(out.float().mean().item())}
+
+
+def serving(n_jobs: int = 300, n_bvh: int = 32, seed: int = 5, slots: int = 8):
+    """Config 5, scaled to n_jobs: pool of n_bvh lit heightfields (1k..4M
+    triangles, log-uniform), 70 % tile renders / 30 % ray batches.  The
+    arrival rate is the throughput of the plain path (one job at a time)
+    on a burst of the same jobs, i.e. the rate that saturates it; both paths
+    then serve the same Poisson arrival sequence."""
+    from renderbox2_b200 import configs
+    from renderbox2_b200.serve import Server, build_pool, config5_jobs, pool_triangle_counts, poisson_arrivals
+    c = configs.CONFIG5
+    t0 = time.time()
+    counts = pool_triangle_counts(n_bvh, c["tri_min"], c["tri_max"], seed)
+    pool = build_pool(counts, seed=seed)
+    jobs = config5_jobs(pool, n_jobs, seed=seed)
+    setup_s = time.time() - t0
+    cont = Server(pool, slots=slots, fifo=False)
+    plain = Server(pool, fifo=True)
+    # warm-up: a few jobs through both
+    cont.run(jobs.subset(range(min(8, n_jobs))))
+    plain.run(jobs.subset(range(min(8, n_jobs))))
+    _, burst = plain.run(jobs.subset(range(n_jobs)))
+    rate = n_jobs / burst["wall_s"]
+    arr = poisson_arrivals(n_jobs, rate, seed=seed + 1)
+    _, s_plain = plain.run(jobs.with_arrivals(arr))
+    _, s_cont = cont.run(jobs.with_arrivals(arr))
+    keep = ("p50_s", "p99_s", "mean_s", "mrays_per_s", "wall_s", "max_concurrent")
+    return {"jobs": n_jobs, "bvhs": n_bvh, "pool_triangles": int(sum(counts)),
+            "arrival_rate_jobs_per_s": round(rate, 2), "setup_s": round(setup_s, 1),
+            "resident_gb": round(s_cont["resident_bytes"] / 1e9, 2),
+            "continuous": {k: round(s_cont[k], 5) for k in keep},
+            "plain_fifo": {k: round(s_plain[k], 5) for k in keep},
+            "p99_speedup": round(s_plain["p99_s"] / max(s_cont["p99_s"], 1e-9), 3),
+            "throughput_ratio": round(s_cont["mrays_per_s"] / max(s_plain["mrays_per_s"], 1e-9), 3)}

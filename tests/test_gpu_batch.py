@@ -57,7 +57,8 @@ def test_batch_equals_plain_launches(rb, orc, cuda):
 
 @pytest.mark.parametrize("cfg", [
     dict(block_threads=64), dict(block_threads=256), dict(chunk=4), dict(chunk=8, fetch_threshold=8),
-    dict(node_order=1), dict(ctas_per_sm=2, fetch_threshold=32),
+    dict(node_order=1), dict(ctas_per_sm=2, fetch_threshold=32), dict(regs=48), dict(regs=40, block_threads=256),
+    dict(regs=40, block_threads=64, chunk=2),
 ])
 def test_batch_configs_give_identical_results(rb, cuda, cfg):
     scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
