@@ -1,14 +1,15 @@
 """Benchmark: incoherent ray-query throughput on one B200 (config 4 workload).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl rb2|reference]
-                  [--mode plain|batched] [--rays-per-scene R] [--scenes S]
+                  [--rays-per-scene R] [--scenes S] [--workload trace|ao|pt|bdpt]
 
 One step = every scene's ray batch traced once: 64 heightfield scenes with
 log-uniform 1k..2M triangles, 1M incoherent diffuse-bounce rays per scene,
 50 % closest-hit and 50 % any-hit (occlusion).  Inputs are resident in HBM
 when the timed region starts; L2 is flushed (256 MB write) between timed
 steps.  `e2e` repeats the step through the host-buffer C-ABI call
-(rb2_trace_host), copies included.  Under torchrun each rank runs the same
+(rb2_trace_host_jobs: pinned host rays in, hits / occlusion bytes out, the
+copies pipelined with traversal over several streams), copies included.  Under torchrun each rank runs the same
 workload on its own GPU (replicas, no collective); `value` = all ranks' rays
 / max-over-ranks time.
 
@@ -221,37 +222,64 @@ def run_rb2(args, rank, world, local_rank):
         plain_ms = timed(lambda: plain_step(True), args.steps, collect_plain)
         batch_ms = timed(lambda: batch.launch(stream), args.steps)
     clocks = clk.summary()
-    plain_total = max_over_ranks(float(sum(plain_ms)), world, dev)
-    batch_total = max_over_ranks(float(sum(batch_ms)), world, dev)
+    plain_rate, plain_total = whole_job_rate(total_rays * args.steps, sum(plain_ms), world, dev)
+    batch_rate, batch_total = whole_job_rate(total_rays * args.steps, sum(batch_ms), world, dev)
     for t in tracers:
         assert t.status() == 0, "device status word set"
     assert batch.status() == 0, "batch status word set"
 
-    # ---- e2e through the host-buffer C-ABI call (pinned host memory).
+    # ---- e2e through the host-buffer C-ABI calls (pinned host memory, copies in the timed region).
+    # Headline: rb2_trace_host_jobs, chunks cycling through several streams so
+    # H2D, traversal and D2H overlap.  Also reported: one blocking
+    # rb2_trace_host call per job (no overlap).
     h_rays = [torch.from_numpy(s["rays"]).pin_memory() for s in scenes]
-    h_hits = [torch.empty((s["rays"].shape[0], 4), dtype=torch.int32).pin_memory() for s in scenes]
+    h_hits = [torch.empty((s["n_ch"], 4), dtype=torch.int32).pin_memory() for s in scenes]
+    h_occ = [torch.empty((s["rays"].shape[0] - s["n_ch"],), dtype=torch.uint8).pin_memory() for s in scenes]
+    h_hits16 = [torch.empty((s["rays"].shape[0], 4), dtype=torch.int32).pin_memory() for s in scenes]
     from renderbox2_b200._native import check, lib
     L = lib()
     sh = stream.cuda_stream
+    pipe = rb.HostPipeline(chunk_rays=args.e2e_chunk, depth=args.e2e_depth)
+    host_jobs = []
+    for k, s in enumerate(scenes):
+        n_ch = s["n_ch"]
+        host_jobs.append((tracers[k], h_rays[k][:n_ch], rb.MODE_CLOSEST, h_hits[k], None))
+        host_jobs.append((tracers[k], h_rays[k][n_ch:], rb.MODE_OCCLUSION, h_occ[k], None))
+    host_arr = pipe.job_array(host_jobs)
+    h2d_bytes = int(total_rays * 32)
+    d2h_bytes = int(n_ch_total * 16 + (total_rays - n_ch_total))
 
     def e2e_step():
+        pipe.trace_jobs(host_arr, stream)
+
+    def e2e_single_step():
         for k, s in enumerate(scenes):
             n_ch = s["n_ch"]
-            hr, hh = h_rays[k], h_hits[k]
+            hr, hh = h_rays[k], h_hits16[k]
             check(L.rb2_trace_host(tracers[k].handle, hr.data_ptr(), n_ch, 0, None, hh.data_ptr(), sh))
             check(L.rb2_trace_host(tracers[k].handle, hr.data_ptr() + 32 * n_ch, s["rays"].shape[0] - n_ch, 1, None,
                                    hh.data_ptr() + 16 * n_ch, sh))
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    torch.cuda.synchronize(dev)
-    barrier(world)
+    def device_ms(fn, steps):
+        """CUDA events on `stream` around `steps` host calls (each call's
+        device work, copies included, is ordered on `stream`)."""
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        t0, t1 = ev(), ev()
+        t0.record(stream)
+        for _ in range(steps):
+            fn()
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+        return t0.elapsed_time(t1)
+
     e2e_steps = max(1, min(args.steps, 5))
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        e2e_step()
-    torch.cuda.synchronize(dev)
-    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, world, dev)
+    e2e_single_steps = max(1, min(args.steps, 2))
+    e2e_rate, _ = whole_job_rate(total_rays * e2e_steps, device_ms(e2e_step, e2e_steps), world, dev)
+    e2e_single_rate, _ = whole_job_rate(total_rays * e2e_single_steps, device_ms(e2e_single_step, e2e_single_steps),
+                                        world, dev)
 
     # ---- roofline: dominant kernel = the batched traversal launch (one per step).
     bytes_info, _, _, _ = oracle_bytes_sample(scenes, 4096)
@@ -281,8 +309,8 @@ def run_rb2(args, rank, world, local_rank):
         from renderbox2_b200.workloads import serving as serving_run
         serving = serving_run(n_jobs=args.serve_jobs)
 
-    value = world * total_rays * args.steps / (batch_total / 1e3) / 1e6
-    plain_value = world * total_rays * args.steps / (plain_total / 1e3) / 1e6
+    value = batch_rate / 1e6
+    plain_value = plain_rate / 1e6
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(batch_total / args.steps, 4), "higher_is_better": True,
@@ -305,9 +333,12 @@ def run_rb2(args, rank, world, local_rank):
                      "alg_bytes_per_launch": round(alg_per_launch),
                      "alg_bytes_per_ray": round(alg_per_launch / total_rays, 1),
                      "traffic_source": "scaled from ncu dram bytes of the 2M-triangle capture"},
-        "e2e": {"value": round(world * total_rays * e2e_steps / (e2e_ms / 1e3) / 1e6, 2), "unit": "Mrays/s",
-                "h2d_bytes_per_step": int(total_rays * 32), "d2h_bytes_per_step": int(total_rays * 16),
-                "path": "rb2_trace_host per scene half (pinned host buffers, copies in the timed region)"},
+        "e2e": {"value": round(e2e_rate / 1e6, 2), "unit": "Mrays/s",
+                "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
+                "path": f"rb2_trace_host_jobs over the 128 jobs (pinned host buffers, chunks of {args.e2e_chunk} "
+                        f"rays through {args.e2e_depth} streams, copies in the timed region, CUDA events)",
+                "single_call_mrays": round(e2e_single_rate / 1e6, 2),
+                "single_call_path": "one blocking rb2_trace_host per job, 16-byte hits for every ray"},
         "gpu_launches": args.steps * (1 + 2 * len(scenes)),
         "gpu_launches_note": "timed region: batched steps (1 traversal launch each) + plain steps (2 per scene)",
         "clocks": clocks,
@@ -421,6 +452,14 @@ def max_over_ranks(x: float, world, dev) -> float:
     return float(t.item())
 
 
+def whole_job_rate(units_per_rank: float, local_ms: float, world: int, dev) -> tuple[float, float]:
+    """Replicas: every rank processes units_per_rank in local_ms; the job's
+    rate is all ranks' units over the slowest rank's time.  Returns
+    (units per second, max-over-ranks ms)."""
+    ms = max_over_ranks(float(local_ms), world, dev)
+    return world * units_per_rank / (ms / 1e3), ms
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -431,6 +470,8 @@ def main():
     ap.add_argument("--rays-per-scene", type=int, default=1 << 20)
     ap.add_argument("--ref-rays-per-scene", type=int, default=2048)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--e2e-chunk", type=int, default=1 << 19, help="rays per chunk of the pipelined host path")
+    ap.add_argument("--e2e-depth", type=int, default=4, help="streams of the pipelined host path")
     ap.add_argument("--serve-jobs", type=int, default=300, help="config-5 jobs in the serving measurement (0: skip)")
     ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt"], default="trace",
                     help="trace: the headline config-4 line; ao/pt/bdpt: configs 1-3 at full size")

@@ -148,6 +148,29 @@ int rb2_trace(rb2_tracer* t, const float* d_rays, uint32_t n, int any_hit, const
 int rb2_trace_host(rb2_tracer* t, const float* h_rays, uint32_t n, int any_hit, const uint8_t* h_mask,
                    rb2_hit* h_hits, void* stream);
 
+/* Host-buffer traces of many jobs, pipelined: rays are cut into chunks that
+ * cycle through `depth` streams, so the upload of one chunk, the traversal of
+ * the previous one and the download of the one before overlap (copy engines
+ * and SMs busy at once).  Host buffers should be pinned for the copies to be
+ * asynchronous.  rb2_trace_host_jobs returns when every output is on the host;
+ * its work starts after what is queued on `stream` and `stream` waits for all
+ * of it (so CUDA events on `stream` bracket it).  The pipeline owns its
+ * streams and device staging (depth x chunk x 49 B); one host thread at a time.
+ * Extends the host-buffer path of rb2_trace_host (same outputs per job). */
+typedef struct rb2_pipeline rb2_pipeline;
+typedef struct {
+    rb2_tracer* tracer;
+    const float* h_rays;      /* 8 floats per ray */
+    uint64_t n;
+    uint32_t mode;            /* RB2_MODE_* (closest/any: rb2_hit out; occlusion: uint8 out) */
+    uint32_t reserved;
+    const uint8_t* h_mask;    /* nullable */
+    void* h_out;
+} rb2_host_job;
+int rb2_pipeline_create(uint64_t chunk_rays, uint32_t depth, rb2_pipeline** out);
+int rb2_pipeline_destroy(rb2_pipeline* p);
+int rb2_trace_host_jobs(rb2_pipeline* p, const rb2_host_job* jobs, uint32_t n_jobs, void* stream);
+
 /* Occlusion-only any-hit: writes 1 byte per ray (1 = occluded). */
 int rb2_trace_occlusion(rb2_tracer* t, const float* d_rays, uint32_t n, const uint8_t* d_mask,
                         uint8_t* d_occluded, void* stream);

@@ -7,8 +7,9 @@ CPU-baseline leg of bench.py -- never by the product library:
   text BVH cache, perspective camera, Moller-Trumbore test) compiled in place
   from the reference sources into oracle/_ref/librb2ref.so (oracle/Makefile).
 * ``trace`` / ``woop_test`` / ``bruteforce``: the CPU restatement of the
-  reference's traversal (oracle/rb2_oracle.c), plus the integrator
-  restatements in oracle/shading.py.
+  reference's traversal (oracle/rb2_oracle.c).
+* ``ao`` / ``pt`` / ``bdpt``: FP64 CPU restatements of the integrators
+  (same file), scalar per pixel, used as statistical references.
 
 Parity is pinned by comparing the restatement with the reference's own
 compiled code and against fixtures in tests/golden/ generated from it.

@@ -42,6 +42,11 @@ class TraceJob(C.Structure):
                 ("reserved", C.c_uint32), ("d_mask", C.c_void_p), ("d_out", C.c_void_p)]
 
 
+class HostJob(C.Structure):
+    _fields_ = [("tracer", C.c_void_p), ("h_rays", C.c_void_p), ("n", C.c_uint64), ("mode", C.c_uint32),
+                ("reserved", C.c_uint32), ("h_mask", C.c_void_p), ("h_out", C.c_void_p)]
+
+
 class BatchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("fetch_threshold", C.c_uint32),
                 ("chunk", C.c_uint32), ("node_order", C.c_uint32), ("regs", C.c_uint32)]
@@ -103,6 +108,9 @@ SIGNATURES = {
     "rb2_trace_occlusion": (C.c_int, [P, P, U32, P, P, P]),
     "rb2_tracer_status": (C.c_int, [P, C.POINTER(U32), P]),
     "rb2_tracer_set_node_order": (C.c_int, [P, U32]),
+    "rb2_pipeline_create": (C.c_int, [U64, U32, C.POINTER(P)]),
+    "rb2_pipeline_destroy": (C.c_int, [P]),
+    "rb2_trace_host_jobs": (C.c_int, [P, C.POINTER(HostJob), U32, P]),
     "rb2_batch_create": (C.c_int, [C.POINTER(TraceJob), U32, C.POINTER(P)]),
     "rb2_batch_destroy": (C.c_int, [P]),
     "rb2_batch_set_config": (C.c_int, [P, C.POINTER(BatchConfig)]),

@@ -335,3 +335,47 @@ class TraceBatch:
         v = C.c_uint32()
         check(lib().rb2_batch_status(self._b, C.byref(v), _stream_handle(stream)))
         return v.value
+
+
+class HostPipeline:
+    """Host-buffer traces of many jobs with copies overlapped with traversal.
+
+    Each job's rays are cut into chunks of `chunk_rays` that cycle through
+    `depth` CUDA streams: the upload of one chunk, the traversal of another
+    and the download of a third run at once.  Use pinned host memory (torch
+    `pin_memory()` tensors) for the copies to be asynchronous.
+
+    jobs: iterable of (tracer, host rays (n, 8) float32, mode, host out, mask
+    or None); out is (n, 4) int32 for MODE_CLOSEST / MODE_ANY and (n,) uint8
+    for MODE_OCCLUSION.  trace_jobs returns when every output is on the host."""
+
+    def __init__(self, chunk_rays: int = 1 << 20, depth: int = 4):
+        self._p = C.c_void_p()
+        check(lib().rb2_pipeline_create(int(chunk_rays), int(depth), C.byref(self._p)))
+
+    def __del__(self):
+        p = getattr(self, "_p", None)
+        if p and p.value:
+            lib().rb2_pipeline_destroy(p)
+            self._p = C.c_void_p()
+
+    @staticmethod
+    def job_array(jobs):
+        from ._native import HostJob
+        jobs = list(jobs)
+        arr = (HostJob * max(1, len(jobs)))()
+        for k, (tr, rays, mode, out, mask) in enumerate(jobs):
+            arr[k].tracer = tr.handle.value
+            arr[k].h_rays = _ptr(rays)
+            arr[k].n = int(rays.shape[0])
+            arr[k].mode = int(mode)
+            arr[k].h_mask = _ptr(mask)
+            arr[k].h_out = _ptr(out)
+        return arr, len(jobs)
+
+    def trace_jobs(self, jobs, stream=None):
+        """jobs: a list of tuples as above, or the result of job_array().  The
+        work is ordered after `stream` (default: the current torch stream)
+        and `stream` waits for it."""
+        arr, n = jobs if isinstance(jobs, tuple) else self.job_array(jobs)
+        check(lib().rb2_trace_host_jobs(self._p, arr, n, _stream_handle(stream)))

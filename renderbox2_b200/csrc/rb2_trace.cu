@@ -667,3 +667,112 @@ DeviceBvhView device_bvh(const rb2_tracer* t)
     return DeviceBvhView{t->d_nodes, t->d_woop, t->d_triidx, t->d_status};
 }
 }  // namespace rb2
+
+// ------------------------------------------------------------------ pipelined host path
+struct rb2_pipeline {
+    struct Slot {
+        cudaStream_t stream = nullptr;
+        cudaEvent_t done = nullptr;
+        float4* d_rays = nullptr;
+        int4* d_out = nullptr;
+        uint8_t* d_mask = nullptr;
+        bool busy = false;
+    };
+    std::vector<Slot> slots;
+    uint64_t chunk = 0;
+    cudaEvent_t entry = nullptr;  // recorded on the caller's stream at entry
+};
+
+extern "C" {
+
+int rb2_pipeline_destroy(rb2_pipeline* p)
+{
+    if (!p) return RB2_OK;
+    for (auto& s : p->slots) {
+        if (s.stream) cudaStreamSynchronize(s.stream);
+        cudaFree(s.d_rays);
+        cudaFree(s.d_out);
+        cudaFree(s.d_mask);
+        if (s.done) cudaEventDestroy(s.done);
+        if (s.stream) cudaStreamDestroy(s.stream);
+    }
+    if (p->entry) cudaEventDestroy(p->entry);
+    delete p;
+    return RB2_OK;
+}
+
+int rb2_pipeline_create(uint64_t chunk_rays, uint32_t depth, rb2_pipeline** out)
+{
+    if (!out || chunk_rays == 0 || chunk_rays > 0xFFFFFFFFull || depth == 0 || depth > 16)
+        return fail(RB2_EINVAL, "pipeline needs 0 < chunk_rays < 2^32 and 0 < depth <= 16");
+    *out = nullptr;
+    std::unique_ptr<rb2_pipeline> p(new rb2_pipeline());
+    p->chunk = chunk_rays;
+    p->slots.resize(depth);
+    if (cudaEventCreateWithFlags(&p->entry, cudaEventDisableTiming) != cudaSuccess) {
+        rb2_pipeline_destroy(p.release());
+        return fail(RB2_ECUDA, "pipeline event");
+    }
+    for (auto& s : p->slots) {
+        cudaError_t e;
+        if ((e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaMalloc(&s.d_rays, chunk_rays * 32)) != cudaSuccess ||
+            (e = cudaMalloc(&s.d_out, chunk_rays * 16)) != cudaSuccess ||
+            (e = cudaMalloc(&s.d_mask, chunk_rays)) != cudaSuccess) {
+            rb2_pipeline_destroy(p.release());
+            return fail(RB2_ENOMEM, std::string("pipeline staging: ") + cudaGetErrorString(e));
+        }
+    }
+    *out = p.release();
+    return RB2_OK;
+}
+
+int rb2_trace_host_jobs(rb2_pipeline* p, const rb2_host_job* jobs, uint32_t n_jobs, void* stream)
+{
+    if (!p || (n_jobs && !jobs)) return fail(RB2_EINVAL, "null argument");
+    const cudaStream_t caller = (cudaStream_t)stream;
+    for (uint32_t i = 0; i < n_jobs; i++) {
+        const rb2_host_job& j = jobs[i];
+        if (!j.tracer || (j.n && (!j.h_rays || !j.h_out)) || j.mode > RB2_MODE_OCCLUSION)
+            return fail(RB2_EINVAL, "bad host job");
+    }
+    const size_t nslots = p->slots.size();
+    // Work ordered after what the caller queued on `stream`.
+    RB2_CUDA(cudaEventRecord(p->entry, caller), "pipeline entry");
+    for (auto& s : p->slots) RB2_CUDA(cudaStreamWaitEvent(s.stream, p->entry, 0), "pipeline entry wait");
+    size_t k = 0;
+    for (uint32_t i = 0; i < n_jobs; i++) {
+        const rb2_host_job& j = jobs[i];
+        const size_t out_b = j.mode == RB2_MODE_OCCLUSION ? 1 : 16;
+        for (uint64_t off = 0; off < j.n; off += p->chunk, k++) {
+            const uint64_t n = std::min<uint64_t>(p->chunk, j.n - off);
+            auto& s = p->slots[k % nslots];
+            if (s.busy) RB2_CUDA(cudaEventSynchronize(s.done), "pipeline slot wait");
+            RB2_CUDA(cudaMemcpyAsync(s.d_rays, j.h_rays + 8 * off, n * 32, cudaMemcpyHostToDevice, s.stream), "chunk upload");
+            if (j.h_mask) RB2_CUDA(cudaMemcpyAsync(s.d_mask, j.h_mask + off, n, cudaMemcpyHostToDevice, s.stream), "mask upload");
+            const uint8_t* mask = j.h_mask ? s.d_mask : nullptr;
+            int rc = j.mode == RB2_MODE_OCCLUSION
+                         ? trace_single(j.tracer, reinterpret_cast<const float*>(s.d_rays), n, rb2dev::kOcclusion, mask,
+                                        s.d_out, s.stream)
+                         : trace_single(j.tracer, reinterpret_cast<const float*>(s.d_rays), n,
+                                        j.mode == RB2_MODE_ANY ? rb2dev::kAny : rb2dev::kClosest, mask, s.d_out, s.stream);
+            if (rc) return rc;
+            RB2_CUDA(cudaMemcpyAsync(static_cast<uint8_t*>(j.h_out) + off * out_b, s.d_out, n * out_b,
+                                     cudaMemcpyDeviceToHost, s.stream), "chunk download");
+            RB2_CUDA(cudaEventRecord(s.done, s.stream), "pipeline event");
+            s.busy = true;
+        }
+    }
+    // `stream` waits for every chunk, so events recorded on it bracket the
+    // whole pipelined job set (copies included).
+    for (auto& s : p->slots) {
+        if (!s.busy) continue;
+        RB2_CUDA(cudaStreamWaitEvent(caller, s.done, 0), "pipeline join");
+        RB2_CUDA(cudaEventSynchronize(s.done), "pipeline drain");
+        s.busy = false;
+    }
+    return RB2_OK;
+}
+
+}  // extern "C"

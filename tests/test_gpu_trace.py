@@ -112,6 +112,47 @@ def test_mask_empty_and_host_path(rb, orc, cuda):
     assert np.array_equal(host_m, got)
 
 
+@pytest.mark.parametrize("chunk,depth", [(1000, 3), (1 << 20, 1), (777, 16)])
+def test_pipelined_host_jobs_match_oracle(rb, orc, cuda, chunk, depth):
+    """rb2_trace_host_jobs over two scenes x three modes, ragged chunking
+    (chunk boundaries inside jobs, last chunk short), masks on some jobs,
+    an empty job: every output equals the oracle's."""
+    torch = cuda
+    pipe = rb.HostPipeline(chunk_rays=chunk, depth=depth)
+    jobs, want = [], []
+    for k, (n_tris, n) in enumerate([(20_000, 4099), (3_000, 2500)]):
+        sc = rb.heightfield_for_triangles(seed=900 + k, n_tris=n_tris)
+        bvh = rb.BVH(sc)
+        tr = rb.CudaTracer(bvh)
+        nodes, woop, tri = bvh.buffers_view()
+        rays, _ = rb.surface_rays(sc, seed=910 + k, n=n)
+        mask = (np.arange(n) % 5 != 1).astype(np.uint8)
+        pinned = torch.from_numpy(rays).pin_memory()
+        for mode, m in ((rb.MODE_CLOSEST, None), (rb.MODE_ANY, mask), (rb.MODE_OCCLUSION, mask)):
+            if mode == rb.MODE_OCCLUSION:
+                out = torch.full((n,), 7, dtype=torch.uint8).pin_memory()
+            else:
+                out = torch.full((n, 4), 7, dtype=torch.int32).pin_memory()
+            jobs.append((tr, pinned, mode, out, None if m is None else torch.from_numpy(m)))
+            ref = orc.trace(nodes, woop, tri, rays, any_hit=mode != rb.MODE_CLOSEST, mask=m)
+            want.append((mode, ref, nodes, woop, tri, rays, out))
+    empty_out = torch.full((1, 4), 7, dtype=torch.int32)
+    jobs.append((jobs[0][0], torch.empty((0, 8), dtype=torch.float32), rb.MODE_CLOSEST, empty_out, None))
+    pipe.trace_jobs(jobs)
+    for mode, ref, nodes, woop, tri, rays, out in want:
+        got = out.numpy()
+        if mode == rb.MODE_CLOSEST:
+            ties, bad, first = compare_closest(orc, got, _oracle_dict(ref), woop, tri, rays)
+            assert bad == 0, f"ray {first}"
+        elif mode == rb.MODE_ANY:
+            assert compare_any(got, ref) == 0
+        else:
+            assert np.array_equal(got.astype(bool), ref["prim"] >= 0)
+    assert (empty_out.numpy() == 7).all()
+    for j in jobs:
+        assert j[0].status() == 0
+
+
 def test_config1_full_size(rb, orc, cuda):
     """Config 1 at full size (131,840 triangles, 512x512 primary rays, 4M
     diffuse rays): primary rays bit-exact against the oracle; for the 4M
