@@ -142,6 +142,27 @@ int rb2_tracer_device_bytes(const rb2_tracer* t, uint64_t* bytes);
 int rb2_trace(rb2_tracer* t, const float* d_rays, uint32_t n, int any_hit, const uint8_t* d_mask,
               rb2_hit* d_hits, void* stream);
 
+/* Device view of a tracer's BVH for kernels that call the header-only
+ * rb2::trace_ray (rb2_device.cuh).  Replaces CudaTracer::get_bvh()
+ * (cudatracer.h:89-101), which returned texture objects.  The pointers stay
+ * valid until rb2_tracer_destroy. */
+typedef struct {
+    const void* nodes;        /* float4 Compact2 inner nodes, 16-byte aligned */
+    const void* woop;         /* float4 Woop rows + terminators */
+    const uint32_t* triidx;   /* original triangle id per Woop slot */
+    uint64_t n_nodes_u4;
+    uint64_t n_woop_u4;
+} rb2_dev_bvh;
+int rb2_tracer_dev_bvh(const rb2_tracer* t, rb2_dev_bvh* out);
+
+/* Bulk trace with one thread per ray (no persistent queue) through the
+ * header-only rb2::trace_ray: the pattern of kernels that trace inside their
+ * own code, as the reference's integrator megakernels do
+ * (integrators/integrator_path.cu:43-261 calls trace_ray).  Same outputs as
+ * rb2_trace with single-lane traversal order. */
+int rb2_trace_per_thread(rb2_tracer* t, const float* d_rays, uint32_t n, int any_hit, const uint8_t* d_mask,
+                         rb2_hit* d_hits, void* stream);
+
 /* Same from/to host memory: copies rays in, traces, copies hits out, and
  * synchronises `stream`.  Scratch device buffers are grown on demand and
  * reused across calls. */

@@ -50,6 +50,43 @@ int rb2_scene_create(const float* v_xyz, uint32_t nv, const uint32_t* idx3, uint
 int rb2_scene_destroy(rb2_scene_dev* s);
 int rb2_scene_device_bytes(const rb2_scene_dev* s, uint64_t* bytes);
 
+/* Device view of a scene for the header-only rb2::trace_ray /
+ * rb2::fill_intersection (rb2_device.cuh).  Replaces SceneBuffer
+ * (core/buffer.h:322-345) for what the trace reads: vertex positions and
+ * per-triangle vertex indices + material id. */
+typedef struct {
+    const void* verts;        /* float4 per vertex (xyz, w unused) */
+    const void* tris;         /* uint4 per triangle (3 vertex indices, material id) */
+    uint32_t nv, ntri;
+} rb2_dev_scene;
+int rb2_scene_dev_view(const rb2_scene_dev* s, rb2_dev_scene* out);
+
+/* ------------------------------------------------------ intersection records --
+ * Replaces CudaTracer::trace(const RayBuffer&, IntersectionBuffer&,
+ * SceneBuffer&, uint8_t* stencil, bool any_hit) (cudatracer.h:87) with the
+ * reference's SoA IntersectionBuffer (core/intersection.h:63-80), minus the
+ * fields that trace leaves unwritten (tangent, bitangent, depth,
+ * contribution).  Device pointers; any may be NULL to skip that field.
+ * Closest hit fills every field of hit rays (kepler_dynamic_fetch.h:313-355)
+ * and `intersected` of all rays; any hit writes `intersected` only; masked
+ * rays get intersected = 0.  Shading normal = geometric normal (no vertex
+ * normals), uv of the accepted triangle.  One persistent traversal launch
+ * with the record written in the same kernel. */
+typedef struct {
+    float* position[3];
+    float* geometric_normal[3];
+    float* shading_normal[3];
+    float* incoming_direction[3];
+    float* uv;                      /* 2 floats per ray (float2) */
+    uint32_t* primitive_id;
+    uint32_t* primitive_material_id;
+    uint8_t* front;
+    uint8_t* intersected;
+    float* epsilon;
+} rb2_isect_buffer;
+int rb2_trace_isect(rb2_tracer* t, const rb2_scene_dev* scene, const float* d_rays, uint32_t n, int any_hit,
+                    const uint8_t* d_mask, const rb2_isect_buffer* out, void* stream);
+
 /* An integrator binds a tracer (BVH) and a device scene and owns the
  * wavefront scratch (grown on demand, reused across renders).  Replaces
  * Integrator::render(Scene*, CudaTracer*, void**, uint32_t) (core/integrator.h:59). */

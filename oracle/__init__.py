@@ -78,6 +78,8 @@ def ref_lib():
         L.rb2ref_camera_rays.restype = C.c_int
         L.rb2ref_intersect_triangle.argtypes = [C.c_void_p] * 5
         L.rb2ref_intersect_triangle.restype = C.c_int
+        L.rb2ref_normal_and_point.argtypes = [C.c_void_p] * 4 + [C.c_float, C.c_void_p, C.c_void_p]
+        L.rb2ref_normal_and_point.restype = C.c_int
         _ref = L
     return _ref
 
@@ -151,6 +153,44 @@ def ref_intersect_triangle(v0, v1, v2, ray8):
     uvt = np.zeros(3, np.float32)
     hit = ref_lib().rb2ref_intersect_triangle(_p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]), _p(uvt))
     return bool(hit), uvt
+
+
+def ref_normal_and_point(v0, v1, v2, ray8, t):
+    """The reference's compute_normal(v0, v1, v2) and Ray(o, d)(t)."""
+    a = [np.ascontiguousarray(x, np.float32) for x in (v0, v1, v2, ray8)]
+    ng, pt = np.zeros(3, np.float32), np.zeros(3, np.float32)
+    ref_lib().rb2ref_normal_and_point(_p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]), float(t), _p(ng), _p(pt))
+    return ng, pt
+
+
+class _IsectSoa(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("position", "ng", "ns", "wi", "uv", "prim", "material", "front",
+                                          "intersected", "epsilon")]
+
+
+def isect(verts, tris4, rays, hits):
+    """Intersection records of closest hits (rb2o_isect): a dict of SoA arrays
+    position/ng/ns/wi (3, n) float32, uv (n, 2), prim, material (n,) uint32,
+    front, intersected (n,) uint8, epsilon (n,) float32.  Fields of missed
+    rays keep their initial value (NaN / 0xFFFFFFFF / 0xFF)."""
+    verts = np.ascontiguousarray(verts, np.float32)
+    tris4 = np.ascontiguousarray(tris4, np.uint32)
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    hits = np.ascontiguousarray(hits, HIT_DTYPE)
+    n = rays.shape[0]
+    out = {k: np.full((3, n), np.nan, np.float32) for k in ("position", "ng", "ns", "wi")}
+    out["uv"] = np.full((n, 2), np.nan, np.float32)
+    out["prim"] = np.full(n, 0xFFFFFFFF, np.uint32)
+    out["material"] = np.full(n, 0xFFFFFFFF, np.uint32)
+    out["front"] = np.full(n, 0xFF, np.uint8)
+    out["intersected"] = np.full(n, 0xFF, np.uint8)
+    out["epsilon"] = np.full(n, np.nan, np.float32)
+    soa = _IsectSoa(**{k: _p(v) for k, v in out.items()})
+    L = orc_lib()
+    L.rb2o_isect.argtypes = [C.c_void_p] * 4 + [C.c_uint32, C.POINTER(_IsectSoa)]
+    L.rb2o_isect.restype = None
+    L.rb2o_isect(_p(verts), _p(tris4), _p(rays), _p(hits), n, C.byref(soa))
+    return out
 
 
 def trace(nodes, woop, triidx, rays, any_hit=False, mask=None, counts=False, nthreads=0):

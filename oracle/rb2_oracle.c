@@ -202,6 +202,43 @@ void rb2o_trace(const uint32_t* nodes, const uint32_t* woop, const uint32_t* tri
     (void)nthreads;
 }
 
+void rb2o_isect(const float* verts, const uint32_t* tris4, const float* rays, const rb2o_hit* hits, uint32_t n,
+                rb2o_isect_soa* out)
+{
+    for (uint32_t i = 0; i < n; i++) {
+        const rb2o_hit* h = hits + i;
+        if (h->prim < 0) { out->intersected[i] = 0; continue; }
+        const uint32_t* tr = tris4 + 4 * (size_t)h->prim;
+        const float* a = verts + 3 * (size_t)tr[0];
+        const float* b = verts + 3 * (size_t)tr[1];
+        const float* c = verts + 3 * (size_t)tr[2];
+        const float e1x = b[0] - a[0], e1y = b[1] - a[1], e1z = b[2] - a[2];
+        const float e2x = c[0] - a[0], e2y = c[1] - a[1], e2z = c[2] - a[2];
+        const float cx = e1y * e2z - e1z * e2y;
+        const float cy = e1z * e2x - e1x * e2z;
+        const float cz = e1x * e2y - e1y * e2x;
+        const float len2 = (cx * cx + cy * cy) + cz * cz;
+        const float inv = 1.0f / sqrtf(len2);
+        const float ng[3] = {cx * inv, cy * inv, cz * inv};
+        const float* r = rays + 8 * (size_t)i;
+        const float t = h->t;
+        for (int k = 0; k < 3; k++) {
+            out->position[(size_t)k * n + i] = r[k] + r[4 + k] * t;
+            out->ng[(size_t)k * n + i] = ng[k];
+            out->ns[(size_t)k * n + i] = ng[k];
+            out->wi[(size_t)k * n + i] = -r[4 + k];
+        }
+        const float dn = (ng[0] * r[4] + ng[1] * r[5]) + ng[2] * r[6];
+        out->front[i] = dn < 0.0f ? 1 : 0;
+        out->uv[2 * (size_t)i] = h->u;
+        out->uv[2 * (size_t)i + 1] = h->v;
+        out->prim[i] = (uint32_t)h->prim;
+        out->material[i] = tr[3];
+        out->epsilon[i] = 1.0e-3f * t;
+        out->intersected[i] = 1;
+    }
+}
+
 int rb2o_woop_test(const uint32_t* woop12, const float* ray8, float tmax, float* tuv)
 {
     ray_setup s;

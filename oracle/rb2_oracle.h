@@ -40,6 +40,32 @@ int rb2o_woop_test(const uint32_t* woop12, const float* ray8, float tmax, float*
 void rb2o_bruteforce(const uint32_t* woop, const uint32_t* triidx, uint32_t n_woop_u4,
                      const float* rays, uint32_t n, rb2o_hit* out, int nthreads);
 
+/* Intersection record of a closest hit, as the reference's bulk kernel fills
+ * IntersectionBuffer (accelerators/sbvh/kepler_dynamic_fetch.h:313-355),
+ * in IEEE single precision with no contraction:
+ *   Ng  = normalize(cross(v1 - v0, v2 - v0)), normalize(x) = x * (1/sqrtf(dot(x,x)))
+ *         (core/primitives.h:267-270), dot = (x.x*y.x + x.y*y.y) + x.z*y.z
+ *   Ns  = Ng (the generated scenes carry no vertex normals)
+ *   position = o + d * t;  wi = -d;  front = dot(Ng, d) < 0
+ *   uv = (u, v) of the accepted triangle;  epsilon = 1e-3f * t
+ *   intersected = 1 on a hit, 0 on a miss or a masked ray; other fields are
+ *   left untouched on a miss.
+ * tris: 4 words per triangle (3 vertex indices, material id). */
+typedef struct {
+    float* position;      /* 3 per ray (SoA planes: x[n], y[n], z[n]) */
+    float* ng;
+    float* ns;
+    float* wi;
+    float* uv;            /* 2 per ray, interleaved */
+    uint32_t* prim;
+    uint32_t* material;
+    uint8_t* front;
+    uint8_t* intersected;
+    float* epsilon;
+} rb2o_isect_soa;
+void rb2o_isect(const float* verts, const uint32_t* tris4, const float* rays, const rb2o_hit* hits, uint32_t n,
+                rb2o_isect_soa* out);
+
 /* ---- shading references (FP64 accumulation) ---------------------------------
  * Scene for the integrator references: vertices (xyz), triangles (3 indices),
  * per-triangle material, per-material albedo/emission (rgb), emissive

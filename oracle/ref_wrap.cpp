@@ -187,4 +187,18 @@ int rb2ref_intersect_triangle(const float* v0, const float* v1, const float* v2,
     return hit ? 1 : 0;
 }
 
+// compute_normal (core/primitives.h:267-270) and Ray::operator() (:171-174)
+// from the reference, for pinning the intersection-record arithmetic.
+int rb2ref_normal_and_point(const float* v0, const float* v1, const float* v2, const float* ray8, float t,
+                            float* ng_out, float* p_out)
+{
+    float3 n = compute_normal(make_float3(v0[0], v0[1], v0[2]), make_float3(v1[0], v1[1], v1[2]),
+                              make_float3(v2[0], v2[1], v2[2]));
+    Ray r(make_float4(ray8[0], ray8[1], ray8[2], ray8[3]), make_float4(ray8[4], ray8[5], ray8[6], ray8[7]));
+    float3 p = r(t);
+    ng_out[0] = n.x; ng_out[1] = n.y; ng_out[2] = n.z;
+    p_out[0] = p.x; p_out[1] = p.y; p_out[2] = p.z;
+    return 0;
+}
+
 }  // extern "C"

@@ -47,6 +47,22 @@ class HostJob(C.Structure):
                 ("reserved", C.c_uint32), ("h_mask", C.c_void_p), ("h_out", C.c_void_p)]
 
 
+class DevBvh(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("woop", C.c_void_p), ("triidx", C.c_void_p), ("n_nodes_u4", C.c_uint64),
+                ("n_woop_u4", C.c_uint64)]
+
+
+class DevScene(C.Structure):
+    _fields_ = [("verts", C.c_void_p), ("tris", C.c_void_p), ("nv", C.c_uint32), ("ntri", C.c_uint32)]
+
+
+class IsectBuffer(C.Structure):
+    _fields_ = [("position", C.c_void_p * 3), ("geometric_normal", C.c_void_p * 3),
+                ("shading_normal", C.c_void_p * 3), ("incoming_direction", C.c_void_p * 3), ("uv", C.c_void_p),
+                ("primitive_id", C.c_void_p), ("primitive_material_id", C.c_void_p), ("front", C.c_void_p),
+                ("intersected", C.c_void_p), ("epsilon", C.c_void_p)]
+
+
 class BatchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("fetch_threshold", C.c_uint32),
                 ("chunk", C.c_uint32), ("node_order", C.c_uint32), ("regs", C.c_uint32)]
@@ -108,6 +124,10 @@ SIGNATURES = {
     "rb2_trace_occlusion": (C.c_int, [P, P, U32, P, P, P]),
     "rb2_tracer_status": (C.c_int, [P, C.POINTER(U32), P]),
     "rb2_tracer_set_node_order": (C.c_int, [P, U32]),
+    "rb2_tracer_dev_bvh": (C.c_int, [P, C.POINTER(DevBvh)]),
+    "rb2_trace_per_thread": (C.c_int, [P, P, U32, I32, P, P, P]),
+    "rb2_scene_dev_view": (C.c_int, [P, C.POINTER(DevScene)]),
+    "rb2_trace_isect": (C.c_int, [P, P, P, U32, I32, P, C.POINTER(IsectBuffer), P]),
     "rb2_pipeline_create": (C.c_int, [U64, U32, C.POINTER(P)]),
     "rb2_pipeline_destroy": (C.c_int, [P]),
     "rb2_trace_host_jobs": (C.c_int, [P, C.POINTER(HostJob), U32, P]),

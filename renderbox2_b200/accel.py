@@ -257,6 +257,24 @@ class CudaTracer:
                                    _stream_handle(stream)))
         return out
 
+    def trace_per_thread(self, rays, any_hit: bool = False, stencil=None, out=None, stream=None):
+        """One thread per ray through the header-only device traversal
+        (rb2_device.cuh): the pattern of kernels that trace in their own code."""
+        import torch
+        n = rays.shape[0]
+        if out is None:
+            out = torch.empty((n, 4), dtype=torch.int32, device=rays.device)
+        check(lib().rb2_trace_per_thread(self._t, _ptr(rays), n, 1 if any_hit else 0, _ptr(stencil), _ptr(out),
+                                         _stream_handle(stream)))
+        return out
+
+    def get_bvh(self) -> dict:
+        """Device view of the BVH (CudaTracer::get_bvh, cudatracer.h:89-101)."""
+        from ._native import DevBvh
+        d = DevBvh()
+        check(lib().rb2_tracer_dev_bvh(self._t, C.byref(d)))
+        return {k: getattr(d, k) for k, _ in DevBvh._fields_}
+
     def status(self, stream=None) -> int:
         v = C.c_uint32()
         check(lib().rb2_tracer_status(self._t, C.byref(v), _stream_handle(stream)))

@@ -121,6 +121,9 @@ struct DeviceBvhView {
 };
 DeviceBvhView device_bvh(const rb2_tracer* t);
 
+// A zeroed-before-use queue head of the tracer's ring (one per launch in flight).
+unsigned long long* tracer_queue_counter(rb2_tracer* t);
+
 inline uint32_t f2u(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
 inline float u2f(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
 

@@ -666,7 +666,20 @@ DeviceBvhView device_bvh(const rb2_tracer* t)
 {
     return DeviceBvhView{t->d_nodes, t->d_woop, t->d_triidx, t->d_status};
 }
+
+unsigned long long* tracer_queue_counter(rb2_tracer* t) { return t->next_counter(); }
 }  // namespace rb2
+
+extern "C" int rb2_tracer_dev_bvh(const rb2_tracer* t, rb2_dev_bvh* out)
+{
+    if (!t || !out) return fail(RB2_EINVAL, "null argument");
+    out->nodes = t->d_nodes;
+    out->woop = t->d_woop;
+    out->triidx = t->d_triidx;
+    out->n_nodes_u4 = t->n_nodes_u4;
+    out->n_woop_u4 = t->n_woop_u4;
+    return RB2_OK;
+}
 
 // ------------------------------------------------------------------ pipelined host path
 struct rb2_pipeline {

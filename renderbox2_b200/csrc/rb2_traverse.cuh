@@ -44,6 +44,24 @@ struct Lane {
     uint64_t ray;       // source-defined index of the ray within its job
 };
 
+// One 32-byte read-only load (sm_100 256-bit ld.global.nc.v8).  `p` must be
+// 32-byte aligned.
+__device__ __forceinline__ void ldg_v8(const float4* p, float4& a, float4& b)
+{
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
+
+// A 64-byte Compact2 node as two 256-bit loads: half the L1 tag lookups and
+// requests of four 128-bit loads.  Nodes are 64-byte aligned (child offsets
+// are multiples of 4 float4 into a 256-byte-aligned allocation).
+__device__ __forceinline__ void load_node(const float4* np, float4& n0xy, float4& n1xy, float4& nz, float4& cn)
+{
+    ldg_v8(np, n0xy, n1xy);
+    ldg_v8(np + 2, nz, cn);
+}
+
 __device__ __forceinline__ float fmin_s(float a, float b) { return a < b ? a : b; }
 __device__ __forceinline__ float fmax_s(float a, float b) { return a > b ? a : b; }
 __device__ __forceinline__ float imin_f(float a, float b) { return __int_as_float(min(__float_as_int(a), __float_as_int(b))); }
@@ -125,10 +143,8 @@ __device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_thr
                 if (!__any_sync(kFull, in)) break;
                 if (in) {
                     const float4* np = L.nodes + L.nodeAddr;
-                    const float4 n0xy = __ldg(np + 0);
-                    const float4 n1xy = __ldg(np + 1);
-                    const float4 nz = __ldg(np + 2);
-                    const float4 cn = __ldg(np + 3);
+                    float4 n0xy, n1xy, nz, cn;
+                    load_node(np, n0xy, n1xy, nz, cn);
                     int c0 = __float_as_int(cn.x), c1 = __float_as_int(cn.y);
 
                     const float c0lox = __fmaf_rn(n0xy.x, L.idx, -L.oodx);

@@ -10,7 +10,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._native import AoParams, BdptParams, PtParams, RenderStats, check, lib
+from ._native import AoParams, BdptParams, DevScene, IsectBuffer, PtParams, RenderStats, check, lib
 from .accel import CudaTracer, Scene, _ptr, _stream_handle
 
 
@@ -41,6 +41,68 @@ class DeviceScene:
     @property
     def handle(self):
         return self._s
+
+    def dev_view(self) -> dict:
+        d = DevScene()
+        check(lib().rb2_scene_dev_view(self._s, C.byref(d)))
+        return {k: getattr(d, k) for k, _ in DevScene._fields_}
+
+
+class IntersectionBuffer:
+    """The reference's SoA IntersectionBuffer (core/intersection.h:63-80) as
+    device tensors: position / geometric_normal / shading_normal /
+    incoming_direction (3, n) float32, uv (n, 2) float32, primitive_id and
+    primitive_material_id (n,) int32 (uint32 bits), front and intersected
+    (n,) uint8, epsilon (n,) float32.  `fields` limits which are allocated
+    (the others are skipped by the kernel)."""
+
+    VEC = ("position", "geometric_normal", "shading_normal", "incoming_direction")
+    ALL = VEC + ("uv", "primitive_id", "primitive_material_id", "front", "intersected", "epsilon")
+
+    def __init__(self, n: int, device="cuda", fields=None):
+        import torch
+        self.n = n
+        fields = self.ALL if fields is None else tuple(fields)
+        self.t = {}
+        for k in fields:
+            if k in self.VEC:
+                self.t[k] = torch.full((3, n), float("nan"), dtype=torch.float32, device=device)
+            elif k == "uv":
+                self.t[k] = torch.full((n, 2), float("nan"), dtype=torch.float32, device=device)
+            elif k == "epsilon":
+                self.t[k] = torch.full((n,), float("nan"), dtype=torch.float32, device=device)
+            elif k in ("front", "intersected"):
+                self.t[k] = torch.full((n,), 0xFF, dtype=torch.uint8, device=device)
+            else:
+                self.t[k] = torch.full((n,), -1, dtype=torch.int32, device=device)
+
+    def __getitem__(self, k):
+        return self.t[k]
+
+    def c_struct(self) -> IsectBuffer:
+        b = IsectBuffer()
+        for k in self.ALL:
+            x = self.t.get(k)
+            if k in self.VEC:
+                arr = getattr(b, k)
+                for j in range(3):
+                    arr[j] = None if x is None else x[j].data_ptr()
+            else:
+                setattr(b, k, None if x is None else x.data_ptr())
+        return b
+
+
+def trace_isect(tracer: CudaTracer, scene: DeviceScene, rays, any_hit: bool = True, stencil=None, out=None,
+                stream=None, fields=None) -> IntersectionBuffer:
+    """CudaTracer::trace(RayBuffer, IntersectionBuffer&, SceneBuffer&, stencil,
+    any_hit) (cudatracer.h:87).  Note the reference's default any_hit=True."""
+    n = rays.shape[0]
+    if out is None:
+        out = IntersectionBuffer(n, rays.device, fields)
+    b = out.c_struct()
+    check(lib().rb2_trace_isect(tracer.handle, scene.handle, _ptr(rays), n, 1 if any_hit else 0, _ptr(stencil),
+                                C.byref(b), _stream_handle(stream)))
+    return out
 
 
 @dataclass

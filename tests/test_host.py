@@ -207,3 +207,62 @@ def test_job_footprints_and_arrivals(rb):
     assert big > 10 * small > 0
     a = poisson_arrivals(5000, rate=100.0, seed=1)
     assert np.all(np.diff(a) > 0) and abs(5000 / a[-1] - 100.0) < 5.0
+
+
+def _compile_cpp(src, out, extra=()):
+    import shutil
+    import subprocess
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    lib = root / "renderbox2_b200" / "_lib"
+    cmd = ["g++", "-std=c++17", "-O1", f"-I{root / 'include'}", "-I/usr/local/cuda/include", str(src),
+           f"-L{lib}", "-lrb2", f"-Wl,-rpath,{lib}", *extra, "-o", str(out)]
+    subprocess.run(cmd, check=True, capture_output=True)
+
+
+def _fnv(b: bytes) -> int:
+    h = 1469598103934665603
+    for x in b:
+        h = ((h ^ x) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def test_cpp_compat_classes_build_and_cache(rb, tmp_path):
+    """rb2.hpp's reference-named classes (Scene/Mesh/BVH/CudaBvh) from C++:
+    the buffers equal a build of the same triangles through the Python layer,
+    and serialize() -> CudaBvh(file, ok) round-trips."""
+    import subprocess
+    from pathlib import Path
+    src = Path(__file__).resolve().parent / "cpp" / "compat_host.cpp"
+    exe = tmp_path / "compat_host"
+    _compile_cpp(src, exe)
+    out = subprocess.run([str(exe), str(tmp_path / "c.bvh")], check=True, capture_output=True, text=True).stdout
+    f = dict(zip(out.split()[0::2], out.split()[1::2]))
+    assert f["roundtrip"] == "1" and f["threw"] == "1"
+    assert int(f["tris"]) == 1154 and int(f["lights"]) == 2
+    # The same triangles through the Python layer.
+    g = 24
+    xs = np.arange(g + 1)
+    verts = []
+    for z in range(g + 1):
+        for x in range(g + 1):
+            y = np.float32(0.05) * np.float32((x * 7 + z * 3) % 5) / np.float32(4.0)
+            verts.append((np.float32(x) / np.float32(g), y, np.float32(z) / np.float32(g)))
+    idx = []
+    for z in range(g):
+        for x in range(g):
+            a = z * (g + 1) + x
+            b, c = a + 1, a + g + 1
+            idx += [(a, c, b), (b, c, c + 1)]
+    base = len(verts)
+    verts += [(0.4, 0.9, 0.4), (0.6, 0.9, 0.4), (0.4, 0.9, 0.6), (0.6, 0.9, 0.6)]
+    idx += [(base, base + 2, base + 1), (base + 1, base + 2, base + 3)]
+    del xs
+    sc = rb.Scene()
+    sc.add_mesh(np.asarray(verts, np.float32), np.asarray(idx, np.uint32))
+    bvh = rb.BVH(sc)
+    nodes, woop, _ = bvh.buffers_view()
+    assert int(f["nodes"]) == nodes.shape[0] and int(f["woop"]) == woop.shape[0]
+    assert int(f["hash"], 16) == _fnv(np.ascontiguousarray(nodes).tobytes())

@@ -151,3 +151,32 @@ def test_pcg32_matches_oracle_restatement(rb, orc):
     assert np.array_equal(rb.pcg32(42, 54, 6), ref)
     # O'Neill's published demo sequence for seed 42, stream 54.
     assert ref[0] == 0xA15C02B7 and ref[1] == 0x7B47F409
+
+
+def test_isect_record_matches_reference_arithmetic(rb, orc):
+    """The oracle's intersection record (geometric normal, hit position) is
+    bit-identical to the reference's own compute_normal and Ray::operator()
+    compiled from its sources; the remaining fields are plain copies."""
+    if not orc.have_ref():
+        pytest.skip("reference library not built")
+    scene = rb.RoomScene(seed=9, n_boxes=6, n_spheres=12, sphere_subdiv=2, n_lights=1)
+    bvh = rb.BVH(scene)
+    nodes, woop, tri = bvh.buffers_view()
+    rays, _ = rb.surface_rays(scene, seed=10, n=3000)
+    hits = orc.trace(nodes, woop, tri, rays)
+    v = np.asarray(scene.vertices, np.float32).reshape(-1, 3)
+    ix = np.asarray(scene.indices, np.uint32).reshape(-1, 3)
+    m = np.asarray(scene.material_ids, np.uint32).reshape(-1)
+    rec = orc.isect(v, np.concatenate([ix, m[:, None]], 1), rays, hits)
+    hit = np.nonzero(hits["prim"] >= 0)[0]
+    assert hit.size > 1000
+    for i in hit:
+        p = hits["prim"][i]
+        ng, pt = orc.ref_normal_and_point(v[ix[p, 0]], v[ix[p, 1]], v[ix[p, 2]], rays[i], hits["t"][i])
+        assert np.array_equal(ng.view(np.uint32), rec["ng"][:, i].view(np.uint32)), i
+        assert np.array_equal(pt.view(np.uint32), rec["position"][:, i].view(np.uint32)), i
+        assert rec["front"][i] == (1 if float(np.dot(ng.astype(np.float64), rays[i, 4:7])) < 0 else 0) or \
+            abs(float(np.dot(ng.astype(np.float64), rays[i, 4:7]))) < 1e-6
+        assert rec["material"][i] == m[p] and rec["prim"][i] == p
+    miss = hits["prim"] < 0
+    assert (rec["intersected"][miss] == 0).all() and np.isnan(rec["position"][:, miss]).all()
