@@ -291,15 +291,18 @@ def run_rb2(args, rank, world, local_rank):
     peak_src = "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
     alg_per_launch = ch_bytes + ah_bytes
     achieved = alg_per_launch / launch_s / 1e9
-    # DRAM traffic per launch: ncu capture of the closest-hit kernel on a
-    # 2M-triangle scene with 1M incoherent rays (profiles/k_trace_closest_2Mtri_full.md)
-    # measured 445.4 MB of DRAM traffic against 2266.2 MB of algorithmic bytes;
-    # scaled to this launch by algorithmic bytes.
-    traffic = alg_per_launch * (445.4 / 2266.2)
+    # DRAM traffic per launch: the ncu capture of the same batched kernel on
+    # 8 scenes x 500k triangles with 4.19M incoherent rays, half closest hit /
+    # half occlusion (profiles/k_trace_jobs_batched_8x500k_full.md), measured
+    # 657.7 MB of DRAM traffic against 7961.2 MB of algorithmic bytes; scaled
+    # to this launch by algorithmic bytes.
+    traffic = alg_per_launch * (657.7 / 7961.2)
 
-    cpu_baseline = None
+    cpu_baseline = builder = None
     if rank == 0 and world == 1:
         cpu_baseline = cpu_baseline_run(scenes, args.cpu_sample_s)
+        if args.cpu_sample_s > 0:
+            builder = build_baseline(scenes)
 
     # ---- config 5: served jobs (continuous batching) vs plain one-at-a-time launches.
     serving = None
@@ -332,7 +335,7 @@ def run_rb2(args, rank, world, local_rank):
                      "kernel": "k_trace_jobs<BLOCK> (batched, 1 launch/step)", "peak_source": peak_src,
                      "alg_bytes_per_launch": round(alg_per_launch),
                      "alg_bytes_per_ray": round(alg_per_launch / total_rays, 1),
-                     "traffic_source": "scaled from ncu dram bytes of the 2M-triangle capture"},
+                     "traffic_source": "scaled from ncu dram bytes of the 8 x 500k-triangle batched capture"},
         "e2e": {"value": round(e2e_rate / 1e6, 2), "unit": "Mrays/s",
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                 "path": f"rb2_trace_host_jobs over the 128 jobs (pinned host buffers, chunks of {args.e2e_chunk} "
@@ -345,6 +348,8 @@ def run_rb2(args, rank, world, local_rank):
     }
     if cpu_baseline is not None:
         line["cpu_baseline"] = cpu_baseline
+    if builder is not None:
+        line["build_baseline"] = builder
     if serving is not None:
         line["serving"] = serving
     if rank == 0:
@@ -359,11 +364,72 @@ def run_workload(args, rank, local_rank):
 
     from renderbox2_b200.workloads import integrator
     torch.cuda.set_device(local_rank)
-    r = integrator(args.workload)
+    keep = {}
+    r = integrator(args.workload, keep=keep)
     if rank == 0:
         names = {"ao": "config 1: ambient occlusion", "pt": "config 2: wavefront path tracing",
                  "bdpt": "config 3: BDPT with light-vertex cache"}
-        print(json.dumps({"metric": "samples/s and Mrays/s", "workload": names[args.workload], **r}), flush=True)
+        line = {"metric": "samples/s and Mrays/s", "workload": names[args.workload], **r}
+        if world_of_env() == 1 and args.cpu_sample_s > 0:
+            line["cpu_baseline"] = integrator_cpu_baseline(args.workload, keep)
+        print(json.dumps(line), flush=True)
+
+
+def world_of_env() -> int:
+    return int(os.environ.get("WORLD_SIZE", "1"))
+
+
+def integrator_cpu_baseline(kind, keep):
+    """The FP64 CPU integrators (oracle) on all host cores over a crop of the
+    same frame: config 1 at full size (all 512 x 512 pixels, 16 AO rays),
+    configs 2 and 3 on the centre 128 x 128 tile at the configs' spp."""
+    import oracle
+    c, scene, bvh = keep["config"], keep["scene"], keep["bvh"]
+    W, H = c["width"], c["height"]
+    cores = os.cpu_count() or 1
+    bufs = bvh.buffers_view()
+    if kind == "ao":
+        ii, jj = np.meshgrid(np.arange(W), np.arange(H))
+        xy = np.stack([ii.ravel() + 0.5, jj.ravel() + 0.5], 1).astype(np.float32)
+        rays = oracle.ref_camera_rays(keep["eye"], keep["lookat"], c["up"], W, H, c["fov"], xy) \
+            if oracle.have_ref() else None
+        if rays is None:
+            return {"unavailable": "reference camera library not built"}
+        t0 = time.perf_counter()
+        oracle.ao(bufs, scene.vertices, scene.indices, rays, c["ao_samples"], c["ao_radius"], seed=c["ao_seed"])
+        dt = time.perf_counter() - t0
+        samples = xy.shape[0] * c["ao_samples"]
+        crop = f"full frame {W}x{H}, {c['ao_samples']} AO rays per pixel"
+    else:
+        T = 128
+        x0, y0 = (W - T) // 2, (H - T) // 2
+        spp = c["spp"]
+        ii, jj = np.meshgrid(np.arange(x0, x0 + T), np.arange(y0, y0 + T))
+        rng = np.random.Generator(np.random.PCG64(5))
+        base = np.stack([ii.ravel(), jj.ravel()], 1)
+        if not oracle.have_ref():
+            return {"unavailable": "reference camera library not built"}
+        lights = np.asarray(scene.light_ids_to_primitive_ids, np.uint32)
+        if kind == "pt":
+            xy = (np.repeat(base, spp, axis=0) + rng.uniform(0, 1, (base.shape[0] * spp, 2))).astype(np.float32)
+            rays = oracle.ref_camera_rays(keep["eye"], keep["lookat"], c["up"], W, H, c["fov"], xy)
+            t0 = time.perf_counter()
+            oracle.pt(bufs, scene.vertices, scene.indices, scene.material_ids, scene.albedo, scene.emission, lights,
+                      rays, c["max_depth"], c["rr_start"], c["rr_prob"], seed=3)
+            dt = time.perf_counter() - t0
+        else:
+            xy = (np.tile(base, (spp, 1)) + rng.uniform(0, 1, (base.shape[0] * spp, 2))).astype(np.float32)
+            rays = oracle.ref_camera_rays(keep["eye"], keep["lookat"], c["up"], W, H, c["fov"], xy)
+            t0 = time.perf_counter()
+            oracle.bdpt(bufs, scene.vertices, scene.indices, scene.material_ids, scene.albedo, scene.emission, lights,
+                        rays, base.shape[0], spp, base.shape[0], c["max_path_length"], c["lvc_connections"], 3, 0.95,
+                        seed=3)
+            dt = time.perf_counter() - t0
+        samples = base.shape[0] * spp
+        crop = f"centre {T}x{T} tile of the {W}x{H} frame at {spp} spp"
+    return {"value": round(samples / dt, 1), "unit": "samples/s", "cores": cores, "kind": "port",
+            "sample": f"{crop}: {samples:,} samples in {dt:.1f}s, FP64 CPU integrator (oracle), "
+                      f"OpenMP over {cores} threads"}
 
 
 def cpu_baseline_run(scenes, budget_s: float):
@@ -388,6 +454,38 @@ def cpu_baseline_run(scenes, budget_s: float):
     return {"value": round(n / dt / 1e6, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
             "sample": f"{per} closest-hit + {per} any-hit rays from each of {len(scenes)} scenes "
                       f"({n:,} rays, {dt:.1f}s), oracle C restatement, OpenMP over {cores} threads"}
+
+
+def build_baseline(scenes, budget_tris: int = 30_000):
+    """SBVH build time: the reference's own host builder (compiled from its
+    sources, single-threaded as written) against this library's builder on
+    the same smallest config-4 scenes (about budget_tris triangles in all),
+    with one thread and with all threads."""
+    import oracle
+
+    import renderbox2_b200 as rb
+    if not oracle.have_ref():
+        return {"unavailable": "reference builder library not built"}
+    pick, tot = [], 0
+    for s in sorted(scenes, key=lambda s: s["tris"]):
+        if tot + s["tris"] > budget_tris and pick:
+            break
+        pick.append(s)
+        tot += s["tris"]
+    t0 = time.perf_counter()
+    for s in pick:
+        oracle.ref_build(s["scene"].vertices, s["scene"].indices)
+    ref_s = time.perf_counter() - t0
+    out = {"scenes": len(pick), "triangles": tot, "reference_s": round(ref_s, 3)}
+    for threads, key in ((1, "rb2_1thread_s"), (0, "rb2_all_threads_s")):
+        t0 = time.perf_counter()
+        for s in pick:
+            rb.BVH(s["scene"], params=rb.BuildParams(num_threads=threads))
+        out[key] = round(time.perf_counter() - t0, 3)
+    out["speedup_1thread"] = round(ref_s / max(out["rb2_1thread_s"], 1e-9), 1)
+    out["speedup_all_threads"] = round(ref_s / max(out["rb2_all_threads_s"], 1e-9), 1)
+    out["cores"] = os.cpu_count() or 1
+    return out
 
 
 def trace_sample(oracle, scenes, per):

@@ -44,22 +44,16 @@ struct Lane {
     uint64_t ray;       // source-defined index of the ray within its job
 };
 
-// One 32-byte read-only load (sm_100 256-bit ld.global.nc.v8).  `p` must be
-// 32-byte aligned.
-__device__ __forceinline__ void ldg_v8(const float4* p, float4& a, float4& b)
-{
-    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
-        : "l"(p));
-}
-
-// A 64-byte Compact2 node as two 256-bit loads: half the L1 tag lookups and
-// requests of four 128-bit loads.  Nodes are 64-byte aligned (child offsets
-// are multiples of 4 float4 into a 256-byte-aligned allocation).
+// A 64-byte Compact2 node as four 128-bit read-only loads.  (Two 256-bit
+// ld.global.nc.v8 loads halve the L1 sector lookups but measured 1-2 %
+// slower at the tuned register budget: the kernel is bound by L2 latency
+// with 40 resident warps per SM, not by L1 throughput.)
 __device__ __forceinline__ void load_node(const float4* np, float4& n0xy, float4& n1xy, float4& nz, float4& cn)
 {
-    ldg_v8(np, n0xy, n1xy);
-    ldg_v8(np + 2, nz, cn);
+    n0xy = __ldg(np + 0);
+    n1xy = __ldg(np + 1);
+    nz = __ldg(np + 2);
+    cn = __ldg(np + 3);
 }
 
 __device__ __forceinline__ float fmin_s(float a, float b) { return a < b ? a : b; }

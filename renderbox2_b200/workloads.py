@@ -22,8 +22,9 @@ def _event_ms(fn, stream, reps=1):
     return e0.elapsed_time(e1) / reps
 
 
-def integrator(kind: str, warmup: int = 1):
-    """Config 1 (AO), 2 (PT) or 3 (BDPT) at full size: samples/s and Mrays/s."""
+def integrator(kind: str, warmup: int = 1, keep: dict | None = None):
+    """Config 1 (AO), 2 (PT) or 3 (BDPT) at full size: samples/s and Mrays/s.
+    `keep` (optional dict) receives the scene, BVH and config used."""
     import torch
 
     import renderbox2_b200 as rb
@@ -72,6 +73,8 @@ def integrator(kind: str, warmup: int = 1):
         torch.cuda.synchronize()
         ms = _event_ms(run, stream)
     st = it.stats(stream)
+    if keep is not None:
+        keep.update(scene=scene, bvh=bvh, config=c, eye=eye, lookat=look)
     rays = (npix if kind == "ao" else 0) + sum(st[k] for k in ("primary_rays", "extension_rays", "shadow_rays",
                                                               "connection_rays", "light_rays"))
     if kind == "ao":
