@@ -46,10 +46,8 @@ struct IsectSource {
         }
         L.nodes = nodes;
         L.woop = woop;
-        L.triidx = triidx;
-        L.mode = mode;
-        L.job = 0;
-        L.ray = slot;
+        L.set_tag(mode, 0);
+        L.ray = (uint32_t)slot;
         setup_ray(L, __ldg(rays + 2 * slot), __ldg(rays + 2 * slot + 1));
         return 1;
     }
@@ -63,8 +61,9 @@ struct IsectSource {
         rb2_hit h;
         h.prim = (int32_t)__ldg(triidx + L.hitIndex);
         h.t = L.hitT;
-        h.u = L.hu;
-        h.v = L.hv;
+        const float2 uv = hit_uv(L);
+        h.u = uv.x;
+        h.v = uv.y;
         rb2::Intersection is;
         rb2::fill_intersection(make_float4(L.ox, L.oy, L.oz, L.tmin), make_float4(L.dx, L.dy, L.dz, 0.0f), h, scene,
                                &is);

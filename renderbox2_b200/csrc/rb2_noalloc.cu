@@ -109,6 +109,8 @@ extern "C" int rb2_trace_batch_noalloc(const rb2_noalloc_job* jobs, uint32_t n_j
         if (j.n && (!j.d_nodes || !j.d_woop || !j.d_triidx || !j.d_rays || !j.d_out))
             return rb2::fail(RB2_EINVAL, "rb2_trace_batch_noalloc: job " + std::to_string(i) + " has a null buffer");
         if (j.mode > RB2_MODE_OCCLUSION) return rb2::fail(RB2_EINVAL, "rb2_trace_batch_noalloc: unknown job mode");
+        if (j.n > rb2dev::kMaxJobRays)
+            return rb2::fail(RB2_EINVAL, "rb2_trace_batch_noalloc: a job holds at most 2^32 - 1 rays");
         if (((uintptr_t)j.d_nodes | (uintptr_t)j.d_woop | (uintptr_t)j.d_rays) & 15u)
             return rb2::fail(RB2_EINVAL, "rb2_trace_batch_noalloc: nodes, Woop rows and rays must be 16-byte aligned");
         if (j.mode != RB2_MODE_OCCLUSION && ((uintptr_t)j.d_out & 15u))

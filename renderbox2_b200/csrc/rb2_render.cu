@@ -96,9 +96,7 @@ struct AoSource {
         const float3 dir = to_world(fr, cosine_hemisphere(rng_u01(seed, slot, 0), rng_u01(seed, slot, 1)));
         L.nodes = nodes;
         L.woop = woop;
-        L.triidx = triidx;
-        L.mode = kOcclusion;
-        L.job = 0;
+        L.set_tag(kOcclusion, 0);
         L.ray = pix;
         setup_ray(L, make_float4(pos.x, pos.y, pos.z, 1.0e-3f * t), make_float4(dir.x, dir.y, dir.z, radius));
         return 1;
@@ -168,9 +166,7 @@ struct QueueSource {
         const uint32_t path = __ldg(queue + slot);
         L_.nodes = nodes;
         L_.woop = woop;
-        L_.triidx = triidx;
-        L_.mode = mode;
-        L_.job = 0;
+        L_.set_tag(mode, 0);
         L_.ray = path;
         setup_ray(L_, rays[2 * (size_t)path], rays[2 * (size_t)path + 1]);
         return 1;
@@ -179,7 +175,7 @@ struct QueueSource {
     __device__ __forceinline__ void finish(const Lane& L_) const
     {
         if (mode == kClosest) {
-            hits[L_.ray] = hit_record(L_);
+            hits[L_.ray] = hit_record(L_, triidx);
         } else if (L == nullptr) {
             if (L_.hitIndex >= 0) contrib[L_.ray] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         } else if (L_.hitIndex < 0) {

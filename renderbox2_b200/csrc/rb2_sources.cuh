@@ -85,9 +85,8 @@ struct JobSource {
         const uint32_t j = find_job(slot);
         const JobDesc& d = jobs[j];
         const uint64_t r = slot - start[j];
-        L.job = j;
-        L.ray = r;
-        L.mode = d.mode;
+        L.set_tag(d.mode, j);
+        L.ray = (uint32_t)r;
         if (d.mask != nullptr && d.mask[r] == 0) {
             const float4 d4 = __ldg(d.rays + 2 * r + 1);
             if (d.mode == kOcclusion) static_cast<uint8_t*>(d.out)[r] = 0;
@@ -96,16 +95,15 @@ struct JobSource {
         }
         L.nodes = d.nodes;
         L.woop = d.woop;
-        L.triidx = d.triidx;
         setup_ray(L, __ldg(d.rays + 2 * r), __ldg(d.rays + 2 * r + 1));
         return 1;
     }
 
     __device__ __forceinline__ void finish(const Lane& L) const
     {
-        const JobDesc& d = jobs[L.job];
-        if (L.mode == kOcclusion) static_cast<uint8_t*>(d.out)[L.ray] = L.hitIndex >= 0 ? 1 : 0;
-        else static_cast<int4*>(d.out)[L.ray] = hit_record(L);
+        const JobDesc& d = jobs[L.job()];
+        if (L.mode() == kOcclusion) static_cast<uint8_t*>(d.out)[L.ray] = L.hitIndex >= 0 ? 1 : 0;
+        else static_cast<int4*>(d.out)[L.ray] = hit_record(L, d.triidx);
     }
 };
 

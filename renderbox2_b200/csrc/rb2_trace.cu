@@ -438,6 +438,7 @@ extern "C" {
 int rb2_batch_create(const rb2_trace_job* jobs, uint32_t n_jobs, rb2_batch** out)
 {
     if (!out || (n_jobs && !jobs)) return fail(RB2_EINVAL, "null argument");
+    if (n_jobs > rb2dev::kJobMask + 1u) return fail(RB2_EINVAL, "at most 2^30 jobs per batch");
     *out = nullptr;
     std::unique_ptr<rb2_batch> b(new rb2_batch());
     std::vector<rb2dev::JobDesc> descs(n_jobs);
@@ -446,6 +447,7 @@ int rb2_batch_create(const rb2_trace_job* jobs, uint32_t n_jobs, rb2_batch** out
         const rb2_trace_job& j = jobs[i];
         if (!j.tracer || (j.n && (!j.d_rays || !j.d_out))) return fail(RB2_EINVAL, "job with null tracer or buffer");
         if (j.mode > RB2_MODE_OCCLUSION) return fail(RB2_EINVAL, "unknown job mode");
+        if (j.n > rb2dev::kMaxJobRays) return fail(RB2_EINVAL, "a job holds at most 2^32 - 1 rays");
         if ((uintptr_t)j.d_rays & 15u) return fail(RB2_EINVAL, "job rays must be 16-byte aligned");
         if (j.mode != RB2_MODE_OCCLUSION && ((uintptr_t)j.d_out & 15u)) return fail(RB2_EINVAL, "job hits must be 16-byte aligned");
         descs[i] = job_of(j.tracer, j.d_rays, j.n, j.mode, j.d_mask, j.d_out);

@@ -29,19 +29,30 @@ constexpr uint32_t kStatusStack = 1u;
 
 enum Mode : uint32_t { kClosest = 0, kAny = 1, kOcclusion = 2 };
 
+constexpr uint32_t kJobMask = 0x3FFFFFFFu;          // job index bits of Lane::tag
+constexpr uint64_t kMaxJobRays = 0xFFFFFFFFull;     // rays per job (Lane::ray is 32-bit)
+
+// Per-lane traversal state.  Kept small on purpose: every register here is
+// live across the whole loop, and the kernel is latency-bound, so fewer
+// registers mean more resident warps (48 registers: 40 warps per SM).  The
+// triangle-index buffer is not carried (sources pass it to hit_record), u, v
+// are recomputed once at the end from the accepted triangle (hit_uv), and the
+// mode shares a word with the job index.
 struct Lane {
     // BVH of the ray's scene
     const float4* nodes;
     const float4* woop;
-    const uint32_t* triidx;
     // ray
     float ox, oy, oz, dx, dy, dz, idx, idy, idz, oodx, oody, oodz, tmin;
     // state
-    float hitT, hu, hv;
+    float hitT;
     int nodeAddr, leafAddr, hitIndex;
-    uint32_t mode;      // Mode
-    uint32_t job;       // source-defined tag (job index)
-    uint64_t ray;       // source-defined index of the ray within its job
+    uint32_t tag;       // Mode << 30 | source-defined job index
+    uint32_t ray;       // source-defined index of the ray within its job
+
+    __device__ __forceinline__ uint32_t mode() const { return tag >> 30; }
+    __device__ __forceinline__ uint32_t job() const { return tag & kJobMask; }
+    __device__ __forceinline__ void set_tag(uint32_t mode, uint32_t job) { tag = (mode << 30) | (job & kJobMask); }
 };
 
 // A 64-byte Compact2 node as four 128-bit read-only loads.  (Two 256-bit
@@ -86,7 +97,6 @@ __device__ __forceinline__ void setup_ray(Lane& L, float4 o4, float4 d4)
     L.leafAddr = 0;
     L.nodeAddr = 0;
     L.hitIndex = -1;
-    L.hu = L.hv = 0.0f;
 }
 
 template <class Source>
@@ -210,10 +220,8 @@ __device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_thr
                                 const float v = __fmaf_rn(t, Dy, Oy);
                                 if (v >= 0.0f && __fadd_rn(u, v) <= 1.0f) {
                                     L.hitT = t;
-                                    L.hu = u;
-                                    L.hv = v;
                                     L.hitIndex = triAddr;
-                                    if (L.mode != kClosest) {
+                                    if (L.mode() != kClosest) {
                                         L.nodeAddr = kSentinel;
                                         break;
                                     }
@@ -235,12 +243,26 @@ __device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_thr
     }
 }
 
-// Result record shared by all sources: prim (original triangle id, -1 miss), t, u, v.
-__device__ __forceinline__ int4 hit_record(const Lane& L)
+// u, v of the accepted triangle, recomputed with the leaf loop's exact
+// operations at t = hitT (the accepted t), so the bits equal those of the
+// test that accepted it.  Valid only when hitIndex >= 0.
+__device__ __forceinline__ float2 hit_uv(const Lane& L)
 {
-    const bool hit = L.hitIndex >= 0;
-    const int prim = hit ? (int)__ldg(L.triidx + L.hitIndex) : -1;
-    return make_int4(prim, __float_as_int(L.hitT), __float_as_int(hit ? L.hu : 0.0f), __float_as_int(hit ? L.hv : 0.0f));
+    const float4 v11 = __ldg(L.woop + L.hitIndex + 1), v22 = __ldg(L.woop + L.hitIndex + 2);
+    const float Ox = __fmaf_rn(L.oz, v11.z, __fmaf_rn(L.oy, v11.y, __fmaf_rn(L.ox, v11.x, v11.w)));
+    const float Dx = __fmaf_rn(L.dz, v11.z, __fmaf_rn(L.dy, v11.y, __fmul_rn(L.dx, v11.x)));
+    const float Oy = __fmaf_rn(L.oz, v22.z, __fmaf_rn(L.oy, v22.y, __fmaf_rn(L.ox, v22.x, v22.w)));
+    const float Dy = __fmaf_rn(L.dz, v22.z, __fmaf_rn(L.dy, v22.y, __fmul_rn(L.dx, v22.x)));
+    return make_float2(__fmaf_rn(L.hitT, Dx, Ox), __fmaf_rn(L.hitT, Dy, Oy));
+}
+
+// Result record shared by all sources: prim (original triangle id, -1 miss), t, u, v.
+__device__ __forceinline__ int4 hit_record(const Lane& L, const uint32_t* triidx)
+{
+    if (L.hitIndex < 0) return make_int4(-1, __float_as_int(L.hitT), 0, 0);
+    const float2 uv = hit_uv(L);
+    return make_int4((int)__ldg(triidx + L.hitIndex), __float_as_int(L.hitT), __float_as_int(uv.x),
+                     __float_as_int(uv.y));
 }
 
 }  // namespace rb2dev
