@@ -87,6 +87,38 @@ typedef struct {
 int rb2_trace_isect(rb2_tracer* t, const rb2_scene_dev* scene, const float* d_rays, uint32_t n, int any_hit,
                     const uint8_t* d_mask, const rb2_isect_buffer* out, void* stream);
 
+/* ------------------------------------------------------------------- film --
+ * Reconstruction filters of the reference's film (core/filter.h:46-132,
+ * core/film.cpp:36-60, renderers/samplerrenderer.cu:103-168): a sample at
+ * raster position (sx, sy) with radiance L adds w * L and w to every pixel
+ * (x, y) with |x - (sx - 0.5)| <= xwidth and |y - (sy - 0.5)| <= ywidth, w
+ * read from a 16 x 16 table of the filter evaluated at cell centres; a pixel's
+ * value is max(0, sum(w L) / sum(w)).  Differences: the table is indexed by
+ * x and y (the reference evaluated fx from the row index, core/film.cpp:56),
+ * and each pixel gathers its samples in a fixed order instead of receiving
+ * atomic adds, so images are deterministic.  RB2_FILTER_NONE is the
+ * integrators' default: the mean of the pixel's own samples. */
+enum { RB2_FILTER_NONE = 0, RB2_FILTER_BOX = 1, RB2_FILTER_TRIANGLE = 2, RB2_FILTER_GAUSSIAN = 3 };
+typedef struct {
+    uint32_t kind;          /* RB2_FILTER_* */
+    float xwidth, ywidth;   /* half-widths in pixels, (0, 16] */
+    float alpha;            /* Gaussian falloff (FilterGaussian's alpha) */
+} rb2_filter;
+
+/* Filter table exactly as the film precomputes it (16 x 16 floats, row y). */
+int rb2_filter_table(const rb2_filter* f, float* table256);
+
+/* Reconstructs an image from `spp` samples per pixel held sample-major
+ * (sample j of pixel p at j * width * height + p): d_xy = raster positions
+ * (2 floats; a sample of pixel p must lie in [px, px + 1) x [py, py + 1)),
+ * d_L = radiance (4 floats, rgb + unused).  d_rgb: 3 floats per pixel. */
+int rb2_film_develop(const rb2_filter* f, uint32_t width, uint32_t height, uint32_t spp, const float* d_xy,
+                     const float* d_L, float* d_rgb, void* stream);
+
+/* Portable float map (PFM, little-endian, bottom row first as the format
+ * defines; rows of h_rgb are top first): the film's image file output. */
+int rb2_image_write_pfm(const char* path, const float* h_rgb, uint32_t width, uint32_t height);
+
 /* An integrator binds a tracer (BVH) and a device scene and owns the
  * wavefront scratch (grown on demand, reused across renders).  Replaces
  * Integrator::render(Scene*, CudaTracer*, void**, uint32_t) (core/integrator.h:59). */
@@ -94,6 +126,8 @@ typedef struct rb2_integrator rb2_integrator;
 int rb2_integrator_create(rb2_tracer* tracer, const rb2_scene_dev* scene, rb2_integrator** out);
 int rb2_integrator_destroy(rb2_integrator* it);
 int rb2_integrator_device_bytes(const rb2_integrator* it, uint64_t* bytes);
+/* Film filter of the path tracer and BDPT (default RB2_FILTER_NONE); NULL resets. */
+int rb2_integrator_set_filter(rb2_integrator* it, const rb2_filter* f);
 
 /* Ambient occlusion (AmbientOcclusionIntegratorParams, core/params.h:126-131;
  * integrators/integrator_ao.cu:42-110): one primary ray per pixel centre,

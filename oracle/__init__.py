@@ -8,6 +8,8 @@ CPU-baseline leg of bench.py -- never by the product library:
   from the reference sources into oracle/_ref/librb2ref.so (oracle/Makefile).
 * ``trace`` / ``woop_test`` / ``bruteforce``: the CPU restatement of the
   reference's traversal (oracle/rb2_oracle.c).
+* ``isect``: the intersection record of a hit (same file).
+* ``filter_table`` / ``film``: the film's filtered reconstruction (same file).
 * ``ao`` / ``pt`` / ``bdpt``: FP64 CPU restatements of the integrators
   (same file), scalar per pixel, used as statistical references.
 
@@ -190,6 +192,33 @@ def isect(verts, tris4, rays, hits):
     L.rb2o_isect.argtypes = [C.c_void_p] * 4 + [C.c_uint32, C.POINTER(_IsectSoa)]
     L.rb2o_isect.restype = None
     L.rb2o_isect(_p(verts), _p(tris4), _p(rays), _p(hits), n, C.byref(soa))
+    return out
+
+
+FILTER_KINDS = {"none": 0, "box": 1, "triangle": 2, "gaussian": 3}
+
+
+def filter_table(kind: str, xwidth: float, ywidth: float, alpha: float = 0.0) -> np.ndarray:
+    """The film's 16 x 16 filter table (rb2o_filter_table)."""
+    L = orc_lib()
+    L.rb2o_filter_table.argtypes = [C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_void_p]
+    L.rb2o_filter_table.restype = None
+    t = np.zeros(256, np.float32)
+    L.rb2o_filter_table(FILTER_KINDS[kind], xwidth, ywidth, alpha, _p(t))
+    return t.reshape(16, 16)
+
+
+def film(kind: str, xwidth: float, ywidth: float, alpha: float, width: int, height: int, spp: int, xy, L4):
+    """Filtered reconstruction (rb2o_film): xy (spp*w*h, 2), L4 (spp*w*h, 4)
+    sample-major; returns (h*w, 3) float32."""
+    Lb = orc_lib()
+    Lb.rb2o_film.argtypes = [C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_uint32,
+                             C.c_void_p, C.c_void_p, C.c_void_p]
+    Lb.rb2o_film.restype = None
+    xy = np.ascontiguousarray(xy, np.float32)
+    L4 = np.ascontiguousarray(L4, np.float32)
+    out = np.zeros((width * height, 3), np.float32)
+    Lb.rb2o_film(FILTER_KINDS[kind], xwidth, ywidth, alpha, width, height, spp, _p(xy), _p(L4), _p(out))
     return out
 
 

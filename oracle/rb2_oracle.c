@@ -239,6 +239,77 @@ void rb2o_isect(const float* verts, const uint32_t* tris4, const float* rays, co
     }
 }
 
+static float film_eval(uint32_t kind, float xw, float yw, float alpha, float x, float y)
+{
+    if (kind == 2) return fmaxf(0.0f, xw - fabsf(x)) * fmaxf(0.0f, yw - fabsf(y));
+    if (kind == 3) {
+        const float ex = expf(-alpha * xw * xw), ey = expf(-alpha * yw * yw);
+        return fmaxf(0.0f, expf(-alpha * x * x) - ex) * fmaxf(0.0f, expf(-alpha * y * y) - ey);
+    }
+    return 1.0f;
+}
+
+void rb2o_filter_table(uint32_t kind, float xw, float yw, float alpha, float* table256)
+{
+    for (int y = 0; y < 16; ++y) {
+        const float fy = ((float)y + 0.5f) * yw / 16.0f;
+        for (int x = 0; x < 16; ++x) {
+            const float fx = ((float)x + 0.5f) * xw / 16.0f;
+            table256[y * 16 + x] = film_eval(kind, xw, yw, alpha, fx, fy);
+        }
+    }
+}
+
+void rb2o_film(uint32_t kind, float xw, float yw, float alpha, uint32_t width, uint32_t height, uint32_t spp,
+               const float* xy, const float* L4, float* rgb)
+{
+    const size_t npix = (size_t)width * height;
+    if (kind == 0) {
+        const float inv = 1.0f / (float)spp;
+        for (size_t p = 0; p < npix; p++) {
+            float a[3] = {0.0f, 0.0f, 0.0f};
+            for (uint32_t j = 0; j < spp; j++)
+                for (int c = 0; c < 3; c++) a[c] = a[c] + L4[4 * ((size_t)j * npix + p) + c];
+            for (int c = 0; c < 3; c++) rgb[3 * p + c] = a[c] * inv;
+        }
+        return;
+    }
+    float table[256];
+    rb2o_filter_table(kind, xw, yw, alpha, table);
+    const float ixw = 1.0f / xw, iyw = 1.0f / yw;
+    /* Candidate source pixels: every pixel whose samples can reach (x, y). */
+    const int rx = (int)floorf(xw + 0.5f) + 1, ry = (int)floorf(yw + 0.5f) + 1;
+    for (int y = 0; y < (int)height; y++) {
+        for (int x = 0; x < (int)width; x++) {
+            float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            for (int qy = y - ry; qy <= y + ry; qy++) {
+                if (qy < 0 || qy >= (int)height) continue;
+                for (int qx = x - rx; qx <= x + rx; qx++) {
+                    if (qx < 0 || qx >= (int)width) continue;
+                    const size_t q = (size_t)qy * width + (size_t)qx;
+                    for (uint32_t j = 0; j < spp; j++) {
+                        const size_t k = (size_t)j * npix + q;
+                        const float dx = xy[2 * k] - 0.5f, dy = xy[2 * k + 1] - 0.5f;
+                        if (x < (int)ceilf(dx - xw) || x > (int)floorf(dx + xw) || y < (int)ceilf(dy - yw) ||
+                            y > (int)floorf(dy + yw))
+                            continue;
+                        const float fx = fabsf((((float)x - dx) * ixw) * 16.0f);
+                        const float fy = fabsf((((float)y - dy) * iyw) * 16.0f);
+                        int ix = (int)floorf(fx), iy = (int)floorf(fy);
+                        if (ix > 15) ix = 15;
+                        if (iy > 15) iy = 15;
+                        const float w = table[iy * 16 + ix];
+                        for (int c = 0; c < 3; c++) a[c] = a[c] + w * L4[4 * k + c];
+                        a[3] = a[3] + w;
+                    }
+                }
+            }
+            const float inv = a[3] != 0.0f ? 1.0f / a[3] : 0.0f;
+            for (int c = 0; c < 3; c++) rgb[3 * ((size_t)y * width + x) + c] = fmaxf(0.0f, a[c] * inv);
+        }
+    }
+}
+
 int rb2o_woop_test(const uint32_t* woop12, const float* ray8, float tmax, float* tuv)
 {
     ray_setup s;

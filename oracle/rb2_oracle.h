@@ -66,6 +66,24 @@ typedef struct {
 void rb2o_isect(const float* verts, const uint32_t* tris4, const float* rays, const rb2o_hit* hits, uint32_t n,
                 rb2o_isect_soa* out);
 
+/* Film reconstruction (renderers/samplerrenderer.cu:103-168, core/film.cpp:36-93,
+ * core/filter.h:46-132) with the table indexed by x and y, in IEEE single
+ * precision with no contraction:
+ *   table[y][x] = filter(((x + 0.5) * xw) / 16, ((y + 0.5) * yw) / 16)
+ *     box 1; triangle max(0, xw - |x|) max(0, yw - |y|);
+ *     Gaussian max(0, exp(-a x x) - exp(-a xw xw)) * (same in y)
+ *   sample s (raster position) reaches pixel (px, py) when
+ *     ceil(s.x - 0.5 - xw) <= px <= floor(s.x - 0.5 + xw) (and in y);
+ *   w = table[min(floor(|(py - (s.y - 0.5)) * (1/yw) * 16|), 15)]
+ *              [min(floor(|(px - (s.x - 0.5)) * (1/xw) * 16|), 15)]
+ *   pixel = max(0, sum(w L) * (1 / sum(w))), 0 when sum(w) = 0; the sums run
+ *   over neighbour rows, then columns, then samples, in increasing order.
+ * kind 0 = mean of the pixel's own samples (sum * (1/spp)).
+ * Samples are sample-major: sample j of pixel p at j * w * h + p. */
+void rb2o_filter_table(uint32_t kind, float xw, float yw, float alpha, float* table256);
+void rb2o_film(uint32_t kind, float xw, float yw, float alpha, uint32_t width, uint32_t height, uint32_t spp,
+               const float* xy, const float* L4, float* rgb);
+
 /* ---- shading references (FP64 accumulation) ---------------------------------
  * Scene for the integrator references: vertices (xyz), triangles (3 indices),
  * per-triangle material, per-material albedo/emission (rgb), emissive

@@ -63,6 +63,10 @@ class IsectBuffer(C.Structure):
                 ("intersected", C.c_void_p), ("epsilon", C.c_void_p)]
 
 
+class Filter(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("xwidth", C.c_float), ("ywidth", C.c_float), ("alpha", C.c_float)]
+
+
 class BatchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("fetch_threshold", C.c_uint32),
                 ("chunk", C.c_uint32), ("node_order", C.c_uint32), ("regs", C.c_uint32)]
@@ -128,6 +132,10 @@ SIGNATURES = {
     "rb2_trace_per_thread": (C.c_int, [P, P, U32, I32, P, P, P]),
     "rb2_scene_dev_view": (C.c_int, [P, C.POINTER(DevScene)]),
     "rb2_trace_isect": (C.c_int, [P, P, P, U32, I32, P, C.POINTER(IsectBuffer), P]),
+    "rb2_filter_table": (C.c_int, [C.POINTER(Filter), P]),
+    "rb2_film_develop": (C.c_int, [C.POINTER(Filter), U32, U32, U32, P, P, P, P]),
+    "rb2_image_write_pfm": (C.c_int, [C.c_char_p, P, U32, U32]),
+    "rb2_integrator_set_filter": (C.c_int, [P, C.POINTER(Filter)]),
     "rb2_pipeline_create": (C.c_int, [U64, U32, C.POINTER(P)]),
     "rb2_pipeline_destroy": (C.c_int, [P]),
     "rb2_trace_host_jobs": (C.c_int, [P, C.POINTER(HostJob), U32, P]),

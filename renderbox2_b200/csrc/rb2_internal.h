@@ -2,6 +2,7 @@
 #pragma once
 
 #include "rb2.h"
+#include "rb2_render.h"
 
 #include <cfloat>
 #include <cmath>
@@ -120,6 +121,9 @@ struct DeviceBvhView {
     unsigned int* status;
 };
 DeviceBvhView device_bvh(const rb2_tracer* t);
+
+// Checks a film filter description (rb2_film_table.cpp).
+int validate_filter(const rb2_filter* f);
 
 // A zeroed-before-use queue head of the tracer's ring (one per launch in flight).
 unsigned long long* tracer_queue_counter(rb2_tracer* t);

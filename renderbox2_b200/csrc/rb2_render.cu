@@ -9,6 +9,7 @@
 #include "rb2_internal.h"
 #include "rb2_render.h"
 #include "rb2_camera.cuh"
+#include "rb2_film.cuh"
 #include "rb2_shading.cuh"
 #include "rb2_traverse.cuh"
 
@@ -201,7 +202,8 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* count, bool pred)
 }
 
 __global__ void k_pt_camera(CamArgs cam, uint64_t seed, uint32_t npix, uint32_t paths, uint32_t sample0,
-                            float4* rays, float4* T, float4* L, uint32_t* q0, WaveCountersDev* wc)
+                            float4* rays, float4* T, float4* L, uint32_t* q0, WaveCountersDev* wc,
+                            float2* xy_out = nullptr)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) wc->n_ext[0] = paths;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < paths; p += gridDim.x * blockDim.x) {
@@ -209,7 +211,9 @@ __global__ void k_pt_camera(CamArgs cam, uint64_t seed, uint32_t npix, uint32_t 
         const uint64_t key = (uint64_t)(sample0 + p / npix) * npix + pix;
         const float jx = rng_u01(seed, key, 0), jy = rng_u01(seed, key, 1);
         float4 o, d;
-        camera_ray(cam.r2c, cam.c2w, (float)(pix % cam.width) + jx, (float)(pix / cam.width) + jy, o, d);
+        const float sx = (float)(pix % cam.width) + jx, sy = (float)(pix / cam.width) + jy;
+        camera_ray(cam.r2c, cam.c2w, sx, sy, o, d);
+        if (xy_out) xy_out[p] = make_float2(sx, sy);
         rays[2 * (size_t)p] = o;
         rays[2 * (size_t)p + 1] = d;
         T[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -913,7 +917,7 @@ int rb2_integrator_destroy(rb2_integrator* it)
 {
     if (!it) return RB2_OK;
     cudaFree(it->d_rays); cudaFree(it->d_hits); cudaFree(it->d_count); cudaFree(it->d_counters);
-    cudaFree(it->d_accum); cudaFree(it->d_wave);
+    cudaFree(it->d_accum); cudaFree(it->d_wave); cudaFree(it->d_film_xy);
     PathState& ps = it->ps;
     cudaFree(ps.T); cudaFree(ps.L); cudaFree(ps.ray); cudaFree(ps.hit); cudaFree(ps.sray); cudaFree(ps.sc);
     cudaFree(ps.q[0]); cudaFree(ps.q[1]); cudaFree(ps.qs);
@@ -989,6 +993,12 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
     int rc;
     if ((rc = ensure_path_state(ps, P))) return rc;
     if ((rc = grow(it->d_accum, it->cap_accum, npix))) return rc;
+    const bool filtered = it->filter.kind != RB2_FILTER_NONE;
+    rb2dev::FilmArgs fa{};
+    if (filtered) {
+        if ((rc = grow(it->d_film_xy, it->cap_film_xy, P))) return rc;
+        if ((rc = film_args(it->filter, cam->width, cam->height, fa))) return rc;
+    }
     if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
     RB2_CUDA(cudaMemsetAsync(it->d_accum, 0, npix * 16, s), "accumulator reset");
     RB2_CUDA(cudaMemsetAsync(it->d_wave, 0, sizeof(WaveCounters), s), "counter reset");
@@ -1005,7 +1015,8 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
     for (uint32_t s0 = 0; s0 < p->spp; s0 += spw) {
         const uint32_t cur_spw = std::min(spw, p->spp - s0);
         const uint32_t paths = (uint32_t)(npix * cur_spw);
-        rb2dev::k_pt_camera<<<g, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, paths, s0, ps.ray, ps.T, ps.L, ps.q[0], wc);
+        rb2dev::k_pt_camera<<<g, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, paths, s0, ps.ray, ps.T, ps.L, ps.q[0], wc,
+                                              filtered ? it->d_film_xy : nullptr);
         RB2_CUDA(cudaGetLastError(), "PT camera");
         uint32_t cur = 0;
         for (uint32_t b = 0; b <= p->max_depth; b++) {
@@ -1025,10 +1036,18 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
             if ((rc = launch_persistent(shadow, paths, it->sms, bv.status, s))) return rc;
             cur ^= 1u;
         }
-        rb2dev::k_pt_accumulate<<<grid_for(npix, it->sms), 256, 0, s>>>(ps.L, (uint32_t)npix, cur_spw, it->d_accum);
+        if (filtered)
+            rb2dev::k_film_gather<<<grid_for(npix, it->sms), 256, 0, s>>>(
+                fa, rb2dev::ArrayPos{it->d_film_xy, (uint32_t)npix}, ps.L, cur_spw, it->d_accum, nullptr);
+        else
+            rb2dev::k_pt_accumulate<<<grid_for(npix, it->sms), 256, 0, s>>>(ps.L, (uint32_t)npix, cur_spw, it->d_accum);
         RB2_CUDA(cudaGetLastError(), "PT accumulate");
     }
-    rb2dev::k_pt_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp, d_rgb);
+    if (filtered)
+        rb2dev::k_film_resolve<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_accum, (uint32_t)npix, d_rgb);
+    else
+        rb2dev::k_pt_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp,
+                                                                      d_rgb);
     RB2_CUDA(cudaGetLastError(), "PT finalize");
     return RB2_OK;
 }
@@ -1050,6 +1069,12 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     if ((rc = ensure_path_state(it->ps, npix))) return rc;
     if ((rc = ensure_bdpt_state(it->bd, NL, n_slots, npix * C))) return rc;
     if ((rc = grow(it->d_accum, it->cap_accum, npix))) return rc;
+    const bool filtered = it->filter.kind != RB2_FILTER_NONE;
+    rb2dev::FilmArgs fa{};
+    if (filtered) {
+        if ((rc = grow(it->d_film_xy, it->cap_film_xy, npix))) return rc;
+        if ((rc = film_args(it->filter, cam->width, cam->height, fa))) return rc;
+    }
     if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
     RB2_CUDA(cudaMemsetAsync(it->d_accum, 0, npix * 16, s), "accumulator reset");
     RB2_CUDA(cudaMemsetAsync(it->d_wave, 0, sizeof(WaveCounters), s), "counter reset");
@@ -1093,7 +1118,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
         RB2_CUDA(cudaGetLastError(), "cache compaction");
         // ---- camera pass.
         rb2dev::k_pt_camera<<<gc, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, (uint32_t)npix, iter, ps.ray, ps.T, ps.L,
-                                               ps.q[0], wc);
+                                               ps.q[0], wc, filtered ? it->d_film_xy : nullptr);
         RB2_CUDA(cudaGetLastError(), "BDPT camera");
         cur = 0;
         for (uint32_t i = 1; i <= K; i++) {
@@ -1117,10 +1142,17 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             RB2_CUDA(cudaGetLastError(), "BDPT connection reduce");
             cur ^= 1u;
         }
-        rb2dev::k_pt_accumulate<<<gc, 256, 0, s>>>(ps.L, (uint32_t)npix, 1u, it->d_accum);
+        if (filtered)
+            rb2dev::k_film_gather<<<gc, 256, 0, s>>>(fa, rb2dev::ArrayPos{it->d_film_xy, (uint32_t)npix}, ps.L, 1u,
+                                                     it->d_accum, nullptr);
+        else
+            rb2dev::k_pt_accumulate<<<gc, 256, 0, s>>>(ps.L, (uint32_t)npix, 1u, it->d_accum);
         RB2_CUDA(cudaGetLastError(), "BDPT accumulate");
     }
-    rb2dev::k_pt_finalize<<<gc, 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp, d_rgb);
+    if (filtered)
+        rb2dev::k_film_resolve<<<gc, 256, 0, s>>>(it->d_accum, (uint32_t)npix, d_rgb);
+    else
+        rb2dev::k_pt_finalize<<<gc, 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp, d_rgb);
     RB2_CUDA(cudaGetLastError(), "BDPT finalize");
     return RB2_OK;
 }

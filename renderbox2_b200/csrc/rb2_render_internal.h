@@ -80,18 +80,28 @@ struct rb2_integrator {
     uint32_t* d_count = nullptr; uint64_t cap_count = 0;
     unsigned long long* d_counters = nullptr;                // queue heads (16)
     float4* d_accum = nullptr; uint64_t cap_accum = 0;
+    float2* d_film_xy = nullptr; uint64_t cap_film_xy = 0;  // sample raster positions (filtered film)
+    rb2_filter filter{RB2_FILTER_NONE, 0.5f, 0.5f, 0.0f};
     PathState ps;
     BdptState bd;
     WaveCounters* d_wave = nullptr;
     uint64_t bytes() const
     {
-        return cap_rays * 32 + cap_hits * 16 + cap_count * 4 + 16 * 8 + cap_accum * 16 + ps.cap * (16 * 8 + 12) +
+        return cap_rays * 32 + cap_hits * 16 + cap_count * 4 + 16 * 8 + cap_accum * 16 + cap_film_xy * 8 +
+               ps.cap * (16 * 8 + 12) +
                sizeof(WaveCounters) + bd.cap_paths * (32 + 16 + 16 + 8) + bd.cap_slots * (6 * 16 + 1) +
                bd.cap_conn * (32 + 16 + 4);
     }
 };
 
+namespace rb2dev {
+struct FilmArgs;
+}
+
 namespace rb2 {
+// Kernel arguments of the film gather for a validated filter (rb2_film.cu).
+int film_args(const rb2_filter& f, uint32_t width, uint32_t height, rb2dev::FilmArgs& out);
+
 // Allocates (or grows) the wavefront path state / cache / connection buffers.
 int ensure_path_state(PathState& ps, uint64_t P);
 int ensure_bdpt_state(BdptState& bd, uint64_t n_paths, uint64_t n_slots, uint64_t n_conn);

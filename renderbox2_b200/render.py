@@ -11,6 +11,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from ._native import AoParams, BdptParams, DevScene, IsectBuffer, PtParams, RenderStats, check, lib
+from ._native import Filter as _Filter
 from .accel import CudaTracer, Scene, _ptr, _stream_handle
 
 
@@ -105,6 +106,48 @@ def trace_isect(tracer: CudaTracer, scene: DeviceScene, rays, any_hit: bool = Tr
     return out
 
 
+FILTER_KINDS = {"none": 0, "box": 1, "triangle": 2, "gaussian": 3}
+
+
+@dataclass
+class Filter:
+    """Film reconstruction filter (core/filter.h:46-132): FilterBox,
+    FilterTriangle, FilterGaussian(xwidth, ywidth, alpha); "none" = mean of
+    the pixel's own samples."""
+    kind: str = "none"
+    xwidth: float = 0.5
+    ywidth: float = 0.5
+    alpha: float = 2.0
+
+    def c_struct(self) -> _Filter:
+        return _Filter(FILTER_KINDS[self.kind], self.xwidth, self.ywidth, self.alpha)
+
+
+def filter_table(f: Filter) -> np.ndarray:
+    """The film's 16 x 16 precomputed filter table."""
+    t = np.zeros(256, np.float32)
+    c = f.c_struct()
+    check(lib().rb2_filter_table(C.byref(c), _ptr(t)))
+    return t.reshape(16, 16)
+
+
+def film_develop(f: Filter, width: int, height: int, spp: int, xy, L, out=None, stream=None):
+    """Filtered image from sample-major samples: xy (spp*w*h, 2) raster
+    positions, L (spp*w*h, 4) radiance, device tensors; returns (h*w, 3)."""
+    import torch
+    if out is None:
+        out = torch.empty((width * height, 3), dtype=torch.float32, device=L.device)
+    c = f.c_struct()
+    check(lib().rb2_film_develop(C.byref(c), width, height, spp, _ptr(xy), _ptr(L), _ptr(out), _stream_handle(stream)))
+    return out
+
+
+def write_pfm(path: str, rgb: np.ndarray, width: int, height: int) -> None:
+    """Writes an (h*w, 3) float image, top row first, as a PFM file."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    check(lib().rb2_image_write_pfm(str(path).encode(), _ptr(rgb), width, height))
+
+
 @dataclass
 class AmbientOcclusionIntegratorParams:
     samples: int = 16
@@ -140,6 +183,14 @@ class Integrator:
         self.tracer, self.scene = tracer, scene
         self._it = C.c_void_p()
         check(lib().rb2_integrator_create(tracer.handle, scene.handle, C.byref(self._it)))
+
+    def set_filter(self, f: "Filter | None"):
+        """Film filter of render_pt / render_bdpt (None: per-pixel mean)."""
+        if f is None:
+            check(lib().rb2_integrator_set_filter(self._it, None))
+        else:
+            c = f.c_struct()
+            check(lib().rb2_integrator_set_filter(self._it, C.byref(c)))
 
     def __del__(self):
         it = getattr(self, "_it", None)

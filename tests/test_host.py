@@ -266,3 +266,32 @@ def test_cpp_compat_classes_build_and_cache(rb, tmp_path):
     nodes, woop, _ = bvh.buffers_view()
     assert int(f["nodes"]) == nodes.shape[0] and int(f["woop"]) == woop.shape[0]
     assert int(f["hash"], 16) == _fnv(np.ascontiguousarray(nodes).tobytes())
+
+
+@pytest.mark.parametrize("kind,alpha", [("box", 0.0), ("triangle", 0.0), ("gaussian", 2.0), ("gaussian", 0.5)])
+def test_filter_table_equals_oracle(rb, orc, kind, alpha):
+    from renderbox2_b200.render import Filter, filter_table
+    for xw, yw in ((0.5, 0.5), (1.5, 2.0), (2.0, 2.0), (3.7, 1.0)):
+        got = filter_table(Filter(kind, xw, yw, alpha))
+        want = orc.filter_table(kind, xw, yw, alpha)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    if kind == "triangle":
+        t = filter_table(Filter(kind, 2.0, 1.0))
+        assert not np.allclose(t[0, :], t[0, 0])   # varies along x (the reference's table did not)
+
+
+def test_filter_validation_and_pfm(rb, tmp_path):
+    from renderbox2_b200.render import Filter, filter_table, write_pfm
+    for bad in (Filter("box", 0.0, 1.0), Filter("box", 1.0, 17.0), Filter("gaussian", 1.0, 1.0, 0.0)):
+        with pytest.raises(rb.Rb2Error):
+            filter_table(bad)
+    img = np.arange(5 * 3 * 3, dtype=np.float32).reshape(15, 3)
+    path = tmp_path / "a.pfm"
+    write_pfm(path, img, 5, 3)
+    raw = path.read_bytes()
+    head = b"PF\n5 3\n-1.0\n"
+    assert raw.startswith(head)
+    data = np.frombuffer(raw[len(head):], "<f4").reshape(3, 5, 3)
+    assert np.array_equal(data[::-1].reshape(15, 3), img)    # bottom row first
+    with pytest.raises(rb.Rb2Error):
+        write_pfm(tmp_path / "missing_dir" / "b.pfm", img, 5, 3)
