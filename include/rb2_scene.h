@@ -43,6 +43,48 @@ int rb2_gen_room(uint64_t seed, uint32_t n_boxes, uint32_t n_spheres, uint32_t s
 int rb2_gen_surface_rays(const float* v_xyz, uint32_t nv, const uint32_t* idx3, uint32_t ntri, uint64_t seed,
                          uint64_t n_rays, float offset_scale, float anyhit_fraction, float* rays, uint8_t* flags);
 
+/* ----------------------------------------------------------- scene files --
+ * Loads the reference's scene description: the XML schema of
+ * io/customfilereader.cpp:47-291 (<scene> with <files><count>1</count>
+ * <file>x.obj</file></files>, <material><name/><bsdf><layers/><bxdf><type/>
+ * <reflectance/>...</bxdf></bsdf></material>..., <object><name/><material/>
+ * </object>..., <lightobjects><light><name/><type/><Le/></light>...
+ * </lightobjects>, <camera><position/><lookat/><up/><fov/></camera>), or a
+ * bare Wavefront OBJ (io/objfilereader.cpp).  Mesh = OBJ object ("o name");
+ * indices are file-global, as the reference keeps them.  Materials keep the
+ * reference's numbering: XML materials in order, then one emitter material
+ * per light.  Triangle material = its object's material, the light's
+ * emitter material for light meshes, 0 for meshes the file does not name.
+ * Differences: a face of n > 3 vertices is fan-triangulated (the reference
+ * kept its first triangle), negative (relative) OBJ indices are accepted,
+ * '#' starts a comment anywhere on a line (the reference skipped any line
+ * containing '#'), geometry before the first "o" goes to a mesh named
+ * "default", and <fov> is read when present (the reference used 90).  The
+ * integrators shade every bxdf type as Lambertian with its reflectance;
+ * rb2_scene_file_bsdf_types reports the declared types. */
+enum {
+    RB2_BSDF_LAMBERTIAN = 0, RB2_BSDF_OREN_NAYAR = 1, RB2_BSDF_MIRROR = 2, RB2_BSDF_GLASS = 3,
+    RB2_BSDF_MICROFACET = 4, RB2_BSDF_EMITTER = 5
+};
+typedef struct rb2_scene_file rb2_scene_file;
+typedef struct {
+    uint32_t n_vertices, n_triangles, n_materials, n_lights, n_meshes;
+    int32_t has_camera;
+    float eye[3], lookat[3], up[3];
+    float fov_deg;
+} rb2_scene_file_info;
+int rb2_scene_file_load(const char* path, rb2_scene_file** out);  /* .xml or .obj */
+int rb2_scene_file_info_get(const rb2_scene_file* f, rb2_scene_file_info* out);
+const float* rb2_scene_file_vertices(const rb2_scene_file* f);        /* 3 floats per vertex */
+const uint32_t* rb2_scene_file_indices(const rb2_scene_file* f);      /* 3 per triangle */
+const uint32_t* rb2_scene_file_tri_material(const rb2_scene_file* f); /* 1 per triangle */
+const float* rb2_scene_file_albedo(const rb2_scene_file* f);          /* 3 per material */
+const float* rb2_scene_file_emission(const rb2_scene_file* f);        /* 3 per material */
+const uint32_t* rb2_scene_file_bsdf_types(const rb2_scene_file* f);   /* RB2_BSDF_* per material */
+/* Mesh i: name and its triangle range [first, first + count). */
+int rb2_scene_file_mesh(const rb2_scene_file* f, uint32_t i, const char** name, uint32_t* first, uint32_t* count);
+void rb2_scene_file_free(rb2_scene_file* f);
+
 /* PCG32 stream (O'Neill 2014): 32-bit outputs, for tests of seeding. */
 int rb2_pcg32_fill(uint64_t seed, uint64_t stream, uint32_t n, uint32_t* out);
 

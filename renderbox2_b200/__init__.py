@@ -5,10 +5,11 @@ this package is a thin ctypes layer over its C ABI (include/rb2*.h)."""
 from ._native import Rb2Error, lib
 from .accel import (BVH, MODE_ANY, MODE_CLOSEST, MODE_OCCLUSION, BuildParams, CudaBvh, CudaTracer, HostPipeline,
                     Platform, Scene, TraceBatch, hits_view)
+from .scenefile import SceneFile, load_scene_file
 from .scenes import PerspectiveCamera, RoomScene, heightfield_for_triangles, heightfield_scene, pcg32, surface_rays
 
 __all__ = [
     "Rb2Error", "lib", "BVH", "BuildParams", "CudaBvh", "CudaTracer", "Platform", "Scene", "hits_view", "TraceBatch",
     "HostPipeline", "MODE_CLOSEST", "MODE_ANY", "MODE_OCCLUSION",
-    "PerspectiveCamera", "RoomScene", "heightfield_for_triangles", "heightfield_scene", "pcg32", "surface_rays",
+    "SceneFile", "load_scene_file", "PerspectiveCamera", "RoomScene", "heightfield_for_triangles", "heightfield_scene", "pcg32", "surface_rays",
 ]
