@@ -36,8 +36,8 @@ def test_xml_materials_lights_camera(rb):
     assert mat_of["left"] == {1} and mat_of["right"] == {2} and mat_of["lamp"] == {3}
     assert mat_of["front"] == {0}          # not named by the file: material 0
     assert s.num_lights == 2 and set(s.light_ids_to_primitive_ids.tolist()) == {22, 23}
-    assert sf.camera == {"eye": [0.5, 0.5, np.float32(-0.9)], "lookat": [0.5, 0.5, 0.5], "up": [0.0, 1.0, 0.0],
-                         "fov": 50.0}
+    assert sf.camera == {"eye": [-0.5, 0.5, np.float32(0.02)], "lookat": [-0.5, 0.5, 0.5], "up": [0.0, 1.0, 0.0],
+                         "fov": 70.0}
     # the loaded scene builds
     bvh = rb.BVH(s)
     assert bvh.counts().n_tris == 24
