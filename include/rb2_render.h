@@ -61,6 +61,49 @@ typedef struct {
 } rb2_dev_scene;
 int rb2_scene_dev_view(const rb2_scene_dev* s, rb2_dev_scene* out);
 
+/* ------------------------------------------------------------- materials --
+ * The reference's layered materials (core/material.h:44-51, at most 4
+ * layers) over its BSDFs (core/reflection.cu): Lambertian, Oren-Nayar
+ * (sigma in degrees, clamped to [0, 90]), specular mirror, specular
+ * transmission ("glass": the reference's glass transmits only), and the
+ * Torrance-Sparrow microfacet BSDF with a Blinn distribution and a
+ * dielectric, conductor or no-op Fresnel term.  Scenes made by
+ * rb2_scene_create use one Lambertian layer per material (albedo);
+ * rb2_scene_set_materials replaces the layers of every material (emission is
+ * kept; an emitter's layers are ignored).  Sampling follows
+ * material_sample_f (core/material.cu:56-211) except that the combined pdf
+ * of a multi-layer material is divided by the number of layers as in
+ * pbrt-v2 (the reference left it undivided) and a glass layer adds no
+ * microfacet term (a missing `break`, material.cu:204-209, Q11). */
+enum {
+    RB2_BSDF_LAMBERTIAN = 0, RB2_BSDF_OREN_NAYAR = 1, RB2_BSDF_MIRROR = 2, RB2_BSDF_GLASS = 3,
+    RB2_BSDF_MICROFACET = 4, RB2_BSDF_EMITTER = 5
+};
+enum { RB2_FRESNEL_DIELECTRIC = 0, RB2_FRESNEL_CONDUCTOR = 1, RB2_FRESNEL_NOOP = 2 };
+typedef struct {
+    uint32_t type;          /* RB2_BSDF_LAMBERTIAN .. RB2_BSDF_MICROFACET */
+    uint32_t fresnel;       /* microfacet: RB2_FRESNEL_* */
+    float color[3];         /* reflectance (R of the microfacet BSDF) */
+    float sigma_deg;        /* Oren-Nayar */
+    float etai, etat;       /* glass; microfacet with a dielectric Fresnel */
+    float exponent;         /* Blinn exponent */
+    float eta[3], k[3];     /* microfacet with a conductor Fresnel */
+} rb2_bsdf_layer;
+typedef struct {
+    uint32_t n_layers;      /* 1..4 (0 only for emitters) */
+    uint32_t reserved;
+    rb2_bsdf_layer layer[4];
+} rb2_material_desc;
+int rb2_scene_set_materials(rb2_scene_dev* s, const rb2_material_desc* materials, uint32_t n_materials);
+
+/* Device evaluation of materials, for tests and tools: for query i with
+ * material d_mat[i] and 9 floats d_q[9i..] = (n, wo, wi) in world space,
+ * d_out[4i..] = (f rgb, pdf) of material_f / material_pdf with specular
+ * layers excluded; with `sample` != 0, d_q holds (n, wo, u1, u2, uc) and
+ * d_out[8i..] = (wi xyz, f rgb, pdf, 1 if a specular layer was sampled). */
+int rb2_material_query(const rb2_scene_dev* s, int sample, const uint32_t* d_mat, const float* d_q, uint32_t n,
+                       float* d_out, void* stream);
+
 /* ------------------------------------------------------ intersection records --
  * Replaces CudaTracer::trace(const RayBuffer&, IntersectionBuffer&,
  * SceneBuffer&, uint8_t* stencil, bool any_hit) (cudatracer.h:87) with the

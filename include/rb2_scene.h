@@ -11,6 +11,8 @@
 
 #include <stdint.h>
 
+#include "rb2_render.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -59,13 +61,10 @@ int rb2_gen_surface_rays(const float* v_xyz, uint32_t nv, const uint32_t* idx3, 
  * kept its first triangle), negative (relative) OBJ indices are accepted,
  * '#' starts a comment anywhere on a line (the reference skipped any line
  * containing '#'), geometry before the first "o" goes to a mesh named
- * "default", and <fov> is read when present (the reference used 90).  The
- * integrators shade every bxdf type as Lambertian with its reflectance;
- * rb2_scene_file_bsdf_types reports the declared types. */
-enum {
-    RB2_BSDF_LAMBERTIAN = 0, RB2_BSDF_OREN_NAYAR = 1, RB2_BSDF_MIRROR = 2, RB2_BSDF_GLASS = 3,
-    RB2_BSDF_MICROFACET = 4, RB2_BSDF_EMITTER = 5
-};
+ * "default", and <fov> is read when present (the reference used 90).  Every
+ * material's layers (up to 4 bxdf entries, MAX_LAYERS in core/material.h)
+ * are returned as rb2_material_desc for rb2_scene_set_materials; emitter
+ * materials have no layers. */
 typedef struct rb2_scene_file rb2_scene_file;
 typedef struct {
     uint32_t n_vertices, n_triangles, n_materials, n_lights, n_meshes;
@@ -80,7 +79,8 @@ const uint32_t* rb2_scene_file_indices(const rb2_scene_file* f);      /* 3 per t
 const uint32_t* rb2_scene_file_tri_material(const rb2_scene_file* f); /* 1 per triangle */
 const float* rb2_scene_file_albedo(const rb2_scene_file* f);          /* 3 per material */
 const float* rb2_scene_file_emission(const rb2_scene_file* f);        /* 3 per material */
-const uint32_t* rb2_scene_file_bsdf_types(const rb2_scene_file* f);   /* RB2_BSDF_* per material */
+const uint32_t* rb2_scene_file_bsdf_types(const rb2_scene_file* f);   /* first layer's RB2_BSDF_* per material */
+const rb2_material_desc* rb2_scene_file_materials(const rb2_scene_file* f);  /* one per material */
 /* Mesh i: name and its triangle range [first, first + count). */
 int rb2_scene_file_mesh(const rb2_scene_file* f, uint32_t i, const char** name, uint32_t* first, uint32_t* count);
 void rb2_scene_file_free(rb2_scene_file* f);

@@ -288,18 +288,70 @@ def is_tie(woop, triidx, slots, ray8, prim_a, prim_b) -> bool:
 # ---------------------------------------------------------------- shading references
 class _Scene(C.Structure):
     _fields_ = [("verts", C.c_void_p), ("tris", C.c_void_p), ("tri_mat", C.c_void_p), ("albedo", C.c_void_p),
-                ("emission", C.c_void_p), ("lights", C.c_void_p), ("n_lights", C.c_uint32)]
+                ("emission", C.c_void_p), ("lights", C.c_void_p), ("n_lights", C.c_uint32),
+                ("materials", C.c_void_p)]
+
+
+# rb2o_layer / rb2o_material (the product's rb2_bsdf_layer / rb2_material_desc layout).
+LAYER_DTYPE = np.dtype([("type", np.uint32), ("fresnel", np.uint32), ("color", np.float32, 3),
+                        ("sigma_deg", np.float32), ("etai", np.float32), ("etat", np.float32),
+                        ("exponent", np.float32), ("eta", np.float32, 3), ("k", np.float32, 3)])
+MATERIAL_DTYPE = np.dtype([("n_layers", np.uint32), ("reserved", np.uint32), ("layer", LAYER_DTYPE, 4)])
+assert LAYER_DTYPE.itemsize == 60 and MATERIAL_DTYPE.itemsize == 248
+
+
+def materials_array(descs) -> np.ndarray:
+    """Material descriptions as an rb2o_material array: `descs` is a ctypes
+    rb2_material_desc array (same bytes) or a structured numpy array."""
+    if isinstance(descs, np.ndarray):
+        return np.ascontiguousarray(descs, MATERIAL_DTYPE)
+    return np.frombuffer(bytes(descs), MATERIAL_DTYPE).copy()
+
+
+def material_query(material, sample: bool, q) -> np.ndarray:
+    """FP64 material functions (rb2o_material_query) for one material over
+    queries q (n, 9); returns (n, 4) f/pdf or (n, 8) wi/f/pdf/specular."""
+    m = materials_array(material).reshape(-1)[:1]
+    q = np.ascontiguousarray(q, np.float64).reshape(-1, 9)
+    L = orc_lib()
+    L.rb2o_material_query.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.rb2o_material_query.restype = None
+    w = 8 if sample else 4
+    out = np.zeros((q.shape[0], w), np.float64)
+    for i in range(q.shape[0]):
+        L.rb2o_material_query(_p(m), 1 if sample else 0, _p(q[i]), out[i].ctypes.data)
+    return out
+
+
+def ref_material(material, sample: bool, q) -> np.ndarray:
+    """The reference's material_f / material_pdf / material_sample_f (compiled
+    from core/reflection.cu and core/material.cu) on the same queries."""
+    m = materials_array(material).reshape(-1)[0]
+    layers = np.ascontiguousarray(m["layer"][: int(m["n_layers"])])
+    q = np.ascontiguousarray(q, np.float32).reshape(-1, 9)
+    L = ref_lib()
+    L.rb2ref_material.argtypes = [C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]
+    L.rb2ref_material.restype = C.c_int
+    w = 8 if sample else 4
+    out = np.zeros((q.shape[0], w), np.float32)
+    for i in range(q.shape[0]):
+        rc = L.rb2ref_material(_p(layers), int(m["n_layers"]), 1 if sample else 0, _p(q[i]), out[i].ctypes.data)
+        if rc != 0:
+            raise RuntimeError("reference material query failed")
+    return out
 
 
 class _Bvh(C.Structure):
     _fields_ = [("nodes", C.c_void_p), ("woop", C.c_void_p), ("triidx", C.c_void_p)]
 
 
-def _scene_struct(vertices, indices, tri_mat, albedo, emission, lights):
+def _scene_struct(vertices, indices, tri_mat, albedo, emission, lights, materials=None):
     keep = [np.ascontiguousarray(vertices, np.float32), np.ascontiguousarray(indices, np.uint32),
             np.ascontiguousarray(tri_mat, np.uint32), np.ascontiguousarray(albedo, np.float32),
             np.ascontiguousarray(emission, np.float32), np.ascontiguousarray(lights, np.uint32)]
-    s = _Scene(*[_p(k) for k in keep[:6]], keep[5].shape[0])
+    mats = None if materials is None else materials_array(materials)
+    keep.append(mats)
+    s = _Scene(*[_p(k) for k in keep[:6]], keep[5].shape[0], _p(mats))
     return s, keep
 
 
@@ -326,13 +378,14 @@ def ao(bvh_buffers, vertices, indices, prim_rays, samples, radius, seed=1, nthre
 
 
 def pt(bvh_buffers, vertices, indices, tri_mat, albedo, emission, lights, rays, max_depth, rr_start, rr_prob,
-       seed=1, nthreads=0):
-    """One FP64 path-traced sample per camera ray; returns (n, 3) radiance."""
+       seed=1, nthreads=0, materials=None):
+    """One FP64 path-traced sample per camera ray; returns (n, 3) radiance.
+    `materials` (optional): layered material descriptions per material."""
     L = orc_lib()
     L.rb2o_pt.argtypes = [C.POINTER(_Bvh), C.POINTER(_Scene), C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                           C.c_float, C.c_uint64, C.c_void_p, C.c_int]
     L.rb2o_pt.restype = None
-    s, ks = _scene_struct(vertices, indices, tri_mat, albedo, emission, lights)
+    s, ks = _scene_struct(vertices, indices, tri_mat, albedo, emission, lights, materials)
     b, kb = _bvh_struct(*bvh_buffers)
     r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
     out = np.empty((r.shape[0], 3), np.float64)

@@ -479,6 +479,219 @@ static double tri_area_d(d3 a, d3 b_, d3 c)
     return 0.5 * sqrt(ddot(cr, cr));
 }
 
+/* ---- layered materials (FP64) ---------------------------------------------------- */
+typedef struct { d3 x, y, z; } frame3;
+static frame3 frame_z(d3 n)
+{
+    frame3 f;
+    f.z = dnorm(n);
+    d3 t = fabs(f.z.x) > 0.99 ? D3(0, 1, 0) : D3(1, 0, 0);
+    f.y = dnorm(dcross(f.z, t));
+    f.x = dcross(f.y, f.z);
+    return f;
+}
+static d3 fr_local(const frame3* f, d3 w) { return D3(ddot(w, f->x), ddot(w, f->y), ddot(w, f->z)); }
+static d3 fr_world(const frame3* f, d3 w) { return dadd(dadd(dmul(f->x, w.x), dmul(f->y, w.y)), dmul(f->z, w.z)); }
+static int same_h(d3 a, d3 b) { return a.z * b.z > 0.0; }
+static double sin2t(d3 w) { double v = 1.0 - w.z * w.z; return v > 0.0 ? v : 0.0; }
+static double clampd(double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static int is_delta(uint32_t k) { return k == 2 || k == 3; }
+static uint32_t bx_bits(uint32_t k) { return k == 2 ? (1u | 16u) : (k == 3 ? (1u | 16u | 2u) : (k == 4 ? (1u | 8u) : (1u | 4u))); }
+
+static double fres_diel(double cosi, double etai, double etat)
+{
+    int entering = cosi > 0.0;
+    double ei = entering ? etai : etat, et = entering ? etat : etai;
+    double sint = ei / et * sqrt(1.0 - cosi * cosi > 0.0 ? 1.0 - cosi * cosi : 0.0);
+    if (sint >= 1.0) return 1.0;
+    double cost = sqrt(1.0 - sint * sint > 0.0 ? 1.0 - sint * sint : 0.0), ci = fabs(cosi);
+    double rpar = (et * ci - ei * cost) / (et * ci + ei * cost);
+    double rperp = (ei * ci - et * cost) / (ei * ci + et * cost);
+    return (rpar * rpar + rperp * rperp) / 2.0;
+}
+static double fres_cond(double cosi, double eta, double k)
+{
+    double tmp = (eta * eta + k * k) * cosi * cosi;
+    double rpar2 = (tmp - 2.0 * eta * cosi + 1.0) / (tmp + 2.0 * eta * cosi + 1.0);
+    double tf = eta * eta + k * k;
+    double rperp2 = (tf - 2.0 * eta * cosi + cosi * cosi) / (tf + 2.0 * eta * cosi + cosi * cosi);
+    return (rpar2 + rperp2) / 2.0;
+}
+static d3 fres(const rb2o_layer* l, double cosi)
+{
+    if (l->fresnel == 1) return D3(fres_cond(cosi, l->eta[0], l->k[0]), fres_cond(cosi, l->eta[1], l->k[1]),
+                                   fres_cond(cosi, l->eta[2], l->k[2]));
+    if (l->fresnel == 0) { double r = fres_diel(clampd(cosi, -1.0, 1.0), l->etai, l->etat); return D3(r, r, r); }
+    return D3(1, 1, 1);
+}
+static d3 col(const rb2o_layer* l) { return D3(l->color[0], l->color[1], l->color[2]); }
+static double blinn_D_d(d3 wh, double e) { return (e + 2.0) / (2.0 * RB2O_PI) * pow(fabs(wh.z), e); }
+static double blinn_pdf_d(d3 wo, d3 wi, double e)
+{
+    d3 wh = dnorm(dadd(wo, wi));
+    double d = ddot(wo, wh);
+    if (d <= 0.0) return 0.0;
+    return ((e + 1.0) * pow(fabs(wh.z), e)) / (2.0 * RB2O_PI * 4.0 * d);
+}
+static d3 mf_eval(const rb2o_layer* l, d3 wi, d3 wo)
+{
+    double co = fabs(wo.z), ci = fabs(wi.z);
+    if (ci == 0.0 || co == 0.0) return D3(0, 0, 0);
+    d3 wh = dadd(wi, wo);
+    if (wh.x == 0.0 && wh.y == 0.0 && wh.z == 0.0) return D3(0, 0, 0);
+    wh = dnorm(wh);
+    d3 F = fres(l, ddot(wi, wh));
+    double nh = fabs(wh.z), woh = fabs(ddot(wo, wh));
+    double g1 = 2.0 * nh / woh, g2 = 2.0 * nh * ci / woh;
+    double G = 1.0;
+    if (g1 < G) G = g1;
+    if (g2 < G) G = g2;
+    double s = blinn_D_d(wh, l->exponent) * G / (4.0 * ci * co);
+    return D3(l->color[0] * s * F.x, l->color[1] * s * F.y, l->color[2] * s * F.z);
+}
+static void on_AB(const rb2o_layer* l, double* A, double* B)
+{
+    double sd = l->sigma_deg < 0.0f ? 0.0 : (l->sigma_deg > 90.0f ? 90.0 : (double)l->sigma_deg);
+    double sg = sd * RB2O_PI / 180.0, s2 = sg * sg;
+    *A = 1.0 - s2 / (2.0 * (s2 + 0.33));
+    *B = 0.45 * s2 / (s2 + 0.09);
+}
+static d3 on_eval(const rb2o_layer* l, d3 wi, d3 wo)
+{
+    double si = sqrt(sin2t(wi)), so = sqrt(sin2t(wo)), maxcos = 0.0;
+    if (si > 1e-4 && so > 1e-4) {
+        double cpi = si == 0.0 ? 1.0 : clampd(wi.x / si, -1, 1), spi = si == 0.0 ? 0.0 : clampd(wi.y / si, -1, 1);
+        double cpo = so == 0.0 ? 1.0 : clampd(wo.x / so, -1, 1), spo = so == 0.0 ? 0.0 : clampd(wo.y / so, -1, 1);
+        double dc = cpi * cpo + spi * spo;
+        maxcos = dc > 0.0 ? dc : 0.0;
+    }
+    double sa, tb;
+    if (fabs(wi.z) > fabs(wo.z)) { sa = so; tb = si / fabs(wi.z); }
+    else { sa = si; tb = so / fabs(wo.z); }
+    double A, B;
+    on_AB(l, &A, &B);
+    return dmul(col(l), (A + B * maxcos * sa * tb) / RB2O_PI);
+}
+static d3 layer_f_d(const rb2o_layer* l, d3 wi, d3 wo)
+{
+    switch (l->type) {
+    case 0: return same_h(wi, wo) ? dmul(col(l), 1.0 / RB2O_PI) : D3(0, 0, 0);
+    case 1: return on_eval(l, wi, wo);
+    case 4: return mf_eval(l, wi, wo);
+    default: return D3(0, 0, 0);
+    }
+}
+static double layer_pdf_d(const rb2o_layer* l, d3 wi, d3 wo)
+{
+    if (l->type == 0 || l->type == 1) return same_h(wi, wo) ? fabs(wi.z) / RB2O_PI : 0.0;
+    if (l->type == 4) return same_h(wi, wo) ? blinn_pdf_d(wo, wi, l->exponent) : 0.0;
+    return 0.0;
+}
+static d3 mat_f(const rb2o_material* m, d3 n, d3 wo_w, d3 wi_w, d3 wo, d3 wi)
+{
+    uint32_t side = ddot(wi_w, n) * ddot(wo_w, n) > 0.0 ? (1u | 4u | 8u) : (2u | 4u | 8u);
+    d3 f = D3(0, 0, 0);
+    for (uint32_t i = 0; i < m->n_layers; i++) {
+        uint32_t bits = bx_bits(m->layer[i].type);
+        if ((bits & side) != bits) continue;
+        f = dadd(f, layer_f_d(&m->layer[i], wi, wo));
+    }
+    return f;
+}
+static double mat_pdf(const rb2o_material* m, d3 wo, d3 wi)
+{
+    double p = 0.0;
+    uint32_t n = 0;
+    for (uint32_t i = 0; i < m->n_layers; i++) {
+        if (is_delta(m->layer[i].type)) continue;
+        n++;
+        p += layer_pdf_d(&m->layer[i], wi, wo);
+    }
+    return n ? p / n : 0.0;
+}
+/* Returns f; wi_w, pdf, specular out. */
+static d3 mat_sample(const rb2o_material* m, d3 n, d3 wo_w, double u1, double u2, double uc, d3* wi_w, double* pdf,
+                     int* specular)
+{
+    *pdf = 0.0;
+    *specular = 0;
+    if (m->n_layers == 0) return D3(0, 0, 0);
+    frame3 fr = frame_z(n);
+    d3 wo = fr_local(&fr, wo_w);
+    uint32_t which = (uint32_t)floor(uc * m->n_layers);
+    if (which > m->n_layers - 1) which = m->n_layers - 1;
+    const rb2o_layer* l = &m->layer[which];
+    d3 wi, f;
+    if (l->type == 2) {
+        wi = D3(-wo.x, -wo.y, wo.z);
+        *pdf = 1.0;
+        f = dmul(col(l), 1.0 / fabs(wi.z));
+    } else if (l->type == 3) {
+        int entering = wo.z > 0.0;
+        double ei = entering ? l->etai : l->etat, et = entering ? l->etat : l->etai, eta = ei / et;
+        double sint2 = eta * eta * sin2t(wo);
+        if (sint2 >= 1.0) return D3(0, 0, 0);
+        double cost = sqrt(1.0 - sint2 > 0.0 ? 1.0 - sint2 : 0.0);
+        if (entering) cost = -cost;
+        wi = D3(eta * -wo.x, eta * -wo.y, cost);
+        *pdf = 1.0;
+        double F = fres_diel(wo.z, l->etai, l->etat);
+        f = dmul(col(l), (et * et) / (ei * ei) * (1.0 - F) / fabs(wi.z));
+    } else if (l->type == 4) {
+        double e = l->exponent, ct = pow(u1, 1.0 / (e + 1.0)), st = sqrt(1.0 - ct * ct > 0.0 ? 1.0 - ct * ct : 0.0);
+        double phi = u2 * 2.0 * RB2O_PI;
+        d3 wh = D3(st * cos(phi), st * sin(phi), ct);
+        if (!same_h(wo, wh)) wh = dmul(wh, -1.0);
+        double d = ddot(wo, wh);
+        wi = dadd(dmul(wo, -1.0), dmul(wh, 2.0 * d));
+        *pdf = d <= 0.0 ? 0.0 : ((e + 1.0) * pow(ct, e)) / (2.0 * RB2O_PI * 4.0 * d);
+        f = same_h(wi, wo) ? mf_eval(l, wi, wo) : D3(0, 0, 0);
+    } else {
+        wi = cos_hemi(u1, u2);
+        if (wo.z < 0.0) wi.z = -wi.z;
+        wi = dnorm(wi);
+        *pdf = same_h(wi, wo) ? fabs(wi.z) / RB2O_PI : 0.0;
+        f = layer_f_d(l, wi, wo);
+    }
+    if (*pdf == 0.0) return D3(0, 0, 0);
+    *wi_w = fr_world(&fr, wi);
+    *specular = is_delta(l->type);
+    if (!*specular) {
+        for (uint32_t i = 0; i < m->n_layers; i++)
+            if (i != which && !is_delta(m->layer[i].type)) *pdf += layer_pdf_d(&m->layer[i], wi, wo);
+        f = mat_f(m, n, wo_w, *wi_w, wo, wi);
+    }
+    *pdf /= m->n_layers;
+    return f;
+}
+
+void rb2o_material_query(const rb2o_material* m, int sample, const double* q, double* out)
+{
+    d3 n = D3(q[0], q[1], q[2]), wo_w = D3(q[3], q[4], q[5]);
+    if (sample) {
+        d3 wi = D3(0, 0, 0);
+        double pdf;
+        int spec;
+        d3 f = mat_sample(m, n, wo_w, q[6], q[7], q[8], &wi, &pdf, &spec);
+        out[0] = wi.x; out[1] = wi.y; out[2] = wi.z; out[3] = f.x; out[4] = f.y; out[5] = f.z; out[6] = pdf;
+        out[7] = spec;
+    } else {
+        frame3 fr = frame_z(n);
+        d3 wi_w = D3(q[6], q[7], q[8]);
+        d3 wo = fr_local(&fr, wo_w), wi = fr_local(&fr, wi_w);
+        d3 f = mat_f(m, n, wo_w, wi_w, wo, wi);
+        out[0] = f.x; out[1] = f.y; out[2] = f.z; out[3] = mat_pdf(m, wo, wi);
+    }
+}
+
+static int plain_lambertian(const rb2o_material* m) { return m->n_layers == 1 && m->layer[0].type == 0; }
+static int has_nondelta(const rb2o_material* m)
+{
+    for (uint32_t i = 0; i < m->n_layers; i++)
+        if (!is_delta(m->layer[i].type)) return 1;
+    return 0;
+}
+
 void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t n, uint32_t max_depth,
              uint32_t rr_start, float rr_prob, uint64_t seed, double* out_rgb, int nthreads)
 {
@@ -508,7 +721,7 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
                 double cosl = ddot(ng, wo);
                 if (cosl > 0.0) {
                     double w = 1.0;
-                    if (bnc > 0) {
+                    if (bnc > 0 && pdf_prev > 0.0) {  /* pdf_prev < 0: specular bounce */
                         double pdf_l = inv_nl * (double)h.t * (double)h.t / (tri_area_d(v0, v1, v2) * cosl);
                         w = pdf_prev / (pdf_prev + pdf_l);
                     }
@@ -516,9 +729,67 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
                 }
                 break;
             }
+            uint64_t key = (uint64_t)i * 64 + bnc;
+            if (s->materials && !plain_lambertian(&s->materials[m])) {
+                /* Layered material: NEE with material_f / material_pdf (skipped for
+                 * purely specular materials), continuation by material_sample_f;
+                 * emission after a specular bounce takes full weight. */
+                const rb2o_material* mt = &s->materials[m];
+                frame3 fr = frame_z(ng);
+                d3 wo_l = fr_local(&fr, wo);
+                if (s->n_lights && has_nondelta(mt)) {
+                    uint32_t j = (uint32_t)(u01(seed, key, 0) * s->n_lights);
+                    if (j >= s->n_lights) j = s->n_lights - 1;
+                    const uint32_t lt = s->lights[j];
+                    const uint32_t* lv = s->tris + 3 * (size_t)lt;
+                    d3 l0 = vtx(s, lv[0]), l1 = vtx(s, lv[1]), l2 = vtx(s, lv[2]);
+                    double su = sqrt(u01(seed, key, 1)), u2 = u01(seed, key, 2);
+                    double b0 = 1.0 - su, b1 = u2 * su;
+                    d3 lp = dadd(dadd(dmul(l0, b0), dmul(l1, b1)), dmul(l2, 1.0 - b0 - b1));
+                    d3 ln = dnorm(dcross(dsub(l1, l0), dsub(l2, l0)));
+                    d3 dv = dsub(lp, pos);
+                    double dist2 = ddot(dv, dv), dist = sqrt(dist2);
+                    d3 wi = dmul(dv, 1.0 / dist);
+                    double cos_l = -ddot(ln, wi);
+                    const float* Le = s->emission + 3 * (size_t)s->tri_mat[lt];
+                    if (cos_l > 0.0 && dist > 0.0) {
+                        d3 wi_l = fr_local(&fr, wi);
+                        d3 f = mat_f(mt, ng, wo, wi, wo_l, wi_l);
+                        if (f.x > 0.0 || f.y > 0.0 || f.z > 0.0) {
+                            double pdf_l = inv_nl * dist2 / (tri_area_d(l0, l1, l2) * cos_l);
+                            double pdf_b = mat_pdf(mt, wo_l, wi_l);
+                            double w = (bnc == max_depth) ? 1.0 : pdf_l / (pdf_l + pdf_b);
+                            float sr[8];
+                            mkray(sr, pos, eps, wi, dist * (1.0 - 1.0e-3));
+                            if (!occluded(b, sr)) {
+                                double k = fabs(ddot(wi, ng)) * w / pdf_l;
+                                L[0] += T[0] * f.x * Le[0] * k;
+                                L[1] += T[1] * f.y * Le[1] * k;
+                                L[2] += T[2] * f.z * Le[2] * k;
+                            }
+                        }
+                    }
+                }
+                if (bnc >= max_depth) break;
+                d3 wi = D3(0, 0, 0);
+                double pdf;
+                int spec;
+                d3 f = mat_sample(mt, ng, wo, u01(seed, key, 3), u01(seed, key, 4), u01(seed, key, 6), &wi, &pdf, &spec);
+                if (!(pdf > 0.0) || !(f.x > 0.0 || f.y > 0.0 || f.z > 0.0)) break;
+                double k = fabs(ddot(wi, ng)) / pdf;
+                T[0] *= f.x * k; T[1] *= f.y * k; T[2] *= f.z * k;
+                pdf_prev = spec ? -1.0 : pdf;
+                if (bnc >= rr_start) {
+                    double lum = 0.212671 * T[0] + 0.715160 * T[1] + 0.072169 * T[2];
+                    double q = lum < rr_prob ? lum : rr_prob;
+                    if (!(u01(seed, key, 5) < q)) break;
+                    for (int c2 = 0; c2 < 3; c2++) T[c2] /= q;
+                }
+                mkray(ray, pos, eps, wi, 3.402823466e+38);
+                continue;
+            }
             d3 nrm = ddot(ng, wo) < 0.0 ? dmul(ng, -1.0) : ng;
             const float* A = s->albedo + 3 * (size_t)m;
-            uint64_t key = (uint64_t)i * 64 + bnc;
             if (s->n_lights) {
                 uint32_t j = (uint32_t)(u01(seed, key, 0) * s->n_lights);
                 if (j >= s->n_lights) j = s->n_lights - 1;

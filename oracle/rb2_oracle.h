@@ -88,6 +88,21 @@ void rb2o_film(uint32_t kind, float xw, float yw, float alpha, uint32_t width, u
  * Scene for the integrator references: vertices (xyz), triangles (3 indices),
  * per-triangle material, per-material albedo/emission (rgb), emissive
  * triangle list (uniform light choice, integrators/integrator_path.cu:122). */
+/* A layered material in the product's rb2_material_desc layout: bxdf layers
+ * (0 Lambertian, 1 Oren-Nayar, 2 mirror, 3 glass, 4 Blinn microfacet; Fresnel
+ * 0 dielectric, 1 conductor, 2 none) following core/reflection.cu:42-299 and
+ * core/material.cu:56-326, with the two documented differences of the
+ * product: a sampled multi-layer pdf is divided by the layer count, and a
+ * glass layer adds no microfacet term. */
+typedef struct {
+    uint32_t type, fresnel;
+    float color[3], sigma_deg, etai, etat, exponent, eta[3], k[3];
+} rb2o_layer;
+typedef struct {
+    uint32_t n_layers, reserved;
+    rb2o_layer layer[4];
+} rb2o_material;
+
 typedef struct {
     const float* verts;
     const uint32_t* tris;
@@ -96,7 +111,13 @@ typedef struct {
     const float* emission;
     const uint32_t* lights;
     uint32_t n_lights;
+    const rb2o_material* materials;  /* nullable: one Lambertian layer (albedo) per material */
 } rb2o_scene;
+
+/* The material functions in FP64 on world-space directions around normal n:
+ * sample == 0: q = (n, wo, wi) -> out = (f rgb, pdf), specular layers excluded;
+ * sample != 0: q = (n, wo, u1, u2, uc) -> out = (wi, f rgb, pdf, specular). */
+void rb2o_material_query(const rb2o_material* m, int sample, const double* q, double* out);
 
 typedef struct {
     const uint32_t* nodes;

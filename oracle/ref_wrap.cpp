@@ -8,10 +8,14 @@
 // It also exposes the reference's text BVH cache (cudabvh.cpp:108-214), its
 // perspective camera (core/camera.cu:30-98) and its host Moller-Trumbore test
 // (core/primitives.cu:51-70) so the CPU restatement and the product can be
-// pinned against them.
+// pinned against them, and its BSDFs and material dispatch
+// (core/reflection.cu, core/material.cu) for the BSDF pin.
 #include <accelerators/sbvh/bvh.h>
 #include <accelerators/sbvh/cudabvh.h>
+#include <core/bsdf.h>
+#include <core/util.h>
 #include <core/camera.h>
+#include <core/material.h>
 #include <core/mesh.h>
 #include <core/primitives.h>
 #include <core/scene.h>
@@ -198,6 +202,121 @@ int rb2ref_normal_and_point(const float* v0, const float* v1, const float* v2, c
     float3 p = r(t);
     ng_out[0] = n.x; ng_out[1] = n.y; ng_out[2] = n.z;
     p_out[0] = p.x; p_out[1] = p.y; p_out[2] = p.z;
+    return 0;
+}
+
+// One bxdf layer in the product's rb2_bsdf_layer layout (60 bytes).
+struct rb2ref_layer {
+    uint32_t type, fresnel;
+    float color[3], sigma_deg, etai, etat, exponent, eta[3], k[3];
+};
+
+// The reference's material_f + material_pdf (sample == 0; q = n, wo, wi) or
+// material_sample_f (sample != 0; q = n, wo, u1, u2, uc) for one material
+// built as the scene reader builds it (io/customfilereader.cpp:99-211):
+// per-type parameter arrays, bxdf type bits, Oren-Nayar A, B from sigma.
+// Non-specular queries use flags BxDF_ALL & ~BxDF_SPECULAR, sampling BxDF_ALL,
+// as the path integrator calls them (integrators/integrator_path.cu:150-222).
+// out = (f rgb, pdf) or (wi xyz, f rgb, pdf, specular).
+int rb2ref_material(const rb2ref_layer* layers, uint32_t n_layers, int sample, const float* q, float* out)
+{
+    if (n_layers == 0 || n_layers > 4) return 1;
+    Material m{};
+    LambertianBsdfParams lam[4];
+    OrenNayarBsdfParams on[4];
+    MirrorBsdfParams mir[4];
+    GlassBsdfParams gl[4];
+    MicrofacetBsdfParams mf[4];
+    uint32_t nl = 0, non = 0, nm = 0, ng = 0, nmf = 0;
+    for (uint32_t i = 0; i < n_layers; i++) {
+        const rb2ref_layer& L = layers[i];
+        const float4 color = make_float4(L.color[0], L.color[1], L.color[2], 0.0f);
+        switch (L.type) {
+        case 0:
+            m.layer_bxdf_type[i] = BxDFType(BxDF_REFLECTION | BxDF_DIFFUSE);
+            m.layer_bsdf_type[i] = BSDF_LAMBERTIAN;
+            m.layer_bsdf_id[i] = nl;
+            lam[nl++].color = color;
+            break;
+        case 1: {
+            m.layer_bxdf_type[i] = BxDFType(BxDF_REFLECTION | BxDF_DIFFUSE);
+            m.layer_bsdf_type[i] = BSDF_OREN_NAYAR;
+            m.layer_bsdf_id[i] = non;
+            OrenNayarBsdfParams& p = on[non++];
+            p.color = color;
+            p.sigma = to_radians(clamp(L.sigma_deg, 0.0f, 90.0f));
+            const float s2 = p.sigma * p.sigma;
+            p.AB.x = 1.0f - (s2 / (2.0f * (s2 + 0.33f)));
+            p.AB.y = 0.45f * s2 / (s2 + 0.09f);
+            break;
+        }
+        case 2:
+            m.layer_bxdf_type[i] = BxDFType(BxDF_REFLECTION | BxDF_SPECULAR);
+            m.layer_bsdf_type[i] = BSDF_MIRROR;
+            m.layer_bsdf_id[i] = nm;
+            mir[nm++].color = color;
+            break;
+        case 3:
+            m.layer_bxdf_type[i] = BxDFType(BxDF_REFLECTION | BxDF_SPECULAR | BxDF_TRANSMISSION);
+            m.layer_bsdf_type[i] = BSDF_GLASS;
+            m.layer_bsdf_id[i] = ng;
+            gl[ng].color = color;
+            gl[ng].etai = L.etai;
+            gl[ng++].etat = L.etat;
+            break;
+        case 4: {
+            m.layer_bxdf_type[i] = BxDFType(BxDF_REFLECTION | BxDF_GLOSSY);
+            m.layer_bsdf_type[i] = BSDF_BLINN_MICROFACET;
+            m.layer_bsdf_id[i] = nmf;
+            MicrofacetBsdfParams& p = mf[nmf++];
+            p.R = color;
+            p.exponent = L.exponent;
+            p.type = L.fresnel == 1 ? FresnelType::FRESNEL_CONDUCTOR
+                                    : (L.fresnel == 0 ? FresnelType::FRESNEL_DIELECTRIC : FresnelType::FRESNEL_NOOP);
+            p.eta = make_float4(L.eta[0], L.eta[1], L.eta[2], 0.0f);
+            p.k = make_float4(L.k[0], L.k[1], L.k[2], 0.0f);
+            p.etai = L.etai;
+            p.etat = L.etat;
+            break;
+        }
+        default:
+            return 1;
+        }
+    }
+    m.num_valid_layers = n_layers;
+    m.m_emitter = 0;
+    MaterialBuffer mb{};
+    mb.m_materials = &m;
+    mb.m_lambertian_bsdfs = lam;
+    mb.m_orennayar_bsdfs = on;
+    mb.m_mirror_bsdfs = mir;
+    mb.m_glass_bsdfs = gl;
+    mb.m_microfacet_bsdfs = mf;
+    mb.m_num_materials = 1;
+    const float3 n = make_float3(q[0], q[1], q[2]);
+    const float3 wo = make_float3(q[3], q[4], q[5]);
+    Frame frame;
+    frame.set_from_z(n);
+    if (sample) {
+        BsdfSample bs;
+        bs.m_dir1 = q[6];
+        bs.m_dir2 = q[7];
+        bs.fComponent = q[8];
+        bs.pad = 0.0f;
+        float3 wi = make_float3(0.0f);
+        float pdf = 0.0f;
+        BxDFType st = BxDFType(0);
+        const float3 f = material_sample_f(mb, 0, wo, frame, n, bs, wi, pdf, BxDF_ALL, st);
+        out[0] = wi.x; out[1] = wi.y; out[2] = wi.z;
+        out[3] = f.x; out[4] = f.y; out[5] = f.z; out[6] = pdf;
+        out[7] = (st & BxDF_SPECULAR) ? 1.0f : 0.0f;
+    } else {
+        const float3 wi = make_float3(q[6], q[7], q[8]);
+        const BxDFType fl = BxDFType(BxDF_ALL & ~BxDF_SPECULAR);
+        const float3 f = material_f(mb, 0, wo, wi, n, frame, fl);
+        out[0] = f.x; out[1] = f.y; out[2] = f.z;
+        out[3] = material_pdf(mb, 0, wo, wi, frame, fl);
+    }
     return 0;
 }
 

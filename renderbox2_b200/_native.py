@@ -63,6 +63,16 @@ class IsectBuffer(C.Structure):
                 ("intersected", C.c_void_p), ("epsilon", C.c_void_p)]
 
 
+class BsdfLayer(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("fresnel", C.c_uint32), ("color", C.c_float * 3), ("sigma_deg", C.c_float),
+                ("etai", C.c_float), ("etat", C.c_float), ("exponent", C.c_float), ("eta", C.c_float * 3),
+                ("k", C.c_float * 3)]
+
+
+class MaterialDesc(C.Structure):
+    _fields_ = [("n_layers", C.c_uint32), ("reserved", C.c_uint32), ("layer", BsdfLayer * 4)]
+
+
 class Filter(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("xwidth", C.c_float), ("ywidth", C.c_float), ("alpha", C.c_float)]
 
@@ -133,6 +143,8 @@ SIGNATURES = {
     "rb2_scene_dev_view": (C.c_int, [P, C.POINTER(DevScene)]),
     "rb2_trace_isect": (C.c_int, [P, P, P, U32, I32, P, C.POINTER(IsectBuffer), P]),
     "rb2_filter_table": (C.c_int, [C.POINTER(Filter), P]),
+    "rb2_scene_set_materials": (C.c_int, [P, C.POINTER(MaterialDesc), U32]),
+    "rb2_material_query": (C.c_int, [P, I32, P, P, U32, P, P]),
     "rb2_film_develop": (C.c_int, [C.POINTER(Filter), U32, U32, U32, P, P, P, P]),
     "rb2_image_write_pfm": (C.c_int, [C.c_char_p, P, U32, U32]),
     "rb2_integrator_set_filter": (C.c_int, [P, C.POINTER(Filter)]),

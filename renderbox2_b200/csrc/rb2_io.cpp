@@ -18,6 +18,7 @@ struct rb2_scene_file {
     std::vector<uint32_t> tri_mat;     // per triangle
     std::vector<float> albedo, emission;
     std::vector<uint32_t> bsdf;
+    std::vector<rb2_material_desc> mats;
     struct Mesh {
         std::string name;
         uint32_t first = 0, count = 0;
@@ -277,6 +278,15 @@ int load_obj(const std::string& path, rb2_scene_file& f)
     return RB2_OK;
 }
 
+rb2_material_desc default_material()
+{
+    rb2_material_desc d{};
+    d.n_layers = 1;
+    d.layer[0].type = RB2_BSDF_LAMBERTIAN;
+    d.layer[0].color[0] = d.layer[0].color[1] = d.layer[0].color[2] = 0.5f;
+    return d;
+}
+
 int bsdf_code(const std::string& t)
 {
     if (t == "lambertian") return RB2_BSDF_LAMBERTIAN;
@@ -311,18 +321,61 @@ int load_xml(const std::string& path, rb2_scene_file& f)
         if (m.name != "material") continue;
         const XNode* name = m.child("name");
         const XNode* bsdf = m.child("bsdf");
-        const XNode* bxdf = bsdf ? bsdf->child("bxdf") : nullptr;
-        if (!name || !bxdf) return fail(RB2_EFORMAT, path + ": material without <name> or <bsdf><bxdf>");
-        const XNode* type = bxdf->child("type");
-        const int code = type ? bsdf_code(type->text) : -1;
-        if (code < 0) return fail(RB2_EFORMAT, path + ": unknown bxdf type in material " + name->text);
-        float rgb[3] = {0.5f, 0.5f, 0.5f};
-        const XNode* refl = bxdf->child("reflectance");
-        if (refl && !parse_float3(refl->text, rgb)) return fail(RB2_EFORMAT, path + ": bad reflectance in " + name->text);
+        if (!name || !bsdf) return fail(RB2_EFORMAT, path + ": material without <name> or <bsdf>");
+        rb2_material_desc desc{};
+        for (const XNode& bx : bsdf->kids) {
+            if (bx.name != "bxdf") continue;
+            if (desc.n_layers == 4) return fail(RB2_EFORMAT, path + ": more than 4 layers in material " + name->text);
+            rb2_bsdf_layer& L = desc.layer[desc.n_layers++];
+            const XNode* type = bx.child("type");
+            const int code = type ? bsdf_code(type->text) : -1;
+            if (code < 0) return fail(RB2_EFORMAT, path + ": unknown bxdf type in material " + name->text);
+            L.type = (uint32_t)code;
+            L.color[0] = L.color[1] = L.color[2] = 0.5f;
+            auto num = [&](const char* tag, float& out) -> bool {
+                const XNode* e = bx.child(tag);
+                if (!e) return false;
+                char* end = nullptr;
+                out = std::strtof(e->text.c_str(), &end);
+                return end != e->text.c_str();
+            };
+            auto vec = [&](const char* tag, float* out) -> bool {
+                const XNode* e = bx.child(tag);
+                return e && parse_float3(e->text, out);
+            };
+            if (const XNode* refl = bx.child("reflectance"))
+                if (!parse_float3(refl->text, L.color))
+                    return fail(RB2_EFORMAT, path + ": bad reflectance in " + name->text);
+            const std::string where = path + ": material " + name->text + ": ";
+            if (code == RB2_BSDF_OREN_NAYAR && !num("sigma", L.sigma_deg)) return fail(RB2_EFORMAT, where + "<sigma> missing");
+            if (code == RB2_BSDF_GLASS && !(num("etai", L.etai) && num("etat", L.etat)))
+                return fail(RB2_EFORMAT, where + "glass needs <etai> and <etat>");
+            if (code == RB2_BSDF_MICROFACET) {
+                const XNode* dist = bx.child("distribution");
+                if (!dist || dist->text != "blinn") return fail(RB2_EFORMAT, where + "only the blinn distribution exists");
+                if (!num("exponent", L.exponent)) return fail(RB2_EFORMAT, where + "<exponent> missing");
+                const XNode* ft = bx.child("fresnel_type");
+                const std::string fts = ft ? ft->text : std::string("fresnel_noop");
+                if (fts == "fresnel_conductor") {
+                    L.fresnel = RB2_FRESNEL_CONDUCTOR;
+                    if (!(vec("eta", L.eta) && vec("k", L.k))) return fail(RB2_EFORMAT, where + "conductor needs <eta> and <k>");
+                } else if (fts == "fresnel_dielectric") {
+                    L.fresnel = RB2_FRESNEL_DIELECTRIC;
+                    if (!(num("etai", L.etai) && num("etat", L.etat)))
+                        return fail(RB2_EFORMAT, where + "dielectric needs <etai> and <etat>");
+                } else if (fts == "fresnel_noop") {
+                    L.fresnel = RB2_FRESNEL_NOOP;
+                } else {
+                    return fail(RB2_EFORMAT, where + "unknown fresnel_type " + fts);
+                }
+            }
+        }
+        if (desc.n_layers == 0) return fail(RB2_EFORMAT, path + ": material " + name->text + " has no <bxdf>");
         mat_of[name->text] = (uint32_t)f.bsdf.size();
-        f.bsdf.push_back((uint32_t)code);
-        f.albedo.insert(f.albedo.end(), rgb, rgb + 3);
+        f.bsdf.push_back(desc.layer[0].type);
+        f.albedo.insert(f.albedo.end(), desc.layer[0].color, desc.layer[0].color + 3);
         f.emission.insert(f.emission.end(), {0.0f, 0.0f, 0.0f});
+        f.mats.push_back(desc);
     }
     std::vector<uint32_t> mesh_mat(f.meshes.size(), 0u);
     for (const XNode& o : root.kids) {
@@ -344,6 +397,7 @@ int load_xml(const std::string& path, rb2_scene_file& f)
             if (!name || !le || !parse_float3(le->text, rgb)) return fail(RB2_EFORMAT, path + ": bad <light>");
             const uint32_t id = (uint32_t)f.bsdf.size();
             f.bsdf.push_back(RB2_BSDF_EMITTER);
+            f.mats.push_back(rb2_material_desc{});
             f.albedo.insert(f.albedo.end(), {0.0f, 0.0f, 0.0f});
             f.emission.insert(f.emission.end(), rgb, rgb + 3);
             for (size_t i = 0; i < f.meshes.size(); i++)
@@ -354,6 +408,7 @@ int load_xml(const std::string& path, rb2_scene_file& f)
         f.bsdf.push_back(RB2_BSDF_LAMBERTIAN);
         f.albedo.insert(f.albedo.end(), {0.5f, 0.5f, 0.5f});
         f.emission.insert(f.emission.end(), {0.0f, 0.0f, 0.0f});
+        f.mats.push_back(default_material());
     }
     f.tri_mat.assign(f.idx.size() / 3, 0u);
     for (size_t i = 0; i < f.meshes.size(); i++)
@@ -393,6 +448,7 @@ int rb2_scene_file_load(const char* path, rb2_scene_file** out)
             f->bsdf.assign(1, RB2_BSDF_LAMBERTIAN);
             f->albedo = {0.5f, 0.5f, 0.5f};
             f->emission = {0.0f, 0.0f, 0.0f};
+            f->mats.assign(1, default_material());
             f->tri_mat.assign(f->idx.size() / 3, 0u);
         }
     } else {
@@ -423,6 +479,7 @@ const uint32_t* rb2_scene_file_tri_material(const rb2_scene_file* f) { return f 
 const float* rb2_scene_file_albedo(const rb2_scene_file* f) { return f ? f->albedo.data() : nullptr; }
 const float* rb2_scene_file_emission(const rb2_scene_file* f) { return f ? f->emission.data() : nullptr; }
 const uint32_t* rb2_scene_file_bsdf_types(const rb2_scene_file* f) { return f ? f->bsdf.data() : nullptr; }
+const rb2_material_desc* rb2_scene_file_materials(const rb2_scene_file* f) { return f ? f->mats.data() : nullptr; }
 
 int rb2_scene_file_mesh(const rb2_scene_file* f, uint32_t i, const char** name, uint32_t* first, uint32_t* count)
 {

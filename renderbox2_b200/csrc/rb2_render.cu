@@ -10,6 +10,7 @@
 #include "rb2_render.h"
 #include "rb2_camera.cuh"
 #include "rb2_film.cuh"
+#include "rb2_material.cuh"
 #include "rb2_shading.cuh"
 #include "rb2_traverse.cuh"
 
@@ -124,7 +125,8 @@ __global__ void k_ao_finalize(const int4* hits, const uint32_t* counts, uint32_t
 // ---- path tracing -----------------------------------------------------------------
 // Random dimensions per (sample key, vertex b): camera jitter uses dims 0-1,
 // vertex b uses 8 dims from 2 + 8b.
-enum : uint32_t { kDimLight = 0, kDimLightU = 1, kDimLightV = 2, kDimBsdfU = 3, kDimBsdfV = 4, kDimRR = 5 };
+enum : uint32_t { kDimLight = 0, kDimLightU = 1, kDimLightV = 2, kDimBsdfU = 3, kDimBsdfV = 4, kDimRR = 5,
+                  kDimBsdfC = 6 };
 __device__ __forceinline__ uint32_t vdim(uint32_t b, uint32_t d) { return 2u + 8u * b + d; }
 
 struct SceneView {
@@ -134,6 +136,7 @@ struct SceneView {
     const float4* emission;
     const uint32_t* lights;
     uint32_t n_lights;
+    const MaterialDev* mats;   // null: every material is one Lambertian layer (albedo)
 };
 
 // Queue-driven ray source: the i-th entry of `queue` names a path whose ray
@@ -240,6 +243,71 @@ __device__ __forceinline__ float tri_area(float3 v0, float3 v1, float3 v2)
 // Shade every path of the current queue at vertex b (integrator_path.cu:84-254):
 // emission (MIS-weighted after the first vertex), next-event estimation with
 // a shadow ray, BSDF sampling of the continuation, Russian roulette.
+// Path vertex on a layered material (core/material.cu, core/reflection.cu):
+// next-event estimation with material_f / material_pdf (skipped for purely
+// specular materials), then material_sample_f for the continuation.  T.w
+// carries the sampled pdf for the emission MIS weight, -1 after a specular
+// bounce (full weight, as integrator_path.cu:94 counts emission after one).
+__device__ __forceinline__ void shade_layered(const SceneView& sc, const MaterialDev& m, uint64_t seed, uint64_t key,
+                                              uint32_t b, uint32_t max_depth, uint32_t rr_start, float rr_prob,
+                                              float inv_nl, float3 pos, float eps, float3 ng, float3 wo, float4& Tp,
+                                              bool& shadow, float4& so, float4& sd, float4& scv, bool& cont,
+                                              float4& new_o, float4& new_d)
+{
+    const Frame fr = frame_from_z(ng);
+    const float3 wo_l = to_local(fr, wo);
+    if (sc.n_lights && (m.flags & kMatHasNonDelta)) {
+        uint32_t j = (uint32_t)(rng_u01(seed, key, vdim(b, kDimLight)) * (float)sc.n_lights);
+        j = min(j, sc.n_lights - 1);
+        const uint4 lt = sc.tris[sc.lights[j]];
+        const float3 l0 = xyz(sc.verts[lt.x]), l1 = xyz(sc.verts[lt.y]), l2 = xyz(sc.verts[lt.z]);
+        const float3 lp = sample_triangle(l0, l1, l2, rng_u01(seed, key, vdim(b, kDimLightU)),
+                                          rng_u01(seed, key, vdim(b, kDimLightV)));
+        const float3 ln = normalize3(cross3(sub(l1, l0), sub(l2, l0)));
+        const float3 dv = sub(lp, pos);
+        const float dist2 = dot3(dv, dv);
+        const float dist = sqrtf(dist2);
+        const float3 wi = mul(dv, 1.0f / dist);
+        const float cos_l = -dot3(ln, wi);
+        if (cos_l > 0.0f && dist > 0.0f) {
+            const float3 wi_l = to_local(fr, wi);
+            const float3 f = material_f(m, ng, wo, wi, wo_l, wi_l);
+            if (f.x > 0.0f || f.y > 0.0f || f.z > 0.0f) {
+                const float4 Le = sc.emission[lt.w];
+                const float pdf_l = inv_nl * dist2 / (tri_area(l0, l1, l2) * cos_l);
+                const float pdf_b = material_pdf(m, wo_l, wi_l);
+                const float w = (b == max_depth) ? 1.0f : pdf_l / (pdf_l + pdf_b);
+                const float k = fabsf(dot3(wi, ng)) * w / pdf_l;
+                scv = make_float4(Tp.x * f.x * Le.x * k, Tp.y * f.y * Le.y * k, Tp.z * f.z * Le.z * k, 0.0f);
+                so = make_float4(pos.x, pos.y, pos.z, eps);
+                sd = make_float4(wi.x, wi.y, wi.z, dist * (1.0f - 1.0e-3f));
+                shadow = scv.x > 0.0f || scv.y > 0.0f || scv.z > 0.0f;
+            }
+        }
+    }
+    if (b >= max_depth) return;
+    float3 wi;
+    float pdf;
+    bool spec;
+    const float3 f = material_sample(m, fr, ng, wo, rng_u01(seed, key, vdim(b, kDimBsdfU)),
+                                     rng_u01(seed, key, vdim(b, kDimBsdfV)), rng_u01(seed, key, vdim(b, kDimBsdfC)), wi,
+                                     pdf, spec);
+    if (!(pdf > 0.0f) || !(f.x > 0.0f || f.y > 0.0f || f.z > 0.0f)) return;
+    const float k = fabsf(dot3(wi, ng)) / pdf;
+    Tp.x *= f.x * k; Tp.y *= f.y * k; Tp.z *= f.z * k;
+    Tp.w = spec ? -1.0f : pdf;
+    cont = isfinite(Tp.x) && isfinite(Tp.y) && isfinite(Tp.z) && (Tp.x > 0.0f || Tp.y > 0.0f || Tp.z > 0.0f);
+    if (cont && b >= rr_start) {
+        const float q = fminf(rr_prob, luminance(xyz(Tp)));
+        if (!(rng_u01(seed, key, vdim(b, kDimRR)) < q)) cont = false;
+        else { Tp.x /= q; Tp.y /= q; Tp.z /= q; }
+    }
+    if (cont) {
+        new_o = make_float4(pos.x, pos.y, pos.z, eps);
+        new_d = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
+    }
+}
+
 __global__ void k_pt_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t sample0, uint32_t b, uint32_t max_depth,
                            uint32_t rr_start, float rr_prob, const uint32_t* q_in, uint32_t* q_out, float4* rays,
                            const int4* hits, float4* T, float4* L, float4* srays, float4* sc_out, uint32_t* qs,
@@ -276,7 +344,7 @@ __global__ void k_pt_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t 
                     const float cosl = dot3(ng, wo);
                     if (cosl > 0.0f) {
                         float w = 1.0f;
-                        if (b > 0) {
+                        if (b > 0 && Tp.w > 0.0f) {  // T.w < 0: the last bounce was specular
                             const float pdf_l = inv_nl * t * t / (tri_area(v0, v1, v2) * cosl);
                             w = Tp.w / (Tp.w + pdf_l);
                         }
@@ -284,6 +352,10 @@ __global__ void k_pt_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t 
                         L[path] = Lp;
                     }
                     // Emitters end the path (integrator_path.cu:94-107).
+                } else if (sc.mats != nullptr && !(sc.mats[tri.w].flags & kMatPlainLambertian)) {
+                    shade_layered(sc, sc.mats[tri.w], seed, key, b, max_depth, rr_start, rr_prob, inv_nl, pos, eps, ng,
+                                  wo, Tp, shadow, so, sd, scv, cont, new_o, new_d);
+                    if (cont) T[path] = Tp;
                 } else {
                     const float3 nrm = dot3(ng, wo) < 0.0f ? mul(ng, -1.0f) : ng;
                     const float4 A = sc.albedo[tri.w];
@@ -887,6 +959,7 @@ int rb2_scene_destroy(rb2_scene_dev* s)
 {
     if (!s) return RB2_OK;
     cudaFree(s->d_verts); cudaFree(s->d_tris); cudaFree(s->d_albedo); cudaFree(s->d_emission); cudaFree(s->d_lights);
+    cudaFree(s->d_mats);
     delete s;
     return RB2_OK;
 }
@@ -1008,7 +1081,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
     std::memcpy(ca.c2w, cam->camera_to_world, sizeof(ca.c2w));
     ca.width = cam->width; ca.height = cam->height; ca.spp = 1; ca.jitter = 1; ca.seed = p->seed;
     const rb2_scene_dev* sd = it->scene;
-    rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights};
+    rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights, sd->d_mats};
     const DeviceBvhView bv = device_bvh(it->tracer);
     WaveCounters* wc = it->d_wave;
     const unsigned g = grid_for(P, it->sms);
@@ -1058,6 +1131,8 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
     if (p->max_path_length < 1 || p->max_path_length > 16) return fail(RB2_EINVAL, "max_path_length must be in [1, 16]");
     if (p->connections < 1 || p->connections > rb2dev::kMaxConnections) return fail(RB2_EINVAL, "connections must be in [1, 8]");
+    if (it->scene->layered)
+        return fail(RB2_ENOTSUP, "BDPT shades single-layer Lambertian materials only; use the path tracer for this scene");
     cudaStream_t s = (cudaStream_t)stream;
     const uint64_t npix = (uint64_t)cam->width * cam->height;
     if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");
@@ -1084,7 +1159,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     std::memcpy(ca.c2w, cam->camera_to_world, sizeof(ca.c2w));
     ca.width = cam->width; ca.height = cam->height; ca.spp = 1; ca.jitter = 1; ca.seed = p->seed;
     const rb2_scene_dev* sd = it->scene;
-    rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights};
+    rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights, sd->d_mats};
     const DeviceBvhView bv = device_bvh(it->tracer);
     const float4* bn = static_cast<const float4*>(bv.nodes);
     const float4* bw = static_cast<const float4*>(bv.woop);

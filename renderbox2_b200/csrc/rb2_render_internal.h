@@ -9,12 +9,18 @@
 
 #include <cstdint>
 
+namespace rb2dev {
+struct MaterialDev;
+}
+
 struct rb2_scene_dev {
     float4* d_verts = nullptr;     // xyz, w unused
     uint4* d_tris = nullptr;       // vertex indices + material id
     float4* d_albedo = nullptr;    // per material
     float4* d_emission = nullptr;  // per material
     uint32_t* d_lights = nullptr;  // emissive triangle ids
+    rb2dev::MaterialDev* d_mats = nullptr;  // layered materials (null: one Lambertian layer = albedo)
+    bool layered = false;                   // some non-emitter material is not a single Lambertian layer
     uint32_t nv = 0, ntri = 0, n_mat = 0, n_lights = 0;
     uint64_t bytes = 0;
 };

@@ -11,14 +11,53 @@ from dataclasses import dataclass
 import numpy as np
 
 from ._native import AoParams, BdptParams, DevScene, IsectBuffer, PtParams, RenderStats, check, lib
+from ._native import BsdfLayer as _BsdfLayer
 from ._native import Filter as _Filter
+from ._native import MaterialDesc as _MaterialDesc
 from .accel import CudaTracer, Scene, _ptr, _stream_handle
 
 
-class DeviceScene:
-    """Scene::gpu_prepare equivalent: vertices, triangles, materials, lights."""
+BSDF_KINDS = {"lambertian": 0, "orennayar": 1, "mirror": 2, "glass": 3, "microfacet": 4}
+FRESNEL_KINDS = {"dielectric": 0, "conductor": 1, "noop": 2}
 
-    def __init__(self, scene: Scene, albedo=None, emission=None):
+
+@dataclass
+class BsdfLayer:
+    """One bxdf of a material (core/params.h:195-245)."""
+    type: str = "lambertian"
+    color: tuple = (0.5, 0.5, 0.5)
+    sigma_deg: float = 0.0                 # Oren-Nayar
+    etai: float = 1.0
+    etat: float = 1.5                      # glass / dielectric Fresnel
+    exponent: float = 20.0                 # Blinn microfacet
+    fresnel: str = "noop"
+    eta: tuple = (0.2, 0.9, 1.1)
+    k: tuple = (3.9, 2.4, 2.2)             # conductor Fresnel
+
+    def c_struct(self) -> _BsdfLayer:
+        return _BsdfLayer(BSDF_KINDS[self.type], FRESNEL_KINDS[self.fresnel], (C.c_float * 3)(*self.color),
+                          self.sigma_deg, self.etai, self.etat, self.exponent, (C.c_float * 3)(*self.eta),
+                          (C.c_float * 3)(*self.k))
+
+
+def material_descs(materials) -> "C.Array":
+    """A ctypes array of rb2_material_desc from lists of BsdfLayer (an
+    empty list = an emitter's material)."""
+    arr = (_MaterialDesc * max(1, len(materials)))()
+    for i, layers in enumerate(materials):
+        assert len(layers) <= 4, "at most 4 layers"
+        arr[i].n_layers = len(layers)
+        for j, l in enumerate(layers):
+            arr[i].layer[j] = l.c_struct()
+    return arr
+
+
+class DeviceScene:
+    """Scene::gpu_prepare equivalent: vertices, triangles, materials, lights.
+    `materials` (or the scene's own `materials` attribute): one list of
+    BsdfLayer, or a ctypes rb2_material_desc array, per material."""
+
+    def __init__(self, scene: Scene, albedo=None, emission=None, materials=None):
         v = np.ascontiguousarray(scene.vertices, np.float32)
         i = np.ascontiguousarray(scene.indices, np.uint32)
         m = np.ascontiguousarray(scene.material_ids, np.uint32)
@@ -32,6 +71,24 @@ class DeviceScene:
         self._s = C.c_void_p()
         check(lib().rb2_scene_create(_ptr(v), v.shape[0], _ptr(i), i.shape[0], _ptr(m), n_mat, _ptr(a), _ptr(e),
                                      C.byref(self._s)))
+        self.n_materials = n_mat
+        materials = getattr(scene, "materials", None) if materials is None else materials
+        if materials is not None:
+            self.set_materials(materials)
+
+    def set_materials(self, materials):
+        arr = materials if isinstance(materials, C.Array) else material_descs(materials)
+        check(lib().rb2_scene_set_materials(self._s, arr, len(arr)))
+
+    def material_query(self, mat_ids, q, sample: bool = False, stream=None):
+        """Device material evaluation (rb2_material_query): q (n, 9) float32
+        device tensor; returns (n, 4) f/pdf or (n, 8) wi/f/pdf/specular."""
+        import torch
+        n = int(q.shape[0])
+        out = torch.empty((n, 8 if sample else 4), dtype=torch.float32, device=q.device)
+        check(lib().rb2_material_query(self._s, 1 if sample else 0, _ptr(mat_ids), _ptr(q), n, _ptr(out),
+                                       _stream_handle(stream)))
+        return out
 
     def __del__(self):
         s = getattr(self, "_s", None)

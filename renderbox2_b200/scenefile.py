@@ -7,7 +7,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._native import check, lib
+from ._native import MaterialDesc, check, lib
 from .accel import Scene
 
 BSDF_NAMES = {0: "lambertian", 1: "orennayar", 2: "mirror", 3: "glass", 4: "microfacet", 5: "emitter"}
@@ -33,14 +33,15 @@ def _sigs(L):
                                       C.POINTER(C.c_uint32)]
     L.rb2_scene_file_mesh.restype = C.c_int
     L.rb2_scene_file_free.argtypes, L.rb2_scene_file_free.restype = [P], None
+    L.rb2_scene_file_materials.argtypes, L.rb2_scene_file_materials.restype = [P], C.POINTER(MaterialDesc)
     L._rb2_scenefile_sigs = True
 
 
 class SceneFile:
     """A loaded scene file: `scene` (Scene with material ids, per-material
-    albedo / emission and the emissive-triangle list), `camera` (dict or
-    None), `bsdf_types` (declared bxdf per material) and `meshes` (name,
-    first triangle, count)."""
+    albedo / emission, the layered material descriptions `materials` and the
+    emissive-triangle list), `camera` (dict or None), `bsdf_types` (first
+    layer's bxdf per material) and `meshes` (name, first triangle, count)."""
 
     def __init__(self, path: str):
         L = lib()
@@ -62,6 +63,8 @@ class SceneFile:
             s.albedo = arr(L.rb2_scene_file_albedo, 3 * nm, np.float32).reshape(-1, 3)
             s.emission = arr(L.rb2_scene_file_emission, 3 * nm, np.float32).reshape(-1, 3)
             types = arr(L.rb2_scene_file_bsdf_types, nm, np.uint32)
+            mp = L.rb2_scene_file_materials(h)
+            s.materials = (MaterialDesc * nm)(*[mp[i] for i in range(nm)])
             s.light_ids_to_primitive_ids = np.nonzero(types[s.material_ids] == 5)[0].astype(np.uint32)
             self.scene = s
             self.bsdf_types = [BSDF_NAMES[int(t)] for t in types]

@@ -1,0 +1,113 @@
+"""GPU parity of the layered materials (rb2_material_query) and of the path
+tracer on scenes that use them, through the C ABI.
+
+Bars: device material functions within single-precision rounding of the FP64
+oracle (itself pinned to the reference's compiled BSDFs, test_oracle.py) for
+every type and for multi-layer materials; the path tracer's image converges to
+the FP64 host path tracer (relative RMSE falling as spp^-1/2 and the image
+mean within 2 %)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _materials():
+    from renderbox2_b200.render import BsdfLayer as B
+    return [
+        [B("lambertian", (0.7, 0.5, 0.3))],
+        [B("orennayar", (0.6, 0.6, 0.6), sigma_deg=25.0)],
+        [B("microfacet", (0.9, 0.8, 0.7), exponent=30.0, fresnel="conductor")],
+        [B("microfacet", (0.9, 0.9, 0.9), exponent=200.0, fresnel="dielectric", etai=1.0, etat=1.5)],
+        [B("microfacet", (0.9, 0.9, 0.9), exponent=50.0, fresnel="noop")],
+        [B("mirror", (0.9, 0.8, 0.9))],
+        [B("glass", (1.0, 0.9, 1.0), etai=1.0, etat=1.5)],
+        [B("lambertian", (0.5, 0.5, 0.5)), B("microfacet", (0.4, 0.4, 0.4), exponent=80.0, fresnel="dielectric",
+                                              etai=1.0, etat=1.5)],
+        [B("orennayar", (0.6, 0.3, 0.3), sigma_deg=40.0), B("mirror", (0.3, 0.3, 0.3)),
+         B("glass", (0.8, 0.8, 0.8), etai=1.0, etat=1.33)],
+    ]
+
+
+def test_device_materials_equal_oracle(rb, orc, cuda):
+    from renderbox2_b200.render import DeviceScene, material_descs
+    torch = cuda
+    mats = _materials()
+    room = rb.RoomScene(seed=3, n_boxes=2, n_spheres=2, sphere_subdiv=1, n_lights=1)
+    n_mat = room.albedo.shape[0]
+    assert n_mat >= len(mats)
+    full = mats + [[mats[0][0]]] * (n_mat - len(mats))
+    ds = DeviceScene(room, materials=full)
+    arr = orc.materials_array(material_descs(full))
+    rng = np.random.Generator(np.random.PCG64(5))
+    n = 3000
+    for k in range(len(mats)):
+        v = rng.normal(size=(3, n, 3))
+        v /= np.linalg.norm(v, axis=2, keepdims=True)
+        ids = torch.full((n,), k, dtype=torch.int32, device="cuda")
+        q = np.concatenate([v[0], v[1], v[2]], 1).astype(np.float32)
+        got = ds.material_query(ids, torch.from_numpy(q).cuda()).cpu().numpy()
+        want = orc.material_query(arr[k:k + 1], False, q.astype(np.float64))
+        np.testing.assert_allclose(got, want, rtol=5e-4, atol=1e-6, err_msg=f"eval, material {k}")
+        u = rng.uniform(size=(n, 3))
+        q2 = np.concatenate([v[0], v[1], u], 1).astype(np.float32)
+        got = ds.material_query(ids, torch.from_numpy(q2).cuda(), sample=True).cpu().numpy()
+        want = orc.material_query(arr[k:k + 1], True, q2.astype(np.float64))
+        # Samples that land on a component boundary (uc * layers near an integer)
+        # may pick different layers in single and double precision: skip those.
+        nl = len(mats[k])
+        edge = np.abs(u[:, 2] * nl - np.round(u[:, 2] * nl)) < 1e-5
+        np.testing.assert_allclose(got[~edge], want[~edge], rtol=3e-3, atol=3e-5, err_msg=f"sample, material {k}")
+
+
+def _layered_room(rb):
+    room = rb.RoomScene(seed=2, n_boxes=10, n_spheres=60, sphere_subdiv=2, n_lights=1, emission=10.0)
+    from renderbox2_b200.render import BsdfLayer as B
+    n_mat = room.albedo.shape[0]
+    mats = [[B("lambertian", tuple(float(c) for c in room.albedo[m]))] for m in range(n_mat)]
+    special = _materials()[1:]
+    # The room's boxes and spheres (materials 6..) take the non-Lambertian materials in turn.
+    for i, m in enumerate(range(6, n_mat - 1)):
+        mats[m] = special[i % len(special)]
+    mats[n_mat - 1] = []   # the light
+    return room, mats
+
+
+def test_layered_path_tracing_converges_to_host_reference(rb, orc, cuda):
+    from renderbox2_b200.configs import CONFIG2 as C2
+    from renderbox2_b200.render import (BidirectionalPathIntegratorLvcParams, DeviceScene, Integrator,
+                                        PathIntegratorParams, material_descs)
+    room, mats = _layered_room(rb)
+    bvh = rb.BVH(room)
+    ds = DeviceScene(room, materials=mats)
+    it = Integrator(rb.CudaTracer(bvh), ds)
+    W, H = 96, 54
+    cam = rb.PerspectiveCamera(C2["eye"], C2["lookat"], C2["up"], (W, H), C2["fov"])
+    step = 4
+    ii, jj = np.meshgrid(np.arange(0, W, step), np.arange(0, H, step))
+    pix = (jj * W + ii).ravel()
+    ref_spp = 4096
+    rng = np.random.Generator(np.random.PCG64(19))
+    xy = (np.repeat(np.stack([ii.ravel(), jj.ravel()], 1), ref_spp, axis=0) +
+          rng.uniform(0, 1, size=(pix.size * ref_spp, 2))).astype(np.float32)
+    rays = orc.ref_camera_rays(C2["eye"], C2["lookat"], C2["up"], W, H, C2["fov"], xy)
+    L = orc.pt(bvh.buffers_view(), room.vertices, room.indices, room.material_ids, room.albedo, room.emission,
+               room.light_ids_to_primitive_ids, rays, C2["max_depth"], C2["rr_start"], C2["rr_prob"], seed=29,
+               materials=material_descs(mats))
+    ref = L.reshape(pix.size, ref_spp, 3).mean(axis=1)
+    assert ref.mean() > 0.0
+    errs = []
+    spps = [64, 256, 1024]
+    for spp in spps:
+        img = it.render_pt(cam, PathIntegratorParams(spp=spp, max_depth=C2["max_depth"], rr_start=C2["rr_start"],
+                                                     rr_prob=C2["rr_prob"], seed=spp)).cpu().numpy()
+        got = img[pix]
+        errs.append(float(np.sqrt(((got - ref) ** 2).mean()) / ref.mean()))
+        if spp == spps[-1]:
+            assert abs(got.mean() / ref.mean() - 1.0) < 0.02, (got.mean(), ref.mean())
+    print("layered PT rel RMSE", dict(zip(spps, errs)))
+    slope = np.polyfit(np.log(spps), np.log(errs), 1)[0]
+    assert -0.7 <= slope <= -0.3, slope
+    # BDPT shades single-layer Lambertian scenes only and says so.
+    with pytest.raises(rb.Rb2Error, match="Lambertian"):
+        it.render_bdpt(cam, BidirectionalPathIntegratorLvcParams(spp=1))
