@@ -123,9 +123,14 @@ typedef struct {
     uint32_t regs;              /* register budget of the kernel variant: 64, 48 or 40 (0 = 64) */
 } rb2_launch_config;
 
-/* Inner-node order of the uploaded Compact2 buffer: the reference's DFS
- * order (cudabvh.cpp:234-288) or breadth-first (top levels contiguous). */
-enum { RB2_NODE_ORDER_DFS = 0, RB2_NODE_ORDER_BFS = 1 };
+/* Node layout of the bulk traversals: the reference's Compact2 buffer in its
+ * DFS order (cudabvh.cpp:234-288), the same nodes breadth-first (top levels
+ * contiguous), or a 4-wide layout collapsed from the binary tree (up to four
+ * exact child boxes per 128-byte node; the same leaves and Woop triangles, so
+ * hits are identical except which of two triangles at the same t is
+ * reported).  Integrators and rb2_tracer_dev_bvh always use the binary
+ * Compact2 buffer. */
+enum { RB2_NODE_ORDER_DFS = 0, RB2_NODE_ORDER_BFS = 1, RB2_NODE_ORDER_WIDE4 = 2 };
 
 /* Ray-query modes. */
 enum { RB2_MODE_CLOSEST = 0, RB2_MODE_ANY = 1, RB2_MODE_OCCLUSION = 2 };

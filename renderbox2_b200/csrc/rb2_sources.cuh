@@ -118,7 +118,8 @@ __host__ __device__ constexpr size_t job_smem_bytes(uint32_t n_jobs, bool inline
 // REGS is the register budget per thread the variant is compiled for (64:
 // 32 resident warps per SM, 48: 40 warps, 40: 48 warps; lower budgets spill a
 // little state to L1).  The autotuner picks the variant by measurement.
-template <int BLOCK, int REGS = 64>
+// WIDE: the jobs' node buffers hold the 4-wide layout (kWideEmpty, rb2_traverse.cuh).
+template <int BLOCK, int REGS = 64, bool WIDE = false>
 __global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK) k_trace_jobs(const __grid_constant__ KernelArgs a)
 {
     extern __shared__ unsigned long long s_start[];
@@ -147,7 +148,7 @@ __global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK) k_trace_jobs(co
     src.counter = a.counter;
     src.chunk = a.chunk;
     src.rem = s_rem;
-    persistent_trace(src, a.fetch_threshold, a.status);
+    persistent_trace<JobSource, WIDE>(src, a.fetch_threshold, a.status);
 }
 
 }  // namespace rb2dev

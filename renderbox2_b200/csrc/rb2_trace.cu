@@ -79,19 +79,21 @@ int cuda_fail(cudaError_t e, const char* what)
         if (e_ != cudaSuccess) return cuda_fail(e_, what);  \
     } while (0)
 
-// Kernel variants: block shape {64, 128, 256} x register budget {64, 48, 40}.
+// Kernel variants: block shape {64, 128, 256} x register budget {64, 48, 40}
+// x node layout {binary, 4-wide}.
 struct Occupancy {
     int sms = 0;
-    int per_sm[3][3] = {};  // [block index][register-budget index]
+    int per_sm[3][3][2] = {};  // [block index][register-budget index][wide]
 };
 
 int block_index(uint32_t block) { return block == 64 ? 0 : (block == 256 ? 2 : 1); }
 int regs_index(uint32_t regs) { return regs == 48 ? 1 : (regs == 40 ? 2 : 0); }
 
 template <int B, int R>
-int occ_of(int& out, size_t smem)
+int occ_of(int* out, size_t smem)
 {
-    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&out, rb2dev::k_trace_jobs<B, R>, B, smem), "occupancy");
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&out[0], rb2dev::k_trace_jobs<B, R, false>, B, smem), "occupancy");
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&out[1], rb2dev::k_trace_jobs<B, R, true>, B, smem), "occupancy");
     return RB2_OK;
 }
 
@@ -108,19 +110,35 @@ int occupancy(Occupancy& o)
     return rc ? RB2_ECUDA : RB2_OK;
 }
 
-template <int B, int R>
+template <int B, int R, bool W>
 void launch_variant(const rb2dev::KernelArgs& a, unsigned blocks, size_t smem, cudaStream_t s)
 {
-    rb2dev::k_trace_jobs<B, R><<<blocks, B, smem, s>>>(a);
+    rb2dev::k_trace_jobs<B, R, W><<<blocks, B, smem, s>>>(a);
+}
+
+template <bool W>
+void launch_shape(int variant, const rb2dev::KernelArgs& a, unsigned g, size_t smem, cudaStream_t s)
+{
+    switch (variant) {
+    case 0: launch_variant<64, 64, W>(a, g, smem, s); break;
+    case 1: launch_variant<64, 48, W>(a, g, smem, s); break;
+    case 2: launch_variant<64, 40, W>(a, g, smem, s); break;
+    case 4: launch_variant<128, 48, W>(a, g, smem, s); break;
+    case 5: launch_variant<128, 40, W>(a, g, smem, s); break;
+    case 6: launch_variant<256, 64, W>(a, g, smem, s); break;
+    case 7: launch_variant<256, 48, W>(a, g, smem, s); break;
+    case 8: launch_variant<256, 40, W>(a, g, smem, s); break;
+    default: launch_variant<128, 64, W>(a, g, smem, s); break;
+    }
 }
 
 // Launches the persistent kernel: grid = SMs x resident CTAs per SM, capped
 // by the work available.
 int launch_jobs(const rb2dev::KernelArgs& a, uint64_t total_rays, uint32_t block, uint32_t ctas_per_sm, uint32_t regs,
-                const Occupancy& occ, cudaStream_t s)
+                bool wide, const Occupancy& occ, cudaStream_t s)
 {
     const int bi = block_index(block), ri = regs_index(regs);
-    const int max_per_sm = std::max(1, occ.per_sm[bi][ri]);
+    const int max_per_sm = std::max(1, occ.per_sm[bi][ri][wide ? 1 : 0]);
     const uint32_t per_sm = ctas_per_sm ? std::min<uint32_t>(ctas_per_sm, (uint32_t)max_per_sm) : (uint32_t)max_per_sm;
     uint64_t blocks = (uint64_t)occ.sms * per_sm;
     const uint64_t warps_needed = (total_rays + 31) / 32;
@@ -128,18 +146,8 @@ int launch_jobs(const rb2dev::KernelArgs& a, uint64_t total_rays, uint32_t block
     blocks = std::min<uint64_t>(blocks, (warps_needed + bthreads / 32 - 1) / (bthreads / 32));
     blocks = std::max<uint64_t>(blocks, 1);
     const size_t smem = rb2dev::job_smem_bytes(a.n_jobs, a.jobs == nullptr);
-    const unsigned g = (unsigned)blocks;
-    switch (bi * 3 + ri) {
-    case 0: launch_variant<64, 64>(a, g, smem, s); break;
-    case 1: launch_variant<64, 48>(a, g, smem, s); break;
-    case 2: launch_variant<64, 40>(a, g, smem, s); break;
-    case 4: launch_variant<128, 48>(a, g, smem, s); break;
-    case 5: launch_variant<128, 40>(a, g, smem, s); break;
-    case 6: launch_variant<256, 64>(a, g, smem, s); break;
-    case 7: launch_variant<256, 48>(a, g, smem, s); break;
-    case 8: launch_variant<256, 40>(a, g, smem, s); break;
-    default: launch_variant<128, 64>(a, g, smem, s); break;
-    }
+    if (wide) launch_shape<true>(bi * 3 + ri, a, (unsigned)blocks, smem, s);
+    else launch_shape<false>(bi * 3 + ri, a, (unsigned)blocks, smem, s);
     RB2_CUDA(cudaGetLastError(), "trace launch");
     return RB2_OK;
 }
@@ -171,6 +179,71 @@ void reorder_nodes(const std::vector<uint32_t>& in, uint32_t order, std::vector<
     }
 }
 
+// Collapses a binary Compact2 node buffer (16 words per node, child = node
+// index * 4 or ~Woop offset) into the 4-wide layout of rb2_traverse.cuh:
+// starting from a node's two children, the inner entry with the largest box
+// surface area is replaced by its two children until four entries are held
+// or none is inner.  Child boxes keep their exact values, so every child test
+// is the binary test of the same box.  Nodes are emitted breadth-first;
+// `depth` returns the deepest wide level.
+void collapse_wide4(const std::vector<uint32_t>& bin, std::vector<uint32_t>& wide, uint32_t& depth)
+{
+    struct Entry {
+        int32_t child;
+        float lo[3], hi[3];
+    };
+    auto entry_of = [&](uint32_t node, int k) {
+        const uint32_t* w = &bin[(size_t)node * 16];
+        Entry e;
+        e.child = (int32_t)w[12 + k];
+        const int xo = k ? 4 : 0, zo = k ? 10 : 8;
+        e.lo[0] = u2f(w[xo + 0]); e.hi[0] = u2f(w[xo + 1]);
+        e.lo[1] = u2f(w[xo + 2]); e.hi[1] = u2f(w[xo + 3]);
+        e.lo[2] = u2f(w[zo + 0]); e.hi[2] = u2f(w[zo + 1]);
+        return e;
+    };
+    auto area = [](const Entry& e) {
+        const float dx = e.hi[0] - e.lo[0], dy = e.hi[1] - e.lo[1], dz = e.hi[2] - e.lo[2];
+        return dx * dy + dy * dz + dz * dx;
+    };
+    wide.clear();
+    std::vector<uint32_t> queue{0}, level{0};
+    depth = 0;
+    for (size_t h = 0; h < queue.size(); h++) {
+        std::vector<Entry> es = {entry_of(queue[h], 0), entry_of(queue[h], 1)};
+        while (es.size() < 4) {
+            int best = -1;
+            float best_a = -1.0f;
+            for (int i = 0; i < (int)es.size(); i++)
+                if (es[i].child >= 0 && area(es[i]) > best_a) { best = i; best_a = area(es[i]); }
+            if (best < 0) break;
+            const uint32_t node = (uint32_t)es[best].child / 4;
+            es[best] = entry_of(node, 0);
+            es.insert(es.begin() + best + 1, entry_of(node, 1));
+        }
+        depth = std::max(depth, level[h] + 1);
+        const size_t base = wide.size();
+        wide.resize(base + 32, 0u);
+        for (int i = 0; i < 4; i++) {
+            uint32_t child = (uint32_t)rb2dev::kWideEmpty;
+            if (i < (int)es.size()) {
+                const Entry& e = es[i];
+                wide[base + 0 + i] = f2u(e.lo[0]); wide[base + 4 + i] = f2u(e.hi[0]);
+                wide[base + 8 + i] = f2u(e.lo[1]); wide[base + 12 + i] = f2u(e.hi[1]);
+                wide[base + 16 + i] = f2u(e.lo[2]); wide[base + 20 + i] = f2u(e.hi[2]);
+                if (e.child >= 0) {
+                    child = (uint32_t)(queue.size() * 8);  // float4 offset of the wide node
+                    queue.push_back((uint32_t)e.child / 4);
+                    level.push_back(level[h] + 1);
+                } else {
+                    child = (uint32_t)e.child;
+                }
+            }
+            wide[base + 24 + i] = child;
+        }
+    }
+}
+
 }  // namespace
 
 struct rb2_tracer {
@@ -181,7 +254,10 @@ struct rb2_tracer {
     uint32_t* d_triidx = nullptr;
     uint64_t n_nodes_u4 = 0, n_woop_u4 = 0;
     std::vector<uint32_t> host_nodes;  // DFS order, kept for re-layout
-    uint32_t node_order = RB2_NODE_ORDER_DFS;
+    uint32_t node_order = RB2_NODE_ORDER_DFS;   // layout the bulk traversals use
+    uint32_t binary_order = RB2_NODE_ORDER_DFS; // order held by d_nodes (integrators use it)
+    float4* d_wide = nullptr;                   // 4-wide layout, built on first use
+    uint64_t n_wide_u4 = 0;
     unsigned long long* d_counters = nullptr;  // kSlots queue heads
     unsigned int* d_status = nullptr;
     uint32_t slot = 0;
@@ -206,7 +282,7 @@ namespace {
 rb2dev::JobDesc job_of(const rb2_tracer* t, const float* rays, uint64_t n, uint32_t mode, const uint8_t* mask, void* out)
 {
     rb2dev::JobDesc d{};
-    d.nodes = t->d_nodes;
+    d.nodes = t->node_order == RB2_NODE_ORDER_WIDE4 ? t->d_wide : t->d_nodes;
     d.woop = t->d_woop;
     d.triidx = t->d_triidx;
     d.rays = reinterpret_cast<const float4*>(rays);
@@ -233,7 +309,7 @@ int trace_single(rb2_tracer* t, const float* d_rays, uint64_t n, uint32_t mode, 
     a.counter = counter;
     a.status = t->d_status;
     const uint32_t block = t->cfg.block_threads ? t->cfg.block_threads : kDefaultBlock;
-    return launch_jobs(a, n, block, t->cfg.ctas_per_sm, t->cfg.regs, t->occ, s);
+    return launch_jobs(a, n, block, t->cfg.ctas_per_sm, t->cfg.regs, t->node_order == RB2_NODE_ORDER_WIDE4, t->occ, s);
 }
 
 bool valid_regs(uint32_t r) { return r == 0 || r == 64 || r == 48 || r == 40; }
@@ -298,6 +374,7 @@ int rb2_tracer_destroy(rb2_tracer* t)
     cudaFree(t->d_rays);
     cudaFree(t->d_hits);
     cudaFree(t->d_mask);
+    cudaFree(t->d_wide);
     delete t;
     return RB2_OK;
 }
@@ -316,12 +393,36 @@ int rb2_tracer_set_launch(rb2_tracer* t, const rb2_launch_config* cfg)
 int rb2_tracer_set_node_order(rb2_tracer* t, uint32_t order)
 {
     if (!t) return fail(RB2_EINVAL, "null argument");
-    if (order != RB2_NODE_ORDER_DFS && order != RB2_NODE_ORDER_BFS) return fail(RB2_EINVAL, "unknown node order");
+    if (order > RB2_NODE_ORDER_WIDE4) return fail(RB2_EINVAL, "unknown node order");
     if (order == t->node_order) return RB2_OK;
-    std::vector<uint32_t> nodes;
-    reorder_nodes(t->host_nodes, order, nodes);
-    RB2_CUDA(cudaDeviceSynchronize(), "sync before re-layout");
-    RB2_CUDA(cudaMemcpy(t->d_nodes, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice), "node upload");
+    if (order == RB2_NODE_ORDER_WIDE4) {
+        if (!t->d_wide) {
+            std::vector<uint32_t> wide;
+            uint32_t depth = 0;
+            collapse_wide4(t->host_nodes, wide, depth);
+            // Each wide level pushes at most three entries.
+            if (3u * depth + 2u > (uint32_t)rb2dev::kStackSizeWide)
+                return fail(RB2_ENOTSUP, "tree too deep for the 4-wide layout's stack");
+            float4* d = nullptr;
+            RB2_CUDA(cudaMalloc(&d, wide.size() * 4), "wide node allocation");
+            if (cudaMemcpy(d, wide.data(), wide.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+                cudaFree(d);
+                return fail(RB2_ECUDA, "wide node upload");
+            }
+            t->d_wide = d;
+            t->n_wide_u4 = wide.size() / 4;
+            t->device_bytes += wide.size() * 4;
+        }
+        t->node_order = order;
+        return RB2_OK;
+    }
+    if (order != t->binary_order) {
+        std::vector<uint32_t> nodes;
+        reorder_nodes(t->host_nodes, order, nodes);
+        RB2_CUDA(cudaDeviceSynchronize(), "sync before re-layout");
+        RB2_CUDA(cudaMemcpy(t->d_nodes, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice), "node upload");
+        t->binary_order = order;
+    }
     t->node_order = order;
     return RB2_OK;
 }
@@ -397,6 +498,7 @@ struct rb2_batch {
     std::vector<rb2_tracer*> tracers;
     rb2dev::JobDesc* d_jobs = nullptr;
     unsigned long long* d_start = nullptr;
+    std::vector<rb2_tracer*> unique_tracers;
     unsigned long long* d_counter = nullptr;
     unsigned int* d_status = nullptr;
     uint64_t total = 0;
@@ -428,7 +530,31 @@ int batch_enqueue(rb2_batch* b, cudaStream_t s)
     a.counter = b->d_counter;
     a.status = b->d_status;
     return launch_jobs(a, b->total, b->cfg.block_threads ? b->cfg.block_threads : kDefaultBlock, b->cfg.ctas_per_sm,
-                       b->cfg.regs, b->occ, s);
+                       b->cfg.regs, b->cfg.node_order == RB2_NODE_ORDER_WIDE4, b->occ, s);
+}
+
+// The job table points at each tracer's current layout; a tracer shared
+// with another batch may have been switched since.
+int batch_check_layout(const rb2_batch* b)
+{
+    for (const rb2_tracer* t : b->unique_tracers)
+        if ((t->node_order == RB2_NODE_ORDER_WIDE4) != (b->cfg.node_order == RB2_NODE_ORDER_WIDE4))
+            return fail(RB2_EINVAL, "a tracer's node layout changed since rb2_batch_set_config; set it again");
+    return RB2_OK;
+}
+
+int batch_upload_jobs(rb2_batch* b)
+{
+    const uint32_t n = (uint32_t)b->jobs.size();
+    if (n == 0) return RB2_OK;
+    std::vector<rb2dev::JobDesc> descs(n);
+    for (uint32_t i = 0; i < n; i++) {
+        const rb2_trace_job& j = b->jobs[i];
+        descs[i] = job_of(j.tracer, j.d_rays, j.n, j.mode, j.d_mask, j.d_out);
+    }
+    RB2_CUDA(cudaDeviceSynchronize(), "sync before job upload");
+    RB2_CUDA(cudaMemcpy(b->d_jobs, descs.data(), sizeof(rb2dev::JobDesc) * n, cudaMemcpyHostToDevice), "job upload");
+    return RB2_OK;
 }
 
 }  // namespace
@@ -454,7 +580,23 @@ int rb2_batch_create(const rb2_trace_job* jobs, uint32_t n_jobs, rb2_batch** out
         start[i + 1] = start[i] + j.n;
     }
     b->jobs.assign(jobs, jobs + n_jobs);
+    for (const auto& j : b->jobs)
+        if (std::find(b->unique_tracers.begin(), b->unique_tracers.end(), j.tracer) == b->unique_tracers.end())
+            b->unique_tracers.push_back(j.tracer);
     b->total = start[n_jobs];
+    // The batch starts in the layout its tracers share (binary DFS when they differ).
+    const uint32_t first = b->unique_tracers.empty() ? RB2_NODE_ORDER_DFS : b->unique_tracers[0]->node_order;
+    bool same = true;
+    for (const rb2_tracer* t : b->unique_tracers) same &= t->node_order == first;
+    b->cfg.node_order = same ? first : RB2_NODE_ORDER_DFS;
+    if (!same) {
+        for (rb2_tracer* t : b->unique_tracers) {
+            int rc2 = rb2_tracer_set_node_order(t, RB2_NODE_ORDER_DFS);
+            if (rc2) return rc2;
+        }
+        for (uint32_t i = 0; i < n_jobs; i++)
+            descs[i] = job_of(jobs[i].tracer, jobs[i].d_rays, jobs[i].n, jobs[i].mode, jobs[i].d_mask, jobs[i].d_out);
+    }
     int rc = occupancy(b->occ);
     if (rc) return rc;
     cudaError_t e;
@@ -490,18 +632,15 @@ int rb2_batch_set_config(rb2_batch* b, const rb2_batch_config* cfg)
     if (cfg->block_threads && cfg->block_threads != 64 && cfg->block_threads != 128 && cfg->block_threads != 256)
         return fail(RB2_ENOTSUP, "block_threads must be 64, 128 or 256");
     if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
-    if (cfg->node_order > RB2_NODE_ORDER_BFS) return fail(RB2_EINVAL, "unknown node order");
+    if (cfg->node_order > RB2_NODE_ORDER_WIDE4) return fail(RB2_EINVAL, "unknown node order");
     if (!valid_regs(cfg->regs)) return fail(RB2_ENOTSUP, "regs must be 64, 48 or 40");
     b->drop_graph();
-    b->cfg = *cfg;
-    std::vector<rb2_tracer*> seen;
-    for (const auto& j : b->jobs) {
-        if (std::find(seen.begin(), seen.end(), j.tracer) != seen.end()) continue;
-        seen.push_back(j.tracer);
-        int rc = rb2_tracer_set_node_order(j.tracer, cfg->node_order);
+    for (rb2_tracer* t : b->unique_tracers) {
+        int rc = rb2_tracer_set_node_order(t, cfg->node_order);
         if (rc) return rc;
     }
-    return RB2_OK;
+    b->cfg = *cfg;
+    return batch_upload_jobs(b);
 }
 
 int rb2_batch_get_config(const rb2_batch* b, rb2_batch_config* cfg)
@@ -533,6 +672,8 @@ int rb2_batch_launch(rb2_batch* b, void* stream)
     if (!b) return fail(RB2_EINVAL, "null argument");
     cudaStream_t s = (cudaStream_t)stream;
     if (b->total == 0) return RB2_OK;
+    int rc = batch_check_layout(b);
+    if (rc) return rc;
     if (b->exec) {
         RB2_CUDA(cudaGraphLaunch(b->exec, s), "graph launch");
         return RB2_OK;
@@ -549,7 +690,7 @@ int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream)
     return RB2_OK;
 }
 
-// Coordinate-descent autotuner over node order, block shape, resident CTAs
+// Coordinate-descent autotuner over node layout (DFS, BFS, 4-wide), block shape, resident CTAs
 // per SM, fetch threshold and queue chunk: each candidate is timed with CUDA
 // events (median of `reps` launches after one warm-up) and the fastest kept.
 int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best_out, double* best_ms_out)
@@ -587,7 +728,7 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     double best_ms = 0;
     int rc = time_cfg(best, best_ms);
     if (rc) return rc;
-    const uint32_t orders[] = {RB2_NODE_ORDER_DFS, RB2_NODE_ORDER_BFS};
+    const uint32_t orders[] = {RB2_NODE_ORDER_DFS, RB2_NODE_ORDER_BFS, RB2_NODE_ORDER_WIDE4};
     const uint32_t blocks[] = {64, 128, 256};
     const uint32_t regs[] = {64, 48, 40};
     const uint32_t thresholds[] = {8, 16, 20, 24, 28};
@@ -605,7 +746,8 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
                 if (ms < best_ms) { best = c; best_ms = ms; }
             }
         }
-        const int maxc = std::max(1, b->occ.per_sm[block_index(best.block_threads)][regs_index(best.regs)]);
+        const int maxc = std::max(
+            1, b->occ.per_sm[block_index(best.block_threads)][regs_index(best.regs)][best.node_order == RB2_NODE_ORDER_WIDE4]);
         for (int k : {maxc, std::max(1, maxc * 3 / 4), std::max(1, maxc / 2)}) {
             rb2_batch_config c = best; c.ctas_per_sm = (uint32_t)k; double ms;
             if ((rc = time_cfg(c, ms))) return rc;

@@ -24,6 +24,14 @@ namespace rb2dev {
 
 constexpr int kSentinel = 0x76543210;
 constexpr int kStackSize = 64;
+// 4-wide node layout (tracer layout RB2_NODE_ORDER_WIDE4): a binary Compact2
+// tree collapsed so each node holds up to four child boxes, 128 bytes:
+// float4 lo.x[4], hi.x[4], lo.y[4], hi.y[4], lo.z[4], hi.z[4], int4 child[4],
+// one unused float4.  Children keep the Compact2 encoding (inner = float4
+// offset of the wide node, leaf = ~Woop offset); kWideEmpty marks an unused
+// slot.  A wide node pushes up to three children, so its stack is deeper.
+constexpr int kWideEmpty = 0x7FFFFFFF;
+constexpr int kStackSizeWide = 192;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kStatusStack = 1u;
 
@@ -99,12 +107,34 @@ __device__ __forceinline__ void setup_ray(Lane& L, float4 o4, float4 d4)
     L.hitIndex = -1;
 }
 
-template <class Source>
+// One child slot of a wide node: the same slab and span arithmetic as the
+// binary node test, so a child passes here exactly when it passes there.
+__device__ __forceinline__ void wide_span(const Lane& L, float lox, float hix, float loy, float hiy, float loz, float hiz,
+                                          float& cmin, float& cmax)
+{
+    const float a0 = __fmaf_rn(lox, L.idx, -L.oodx), a1 = __fmaf_rn(hix, L.idx, -L.oodx);
+    const float b0 = __fmaf_rn(loy, L.idy, -L.oody), b1 = __fmaf_rn(hiy, L.idy, -L.oody);
+    const float c0 = __fmaf_rn(loz, L.idz, -L.oodz), c1 = __fmaf_rn(hiz, L.idz, -L.oodz);
+    cmin = span_begin(a0, a1, b0, b1, c0, c1, L.tmin);
+    cmax = span_end(a0, a1, b0, b1, c0, c1, L.hitT);
+}
+
+// Orders (key, child) pairs so key[0] is the smallest.
+__device__ __forceinline__ void cswap(float& ka, int& ca, float& kb, int& cb)
+{
+    if (kb < ka) {
+        const float tk = ka; ka = kb; kb = tk;
+        const int tc = ca; ca = cb; cb = tc;
+    }
+}
+
+template <class Source, bool WIDE = false>
 __device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_threshold, unsigned int* status)
 {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
-    int stack[kStackSize + 2];
+    constexpr int kStack = WIDE ? kStackSizeWide : kStackSize;
+    int stack[kStack + 2];
     int sp = 0;
     Lane L;
     L.nodeAddr = kSentinel;
@@ -145,7 +175,7 @@ __device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_thr
             for (;;) {
                 const bool in = has_ray && (unsigned)L.nodeAddr < (unsigned)kSentinel;
                 if (!__any_sync(kFull, in)) break;
-                if (in) {
+                if (in && !WIDE) {
                     const float4* np = L.nodes + L.nodeAddr;
                     float4 n0xy, n1xy, nz, cn;
                     load_node(np, n0xy, n1xy, nz, cn);
@@ -188,6 +218,50 @@ __device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_thr
                                 stack[++sp] = c1;
                             }
                         }
+                    }
+                    if (L.nodeAddr < 0 && L.leafAddr >= 0) {
+                        L.leafAddr = L.nodeAddr;
+                        L.nodeAddr = stack[sp--];
+                    }
+                }
+                if (WIDE && in) {
+                    const float4* np = L.nodes + L.nodeAddr;
+                    const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+                    const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+                    const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
+                    float k0, k1, k2, k3, m;
+                    wide_span(L, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, k0, m);
+                    if (!(ch.x != kWideEmpty && m >= k0)) k0 = __int_as_float(0x7f800000);
+                    wide_span(L, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, k1, m);
+                    if (!(ch.y != kWideEmpty && m >= k1)) k1 = __int_as_float(0x7f800000);
+                    wide_span(L, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, k2, m);
+                    if (!(ch.z != kWideEmpty && m >= k2)) k2 = __int_as_float(0x7f800000);
+                    wide_span(L, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, k3, m);
+                    if (!(ch.w != kWideEmpty && m >= k3)) k3 = __int_as_float(0x7f800000);
+                    const int hits = (k0 != __int_as_float(0x7f800000)) + (k1 != __int_as_float(0x7f800000)) +
+                                     (k2 != __int_as_float(0x7f800000)) + (k3 != __int_as_float(0x7f800000));
+                    int c0 = ch.x, c1 = ch.y, c2 = ch.z, c3 = ch.w;
+                    // Five compare-exchanges sort four keys (nearest entry first).
+                    cswap(k0, c0, k1, c1);
+                    cswap(k2, c2, k3, c3);
+                    cswap(k0, c0, k2, c2);
+                    cswap(k1, c1, k3, c3);
+                    cswap(k1, c1, k2, c2);
+                    if (hits == 0) {
+                        L.nodeAddr = stack[sp--];
+                    } else if (sp + hits - 1 > kStack) {
+                        // Unreachable for trees whose wide depth was validated; a
+                        // corrupt tree abandons the ray and reports it.
+                        atomicOr(status, kStatusStack);
+                        L.nodeAddr = kSentinel;
+                        L.leafAddr = 0;
+                        L.hitIndex = -1;
+                    } else {
+                        // Farther children first, so the next nearest pops first.
+                        if (hits > 3) stack[++sp] = c3;
+                        if (hits > 2) stack[++sp] = c2;
+                        if (hits > 1) stack[++sp] = c1;
+                        L.nodeAddr = c0;
                     }
                     if (L.nodeAddr < 0 && L.leafAddr >= 0) {
                         L.leafAddr = L.nodeAddr;

@@ -1,7 +1,10 @@
 """GPU tests of the batched job-table launch (config 4 pattern): many scenes
 and uneven ray batches in one persistent launch must give exactly the
 results of per-scene launches, for every launch configuration the autotuner
-can pick, including graph replay and the breadth-first node order."""
+can pick, including graph replay and the breadth-first node order.  With the
+4-wide node layout the traversal order differs, so closest hits must be equal
+except at confirmed ties, any-hit jobs must agree on occlusion, and
+occlusion jobs must be byte-identical."""
 import numpy as np
 import pytest
 
@@ -41,6 +44,27 @@ def _check(outs, plain, torch):
         assert torch.equal(o, p)
 
 
+MODES = None
+
+
+def _check_any_layout(rb, orc, scenes, jobs, outs, plain, torch):
+    """Layout-independent equality (see the module docstring)."""
+    from parity import compare_closest
+    torch.cuda.synchronize()
+    for (sc, bvh, r), (tr, d, mode, o, _), p in zip(scenes, jobs, plain):
+        got, ref = o.cpu().numpy(), p.cpu().numpy()
+        if mode == rb.MODE_OCCLUSION or r.shape[0] == 0:
+            assert np.array_equal(got, ref)
+        elif mode == rb.MODE_ANY:
+            assert np.array_equal(got[:, 0] >= 0, ref[:, 0] >= 0)
+        else:
+            nodes, woop, tri = bvh.buffers_view()
+            f = ref.view(np.float32)
+            want = {"prim": ref[:, 0], "t": f[:, 1], "u": f[:, 2], "v": f[:, 3]}
+            ties, bad, first = compare_closest(orc, got, want, woop, tri, r)
+            assert bad == 0, f"ray {first}"
+
+
 def test_batch_equals_plain_launches(rb, orc, cuda):
     scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
     batch = rb.TraceBatch(jobs)
@@ -58,24 +82,29 @@ def test_batch_equals_plain_launches(rb, orc, cuda):
 @pytest.mark.parametrize("cfg", [
     dict(block_threads=64), dict(block_threads=256), dict(chunk=4), dict(chunk=8, fetch_threshold=8),
     dict(node_order=1), dict(ctas_per_sm=2, fetch_threshold=32), dict(regs=48), dict(regs=40, block_threads=256),
-    dict(regs=40, block_threads=64, chunk=2),
+    dict(regs=40, block_threads=64, chunk=2), dict(node_order=2), dict(node_order=2, regs=48, block_threads=256),
+    dict(node_order=2, regs=40, chunk=4),
 ])
-def test_batch_configs_give_identical_results(rb, cuda, cfg):
+def test_batch_configs_give_identical_results(rb, orc, cuda, cfg):
     scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
     batch = rb.TraceBatch(jobs)
     batch.set_config(**cfg)
     for o in outs:
         o.fill_(7)
     batch.launch()
-    _check(outs, plain, cuda)
+    if cfg.get("node_order") == 2:
+        _check_any_layout(rb, orc, scenes, jobs, outs, plain, cuda)
+    else:
+        _check(outs, plain, cuda)
+    assert batch.status() == 0
     batch.set_config(node_order=0)
 
 
-def test_graph_replay_and_autotune(rb, cuda):
+def test_graph_replay_and_autotune(rb, orc, cuda):
     scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
     batch = rb.TraceBatch(jobs)
     best, ms = batch.autotune(reps=2)
-    assert ms > 0 and best["block_threads"] in (64, 128, 256)
+    assert ms > 0 and best["block_threads"] in (64, 128, 256) and best["node_order"] in (0, 1, 2)
     s = cuda.cuda.Stream()
     batch.capture(s)
     for _ in range(2):
@@ -84,8 +113,46 @@ def test_graph_replay_and_autotune(rb, cuda):
         cuda.cuda.synchronize()
         batch.launch(s)
         s.synchronize()
-        _check(outs, plain, cuda)
+        _check_any_layout(rb, orc, scenes, jobs, outs, plain, cuda)
     batch.set_config(node_order=0)
+
+
+def test_wide_layout_single_tracer_and_layout_guard(rb, orc, cuda):
+    """A tracer switched to the 4-wide layout traces like the binary one
+    (closest hits equal but for confirmed ties, occlusion identical); a batch
+    whose tracer was switched by someone else refuses to launch until its
+    configuration is set again."""
+    from parity import compare_closest
+    sc = rb.heightfield_for_triangles(seed=15, n_tris=300_000, n_boxes=40)
+    bvh = rb.BVH(sc)
+    tr = rb.CudaTracer(bvh)
+    r, _ = rb.surface_rays(sc, seed=16, n=200_000)
+    d = cuda.from_numpy(r).cuda()
+    a = tr.trace(d).cpu().numpy()
+    occ_a = tr.trace_occlusion(d).cpu().numpy()
+    assert rb.lib().rb2_tracer_set_node_order(tr.handle, 2) == 0
+    b = tr.trace(d).cpu().numpy()
+    occ_b = tr.trace_occlusion(d).cpu().numpy()
+    assert np.array_equal(occ_a, occ_b)
+    nodes, woop, tri = bvh.buffers_view()
+    f = a.view(np.float32)
+    ties, bad, first = compare_closest(orc, b, {"prim": a[:, 0], "t": f[:, 1], "u": f[:, 2], "v": f[:, 3]}, woop, tri, r)
+    assert bad == 0, f"ray {first}"
+    want = orc.trace(nodes, woop, tri, r)
+    ties, bad, first = compare_closest(orc, b, {k: want[k] for k in ("prim", "t", "u", "v")}, woop, tri, r)
+    assert bad == 0, f"ray {first} vs oracle"
+    # integrator-facing device view stays binary
+    assert tr.get_bvh()["n_nodes_u4"] == nodes.shape[0]
+    out = cuda.empty((1000, 4), dtype=cuda.int32, device="cuda")
+    batch = rb.TraceBatch([(tr, d[:1000], rb.MODE_CLOSEST, out, None)])
+    batch.launch()
+    assert rb.lib().rb2_tracer_set_node_order(tr.handle, 0) == 0
+    with pytest.raises(rb.Rb2Error, match="layout"):
+        batch.launch()
+    batch.set_config(node_order=0)
+    batch.launch()
+    cuda.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), a[:1000])
 
 
 def test_bfs_node_order_on_single_tracer(rb, cuda):
