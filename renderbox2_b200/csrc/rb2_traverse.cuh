@@ -63,6 +63,15 @@ struct Lane {
     __device__ __forceinline__ void set_tag(uint32_t mode, uint32_t job) { tag = (mode << 30) | (job & kJobMask); }
 };
 
+// One 32-byte read-only load (sm_100 256-bit ld.global.nc.v8); `p` must be
+// 32-byte aligned.
+__device__ __forceinline__ void ldg_v8(const float4* p, float4& a, float4& b)
+{
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
+
 // A 64-byte Compact2 node as four 128-bit read-only loads.  (Two 256-bit
 // ld.global.nc.v8 loads halve the L1 sector lookups but measured 1-2 %
 // slower at the tuned register budget: the kernel is bound by L2 latency
@@ -226,8 +235,14 @@ __device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_thr
                 }
                 if (WIDE && in) {
                     const float4* np = L.nodes + L.nodeAddr;
-                    const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
-                    const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+                    // A wide node is 128-byte aligned: three 256-bit loads for the
+                    // boxes, one 128-bit load for the children.  (Measured: four
+                    // 256-bit loads of per-child records were slower, and seven
+                    // 128-bit loads slower still.)
+                    float4 lx, hx, ly, hy, lz, hz;
+                    ldg_v8(np + 0, lx, hx);
+                    ldg_v8(np + 2, ly, hy);
+                    ldg_v8(np + 4, lz, hz);
                     const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
                     float k0, k1, k2, k3, m;
                     wide_span(L, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, k0, m);
