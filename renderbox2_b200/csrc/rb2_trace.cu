@@ -764,6 +764,20 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
             if (ms < best_ms) { best = c; best_ms = ms; }
         }
     }
+    // Last look at the layout under the final launch shape, each candidate
+    // re-timed together with the incumbent so drift between passes cannot
+    // decide it.
+    {
+        double inc_ms;
+        if ((rc = time_cfg(best, inc_ms))) return rc;
+        best_ms = inc_ms;
+        for (uint32_t o : orders) {
+            if (o == best.node_order) continue;
+            rb2_batch_config c = best; c.node_order = o; double ms;
+            if ((rc = time_cfg(c, ms))) return rc;
+            if (ms < best_ms) { best = c; best_ms = ms; }
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     rc = rb2_batch_set_config(b, &best);
