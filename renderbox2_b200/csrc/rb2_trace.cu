@@ -701,6 +701,18 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     cudaEvent_t e0, e1;
     RB2_CUDA(cudaEventCreate(&e0), "event");
     RB2_CUDA(cudaEventCreate(&e1), "event");
+    // Each timed launch starts with a cold L2 (a write of twice its size,
+    // outside the timing), as a launch does after other work.
+    int dev = 0, l2 = 0;
+    RB2_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    RB2_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev), "L2 size");
+    const size_t flush_bytes = std::max<size_t>(2 * (size_t)l2, 1 << 20);
+    void* flush = nullptr;
+    if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) flush = nullptr;  // tune warm if memory is short
+    struct FlushFree {
+        void* p;
+        ~FlushFree() { if (p) cudaFree(p); }
+    } flush_guard{flush};
     auto time_cfg = [&](const rb2_batch_config& c, double& ms) -> int {
         int rc = rb2_batch_set_config(b, &c);
         if (rc) return rc;
@@ -708,6 +720,7 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
         if (rc) return rc;
         std::vector<float> t(reps);
         for (uint32_t r = 0; r < reps; r++) {
+            if (flush) RB2_CUDA(cudaMemsetAsync(flush, (int)(r & 0xFF), flush_bytes, s), "L2 flush");
             RB2_CUDA(cudaEventRecord(e0, s), "event");
             rc = batch_enqueue(b, s);
             if (rc) return rc;
