@@ -690,7 +690,8 @@ int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream)
     return RB2_OK;
 }
 
-// Coordinate-descent autotuner over node layout (DFS, BFS, 4-wide), block shape, resident CTAs
+// Coordinate-descent autotuner: node layout (DFS, BFS, 4-wide) x block shape x
+// register budget jointly, then resident CTAs
 // per SM, fetch threshold and queue chunk: each candidate is timed with CUDA
 // events (median of `reps` launches after one warm-up) and the fastest kept.
 int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best_out, double* best_ms_out)
@@ -747,16 +748,17 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     const uint32_t thresholds[] = {8, 16, 20, 24, 28};
     const uint32_t chunks[] = {1, 2, 4, 8};
     for (int pass = 0; pass < 2; pass++) {
+        // Layout, block shape and register budget interact (the 4-wide layout
+        // needs more registers), so they are searched jointly.
         for (uint32_t o : orders) {
-            rb2_batch_config c = best; c.node_order = o; double ms;
-            if ((rc = time_cfg(c, ms))) return rc;
-            if (ms < best_ms) { best = c; best_ms = ms; }
-        }
-        for (uint32_t bl : blocks) {
-            for (uint32_t rg : regs) {
-                rb2_batch_config c = best; c.block_threads = bl; c.regs = rg; c.ctas_per_sm = 0; double ms;
-                if ((rc = time_cfg(c, ms))) return rc;
-                if (ms < best_ms) { best = c; best_ms = ms; }
+            for (uint32_t bl : blocks) {
+                for (uint32_t rg : regs) {
+                    rb2_batch_config c = best;
+                    c.node_order = o; c.block_threads = bl; c.regs = rg; c.ctas_per_sm = 0;
+                    double ms;
+                    if ((rc = time_cfg(c, ms))) return rc;
+                    if (ms < best_ms) { best = c; best_ms = ms; }
+                }
             }
         }
         const int maxc = std::max(
