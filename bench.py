@@ -297,9 +297,9 @@ def run_rb2(args, rank, world, local_rank):
     # DRAM traffic per launch: the ncu capture of the same batched kernel on
     # 8 scenes x 500k triangles with 4.19M incoherent rays, half closest hit /
     # half occlusion (profiles/k_trace_jobs_batched_8x500k_full.md), measured
-    # 657.7 MB of DRAM traffic against 7961.2 MB of algorithmic bytes; scaled
+    # 618.5 MB of DRAM traffic against 7961.2 MB of algorithmic bytes; scaled
     # to this launch by algorithmic bytes.
-    traffic = alg_per_launch * (657.7 / 7961.2)
+    traffic = alg_per_launch * (618.5 / 7961.2)
 
     cpu_baseline = builder = None
     if rank == 0 and world == 1:

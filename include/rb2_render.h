@@ -169,6 +169,11 @@ typedef struct rb2_integrator rb2_integrator;
 int rb2_integrator_create(rb2_tracer* tracer, const rb2_scene_dev* scene, rb2_integrator** out);
 int rb2_integrator_destroy(rb2_integrator* it);
 int rb2_integrator_device_bytes(const rb2_integrator* it, uint64_t* bytes);
+/* Launch shape of the integrator's persistent traversals: block_threads 128
+ * or 256, regs 64 or 48, fetch_threshold (zero fields: 128, 48, 24, the
+ * fastest of the four shapes measured on configs 1-3, all within 3 % of each
+ * other; ctas_per_sm is ignored).  Images do not depend on the shape. */
+int rb2_integrator_set_launch(rb2_integrator* it, const rb2_launch_config* cfg);
 /* Film filter of the path tracer and BDPT (default RB2_FILTER_NONE); NULL resets. */
 int rb2_integrator_set_filter(rb2_integrator* it, const rb2_filter* f);
 

@@ -144,6 +144,7 @@ SIGNATURES = {
     "rb2_trace_isect": (C.c_int, [P, P, P, U32, I32, P, C.POINTER(IsectBuffer), P]),
     "rb2_filter_table": (C.c_int, [C.POINTER(Filter), P]),
     "rb2_scene_set_materials": (C.c_int, [P, C.POINTER(MaterialDesc), U32]),
+    "rb2_integrator_set_launch": (C.c_int, [P, C.POINTER(LaunchConfig)]),
     "rb2_material_query": (C.c_int, [P, I32, P, P, U32, P, P]),
     "rb2_film_develop": (C.c_int, [C.POINTER(Filter), U32, U32, U32, P, P, P, P]),
     "rb2_image_write_pfm": (C.c_int, [C.c_char_p, P, U32, U32]),

@@ -110,8 +110,11 @@ struct AoSource {
     }
 };
 
-template <int BLOCK, class Src>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_persistent(Src src, uint32_t fetch_threshold, unsigned int* status)
+// Integrator traversal: block BLOCK, register budget REGS (64: 32 warps per
+// SM, 48: 40 warps), binary Compact2 layout.
+template <int BLOCK, int REGS, class Src>
+__global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK)
+    k_persistent(Src src, uint32_t fetch_threshold, unsigned int* status)
 {
     persistent_trace(src, fetch_threshold, status);
 }
@@ -812,17 +815,29 @@ __global__ void k_pt_finalize(const float4* accum, uint32_t npix, float inv_spp,
 
 namespace {
 
-template <class Src>
-int launch_persistent(const Src& src, uint64_t work, int sms, unsigned int* status, cudaStream_t s)
+template <int B, int R, class Src>
+int launch_persistent_variant(const Src& src, uint64_t work, int sms, uint32_t threshold, unsigned int* status,
+                              cudaStream_t s)
 {
     int per_sm = 0;
-    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb2dev::k_persistent<128, Src>, 128, 0), "occupancy");
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb2dev::k_persistent<B, R, Src>, B, 0), "occupancy");
     uint64_t blocks = (uint64_t)sms * (uint64_t)std::max(1, per_sm);
-    blocks = std::min<uint64_t>(blocks, (work + 127) / 128);
+    blocks = std::min<uint64_t>(blocks, (work + B - 1) / B);
     blocks = std::max<uint64_t>(blocks, 1);
-    rb2dev::k_persistent<128, Src><<<(unsigned)blocks, 128, 0, s>>>(src, 20u, status);
+    rb2dev::k_persistent<B, R, Src><<<(unsigned)blocks, B, 0, s>>>(src, threshold, status);
     RB2_CUDA(cudaGetLastError(), "persistent launch");
     return RB2_OK;
+}
+
+template <class Src>
+int launch_persistent(const Src& src, uint64_t work, const rb2_integrator* it, unsigned int* status, cudaStream_t s)
+{
+    const uint32_t th = it->tr_threshold;
+    if (it->tr_block == 256)
+        return it->tr_regs == 48 ? launch_persistent_variant<256, 48>(src, work, it->sms, th, status, s)
+                                 : launch_persistent_variant<256, 64>(src, work, it->sms, th, status, s);
+    return it->tr_regs == 48 ? launch_persistent_variant<128, 48>(src, work, it->sms, th, status, s)
+                             : launch_persistent_variant<128, 64>(src, work, it->sms, th, status, s);
 }
 
 unsigned grid_for(uint64_t n, int sms) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 8)); }
@@ -1003,6 +1018,19 @@ int rb2_integrator_destroy(rb2_integrator* it)
     return RB2_OK;
 }
 
+int rb2_integrator_set_launch(rb2_integrator* it, const rb2_launch_config* cfg)
+{
+    if (!it || !cfg) return fail(RB2_EINVAL, "null argument");
+    if (cfg->block_threads && cfg->block_threads != 128 && cfg->block_threads != 256)
+        return fail(RB2_ENOTSUP, "integrator traversal block_threads must be 128 or 256");
+    if (cfg->regs && cfg->regs != 64 && cfg->regs != 48) return fail(RB2_ENOTSUP, "integrator regs must be 64 or 48");
+    if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
+    it->tr_block = cfg->block_threads ? cfg->block_threads : 128;
+    it->tr_regs = cfg->regs ? cfg->regs : 48;
+    it->tr_threshold = cfg->fetch_threshold ? cfg->fetch_threshold : 24;
+    return RB2_OK;
+}
+
 int rb2_integrator_device_bytes(const rb2_integrator* it, uint64_t* bytes)
 {
     if (!it || !bytes) return fail(RB2_EINVAL, "null argument");
@@ -1044,7 +1072,7 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
     src.samples = p->samples;
     src.radius = p->radius;
     src.seed = p->seed;
-    if ((rc = launch_persistent(src, src.n_slots, it->sms, bv.status, s))) return rc;
+    if ((rc = launch_persistent(src, src.n_slots, it, bv.status, s))) return rc;
     // 4. AO = unoccluded fraction (misses contribute 0, integrator_ao.cu:56-84).
     rb2dev::k_ao_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_hits, it->d_count, (uint32_t)npix, p->samples, d_ao);
     RB2_CUDA(cudaGetLastError(), "AO finalize");
@@ -1097,7 +1125,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
             rb2dev::QueueSource ext{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop), bv.triidx,
                                     ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext, rb2dev::kClosest,
                                     ps.hit, nullptr, nullptr};
-            if ((rc = launch_persistent(ext, paths, it->sms, bv.status, s))) return rc;
+            if ((rc = launch_persistent(ext, paths, it, bv.status, s))) return rc;
             rb2dev::k_pt_shade<<<g, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, s0, b, p->max_depth, p->rr_start, p->rr_prob,
                                                 ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L, ps.sray, ps.sc,
                                                 ps.qs, wc, cur);
@@ -1106,7 +1134,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
             rb2dev::QueueSource shadow{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop),
                                        bv.triidx, ps.qs, &wc->n_shadow, ps.sray, &wc->head_shadow,
                                        rb2dev::kOcclusion, nullptr, ps.L, ps.sc};
-            if ((rc = launch_persistent(shadow, paths, it->sms, bv.status, s))) return rc;
+            if ((rc = launch_persistent(shadow, paths, it, bv.status, s))) return rc;
             cur ^= 1u;
         }
         if (filtered)
@@ -1179,7 +1207,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
             rb2dev::QueueSource lsrc{bn, bw, bv.triidx, bd.lq[cur], &wc->n_ext[cur], bd.lray, &wc->head_ext,
                                      rb2dev::kClosest, bd.lhit, nullptr, nullptr};
-            if ((rc = launch_persistent(lsrc, NL, it->sms, bv.status, s))) return rc;
+            if ((rc = launch_persistent(lsrc, NL, it, bv.status, s))) return rc;
             rb2dev::k_bd_light_shade<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)iter * NL, d, Dl, p->rr_start, p->rr_prob,
                                                         bd.lq[cur], bd.lq[cur ^ 1u], bd.lray, bd.lhit, bd.lbeta, bd.s_pos,
                                                         bd.s_nrm, bd.s_beta, bd.s_valid, wc, cur);
@@ -1200,7 +1228,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
             rb2dev::QueueSource ext{bn, bw, bv.triidx, ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext,
                                     rb2dev::kClosest, ps.hit, nullptr, nullptr};
-            if ((rc = launch_persistent(ext, npix, it->sms, bv.status, s))) return rc;
+            if ((rc = launch_persistent(ext, npix, it, bv.status, s))) return rc;
             rb2dev::k_bd_cam_shade<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, iter, i, K, C, p->rr_start, p->rr_prob,
                                                       (float)NL, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L,
                                                       ps.sray, ps.sc, ps.qs, bd.cray, bd.cc, bd.cq, bd.d_pos, bd.d_nrm,
@@ -1209,10 +1237,10 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             rb2dev::k_bd_stats<<<1, 1, 0, s>>>(wc);
             rb2dev::QueueSource nee{bn, bw, bv.triidx, ps.qs, &wc->n_shadow, ps.sray, &wc->head_shadow,
                                     rb2dev::kOcclusion, nullptr, ps.L, ps.sc};
-            if ((rc = launch_persistent(nee, npix, it->sms, bv.status, s))) return rc;
+            if ((rc = launch_persistent(nee, npix, it, bv.status, s))) return rc;
             rb2dev::QueueSource con{bn, bw, bv.triidx, bd.cq, &wc->n_conn, bd.cray, &wc->head_conn,
                                     rb2dev::kOcclusion, nullptr, nullptr, bd.cc};
-            if ((rc = launch_persistent(con, npix * C, it->sms, bv.status, s))) return rc;
+            if ((rc = launch_persistent(con, npix * C, it, bv.status, s))) return rc;
             rb2dev::k_bd_conn_reduce<<<gc, 256, 0, s>>>(ps.q[cur], wc, cur, C, bd.cc, ps.L);
             RB2_CUDA(cudaGetLastError(), "BDPT connection reduce");
             cur ^= 1u;

@@ -80,6 +80,8 @@ struct rb2_integrator {
     rb2_tracer* tracer = nullptr;
     const rb2_scene_dev* scene = nullptr;
     int sms = 0;
+    // launch shape of the integrator's traversal kernels (rb2_integrator_set_launch)
+    uint32_t tr_block = 128, tr_regs = 48, tr_threshold = 24;
     // generic scratch
     float4* d_rays = nullptr; uint64_t cap_rays = 0;        // 2 per ray
     int4* d_hits = nullptr; uint64_t cap_hits = 0;

@@ -241,6 +241,12 @@ class Integrator:
         self._it = C.c_void_p()
         check(lib().rb2_integrator_create(tracer.handle, scene.handle, C.byref(self._it)))
 
+    def set_launch(self, block_threads: int = 0, regs: int = 0, fetch_threshold: int = 0):
+        """Launch shape of the integrator's traversal kernels (0 = default)."""
+        from ._native import LaunchConfig
+        c = LaunchConfig(block_threads, 0, fetch_threshold, regs)
+        check(lib().rb2_integrator_set_launch(self._it, C.byref(c)))
+
     def set_filter(self, f: "Filter | None"):
         """Film filter of render_pt / render_bdpt (None: per-pixel mean)."""
         if f is None:
