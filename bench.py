@@ -373,8 +373,12 @@ def run_workload(args, rank, local_rank):
         names = {"ao": "config 1: ambient occlusion", "pt": "config 2: wavefront path tracing",
                  "bdpt": "config 3: BDPT with light-vertex cache"}
         line = {"metric": "samples/s and Mrays/s", "workload": names[args.workload], **r}
-        if world_of_env() == 1 and args.cpu_sample_s > 0:
-            line["cpu_baseline"] = integrator_cpu_baseline(args.workload, keep)
+        if world_of_env() == 1:
+            base, counts = integrator_cpu_baseline(args.workload, keep)
+            if args.cpu_sample_s > 0:
+                line["cpu_baseline"] = base
+            if counts is not None:
+                line["roofline"] = integrator_roofline(args.workload, r, counts)
         print(json.dumps(line), flush=True)
 
 
@@ -383,35 +387,35 @@ def world_of_env() -> int:
 
 
 def integrator_cpu_baseline(kind, keep):
-    """The FP64 CPU integrators (oracle) on all host cores over a crop of the
+    """The FP64 CPU integrators (oracle) on all host cores over a sample of the
     same frame: config 1 at full size (all 512 x 512 pixels, 16 AO rays),
-    configs 2 and 3 on the centre 128 x 128 tile at the configs' spp."""
+    configs 2 and 3 on a grid of 128 x 72 pixels spread over the whole frame at
+    the configs' spp.  Also returns the oracle's canonical visit counts per
+    ray type over that sample (for the trace-stage roofline)."""
     import oracle
     c, scene, bvh = keep["config"], keep["scene"], keep["bvh"]
     W, H = c["width"], c["height"]
     cores = os.cpu_count() or 1
     bufs = bvh.buffers_view()
+    if not oracle.have_ref():
+        return {"unavailable": "reference camera library not built"}, None
+    oracle.counts_reset(True)
     if kind == "ao":
         ii, jj = np.meshgrid(np.arange(W), np.arange(H))
         xy = np.stack([ii.ravel() + 0.5, jj.ravel() + 0.5], 1).astype(np.float32)
-        rays = oracle.ref_camera_rays(keep["eye"], keep["lookat"], c["up"], W, H, c["fov"], xy) \
-            if oracle.have_ref() else None
-        if rays is None:
-            return {"unavailable": "reference camera library not built"}
+        rays = oracle.ref_camera_rays(keep["eye"], keep["lookat"], c["up"], W, H, c["fov"], xy)
         t0 = time.perf_counter()
         oracle.ao(bufs, scene.vertices, scene.indices, rays, c["ao_samples"], c["ao_radius"], seed=c["ao_seed"])
         dt = time.perf_counter() - t0
         samples = xy.shape[0] * c["ao_samples"]
         crop = f"full frame {W}x{H}, {c['ao_samples']} AO rays per pixel"
     else:
-        T = 128
-        x0, y0 = (W - T) // 2, (H - T) // 2
+        gx, gy = 128, 72
+        sx, sy = W // gx, H // gy
         spp = c["spp"]
-        ii, jj = np.meshgrid(np.arange(x0, x0 + T), np.arange(y0, y0 + T))
+        ii, jj = np.meshgrid(np.arange(gx) * sx + sx // 2, np.arange(gy) * sy + sy // 2)
         rng = np.random.Generator(np.random.PCG64(5))
         base = np.stack([ii.ravel(), jj.ravel()], 1)
-        if not oracle.have_ref():
-            return {"unavailable": "reference camera library not built"}
         lights = np.asarray(scene.light_ids_to_primitive_ids, np.uint32)
         if kind == "pt":
             xy = (np.repeat(base, spp, axis=0) + rng.uniform(0, 1, (base.shape[0] * spp, 2))).astype(np.float32)
@@ -429,10 +433,47 @@ def integrator_cpu_baseline(kind, keep):
                         seed=3)
             dt = time.perf_counter() - t0
         samples = base.shape[0] * spp
-        crop = f"centre {T}x{T} tile of the {W}x{H} frame at {spp} spp"
-    return {"value": round(samples / dt, 1), "unit": "samples/s", "cores": cores, "kind": "port",
-            "sample": f"{crop}: {samples:,} samples in {dt:.1f}s, FP64 CPU integrator (oracle), "
-                      f"OpenMP over {cores} threads"}
+        crop = f"{gx}x{gy} pixels on a stride-{sx}x{sy} grid over the {W}x{H} frame at {spp} spp"
+    counts = oracle.counts_read()
+    oracle.counts_reset(False)
+    return ({"value": round(samples / dt, 1), "unit": "samples/s", "cores": cores, "kind": "port",
+             "sample": f"{crop}: {samples:,} samples in {dt:.1f}s, FP64 CPU integrator (oracle), "
+                       f"OpenMP over {cores} threads"}, counts)
+
+
+def integrator_roofline(kind, r, counts):
+    """Trace-stage roofline of configs 1-3: algorithmic bytes of the frame's
+    rays (GPU ray counts per type x the oracle's mean bytes per ray of that
+    type, from its own rays of the same distributions) / the GPU time of the
+    traversal launches (CUDA events around each)."""
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    out_b = {"camera": 16, "extension": 16, "light": 16, "shadow": 1, "connection": 1}
+
+    def bpr(t):
+        c = counts[t]
+        if not c["rays"]:
+            return 0.0
+        return 32 + (64 * c["nodes"] + 48 * c["tris"] + 16 * c["leafterms"]) / c["rays"] + out_b[t]
+
+    st = r["stats"]
+    if kind == "ao":
+        npix = r["width"] * r["height"]
+        hit_frac = counts["shadow"]["rays"] / max(1, counts["camera"]["rays"] * (r["samples"] // npix))
+        gpu = {"camera": npix, "shadow": r["samples"] * hit_frac}
+    else:
+        gpu = {"camera": st["primary_rays"], "extension": st["extension_rays"], "shadow": st["shadow_rays"],
+               "connection": st["connection_rays"], "light": st["light_rays"]}
+    alg = sum(n * bpr(t) for t, n in gpu.items())
+    trace_s = st["trace_ms"] / 1e3
+    if trace_s <= 0:
+        return None
+    ach = alg / trace_s / 1e9
+    return {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
+            "traffic": None, "alg_bytes_per_frame": round(alg), "trace_ms": round(st["trace_ms"], 3),
+            "bytes_per_ray": {t: round(bpr(t), 1) for t in gpu},
+            "note": "peak = measured HBM copy; the BVHs of configs 1 and 2 fit the 126 MB L2, so the traversal "
+                    "there is L2-bound and frac can exceed what HBM alone would allow"}
 
 
 def cpu_baseline_run(scenes, budget_s: float):

@@ -232,11 +232,15 @@ typedef struct {
 } rb2_bdpt_params;
 int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_params* p, float* d_rgb, void* stream);
 
-/* Statistics of the last render on this integrator (rays traced per kind). */
+/* Statistics of the last render on this integrator (rays traced per kind);
+ * trace_ms = GPU time of its traversal launches (CUDA events around each),
+ * measured only while rb2_integrator_set_timing(it, 1) is on, else 0. */
 typedef struct {
     uint64_t primary_rays, extension_rays, shadow_rays, connection_rays, light_rays;
     uint64_t lvc_vertices;
+    double trace_ms;
 } rb2_render_stats;
+int rb2_integrator_set_timing(rb2_integrator* it, int on);
 int rb2_integrator_stats(rb2_integrator* it, rb2_render_stats* out, void* stream);
 
 #ifdef __cplusplus

@@ -195,6 +195,28 @@ def isect(verts, tris4, rays, hits):
     return out
 
 
+RAY_TYPES = ("camera", "extension", "shadow", "connection", "light")
+
+
+def counts_reset(on: bool = True) -> None:
+    """Starts (or stops) the integrator references' per-ray-type visit counts."""
+    L = orc_lib()
+    L.rb2o_counts_reset.argtypes = [C.c_int]
+    L.rb2o_counts_reset.restype = None
+    L.rb2o_counts_reset(1 if on else 0)
+
+
+def counts_read() -> dict:
+    """{ray type: {nodes, tris, leafterms, rays}} accumulated since counts_reset."""
+    L = orc_lib()
+    L.rb2o_counts_read.argtypes = [C.c_void_p]
+    L.rb2o_counts_read.restype = None
+    out = np.zeros((len(RAY_TYPES), 4), np.uint64)
+    L.rb2o_counts_read(out.ctypes.data)
+    return {t: dict(zip(("nodes", "tris", "leafterms", "rays"), (int(x) for x in out[i])))
+            for i, t in enumerate(RAY_TYPES)}
+
+
 FILTER_KINDS = {"none": 0, "box": 1, "triangle": 2, "gaussian": 3}
 
 

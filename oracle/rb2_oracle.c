@@ -432,12 +432,55 @@ static inline void mkray(float* r8, d3 o, double tmin, d3 d, double tmax)
     r8[4] = (float)d.x; r8[5] = (float)d.y; r8[6] = (float)d.z; r8[7] = (float)tmax;
 }
 
-static inline int occluded(const rb2o_bvh* b, const float* r8)
+/* Visit counters of the integrator references, per ray type (RB2O_RAY_*):
+ * nodes, triangles, leaf terminators, rays; off unless rb2o_counts_reset(1). */
+static uint64_t g_cnt[RB2O_RAY_TYPES][4];
+static int g_counting = 0;
+
+void rb2o_counts_reset(int on)
+{
+    memset(g_cnt, 0, sizeof(g_cnt));
+    g_counting = on;
+}
+
+void rb2o_counts_read(uint64_t* out)
+{
+    memcpy(out, g_cnt, sizeof(g_cnt));
+}
+
+static void trace_ct(const rb2o_bvh* b, const float* r, int any_hit, rb2o_hit* h, int type)
+{
+    if (!g_counting) {
+        trace_one(b->nodes, b->woop, b->triidx, r, any_hit, h, NULL);
+        return;
+    }
+    rb2o_counts c;
+    trace_one(b->nodes, b->woop, b->triidx, r, any_hit, h, &c);
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+    g_cnt[type][0] += c.nodes;
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+    g_cnt[type][1] += c.tris;
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+    g_cnt[type][2] += c.leafterms;
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+    g_cnt[type][3] += 1;
+}
+
+static inline int occluded_t(const rb2o_bvh* b, const float* r8, int type)
 {
     rb2o_hit h;
-    trace_one(b->nodes, b->woop, b->triidx, r8, 1, &h, NULL);
+    trace_ct(b, r8, 1, &h, type);
     return h.prim >= 0;
 }
+#define occluded(b, r8) occluded_t((b), (r8), RB2O_RAY_SHADOW)
 
 void rb2o_ao(const rb2o_bvh* b, const rb2o_scene* s, const float* prim_rays, uint32_t n, uint32_t samples,
              float radius, uint64_t seed, double* out, int nthreads)
@@ -449,7 +492,7 @@ void rb2o_ao(const rb2o_bvh* b, const rb2o_scene* s, const float* prim_rays, uin
     for (int64_t i = 0; i < (int64_t)n; i++) {
         const float* r = prim_rays + 8 * i;
         rb2o_hit h;
-        trace_one(b->nodes, b->woop, b->triidx, r, 0, &h, NULL);
+        trace_ct(b, r, 0, &h, RB2O_RAY_CAMERA);
         if (h.prim < 0) { out[i] = 0.0; continue; }
         const uint32_t* t = s->tris + 3 * (size_t)h.prim;
         d3 v0 = vtx(s, t[0]), v1 = vtx(s, t[1]), v2 = vtx(s, t[2]);
@@ -706,7 +749,7 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
         const double inv_nl = s->n_lights ? 1.0 / (double)s->n_lights : 0.0;
         for (uint32_t bnc = 0;; bnc++) {
             rb2o_hit h;
-            trace_one(b->nodes, b->woop, b->triidx, ray, 0, &h, NULL);
+            trace_ct(b, ray, 0, &h, bnc == 0 ? RB2O_RAY_CAMERA : RB2O_RAY_EXTENSION);
             if (h.prim < 0) break;
             const uint32_t* t = s->tris + 3 * (size_t)h.prim;
             const uint32_t m = s->tri_mat[h.prim];
@@ -888,7 +931,7 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
             mkray(ray, y0, 1.0e-4, dir, 3.402823466e+38);
             for (uint32_t d = 1; d <= Dl; d++) {
                 rb2o_hit h;
-                trace_one(b->nodes, b->woop, b->triidx, ray, 0, &h, NULL);
+                trace_ct(b, ray, 0, &h, RB2O_RAY_LIGHT);
                 if (h.prim < 0) break;
                 const uint32_t* t = s->tris + 3 * (size_t)h.prim;
                 const uint32_t m = s->tri_mat[h.prim];
@@ -932,7 +975,7 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
             const uint64_t key = (uint64_t)it * n_cam + (uint64_t)ci;
             for (uint32_t i = 1; i <= K; i++) {
                 rb2o_hit h;
-                trace_one(b->nodes, b->woop, b->triidx, ray, 0, &h, NULL);
+                trace_ct(b, ray, 0, &h, i == 1 ? RB2O_RAY_CAMERA : RB2O_RAY_EXTENSION);
                 if (h.prim < 0) break;
                 const uint32_t* t = s->tris + 3 * (size_t)h.prim;
                 const uint32_t m = s->tri_mat[h.prim];
@@ -989,7 +1032,7 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                         if (!(cos_c > 0.0 && cos_v > 0.0)) continue;
                         float cr[8];
                         mkray(cr, pos, eps, dir, dist * (1.0 - 1.0e-3));
-                        if (occluded(b, cr)) continue;
+                        if (occluded_t(b, cr, RB2O_RAY_CONNECTION)) continue;
                         const float* Av = s->albedo + 3 * (size_t)V->mat;
                         double g = cos_c * cos_v / dist2 / (RB2O_PI * RB2O_PI) * ((double)M / (double)n_light_paths) /
                                    ((double)(V->s + i) * (double)C);

@@ -125,6 +125,14 @@ typedef struct {
     const uint32_t* triidx;
 } rb2o_bvh;
 
+/* Visit counters of the integrator references (ao, pt, bdpt) per ray type:
+ * out[type * 4 + k], k = nodes, triangles, leaf terminators, rays.  Counting
+ * is off until rb2o_counts_reset(1). */
+enum { RB2O_RAY_CAMERA = 0, RB2O_RAY_EXTENSION = 1, RB2O_RAY_SHADOW = 2, RB2O_RAY_CONNECTION = 3, RB2O_RAY_LIGHT = 4,
+       RB2O_RAY_TYPES = 5 };
+void rb2o_counts_reset(int on);
+void rb2o_counts_read(uint64_t* out);
+
 /* Ambient occlusion (integrators/integrator_ao.cu:51-84): per primary ray, the
  * unoccluded fraction of `samples` cosine-distributed rays about the
  * viewer-facing geometric normal, tmin 1e-3 t, tmax radius; 0 on a miss. */

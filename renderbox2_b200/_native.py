@@ -98,7 +98,8 @@ class BdptParams(C.Structure):
 
 class RenderStats(C.Structure):
     _fields_ = [("primary_rays", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
-                ("connection_rays", C.c_uint64), ("light_rays", C.c_uint64), ("lvc_vertices", C.c_uint64)]
+                ("connection_rays", C.c_uint64), ("light_rays", C.c_uint64), ("lvc_vertices", C.c_uint64),
+                ("trace_ms", C.c_double)]
 
 
 class Camera(C.Structure):
@@ -145,6 +146,7 @@ SIGNATURES = {
     "rb2_filter_table": (C.c_int, [C.POINTER(Filter), P]),
     "rb2_scene_set_materials": (C.c_int, [P, C.POINTER(MaterialDesc), U32]),
     "rb2_integrator_set_launch": (C.c_int, [P, C.POINTER(LaunchConfig)]),
+    "rb2_integrator_set_timing": (C.c_int, [P, I32]),
     "rb2_material_query": (C.c_int, [P, I32, P, P, U32, P, P]),
     "rb2_film_develop": (C.c_int, [C.POINTER(Filter), U32, U32, U32, P, P, P, P]),
     "rb2_image_write_pfm": (C.c_int, [C.c_char_p, P, U32, U32]),

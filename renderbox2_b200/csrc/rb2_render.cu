@@ -830,7 +830,7 @@ int launch_persistent_variant(const Src& src, uint64_t work, int sms, uint32_t t
 }
 
 template <class Src>
-int launch_persistent(const Src& src, uint64_t work, const rb2_integrator* it, unsigned int* status, cudaStream_t s)
+int launch_persistent_shape(const Src& src, uint64_t work, const rb2_integrator* it, unsigned int* status, cudaStream_t s)
 {
     const uint32_t th = it->tr_threshold;
     if (it->tr_block == 256)
@@ -838,6 +838,24 @@ int launch_persistent(const Src& src, uint64_t work, const rb2_integrator* it, u
                                  : launch_persistent_variant<256, 64>(src, work, it->sms, th, status, s);
     return it->tr_regs == 48 ? launch_persistent_variant<128, 48>(src, work, it->sms, th, status, s)
                              : launch_persistent_variant<128, 64>(src, work, it->sms, th, status, s);
+}
+
+// With timing on, each traversal launch is bracketed by an event pair.
+template <class Src>
+int launch_persistent(const Src& src, uint64_t work, rb2_integrator* it, unsigned int* status, cudaStream_t s)
+{
+    if (!it->timing) return launch_persistent_shape(src, work, it, status, s);
+    while (it->ev.size() < it->ev_used + 2) {
+        cudaEvent_t e;
+        RB2_CUDA(cudaEventCreate(&e), "timing event");
+        it->ev.push_back(e);
+    }
+    RB2_CUDA(cudaEventRecord(it->ev[it->ev_used], s), "timing event");
+    const int rc = launch_persistent_shape(src, work, it, status, s);
+    if (rc) return rc;
+    RB2_CUDA(cudaEventRecord(it->ev[it->ev_used + 1], s), "timing event");
+    it->ev_used += 2;
+    return RB2_OK;
 }
 
 unsigned grid_for(uint64_t n, int sms) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 8)); }
@@ -1006,6 +1024,7 @@ int rb2_integrator_destroy(rb2_integrator* it)
     if (!it) return RB2_OK;
     cudaFree(it->d_rays); cudaFree(it->d_hits); cudaFree(it->d_count); cudaFree(it->d_counters);
     cudaFree(it->d_accum); cudaFree(it->d_wave); cudaFree(it->d_film_xy);
+    for (cudaEvent_t e : it->ev) cudaEventDestroy(e);
     PathState& ps = it->ps;
     cudaFree(ps.T); cudaFree(ps.L); cudaFree(ps.ray); cudaFree(ps.hit); cudaFree(ps.sray); cudaFree(ps.sc);
     cudaFree(ps.q[0]); cudaFree(ps.q[1]); cudaFree(ps.qs);
@@ -1041,6 +1060,7 @@ int rb2_integrator_device_bytes(const rb2_integrator* it, uint64_t* bytes)
 int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params* p, float* d_ao, void* stream)
 {
     if (!it || !cam || !p || !d_ao) return fail(RB2_EINVAL, "null argument");
+    it->ev_used = 0;
     if (p->samples == 0 || !(p->radius > 0.0f)) return fail(RB2_EINVAL, "AO needs samples > 0 and radius > 0");
     cudaStream_t s = (cudaStream_t)stream;
     const uint64_t npix = (uint64_t)cam->width * cam->height;
@@ -1051,9 +1071,21 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
         return rc;
     // 1. Primary rays through pixel centres, 2. closest hit (IntegratorAO::compute, integrator_ao.cu:92-101).
     if ((rc = rb2_camera_rays(cam, 1, 0, 0, reinterpret_cast<float*>(it->d_rays), stream))) return rc;
+    if (it->timing) {
+        while (it->ev.size() < it->ev_used + 2) {
+            cudaEvent_t e;
+            RB2_CUDA(cudaEventCreate(&e), "timing event");
+            it->ev.push_back(e);
+        }
+        RB2_CUDA(cudaEventRecord(it->ev[it->ev_used], s), "timing event");
+    }
     if ((rc = rb2_trace(it->tracer, reinterpret_cast<const float*>(it->d_rays), (uint32_t)npix, 0, nullptr,
                         reinterpret_cast<rb2_hit*>(it->d_hits), stream)))
         return rc;
+    if (it->timing) {
+        RB2_CUDA(cudaEventRecord(it->ev[it->ev_used + 1], s), "timing event");
+        it->ev_used += 2;
+    }
     // 3. AO rays generated and traced in one persistent launch, unoccluded counts per pixel.
     RB2_CUDA(cudaMemsetAsync(it->d_count, 0, npix * sizeof(uint32_t), s), "AO count reset");
     RB2_CUDA(cudaMemsetAsync(it->d_counters, 0, sizeof(unsigned long long), s), "queue reset");
@@ -1082,6 +1114,7 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
 int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, float* d_rgb, void* stream)
 {
     if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
+    it->ev_used = 0;
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
     if (p->max_depth > 64) return fail(RB2_EINVAL, "max_depth must be <= 64");
     cudaStream_t s = (cudaStream_t)stream;
@@ -1156,6 +1189,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
 int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_params* p, float* d_rgb, void* stream)
 {
     if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
+    it->ev_used = 0;
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
     if (p->max_path_length < 1 || p->max_path_length > 16) return fail(RB2_EINVAL, "max_path_length must be in [1, 16]");
     if (p->connections < 1 || p->connections > rb2dev::kMaxConnections) return fail(RB2_EINVAL, "connections must be in [1, 8]");
@@ -1264,6 +1298,16 @@ int rb2_integrator_stats(rb2_integrator* it, rb2_render_stats* out, void* stream
 {
     if (!it || !out) return fail(RB2_EINVAL, "null argument");
     std::memset(out, 0, sizeof(*out));
+    if (it->timing) {
+        double ms = 0.0;
+        for (uint32_t k = 0; k + 1 < it->ev_used; k += 2) {
+            float e = 0.0f;
+            RB2_CUDA(cudaEventSynchronize(it->ev[k + 1]), "timing sync");
+            RB2_CUDA(cudaEventElapsedTime(&e, it->ev[k], it->ev[k + 1]), "timing read");
+            ms += e;
+        }
+        out->trace_ms = ms;
+    }
     if (!it->d_wave) return RB2_OK;
     WaveCounters w;
     cudaStream_t s = (cudaStream_t)stream;
@@ -1275,6 +1319,14 @@ int rb2_integrator_stats(rb2_integrator* it, rb2_render_stats* out, void* stream
     out->connection_rays = w.stats[3];
     out->light_rays = w.stats[4];
     out->lvc_vertices = w.stats[5];
+    return RB2_OK;
+}
+
+int rb2_integrator_set_timing(rb2_integrator* it, int on)
+{
+    if (!it) return fail(RB2_EINVAL, "null argument");
+    it->timing = on != 0;
+    it->ev_used = 0;
     return RB2_OK;
 }
 

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 namespace rb2dev {
 struct MaterialDev;
@@ -82,6 +83,10 @@ struct rb2_integrator {
     int sms = 0;
     // launch shape of the integrator's traversal kernels (rb2_integrator_set_launch)
     uint32_t tr_block = 128, tr_regs = 48, tr_threshold = 24;
+    // traversal timing (rb2_integrator_set_timing): an event pair per launch
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;
+    uint32_t ev_used = 0;
     // generic scratch
     float4* d_rays = nullptr; uint64_t cap_rays = 0;        // 2 per ray
     int4* d_hits = nullptr; uint64_t cap_hits = 0;

@@ -44,6 +44,7 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None):
     bvh = rb.BVH(scene)
     build_s = time.time() - t0
     it = Integrator(rb.CudaTracer(bvh), DeviceScene(scene))
+    it.set_timing(True)  # traversal launches bracketed by CUDA events (stats "trace_ms")
     scale = c.get("room_size", 1.0)
     eye = [x * scale for x in c["eye"]]
     look = [x * scale for x in c["lookat"]]
