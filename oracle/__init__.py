@@ -416,13 +416,16 @@ def pt(bvh_buffers, vertices, indices, tri_mat, albedo, emission, lights, rays, 
 
 
 def bdpt(bvh_buffers, vertices, indices, tri_mat, albedo, emission, lights, cam_rays, n_cam, n_iter, n_light_paths,
-         K, C, rr_start, rr_prob, seed=1, nthreads=0):
-    """FP64 BDPT-LVC mean radiance per camera pixel over n_iter iterations."""
+         K, C, rr_start, rr_prob, seed=1, nthreads=0, materials=None):
+    """FP64 BDPT-LVC mean radiance per camera pixel over n_iter iterations.
+
+    `materials` (optional): layered material descriptions per material; no
+    layer may be specular (mirror or glass)."""
     L = orc_lib()
     L.rb2o_bdpt.argtypes = [C_.POINTER(_Bvh), C_.POINTER(_Scene), C_.c_void_p, C_.c_uint32, C_.c_uint32, C_.c_uint32,
                             C_.c_uint32, C_.c_uint32, C_.c_uint32, C_.c_float, C_.c_uint64, C_.c_void_p, C_.c_int]
     L.rb2o_bdpt.restype = None
-    s, ks = _scene_struct(vertices, indices, tri_mat, albedo, emission, lights)
+    s, ks = _scene_struct(vertices, indices, tri_mat, albedo, emission, lights, materials)
     b, kb = _bvh_struct(*bvh_buffers)
     r = np.ascontiguousarray(cam_rays, np.float32).reshape(-1, 8)
     assert r.shape[0] == n_cam * n_iter

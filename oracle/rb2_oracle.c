@@ -887,7 +887,7 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
  * cached (Dl = K - 2); then one camera path per camera ray with emission
  * (s = 0), NEE (s = 1) and C uniform cache connections (s >= 2, scaled by
  * cache size / light paths), each strategy of a k-segment path weighted 1/k. */
-typedef struct { d3 pos, nrm, beta; uint32_t s, mat; } lvc_vertex;
+typedef struct { d3 pos, nrm, beta, wi, ng; uint32_t s, mat; } lvc_vertex;
 
 void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, uint32_t n_cam, uint32_t n_iter,
                uint32_t n_light_paths, uint32_t K, uint32_t C, uint32_t rr_start, float rr_prob, uint64_t seed,
@@ -947,8 +947,31 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                 sparse[slot].pos = pos; sparse[slot].nrm = nrm;
                 sparse[slot].beta = D3(beta[0], beta[1], beta[2]);
                 sparse[slot].s = d + 1; sparse[slot].mat = m;
+                sparse[slot].wi = wo; sparse[slot].ng = ng;
                 valid[slot] = 1;
                 if (d >= Dl) break;
+                if (s->materials && !plain_lambertian(&s->materials[m])) {
+                    /* Layered (non-specular) material: sample its BSDF toward the next light vertex. */
+                    d3 wn = D3(0, 0, 0);
+                    double pdf;
+                    int spec;
+                    d3 f = mat_sample(&s->materials[m], ng, wo, u01(ls, key, 8 + 8 * d), u01(ls, key, 9 + 8 * d),
+                                      u01(ls, key, 11 + 8 * d), &wn, &pdf, &spec);
+                    if (!(pdf > 0.0) || !(f.x > 0.0 || f.y > 0.0 || f.z > 0.0)) break;
+                    /* Light flows from wo toward wn: the adjoint f(wn -> wo) (the Blinn
+                     * shadowing term is not symmetric in its two directions). */
+                    frame3 frl = frame_z(ng);
+                    f = mat_f(&s->materials[m], ng, wn, wo, fr_local(&frl, wn), fr_local(&frl, wo));
+                    double k = fabs(ddot(wn, nrm)) / pdf;
+                    double fac[3] = {f.x * k, f.y * k, f.z * k};
+                    double lum = 0.212671 * fac[0] + 0.715160 * fac[1] + 0.072169 * fac[2];
+                    double q = lum < 1.0 ? lum : 1.0;
+                    if (d < rr_start) q = 1.0; else if (q > rr_prob) q = rr_prob;
+                    if (!(q > 0.0 && u01(ls, key, 10 + 8 * d) < q)) break;
+                    for (int c2 = 0; c2 < 3; c2++) beta[c2] *= fac[c2] / q;
+                    mkray(ray, pos, 1.0e-3 * (double)h.t, wn, 3.402823466e+38);
+                    continue;
+                }
                 const float* A = s->albedo + 3 * (size_t)m;
                 d3 lc = cos_hemi(u01(ls, key, 8 + 8 * d), u01(ls, key, 9 + 8 * d));
                 if (!(lc.z > 0.0)) break;
@@ -994,6 +1017,11 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                 d3 nrm = ddot(ng, wo) < 0.0 ? dmul(ng, -1.0) : ng;
                 const float* A = s->albedo + 3 * (size_t)m;
                 uint64_t vkey = key * 64 + i;
+                /* Layered materials (non-specular): f from the material functions,
+                 * in the frame of the geometric normal as the path tracer uses. */
+                const rb2o_material* mc = (s->materials && !plain_lambertian(&s->materials[m])) ? &s->materials[m] : NULL;
+                frame3 frc = frame_z(ng);
+                d3 wo_l = fr_local(&frc, wo);
                 if (s->n_lights && i + 1 <= K) {
                     uint32_t j = (uint32_t)(u01(seed, vkey, 0) * s->n_lights);
                     if (j >= s->n_lights) j = s->n_lights - 1;
@@ -1009,7 +1037,20 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                     d3 wi = dmul(dv, 1.0 / dist);
                     double cos_l = -ddot(ln, wi), cos_s = ddot(nrm, wi);
                     const float* Le = s->emission + 3 * (size_t)s->tri_mat[lt];
-                    if (cos_l > 0.0 && cos_s > 0.0 && dist > 0.0) {
+                    if (mc && cos_l > 0.0 && dist > 0.0) {
+                        d3 f = mat_f(mc, ng, wo, wi, wo_l, fr_local(&frc, wi));
+                        if (f.x > 0.0 || f.y > 0.0 || f.z > 0.0) {
+                            double pdf_l = inv_nl * dist2 / (tri_area_d(l0, l1, l2) * cos_l);
+                            float sr[8];
+                            mkray(sr, pos, eps, wi, dist * (1.0 - 1.0e-3));
+                            if (!occluded(b, sr)) {
+                                double k = fabs(cos_s) / pdf_l / (double)(i + 1);
+                                L[0] += T[0] * f.x * Le[0] * k;
+                                L[1] += T[1] * f.y * Le[1] * k;
+                                L[2] += T[2] * f.z * Le[2] * k;
+                            }
+                        }
+                    } else if (!mc && cos_l > 0.0 && cos_s > 0.0 && dist > 0.0) {
                         double pdf_l = inv_nl * dist2 / (tri_area_d(l0, l1, l2) * cos_l);
                         float sr[8];
                         mkray(sr, pos, eps, wi, dist * (1.0 - 1.0e-3));
@@ -1029,6 +1070,33 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                         if (!(dist > 0.0)) continue;
                         d3 dir = dmul(dv, 1.0 / dist);
                         double cos_c = ddot(nrm, dir), cos_v = -ddot(V->nrm, dir);
+                        const rb2o_material* mv =
+                            (s->materials && !plain_lambertian(&s->materials[V->mat])) ? &s->materials[V->mat] : NULL;
+                        if (mc || mv) {
+                            /* f at both ends from the material functions (Lambertian: A / pi on the lit side). */
+                            d3 fc = mc ? mat_f(mc, ng, wo, dir, wo_l, fr_local(&frc, dir))
+                                       : (cos_c > 0.0 ? dmul(D3(A[0], A[1], A[2]), 1.0 / RB2O_PI) : D3(0, 0, 0));
+                            d3 fv;
+                            if (mv) {
+                                frame3 frv = frame_z(V->ng);
+                                d3 wov = dmul(dir, -1.0);
+                                fv = mat_f(mv, V->ng, wov, V->wi, fr_local(&frv, wov), fr_local(&frv, V->wi));
+                            } else {
+                                const float* Av = s->albedo + 3 * (size_t)V->mat;
+                                fv = cos_v > 0.0 ? dmul(D3(Av[0], Av[1], Av[2]), 1.0 / RB2O_PI) : D3(0, 0, 0);
+                            }
+                            d3 ff = D3(fc.x * fv.x, fc.y * fv.y, fc.z * fv.z);
+                            if (!(ff.x > 0.0 || ff.y > 0.0 || ff.z > 0.0)) continue;
+                            float cr[8];
+                            mkray(cr, pos, eps, dir, dist * (1.0 - 1.0e-3));
+                            if (occluded_t(b, cr, RB2O_RAY_CONNECTION)) continue;
+                            double g = fabs(cos_c) * fabs(cos_v) / dist2 * ((double)M / (double)n_light_paths) /
+                                       ((double)(V->s + i) * (double)C);
+                            L[0] += T[0] * ff.x * V->beta.x * g;
+                            L[1] += T[1] * ff.y * V->beta.y * g;
+                            L[2] += T[2] * ff.z * V->beta.z * g;
+                            continue;
+                        }
                         if (!(cos_c > 0.0 && cos_v > 0.0)) continue;
                         float cr[8];
                         mkray(cr, pos, eps, dir, dist * (1.0 - 1.0e-3));
@@ -1041,6 +1109,24 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                     }
                 }
                 if (i >= K) break;
+                if (mc) {
+                    d3 wn = D3(0, 0, 0);
+                    double pdf;
+                    int spec;
+                    d3 f = mat_sample(mc, ng, wo, u01(seed, vkey, 3), u01(seed, vkey, 4), u01(seed, vkey, 6), &wn, &pdf,
+                                      &spec);
+                    if (!(pdf > 0.0) || !(f.x > 0.0 || f.y > 0.0 || f.z > 0.0)) break;
+                    double k = fabs(ddot(wn, nrm)) / pdf;
+                    T[0] *= f.x * k; T[1] *= f.y * k; T[2] *= f.z * k;
+                    if (i - 1 >= rr_start) {
+                        double lum = 0.212671 * T[0] + 0.715160 * T[1] + 0.072169 * T[2];
+                        double q = lum < rr_prob ? lum : rr_prob;
+                        if (!(u01(seed, vkey, 5) < q)) break;
+                        for (int c = 0; c < 3; c++) T[c] /= q;
+                    }
+                    mkray(ray, pos, eps, wn, 3.402823466e+38);
+                    continue;
+                }
                 d3 fx, fy;
                 frame(nrm, &fx, &fy);
                 d3 lc = cos_hemi(u01(seed, vkey, 3), u01(seed, vkey, 4));

@@ -483,13 +483,23 @@ __global__ void k_bd_light_init(SceneView sc, uint64_t seed, uint64_t key0, uint
     }
 }
 
+// Layered material of a surface, or null for a single Lambertian layer (the
+// albedo fast path).
+__device__ __forceinline__ const MaterialDev* layered_material(const SceneView& sc, uint32_t mat)
+{
+    return (sc.mats && !(sc.mats[mat].flags & kMatPlainLambertian)) ? &sc.mats[mat] : nullptr;
+}
+
 // Light vertex d (1-based surface vertex): store it in the sparse cache slot
 // (path, d) and continue the subpath by BSDF sampling with Russian roulette on
-// the per-bounce factor (integrator_bdpt_lvc_sk.cu:93-166).
+// the per-bounce factor (integrator_bdpt_lvc_sk.cu:93-166).  On a layered
+// (non-specular) material the continuation samples material_sample_f and the
+// factor is f |cos| / pdf; s_wi (null when every material is one Lambertian
+// layer) keeps the direction toward the previous vertex for the connection's f.
 __global__ void k_bd_light_shade(SceneView sc, uint64_t seed, uint64_t key0, uint32_t d, uint32_t Dl, uint32_t rr_start,
                                  float rr_prob, const uint32_t* q_in, uint32_t* q_out, float4* lray, const int4* lhit,
-                                 float4* lbeta, float4* s_pos, float4* s_nrm, float4* s_beta, uint8_t* s_valid,
-                                 WaveCountersDev* wc, uint32_t cur)
+                                 float4* lbeta, float4* s_pos, float4* s_nrm, float4* s_beta, float4* s_wi,
+                                 uint8_t* s_valid, WaveCountersDev* wc, uint32_t cur)
 {
     const uint32_t n = wc->n_ext[cur];
     const uint64_t ls = seed ^ kLightSalt;
@@ -519,7 +529,35 @@ __global__ void k_bd_light_shade(SceneView sc, uint64_t seed, uint64_t key0, uin
                     s_nrm[slot] = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(tri.w));
                     s_beta[slot] = beta;
                     s_valid[slot] = 1;
-                    if (d < Dl) {
+                    if (s_wi) s_wi[slot] = make_float4(wo.x, wo.y, wo.z, dot3(ng, nrm) < 0.0f ? -1.0f : 1.0f);
+                    const MaterialDev* lm = layered_material(sc, tri.w);
+                    if (d < Dl && lm) {
+                        const uint64_t key = key0 + path;
+                        float3 wi;
+                        float pdf;
+                        bool spec;
+                        const Frame frl = frame_from_z(ng);
+                        float3 f = material_sample(*lm, frl, ng, wo, rng_u01(ls, key, 8 + 8 * d),
+                                                   rng_u01(ls, key, 9 + 8 * d), rng_u01(ls, key, 11 + 8 * d), wi, pdf, spec);
+                        if (pdf > 0.0f && (f.x > 0.0f || f.y > 0.0f || f.z > 0.0f)) {
+                            // Light flows from wo toward wi: the adjoint f(wi -> wo), since the
+                            // Blinn shadowing term is not symmetric in its two directions.
+                            f = material_f(*lm, ng, wi, wo, to_local(frl, wi), to_local(frl, wo));
+                            const float k = fabsf(dot3(wi, ng)) / pdf;
+                            const float3 fac = f3(f.x * k, f.y * k, f.z * k);
+                            float q = fminf(1.0f, luminance(fac));
+                            if (d < rr_start) q = 1.0f;
+                            else q = fminf(q, rr_prob);
+                            cont = q > 0.0f && isfinite(fac.x) && isfinite(fac.y) && isfinite(fac.z) &&
+                                   rng_u01(ls, key, 10 + 8 * d) < q;
+                            if (cont) {
+                                beta.x *= fac.x / q; beta.y *= fac.y / q; beta.z *= fac.z / q;
+                                lbeta[path] = beta;
+                                no = make_float4(pos.x, pos.y, pos.z, 1.0e-3f * t);
+                                nd = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
+                            }
+                        }
+                    } else if (d < Dl) {
                         const uint64_t key = key0 + path;
                         const float4 A = sc.albedo[tri.w];
                         const float3 loc = cosine_hemisphere(rng_u01(ls, key, 8 + 8 * d), rng_u01(ls, key, 9 + 8 * d));
@@ -604,7 +642,8 @@ __global__ void k_lvc_scan_top(uint32_t* block_sums, uint32_t n_blocks, WaveCoun
 
 // Scatter valid slots in slot order: thread t of a chunk owns 8 consecutive slots.
 __global__ void k_lvc_scatter(const uint8_t* valid, uint64_t n_slots, const uint32_t* block_offsets, const float4* s_pos,
-                              const float4* s_nrm, const float4* s_beta, float4* d_pos, float4* d_nrm, float4* d_beta)
+                              const float4* s_nrm, const float4* s_beta, const float4* s_wi, float4* d_pos, float4* d_nrm,
+                              float4* d_beta, float4* d_wi)
 {
     constexpr uint32_t kPer = kScanChunk / kScanThreads;
     __shared__ uint32_t s_warp[kScanThreads / 32];
@@ -628,6 +667,7 @@ __global__ void k_lvc_scatter(const uint8_t* valid, uint64_t n_slots, const uint
             d_pos[out] = s_pos[i];
             d_nrm[out] = s_nrm[i];
             d_beta[out] = s_beta[i];
+            if (s_wi) d_wi[out] = s_wi[i];
             out++;
         }
     }
@@ -635,13 +675,16 @@ __global__ void k_lvc_scatter(const uint8_t* valid, uint64_t n_slots, const uint
 
 // Camera vertex i (1-based): emission (s = 0), next-event estimation (s = 1),
 // connections to cached light vertices (s >= 2), continuation.  Every
-// strategy of a k-segment path is weighted 1/k.
+// strategy of a k-segment path is weighted 1/k.  A layered (non-specular)
+// vertex at either end of a strategy takes f from material_f in the frame of
+// its geometric normal (the path tracer's convention) and continues by
+// material_sample_f; single-Lambertian vertices keep the albedo fast path.
 __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t iter, uint32_t i, uint32_t Kmax,
                                uint32_t C, uint32_t rr_start, float rr_prob, float n_light_paths, const uint32_t* q_in,
                                uint32_t* q_out, float4* rays, const int4* hits, float4* T, float4* L, float4* srays,
                                float4* sc_out, uint32_t* qs, float4* cray, float4* cc, uint32_t* cq,
                                const float4* lvc_pos, const float4* lvc_nrm, const float4* lvc_beta,
-                               WaveCountersDev* wc, uint32_t cur)
+                               const float4* lvc_wi, WaveCountersDev* wc, uint32_t cur)
 {
     const uint32_t n = wc->n_ext[cur];
     const uint32_t M = wc->lvc_count;
@@ -682,6 +725,9 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                 } else {
                     const float3 nrm = dot3(ng, wo) < 0.0f ? mul(ng, -1.0f) : ng;
                     const float4 A = sc.albedo[tri.w];
+                    const MaterialDev* mc = layered_material(sc, tri.w);
+                    const Frame frc = frame_from_z(ng);
+                    const float3 wo_l = to_local(frc, wo);
                     if (sc.n_lights && i + 1 <= Kmax) {  // s = 1, k = i + 1
                         uint32_t j = min((uint32_t)(rng_u01(seed, key, vdim(b, kDimLight)) * (float)sc.n_lights),
                                          sc.n_lights - 1);
@@ -695,7 +741,15 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                         const float3 wi = mul(dv, 1.0f / dist);
                         const float cos_l = -dot3(ln, wi), cos_s = dot3(nrm, wi);
                         const float4 Le = sc.emission[lt.w];
-                        if (cos_l > 0.0f && cos_s > 0.0f && dist > 0.0f) {
+                        if (mc && cos_l > 0.0f && dist > 0.0f) {
+                            const float3 f = material_f(*mc, ng, wo, wi, wo_l, to_local(frc, wi));
+                            const float pdf_l = inv_nl * dist2 / (tri_area(l0, l1, l2) * cos_l);
+                            const float k = fabsf(cos_s) / (pdf_l * (float)(i + 1));
+                            scv = make_float4(Tp.x * f.x * Le.x * k, Tp.y * f.y * Le.y * k, Tp.z * f.z * Le.z * k, 0.0f);
+                            so = make_float4(pos.x, pos.y, pos.z, eps);
+                            sd = make_float4(wi.x, wi.y, wi.z, dist * (1.0f - 1.0e-3f));
+                            shadow = scv.x > 0.0f || scv.y > 0.0f || scv.z > 0.0f;
+                        } else if (!mc && cos_l > 0.0f && cos_s > 0.0f && dist > 0.0f) {
                             const float pdf_l = inv_nl * dist2 / (tri_area(l0, l1, l2) * cos_l);
                             const float k = cos_s * kInvPi / (pdf_l * (float)(i + 1));
                             scv = make_float4(Tp.x * A.x * Le.x * k, Tp.y * A.y * Le.y * k, Tp.z * A.z * Le.z * k, 0.0f);
@@ -716,13 +770,34 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                             if (!(dist > 0.0f)) continue;
                             const float3 dir = mul(dv, 1.0f / dist);
                             const float cos_c = dot3(nrm, dir), cos_v = -dot3(xyz(vn4), dir);
-                            if (!(cos_c > 0.0f && cos_v > 0.0f)) continue;
-                            const float4 Av = sc.albedo[__float_as_uint(vn4.w)];
+                            const uint32_t vmat = __float_as_uint(vn4.w);
+                            const MaterialDev* mv = lvc_wi ? layered_material(sc, vmat) : nullptr;
+                            const float4 Av = sc.albedo[vmat];
                             const float4 bv = lvc_beta[v];
-                            const float g = cos_c * cos_v / dist2 * kInvPi * kInvPi * ((float)M / n_light_paths) /
-                                            ((float)(s + i) * (float)C);
-                            const float4 cv = make_float4(Tp.x * A.x * Av.x * bv.x * g, Tp.y * A.y * Av.y * bv.y * g,
-                                                          Tp.z * A.z * Av.z * bv.z * g, 0.0f);
+                            float4 cv;
+                            if (mc || mv) {
+                                float3 fc = f3(0.0f, 0.0f, 0.0f), fv = f3(0.0f, 0.0f, 0.0f);
+                                if (mc) fc = material_f(*mc, ng, wo, dir, wo_l, to_local(frc, dir));
+                                else if (cos_c > 0.0f) fc = f3(A.x * kInvPi, A.y * kInvPi, A.z * kInvPi);
+                                if (mv) {
+                                    const float4 w4 = lvc_wi[v];
+                                    const float3 ngv = mul(xyz(vn4), w4.w), wiv = xyz(w4), wov = mul(dir, -1.0f);
+                                    const Frame frv = frame_from_z(ngv);
+                                    fv = material_f(*mv, ngv, wov, wiv, to_local(frv, wov), to_local(frv, wiv));
+                                } else if (cos_v > 0.0f) {
+                                    fv = f3(Av.x * kInvPi, Av.y * kInvPi, Av.z * kInvPi);
+                                }
+                                const float g = fabsf(cos_c) * fabsf(cos_v) / dist2 * ((float)M / n_light_paths) /
+                                                ((float)(s + i) * (float)C);
+                                cv = make_float4(Tp.x * fc.x * fv.x * bv.x * g, Tp.y * fc.y * fv.y * bv.y * g,
+                                                 Tp.z * fc.z * fv.z * bv.z * g, 0.0f);
+                            } else {
+                                if (!(cos_c > 0.0f && cos_v > 0.0f)) continue;
+                                const float g = cos_c * cos_v / dist2 * kInvPi * kInvPi * ((float)M / n_light_paths) /
+                                                ((float)(s + i) * (float)C);
+                                cv = make_float4(Tp.x * A.x * Av.x * bv.x * g, Tp.y * A.y * Av.y * bv.y * g,
+                                                 Tp.z * A.z * Av.z * bv.z * g, 0.0f);
+                            }
                             if (!(cv.x > 0.0f || cv.y > 0.0f || cv.z > 0.0f)) continue;
                             cc[(size_t)path * C + c] = cv;
                             cro[c] = make_float4(pos.x, pos.y, pos.z, eps);
@@ -730,7 +805,30 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                             conn[c] = true;
                         }
                     }
-                    if (i < Kmax) {
+                    if (i < Kmax && mc) {
+                        float3 wi;
+                        float pdf;
+                        bool spec;
+                        const float3 f = material_sample(*mc, frc, ng, wo, rng_u01(seed, key, vdim(b, kDimBsdfU)),
+                                                         rng_u01(seed, key, vdim(b, kDimBsdfV)),
+                                                         rng_u01(seed, key, vdim(b, kDimBsdfC)), wi, pdf, spec);
+                        if (pdf > 0.0f && (f.x > 0.0f || f.y > 0.0f || f.z > 0.0f)) {
+                            const float k = fabsf(dot3(wi, ng)) / pdf;
+                            Tp.x *= f.x * k; Tp.y *= f.y * k; Tp.z *= f.z * k; Tp.w = pdf;
+                            cont = isfinite(Tp.x) && isfinite(Tp.y) && isfinite(Tp.z) &&
+                                   (Tp.x > 0.0f || Tp.y > 0.0f || Tp.z > 0.0f);
+                            if (cont && b >= rr_start) {
+                                const float q = fminf(rr_prob, luminance(xyz(Tp)));
+                                if (!(rng_u01(seed, key, vdim(b, kDimRR)) < q)) cont = false;
+                                else { Tp.x /= q; Tp.y /= q; Tp.z /= q; }
+                            }
+                            if (cont) {
+                                T[path] = Tp;
+                                new_o = make_float4(pos.x, pos.y, pos.z, eps);
+                                new_d = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
+                            }
+                        }
+                    } else if (i < Kmax) {
                         const float3 loc = cosine_hemisphere(rng_u01(seed, key, vdim(b, kDimBsdfU)),
                                                              rng_u01(seed, key, vdim(b, kDimBsdfV)));
                         if (loc.z > 0.0f) {
@@ -894,16 +992,17 @@ int ensure_bdpt_state(BdptState& bd, uint64_t n_paths, uint64_t n_slots, uint64_
         bd.cap_paths = n_paths;
     }
     if (n_slots > bd.cap_slots) {
-        for (void* p : {(void*)bd.s_pos, (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_valid, (void*)bd.d_pos,
-                        (void*)bd.d_nrm, (void*)bd.d_beta, (void*)bd.block_sums})
+        for (void* p : {(void*)bd.s_pos, (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_wi, (void*)bd.s_valid,
+                        (void*)bd.d_pos, (void*)bd.d_nrm, (void*)bd.d_beta, (void*)bd.d_wi, (void*)bd.block_sums})
             cudaFree(p);
-        bd.s_pos = bd.s_nrm = bd.s_beta = bd.d_pos = bd.d_nrm = bd.d_beta = nullptr;
+        bd.s_pos = bd.s_nrm = bd.s_beta = bd.s_wi = bd.d_pos = bd.d_nrm = bd.d_beta = bd.d_wi = nullptr;
         bd.s_valid = nullptr; bd.block_sums = nullptr; bd.cap_slots = 0;
         const uint64_t nb = (n_slots + rb2dev::kScanChunk - 1) / rb2dev::kScanChunk;
         if ((e = cudaMalloc(&bd.s_pos, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.s_nrm, n_slots * 16)) != cudaSuccess ||
             (e = cudaMalloc(&bd.s_beta, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.s_valid, n_slots)) != cudaSuccess ||
             (e = cudaMalloc(&bd.d_pos, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.d_nrm, n_slots * 16)) != cudaSuccess ||
-            (e = cudaMalloc(&bd.d_beta, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.block_sums, nb * 4)) != cudaSuccess)
+            (e = cudaMalloc(&bd.d_beta, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.s_wi, n_slots * 16)) != cudaSuccess ||
+            (e = cudaMalloc(&bd.d_wi, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.block_sums, nb * 4)) != cudaSuccess)
             return fail(RB2_ENOMEM, std::string("light vertex cache: ") + cudaGetErrorString(e));
         bd.cap_slots = n_slots;
     }
@@ -1030,8 +1129,9 @@ int rb2_integrator_destroy(rb2_integrator* it)
     cudaFree(ps.q[0]); cudaFree(ps.q[1]); cudaFree(ps.qs);
     BdptState& bd = it->bd;
     for (void* p : {(void*)bd.lray, (void*)bd.lbeta, (void*)bd.lhit, (void*)bd.lq[0], (void*)bd.lq[1], (void*)bd.s_pos,
-                    (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_valid, (void*)bd.d_pos, (void*)bd.d_nrm,
-                    (void*)bd.d_beta, (void*)bd.block_sums, (void*)bd.cray, (void*)bd.cc, (void*)bd.cq})
+                    (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_wi, (void*)bd.s_valid, (void*)bd.d_pos,
+                    (void*)bd.d_nrm, (void*)bd.d_beta, (void*)bd.d_wi, (void*)bd.block_sums, (void*)bd.cray,
+                    (void*)bd.cc, (void*)bd.cq})
         cudaFree(p);
     delete it;
     return RB2_OK;
@@ -1193,8 +1293,9 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
     if (p->max_path_length < 1 || p->max_path_length > 16) return fail(RB2_EINVAL, "max_path_length must be in [1, 16]");
     if (p->connections < 1 || p->connections > rb2dev::kMaxConnections) return fail(RB2_EINVAL, "connections must be in [1, 8]");
-    if (it->scene->layered)
-        return fail(RB2_ENOTSUP, "BDPT shades single-layer Lambertian materials only; use the path tracer for this scene");
+    if (it->scene->has_delta)
+        return fail(RB2_ENOTSUP, "BDPT connects through non-specular materials only (a material has a mirror or glass "
+                                 "layer); use the path tracer for this scene");
     cudaStream_t s = (cudaStream_t)stream;
     const uint64_t npix = (uint64_t)cam->width * cam->height;
     if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");
@@ -1228,6 +1329,9 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     WaveCounters* wc = it->d_wave;
     PathState& ps = it->ps;
     BdptState& bd = it->bd;
+    // Light-vertex directions are cached only when a layered material needs them.
+    float4* s_wi = it->scene->layered ? bd.s_wi : nullptr;
+    float4* d_wi = it->scene->layered ? bd.d_wi : nullptr;
     const unsigned gl = grid_for(NL, it->sms), gc = grid_for(npix, it->sms);
     const uint64_t n_chunks = (n_slots + rb2dev::kScanChunk - 1) / rb2dev::kScanChunk;
     for (uint32_t iter = 0; iter < p->spp; iter++) {
@@ -1244,14 +1348,14 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             if ((rc = launch_persistent(lsrc, NL, it, bv.status, s))) return rc;
             rb2dev::k_bd_light_shade<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)iter * NL, d, Dl, p->rr_start, p->rr_prob,
                                                         bd.lq[cur], bd.lq[cur ^ 1u], bd.lray, bd.lhit, bd.lbeta, bd.s_pos,
-                                                        bd.s_nrm, bd.s_beta, bd.s_valid, wc, cur);
+                                                        bd.s_nrm, bd.s_beta, s_wi, bd.s_valid, wc, cur);
             RB2_CUDA(cudaGetLastError(), "BDPT light shade");
             cur ^= 1u;
         }
         rb2dev::k_lvc_count<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(bd.s_valid, n_slots, bd.block_sums);
         rb2dev::k_lvc_scan_top<<<1, 1024, 0, s>>>(bd.block_sums, (uint32_t)n_chunks, wc);
         rb2dev::k_lvc_scatter<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(
-            bd.s_valid, n_slots, bd.block_sums, bd.s_pos, bd.s_nrm, bd.s_beta, bd.d_pos, bd.d_nrm, bd.d_beta);
+            bd.s_valid, n_slots, bd.block_sums, bd.s_pos, bd.s_nrm, bd.s_beta, s_wi, bd.d_pos, bd.d_nrm, bd.d_beta, d_wi);
         RB2_CUDA(cudaGetLastError(), "cache compaction");
         // ---- camera pass.
         rb2dev::k_pt_camera<<<gc, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, (uint32_t)npix, iter, ps.ray, ps.T, ps.L,
@@ -1266,7 +1370,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             rb2dev::k_bd_cam_shade<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, iter, i, K, C, p->rr_start, p->rr_prob,
                                                       (float)NL, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L,
                                                       ps.sray, ps.sc, ps.qs, bd.cray, bd.cc, bd.cq, bd.d_pos, bd.d_nrm,
-                                                      bd.d_beta, wc, cur);
+                                                      bd.d_beta, d_wi, wc, cur);
             RB2_CUDA(cudaGetLastError(), "BDPT camera shade");
             rb2dev::k_bd_stats<<<1, 1, 0, s>>>(wc);
             rb2dev::QueueSource nee{bn, bw, bv.triidx, ps.qs, &wc->n_shadow, ps.sray, &wc->head_shadow,

@@ -22,6 +22,7 @@ struct rb2_scene_dev {
     uint32_t* d_lights = nullptr;  // emissive triangle ids
     rb2dev::MaterialDev* d_mats = nullptr;  // layered materials (null: one Lambertian layer = albedo)
     bool layered = false;                   // some non-emitter material is not a single Lambertian layer
+    bool has_delta = false;                 // some non-emitter material has a mirror or glass layer
     uint32_t nv = 0, ntri = 0, n_mat = 0, n_lights = 0;
     uint64_t bytes = 0;
 };
@@ -64,10 +65,12 @@ struct BdptState {
     float4* s_pos = nullptr;    // xyz, w = light-subpath vertex count s (as float)
     float4* s_nrm = nullptr;    // normal facing the arriving light, w = material id bits
     float4* s_beta = nullptr;
+    float4* s_wi = nullptr;     // toward the previous light vertex, w = sign of ng . nrm
     uint8_t* s_valid = nullptr;
     float4* d_pos = nullptr;
     float4* d_nrm = nullptr;
     float4* d_beta = nullptr;
+    float4* d_wi = nullptr;
     uint32_t* block_sums = nullptr;
     uint64_t cap_slots = 0;
     // connection rays of camera vertices (connections per path)
@@ -102,7 +105,7 @@ struct rb2_integrator {
     {
         return cap_rays * 32 + cap_hits * 16 + cap_count * 4 + 16 * 8 + cap_accum * 16 + cap_film_xy * 8 +
                ps.cap * (16 * 8 + 12) +
-               sizeof(WaveCounters) + bd.cap_paths * (32 + 16 + 16 + 8) + bd.cap_slots * (6 * 16 + 1) +
+               sizeof(WaveCounters) + bd.cap_paths * (32 + 16 + 16 + 8) + bd.cap_slots * (8 * 16 + 1) +
                bd.cap_conn * (32 + 16 + 4);
     }
 };
