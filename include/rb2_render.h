@@ -191,7 +191,9 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
 
 /* Wavefront path tracing (PathIntegratorParams, core/params.h:88-94;
  * integrators/integrator_path.cu:43-283, the reference's declared
- * MODE_MULTI_KERNEL3).  Lambertian surfaces, next-event estimation to a
+ * MODE_MULTI_KERNEL3).  Lambertian surfaces, or the scene's layered
+ * materials (rb2_scene_set_materials; emission after a specular bounce takes
+ * full weight), next-event estimation to a
  * uniformly chosen emissive triangle combined with BSDF sampling by the
  * balance heuristic, Russian roulette from bounce rr_start with continue
  * probability min(rr_prob, luminance(throughput)) and division by it.
@@ -220,7 +222,11 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
  * (k <= max_path_length) is weighted 1/k: all k strategies are sampled, so the
  * estimator is unbiased.  (The reference weights connections by
  * 1/((bounce+1)+depth) but gives NEE full weight and omits the cache-size
- * factor.)  d_rgb[3*pixel] = mean radiance over spp iterations. */
+ * factor.)  Layered materials are supported when no non-emitter material has a
+ * mirror or glass layer (else RB2_ENOTSUP): vertices take f from the material
+ * functions, and light subpaths continue with the adjoint f(sampled -> incoming)
+ * because the Blinn microfacet's shadowing term is not symmetric.
+ * d_rgb[3*pixel] = mean radiance over spp iterations. */
 typedef struct {
     uint32_t spp;
     uint32_t max_path_length;   /* segments, camera to light (config 3: 6) */

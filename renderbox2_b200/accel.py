@@ -228,6 +228,11 @@ class CudaTracer:
         cfg = LaunchConfig(0, ctas_per_sm, fetch_threshold, 0)
         check(lib().rb2_tracer_set_launch(self._t, C.byref(cfg)))
 
+    def set_node_order(self, order: int):
+        """Node layout of the bulk traversals: NODE_ORDER_DFS (the Compact2
+        buffer as built), NODE_ORDER_BFS or NODE_ORDER_WIDE4."""
+        check(lib().rb2_tracer_set_node_order(self._t, int(order)))
+
     def trace(self, rays, any_hit: bool = False, stencil=None, out=None, stream=None):
         """rays: CUDA float32 tensor (n, 8).  Returns an int32 tensor (n, 4) of
         (prim, t bits, u bits, v bits); see hits_view()."""
@@ -292,6 +297,7 @@ def hits_view(hits):
 
 
 MODE_CLOSEST, MODE_ANY, MODE_OCCLUSION = 0, 1, 2
+NODE_ORDER_DFS, NODE_ORDER_BFS, NODE_ORDER_WIDE4 = 0, 1, 2
 
 
 class TraceBatch:
