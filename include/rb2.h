@@ -128,9 +128,12 @@ typedef struct {
  * contiguous), or a 4-wide layout collapsed from the binary tree (up to four
  * exact child boxes per 128-byte node; the same leaves and Woop triangles, so
  * hits are identical except which of two triangles at the same t is
- * reported).  Integrators and rb2_tracer_dev_bvh always use the binary
- * Compact2 buffer. */
-enum { RB2_NODE_ORDER_DFS = 0, RB2_NODE_ORDER_BFS = 1, RB2_NODE_ORDER_WIDE4 = 2 };
+ * reported), or a compressed 8-wide layout (RB2_NODE_ORDER_CW8: eight child
+ * boxes quantized to 8 bits per plane in an 80-byte node, conservatively
+ * enlarged, and the same Woop triangles stored per node; closest hits are
+ * identical except for ties in t).  Integrators and rb2_tracer_dev_bvh always
+ * use the binary Compact2 buffer. */
+enum { RB2_NODE_ORDER_DFS = 0, RB2_NODE_ORDER_BFS = 1, RB2_NODE_ORDER_WIDE4 = 2, RB2_NODE_ORDER_CW8 = 3 };
 
 /* Ray-query modes. */
 enum { RB2_MODE_CLOSEST = 0, RB2_MODE_ANY = 1, RB2_MODE_OCCLUSION = 2 };
@@ -208,6 +211,16 @@ int rb2_tracer_status(rb2_tracer* t, uint32_t* status, void* stream);
 /* Re-uploads the tracer's nodes in another order (RB2_NODE_ORDER_*); results
  * are unchanged, only memory locality differs.  Synchronises the device. */
 int rb2_tracer_set_node_order(rb2_tracer* t, uint32_t order);
+
+/* The compressed 8-wide layout of a host BVH, as the tracer builds it for
+ * RB2_NODE_ORDER_CW8, for tools and tests: call with NULL arrays for the
+ * counts, then with arrays of n_nodes * 20, n_tris * 12 and n_tris words
+ * (node words, Woop rows, original triangle ids). */
+typedef struct {
+    uint32_t n_nodes, n_tris, depth, reserved;
+} rb2_cw8_counts;
+int rb2_bvh_cw8_layout(const rb2_host_bvh* bvh, rb2_cw8_counts* counts, uint32_t* nodes, uint32_t* woop,
+                       uint32_t* triidx);
 
 /* -------------------------------------------------------------- batching --
  * Many scenes and ray batches of uneven size in ONE persistent launch: every

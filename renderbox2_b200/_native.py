@@ -32,6 +32,10 @@ class BvhCounts(C.Structure):
     ]
 
 
+class Cw8Counts(C.Structure):
+    _fields_ = [("n_nodes", C.c_uint32), ("n_tris", C.c_uint32), ("depth", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class LaunchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("ctas_per_sm", C.c_uint32),
                 ("fetch_threshold", C.c_uint32), ("regs", C.c_uint32)]
@@ -139,6 +143,7 @@ SIGNATURES = {
     "rb2_trace_occlusion": (C.c_int, [P, P, U32, P, P, P]),
     "rb2_tracer_status": (C.c_int, [P, C.POINTER(U32), P]),
     "rb2_tracer_set_node_order": (C.c_int, [P, U32]),
+    "rb2_bvh_cw8_layout": (C.c_int, [P, C.POINTER(Cw8Counts), P, P, P]),
     "rb2_tracer_dev_bvh": (C.c_int, [P, C.POINTER(DevBvh)]),
     "rb2_trace_per_thread": (C.c_int, [P, P, U32, I32, P, P, P]),
     "rb2_scene_dev_view": (C.c_int, [P, C.POINTER(DevScene)]),

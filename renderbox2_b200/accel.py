@@ -16,7 +16,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from ._native import BuildParams as _BuildParams
-from ._native import BvhCounts, LaunchConfig, check, lib
+from ._native import BvhCounts, Cw8Counts, LaunchConfig, check, lib
 
 
 def _ptr(a) -> int:
@@ -190,6 +190,18 @@ class BVH:
     def get_tri_index_buffer(self) -> np.ndarray:
         return self._buf(lib().rb2_bvh_triidx, self.counts().n_triidx, 1)
 
+    def cw8_layout(self) -> dict:
+        """The compressed 8-wide layout the tracer builds for NODE_ORDER_CW8:
+        nodes (n, 20) uint32 words, woop (n_tris, 12) uint32 Woop rows, triidx
+        (n_tris,) original triangle ids, depth (wide levels)."""
+        c = Cw8Counts()
+        check(lib().rb2_bvh_cw8_layout(self._h, C.byref(c), None, None, None))
+        nodes = np.zeros((c.n_nodes, 20), np.uint32)
+        woop = np.zeros((c.n_tris, 12), np.uint32)
+        tri = np.zeros((c.n_tris,), np.uint32)
+        check(lib().rb2_bvh_cw8_layout(self._h, C.byref(c), _ptr(nodes), _ptr(woop), _ptr(tri)))
+        return {"nodes": nodes, "woop": woop, "triidx": tri, "depth": int(c.depth)}
+
     def serialize(self, path: str) -> None:
         check(lib().rb2_bvh_save(self._h, str(path).encode()))
 
@@ -230,7 +242,7 @@ class CudaTracer:
 
     def set_node_order(self, order: int):
         """Node layout of the bulk traversals: NODE_ORDER_DFS (the Compact2
-        buffer as built), NODE_ORDER_BFS or NODE_ORDER_WIDE4."""
+        buffer as built), NODE_ORDER_BFS, NODE_ORDER_WIDE4 or NODE_ORDER_CW8."""
         check(lib().rb2_tracer_set_node_order(self._t, int(order)))
 
     def trace(self, rays, any_hit: bool = False, stencil=None, out=None, stream=None):
@@ -297,7 +309,7 @@ def hits_view(hits):
 
 
 MODE_CLOSEST, MODE_ANY, MODE_OCCLUSION = 0, 1, 2
-NODE_ORDER_DFS, NODE_ORDER_BFS, NODE_ORDER_WIDE4 = 0, 1, 2
+NODE_ORDER_DFS, NODE_ORDER_BFS, NODE_ORDER_WIDE4, NODE_ORDER_CW8 = 0, 1, 2, 3
 
 
 class TraceBatch:

@@ -113,6 +113,17 @@ int build_tree(const float* v, uint32_t nv, const uint32_t* idx, uint32_t ntri, 
 int validate_compact2(const uint32_t* nodes, uint64_t n_nodes_u4, const uint32_t* woop, uint64_t n_woop_u4,
                       const uint32_t* triidx, uint64_t n_triidx, uint32_t n_tris_hint, uint32_t* max_depth_out);
 
+// Compressed 8-wide layout (rb2_cw8.cpp) collapsed from a Compact2 buffer set
+// that validate_compact2 accepted.
+struct Cw8Layout {
+    std::vector<uint32_t> nodes;   // 20 words per node
+    std::vector<uint32_t> woop;    // 12 words (3 Woop rows) per triangle
+    std::vector<uint32_t> triidx;  // original triangle id per triangle
+    uint32_t n_nodes = 0, n_tris = 0, depth = 0;
+};
+int collapse_cw8(const uint32_t* nodes, uint64_t n_nodes_u4, const uint32_t* woop, const uint32_t* triidx,
+                 Cw8Layout& out);
+
 // Device view of a tracer's BVH (defined in rb2_trace.cu) for integrator kernels.
 struct DeviceBvhView {
     const void* nodes;    // float4*

@@ -6,6 +6,7 @@
 #pragma once
 
 #include "rb2_traverse.cuh"
+#include "rb2_traverse_cw8.cuh"
 
 namespace rb2dev {
 
@@ -24,6 +25,9 @@ struct JobDesc {
 static_assert(sizeof(JobDesc) == 64, "job descriptor layout");
 
 constexpr uint32_t kMaxSmemJobs = 1024;
+
+// Node layouts of the traversal kernel variants.
+enum Layout : int { kLayoutBinary = 0, kLayoutWide4 = 1, kLayoutCw8 = 2 };
 
 struct KernelArgs {
     const JobDesc* jobs;                 // nullptr: use inline_job (n_jobs == 1)
@@ -118,8 +122,9 @@ __host__ __device__ constexpr size_t job_smem_bytes(uint32_t n_jobs, bool inline
 // REGS is the register budget per thread the variant is compiled for (64:
 // 32 resident warps per SM, 48: 40 warps, 40: 48 warps; lower budgets spill a
 // little state to L1).  The autotuner picks the variant by measurement.
-// WIDE: the jobs' node buffers hold the 4-wide layout (kWideEmpty, rb2_traverse.cuh).
-template <int BLOCK, int REGS = 64, bool WIDE = false>
+// LAYOUT: what the jobs' node buffers hold: kLayoutBinary (Compact2),
+// kLayoutWide4 (kWideEmpty, rb2_traverse.cuh) or kLayoutCw8 (rb2_traverse_cw8.cuh).
+template <int BLOCK, int REGS = 64, int LAYOUT = kLayoutBinary>
 __global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK) k_trace_jobs(const __grid_constant__ KernelArgs a)
 {
     extern __shared__ unsigned long long s_start[];
@@ -148,7 +153,8 @@ __global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK) k_trace_jobs(co
     src.counter = a.counter;
     src.chunk = a.chunk;
     src.rem = s_rem;
-    persistent_trace<JobSource, WIDE>(src, a.fetch_threshold, a.status);
+    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8<JobSource>(src, a.fetch_threshold, a.status);
+    else persistent_trace<JobSource, LAYOUT == kLayoutWide4>(src, a.fetch_threshold, a.status);
 }
 
 }  // namespace rb2dev

@@ -80,11 +80,18 @@ int cuda_fail(cudaError_t e, const char* what)
     } while (0)
 
 // Kernel variants: block shape {64, 128, 256} x register budget {64, 48, 40}
-// x node layout {binary, 4-wide}.
+// x node layout {binary, 4-wide, compressed 8-wide}.
 struct Occupancy {
     int sms = 0;
-    int per_sm[3][3][2] = {};  // [block index][register-budget index][wide]
+    int per_sm[3][3][3] = {};  // [block index][register-budget index][rb2dev::Layout]
 };
+
+// Kernel layout of a node order.
+int layout_of(uint32_t node_order)
+{
+    return node_order == RB2_NODE_ORDER_WIDE4 ? rb2dev::kLayoutWide4
+                                              : (node_order == RB2_NODE_ORDER_CW8 ? rb2dev::kLayoutCw8 : rb2dev::kLayoutBinary);
+}
 
 int block_index(uint32_t block) { return block == 64 ? 0 : (block == 256 ? 2 : 1); }
 int regs_index(uint32_t regs) { return regs == 48 ? 1 : (regs == 40 ? 2 : 0); }
@@ -92,8 +99,12 @@ int regs_index(uint32_t regs) { return regs == 48 ? 1 : (regs == 40 ? 2 : 0); }
 template <int B, int R>
 int occ_of(int* out, size_t smem)
 {
-    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&out[0], rb2dev::k_trace_jobs<B, R, false>, B, smem), "occupancy");
-    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&out[1], rb2dev::k_trace_jobs<B, R, true>, B, smem), "occupancy");
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&out[0], rb2dev::k_trace_jobs<B, R, rb2dev::kLayoutBinary>, B, smem),
+             "occupancy");
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&out[1], rb2dev::k_trace_jobs<B, R, rb2dev::kLayoutWide4>, B, smem),
+             "occupancy");
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&out[2], rb2dev::k_trace_jobs<B, R, rb2dev::kLayoutCw8>, B, smem),
+             "occupancy");
     return RB2_OK;
 }
 
@@ -110,13 +121,13 @@ int occupancy(Occupancy& o)
     return rc ? RB2_ECUDA : RB2_OK;
 }
 
-template <int B, int R, bool W>
+template <int B, int R, int W>
 void launch_variant(const rb2dev::KernelArgs& a, unsigned blocks, size_t smem, cudaStream_t s)
 {
     rb2dev::k_trace_jobs<B, R, W><<<blocks, B, smem, s>>>(a);
 }
 
-template <bool W>
+template <int W>
 void launch_shape(int variant, const rb2dev::KernelArgs& a, unsigned g, size_t smem, cudaStream_t s)
 {
     switch (variant) {
@@ -135,10 +146,10 @@ void launch_shape(int variant, const rb2dev::KernelArgs& a, unsigned g, size_t s
 // Launches the persistent kernel: grid = SMs x resident CTAs per SM, capped
 // by the work available.
 int launch_jobs(const rb2dev::KernelArgs& a, uint64_t total_rays, uint32_t block, uint32_t ctas_per_sm, uint32_t regs,
-                bool wide, const Occupancy& occ, cudaStream_t s)
+                int layout, const Occupancy& occ, cudaStream_t s)
 {
     const int bi = block_index(block), ri = regs_index(regs);
-    const int max_per_sm = std::max(1, occ.per_sm[bi][ri][wide ? 1 : 0]);
+    const int max_per_sm = std::max(1, occ.per_sm[bi][ri][layout]);
     const uint32_t per_sm = ctas_per_sm ? std::min<uint32_t>(ctas_per_sm, (uint32_t)max_per_sm) : (uint32_t)max_per_sm;
     uint64_t blocks = (uint64_t)occ.sms * per_sm;
     const uint64_t warps_needed = (total_rays + 31) / 32;
@@ -146,8 +157,9 @@ int launch_jobs(const rb2dev::KernelArgs& a, uint64_t total_rays, uint32_t block
     blocks = std::min<uint64_t>(blocks, (warps_needed + bthreads / 32 - 1) / (bthreads / 32));
     blocks = std::max<uint64_t>(blocks, 1);
     const size_t smem = rb2dev::job_smem_bytes(a.n_jobs, a.jobs == nullptr);
-    if (wide) launch_shape<true>(bi * 3 + ri, a, (unsigned)blocks, smem, s);
-    else launch_shape<false>(bi * 3 + ri, a, (unsigned)blocks, smem, s);
+    if (layout == rb2dev::kLayoutWide4) launch_shape<rb2dev::kLayoutWide4>(bi * 3 + ri, a, (unsigned)blocks, smem, s);
+    else if (layout == rb2dev::kLayoutCw8) launch_shape<rb2dev::kLayoutCw8>(bi * 3 + ri, a, (unsigned)blocks, smem, s);
+    else launch_shape<rb2dev::kLayoutBinary>(bi * 3 + ri, a, (unsigned)blocks, smem, s);
     RB2_CUDA(cudaGetLastError(), "trace launch");
     return RB2_OK;
 }
@@ -258,6 +270,9 @@ struct rb2_tracer {
     uint32_t binary_order = RB2_NODE_ORDER_DFS; // order held by d_nodes (integrators use it)
     float4* d_wide = nullptr;                   // 4-wide layout, built on first use
     uint64_t n_wide_u4 = 0;
+    float4* d_cw_nodes = nullptr;               // compressed 8-wide layout, built on first use
+    float4* d_cw_woop = nullptr;
+    uint32_t* d_cw_triidx = nullptr;            // per Woop row, as d_triidx
     unsigned long long* d_counters = nullptr;  // kSlots queue heads
     unsigned int* d_status = nullptr;
     uint32_t slot = 0;
@@ -282,9 +297,10 @@ namespace {
 rb2dev::JobDesc job_of(const rb2_tracer* t, const float* rays, uint64_t n, uint32_t mode, const uint8_t* mask, void* out)
 {
     rb2dev::JobDesc d{};
-    d.nodes = t->node_order == RB2_NODE_ORDER_WIDE4 ? t->d_wide : t->d_nodes;
-    d.woop = t->d_woop;
-    d.triidx = t->d_triidx;
+    const bool cw = t->node_order == RB2_NODE_ORDER_CW8;
+    d.nodes = t->node_order == RB2_NODE_ORDER_WIDE4 ? t->d_wide : (cw ? t->d_cw_nodes : t->d_nodes);
+    d.woop = cw ? t->d_cw_woop : t->d_woop;
+    d.triidx = cw ? t->d_cw_triidx : t->d_triidx;
     d.rays = reinterpret_cast<const float4*>(rays);
     d.mask = mask;
     d.out = out;
@@ -309,10 +325,48 @@ int trace_single(rb2_tracer* t, const float* d_rays, uint64_t n, uint32_t mode, 
     a.counter = counter;
     a.status = t->d_status;
     const uint32_t block = t->cfg.block_threads ? t->cfg.block_threads : kDefaultBlock;
-    return launch_jobs(a, n, block, t->cfg.ctas_per_sm, t->cfg.regs, t->node_order == RB2_NODE_ORDER_WIDE4, t->occ, s);
+    return launch_jobs(a, n, block, t->cfg.ctas_per_sm, t->cfg.regs, layout_of(t->node_order), t->occ, s);
 }
 
 bool valid_regs(uint32_t r) { return r == 0 || r == 64 || r == 48 || r == 40; }
+
+// Builds the compressed 8-wide layout from the tracer's Compact2 buffers and
+// uploads it (nodes, Woop rows, and a triangle id per Woop row so hit records
+// index it as they index the binary buffer).
+int upload_cw8(rb2_tracer* t)
+{
+    std::vector<uint32_t> woop(t->n_woop_u4 * 4), triidx(t->n_woop_u4);
+    RB2_CUDA(cudaDeviceSynchronize(), "sync before re-layout");
+    RB2_CUDA(cudaMemcpy(woop.data(), t->d_woop, woop.size() * 4, cudaMemcpyDeviceToHost), "Woop read");
+    RB2_CUDA(cudaMemcpy(triidx.data(), t->d_triidx, triidx.size() * 4, cudaMemcpyDeviceToHost), "index read");
+    Cw8Layout cw;
+    int rc = collapse_cw8(t->host_nodes.data(), t->host_nodes.size() / 4, woop.data(), triidx.data(), cw);
+    if (rc) return rc;
+    if (cw.depth > (uint32_t)rb2dev::kStackSizeCw8)
+        return fail(RB2_ENOTSUP, "tree too deep for the compressed 8-wide layout's stack");
+    std::vector<uint32_t> tri3((size_t)cw.n_tris * 3 + 4, 0u);
+    for (uint32_t i = 0; i < cw.n_tris; i++) tri3[(size_t)i * 3] = cw.triidx[i];
+    const size_t nb = cw.nodes.size() * 4, wb = std::max<size_t>(cw.woop.size() * 4, 16), ib = tri3.size() * 4;
+    float4 *dn = nullptr, *dw = nullptr;
+    uint32_t* di = nullptr;
+    cudaError_t e;
+    if ((e = cudaMalloc(&dn, nb)) != cudaSuccess || (e = cudaMalloc(&dw, wb)) != cudaSuccess ||
+        (e = cudaMalloc(&di, ib)) != cudaSuccess) {
+        cudaFree(dn); cudaFree(dw); cudaFree(di);
+        return fail(RB2_ENOMEM, std::string("compressed 8-wide layout: ") + cudaGetErrorString(e));
+    }
+    if ((e = cudaMemcpy(dn, cw.nodes.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(dw, cw.woop.data(), cw.woop.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(di, tri3.data(), ib, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        cudaFree(dn); cudaFree(dw); cudaFree(di);
+        return cuda_fail(e, "compressed 8-wide upload");
+    }
+    t->d_cw_nodes = dn;
+    t->d_cw_woop = dw;
+    t->d_cw_triidx = di;
+    t->device_bytes += nb + wb + ib;
+    return RB2_OK;
+}
 
 }  // namespace
 
@@ -375,6 +429,9 @@ int rb2_tracer_destroy(rb2_tracer* t)
     cudaFree(t->d_hits);
     cudaFree(t->d_mask);
     cudaFree(t->d_wide);
+    cudaFree(t->d_cw_nodes);
+    cudaFree(t->d_cw_woop);
+    cudaFree(t->d_cw_triidx);
     delete t;
     return RB2_OK;
 }
@@ -393,8 +450,16 @@ int rb2_tracer_set_launch(rb2_tracer* t, const rb2_launch_config* cfg)
 int rb2_tracer_set_node_order(rb2_tracer* t, uint32_t order)
 {
     if (!t) return fail(RB2_EINVAL, "null argument");
-    if (order > RB2_NODE_ORDER_WIDE4) return fail(RB2_EINVAL, "unknown node order");
+    if (order > RB2_NODE_ORDER_CW8) return fail(RB2_EINVAL, "unknown node order");
     if (order == t->node_order) return RB2_OK;
+    if (order == RB2_NODE_ORDER_CW8) {
+        if (!t->d_cw_nodes) {
+            int rc = upload_cw8(t);
+            if (rc) return rc;
+        }
+        t->node_order = order;
+        return RB2_OK;
+    }
     if (order == RB2_NODE_ORDER_WIDE4) {
         if (!t->d_wide) {
             std::vector<uint32_t> wide;
@@ -530,7 +595,7 @@ int batch_enqueue(rb2_batch* b, cudaStream_t s)
     a.counter = b->d_counter;
     a.status = b->d_status;
     return launch_jobs(a, b->total, b->cfg.block_threads ? b->cfg.block_threads : kDefaultBlock, b->cfg.ctas_per_sm,
-                       b->cfg.regs, b->cfg.node_order == RB2_NODE_ORDER_WIDE4, b->occ, s);
+                       b->cfg.regs, layout_of(b->cfg.node_order), b->occ, s);
 }
 
 // The job table points at each tracer's current layout; a tracer shared
@@ -538,7 +603,7 @@ int batch_enqueue(rb2_batch* b, cudaStream_t s)
 int batch_check_layout(const rb2_batch* b)
 {
     for (const rb2_tracer* t : b->unique_tracers)
-        if ((t->node_order == RB2_NODE_ORDER_WIDE4) != (b->cfg.node_order == RB2_NODE_ORDER_WIDE4))
+        if (layout_of(t->node_order) != layout_of(b->cfg.node_order))
             return fail(RB2_EINVAL, "a tracer's node layout changed since rb2_batch_set_config; set it again");
     return RB2_OK;
 }
@@ -632,7 +697,7 @@ int rb2_batch_set_config(rb2_batch* b, const rb2_batch_config* cfg)
     if (cfg->block_threads && cfg->block_threads != 64 && cfg->block_threads != 128 && cfg->block_threads != 256)
         return fail(RB2_ENOTSUP, "block_threads must be 64, 128 or 256");
     if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
-    if (cfg->node_order > RB2_NODE_ORDER_WIDE4) return fail(RB2_EINVAL, "unknown node order");
+    if (cfg->node_order > RB2_NODE_ORDER_CW8) return fail(RB2_EINVAL, "unknown node order");
     if (!valid_regs(cfg->regs)) return fail(RB2_ENOTSUP, "regs must be 64, 48 or 40");
     b->drop_graph();
     for (rb2_tracer* t : b->unique_tracers) {
@@ -690,7 +755,8 @@ int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream)
     return RB2_OK;
 }
 
-// Coordinate-descent autotuner: node layout (DFS, BFS, 4-wide) x block shape x
+// Coordinate-descent autotuner: node layout (DFS, BFS, 4-wide, compressed
+// 8-wide) x block shape x
 // register budget jointly, then resident CTAs
 // per SM, fetch threshold and queue chunk: each candidate is timed with CUDA
 // events (median of `reps` launches after one warm-up) and the fastest kept.
@@ -742,7 +808,7 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     double best_ms = 0;
     int rc = time_cfg(best, best_ms);
     if (rc) return rc;
-    const uint32_t orders[] = {RB2_NODE_ORDER_DFS, RB2_NODE_ORDER_BFS, RB2_NODE_ORDER_WIDE4};
+    const uint32_t orders[] = {RB2_NODE_ORDER_DFS, RB2_NODE_ORDER_BFS, RB2_NODE_ORDER_WIDE4, RB2_NODE_ORDER_CW8};
     const uint32_t blocks[] = {64, 128, 256};
     const uint32_t regs[] = {64, 48, 40};
     const uint32_t thresholds[] = {8, 16, 20, 24, 28};
@@ -762,7 +828,7 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
             }
         }
         const int maxc = std::max(
-            1, b->occ.per_sm[block_index(best.block_threads)][regs_index(best.regs)][best.node_order == RB2_NODE_ORDER_WIDE4]);
+            1, b->occ.per_sm[block_index(best.block_threads)][regs_index(best.regs)][layout_of(best.node_order)]);
         for (int k : {maxc, std::max(1, maxc * 3 / 4), std::max(1, maxc / 2)}) {
             rb2_batch_config c = best; c.ctas_per_sm = (uint32_t)k; double ms;
             if ((rc = time_cfg(c, ms))) return rc;

@@ -1,0 +1,221 @@
+// Persistent traversal of the compressed 8-wide layout (RB2_NODE_ORDER_CW8,
+// node format in rb2_cw8.cpp), after Ylitie, Karras and Laine, "Efficient
+// Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs" (HPG 2017).
+//
+// Per lane: a node group (child_base of a visited node and a mask of its hit
+// inner children, bits 24-31 in octant-permuted order, the node's inner-child
+// mask in bits 0-7), a triangle group (tri_base and a mask of hit leaf
+// triangles, bits 0-23) and a stack of node groups.  The warp walks nodes
+// until every busy lane holds triangles (the counterpart of the binary
+// kernel's postponed leaf), then tests triangles, then refills lanes from the
+// ray source as the binary kernel does (same RaySource policy, same dynamic
+// fetch).  Triangles are the binary layout's Woop rows with the same test
+// arithmetic, so an accepted hit has the same t, u, v bits; boxes are
+// conservative, so the closest hit equals the binary traversal's except for
+// exact ties in t.
+#pragma once
+
+#include <cuda_fp16.h>
+
+#include "rb2_traverse.cuh"
+
+namespace rb2dev {
+
+// Node groups on the stack: at most one per wide level.  The host refuses a
+// layout deeper than this (rb2_tracer_set_node_order).
+constexpr int kStackSizeCw8 = 72;
+constexpr uint32_t kCw8NodeWords = 20;
+
+// Two quantized planes (bytes 2h and 2h + 1 of w) as floats 1024 + q: each
+// byte becomes the mantissa of a half-precision 1024 (0x64xx), converted
+// exactly.  The 1024 is folded into the per-node slab offset.
+__device__ __forceinline__ float2 cw8_planes(uint32_t w, int h)
+{
+    const uint32_t p = __byte_perm(w, 0x6464u, h ? 0x4342u : 0x4140u);
+    const __half2 v = *reinterpret_cast<const __half2*>(&p);
+    return __half22float2(v);
+}
+
+// Woop test of one triangle (the binary leaf loop's arithmetic); updates
+// hitT / hitIndex and returns true when it accepts.
+__device__ __forceinline__ bool cw8_triangle(Lane& L, int triAddr)
+{
+    const float4* wp = L.woop + triAddr;
+    const float4 v00 = __ldg(wp + 0);
+    const float4 v11 = __ldg(wp + 1);
+    const float4 v22 = __ldg(wp + 2);
+    const float Oz = __fmaf_rn(-L.oz, v00.z, __fmaf_rn(-L.oy, v00.y, __fmaf_rn(-L.ox, v00.x, v00.w)));
+    const float Dz = __fmaf_rn(L.dz, v00.z, __fmaf_rn(L.dy, v00.y, __fmul_rn(L.dx, v00.x)));
+    const float t = __fmul_rn(Oz, __fdiv_rn(1.0f, Dz));
+    if (!(t > L.tmin && t < L.hitT)) return false;
+    const float Ox = __fmaf_rn(L.oz, v11.z, __fmaf_rn(L.oy, v11.y, __fmaf_rn(L.ox, v11.x, v11.w)));
+    const float Dx = __fmaf_rn(L.dz, v11.z, __fmaf_rn(L.dy, v11.y, __fmul_rn(L.dx, v11.x)));
+    const float u = __fmaf_rn(t, Dx, Ox);
+    if (!(u >= 0.0f)) return false;
+    const float Oy = __fmaf_rn(L.oz, v22.z, __fmaf_rn(L.oy, v22.y, __fmaf_rn(L.ox, v22.x, v22.w)));
+    const float Dy = __fmaf_rn(L.dz, v22.z, __fmaf_rn(L.dy, v22.y, __fmul_rn(L.dx, v22.x)));
+    const float v = __fmaf_rn(t, Dy, Oy);
+    if (!(v >= 0.0f && __fadd_rn(u, v) <= 1.0f)) return false;
+    L.hitT = t;
+    L.hitIndex = triAddr;
+    return true;
+}
+
+template <class Source>
+__device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch_threshold, unsigned int* status)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    uint2 stack[kStackSizeCw8];
+    int sp = 0;
+    Lane L;
+    L.hitIndex = -1;
+    uint32_t ng_base = 0, ng_bits = 0, tg_base = 0, tg_bits = 0;
+    bool has_ray = false, retired = false;
+
+    for (;;) {
+        // ---- refill: lanes without a ray claim the next slots from the queue.
+        const bool need = !has_ray && !retired;
+        const unsigned needm = __ballot_sync(kFull, need);
+        if (needm) {
+            const int leader = __ffs(needm) - 1;
+            unsigned long long b1 = 0, b2 = 0;
+            unsigned n1 = 0;
+            if ((int)lane == leader) src.claim((unsigned)__popc(needm), b1, n1, b2);
+            b1 = __shfl_sync(kFull, b1, leader);
+            b2 = __shfl_sync(kFull, b2, leader);
+            n1 = __shfl_sync(kFull, n1, leader);
+            if (need) {
+                const unsigned rank = (unsigned)__popc(needm & lt_mask);
+                const unsigned long long slot = rank < n1 ? b1 + rank : b2 + (rank - n1);
+                const int r = src.fetch(slot, L);
+                if (r == 0) {
+                    retired = true;
+                } else if (r > 0) {
+                    sp = 0;
+                    ng_base = 0;             // the root: node 0, reached through bit 31
+                    ng_bits = 0x80000000u;   // with an empty inner-child mask
+                    tg_bits = 0;
+                    has_ray = true;
+                }
+            }
+        }
+        if (__all_sync(kFull, retired)) break;
+
+        while (__any_sync(kFull, has_ray)) {
+            // ---- nodes, until every busy lane holds triangles or is done.
+            for (;;) {
+                const bool in = has_ray && tg_bits == 0 && (ng_bits > 0x00FFFFFFu || sp > 0);
+                if (!__any_sync(kFull, in)) break;
+                if (in) {
+                    if (ng_bits <= 0x00FFFFFFu) {
+                        --sp;
+                        ng_base = stack[sp].x;
+                        ng_bits = stack[sp].y;
+                    }
+                    const uint32_t oct_inv = 7u ^ ((__float_as_uint(L.idx) >> 31) | ((__float_as_uint(L.idy) >> 31) << 1) |
+                                                   ((__float_as_uint(L.idz) >> 31) << 2));
+                    const uint32_t k = 31u - (uint32_t)__clz(ng_bits);
+                    ng_bits &= ~(1u << k);
+                    const uint32_t slot = (k - 24u) ^ oct_inv;
+                    const uint32_t node = ng_base + (uint32_t)__popc(ng_bits & ((1u << slot) - 1u));
+                    bool ok = true;
+                    if (ng_bits > 0x00FFFFFFu) {
+                        if (sp >= kStackSizeCw8) {
+                            // Unreachable for layouts whose depth was validated; a corrupt
+                            // layout abandons the ray and reports it.
+                            atomicOr(status, kStatusStack);
+                            ok = false;
+                        } else {
+                            stack[sp].x = ng_base;
+                            stack[sp].y = ng_bits;
+                            ++sp;
+                        }
+                    }
+                    if (!ok) {
+                        L.hitIndex = -1;
+                        ng_bits = 0;
+                        sp = 0;
+                    } else {
+                        const float4* np = L.nodes + (size_t)node * (kCw8NodeWords / 4);
+                        const float4 h0 = __ldg(np + 0), h1 = __ldg(np + 1);
+                        const float4 qx = __ldg(np + 2), qy = __ldg(np + 3), qz = __ldg(np + 4);
+                        const uint32_t ew = __float_as_uint(h0.w);
+                        const float sx = __fmul_rn(__uint_as_float((ew & 0xFFu) << 23), L.idx);
+                        const float sy = __fmul_rn(__uint_as_float(((ew >> 8) & 0xFFu) << 23), L.idy);
+                        const float sz = __fmul_rn(__uint_as_float(((ew >> 16) & 0xFFu) << 23), L.idz);
+                        // Slab offsets less 1024 cells (planes arrive as 1024 + q).
+                        const float ax = __fmaf_rn(-1024.0f, sx, __fmul_rn(__fsub_rn(h0.x, L.ox), L.idx));
+                        const float ay = __fmaf_rn(-1024.0f, sy, __fmul_rn(__fsub_rn(h0.y, L.oy), L.idy));
+                        const float az = __fmaf_rn(-1024.0f, sz, __fmul_rn(__fsub_rn(h0.z, L.oz), L.idz));
+                        // Near and far plane words per axis (the high plane is near for a
+                        // negative direction), children 0-3 in the first word, 4-7 in the second.
+                        const bool rx = L.idx < 0.0f, ry = L.idy < 0.0f, rz = L.idz < 0.0f;
+                        const uint32_t nx0 = __float_as_uint(rx ? qx.z : qx.x), nx1 = __float_as_uint(rx ? qx.w : qx.y);
+                        const uint32_t fx0 = __float_as_uint(rx ? qx.x : qx.z), fx1 = __float_as_uint(rx ? qx.y : qx.w);
+                        const uint32_t ny0 = __float_as_uint(ry ? qy.z : qy.x), ny1 = __float_as_uint(ry ? qy.w : qy.y);
+                        const uint32_t fy0 = __float_as_uint(ry ? qy.x : qy.z), fy1 = __float_as_uint(ry ? qy.y : qy.w);
+                        const uint32_t nz0 = __float_as_uint(rz ? qz.z : qz.x), nz1 = __float_as_uint(rz ? qz.w : qz.y);
+                        const uint32_t fz0 = __float_as_uint(rz ? qz.x : qz.z), fz1 = __float_as_uint(rz ? qz.y : qz.w);
+                        // Meta bytes, four children per word: inner children (offset >= 24,
+                        // bits 4 and 3 set) get their slot permuted by the ray octant; each
+                        // child contributes its unary bits at its (permuted) index.
+                        uint32_t bidx[2], cbit[2];
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const uint32_t m = __float_as_uint(h ? h1.w : h1.z);
+                            const uint32_t inner = (m & (m << 1)) & 0x10101010u;
+                            bidx[h] = (m ^ ((inner >> 4) * oct_inv)) & 0x1F1F1F1Fu;
+                            cbit[h] = (m >> 5) & 0x07070707u;
+                        }
+                        uint32_t hits = 0;
+#pragma unroll
+                        for (int s = 0; s < 8; s += 2) {
+                            const int w = s >> 2, hh = (s >> 1) & 1;
+                            const float2 nx = cw8_planes(w ? nx1 : nx0, hh), fx = cw8_planes(w ? fx1 : fx0, hh);
+                            const float2 ny = cw8_planes(w ? ny1 : ny0, hh), fy = cw8_planes(w ? fy1 : fy0, hh);
+                            const float2 nz = cw8_planes(w ? nz1 : nz0, hh), fz = cw8_planes(w ? fz1 : fz0, hh);
+#pragma unroll
+                            for (int e = 0; e < 2; e++) {
+                                const float tnx = __fmaf_rn(e ? nx.y : nx.x, sx, ax), tfx = __fmaf_rn(e ? fx.y : fx.x, sx, ax);
+                                const float tny = __fmaf_rn(e ? ny.y : ny.x, sy, ay), tfy = __fmaf_rn(e ? fy.y : fy.x, sy, ay);
+                                const float tnz = __fmaf_rn(e ? nz.y : nz.x, sz, az), tfz = __fmaf_rn(e ? fz.y : fz.x, sz, az);
+                                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, L.tmin));
+                                const float tf = fminf(fminf(tfx, tfy), fminf(tfz, L.hitT));
+                                if (tn <= tf) {
+                                    const uint32_t sel = 0x4440u | (uint32_t)((s + e) & 3);
+                                    hits |= __byte_perm(cbit[w], 0u, sel) << __byte_perm(bidx[w], 0u, sel);
+                                }
+                            }
+                        }
+                        ng_base = __float_as_uint(h1.x);
+                        ng_bits = (hits & 0xFF000000u) | (ew >> 24);
+                        tg_base = __float_as_uint(h1.y);
+                        tg_bits = hits & 0x00FFFFFFu;
+                    }
+                }
+            }
+
+            // ---- triangles of the current group, then finish lanes with no work left.
+            if (has_ray) {
+                while (tg_bits) {
+                    const int i = __ffs(tg_bits) - 1;
+                    tg_bits &= tg_bits - 1u;
+                    if (cw8_triangle(L, 3 * (int)(tg_base + (uint32_t)i)) && L.mode() != kClosest) {
+                        tg_bits = 0;
+                        ng_bits = 0;
+                        sp = 0;
+                    }
+                }
+                if (ng_bits <= 0x00FFFFFFu && sp == 0) {
+                    src.finish(L);
+                    has_ray = false;
+                }
+            }
+            // Dynamic fetch (kepler_dynamic_fetch.h:308-310).
+            if ((unsigned)__popc(__ballot_sync(kFull, has_ray)) < fetch_threshold) break;
+        }
+    }
+}
+
+}  // namespace rb2dev

@@ -1,0 +1,104 @@
+"""CPU tests of the compressed 8-wide layout (RB2_NODE_ORDER_CW8) that the
+tracer collapses from the binary Compact2 tree: every triangle reference of
+the binary leaves is present exactly once, node indices and triangle ranges
+are in bounds, and the leaf holding the oracle's closest hit is reachable: the
+hit point lies inside the leaf's quantized box and every ancestor's, so the
+conservative box tests of the wide traversal cannot miss it."""
+import collections
+
+import numpy as np
+import pytest
+
+
+def _decode(nodes):
+    n = nodes.shape[0]
+    b = nodes.view(np.uint8).reshape(n, 80)
+    p = nodes[:, 0:3].view(np.float32).astype(np.float64)
+    scale = np.ldexp(1.0, b[:, 12:15].astype(np.int32) - 127)
+    imask = b[:, 15].astype(np.uint32)
+    child_base = nodes[:, 4].astype(np.int64)
+    tri_base = nodes[:, 5].astype(np.int64)
+    meta = b[:, 24:32].astype(np.uint32)
+    q = {}
+    for a, (lo, hi) in enumerate(((32, 40), (48, 56), (64, 72))):
+        q[("lo", a)] = b[:, lo:lo + 8].astype(np.float64)
+        q[("hi", a)] = b[:, hi:hi + 8].astype(np.float64)
+    lo = np.stack([p[:, a:a + 1] + q[("lo", a)] * scale[:, a:a + 1] for a in range(3)], -1)  # (n, 8, 3)
+    hi = np.stack([p[:, a:a + 1] + q[("hi", a)] * scale[:, a:a + 1] for a in range(3)], -1)
+    return imask, child_base, tri_base, meta, lo, hi
+
+
+def _binary_leaf_refs(bvh):
+    nodes, woop, tri = bvh.buffers_view()
+    refs = []
+    for w in nodes.reshape(-1, 16)[:, 12:14].view(np.int32).ravel():
+        if w < 0:
+            k = ~int(w)
+            while woop[k, 0] != 0x80000000:
+                refs.append(int(tri[k]))
+                k += 3
+    return refs
+
+
+@pytest.mark.parametrize("seed,n_tris,n_boxes", [(3, 2_000, 4), (8, 40_000, 30)])
+def test_cw8_layout_is_complete_and_conservative(rb, orc, seed, n_tris, n_boxes):
+    sc = rb.heightfield_for_triangles(seed=seed, n_tris=n_tris, n_boxes=n_boxes)
+    bvh = rb.BVH(sc)
+    cw = bvh.cw8_layout()
+    nodes, triidx = cw["nodes"], cw["triidx"]
+    n, nt = nodes.shape[0], triidx.shape[0]
+    assert 1 <= cw["depth"] <= 72
+    assert collections.Counter(triidx.tolist()) == collections.Counter(_binary_leaf_refs(bvh))
+    # Woop rows are the binary layout's rows of the same references.
+    nodes_b, woop_b, tri_b = bvh.buffers_view()
+    rows_b = collections.defaultdict(set)
+    for w in nodes_b.reshape(-1, 16)[:, 12:14].view(np.int32).ravel():
+        if w < 0:
+            k = ~int(w)
+            while woop_b[k, 0] != 0x80000000:
+                rows_b[int(tri_b[k])].add(woop_b[k:k + 3].tobytes())
+                k += 3
+    for i in range(nt):
+        assert cw["woop"][i].tobytes() in rows_b[int(triidx[i])]
+    imask, child_base, tri_base, meta, lo, hi = _decode(nodes)
+    parent = {}
+    tri_loc = collections.defaultdict(list)
+    for i in range(n):
+        for s in range(8):
+            m = int(meta[i, s])
+            if m == 0:
+                continue
+            off, bits = m & 31, m >> 5
+            if off >= 24:
+                assert bits == 1 and off == 24 + s and (imask[i] >> s) & 1
+                c = int(child_base[i]) + bin(int(imask[i]) & ((1 << s) - 1)).count("1")
+                assert 0 < c < n and c not in parent
+                parent[c] = (i, s)
+            else:
+                assert bits in (1, 3, 7) and not (imask[i] >> s) & 1
+                cnt = bits.bit_length()
+                assert off + cnt <= 24 and int(tri_base[i]) + off + cnt <= nt
+                for k in range(cnt):
+                    tri_loc[int(triidx[int(tri_base[i]) + off + k])].append((i, s))
+    assert len(parent) == n - 1          # a tree: every node but the root has one parent
+    # Reachability of the oracle's closest hits.
+    r, _ = rb.surface_rays(sc, seed=seed + 1, n=3000)
+    want = orc.trace(*bvh.buffers_view(), r)
+    hit = np.nonzero(want["prim"] >= 0)[0]
+    assert hit.size > 100
+    for k in hit:
+        P = r[k, :3].astype(np.float64) + float(want["t"][k]) * r[k, 4:7].astype(np.float64)
+        ok = False
+        for node, s in tri_loc[int(want["prim"][k])]:
+            inside = True
+            while True:
+                if not ((lo[node, s] <= P).all() and (P <= hi[node, s]).all()):
+                    inside = False
+                    break
+                if node == 0:
+                    break
+                node, s = parent[node]
+            if inside:
+                ok = True
+                break
+        assert ok, f"ray {k}: hit point outside every chain of boxes of triangle {want['prim'][k]}"

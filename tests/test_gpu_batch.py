@@ -2,9 +2,9 @@
 and uneven ray batches in one persistent launch must give exactly the
 results of per-scene launches, for every launch configuration the autotuner
 can pick, including graph replay and the breadth-first node order.  With the
-4-wide node layout the traversal order differs, so closest hits must be equal
-except at confirmed ties, any-hit jobs must agree on occlusion, and
-occlusion jobs must be byte-identical."""
+4-wide and compressed 8-wide node layouts the traversal order differs, so
+closest hits must be equal except at confirmed ties, any-hit jobs must agree
+on occlusion, and occlusion jobs must be byte-identical."""
 import numpy as np
 import pytest
 
@@ -83,7 +83,8 @@ def test_batch_equals_plain_launches(rb, orc, cuda):
     dict(block_threads=64), dict(block_threads=256), dict(chunk=4), dict(chunk=8, fetch_threshold=8),
     dict(node_order=1), dict(ctas_per_sm=2, fetch_threshold=32), dict(regs=48), dict(regs=40, block_threads=256),
     dict(regs=40, block_threads=64, chunk=2), dict(node_order=2), dict(node_order=2, regs=48, block_threads=256),
-    dict(node_order=2, regs=40, chunk=4),
+    dict(node_order=2, regs=40, chunk=4), dict(node_order=3), dict(node_order=3, regs=48, block_threads=256),
+    dict(node_order=3, regs=40, chunk=4, fetch_threshold=8),
 ])
 def test_batch_configs_give_identical_results(rb, orc, cuda, cfg):
     scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
@@ -92,7 +93,7 @@ def test_batch_configs_give_identical_results(rb, orc, cuda, cfg):
     for o in outs:
         o.fill_(7)
     batch.launch()
-    if cfg.get("node_order") == 2:
+    if cfg.get("node_order") in (2, 3):
         _check_any_layout(rb, orc, scenes, jobs, outs, plain, cuda)
     else:
         _check(outs, plain, cuda)
@@ -104,7 +105,7 @@ def test_graph_replay_and_autotune(rb, orc, cuda):
     scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
     batch = rb.TraceBatch(jobs)
     best, ms = batch.autotune(reps=2)
-    assert ms > 0 and best["block_threads"] in (64, 128, 256) and best["node_order"] in (0, 1, 2)
+    assert ms > 0 and best["block_threads"] in (64, 128, 256) and best["node_order"] in (0, 1, 2, 3)
     s = cuda.cuda.Stream()
     batch.capture(s)
     for _ in range(2):
@@ -164,3 +165,33 @@ def test_bfs_node_order_on_single_tracer(rb, cuda):
     rb.lib().rb2_tracer_set_node_order(tr.handle, 1)
     b = tr.trace(d)
     assert cuda.equal(a, b)
+
+
+@pytest.mark.parametrize("seed,n_tris,n_boxes,n_rays", [(15, 300_000, 40, 200_000), (21, 4_000, 64, 100_000)])
+def test_cw8_layout_single_tracer(rb, orc, cuda, seed, n_tris, n_boxes, n_rays):
+    """A tracer switched to the compressed 8-wide layout: closest hits equal
+    the oracle's but for confirmed ties, occlusion is byte-identical, the
+    status word stays clean, and switching back restores the binary results."""
+    from parity import compare_closest
+    sc = rb.heightfield_for_triangles(seed=seed, n_tris=n_tris, n_boxes=n_boxes)
+    bvh = rb.BVH(sc)
+    tr = rb.CudaTracer(bvh)
+    r, _ = rb.surface_rays(sc, seed=seed + 1, n=n_rays)
+    r[::4, 4:7] *= -1.0
+    d = cuda.from_numpy(r).cuda()
+    a = tr.trace(d).cpu().numpy()
+    occ_a = tr.trace_occlusion(d).cpu().numpy()
+    assert rb.lib().rb2_tracer_set_node_order(tr.handle, rb.NODE_ORDER_CW8) == 0
+    b = tr.trace(d).cpu().numpy()
+    occ_b = tr.trace_occlusion(d).cpu().numpy()
+    anyh = tr.trace(d, any_hit=True).cpu().numpy()
+    assert tr.status() == 0
+    assert np.array_equal(occ_a, occ_b)
+    assert np.array_equal(anyh[:, 0] >= 0, a[:, 0] >= 0)
+    nodes, woop, tri = bvh.buffers_view()
+    want = orc.trace(nodes, woop, tri, r)
+    ties, bad, first = compare_closest(orc, b, {k: want[k] for k in ("prim", "t", "u", "v")}, woop, tri, r)
+    print("cw8 ties", ties)
+    assert bad == 0, f"ray {first} vs oracle"
+    assert rb.lib().rb2_tracer_set_node_order(tr.handle, rb.NODE_ORDER_DFS) == 0
+    assert np.array_equal(tr.trace(d).cpu().numpy(), a)
