@@ -296,10 +296,15 @@ def run_rb2(args, rank, world, local_rank):
     achieved = alg_per_launch / launch_s / 1e9
     # DRAM traffic per launch: the ncu capture of the same batched kernel on
     # 8 scenes x 500k triangles with 4.19M incoherent rays, half closest hit /
-    # half occlusion (profiles/k_trace_jobs_batched_8x500k_full.md), measured
-    # 618.5 MB of DRAM traffic against 7961.2 MB of algorithmic bytes; scaled
-    # to this launch by algorithmic bytes.
-    traffic = alg_per_launch * (618.5 / 7961.2)
+    # half occlusion, measured against 7961.2 MB of algorithmic bytes: 618.5 MB
+    # for the binary layout (profiles/k_trace_jobs_batched_8x500k_full.md) and
+    # 452.0 MB for the compressed 8-wide layout
+    # (profiles/k_trace_jobs_cw8_batched_8x500k_full.md); scaled to this launch
+    # by algorithmic bytes.
+    cw8 = tuned is not None and tuned.get("node_order") == 3
+    traffic = alg_per_launch * ((452.0 if cw8 else 618.5) / 7961.2)
+    layout_name = {0: "binary DFS", 1: "binary BFS", 2: "4-wide", 3: "compressed 8-wide"}.get(
+        (tuned or {}).get("node_order", 0), "binary DFS")
 
     cpu_baseline = builder = None
     if rank == 0 and world == 1:
@@ -335,7 +340,8 @@ def run_rb2(args, rank, world, local_rank):
         "plain_any_hit_mrays": round(world * (total_rays - n_ch_total) * args.steps / (ah_ms.sum() / 1e3) / 1e6, 2),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(achieved / hbm_peak, 4), "traffic": round(traffic),
-                     "kernel": "k_trace_jobs<BLOCK> (batched, 1 launch/step)", "peak_source": peak_src,
+                     "kernel": f"k_trace_jobs<BLOCK, REGS, LAYOUT> (batched, 1 launch/step, {layout_name} nodes)",
+                     "peak_source": peak_src,
                      "alg_bytes_per_launch": round(alg_per_launch),
                      "alg_bytes_per_ray": round(alg_per_launch / total_rays, 1),
                      "traffic_source": "scaled from ncu dram bytes of the 8 x 500k-triangle batched capture"},

@@ -211,6 +211,7 @@ int rb2_tracer_status(rb2_tracer* t, uint32_t* status, void* stream);
 /* Re-uploads the tracer's nodes in another order (RB2_NODE_ORDER_*); results
  * are unchanged, only memory locality differs.  Synchronises the device. */
 int rb2_tracer_set_node_order(rb2_tracer* t, uint32_t order);
+int rb2_tracer_get_node_order(const rb2_tracer* t, uint32_t* order);
 
 /* The compressed 8-wide layout of a host BVH, as the tracer builds it for
  * RB2_NODE_ORDER_CW8, for tools and tests: call with NULL arrays for the

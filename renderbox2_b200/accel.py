@@ -242,8 +242,15 @@ class CudaTracer:
 
     def set_node_order(self, order: int):
         """Node layout of the bulk traversals: NODE_ORDER_DFS (the Compact2
-        buffer as built), NODE_ORDER_BFS, NODE_ORDER_WIDE4 or NODE_ORDER_CW8."""
+        buffer as built), NODE_ORDER_BFS, NODE_ORDER_WIDE4 or NODE_ORDER_CW8.
+        Integrators traverse the compressed 8-wide layout when it is set, the
+        binary buffer otherwise."""
         check(lib().rb2_tracer_set_node_order(self._t, int(order)))
+
+    def node_order(self) -> int:
+        v = C.c_uint32()
+        check(lib().rb2_tracer_get_node_order(self._t, C.byref(v)))
+        return v.value
 
     def trace(self, rays, any_hit: bool = False, stencil=None, out=None, stream=None):
         """rays: CUDA float32 tensor (n, 8).  Returns an int32 tensor (n, 4) of

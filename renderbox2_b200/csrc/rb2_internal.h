@@ -124,14 +124,17 @@ struct Cw8Layout {
 int collapse_cw8(const uint32_t* nodes, uint64_t n_nodes_u4, const uint32_t* woop, const uint32_t* triidx,
                  Cw8Layout& out);
 
-// Device view of a tracer's BVH (defined in rb2_trace.cu) for integrator kernels.
+// Device view of a tracer's BVH (defined in rb2_trace.cu) for integrator
+// kernels: the compressed 8-wide layout when the tracer uses it and the caller
+// can traverse it (cw8 set), else the binary Compact2 buffer.
 struct DeviceBvhView {
     const void* nodes;    // float4*
     const void* woop;     // float4*
     const uint32_t* triidx;
     unsigned int* status;
+    bool cw8;
 };
-DeviceBvhView device_bvh(const rb2_tracer* t);
+DeviceBvhView device_bvh(const rb2_tracer* t, bool allow_cw8 = false);
 
 // Checks a film filter description (rb2_film_table.cpp).
 int validate_filter(const rb2_filter* f);

@@ -13,6 +13,7 @@
 #include "rb2_material.cuh"
 #include "rb2_shading.cuh"
 #include "rb2_traverse.cuh"
+#include "rb2_traverse_cw8.cuh"
 
 #include <cuda_runtime.h>
 
@@ -111,12 +112,13 @@ struct AoSource {
 };
 
 // Integrator traversal: block BLOCK, register budget REGS (64: 32 warps per
-// SM, 48: 40 warps), binary Compact2 layout.
-template <int BLOCK, int REGS, class Src>
+// SM, 48: 40 warps), binary Compact2 or compressed 8-wide layout.
+template <int BLOCK, int REGS, class Src, int LAYOUT>
 __global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK)
     k_persistent(Src src, uint32_t fetch_threshold, unsigned int* status)
 {
-    persistent_trace(src, fetch_threshold, status);
+    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8(src, fetch_threshold, status);
+    else persistent_trace(src, fetch_threshold, status);
 }
 
 __global__ void k_ao_finalize(const int4* hits, const uint32_t* counts, uint32_t npix, uint32_t samples, float* out)
@@ -913,43 +915,54 @@ __global__ void k_pt_finalize(const float4* accum, uint32_t npix, float inv_spp,
 
 namespace {
 
-template <int B, int R, class Src>
+template <int B, int R, int LAYOUT, class Src>
 int launch_persistent_variant(const Src& src, uint64_t work, int sms, uint32_t threshold, unsigned int* status,
                               cudaStream_t s)
 {
     int per_sm = 0;
-    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb2dev::k_persistent<B, R, Src>, B, 0), "occupancy");
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb2dev::k_persistent<B, R, Src, LAYOUT>, B, 0),
+             "occupancy");
     uint64_t blocks = (uint64_t)sms * (uint64_t)std::max(1, per_sm);
     blocks = std::min<uint64_t>(blocks, (work + B - 1) / B);
     blocks = std::max<uint64_t>(blocks, 1);
-    rb2dev::k_persistent<B, R, Src><<<(unsigned)blocks, B, 0, s>>>(src, threshold, status);
+    rb2dev::k_persistent<B, R, Src, LAYOUT><<<(unsigned)blocks, B, 0, s>>>(src, threshold, status);
     RB2_CUDA(cudaGetLastError(), "persistent launch");
     return RB2_OK;
 }
 
-template <class Src>
+template <int LAYOUT, class Src>
 int launch_persistent_shape(const Src& src, uint64_t work, const rb2_integrator* it, unsigned int* status, cudaStream_t s)
 {
     const uint32_t th = it->tr_threshold;
     if (it->tr_block == 256)
-        return it->tr_regs == 48 ? launch_persistent_variant<256, 48>(src, work, it->sms, th, status, s)
-                                 : launch_persistent_variant<256, 64>(src, work, it->sms, th, status, s);
-    return it->tr_regs == 48 ? launch_persistent_variant<128, 48>(src, work, it->sms, th, status, s)
-                             : launch_persistent_variant<128, 64>(src, work, it->sms, th, status, s);
+        return it->tr_regs == 48 ? launch_persistent_variant<256, 48, LAYOUT>(src, work, it->sms, th, status, s)
+                                 : launch_persistent_variant<256, 64, LAYOUT>(src, work, it->sms, th, status, s);
+    return it->tr_regs == 48 ? launch_persistent_variant<128, 48, LAYOUT>(src, work, it->sms, th, status, s)
+                             : launch_persistent_variant<128, 64, LAYOUT>(src, work, it->sms, th, status, s);
 }
 
-// With timing on, each traversal launch is bracketed by an event pair.
 template <class Src>
-int launch_persistent(const Src& src, uint64_t work, rb2_integrator* it, unsigned int* status, cudaStream_t s)
+int launch_persistent_layout(const Src& src, uint64_t work, const rb2_integrator* it, unsigned int* status, bool cw8,
+                             cudaStream_t s)
 {
-    if (!it->timing) return launch_persistent_shape(src, work, it, status, s);
+    return cw8 ? launch_persistent_shape<rb2dev::kLayoutCw8>(src, work, it, status, s)
+               : launch_persistent_shape<rb2dev::kLayoutBinary>(src, work, it, status, s);
+}
+
+// With timing on, each traversal launch is bracketed by an event pair.  The
+// layout is the view's (the tracer's compressed 8-wide layout when it uses one).
+template <class Src>
+int launch_persistent(const Src& src, uint64_t work, rb2_integrator* it, const DeviceBvhView& bv, cudaStream_t s)
+{
+    unsigned int* status = bv.status;
+    if (!it->timing) return launch_persistent_layout(src, work, it, status, bv.cw8, s);
     while (it->ev.size() < it->ev_used + 2) {
         cudaEvent_t e;
         RB2_CUDA(cudaEventCreate(&e), "timing event");
         it->ev.push_back(e);
     }
     RB2_CUDA(cudaEventRecord(it->ev[it->ev_used], s), "timing event");
-    const int rc = launch_persistent_shape(src, work, it, status, s);
+    const int rc = launch_persistent_layout(src, work, it, status, bv.cw8, s);
     if (rc) return rc;
     RB2_CUDA(cudaEventRecord(it->ev[it->ev_used + 1], s), "timing event");
     it->ev_used += 2;
@@ -1189,7 +1202,7 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
     // 3. AO rays generated and traced in one persistent launch, unoccluded counts per pixel.
     RB2_CUDA(cudaMemsetAsync(it->d_count, 0, npix * sizeof(uint32_t), s), "AO count reset");
     RB2_CUDA(cudaMemsetAsync(it->d_counters, 0, sizeof(unsigned long long), s), "queue reset");
-    const DeviceBvhView bv = device_bvh(it->tracer);
+    const DeviceBvhView bv = device_bvh(it->tracer, true);
     rb2dev::AoSource src;
     src.nodes = static_cast<const float4*>(bv.nodes);
     src.woop = static_cast<const float4*>(bv.woop);
@@ -1204,7 +1217,7 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
     src.samples = p->samples;
     src.radius = p->radius;
     src.seed = p->seed;
-    if ((rc = launch_persistent(src, src.n_slots, it, bv.status, s))) return rc;
+    if ((rc = launch_persistent(src, src.n_slots, it, bv, s))) return rc;
     // 4. AO = unoccluded fraction (misses contribute 0, integrator_ao.cu:56-84).
     rb2dev::k_ao_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_hits, it->d_count, (uint32_t)npix, p->samples, d_ao);
     RB2_CUDA(cudaGetLastError(), "AO finalize");
@@ -1243,7 +1256,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
     ca.width = cam->width; ca.height = cam->height; ca.spp = 1; ca.jitter = 1; ca.seed = p->seed;
     const rb2_scene_dev* sd = it->scene;
     rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights, sd->d_mats};
-    const DeviceBvhView bv = device_bvh(it->tracer);
+    const DeviceBvhView bv = device_bvh(it->tracer, true);
     WaveCounters* wc = it->d_wave;
     const unsigned g = grid_for(P, it->sms);
     for (uint32_t s0 = 0; s0 < p->spp; s0 += spw) {
@@ -1258,7 +1271,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
             rb2dev::QueueSource ext{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop), bv.triidx,
                                     ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext, rb2dev::kClosest,
                                     ps.hit, nullptr, nullptr};
-            if ((rc = launch_persistent(ext, paths, it, bv.status, s))) return rc;
+            if ((rc = launch_persistent(ext, paths, it, bv, s))) return rc;
             rb2dev::k_pt_shade<<<g, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, s0, b, p->max_depth, p->rr_start, p->rr_prob,
                                                 ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L, ps.sray, ps.sc,
                                                 ps.qs, wc, cur);
@@ -1267,7 +1280,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
             rb2dev::QueueSource shadow{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop),
                                        bv.triidx, ps.qs, &wc->n_shadow, ps.sray, &wc->head_shadow,
                                        rb2dev::kOcclusion, nullptr, ps.L, ps.sc};
-            if ((rc = launch_persistent(shadow, paths, it, bv.status, s))) return rc;
+            if ((rc = launch_persistent(shadow, paths, it, bv, s))) return rc;
             cur ^= 1u;
         }
         if (filtered)
@@ -1323,7 +1336,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     ca.width = cam->width; ca.height = cam->height; ca.spp = 1; ca.jitter = 1; ca.seed = p->seed;
     const rb2_scene_dev* sd = it->scene;
     rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights, sd->d_mats};
-    const DeviceBvhView bv = device_bvh(it->tracer);
+    const DeviceBvhView bv = device_bvh(it->tracer, true);
     const float4* bn = static_cast<const float4*>(bv.nodes);
     const float4* bw = static_cast<const float4*>(bv.woop);
     WaveCounters* wc = it->d_wave;
@@ -1345,7 +1358,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
             rb2dev::QueueSource lsrc{bn, bw, bv.triidx, bd.lq[cur], &wc->n_ext[cur], bd.lray, &wc->head_ext,
                                      rb2dev::kClosest, bd.lhit, nullptr, nullptr};
-            if ((rc = launch_persistent(lsrc, NL, it, bv.status, s))) return rc;
+            if ((rc = launch_persistent(lsrc, NL, it, bv, s))) return rc;
             rb2dev::k_bd_light_shade<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)iter * NL, d, Dl, p->rr_start, p->rr_prob,
                                                         bd.lq[cur], bd.lq[cur ^ 1u], bd.lray, bd.lhit, bd.lbeta, bd.s_pos,
                                                         bd.s_nrm, bd.s_beta, s_wi, bd.s_valid, wc, cur);
@@ -1366,7 +1379,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
             rb2dev::QueueSource ext{bn, bw, bv.triidx, ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext,
                                     rb2dev::kClosest, ps.hit, nullptr, nullptr};
-            if ((rc = launch_persistent(ext, npix, it, bv.status, s))) return rc;
+            if ((rc = launch_persistent(ext, npix, it, bv, s))) return rc;
             rb2dev::k_bd_cam_shade<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, iter, i, K, C, p->rr_start, p->rr_prob,
                                                       (float)NL, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L,
                                                       ps.sray, ps.sc, ps.qs, bd.cray, bd.cc, bd.cq, bd.d_pos, bd.d_nrm,
@@ -1375,10 +1388,10 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             rb2dev::k_bd_stats<<<1, 1, 0, s>>>(wc);
             rb2dev::QueueSource nee{bn, bw, bv.triidx, ps.qs, &wc->n_shadow, ps.sray, &wc->head_shadow,
                                     rb2dev::kOcclusion, nullptr, ps.L, ps.sc};
-            if ((rc = launch_persistent(nee, npix, it, bv.status, s))) return rc;
+            if ((rc = launch_persistent(nee, npix, it, bv, s))) return rc;
             rb2dev::QueueSource con{bn, bw, bv.triidx, bd.cq, &wc->n_conn, bd.cray, &wc->head_conn,
                                     rb2dev::kOcclusion, nullptr, nullptr, bd.cc};
-            if ((rc = launch_persistent(con, npix * C, it, bv.status, s))) return rc;
+            if ((rc = launch_persistent(con, npix * C, it, bv, s))) return rc;
             rb2dev::k_bd_conn_reduce<<<gc, 256, 0, s>>>(ps.q[cur], wc, cur, C, bd.cc, ps.L);
             RB2_CUDA(cudaGetLastError(), "BDPT connection reduce");
             cur ^= 1u;

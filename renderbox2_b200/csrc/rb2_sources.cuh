@@ -26,8 +26,6 @@ static_assert(sizeof(JobDesc) == 64, "job descriptor layout");
 
 constexpr uint32_t kMaxSmemJobs = 1024;
 
-// Node layouts of the traversal kernel variants.
-enum Layout : int { kLayoutBinary = 0, kLayoutWide4 = 1, kLayoutCw8 = 2 };
 
 struct KernelArgs {
     const JobDesc* jobs;                 // nullptr: use inline_job (n_jobs == 1)

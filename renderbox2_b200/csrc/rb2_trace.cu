@@ -492,6 +492,13 @@ int rb2_tracer_set_node_order(rb2_tracer* t, uint32_t order)
     return RB2_OK;
 }
 
+int rb2_tracer_get_node_order(const rb2_tracer* t, uint32_t* order)
+{
+    if (!t || !order) return fail(RB2_EINVAL, "null argument");
+    *order = t->node_order;
+    return RB2_OK;
+}
+
 int rb2_tracer_device_bytes(const rb2_tracer* t, uint64_t* bytes)
 {
     if (!t || !bytes) return fail(RB2_EINVAL, "null argument");
@@ -755,11 +762,12 @@ int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream)
     return RB2_OK;
 }
 
-// Coordinate-descent autotuner: node layout (DFS, BFS, 4-wide, compressed
-// 8-wide) x block shape x
-// register budget jointly, then resident CTAs
-// per SM, fetch threshold and queue chunk: each candidate is timed with CUDA
-// events (median of `reps` launches after one warm-up) and the fastest kept.
+// Autotuner: for each node layout (DFS, BFS, 4-wide, compressed 8-wide) a
+// coordinate-descent search of its launch shape (block x register budget
+// jointly, then resident CTAs per SM, then the fetch threshold); the fastest
+// layout gets a second pass and the queue chunk.  Each candidate is timed
+// with CUDA events (median of `reps` launches after one warm-up, cold L2) and
+// the fastest kept.
 int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best_out, double* best_ms_out)
 {
     if (!b) return fail(RB2_EINVAL, "null argument");
@@ -813,48 +821,61 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     const uint32_t regs[] = {64, 48, 40};
     const uint32_t thresholds[] = {8, 16, 20, 24, 28};
     const uint32_t chunks[] = {1, 2, 4, 8};
-    for (int pass = 0; pass < 2; pass++) {
-        // Layout, block shape and register budget interact (the 4-wide layout
-        // needs more registers), so they are searched jointly.
-        for (uint32_t o : orders) {
-            for (uint32_t bl : blocks) {
-                for (uint32_t rg : regs) {
-                    rb2_batch_config c = best;
-                    c.node_order = o; c.block_threads = bl; c.regs = rg; c.ctas_per_sm = 0;
-                    double ms;
-                    if ((rc = time_cfg(c, ms))) return rc;
-                    if (ms < best_ms) { best = c; best_ms = ms; }
-                }
+    // One coordinate-descent pass over the launch shape of a fixed layout:
+    // block x register budget jointly, then resident CTAs, then the threshold.
+    auto tune_shape = [&](rb2_batch_config& cur, double& cur_ms) -> int {
+        int rc2;
+        for (uint32_t bl : blocks) {
+            for (uint32_t rg : regs) {
+                rb2_batch_config c = cur;
+                c.block_threads = bl; c.regs = rg; c.ctas_per_sm = 0;
+                double ms;
+                if ((rc2 = time_cfg(c, ms))) return rc2;
+                if (ms < cur_ms) { cur = c; cur_ms = ms; }
             }
         }
-        const int maxc = std::max(
-            1, b->occ.per_sm[block_index(best.block_threads)][regs_index(best.regs)][layout_of(best.node_order)]);
+        const int maxc =
+            std::max(1, b->occ.per_sm[block_index(cur.block_threads)][regs_index(cur.regs)][layout_of(cur.node_order)]);
         for (int k : {maxc, std::max(1, maxc * 3 / 4), std::max(1, maxc / 2)}) {
-            rb2_batch_config c = best; c.ctas_per_sm = (uint32_t)k; double ms;
-            if ((rc = time_cfg(c, ms))) return rc;
-            if (ms < best_ms) { best = c; best_ms = ms; }
+            rb2_batch_config c = cur; c.ctas_per_sm = (uint32_t)k; double ms;
+            if ((rc2 = time_cfg(c, ms))) return rc2;
+            if (ms < cur_ms) { cur = c; cur_ms = ms; }
         }
         for (uint32_t th : thresholds) {
-            rb2_batch_config c = best; c.fetch_threshold = th; double ms;
-            if ((rc = time_cfg(c, ms))) return rc;
-            if (ms < best_ms) { best = c; best_ms = ms; }
+            rb2_batch_config c = cur; c.fetch_threshold = th; double ms;
+            if ((rc2 = time_cfg(c, ms))) return rc2;
+            if (ms < cur_ms) { cur = c; cur_ms = ms; }
         }
-        for (uint32_t ch : chunks) {
-            rb2_batch_config c = best; c.chunk = ch; double ms;
-            if ((rc = time_cfg(c, ms))) return rc;
-            if (ms < best_ms) { best = c; best_ms = ms; }
-        }
+        return RB2_OK;
+    };
+    // Each layout gets its own shape search (the layouts favour different
+    // register budgets and thresholds); the winner gets a second pass and the
+    // queue chunk.
+    std::vector<rb2_batch_config> per_layout;
+    for (uint32_t o : orders) {
+        rb2_batch_config c = best;
+        c.node_order = o;
+        double ms;
+        if ((rc = time_cfg(c, ms))) return rc;
+        if ((rc = tune_shape(c, ms))) return rc;
+        per_layout.push_back(c);
+        if (ms < best_ms) { best = c; best_ms = ms; }
     }
-    // Last look at the layout under the final launch shape, each candidate
-    // re-timed together with the incumbent so drift between passes cannot
-    // decide it.
+    if ((rc = tune_shape(best, best_ms))) return rc;
+    for (uint32_t ch : chunks) {
+        rb2_batch_config c = best; c.chunk = ch; double ms;
+        if ((rc = time_cfg(c, ms))) return rc;
+        if (ms < best_ms) { best = c; best_ms = ms; }
+    }
+    // Last look at the layouts, each with its own tuned shape, re-timed
+    // together with the incumbent so drift between searches cannot decide it.
     {
         double inc_ms;
         if ((rc = time_cfg(best, inc_ms))) return rc;
         best_ms = inc_ms;
-        for (uint32_t o : orders) {
-            if (o == best.node_order) continue;
-            rb2_batch_config c = best; c.node_order = o; double ms;
+        for (const rb2_batch_config& c : per_layout) {
+            if (c.node_order == best.node_order) continue;
+            double ms;
             if ((rc = time_cfg(c, ms))) return rc;
             if (ms < best_ms) { best = c; best_ms = ms; }
         }
@@ -901,9 +922,11 @@ int rb2_camera_rays_at(const rb2_camera* cam, const float* d_raster_xy, uint32_t
 }  // extern "C"
 
 namespace rb2 {
-DeviceBvhView device_bvh(const rb2_tracer* t)
+DeviceBvhView device_bvh(const rb2_tracer* t, bool allow_cw8)
 {
-    return DeviceBvhView{t->d_nodes, t->d_woop, t->d_triidx, t->d_status};
+    if (allow_cw8 && t->node_order == RB2_NODE_ORDER_CW8)
+        return DeviceBvhView{t->d_cw_nodes, t->d_cw_woop, t->d_cw_triidx, t->d_status, true};
+    return DeviceBvhView{t->d_nodes, t->d_woop, t->d_triidx, t->d_status, false};
 }
 
 unsigned long long* tracer_queue_counter(rb2_tracer* t) { return t->next_counter(); }

@@ -37,6 +37,9 @@ constexpr uint32_t kStatusStack = 1u;
 
 enum Mode : uint32_t { kClosest = 0, kAny = 1, kOcclusion = 2 };
 
+// Node layouts of the traversal kernel variants.
+enum Layout : int { kLayoutBinary = 0, kLayoutWide4 = 1, kLayoutCw8 = 2 };
+
 constexpr uint32_t kJobMask = 0x3FFFFFFFu;          // job index bits of Lane::tag
 constexpr uint64_t kMaxJobRays = 0xFFFFFFFFull;     // rays per job (Lane::ray is 32-bit)
 

@@ -207,7 +207,7 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                         sp = 0;
                     }
                 }
-                if (ng_bits <= 0x00FFFFFFu && sp == 0) {
+                if (tg_bits == 0 && ng_bits <= 0x00FFFFFFu && sp == 0) {
                     src.finish(L);
                     has_ray = false;
                 }

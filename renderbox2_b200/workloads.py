@@ -22,9 +22,11 @@ def _event_ms(fn, stream, reps=1):
     return e0.elapsed_time(e1) / reps
 
 
-def integrator(kind: str, warmup: int = 1, keep: dict | None = None):
+def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order: int | None = None):
     """Config 1 (AO), 2 (PT) or 3 (BDPT) at full size: samples/s and Mrays/s.
-    `keep` (optional dict) receives the scene, BVH and config used."""
+    `keep` (optional dict) receives the scene, BVH and config used.  The
+    traversal layout is `node_order`, or (None) the faster of the binary BFS
+    and the compressed 8-wide layout on one timed frame each."""
     import torch
 
     import renderbox2_b200 as rb
@@ -43,7 +45,8 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None):
                              n_lights=c["n_lights"], emission=c["emission"], room_size=c["room_size"])
     bvh = rb.BVH(scene)
     build_s = time.time() - t0
-    it = Integrator(rb.CudaTracer(bvh), DeviceScene(scene))
+    tracer = rb.CudaTracer(bvh)
+    it = Integrator(tracer, DeviceScene(scene))
     it.set_timing(True)  # traversal launches bracketed by CUDA events (stats "trace_ms")
     scale = c.get("room_size", 1.0)
     eye = [x * scale for x in c["eye"]]
@@ -69,6 +72,16 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None):
             out = torch.empty((npix, 3), dtype=torch.float32, device="cuda")
             run = lambda: it.render_bdpt(cam, p, out=out, stream=stream)  # noqa: E731
             samples = npix * c["spp"]
+        orders = [node_order] if node_order is not None else [rb.NODE_ORDER_BFS, rb.NODE_ORDER_CW8]
+        probe = {}
+        for o in orders:
+            tracer.set_node_order(o)
+            run()
+            torch.cuda.synchronize()
+            if len(orders) > 1:
+                probe[o] = _event_ms(run, stream)
+        if probe:
+            tracer.set_node_order(min(probe, key=probe.get))
         for _ in range(warmup):
             run()
         torch.cuda.synchronize()
@@ -83,7 +96,9 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None):
     return {"workload": kind, "triangles": scene.num_triangles, "width": c["width"], "height": c["height"],
             "samples": int(samples), "ms": round(ms, 3), "samples_per_s": round(samples / (ms / 1e3), 1),
             "mrays_per_s": round(rays / (ms / 1e3) / 1e6, 2), "rays": int(rays), "build_s": round(build_s, 2),
-            "stats": st, "image_mean": float(out.float().mean().item())}
+            "stats": st, "image_mean": float(out.float().mean().item()),
+            "node_order": {0: "dfs", 1: "bfs", 2: "wide4", 3: "cw8"}[tracer.node_order()],
+            "layout_probe_ms": {str(k): round(v, 3) for k, v in probe.items()}}
 
 
 def serving(n_jobs: int = 300, n_bvh: int = 32, seed: int = 5, slots: int = 8):

@@ -157,3 +157,35 @@ def test_bdpt_and_pt_agree_on_expectation(rb, cuda):
     rel = np.abs(bd.mean(0) - pt.mean(0)) / pt.mean(0)
     print("BDPT vs PT mean rel diff", rel)
     assert (rel < 0.03).all()
+
+
+def test_integrators_on_compressed_wide_layout(rb, cuda):
+    """With the tracer switched to the compressed 8-wide layout the
+    integrators trace through it; hits equal the binary traversal's except for
+    ties in t, so AO, PT and BDPT images are the binary-layout images (all but
+    a negligible fraction of pixels bit-identical)."""
+    from renderbox2_b200.configs import CONFIG2 as C2
+    from renderbox2_b200.render import (AmbientOcclusionIntegratorParams, BidirectionalPathIntegratorLvcParams,
+                                        DeviceScene, Integrator, PathIntegratorParams)
+    room = _room(rb)
+    tr = rb.CudaTracer(rb.BVH(room))
+    it = Integrator(tr, DeviceScene(room))
+    cam = rb.PerspectiveCamera(C2["eye"], C2["lookat"], C2["up"], (160, 90), C2["fov"])
+
+    def images():
+        ao = it.render_ao(cam, AmbientOcclusionIntegratorParams(samples=8, radius=0.5)).cpu().numpy()
+        pt = it.render_pt(cam, PathIntegratorParams(spp=8, max_depth=6)).cpu().numpy()
+        bd = it.render_bdpt(cam, BidirectionalPathIntegratorLvcParams(spp=4, max_path_length=6)).cpu().numpy()
+        return ao, pt, bd
+
+    ref = images()
+    assert tr.status() == 0
+    tr.set_node_order(rb.NODE_ORDER_CW8)
+    got = images()
+    assert tr.status() == 0
+    for name, a, b in zip(("ao", "pt", "bdpt"), ref, got):
+        assert np.isfinite(b).all()
+        diff = (a != b).reshape(a.shape[0], -1).any(axis=1).mean()
+        print(name, "differing pixels", diff)
+        assert diff <= 1e-3, name
+    tr.set_node_order(rb.NODE_ORDER_DFS)
