@@ -147,7 +147,7 @@ class BVH:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and h.value:
+        if h and h.value and lib is not None:  # lib is None at interpreter shutdown
             lib().rb2_host_bvh_free(h)
             self._h = C.c_void_p()
 
@@ -223,7 +223,7 @@ class CudaTracer:
 
     def __del__(self):
         t = getattr(self, "_t", None)
-        if t and t.value:
+        if t and t.value and lib is not None:  # lib is None at interpreter shutdown
             lib().rb2_tracer_destroy(t)
             self._t = C.c_void_p()
 
@@ -343,7 +343,7 @@ class TraceBatch:
 
     def __del__(self):
         b = getattr(self, "_b", None)
-        if b and b.value:
+        if b and b.value and lib is not None:  # lib is None at interpreter shutdown
             lib().rb2_batch_destroy(b)
             self._b = C.c_void_p()
 
@@ -398,7 +398,7 @@ class HostPipeline:
 
     def __del__(self):
         p = getattr(self, "_p", None)
-        if p and p.value:
+        if p and p.value and lib is not None:  # lib is None at interpreter shutdown
             lib().rb2_pipeline_destroy(p)
             self._p = C.c_void_p()
 

@@ -92,7 +92,7 @@ class DeviceScene:
 
     def __del__(self):
         s = getattr(self, "_s", None)
-        if s and s.value:
+        if s and s.value and lib is not None:  # lib is None at interpreter shutdown
             lib().rb2_scene_destroy(s)
             self._s = C.c_void_p()
 
@@ -261,7 +261,7 @@ class Integrator:
 
     def __del__(self):
         it = getattr(self, "_it", None)
-        if it and it.value:
+        if it and it.value and lib is not None:  # lib is None at interpreter shutdown
             lib().rb2_integrator_destroy(it)
             self._it = C.c_void_p()
 

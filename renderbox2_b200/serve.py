@@ -108,7 +108,7 @@ class Server:
 
     def __del__(self):
         s = getattr(self, "_s", None)
-        if s and s.value:
+        if s and s.value and _lib is not None:  # module globals are None at interpreter shutdown
             _lib().rb2_server_destroy(s)
             self._s = C.c_void_p()
 
