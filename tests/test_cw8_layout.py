@@ -40,10 +40,52 @@ def _binary_leaf_refs(bvh):
     return refs
 
 
+def _degenerate_scene(rb):
+    """300 coincident triangles (no split separates them, so the SBVH's
+    leaves hold hundreds of refs: the layout's ref-list nodes) among 50 small
+    scattered ones."""
+    rng = np.random.Generator(np.random.PCG64(1))
+    v, idx = [], []
+    for _ in range(300):
+        b = len(v)
+        v += [(0, 0, 0), (1, 0, 0), (0, 1, 0)]
+        idx.append((b, b + 1, b + 2))
+    for _ in range(50):
+        c = rng.uniform(-2, 2, 3)
+        b = len(v)
+        v += [tuple(c), tuple(c + rng.uniform(0, .2, 3)), tuple(c + rng.uniform(0, .2, 3))]
+        idx.append((b, b + 1, b + 2))
+    return rb.Scene().add_mesh(np.array(v, np.float32), np.array(idx, np.uint32))
+
+
+def _rays_at_cluster(n, seed):
+    """Rays from above and below the unit triangle toward points inside it."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    o = rng.uniform(-1.0, 2.0, (n, 3))
+    o[:, 2] = np.where(rng.uniform(size=n) < 0.5, 2.0, -2.0)
+    u = rng.uniform(size=(n, 2))
+    u = np.where(u.sum(1, keepdims=True) > 1, 1 - u, u)
+    tgt = np.stack([u[:, 0], u[:, 1], np.zeros(n)], 1)
+    d = tgt - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.zeros((n, 8), np.float32)
+    r[:, :3], r[:, 4:7], r[:, 7] = o, d, 3.0e38
+    return r
+
+
+def test_cw8_layout_splits_large_leaves(rb, orc):
+    bvh = rb.BVH(_degenerate_scene(rb))
+    _check_layout(rb, orc, bvh, _rays_at_cluster(2000, 5))
+
+
 @pytest.mark.parametrize("seed,n_tris,n_boxes", [(3, 2_000, 4), (8, 40_000, 30)])
 def test_cw8_layout_is_complete_and_conservative(rb, orc, seed, n_tris, n_boxes):
     sc = rb.heightfield_for_triangles(seed=seed, n_tris=n_tris, n_boxes=n_boxes)
-    bvh = rb.BVH(sc)
+    r, _ = rb.surface_rays(sc, seed=seed + 1, n=3000)
+    _check_layout(rb, orc, rb.BVH(sc), r)
+
+
+def _check_layout(rb, orc, bvh, r):
     cw = bvh.cw8_layout()
     nodes, triidx = cw["nodes"], cw["triidx"]
     n, nt = nodes.shape[0], triidx.shape[0]
@@ -82,7 +124,6 @@ def test_cw8_layout_is_complete_and_conservative(rb, orc, seed, n_tris, n_boxes)
                     tri_loc[int(triidx[int(tri_base[i]) + off + k])].append((i, s))
     assert len(parent) == n - 1          # a tree: every node but the root has one parent
     # Reachability of the oracle's closest hits.
-    r, _ = rb.surface_rays(sc, seed=seed + 1, n=3000)
     want = orc.trace(*bvh.buffers_view(), r)
     hit = np.nonzero(want["prim"] >= 0)[0]
     assert hit.size > 100

@@ -195,3 +195,25 @@ def test_cw8_layout_single_tracer(rb, orc, cuda, seed, n_tris, n_boxes, n_rays):
     assert bad == 0, f"ray {first} vs oracle"
     assert rb.lib().rb2_tracer_set_node_order(tr.handle, rb.NODE_ORDER_DFS) == 0
     assert np.array_equal(tr.trace(d).cpu().numpy(), a)
+
+
+def test_cw8_layout_with_ref_list_nodes(rb, orc, cuda):
+    """Leaves of hundreds of coincident triangles go into the compressed
+    layout's ref-list nodes: closest hits still equal the oracle's (ties
+    confirmed), occlusion is identical."""
+    from parity import compare_closest
+    from test_cw8_layout import _degenerate_scene, _rays_at_cluster
+    bvh = rb.BVH(_degenerate_scene(rb))
+    tr = rb.CudaTracer(bvh)
+    r = _rays_at_cluster(50_000, 7)
+    d = cuda.from_numpy(r).cuda()
+    occ_a = tr.trace_occlusion(d).cpu().numpy()
+    tr.set_node_order(rb.NODE_ORDER_CW8)
+    b = tr.trace(d).cpu().numpy()
+    assert np.array_equal(tr.trace_occlusion(d).cpu().numpy(), occ_a)
+    assert tr.status() == 0
+    nodes, woop, tri = bvh.buffers_view()
+    want = orc.trace(nodes, woop, tri, r)
+    ties, bad, first = compare_closest(orc, b, {k: want[k] for k in ("prim", "t", "u", "v")}, woop, tri, r)
+    print("cw8 ref-list ties", ties)
+    assert bad == 0, f"ray {first}"
