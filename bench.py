@@ -618,7 +618,7 @@ def main():
     ap.add_argument("--rays-per-scene", type=int, default=1 << 20)
     ap.add_argument("--ref-rays-per-scene", type=int, default=2048)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
-    ap.add_argument("--e2e-chunk", type=int, default=1 << 19, help="rays per chunk of the pipelined host path")
+    ap.add_argument("--e2e-chunk", type=int, default=1 << 20, help="rays per chunk of the pipelined host path")
     ap.add_argument("--e2e-depth", type=int, default=4, help="streams of the pipelined host path")
     ap.add_argument("--serve-jobs", type=int, default=300, help="config-5 jobs in the serving measurement (0: skip)")
     ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt"], default="trace",
