@@ -174,6 +174,13 @@ int rb2_integrator_device_bytes(const rb2_integrator* it, uint64_t* bytes);
  * fastest of the four shapes measured on configs 1-3, all within 3 % of each
  * other; ctas_per_sm is ignored).  Images do not depend on the shape. */
 int rb2_integrator_set_launch(rb2_integrator* it, const rb2_launch_config* cfg);
+/* Paths in flight per wave (0 = defaults: 32M paths for the path tracer,
+ * 8M camera paths for BDPT).  The path tracer runs as many samples per pixel
+ * at once as fit (unless rb2_pt_params.spp_per_wave is set); BDPT runs as many
+ * iterations at once as fit, each with its own light-vertex cache.  Larger
+ * waves mean larger traversal launches (less time in launch tails) and more
+ * device memory.  Unfiltered images do not depend on the wave size. */
+int rb2_integrator_set_wave(rb2_integrator* it, uint64_t paths);
 /* Film filter of the path tracer and BDPT (default RB2_FILTER_NONE); NULL resets. */
 int rb2_integrator_set_filter(rb2_integrator* it, const rb2_filter* f);
 

@@ -143,6 +143,7 @@ SIGNATURES = {
     "rb2_trace_occlusion": (C.c_int, [P, P, U32, P, P, P]),
     "rb2_tracer_status": (C.c_int, [P, C.POINTER(U32), P]),
     "rb2_tracer_set_node_order": (C.c_int, [P, U32]),
+    "rb2_integrator_set_wave": (C.c_int, [P, C.c_uint64]),
     "rb2_tracer_get_node_order": (C.c_int, [P, C.POINTER(U32)]),
     "rb2_bvh_cw8_layout": (C.c_int, [P, C.POINTER(Cw8Counts), P, P, P]),
     "rb2_tracer_dev_bvh": (C.c_int, [P, C.POINTER(DevBvh)]),

@@ -675,21 +675,46 @@ __global__ void k_lvc_scatter(const uint8_t* valid, uint64_t n_slots, const uint
     }
 }
 
+// Dense-cache offset of each iteration of a wave: the valid slots before slot
+// i x per_iter (i = 0..w), the scan's offset of the boundary's chunk plus a
+// count inside that chunk.  One block per boundary; a boundary at or past the
+// end gets the total.
+__global__ void k_lvc_wave_offsets(const uint8_t* valid, uint64_t n_slots, const uint32_t* block_offsets,
+                                   uint64_t per_iter, const WaveCountersDev* wc, uint32_t* lvc_off)
+{
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    const uint64_t b = (uint64_t)blockIdx.x * per_iter;
+    if (b >= n_slots) {  // uniform over the block
+        if (threadIdx.x == 0) lvc_off[blockIdx.x] = wc->lvc_count;
+        return;
+    }
+    const uint64_t chunk = b / kScanChunk;
+    uint32_t c = 0;
+    for (uint64_t k = chunk * kScanChunk + threadIdx.x; k < b; k += kScanThreads) c += valid[k];
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (uint32_t w = 0; w < kScanThreads / 32; w++) tot += s_warp[w];
+        lvc_off[blockIdx.x] = block_offsets[chunk] + tot;
+    }
+}
+
 // Camera vertex i (1-based): emission (s = 0), next-event estimation (s = 1),
 // connections to cached light vertices (s >= 2), continuation.  Every
 // strategy of a k-segment path is weighted 1/k.  A layered (non-specular)
 // vertex at either end of a strategy takes f from material_f in the frame of
 // its geometric normal (the path tracer's convention) and continues by
 // material_sample_f; single-Lambertian vertices keep the albedo fast path.
-__global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t iter, uint32_t i, uint32_t Kmax,
+__global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t it0, uint32_t i, uint32_t Kmax,
                                uint32_t C, uint32_t rr_start, float rr_prob, float n_light_paths, const uint32_t* q_in,
                                uint32_t* q_out, float4* rays, const int4* hits, float4* T, float4* L, float4* srays,
                                float4* sc_out, uint32_t* qs, float4* cray, float4* cc, uint32_t* cq,
                                const float4* lvc_pos, const float4* lvc_nrm, const float4* lvc_beta,
-                               const float4* lvc_wi, WaveCountersDev* wc, uint32_t cur)
+                               const float4* lvc_wi, const uint32_t* lvc_off, WaveCountersDev* wc, uint32_t cur)
 {
     const uint32_t n = wc->n_ext[cur];
-    const uint32_t M = wc->lvc_count;
     const float inv_nl = sc.n_lights ? 1.0f / (float)sc.n_lights : 0.0f;
     const uint32_t b = i - 1;  // random-dimension block of this vertex
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
@@ -705,7 +730,11 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
             for (uint32_t c = 0; c < C; c++) cc[(size_t)path * C + c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             const int4 h = hits[path];
             if (h.x >= 0) {
-                const uint64_t key = (uint64_t)iter * npix + (path % npix);
+                // Path p of the wave is pixel p % npix of iteration it0 + p / npix, whose
+                // cached light vertices are the dense range [lvc_off[li], lvc_off[li + 1]).
+                const uint64_t key = (uint64_t)it0 * npix + path;
+                const uint32_t li = path / npix;
+                const uint32_t vbase = lvc_off[li], M = lvc_off[li + 1] - vbase;
                 const float4 o4 = rays[2 * (size_t)path], d4 = rays[2 * (size_t)path + 1];
                 const float t = __int_as_float(h.y);
                 const float3 d = xyz(d4);
@@ -762,7 +791,8 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                     }
                     if (M > 0 && i + 2 <= Kmax) {  // s >= 2
                         for (uint32_t c = 0; c < C; c++) {
-                            const uint32_t v = min((uint32_t)(rng_u01(seed, key, vdim(b, 6) + 520u * (c + 1)) * (float)M), M - 1);
+                            const uint32_t v =
+                                vbase + min((uint32_t)(rng_u01(seed, key, vdim(b, 6) + 520u * (c + 1)) * (float)M), M - 1);
                             const float4 vp4 = lvc_pos[v];
                             const uint32_t s = (uint32_t)vp4.w;
                             if (s + i > Kmax) continue;
@@ -995,6 +1025,8 @@ int ensure_path_state(PathState& ps, uint64_t P)
 int ensure_bdpt_state(BdptState& bd, uint64_t n_paths, uint64_t n_slots, uint64_t n_conn)
 {
     cudaError_t e = cudaSuccess;
+    if (!bd.lvc_off && (e = cudaMalloc(&bd.lvc_off, (kMaxBdptWave + 1) * sizeof(uint32_t))) != cudaSuccess)
+        return fail(RB2_ENOMEM, std::string("cache offsets: ") + cudaGetErrorString(e));
     if (n_paths > bd.cap_paths) {
         for (void* p : {(void*)bd.lray, (void*)bd.lbeta, (void*)bd.lhit, (void*)bd.lq[0], (void*)bd.lq[1]}) cudaFree(p);
         bd.lray = bd.lbeta = nullptr; bd.lhit = nullptr; bd.lq[0] = bd.lq[1] = nullptr; bd.cap_paths = 0;
@@ -1030,9 +1062,10 @@ int ensure_bdpt_state(BdptState& bd, uint64_t n_paths, uint64_t n_slots, uint64_
     return RB2_OK;
 }
 
-uint64_t pt_paths_in_flight(uint64_t npix, uint32_t spp, uint32_t spp_per_wave)
+uint64_t pt_paths_in_flight(uint64_t npix, uint32_t spp, uint32_t spp_per_wave, uint64_t auto_paths)
 {
-    uint32_t spw = spp_per_wave ? spp_per_wave : (uint32_t)std::max<uint64_t>(1, (8ull << 20) / std::max<uint64_t>(1, npix));
+    uint32_t spw = spp_per_wave ? spp_per_wave
+                                : (uint32_t)std::max<uint64_t>(1, auto_paths / std::max<uint64_t>(1, npix));
     spw = std::min(spw, std::max<uint32_t>(1, spp));
     return npix * spw;
 }
@@ -1144,7 +1177,7 @@ int rb2_integrator_destroy(rb2_integrator* it)
     for (void* p : {(void*)bd.lray, (void*)bd.lbeta, (void*)bd.lhit, (void*)bd.lq[0], (void*)bd.lq[1], (void*)bd.s_pos,
                     (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_wi, (void*)bd.s_valid, (void*)bd.d_pos,
                     (void*)bd.d_nrm, (void*)bd.d_beta, (void*)bd.d_wi, (void*)bd.block_sums, (void*)bd.cray,
-                    (void*)bd.cc, (void*)bd.cq})
+                    (void*)bd.cc, (void*)bd.cq, (void*)bd.lvc_off})
         cudaFree(p);
     delete it;
     return RB2_OK;
@@ -1234,7 +1267,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
     const uint64_t npix = (uint64_t)cam->width * cam->height;
     if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");
     // Samples per pixel in flight: about 8M paths per wave by default.
-    const uint64_t P = pt_paths_in_flight(npix, p->spp, p->spp_per_wave);
+    const uint64_t P = pt_paths_in_flight(npix, p->spp, p->spp_per_wave, it->wave_paths ? it->wave_paths : kRenderWavePaths);
     const uint32_t spw = (uint32_t)(P / npix);
     PathState& ps = it->ps;
     int rc;
@@ -1315,15 +1348,25 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     const uint32_t K = p->max_path_length, C = p->connections;
     const uint32_t Dl = K >= 2 ? K - 2 : 0;  // cached light vertices y1..y_{K-2} suffice for k <= K
     const uint64_t NL = p->num_light_paths ? p->num_light_paths : npix;
-    const uint64_t n_slots = std::max<uint64_t>(1, NL * std::max<uint32_t>(Dl, 1));
+    // Iterations per wave: as many as fit the wave budget in camera and light
+    // paths, spread evenly over the waves, with every wave index 32-bit.
+    const uint64_t budget = it->wave_paths ? it->wave_paths : kBdptWavePaths;
+    uint64_t wmax = std::max<uint64_t>(1, budget / std::max(npix, NL));
+    wmax = std::min<uint64_t>({wmax, (uint64_t)p->spp, (uint64_t)kMaxBdptWave, 0xFFFFFFFFull / (npix * C),
+                               0xFFFFFFFFull / NL});
+    wmax = std::max<uint64_t>(wmax, 1);
+    const uint32_t n_waves = (uint32_t)((p->spp + wmax - 1) / wmax);
+    const uint32_t Wv = (p->spp + n_waves - 1) / n_waves;
+    const uint64_t per_iter = NL * std::max<uint32_t>(Dl, 1);   // cache slots of one iteration
+    const uint64_t n_slots = per_iter * Wv;
     int rc;
-    if ((rc = ensure_path_state(it->ps, npix))) return rc;
-    if ((rc = ensure_bdpt_state(it->bd, NL, n_slots, npix * C))) return rc;
+    if ((rc = ensure_path_state(it->ps, npix * Wv))) return rc;
+    if ((rc = ensure_bdpt_state(it->bd, NL * Wv, n_slots, npix * Wv * C))) return rc;
     if ((rc = grow(it->d_accum, it->cap_accum, npix))) return rc;
     const bool filtered = it->filter.kind != RB2_FILTER_NONE;
     rb2dev::FilmArgs fa{};
     if (filtered) {
-        if ((rc = grow(it->d_film_xy, it->cap_film_xy, npix))) return rc;
+        if ((rc = grow(it->d_film_xy, it->cap_film_xy, npix * Wv))) return rc;
         if ((rc = film_args(it->filter, cam->width, cam->height, fa))) return rc;
     }
     if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
@@ -1345,33 +1388,41 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     // Light-vertex directions are cached only when a layered material needs them.
     float4* s_wi = it->scene->layered ? bd.s_wi : nullptr;
     float4* d_wi = it->scene->layered ? bd.d_wi : nullptr;
-    const unsigned gl = grid_for(NL, it->sms), gc = grid_for(npix, it->sms);
-    const uint64_t n_chunks = (n_slots + rb2dev::kScanChunk - 1) / rb2dev::kScanChunk;
-    for (uint32_t iter = 0; iter < p->spp; iter++) {
+    for (uint32_t it0 = 0; it0 < p->spp; it0 += Wv) {
+        // Wave of w iterations: light path l is path l % NL of iteration it0 + l / NL,
+        // camera path c is pixel c % npix of iteration it0 + c / npix.  The random
+        // keys are those of the iterations run one at a time.
+        const uint32_t w = std::min(Wv, p->spp - it0);
+        const uint64_t n_light = NL * w, n_cam = npix * w, wave_slots = per_iter * w;
+        const unsigned gl = grid_for(n_light, it->sms), gc = grid_for(n_cam, it->sms), gp = grid_for(npix, it->sms);
+        const uint64_t n_chunks = (wave_slots + rb2dev::kScanChunk - 1) / rb2dev::kScanChunk;
         // ---- light pass: subpaths into the sparse cache, then compaction.
-        RB2_CUDA(cudaMemsetAsync(bd.s_valid, 0, n_slots, s), "cache reset");
-        rb2dev::k_bd_light_init<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)iter * NL, (uint32_t)NL, bd.lray, bd.lbeta,
-                                                   bd.lq[0], wc);
+        RB2_CUDA(cudaMemsetAsync(bd.s_valid, 0, wave_slots, s), "cache reset");
+        rb2dev::k_bd_light_init<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)it0 * NL, (uint32_t)n_light, bd.lray,
+                                                   bd.lbeta, bd.lq[0], wc);
         RB2_CUDA(cudaGetLastError(), "BDPT light init");
         uint32_t cur = 0;
         for (uint32_t d = 1; d <= Dl; d++) {
             rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
             rb2dev::QueueSource lsrc{bn, bw, bv.triidx, bd.lq[cur], &wc->n_ext[cur], bd.lray, &wc->head_ext,
                                      rb2dev::kClosest, bd.lhit, nullptr, nullptr};
-            if ((rc = launch_persistent(lsrc, NL, it, bv, s))) return rc;
-            rb2dev::k_bd_light_shade<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)iter * NL, d, Dl, p->rr_start, p->rr_prob,
+            if ((rc = launch_persistent(lsrc, n_light, it, bv, s))) return rc;
+            rb2dev::k_bd_light_shade<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)it0 * NL, d, Dl, p->rr_start, p->rr_prob,
                                                         bd.lq[cur], bd.lq[cur ^ 1u], bd.lray, bd.lhit, bd.lbeta, bd.s_pos,
                                                         bd.s_nrm, bd.s_beta, s_wi, bd.s_valid, wc, cur);
             RB2_CUDA(cudaGetLastError(), "BDPT light shade");
             cur ^= 1u;
         }
-        rb2dev::k_lvc_count<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(bd.s_valid, n_slots, bd.block_sums);
+        rb2dev::k_lvc_count<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(bd.s_valid, wave_slots, bd.block_sums);
         rb2dev::k_lvc_scan_top<<<1, 1024, 0, s>>>(bd.block_sums, (uint32_t)n_chunks, wc);
         rb2dev::k_lvc_scatter<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(
-            bd.s_valid, n_slots, bd.block_sums, bd.s_pos, bd.s_nrm, bd.s_beta, s_wi, bd.d_pos, bd.d_nrm, bd.d_beta, d_wi);
+            bd.s_valid, wave_slots, bd.block_sums, bd.s_pos, bd.s_nrm, bd.s_beta, s_wi, bd.d_pos, bd.d_nrm, bd.d_beta,
+            d_wi);
+        rb2dev::k_lvc_wave_offsets<<<w + 1, rb2dev::kScanThreads, 0, s>>>(bd.s_valid, wave_slots, bd.block_sums,
+                                                                          per_iter, wc, bd.lvc_off);
         RB2_CUDA(cudaGetLastError(), "cache compaction");
         // ---- camera pass.
-        rb2dev::k_pt_camera<<<gc, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, (uint32_t)npix, iter, ps.ray, ps.T, ps.L,
+        rb2dev::k_pt_camera<<<gc, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, (uint32_t)n_cam, it0, ps.ray, ps.T, ps.L,
                                                ps.q[0], wc, filtered ? it->d_film_xy : nullptr);
         RB2_CUDA(cudaGetLastError(), "BDPT camera");
         cur = 0;
@@ -1379,34 +1430,39 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
             rb2dev::QueueSource ext{bn, bw, bv.triidx, ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext,
                                     rb2dev::kClosest, ps.hit, nullptr, nullptr};
-            if ((rc = launch_persistent(ext, npix, it, bv, s))) return rc;
-            rb2dev::k_bd_cam_shade<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, iter, i, K, C, p->rr_start, p->rr_prob,
+            if ((rc = launch_persistent(ext, n_cam, it, bv, s))) return rc;
+            rb2dev::k_bd_cam_shade<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, it0, i, K, C, p->rr_start, p->rr_prob,
                                                       (float)NL, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L,
                                                       ps.sray, ps.sc, ps.qs, bd.cray, bd.cc, bd.cq, bd.d_pos, bd.d_nrm,
-                                                      bd.d_beta, d_wi, wc, cur);
+                                                      bd.d_beta, d_wi, bd.lvc_off, wc, cur);
             RB2_CUDA(cudaGetLastError(), "BDPT camera shade");
             rb2dev::k_bd_stats<<<1, 1, 0, s>>>(wc);
             rb2dev::QueueSource nee{bn, bw, bv.triidx, ps.qs, &wc->n_shadow, ps.sray, &wc->head_shadow,
                                     rb2dev::kOcclusion, nullptr, ps.L, ps.sc};
-            if ((rc = launch_persistent(nee, npix, it, bv, s))) return rc;
+            if ((rc = launch_persistent(nee, n_cam, it, bv, s))) return rc;
             rb2dev::QueueSource con{bn, bw, bv.triidx, bd.cq, &wc->n_conn, bd.cray, &wc->head_conn,
                                     rb2dev::kOcclusion, nullptr, nullptr, bd.cc};
-            if ((rc = launch_persistent(con, npix * C, it, bv, s))) return rc;
+            if ((rc = launch_persistent(con, n_cam * C, it, bv, s))) return rc;
             rb2dev::k_bd_conn_reduce<<<gc, 256, 0, s>>>(ps.q[cur], wc, cur, C, bd.cc, ps.L);
             RB2_CUDA(cudaGetLastError(), "BDPT connection reduce");
             cur ^= 1u;
         }
+        // Unfiltered, the iterations are added to the accumulator in order, so the
+        // image is bit-identical to running them one at a time; the filtered
+        // gather sums a neighbourhood sample by sample, so its rounding depends
+        // on the wave size (and is deterministic for a given one).
         if (filtered)
-            rb2dev::k_film_gather<<<gc, 256, 0, s>>>(fa, rb2dev::ArrayPos{it->d_film_xy, (uint32_t)npix}, ps.L, 1u,
+            rb2dev::k_film_gather<<<gp, 256, 0, s>>>(fa, rb2dev::ArrayPos{it->d_film_xy, (uint32_t)npix}, ps.L, w,
                                                      it->d_accum, nullptr);
         else
-            rb2dev::k_pt_accumulate<<<gc, 256, 0, s>>>(ps.L, (uint32_t)npix, 1u, it->d_accum);
+            rb2dev::k_pt_accumulate<<<gp, 256, 0, s>>>(ps.L, (uint32_t)npix, w, it->d_accum);
         RB2_CUDA(cudaGetLastError(), "BDPT accumulate");
     }
+    const unsigned gp = grid_for(npix, it->sms);
     if (filtered)
-        rb2dev::k_film_resolve<<<gc, 256, 0, s>>>(it->d_accum, (uint32_t)npix, d_rgb);
+        rb2dev::k_film_resolve<<<gp, 256, 0, s>>>(it->d_accum, (uint32_t)npix, d_rgb);
     else
-        rb2dev::k_pt_finalize<<<gc, 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp, d_rgb);
+        rb2dev::k_pt_finalize<<<gp, 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp, d_rgb);
     RB2_CUDA(cudaGetLastError(), "BDPT finalize");
     return RB2_OK;
 }
@@ -1436,6 +1492,13 @@ int rb2_integrator_stats(rb2_integrator* it, rb2_render_stats* out, void* stream
     out->connection_rays = w.stats[3];
     out->light_rays = w.stats[4];
     out->lvc_vertices = w.stats[5];
+    return RB2_OK;
+}
+
+int rb2_integrator_set_wave(rb2_integrator* it, uint64_t paths)
+{
+    if (!it) return fail(RB2_EINVAL, "null argument");
+    it->wave_paths = paths;
     return RB2_OK;
 }
 

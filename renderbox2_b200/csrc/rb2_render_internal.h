@@ -73,6 +73,7 @@ struct BdptState {
     float4* d_wi = nullptr;
     uint32_t* block_sums = nullptr;
     uint64_t cap_slots = 0;
+    uint32_t* lvc_off = nullptr;   // dense-cache offset of each iteration of a wave (kMaxBdptWave + 1)
     // connection rays of camera vertices (connections per path)
     float4* cray = nullptr;
     float4* cc = nullptr;
@@ -86,6 +87,8 @@ struct rb2_integrator {
     int sms = 0;
     // launch shape of the integrator's traversal kernels (rb2_integrator_set_launch)
     uint32_t tr_block = 128, tr_regs = 48, tr_threshold = 24;
+    // paths in flight per wave (rb2_integrator_set_wave; 0: the defaults below)
+    uint64_t wave_paths = 0;
     // traversal timing (rb2_integrator_set_timing): an event pair per launch
     bool timing = false;
     std::vector<cudaEvent_t> ev;
@@ -125,5 +128,19 @@ int ensure_bdpt_state(BdptState& bd, uint64_t n_paths, uint64_t n_slots, uint64_
 // paths in flight and `npix` pixels run without further device allocation.
 int integrator_reserve_pt(rb2_integrator* it, uint64_t paths, uint64_t npix);
 // Paths in flight that rb2_render_pt uses for an image of npix pixels at spp.
-uint64_t pt_paths_in_flight(uint64_t npix, uint32_t spp, uint32_t spp_per_wave);
+// Paths in flight of a path-traced render: npix x spp_per_wave, or (0) as
+// many samples per pixel as fit `auto_paths` (at least one, at most spp).
+// Renders default to 32M paths (about 4.4 GB of path state): on config 2,
+// 8M paths per wave measured 469 ms a frame, 16M 452 ms, 32M 445 ms (fewer
+// launch tails).  Serving slots size for 8M so a slot stays about 1.1 GB.
+constexpr uint64_t kRenderWavePaths = 32ull << 20;
+constexpr uint64_t kServeWavePaths = 8ull << 20;
+// BDPT runs several iterations (one camera sample per pixel each) per wave:
+// as many as fit 8M camera paths, at most kMaxBdptWave.  Config 3 (921,600
+// pixels, 16 iterations) measured 163 ms a frame one iteration at a time and
+// about 125-130 ms with 4-16 in flight: the traversal launches grow from
+// 0.9M to several million rays and their tails shrink in proportion.
+constexpr uint64_t kBdptWavePaths = 8ull << 20;
+constexpr uint32_t kMaxBdptWave = 64;
+uint64_t pt_paths_in_flight(uint64_t npix, uint32_t spp, uint32_t spp_per_wave, uint64_t auto_paths = kRenderWavePaths);
 }  // namespace rb2

@@ -53,7 +53,7 @@ extern "C" uint64_t rb2_job_footprint(const rb2_job* j)
     if (!j) return 0;
     if (j->kind == RB2_JOB_RAYS) return j->n_rays * (32 + out_bytes_per_ray(j->mode));
     const uint64_t npix = (uint64_t)j->tile * j->tile;
-    const uint64_t P = pt_paths_in_flight(npix, j->spp, 0);
+    const uint64_t P = pt_paths_in_flight(npix, j->spp, 0, kServeWavePaths);
     // path state (T, L, ray, hit, shadow ray, contribution, three queues) + accumulator + image
     return P * (16 + 16 + 32 + 16 + 32 + 16 + 12) + npix * (16 + 12) + sizeof(WaveCounters);
 }
@@ -95,7 +95,7 @@ extern "C" int rb2_server_create(rb2_tracer* const* tracers, rb2_scene_dev* cons
     const uint64_t max_npix = (uint64_t)c.max_tile * c.max_tile;
     // Path state for the largest tile at up to 64 spp in flight (larger spp
     // counts stream through the same state in waves).
-    const uint64_t max_paths = pt_paths_in_flight(max_npix, 64, 0);
+    const uint64_t max_paths = pt_paths_in_flight(max_npix, 64, 0, kServeWavePaths);
     for (uint64_t i = 0; i < n_bvh; i++) {
         uint64_t b = 0;
         rb2_tracer_device_bytes(tracers[i], &b);
@@ -157,7 +157,10 @@ int enqueue(rb2_server* s, Slot& sl, const rb2_job& j)
     rb2_camera cam;
     int rc = rb2_camera_init(&cam, j.eye, j.lookat, j.up, j.tile, j.tile, j.fov_deg);
     if (rc) return rc;
-    rb2_pt_params p{j.spp, j.max_depth, j.rr_start, j.rr_prob, j.seed, 0, 0};
+    // The slot's path state was reserved for the serving wave size.
+    const uint64_t npix = (uint64_t)j.tile * j.tile;
+    const uint32_t spw = (uint32_t)(pt_paths_in_flight(npix, j.spp, 0, kServeWavePaths) / npix);
+    rb2_pt_params p{j.spp, j.max_depth, j.rr_start, j.rr_prob, j.seed, spw, 0};
     if ((rc = rb2_render_pt(sl.it, &cam, &p, sl.d_img, st))) return rc;
     cudaError_t e = cudaMemcpyAsync(j.h_out, sl.d_img, (size_t)j.tile * j.tile * 12, cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return fail(RB2_ECUDA, std::string("tile download: ") + cudaGetErrorString(e));

@@ -247,6 +247,10 @@ class Integrator:
         c = LaunchConfig(block_threads, 0, fetch_threshold, regs)
         check(lib().rb2_integrator_set_launch(self._it, C.byref(c)))
 
+    def set_wave(self, paths: int = 0):
+        """Paths in flight per wave (0: defaults); see rb2_integrator_set_wave."""
+        check(lib().rb2_integrator_set_wave(self._it, int(paths)))
+
     def set_timing(self, on: bool = True):
         """Time the traversal launches of each render (stats()["trace_ms"])."""
         check(lib().rb2_integrator_set_timing(self._it, 1 if on else 0))

@@ -189,3 +189,34 @@ def test_integrators_on_compressed_wide_layout(rb, cuda):
         print(name, "differing pixels", diff)
         assert diff <= 1e-3, name
     tr.set_node_order(rb.NODE_ORDER_DFS)
+
+
+@pytest.mark.parametrize("layered", [False, True])
+def test_bdpt_waves_are_bit_identical(rb, cuda, layered):
+    """BDPT runs several iterations per wave, each with its own light-vertex
+    cache range; with the same random keys, the unfiltered image and the ray
+    counts equal those of one iteration at a time, for any wave size."""
+    from renderbox2_b200.configs import CONFIG2 as C2
+    from renderbox2_b200.render import BidirectionalPathIntegratorLvcParams, DeviceScene, Integrator
+    if layered:
+        from test_gpu_material import _glossy_room
+        room, mats = _glossy_room(rb)
+        ds = DeviceScene(room, materials=mats)
+    else:
+        room = _room(rb)
+        ds = DeviceScene(room)
+    it = Integrator(rb.CudaTracer(rb.BVH(room)), ds)
+    W, H = 160, 90
+    cam = rb.PerspectiveCamera(C2["eye"], C2["lookat"], C2["up"], (W, H), C2["fov"])
+    p = BidirectionalPathIntegratorLvcParams(spp=8, max_path_length=6, connections=2, num_light_paths=10_000, seed=5)
+    imgs, stats = [], []
+    for wave in (W * H, 3 * W * H, 0):   # 1 iteration per wave, 3 (3 + 3 + 2), all 8 (default budget)
+        it.set_wave(wave)
+        imgs.append(it.render_bdpt(cam, p).cpu())
+        st = it.stats()
+        stats.append({k: st[k] for k in ("primary_rays", "extension_rays", "shadow_rays", "connection_rays",
+                                         "light_rays", "lvc_vertices")})
+    assert imgs[0].float().mean() > 0
+    for k in (1, 2):
+        assert cuda.equal(imgs[0], imgs[k]), f"wave {k}"
+        assert stats[0] == stats[k]
