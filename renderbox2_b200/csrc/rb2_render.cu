@@ -642,36 +642,30 @@ __global__ void k_lvc_scan_top(uint32_t* block_sums, uint32_t n_blocks, WaveCoun
     }
 }
 
-// Scatter valid slots in slot order: thread t of a chunk owns 8 consecutive slots.
-__global__ void k_lvc_scatter(const uint8_t* valid, uint64_t n_slots, const uint32_t* block_offsets, const float4* s_pos,
-                              const float4* s_nrm, const float4* s_beta, const float4* s_wi, float4* d_pos, float4* d_nrm,
-                              float4* d_beta, float4* d_wi)
+// Dense list of the valid slots, in slot order: a chunk is read in rounds of
+// kScanThreads consecutive slots (coalesced flags, coalesced index writes); a
+// round's valid slots go after the chunk's offset and the earlier rounds'.
+// Connections read the sparse cache through this list, so no vertex data is
+// copied.
+__global__ void k_lvc_scatter(const uint8_t* valid, uint64_t n_slots, const uint32_t* block_offsets, uint32_t* slot_of)
 {
-    constexpr uint32_t kPer = kScanChunk / kScanThreads;
     __shared__ uint32_t s_warp[kScanThreads / 32];
-    const uint64_t base = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)threadIdx.x * kPer;
-    uint32_t c = 0;
-    for (uint32_t k = 0; k < kPer; k++) c += (base + k < n_slots) ? valid[base + k] : 0u;
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t incl = c;
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(kFull, incl, o);
-        if ((int)lane >= o) incl += y;
-    }
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    uint32_t warp_off = 0;
-    for (uint32_t w = 0; w < warp; w++) warp_off += s_warp[w];
-    uint32_t out = block_offsets[blockIdx.x] + warp_off + incl - c;
-    for (uint32_t k = 0; k < kPer; k++) {
-        const uint64_t i = base + k;
-        if (i < n_slots && valid[i]) {
-            d_pos[out] = s_pos[i];
-            d_nrm[out] = s_nrm[i];
-            d_beta[out] = s_beta[i];
-            if (s_wi) d_wi[out] = s_wi[i];
-            out++;
+    uint32_t run = block_offsets[blockIdx.x];
+    for (uint32_t r = 0; r < kScanChunk / kScanThreads; r++) {
+        const uint64_t i = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)r * kScanThreads + threadIdx.x;
+        const bool v = i < n_slots && valid[i] != 0;
+        const unsigned m = __ballot_sync(kFull, v);
+        if (lane == 0) s_warp[warp] = (uint32_t)__popc(m);
+        __syncthreads();
+        uint32_t off = run, tot = 0;
+        for (uint32_t w = 0; w < kScanThreads / 32; w++) {
+            if (w < warp) off += s_warp[w];
+            tot += s_warp[w];
         }
+        if (v) slot_of[off + (uint32_t)__popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
+        run += tot;
+        __syncthreads();  // s_warp is rewritten by the next round
     }
 }
 
@@ -712,7 +706,8 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                                uint32_t* q_out, float4* rays, const int4* hits, float4* T, float4* L, float4* srays,
                                float4* sc_out, uint32_t* qs, float4* cray, float4* cc, uint32_t* cq,
                                const float4* lvc_pos, const float4* lvc_nrm, const float4* lvc_beta,
-                               const float4* lvc_wi, const uint32_t* lvc_off, WaveCountersDev* wc, uint32_t cur)
+                               const float4* lvc_wi, const uint32_t* lvc_slot, const uint32_t* lvc_off,
+                               WaveCountersDev* wc, uint32_t cur)
 {
     const uint32_t n = wc->n_ext[cur];
     const float inv_nl = sc.n_lights ? 1.0f / (float)sc.n_lights : 0.0f;
@@ -791,8 +786,9 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                     }
                     if (M > 0 && i + 2 <= Kmax) {  // s >= 2
                         for (uint32_t c = 0; c < C; c++) {
-                            const uint32_t v =
-                                vbase + min((uint32_t)(rng_u01(seed, key, vdim(b, 6) + 520u * (c + 1)) * (float)M), M - 1);
+                            const uint32_t v = lvc_slot[vbase + min((uint32_t)(rng_u01(seed, key, vdim(b, 6) +
+                                                                                         520u * (c + 1)) * (float)M),
+                                                                    M - 1)];
                             const float4 vp4 = lvc_pos[v];
                             const uint32_t s = (uint32_t)vp4.w;
                             if (s + i > Kmax) continue;
@@ -1038,16 +1034,15 @@ int ensure_bdpt_state(BdptState& bd, uint64_t n_paths, uint64_t n_slots, uint64_
     }
     if (n_slots > bd.cap_slots) {
         for (void* p : {(void*)bd.s_pos, (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_wi, (void*)bd.s_valid,
-                        (void*)bd.d_pos, (void*)bd.d_nrm, (void*)bd.d_beta, (void*)bd.d_wi, (void*)bd.block_sums})
+                        (void*)bd.d_slot, (void*)bd.block_sums})
             cudaFree(p);
-        bd.s_pos = bd.s_nrm = bd.s_beta = bd.s_wi = bd.d_pos = bd.d_nrm = bd.d_beta = bd.d_wi = nullptr;
-        bd.s_valid = nullptr; bd.block_sums = nullptr; bd.cap_slots = 0;
+        bd.s_pos = bd.s_nrm = bd.s_beta = bd.s_wi = nullptr;
+        bd.s_valid = nullptr; bd.d_slot = nullptr; bd.block_sums = nullptr; bd.cap_slots = 0;
         const uint64_t nb = (n_slots + rb2dev::kScanChunk - 1) / rb2dev::kScanChunk;
         if ((e = cudaMalloc(&bd.s_pos, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.s_nrm, n_slots * 16)) != cudaSuccess ||
             (e = cudaMalloc(&bd.s_beta, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.s_valid, n_slots)) != cudaSuccess ||
-            (e = cudaMalloc(&bd.d_pos, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.d_nrm, n_slots * 16)) != cudaSuccess ||
-            (e = cudaMalloc(&bd.d_beta, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.s_wi, n_slots * 16)) != cudaSuccess ||
-            (e = cudaMalloc(&bd.d_wi, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.block_sums, nb * 4)) != cudaSuccess)
+            (e = cudaMalloc(&bd.d_slot, n_slots * 4)) != cudaSuccess || (e = cudaMalloc(&bd.s_wi, n_slots * 16)) != cudaSuccess ||
+            (e = cudaMalloc(&bd.block_sums, nb * 4)) != cudaSuccess)
             return fail(RB2_ENOMEM, std::string("light vertex cache: ") + cudaGetErrorString(e));
         bd.cap_slots = n_slots;
     }
@@ -1175,8 +1170,8 @@ int rb2_integrator_destroy(rb2_integrator* it)
     cudaFree(ps.q[0]); cudaFree(ps.q[1]); cudaFree(ps.qs);
     BdptState& bd = it->bd;
     for (void* p : {(void*)bd.lray, (void*)bd.lbeta, (void*)bd.lhit, (void*)bd.lq[0], (void*)bd.lq[1], (void*)bd.s_pos,
-                    (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_wi, (void*)bd.s_valid, (void*)bd.d_pos,
-                    (void*)bd.d_nrm, (void*)bd.d_beta, (void*)bd.d_wi, (void*)bd.block_sums, (void*)bd.cray,
+                    (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_wi, (void*)bd.s_valid, (void*)bd.d_slot,
+                    (void*)bd.block_sums, (void*)bd.cray,
                     (void*)bd.cc, (void*)bd.cq, (void*)bd.lvc_off})
         cudaFree(p);
     delete it;
@@ -1350,14 +1345,15 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     const uint64_t NL = p->num_light_paths ? p->num_light_paths : npix;
     // Iterations per wave: as many as fit the wave budget in camera and light
     // paths, spread evenly over the waves, with every wave index 32-bit.
+    const uint64_t per_iter = NL * std::max<uint32_t>(Dl, 1);   // cache slots of one iteration
+    if (per_iter > 0xFFFFFFFFull) return fail(RB2_EINVAL, "num_light_paths x cached depth must fit 32-bit slot indices");
     const uint64_t budget = it->wave_paths ? it->wave_paths : kBdptWavePaths;
     uint64_t wmax = std::max<uint64_t>(1, budget / std::max(npix, NL));
     wmax = std::min<uint64_t>({wmax, (uint64_t)p->spp, (uint64_t)kMaxBdptWave, 0xFFFFFFFFull / (npix * C),
-                               0xFFFFFFFFull / NL});
+                               0xFFFFFFFFull / per_iter});
     wmax = std::max<uint64_t>(wmax, 1);
     const uint32_t n_waves = (uint32_t)((p->spp + wmax - 1) / wmax);
     const uint32_t Wv = (p->spp + n_waves - 1) / n_waves;
-    const uint64_t per_iter = NL * std::max<uint32_t>(Dl, 1);   // cache slots of one iteration
     const uint64_t n_slots = per_iter * Wv;
     int rc;
     if ((rc = ensure_path_state(it->ps, npix * Wv))) return rc;
@@ -1387,7 +1383,6 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     BdptState& bd = it->bd;
     // Light-vertex directions are cached only when a layered material needs them.
     float4* s_wi = it->scene->layered ? bd.s_wi : nullptr;
-    float4* d_wi = it->scene->layered ? bd.d_wi : nullptr;
     for (uint32_t it0 = 0; it0 < p->spp; it0 += Wv) {
         // Wave of w iterations: light path l is path l % NL of iteration it0 + l / NL,
         // camera path c is pixel c % npix of iteration it0 + c / npix.  The random
@@ -1416,8 +1411,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
         rb2dev::k_lvc_count<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(bd.s_valid, wave_slots, bd.block_sums);
         rb2dev::k_lvc_scan_top<<<1, 1024, 0, s>>>(bd.block_sums, (uint32_t)n_chunks, wc);
         rb2dev::k_lvc_scatter<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(
-            bd.s_valid, wave_slots, bd.block_sums, bd.s_pos, bd.s_nrm, bd.s_beta, s_wi, bd.d_pos, bd.d_nrm, bd.d_beta,
-            d_wi);
+            bd.s_valid, wave_slots, bd.block_sums, bd.d_slot);
         rb2dev::k_lvc_wave_offsets<<<w + 1, rb2dev::kScanThreads, 0, s>>>(bd.s_valid, wave_slots, bd.block_sums,
                                                                           per_iter, wc, bd.lvc_off);
         RB2_CUDA(cudaGetLastError(), "cache compaction");
@@ -1433,8 +1427,8 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             if ((rc = launch_persistent(ext, n_cam, it, bv, s))) return rc;
             rb2dev::k_bd_cam_shade<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, it0, i, K, C, p->rr_start, p->rr_prob,
                                                       (float)NL, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L,
-                                                      ps.sray, ps.sc, ps.qs, bd.cray, bd.cc, bd.cq, bd.d_pos, bd.d_nrm,
-                                                      bd.d_beta, d_wi, bd.lvc_off, wc, cur);
+                                                      ps.sray, ps.sc, ps.qs, bd.cray, bd.cc, bd.cq, bd.s_pos, bd.s_nrm,
+                                                      bd.s_beta, s_wi, bd.d_slot, bd.lvc_off, wc, cur);
             RB2_CUDA(cudaGetLastError(), "BDPT camera shade");
             rb2dev::k_bd_stats<<<1, 1, 0, s>>>(wc);
             rb2dev::QueueSource nee{bn, bw, bv.triidx, ps.qs, &wc->n_shadow, ps.sray, &wc->head_shadow,

@@ -61,16 +61,13 @@ struct BdptState {
     int4* lhit = nullptr;
     uint32_t* lq[2] = {nullptr, nullptr};
     uint64_t cap_paths = 0;
-    // cache, sparse (path, depth) slots and dense compacted copy
+    // cache: sparse (path, depth) slots and the dense list of valid slot indices
     float4* s_pos = nullptr;    // xyz, w = light-subpath vertex count s (as float)
     float4* s_nrm = nullptr;    // normal facing the arriving light, w = material id bits
     float4* s_beta = nullptr;
     float4* s_wi = nullptr;     // toward the previous light vertex, w = sign of ng . nrm
     uint8_t* s_valid = nullptr;
-    float4* d_pos = nullptr;
-    float4* d_nrm = nullptr;
-    float4* d_beta = nullptr;
-    float4* d_wi = nullptr;
+    uint32_t* d_slot = nullptr;    // valid slots in slot order (the compacted cache)
     uint32_t* block_sums = nullptr;
     uint64_t cap_slots = 0;
     uint32_t* lvc_off = nullptr;   // dense-cache offset of each iteration of a wave (kMaxBdptWave + 1)
@@ -108,7 +105,7 @@ struct rb2_integrator {
     {
         return cap_rays * 32 + cap_hits * 16 + cap_count * 4 + 16 * 8 + cap_accum * 16 + cap_film_xy * 8 +
                ps.cap * (16 * 8 + 12) +
-               sizeof(WaveCounters) + bd.cap_paths * (32 + 16 + 16 + 8) + bd.cap_slots * (8 * 16 + 1) +
+               sizeof(WaveCounters) + bd.cap_paths * (32 + 16 + 16 + 8) + bd.cap_slots * (4 * 16 + 1 + 4) +
                bd.cap_conn * (32 + 16 + 4);
     }
 };
