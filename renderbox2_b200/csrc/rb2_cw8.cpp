@@ -2,12 +2,12 @@
 // from a binary Compact2 tree (the reference's layout,
 // accelerators/sbvh/cudabvh.cpp:216-296).
 //
-// The node format restates the compressed wide BVH of Ylitie, Karras and
+// The node format follows the compressed wide BVH of Ylitie, Karras and
 // Laine, "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide
 // BVHs" (HPG 2017): eight child boxes quantized to 8 bits per plane in a
-// per-node grid (origin p, power-of-two scale per axis), one meta byte per
-// child slot, inner children stored contiguously from child_base and leaf
-// triangles contiguously from tri_base, child slots assigned by ray octant so
+// per-node grid (origin p, power-of-two scale per axis), inner children
+// stored contiguously from child_base and leaf triangles contiguously from
+// tri_base, child slots assigned by ray octant so
 // that visiting hit children in bit order is roughly front to back, and the
 // binary tree's subtrees distributed over slots by the paper's SAH dynamic
 // program.  Node
@@ -15,8 +15,12 @@
 //   [0..2]  p.xyz (float)
 //   [3]     exponent bytes ex | ey << 8 | ez << 16 (biased by 127), imask << 24
 //   [4]     child_base (node index)     [5] tri_base (triangle index)
-//   [6..7]  meta[8]: 0 empty; 0x20 | (24 + slot) inner; (unary count << 5) | offset for a
-//           leaf of 1-3 triangles at tri_base + offset (offset + count <= 24)
+//   [6]     triangle mask: bits 3s .. 3s + n - 1 set for a leaf slot s of n (1-3)
+//           triangles; triangle bit b is triangle tri_base + popc(mask below b)
+//           (triangles stored in slot order)    [7] unused
+// (In place of the paper's per-slot meta bytes: the traversal then builds its
+// node and triangle masks from the 8-bit mask of hit slots with two table
+// lookups instead of decoding a byte per child.)
 //   [8..9]  qlo.x[8]   [10..11] qhi.x[8]
 //   [12..13] qlo.y[8]  [14..15] qhi.y[8]
 //   [16..17] qlo.z[8]  [18..19] qhi.z[8]
@@ -301,10 +305,10 @@ void Collapser::emit(std::vector<Item> items, uint32_t level, std::vector<Pendin
     uint32_t imask = 0;
     const uint32_t child_base = (uint32_t)queue.size();
     const uint32_t tri_base = out->n_tris;
-    uint8_t meta[8] = {}, qlo[3][8], qhi[3][8];
+    uint8_t qlo[3][8], qhi[3][8];
+    uint32_t tmask = 0;
     for (int a = 0; a < 3; a++)
         for (int s = 0; s < 8; s++) { qlo[a][s] = 255; qhi[a][s] = 0; }
-    uint32_t tri_off = 0;
     for (int s = 0; s < 8; s++) {
         const int e = entry_of_slot[s];
         if (e < 0) continue;
@@ -318,7 +322,6 @@ void Collapser::emit(std::vector<Item> items, uint32_t level, std::vector<Pendin
         }
         if (sl.inner) {
             imask |= 1u << s;
-            meta[s] = (uint8_t)(0x20u | (24u + (uint32_t)s));
             Pending q{};
             q.node = it.node;
             q.level = level + 1;
@@ -330,20 +333,20 @@ void Collapser::emit(std::vector<Item> items, uint32_t level, std::vector<Pendin
             }
             queue.push_back(q);
         } else {
-            meta[s] = (uint8_t)((((1u << sl.nref) - 1u) << 5) | tri_off);
+            tmask |= ((1u << sl.nref) - 1u) << (3 * s);
             for (uint32_t r = 0; r < sl.nref; r++) {
                 const uint32_t wo = refs[sl.ref0 + r];
                 out->woop.insert(out->woop.end(), woop + (size_t)wo * 4, woop + (size_t)wo * 4 + 12);
                 out->triidx.push_back(triidx[wo]);
             }
-            tri_off += sl.nref;
             out->n_tris += sl.nref;
         }
     }
     w[3] = (uint32_t)(ex[0] + 127) | ((uint32_t)(ex[1] + 127) << 8) | ((uint32_t)(ex[2] + 127) << 16) | (imask << 24);
     w[4] = child_base;
     w[5] = tri_base;
-    for (int s = 0; s < 8; s++) w[6 + s / 4] |= (uint32_t)meta[s] << (8 * (s % 4));
+    w[6] = tmask;
+    w[7] = 0;
     for (int a = 0; a < 3; a++)
         for (int s = 0; s < 8; s++) {
             w[8 + 4 * a + s / 4] |= (uint32_t)qlo[a][s] << (8 * (s % 4));

@@ -4,8 +4,10 @@
 //
 // Per lane: a node group (child_base of a visited node and a mask of its hit
 // inner children, bits 24-31 in octant-permuted order, the node's inner-child
-// mask in bits 0-7), a triangle group (tri_base and a mask of hit leaf
-// triangles, bits 0-23) and a stack of node groups.  The warp walks nodes
+// mask in bits 0-7), a triangle group (tri_base, the node's triangle mask and
+// the hit triangles among its bits) and a stack of node groups.  A node test
+// yields an 8-bit mask of hit slots; two table lookups turn it into both
+// groups (instead of the paper's per-child meta-byte decoding).  The warp walks nodes
 // until every busy lane holds triangles (the counterpart of the binary
 // kernel's postponed leaf), then tests triangles, then refills lanes from the
 // ray source as the binary kernel does (same RaySource policy, same dynamic
@@ -70,8 +72,26 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
     int sp = 0;
     Lane L;
     L.hitIndex = -1;
-    uint32_t ng_base = 0, ng_bits = 0, tg_base = 0, tg_bits = 0;
+    uint32_t ng_base = 0, ng_bits = 0, tg_base = 0, tg_bits = 0, tg_mask = 0;
     bool has_ray = false, retired = false;
+
+    // Tables shared by the block: s_perm[o][m] moves bit s of an 8-bit slot
+    // mask to bit s ^ o (inner children in ray-octant order); s_spread[m]
+    // moves bit s to bit 3s (a slot's three triangle bits).
+    __shared__ uint8_t s_perm[8 * 256];
+    __shared__ uint32_t s_spread[256];
+    for (uint32_t i = threadIdx.x; i < 8u * 256u; i += blockDim.x) {
+        const uint32_t o = i >> 8, m = i & 255u;
+        uint32_t r = 0;
+        for (uint32_t s = 0; s < 8; s++) r |= ((m >> s) & 1u) << (s ^ o);
+        s_perm[i] = (uint8_t)r;
+    }
+    for (uint32_t m = threadIdx.x; m < 256u; m += blockDim.x) {
+        uint32_t r = 0;
+        for (uint32_t s = 0; s < 8; s++) r |= ((m >> s) & 1u) << (3 * s);
+        s_spread[m] = r;
+    }
+    __syncthreads();
 
     for (;;) {
         // ---- refill: lanes without a ray claim the next slots from the queue.
@@ -157,18 +177,7 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                         const uint32_t fy0 = __float_as_uint(ry ? qy.x : qy.z), fy1 = __float_as_uint(ry ? qy.y : qy.w);
                         const uint32_t nz0 = __float_as_uint(rz ? qz.z : qz.x), nz1 = __float_as_uint(rz ? qz.w : qz.y);
                         const uint32_t fz0 = __float_as_uint(rz ? qz.x : qz.z), fz1 = __float_as_uint(rz ? qz.y : qz.w);
-                        // Meta bytes, four children per word: inner children (offset >= 24,
-                        // bits 4 and 3 set) get their slot permuted by the ray octant; each
-                        // child contributes its unary bits at its (permuted) index.
-                        uint32_t bidx[2], cbit[2];
-#pragma unroll
-                        for (int h = 0; h < 2; h++) {
-                            const uint32_t m = __float_as_uint(h ? h1.w : h1.z);
-                            const uint32_t inner = (m & (m << 1)) & 0x10101010u;
-                            bidx[h] = (m ^ ((inner >> 4) * oct_inv)) & 0x1F1F1F1Fu;
-                            cbit[h] = (m >> 5) & 0x07070707u;
-                        }
-                        uint32_t hits = 0;
+                        uint32_t hm = 0;  // slots whose box the ray enters
 #pragma unroll
                         for (int s = 0; s < 8; s += 2) {
                             const int w = s >> 2, hh = (s >> 1) & 1;
@@ -182,16 +191,18 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                                 const float tnz = __fmaf_rn(e ? nz.y : nz.x, sz, az), tfz = __fmaf_rn(e ? fz.y : fz.x, sz, az);
                                 const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, L.tmin));
                                 const float tf = fminf(fminf(tfx, tfy), fminf(tfz, L.hitT));
-                                if (tn <= tf) {
-                                    const uint32_t sel = 0x4440u | (uint32_t)((s + e) & 3);
-                                    hits |= __byte_perm(cbit[w], 0u, sel) << __byte_perm(bidx[w], 0u, sel);
-                                }
+                                if (tn <= tf) hm |= 1u << (s + e);
                             }
                         }
+                        // Hit inner slots, octant-permuted, into bits 24-31 (above the
+                        // node's inner-child mask); hit leaf slots' triangles from the
+                        // node's triangle mask (inner and empty slots have no bits there).
+                        const uint32_t imask = ew >> 24;
                         ng_base = __float_as_uint(h1.x);
-                        ng_bits = (hits & 0xFF000000u) | (ew >> 24);
+                        ng_bits = ((uint32_t)s_perm[(oct_inv << 8) | (hm & imask)] << 24) | imask;
                         tg_base = __float_as_uint(h1.y);
-                        tg_bits = hits & 0x00FFFFFFu;
+                        tg_mask = __float_as_uint(h1.z);
+                        tg_bits = (s_spread[hm] * 7u) & tg_mask;
                     }
                 }
             }
@@ -201,7 +212,9 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                 while (tg_bits) {
                     const int i = __ffs(tg_bits) - 1;
                     tg_bits &= tg_bits - 1u;
-                    if (cw8_triangle(L, 3 * (int)(tg_base + (uint32_t)i)) && L.mode() != kClosest) {
+                    // Triangle bit i is the node's (mask bits below i)-th triangle.
+                    const uint32_t tri = tg_base + (uint32_t)__popc(tg_mask & ((1u << i) - 1u));
+                    if (cw8_triangle(L, 3 * (int)tri) && L.mode() != kClosest) {
                         tg_bits = 0;
                         ng_bits = 0;
                         sp = 0;

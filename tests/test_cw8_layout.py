@@ -18,14 +18,14 @@ def _decode(nodes):
     imask = b[:, 15].astype(np.uint32)
     child_base = nodes[:, 4].astype(np.int64)
     tri_base = nodes[:, 5].astype(np.int64)
-    meta = b[:, 24:32].astype(np.uint32)
+    tmask = nodes[:, 6].astype(np.uint32)
     q = {}
     for a, (lo, hi) in enumerate(((32, 40), (48, 56), (64, 72))):
         q[("lo", a)] = b[:, lo:lo + 8].astype(np.float64)
         q[("hi", a)] = b[:, hi:hi + 8].astype(np.float64)
     lo = np.stack([p[:, a:a + 1] + q[("lo", a)] * scale[:, a:a + 1] for a in range(3)], -1)  # (n, 8, 3)
     hi = np.stack([p[:, a:a + 1] + q[("hi", a)] * scale[:, a:a + 1] for a in range(3)], -1)
-    return imask, child_base, tri_base, meta, lo, hi
+    return imask, child_base, tri_base, tmask, lo, hi
 
 
 def _binary_leaf_refs(bvh):
@@ -102,24 +102,23 @@ def _check_layout(rb, orc, bvh, r):
                 k += 3
     for i in range(nt):
         assert cw["woop"][i].tobytes() in rows_b[int(triidx[i])]
-    imask, child_base, tri_base, meta, lo, hi = _decode(nodes)
+    imask, child_base, tri_base, tmask, lo, hi = _decode(nodes)
     parent = {}
     tri_loc = collections.defaultdict(list)
+    assert (nodes[:, 7] == 0).all() and (tmask < (1 << 24)).all()
     for i in range(n):
         for s in range(8):
-            m = int(meta[i, s])
-            if m == 0:
-                continue
-            off, bits = m & 31, m >> 5
-            if off >= 24:
-                assert bits == 1 and off == 24 + s and (imask[i] >> s) & 1
+            bits = (int(tmask[i]) >> (3 * s)) & 7
+            if (imask[i] >> s) & 1:
+                assert bits == 0
                 c = int(child_base[i]) + bin(int(imask[i]) & ((1 << s) - 1)).count("1")
                 assert 0 < c < n and c not in parent
                 parent[c] = (i, s)
-            else:
-                assert bits in (1, 3, 7) and not (imask[i] >> s) & 1
+            elif bits:
+                assert bits in (1, 3, 7)
+                off = bin(int(tmask[i]) & ((1 << (3 * s)) - 1)).count("1")
                 cnt = bits.bit_length()
-                assert off + cnt <= 24 and int(tri_base[i]) + off + cnt <= nt
+                assert int(tri_base[i]) + off + cnt <= nt
                 for k in range(cnt):
                     tri_loc[int(triidx[int(tri_base[i]) + off + k])].append((i, s))
     assert len(parent) == n - 1          # a tree: every node but the root has one parent
