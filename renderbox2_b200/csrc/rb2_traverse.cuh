@@ -301,7 +301,7 @@ __device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_thr
 
                         const float Oz = __fmaf_rn(-L.oz, v00.z, __fmaf_rn(-L.oy, v00.y, __fmaf_rn(-L.ox, v00.x, v00.w)));
                         const float Dz = __fmaf_rn(L.dz, v00.z, __fmaf_rn(L.dy, v00.y, __fmul_rn(L.dx, v00.x)));
-                        const float t = __fmul_rn(Oz, __fdiv_rn(1.0f, Dz));
+                        const float t = __fmul_rn(Oz, __frcp_rn(Dz));  // IEEE 1 / Dz, as __fdiv_rn(1, Dz)
                         if (t > L.tmin && t < L.hitT) {
                             const float Ox = __fmaf_rn(L.oz, v11.z, __fmaf_rn(L.oy, v11.y, __fmaf_rn(L.ox, v11.x, v11.w)));
                             const float Dx = __fmaf_rn(L.dz, v11.z, __fmaf_rn(L.dy, v11.y, __fmul_rn(L.dx, v11.x)));
