@@ -960,10 +960,11 @@ template <int LAYOUT, class Src>
 int launch_persistent_shape(const Src& src, uint64_t work, const rb2_integrator* it, unsigned int* status, cudaStream_t s)
 {
     const uint32_t th = it->tr_threshold;
+    const uint32_t regs = it->tr_regs ? it->tr_regs : (LAYOUT == rb2dev::kLayoutCw8 ? 64u : 48u);
     if (it->tr_block == 256)
-        return it->tr_regs == 48 ? launch_persistent_variant<256, 48, LAYOUT>(src, work, it->sms, th, status, s)
+        return regs == 48 ? launch_persistent_variant<256, 48, LAYOUT>(src, work, it->sms, th, status, s)
                                  : launch_persistent_variant<256, 64, LAYOUT>(src, work, it->sms, th, status, s);
-    return it->tr_regs == 48 ? launch_persistent_variant<128, 48, LAYOUT>(src, work, it->sms, th, status, s)
+    return regs == 48 ? launch_persistent_variant<128, 48, LAYOUT>(src, work, it->sms, th, status, s)
                              : launch_persistent_variant<128, 64, LAYOUT>(src, work, it->sms, th, status, s);
 }
 
@@ -1186,7 +1187,7 @@ int rb2_integrator_set_launch(rb2_integrator* it, const rb2_launch_config* cfg)
     if (cfg->regs && cfg->regs != 64 && cfg->regs != 48) return fail(RB2_ENOTSUP, "integrator regs must be 64 or 48");
     if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
     it->tr_block = cfg->block_threads ? cfg->block_threads : 128;
-    it->tr_regs = cfg->regs ? cfg->regs : 48;
+    it->tr_regs = cfg->regs;
     it->tr_threshold = cfg->fetch_threshold ? cfg->fetch_threshold : 24;
     return RB2_OK;
 }

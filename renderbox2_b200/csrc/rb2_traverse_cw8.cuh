@@ -73,6 +73,7 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
     Lane L;
     L.hitIndex = -1;
     uint32_t ng_base = 0, ng_bits = 0, tg_base = 0, tg_bits = 0, tg_mask = 0;
+    uint32_t tg2_base = 0, tg2_bits = 0, tg2_mask = 0;  // a second pending triangle group
     bool has_ray = false, retired = false;
 
     // Tables shared by the block: s_perm[o][m] moves bit s of an 8-bit slot
@@ -116,6 +117,7 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                     ng_base = 0;             // the root: node 0, reached through bit 31
                     ng_bits = 0x80000000u;   // with an empty inner-child mask
                     tg_bits = 0;
+                    tg2_bits = 0;
                     has_ray = true;
                 }
             }
@@ -125,7 +127,7 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
         while (__any_sync(kFull, has_ray)) {
             // ---- nodes, until every busy lane holds triangles or is done.
             for (;;) {
-                const bool in = has_ray && tg_bits == 0 && (ng_bits > 0x00FFFFFFu || sp > 0);
+                const bool in = has_ray && tg2_bits == 0 && (ng_bits > 0x00FFFFFFu || sp > 0);
                 if (!__any_sync(kFull, in)) break;
                 if (in) {
                     if (ng_bits <= 0x00FFFFFFu) {
@@ -200,27 +202,37 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                         const uint32_t imask = ew >> 24;
                         ng_base = __float_as_uint(h1.x);
                         ng_bits = ((uint32_t)s_perm[(oct_inv << 8) | (hm & imask)] << 24) | imask;
-                        tg_base = __float_as_uint(h1.y);
-                        tg_mask = __float_as_uint(h1.z);
-                        tg_bits = (s_spread[hm] * 7u) & tg_mask;
+                        const uint32_t tmask = __float_as_uint(h1.z), tbits = (s_spread[hm] * 7u) & tmask;
+                        if (tbits) {
+                            if (tg_bits == 0) {
+                                tg_base = __float_as_uint(h1.y); tg_mask = tmask; tg_bits = tbits;
+                            } else {
+                                tg2_base = __float_as_uint(h1.y); tg2_mask = tmask; tg2_bits = tbits;
+                            }
+                        }
                     }
                 }
             }
 
             // ---- triangles of the current group, then finish lanes with no work left.
             if (has_ray) {
-                while (tg_bits) {
+                for (;;) {
+                    if (tg_bits == 0) {
+                        if (tg2_bits == 0) break;
+                        tg_base = tg2_base; tg_mask = tg2_mask; tg_bits = tg2_bits; tg2_bits = 0;
+                    }
                     const int i = __ffs(tg_bits) - 1;
                     tg_bits &= tg_bits - 1u;
                     // Triangle bit i is the node's (mask bits below i)-th triangle.
                     const uint32_t tri = tg_base + (uint32_t)__popc(tg_mask & ((1u << i) - 1u));
                     if (cw8_triangle(L, 3 * (int)tri) && L.mode() != kClosest) {
                         tg_bits = 0;
+                        tg2_bits = 0;
                         ng_bits = 0;
                         sp = 0;
                     }
                 }
-                if (tg_bits == 0 && ng_bits <= 0x00FFFFFFu && sp == 0) {
+                if (ng_bits <= 0x00FFFFFFu && sp == 0) {
                     src.finish(L);
                     has_ray = false;
                 }
