@@ -73,6 +73,14 @@ def _rays_at_cluster(n, seed):
     return r
 
 
+def test_cw8_layout_on_a_room(rb, orc):
+    """The config-2 style room: axis-aligned walls and boxes (flat leaf boxes)
+    and icospheres."""
+    sc = rb.RoomScene(seed=4, n_boxes=12, n_spheres=40, sphere_subdiv=2, n_lights=2)
+    r, _ = rb.surface_rays(sc, seed=9, n=3000)
+    _check_layout(rb, orc, rb.BVH(sc), r)
+
+
 def test_cw8_layout_splits_large_leaves(rb, orc):
     bvh = rb.BVH(_degenerate_scene(rb))
     _check_layout(rb, orc, bvh, _rays_at_cluster(2000, 5))
