@@ -247,6 +247,7 @@ void Collapser::emit(std::vector<Item> items, uint32_t level, std::vector<Pendin
         uint32_t ref0, nref;
     };
     std::vector<Slot> entries;
+    entries.reserve(8);
     for (int i = 0; i < (int)items.size(); i++) {
         if (items[i].node >= 0 || demoted[i]) { entries.push_back({i, true, 0, 0}); continue; }
         for (uint32_t r = 0; r < items[i].nref; r += 3)
@@ -268,19 +269,25 @@ void Collapser::emit(std::vector<Item> items, uint32_t level, std::vector<Pendin
             double c;
             int e, s;
         };
-        std::vector<Cost> costs;
-        for (int e = 0; e < (int)entries.size(); e++) {
+        Cost costs[64];  // at most eight entries (the demotion above keeps slots <= 8)
+        int nc = 0;
+        for (int e = 0; e < (int)entries.size() && e < 8; e++) {
             const Item& it = items[entries[e].item];
             double d[3];
             for (int a = 0; a < 3; a++) d[a] = 0.5 * (it.lo[a] + it.hi[a]) - 0.5 * (ulo[a] + uhi[a]);
             for (int s = 0; s < 8; s++) {
                 const double c = (s & 1 ? -d[0] : d[0]) + (s & 2 ? -d[1] : d[1]) + (s & 4 ? -d[2] : d[2]);
-                costs.push_back({c, e, s});
+                costs[nc++] = {c, e, s};
             }
         }
-        std::stable_sort(costs.begin(), costs.end(), [](const Cost& a, const Cost& b) { return a.c < b.c; });
-        for (const Cost& c : costs)
+        // Ties in cost resolve in (entry, slot) order.
+        std::sort(costs, costs + nc, [](const Cost& a, const Cost& b) {
+            return a.c < b.c || (a.c == b.c && (a.e < b.e || (a.e == b.e && a.s < b.s)));
+        });
+        for (int k = 0; k < nc; k++) {
+            const Cost& c = costs[k];
             if (slot_of_entry[c.e] < 0 && entry_of_slot[c.s] < 0) { slot_of_entry[c.e] = c.s; entry_of_slot[c.s] = c.e; }
+        }
     }
     // Quantization grid.
     float p[3];
@@ -366,6 +373,12 @@ int collapse_cw8(const uint32_t* nodes, uint64_t n_nodes_u4, const uint32_t* woo
     c.woop = woop;
     c.triidx = triidx;
     c.out = &out;
+    // Size hints from the binary inner-node count (about 3 per wide node,
+    // about 3 triangle refs per binary leaf).
+    const size_t n_inner = (size_t)(n_nodes_u4 / 4);
+    out.nodes.reserve((n_inner / 3 + 1) * 20);
+    out.woop.reserve((n_inner + 1) * 3 * 12);
+    out.triidx.reserve((n_inner + 1) * 3);
     double m = 0.0;
     for (int k = 0; k < 2; k++) {
         const Item r = c.child(0, k, false);
