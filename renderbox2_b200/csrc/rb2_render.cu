@@ -342,12 +342,12 @@ __global__ void k_pt_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t 
                 const float3 ng = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
                 const float3 wo = mul(d, -1.0f);
                 float4 Tp = T[path];
-                float4 Lp = L[path];
                 const float4 E = sc.emission[tri.w];
                 if (E.x > 0.0f || E.y > 0.0f || E.z > 0.0f) {
                     // DiffuseAreaLight::L (core/lights.cu:70-78): one-sided emitter.
                     const float cosl = dot3(ng, wo);
                     if (cosl > 0.0f) {
+                        float4 Lp = L[path];  // read only where a path gains emission
                         float w = 1.0f;
                         if (b > 0 && Tp.w > 0.0f) {  // T.w < 0: the last bounce was specular
                             const float pdf_l = inv_nl * t * t / (tri_area(v0, v1, v2) * cosl);
