@@ -38,6 +38,19 @@ __device__ __forceinline__ float2 cw8_planes(uint32_t w, int h)
     return __half22float2(v);
 }
 
+// Two IEEE single-precision FMAs in one paired instruction (sm_100 f32x2).
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
+{
+    unsigned long long ra, rb, rc, rd;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(ra) : "f"(a.x), "f"(a.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(rb) : "f"(b.x), "f"(b.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(rc) : "f"(c.x), "f"(c.y));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rd) : "l"(ra), "l"(rb), "l"(rc));
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(rd));
+    return r;
+}
+
 // Woop test of one triangle (the binary leaf loop's arithmetic); updates
 // hitT / hitIndex and returns true when it accepts.
 __device__ __forceinline__ bool cw8_triangle(Lane& L, int triAddr)
@@ -180,17 +193,23 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                         const uint32_t nz0 = __float_as_uint(rz ? qz.z : qz.x), nz1 = __float_as_uint(rz ? qz.w : qz.y);
                         const uint32_t fz0 = __float_as_uint(rz ? qz.x : qz.z), fz1 = __float_as_uint(rz ? qz.y : qz.w);
                         uint32_t hm = 0;  // slots whose box the ray enters
+                        const float2 sx2 = make_float2(sx, sx), sy2 = make_float2(sy, sy), sz2 = make_float2(sz, sz);
+                        const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), az2 = make_float2(az, az);
 #pragma unroll
                         for (int s = 0; s < 8; s += 2) {
                             const int w = s >> 2, hh = (s >> 1) & 1;
                             const float2 nx = cw8_planes(w ? nx1 : nx0, hh), fx = cw8_planes(w ? fx1 : fx0, hh);
                             const float2 ny = cw8_planes(w ? ny1 : ny0, hh), fy = cw8_planes(w ? fy1 : fy0, hh);
                             const float2 nz = cw8_planes(w ? nz1 : nz0, hh), fz = cw8_planes(w ? fz1 : fz0, hh);
+                            // Slab distances of the two children, one paired FMA per plane.
+                            const float2 tnx2 = fma2(nx, sx2, ax2), tfx2 = fma2(fx, sx2, ax2);
+                            const float2 tny2 = fma2(ny, sy2, ay2), tfy2 = fma2(fy, sy2, ay2);
+                            const float2 tnz2 = fma2(nz, sz2, az2), tfz2 = fma2(fz, sz2, az2);
 #pragma unroll
                             for (int e = 0; e < 2; e++) {
-                                const float tnx = __fmaf_rn(e ? nx.y : nx.x, sx, ax), tfx = __fmaf_rn(e ? fx.y : fx.x, sx, ax);
-                                const float tny = __fmaf_rn(e ? ny.y : ny.x, sy, ay), tfy = __fmaf_rn(e ? fy.y : fy.x, sy, ay);
-                                const float tnz = __fmaf_rn(e ? nz.y : nz.x, sz, az), tfz = __fmaf_rn(e ? fz.y : fz.x, sz, az);
+                                const float tnx = e ? tnx2.y : tnx2.x, tfx = e ? tfx2.y : tfx2.x;
+                                const float tny = e ? tny2.y : tny2.x, tfy = e ? tfy2.y : tfy2.x;
+                                const float tnz = e ? tnz2.y : tnz2.x, tfz = e ? tfz2.y : tfz2.x;
                                 const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, L.tmin));
                                 const float tf = fminf(fminf(tfx, tfy), fminf(tfz, L.hitT));
                                 if (tn <= tf) hm |= 1u << (s + e);
