@@ -131,9 +131,10 @@ typedef struct {
  * reported), or a compressed 8-wide layout (RB2_NODE_ORDER_CW8: eight child
  * boxes quantized to 8 bits per plane in an 80-byte node, conservatively
  * enlarged, and the same Woop triangles stored per node; closest hits are
- * identical except for ties in t).  Integrators traverse the compressed
- * 8-wide layout when it is set and the binary Compact2 buffer otherwise;
- * rb2_tracer_dev_bvh and rb2_trace_isect always use the binary buffer. */
+ * identical except for ties in t).  Integrators and rb2_trace_isect traverse
+ * the compressed 8-wide layout when it is set and the binary Compact2 buffer
+ * otherwise; rb2_tracer_dev_bvh (the header-only device traversal) always
+ * uses the binary buffer. */
 enum { RB2_NODE_ORDER_DFS = 0, RB2_NODE_ORDER_BFS = 1, RB2_NODE_ORDER_WIDE4 = 2, RB2_NODE_ORDER_CW8 = 3 };
 
 /* Ray-query modes. */

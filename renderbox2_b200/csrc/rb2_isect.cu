@@ -11,6 +11,7 @@
 #include "rb2_render.h"
 #include "rb2_render_internal.h"
 #include "rb2_traverse.cuh"
+#include "rb2_traverse_cw8.cuh"
 
 #include <cuda_runtime.h>
 
@@ -79,12 +80,14 @@ struct IsectSource {
     }
 };
 
-template <int BLOCK>
+// LAYOUT: binary Compact2 or compressed 8-wide nodes (the tracer's layout).
+template <int BLOCK, int LAYOUT>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
     k_trace_isect(const __grid_constant__ IsectSource src, uint32_t fetch_threshold, unsigned int* status)
 {
     IsectSource s = src;
-    persistent_trace(s, fetch_threshold, status);
+    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8(s, fetch_threshold, status);
+    else persistent_trace(s, fetch_threshold, status);
 }
 
 __global__ void k_trace_per_thread(rb2_dev_bvh bvh, const float4* rays, const uint8_t* mask, uint32_t n, int any_hit,
@@ -147,7 +150,7 @@ int rb2_trace_isect(rb2_tracer* t, const rb2_scene_dev* scene, const float* d_ra
     }
     if (n == 0) return RB2_OK;
     const cudaStream_t s = (cudaStream_t)stream;
-    const DeviceBvhView bv = device_bvh(t);
+    const DeviceBvhView bv = device_bvh(t, true);  // the compressed layout when the tracer uses it
     rb2dev::IsectSource src{};
     src.nodes = static_cast<const float4*>(bv.nodes);
     src.woop = static_cast<const float4*>(bv.woop);
@@ -164,10 +167,11 @@ int rb2_trace_isect(rb2_tracer* t, const rb2_scene_dev* scene, const float* d_ra
     int dev = 0, sms = 0, per_sm = 0;
     RB2_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
     RB2_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb2dev::k_trace_isect<128>, 128, 0), "occupancy");
+    auto kern = bv.cw8 ? rb2dev::k_trace_isect<128, rb2dev::kLayoutCw8> : rb2dev::k_trace_isect<128, rb2dev::kLayoutBinary>;
+    RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0), "occupancy");
     uint64_t blocks = (uint64_t)sms * (uint64_t)std::max(1, per_sm);
     blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, ((uint64_t)n + 127) / 128));
-    rb2dev::k_trace_isect<128><<<(unsigned)blocks, 128, 0, s>>>(src, 20u, bv.status);
+    kern<<<(unsigned)blocks, 128, 0, s>>>(src, 20u, bv.status);
     RB2_CUDA(cudaGetLastError(), "isect launch");
     return RB2_OK;
 }

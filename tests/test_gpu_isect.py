@@ -33,13 +33,16 @@ def _bits(x):
     return np.ascontiguousarray(x).view(np.uint32)
 
 
-@pytest.mark.parametrize("masked", [False, True])
-def test_trace_isect_closest_matches_oracle(rb, orc, cuda, masked):
+@pytest.mark.parametrize("masked,order", [(False, 0), (True, 0), (False, 3), (True, 3)])
+def test_trace_isect_closest_matches_oracle(rb, orc, cuda, masked, order):
+    """order 3: the tracer on the compressed 8-wide layout, which
+    rb2_trace_isect then traverses."""
     from renderbox2_b200.render import DeviceScene, trace_isect
     torch = cuda
     scene = _room(rb)
     bvh = rb.BVH(scene)
     tr = rb.CudaTracer(bvh)
+    tr.set_node_order(order)
     ds = DeviceScene(scene)
     nodes, woop, tri = bvh.buffers_view()
     rays = _rays(rb, scene, 20_011, seed=42)
