@@ -69,7 +69,9 @@ def test_trace_isect_closest_matches_oracle(rb, orc, cuda, masked, order):
         h2 = hits.copy()
         h2["prim"][tie] = gp[tie].astype(np.int32)
         want = orc.isect(np.asarray(scene.vertices, np.float32), _tris4(scene), rays, h2)
-    assert tie.sum() <= max(2, hit.sum() // 10000)
+    # Ties are rare and all confirmed above; the compressed layout visits
+    # leaves in another order, so it reports the other triangle more often.
+    assert tie.sum() <= (max(2, hit.sum() // 10000) if order == 0 else max(16, hit.sum() // 500))
     for k_got, k_want in (("position", "position"), ("geometric_normal", "ng"), ("shading_normal", "ns"),
                           ("incoming_direction", "wi")):
         assert np.array_equal(_bits(got[k_got][:, hit]), _bits(want[k_want][:, hit])), k_got
