@@ -226,15 +226,20 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
  * (path, depth), so the cache is deterministic); each camera vertex then adds
  * emission (s = 0), next-event estimation (s = 1) and `connections`
  * connections to uniformly chosen cached vertices (s >= 2, scaled by
- * cached vertices / light paths).  Every strategy of a path of k segments
- * (k <= max_path_length) is weighted 1/k: all k strategies are sampled, so the
- * estimator is unbiased.  (The reference weights connections by
- * 1/((bounce+1)+depth) but gives NEE full weight and omits the cache-size
- * factor.)  Layered materials are supported when no non-emitter material has a
- * mirror or glass layer (else RB2_ENOTSUP): vertices take f from the material
- * functions, and light subpaths continue with the adjoint f(sampled -> incoming)
- * because the Blinn microfacet's shadowing term is not symmetric.
- * d_rgb[3*pixel] = mean radiance over spp iterations. */
+ * cached vertices / light paths).  A path of k segments (k <= max_path_length)
+ * is sampled by emission and by a connection across each edge whose two
+ * endpoints scatter non-specularly on that path (the camera counts as
+ * specular, the light point as non-specular); each of those n strategies is
+ * weighted 1/n, which is 1/k when no vertex is specular, so the estimator is
+ * unbiased.  (The reference weights connections by 1/((bounce+1)+depth) but
+ * gives NEE full weight and omits the cache-size factor.)  Layered materials,
+ * mirror and glass layers included: vertices take f from the material
+ * functions (a connection uses the non-specular part), vertices of purely
+ * specular materials are not cached, light subpaths continue with the adjoint
+ * f(sampled -> incoming) because the Blinn microfacet's shadowing term is not
+ * symmetric, and a glass transmission sampled on a light subpath takes the
+ * adjoint factor (eta of the outgoing side / eta of the incoming side)^6 times
+ * the camera-side factor.  d_rgb[3*pixel] = mean radiance over spp iterations. */
 typedef struct {
     uint32_t spp;
     uint32_t max_path_length;   /* segments, camera to light (config 3: 6) */

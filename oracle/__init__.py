@@ -419,8 +419,8 @@ def bdpt(bvh_buffers, vertices, indices, tri_mat, albedo, emission, lights, cam_
          K, C, rr_start, rr_prob, seed=1, nthreads=0, materials=None):
     """FP64 BDPT-LVC mean radiance per camera pixel over n_iter iterations.
 
-    `materials` (optional): layered material descriptions per material; no
-    layer may be specular (mirror or glass)."""
+    `materials` (optional): layered material descriptions per material,
+    mirror and glass layers included."""
     L = orc_lib()
     L.rb2o_bdpt.argtypes = [C_.POINTER(_Bvh), C_.POINTER(_Scene), C_.c_void_p, C_.c_uint32, C_.c_uint32, C_.c_uint32,
                             C_.c_uint32, C_.c_uint32, C_.c_uint32, C_.c_float, C_.c_uint64, C_.c_void_p, C_.c_int]

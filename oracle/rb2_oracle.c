@@ -653,11 +653,14 @@ static double mat_pdf(const rb2o_material* m, d3 wo, d3 wi)
     return n ? p / n : 0.0;
 }
 /* Returns f; wi_w, pdf, specular out. */
+/* eta_io (nullable): for a sampled glass layer, the index of wo's side over
+ * wi's side (1 otherwise). */
 static d3 mat_sample(const rb2o_material* m, d3 n, d3 wo_w, double u1, double u2, double uc, d3* wi_w, double* pdf,
-                     int* specular)
+                     int* specular, double* eta_io)
 {
     *pdf = 0.0;
     *specular = 0;
+    if (eta_io) *eta_io = 1.0;
     if (m->n_layers == 0) return D3(0, 0, 0);
     frame3 fr = frame_z(n);
     d3 wo = fr_local(&fr, wo_w);
@@ -680,6 +683,7 @@ static d3 mat_sample(const rb2o_material* m, d3 n, d3 wo_w, double u1, double u2
         *pdf = 1.0;
         double F = fres_diel(wo.z, l->etai, l->etat);
         f = dmul(col(l), (et * et) / (ei * ei) * (1.0 - F) / fabs(wi.z));
+        if (eta_io) *eta_io = ei / et;
     } else if (l->type == 4) {
         double e = l->exponent, ct = pow(u1, 1.0 / (e + 1.0)), st = sqrt(1.0 - ct * ct > 0.0 ? 1.0 - ct * ct : 0.0);
         double phi = u2 * 2.0 * RB2O_PI;
@@ -715,7 +719,7 @@ void rb2o_material_query(const rb2o_material* m, int sample, const double* q, do
         d3 wi = D3(0, 0, 0);
         double pdf;
         int spec;
-        d3 f = mat_sample(m, n, wo_w, q[6], q[7], q[8], &wi, &pdf, &spec);
+        d3 f = mat_sample(m, n, wo_w, q[6], q[7], q[8], &wi, &pdf, &spec, NULL);
         out[0] = wi.x; out[1] = wi.y; out[2] = wi.z; out[3] = f.x; out[4] = f.y; out[5] = f.z; out[6] = pdf;
         out[7] = spec;
     } else {
@@ -817,7 +821,8 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
                 d3 wi = D3(0, 0, 0);
                 double pdf;
                 int spec;
-                d3 f = mat_sample(mt, ng, wo, u01(seed, key, 3), u01(seed, key, 4), u01(seed, key, 6), &wi, &pdf, &spec);
+                d3 f = mat_sample(mt, ng, wo, u01(seed, key, 3), u01(seed, key, 4), u01(seed, key, 6), &wi, &pdf, &spec,
+                                  NULL);
                 if (!(pdf > 0.0) || !(f.x > 0.0 || f.y > 0.0 || f.z > 0.0)) break;
                 double k = fabs(ddot(wi, ng)) / pdf;
                 T[0] *= f.x * k; T[1] *= f.y * k; T[2] *= f.z * k;
@@ -886,8 +891,14 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
  * uniform point, cosine direction), every non-emitter surface vertex y1..y_Dl
  * cached (Dl = K - 2); then one camera path per camera ray with emission
  * (s = 0), NEE (s = 1) and C uniform cache connections (s >= 2, scaled by
- * cache size / light paths), each strategy of a k-segment path weighted 1/k. */
-typedef struct { d3 pos, nrm, beta, wi, ng; uint32_t s, mat; } lvc_vertex;
+ * cache size / light paths).  A k-segment path is sampled by emission and by a
+ * connection across each edge whose endpoints both scatter non-specularly (the
+ * camera counts as specular, the light point not); each of those n strategies
+ * is weighted 1/n (1/k without specular vertices).  Vertices of purely
+ * specular materials are not cached. */
+/* el: valid connection edges on the light side with this vertex as a
+ * (non-specular) endpoint; see the strategy counting in rb2o_bdpt. */
+typedef struct { d3 pos, nrm, beta, wi, ng; double el; uint32_t s, mat; } lvc_vertex;
 
 void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, uint32_t n_cam, uint32_t n_iter,
                uint32_t n_light_paths, uint32_t K, uint32_t C, uint32_t rr_start, float rr_prob, uint64_t seed,
@@ -929,6 +940,8 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
             double beta[3] = {Le[0] * kk, Le[1] * kk, Le[2] * kk};
             float ray[8];
             mkray(ray, y0, 1.0e-4, dir, 3.402823466e+38);
+            int nsp_prev = 1;      /* the light point scatters non-specularly */
+            uint32_t edges = 0;    /* valid connection edges so far */
             for (uint32_t d = 1; d <= Dl; d++) {
                 rb2o_hit h;
                 trace_ct(b, ray, 0, &h, RB2O_RAY_LIGHT);
@@ -944,24 +957,36 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                 d3 nrm = ddot(ng, wo) < 0.0 ? dmul(ng, -1.0) : ng;
                 d3 pos = dadd(D3(ray[0], ray[1], ray[2]), dmul(dd, h.t));
                 size_t slot = (size_t)p * Dl + (d - 1);
-                sparse[slot].pos = pos; sparse[slot].nrm = nrm;
-                sparse[slot].beta = D3(beta[0], beta[1], beta[2]);
-                sparse[slot].s = d + 1; sparse[slot].mat = m;
-                sparse[slot].wi = wo; sparse[slot].ng = ng;
-                valid[slot] = 1;
+                /* Purely specular vertices cannot be connected to: not cached. */
+                if (!s->materials || plain_lambertian(&s->materials[m]) || has_nondelta(&s->materials[m])) {
+                    sparse[slot].pos = pos; sparse[slot].nrm = nrm;
+                    sparse[slot].beta = D3(beta[0], beta[1], beta[2]);
+                    sparse[slot].s = d + 1; sparse[slot].mat = m;
+                    sparse[slot].wi = wo; sparse[slot].ng = ng;
+                    sparse[slot].el = (double)(edges + (uint32_t)nsp_prev);
+                    valid[slot] = 1;
+                }
                 if (d >= Dl) break;
                 if (s->materials && !plain_lambertian(&s->materials[m])) {
                     /* Layered (non-specular) material: sample its BSDF toward the next light vertex. */
                     d3 wn = D3(0, 0, 0);
-                    double pdf;
+                    double pdf, eta_io;
                     int spec;
                     d3 f = mat_sample(&s->materials[m], ng, wo, u01(ls, key, 8 + 8 * d), u01(ls, key, 9 + 8 * d),
-                                      u01(ls, key, 11 + 8 * d), &wn, &pdf, &spec);
+                                      u01(ls, key, 11 + 8 * d), &wn, &pdf, &spec, &eta_io);
                     if (!(pdf > 0.0) || !(f.x > 0.0 || f.y > 0.0 || f.z > 0.0)) break;
-                    /* Light flows from wo toward wn: the adjoint f(wn -> wo) (the Blinn
-                     * shadowing term is not symmetric in its two directions). */
-                    frame3 frl = frame_z(ng);
-                    f = mat_f(&s->materials[m], ng, wn, wo, fr_local(&frl, wn), fr_local(&frl, wo));
+                    if (!spec) {
+                        /* Light flows from wo toward wn: the adjoint f(wn -> wo) (the Blinn
+                         * shadowing term is not symmetric in its two directions). */
+                        frame3 frl = frame_z(ng);
+                        f = mat_f(&s->materials[m], ng, wn, wo, fr_local(&frl, wn), fr_local(&frl, wo));
+                    } else {
+                        /* Adjoint of a glass transmission: (eta_o / eta_i)^6 times the
+                         * sampled factor (the camera-side (eta_i / eta_o)^2 and the solid
+                         * angle map of the refraction); 1 for a mirror. */
+                        double e2 = eta_io * eta_io;
+                        f = dmul(f, e2 * e2 * e2);
+                    }
                     double k = fabs(ddot(wn, nrm)) / pdf;
                     double fac[3] = {f.x * k, f.y * k, f.z * k};
                     double lum = 0.212671 * fac[0] + 0.715160 * fac[1] + 0.072169 * fac[2];
@@ -969,6 +994,8 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                     if (d < rr_start) q = 1.0; else if (q > rr_prob) q = rr_prob;
                     if (!(q > 0.0 && u01(ls, key, 10 + 8 * d) < q)) break;
                     for (int c2 = 0; c2 < 3; c2++) beta[c2] *= fac[c2] / q;
+                    edges += (nsp_prev && !spec) ? 1u : 0u;
+                    nsp_prev = !spec;
                     mkray(ray, pos, 1.0e-3 * (double)h.t, wn, 3.402823466e+38);
                     continue;
                 }
@@ -982,6 +1009,8 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                 if (d < rr_start) q = 1.0; else if (q > rr_prob) q = rr_prob;
                 if (!(q > 0.0 && u01(ls, key, 10 + 8 * d) < q)) break;
                 for (int c = 0; c < 3; c++) beta[c] *= A[c] / q;
+                edges += nsp_prev ? 1u : 0u;
+                nsp_prev = 1;
                 mkray(ray, pos, 1.0e-3 * (double)h.t, wi, 3.402823466e+38);
             }
         }
@@ -993,6 +1022,12 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
 #endif
         for (int64_t ci = 0; ci < (int64_t)n_cam; ci++) {
             double L[3] = {0, 0, 0}, T[3] = {1, 1, 1};
+            /* Strategy counting: a k-segment path is weighted 1 / n_valid, n_valid =
+             * 1 + (edges whose endpoints both scatter non-specularly); cnsp: the
+             * previous camera vertex scattered non-specularly (the camera counts as
+             * specular), cedges: valid edges among the camera vertices so far. */
+            int cnsp = 0;
+            uint32_t cedges = 0;
             float ray[8];
             for (int k = 0; k < 8; k++) ray[k] = cam_rays[8 * ((size_t)it * n_cam + ci) + k];
             const uint64_t key = (uint64_t)it * n_cam + (uint64_t)ci;
@@ -1011,7 +1046,7 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                 const float* E = s->emission + 3 * (size_t)m;
                 if (E[0] > 0.0f || E[1] > 0.0f || E[2] > 0.0f) {
                     if (ddot(ng, wo) > 0.0)
-                        for (int c = 0; c < 3; c++) L[c] += T[c] * E[c] / (double)i;
+                        for (int c = 0; c < 3; c++) L[c] += T[c] * E[c] / (double)(1u + cedges + (uint32_t)cnsp);
                     break;
                 }
                 d3 nrm = ddot(ng, wo) < 0.0 ? dmul(ng, -1.0) : ng;
@@ -1044,7 +1079,7 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                             float sr[8];
                             mkray(sr, pos, eps, wi, dist * (1.0 - 1.0e-3));
                             if (!occluded(b, sr)) {
-                                double k = fabs(cos_s) / pdf_l / (double)(i + 1);
+                                double k = fabs(cos_s) / pdf_l / (double)(2u + cedges + (uint32_t)cnsp);
                                 L[0] += T[0] * f.x * Le[0] * k;
                                 L[1] += T[1] * f.y * Le[1] * k;
                                 L[2] += T[2] * f.z * Le[2] * k;
@@ -1056,7 +1091,8 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                         mkray(sr, pos, eps, wi, dist * (1.0 - 1.0e-3));
                         if (!occluded(b, sr))
                             for (int c = 0; c < 3; c++)
-                                L[c] += T[c] * (A[c] / RB2O_PI) * Le[c] * cos_s / pdf_l / (double)(i + 1);
+                                L[c] += T[c] * (A[c] / RB2O_PI) * Le[c] * cos_s / pdf_l /
+                                        (double)(2u + cedges + (uint32_t)cnsp);
                     }
                 }
                 if (M > 0 && i + 2 <= K) {
@@ -1091,7 +1127,7 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                             mkray(cr, pos, eps, dir, dist * (1.0 - 1.0e-3));
                             if (occluded_t(b, cr, RB2O_RAY_CONNECTION)) continue;
                             double g = fabs(cos_c) * fabs(cos_v) / dist2 * ((double)M / (double)n_light_paths) /
-                                       ((double)(V->s + i) * (double)C);
+                                       ((2.0 + (double)cedges + (double)cnsp + V->el) * (double)C);
                             L[0] += T[0] * ff.x * V->beta.x * g;
                             L[1] += T[1] * ff.y * V->beta.y * g;
                             L[2] += T[2] * ff.z * V->beta.z * g;
@@ -1103,7 +1139,7 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                         if (occluded_t(b, cr, RB2O_RAY_CONNECTION)) continue;
                         const float* Av = s->albedo + 3 * (size_t)V->mat;
                         double g = cos_c * cos_v / dist2 / (RB2O_PI * RB2O_PI) * ((double)M / (double)n_light_paths) /
-                                   ((double)(V->s + i) * (double)C);
+                                   ((2.0 + (double)cedges + (double)cnsp + V->el) * (double)C);
                         double bv[3] = {V->beta.x, V->beta.y, V->beta.z};
                         for (int c = 0; c < 3; c++) L[c] += T[c] * A[c] * Av[c] * bv[c] * g;
                     }
@@ -1114,7 +1150,7 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                     double pdf;
                     int spec;
                     d3 f = mat_sample(mc, ng, wo, u01(seed, vkey, 3), u01(seed, vkey, 4), u01(seed, vkey, 6), &wn, &pdf,
-                                      &spec);
+                                      &spec, NULL);
                     if (!(pdf > 0.0) || !(f.x > 0.0 || f.y > 0.0 || f.z > 0.0)) break;
                     double k = fabs(ddot(wn, nrm)) / pdf;
                     T[0] *= f.x * k; T[1] *= f.y * k; T[2] *= f.z * k;
@@ -1124,6 +1160,8 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                         if (!(u01(seed, vkey, 5) < q)) break;
                         for (int c = 0; c < 3; c++) T[c] /= q;
                     }
+                    cedges += (cnsp && !spec) ? 1u : 0u;
+                    cnsp = !spec;
                     mkray(ray, pos, eps, wn, 3.402823466e+38);
                     continue;
                 }
@@ -1140,6 +1178,8 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
                     if (!(u01(seed, vkey, 5) < q)) break;
                     for (int c = 0; c < 3; c++) T[c] /= q;
                 }
+                cedges += cnsp ? 1u : 0u;
+                cnsp = 1;
                 mkray(ray, pos, eps, wi, 3.402823466e+38);
             }
             for (int c = 0; c < 3; c++) out_rgb[3 * ci + c] += L[c] / (double)n_iter;

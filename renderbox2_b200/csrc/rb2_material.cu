@@ -92,7 +92,7 @@ int rb2_scene_set_materials(rb2_scene_dev* s, const rb2_material_desc* materials
     if ((e = cudaMemcpy(alb.data(), s->d_albedo, s->n_mat * sizeof(float4), cudaMemcpyDeviceToHost)) != cudaSuccess)
         return cuda_fail(e, "albedo read");
     std::vector<rb2dev::MaterialDev> mats(s->n_mat);
-    bool layered = false, has_delta = false;
+    bool layered = false;
     for (uint32_t m = 0; m < s->n_mat; m++) {
         const rb2_material_desc& d = materials[m];
         rb2dev::MaterialDev& md = mats[m];
@@ -111,8 +111,6 @@ int rb2_scene_set_materials(rb2_scene_dev* s, const rb2_material_desc* materials
         md.flags = (plain ? rb2dev::kMatPlainLambertian : 0u) | (nondelta ? rb2dev::kMatHasNonDelta : 0u);
         if (plain) alb[m] = make_float4(d.layer[0].color[0], d.layer[0].color[1], d.layer[0].color[2], 0.0f);
         layered |= !plain;
-        for (uint32_t i = 0; i < d.n_layers; i++)
-            has_delta |= d.layer[i].type == RB2_BSDF_MIRROR || d.layer[i].type == RB2_BSDF_GLASS;
     }
     rb2dev::MaterialDev* dm = nullptr;
     if ((e = cudaMalloc(&dm, mats.size() * sizeof(rb2dev::MaterialDev))) != cudaSuccess)
@@ -128,7 +126,6 @@ int rb2_scene_set_materials(rb2_scene_dev* s, const rb2_material_desc* materials
     }
     s->d_mats = dm;
     s->layered = layered;
-    s->has_delta = has_delta;
     s->bytes += (uint64_t)s->n_mat * sizeof(rb2dev::MaterialDev);
     return RB2_OK;
 }

@@ -231,11 +231,16 @@ __device__ __forceinline__ float material_pdf(const MaterialDev& m, float3 wo, f
 
 // material_sample_f (core/material.cu:56-211) over all layers.  Returns f and
 // sets wi (world), pdf and whether a specular layer was sampled.
+// eta_io (optional): for a sampled glass layer, the index ratio of wo's side
+// to wi's side (1 for every other sample); light subpaths use it to form the
+// adjoint of the transmission factor.
 __device__ __forceinline__ float3 material_sample(const MaterialDev& m, const Frame& fr, float3 ng, float3 wo_w, float u1,
-                                                  float u2, float uc, float3& wi_w, float& pdf, bool& specular)
+                                                  float u2, float uc, float3& wi_w, float& pdf, bool& specular,
+                                                  float* eta_io = nullptr)
 {
     specular = false;
     pdf = 0.0f;
+    if (eta_io) *eta_io = 1.0f;
     const uint32_t n = m.n_layers;
     if (n == 0) return f3(0.0f, 0.0f, 0.0f);
     const uint32_t which = min((uint32_t)floorf(uc * (float)n), n - 1);
@@ -245,6 +250,10 @@ __device__ __forceinline__ float3 material_sample(const MaterialDev& m, const Fr
     if (pdf == 0.0f) return f3(0.0f, 0.0f, 0.0f);
     wi_w = to_world(fr, wi);
     specular = kind_is_delta(layer_kind(m.layer[which]));
+    if (eta_io && layer_kind(m.layer[which]) == kGlass) {
+        const LayerDev& l = m.layer[which];
+        *eta_io = wo.z > 0.0f ? l.q1.w / l.q2.w : l.q2.w / l.q1.w;
+    }
     if (!specular) {
         for (uint32_t i = 0; i < n; i++)
             if (i != which && !kind_is_delta(layer_kind(m.layer[i]))) pdf += layer_pdf(m.layer[i], wi, wo);

@@ -459,6 +459,24 @@ constexpr uint32_t kMaxConnections = 8;
 constexpr uint64_t kLightSalt = 0xA24BAED4963EE407ull;
 constexpr float kLightRayTmin = 1.0e-4f;
 
+// ---- Strategy counting with specular vertices.  A path of k segments
+// x_1..x_k (x_k on a light) can be sampled by strategy s = 0 (the camera
+// subpath hits the light) and, for each edge (x_j, x_j+1), j = 1..k-1, by the
+// connection across it, which is possible only when neither endpoint scatters
+// specularly on this path (f at a connection vertex is the non-specular part).
+// Every possible strategy is weighted 1 / n_valid, n_valid = 1 + (edges whose
+// endpoints both scatter non-specularly), which is k when no vertex is
+// specular.  A subpath carries the count of valid edges so far and whether its
+// last vertex scattered non-specularly, packed in one word.
+__device__ __forceinline__ uint32_t bd_state(uint32_t nonspec_prev, uint32_t edges) { return nonspec_prev | (edges << 1); }
+__device__ __forceinline__ uint32_t bd_edges(uint32_t st) { return st >> 1; }
+__device__ __forceinline__ uint32_t bd_nonspec(uint32_t st) { return st & 1u; }
+// After a vertex that scattered (non-)specularly.
+__device__ __forceinline__ uint32_t bd_advance(uint32_t st, bool nonspec)
+{
+    return bd_state(nonspec ? 1u : 0u, bd_edges(st) + (bd_nonspec(st) && nonspec ? 1u : 0u));
+}
+
 // Light subpath start (integrators/integrator_bdpt_lvc_sk.cu:61-83): uniform
 // emissive triangle, uniform point, cosine-distributed direction about its
 // normal (one-sided emitter).  Throughput Le cos / (pdf_A pdf_w) = Le NL A pi.
@@ -478,7 +496,9 @@ __global__ void k_bd_light_init(SceneView sc, uint64_t seed, uint64_t key0, uint
         const float3 dir = normalize3(to_world(frame_from_z(ln), cosine_hemisphere(rng_u01(ls, key, 3), rng_u01(ls, key, 4))));
         const float4 Le = sc.emission[lt.w];
         const float k = (float)sc.n_lights * tri_area(l0, l1, l2) * 3.14159265358979f;
-        lbeta[p] = make_float4(Le.x * k, Le.y * k, Le.z * k, 0.0f);
+        // w: strategy bookkeeping (non-specular previous vertex, valid edges so far);
+        // the light point itself is non-specular.
+        lbeta[p] = make_float4(Le.x * k, Le.y * k, Le.z * k, __uint_as_float(bd_state(1u, 0u)));
         lray[2 * (size_t)p] = make_float4(y0.x, y0.y, y0.z, kLightRayTmin);
         lray[2 * (size_t)p + 1] = make_float4(dir.x, dir.y, dir.z, 3.402823466e+38f);
         lq0[p] = p;
@@ -495,9 +515,10 @@ __device__ __forceinline__ const MaterialDev* layered_material(const SceneView& 
 // Light vertex d (1-based surface vertex): store it in the sparse cache slot
 // (path, d) and continue the subpath by BSDF sampling with Russian roulette on
 // the per-bounce factor (integrator_bdpt_lvc_sk.cu:93-166).  On a layered
-// (non-specular) material the continuation samples material_sample_f and the
-// factor is f |cos| / pdf; s_wi (null when every material is one Lambertian
-// layer) keeps the direction toward the previous vertex for the connection's f.
+// material the continuation samples material_sample_f and the factor is
+// f |cos| / pdf (f the adjoint); s_wi (null when every material is one
+// Lambertian layer) keeps the direction toward the previous vertex for the
+// connection's f.
 __global__ void k_bd_light_shade(SceneView sc, uint64_t seed, uint64_t key0, uint32_t d, uint32_t Dl, uint32_t rr_start,
                                  float rr_prob, const uint32_t* q_in, uint32_t* q_out, float4* lray, const int4* lhit,
                                  float4* lbeta, float4* s_pos, float4* s_nrm, float4* s_beta, float4* s_wi,
@@ -526,25 +547,41 @@ __global__ void k_bd_light_shade(SceneView sc, uint64_t seed, uint64_t key0, uin
                     const float3 wo = mul(dd, -1.0f);
                     const float3 nrm = dot3(ng, wo) < 0.0f ? mul(ng, -1.0f) : ng;
                     float4 beta = lbeta[path];
+                    const uint32_t st = __float_as_uint(beta.w);
                     const size_t slot = (size_t)path * Dl + (d - 1);
-                    s_pos[slot] = make_float4(pos.x, pos.y, pos.z, (float)(d + 1));
-                    s_nrm[slot] = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(tri.w));
-                    s_beta[slot] = beta;
-                    s_valid[slot] = 1;
-                    if (s_wi) s_wi[slot] = make_float4(wo.x, wo.y, wo.z, dot3(ng, nrm) < 0.0f ? -1.0f : 1.0f);
                     const MaterialDev* lm = layered_material(sc, tri.w);
+                    // A vertex whose material is purely specular cannot be connected to:
+                    // it is not cached.  The cached w is the light side's valid-edge count
+                    // with this vertex as a (non-specular) connection endpoint.
+                    if (!lm || (lm->flags & kMatHasNonDelta)) {
+                        s_pos[slot] = make_float4(pos.x, pos.y, pos.z, (float)(d + 1));
+                        s_nrm[slot] = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(tri.w));
+                        s_beta[slot] = make_float4(beta.x, beta.y, beta.z, (float)(bd_edges(st) + bd_nonspec(st)));
+                        s_valid[slot] = 1;
+                        if (s_wi) s_wi[slot] = make_float4(wo.x, wo.y, wo.z, dot3(ng, nrm) < 0.0f ? -1.0f : 1.0f);
+                    }
                     if (d < Dl && lm) {
                         const uint64_t key = key0 + path;
                         float3 wi;
-                        float pdf;
+                        float pdf, eta_io;
                         bool spec;
                         const Frame frl = frame_from_z(ng);
                         float3 f = material_sample(*lm, frl, ng, wo, rng_u01(ls, key, 8 + 8 * d),
-                                                   rng_u01(ls, key, 9 + 8 * d), rng_u01(ls, key, 11 + 8 * d), wi, pdf, spec);
+                                                   rng_u01(ls, key, 9 + 8 * d), rng_u01(ls, key, 11 + 8 * d), wi, pdf, spec,
+                                                   &eta_io);
                         if (pdf > 0.0f && (f.x > 0.0f || f.y > 0.0f || f.z > 0.0f)) {
-                            // Light flows from wo toward wi: the adjoint f(wi -> wo), since the
-                            // Blinn shadowing term is not symmetric in its two directions.
-                            f = material_f(*lm, ng, wi, wo, to_local(frl, wi), to_local(frl, wo));
+                            if (!spec) {
+                                // Light flows from wo toward wi: the adjoint f(wi -> wo), since the
+                                // Blinn shadowing term is not symmetric in its two directions.
+                                f = material_f(*lm, ng, wi, wo, to_local(frl, wi), to_local(frl, wo));
+                            } else if (eta_io != 1.0f) {
+                                // Adjoint of the glass transmission: the camera-side factor
+                                // carries (eta of wi / eta of wo)^2, and the refraction maps
+                                // solid angle by (eta_o / eta_i)^2 cos_o / cos_i, so the factor
+                                // seen from the light is the sampled one times eta_io^6.
+                                const float e2 = eta_io * eta_io, e6 = e2 * e2 * e2;
+                                f = f3(f.x * e6, f.y * e6, f.z * e6);
+                            }
                             const float k = fabsf(dot3(wi, ng)) / pdf;
                             const float3 fac = f3(f.x * k, f.y * k, f.z * k);
                             float q = fminf(1.0f, luminance(fac));
@@ -554,6 +591,7 @@ __global__ void k_bd_light_shade(SceneView sc, uint64_t seed, uint64_t key0, uin
                                    rng_u01(ls, key, 10 + 8 * d) < q;
                             if (cont) {
                                 beta.x *= fac.x / q; beta.y *= fac.y / q; beta.z *= fac.z / q;
+                                beta.w = __uint_as_float(bd_advance(st, !spec));
                                 lbeta[path] = beta;
                                 no = make_float4(pos.x, pos.y, pos.z, 1.0e-3f * t);
                                 nd = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
@@ -571,6 +609,7 @@ __global__ void k_bd_light_shade(SceneView sc, uint64_t seed, uint64_t key0, uin
                             cont = q > 0.0f && rng_u01(ls, key, 10 + 8 * d) < q;
                             if (cont) {
                                 beta.x *= A.x / q; beta.y *= A.y / q; beta.z *= A.z / q;
+                                beta.w = __uint_as_float(bd_advance(st, true));
                                 lbeta[path] = beta;
                                 no = make_float4(pos.x, pos.y, pos.z, 1.0e-3f * t);
                                 nd = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
@@ -697,8 +736,8 @@ __global__ void k_lvc_wave_offsets(const uint8_t* valid, uint64_t n_slots, const
 
 // Camera vertex i (1-based): emission (s = 0), next-event estimation (s = 1),
 // connections to cached light vertices (s >= 2), continuation.  Every
-// strategy of a k-segment path is weighted 1/k.  A layered (non-specular)
-// vertex at either end of a strategy takes f from material_f in the frame of
+// strategy of a path is weighted 1/n_valid (the strategy counting above).  A
+// layered vertex at either end of a connection takes f from material_f in the frame of
 // its geometric normal (the path tracer's convention) and continues by
 // material_sample_f; single-Lambertian vertices keep the albedo fast path.
 __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t it0, uint32_t i, uint32_t Kmax,
@@ -740,11 +779,16 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                 const float3 ng = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
                 const float3 wo = mul(d, -1.0f);
                 float4 Tp = T[path];
+                // Valid-edge count of the camera subpath before this vertex, plus the
+                // edge to it when the previous vertex scattered non-specularly (the
+                // camera itself counts as specular: T.w starts at 0).
+                const uint32_t cst = __float_as_uint(Tp.w);
+                const uint32_t cbase = bd_edges(cst) + bd_nonspec(cst);
                 const float4 E = sc.emission[tri.w];
                 if (E.x > 0.0f || E.y > 0.0f || E.z > 0.0f) {
                     if (dot3(ng, wo) > 0.0f) {  // s = 0, k = i
                         float4 Lp = L[path];
-                        const float w = 1.0f / (float)i;
+                        const float w = 1.0f / (float)(1u + cbase);  // s = 0
                         Lp.x += Tp.x * E.x * w; Lp.y += Tp.y * E.y * w; Lp.z += Tp.z * E.z * w;
                         L[path] = Lp;
                     }
@@ -770,14 +814,14 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                         if (mc && cos_l > 0.0f && dist > 0.0f) {
                             const float3 f = material_f(*mc, ng, wo, wi, wo_l, to_local(frc, wi));
                             const float pdf_l = inv_nl * dist2 / (tri_area(l0, l1, l2) * cos_l);
-                            const float k = fabsf(cos_s) / (pdf_l * (float)(i + 1));
+                            const float k = fabsf(cos_s) / (pdf_l * (float)(2u + cbase));
                             scv = make_float4(Tp.x * f.x * Le.x * k, Tp.y * f.y * Le.y * k, Tp.z * f.z * Le.z * k, 0.0f);
                             so = make_float4(pos.x, pos.y, pos.z, eps);
                             sd = make_float4(wi.x, wi.y, wi.z, dist * (1.0f - 1.0e-3f));
                             shadow = scv.x > 0.0f || scv.y > 0.0f || scv.z > 0.0f;
                         } else if (!mc && cos_l > 0.0f && cos_s > 0.0f && dist > 0.0f) {
                             const float pdf_l = inv_nl * dist2 / (tri_area(l0, l1, l2) * cos_l);
-                            const float k = cos_s * kInvPi / (pdf_l * (float)(i + 1));
+                            const float k = cos_s * kInvPi / (pdf_l * (float)(2u + cbase));
                             scv = make_float4(Tp.x * A.x * Le.x * k, Tp.y * A.y * Le.y * k, Tp.z * A.z * Le.z * k, 0.0f);
                             so = make_float4(pos.x, pos.y, pos.z, eps);
                             sd = make_float4(wi.x, wi.y, wi.z, dist * (1.0f - 1.0e-3f));
@@ -816,13 +860,13 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                                     fv = f3(Av.x * kInvPi, Av.y * kInvPi, Av.z * kInvPi);
                                 }
                                 const float g = fabsf(cos_c) * fabsf(cos_v) / dist2 * ((float)M / n_light_paths) /
-                                                ((float)(s + i) * (float)C);
+                                                ((2.0f + (float)cbase + bv.w) * (float)C);
                                 cv = make_float4(Tp.x * fc.x * fv.x * bv.x * g, Tp.y * fc.y * fv.y * bv.y * g,
                                                  Tp.z * fc.z * fv.z * bv.z * g, 0.0f);
                             } else {
                                 if (!(cos_c > 0.0f && cos_v > 0.0f)) continue;
                                 const float g = cos_c * cos_v / dist2 * kInvPi * kInvPi * ((float)M / n_light_paths) /
-                                                ((float)(s + i) * (float)C);
+                                                ((2.0f + (float)cbase + bv.w) * (float)C);
                                 cv = make_float4(Tp.x * A.x * Av.x * bv.x * g, Tp.y * A.y * Av.y * bv.y * g,
                                                  Tp.z * A.z * Av.z * bv.z * g, 0.0f);
                             }
@@ -842,7 +886,8 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                                                          rng_u01(seed, key, vdim(b, kDimBsdfC)), wi, pdf, spec);
                         if (pdf > 0.0f && (f.x > 0.0f || f.y > 0.0f || f.z > 0.0f)) {
                             const float k = fabsf(dot3(wi, ng)) / pdf;
-                            Tp.x *= f.x * k; Tp.y *= f.y * k; Tp.z *= f.z * k; Tp.w = pdf;
+                            Tp.x *= f.x * k; Tp.y *= f.y * k; Tp.z *= f.z * k;
+                            Tp.w = __uint_as_float(bd_advance(cst, !spec));
                             cont = isfinite(Tp.x) && isfinite(Tp.y) && isfinite(Tp.z) &&
                                    (Tp.x > 0.0f || Tp.y > 0.0f || Tp.z > 0.0f);
                             if (cont && b >= rr_start) {
@@ -861,7 +906,8 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
                                                              rng_u01(seed, key, vdim(b, kDimBsdfV)));
                         if (loc.z > 0.0f) {
                             const float3 wi = normalize3(to_world(frame_from_z(nrm), loc));
-                            Tp.x *= A.x; Tp.y *= A.y; Tp.z *= A.z; Tp.w = loc.z * kInvPi;
+                            Tp.x *= A.x; Tp.y *= A.y; Tp.z *= A.z;
+                            Tp.w = __uint_as_float(bd_advance(cst, true));
                             cont = Tp.x > 0.0f || Tp.y > 0.0f || Tp.z > 0.0f;
                             if (cont && b >= rr_start) {
                                 const float q = fminf(rr_prob, luminance(xyz(Tp)));
@@ -1335,9 +1381,6 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
     if (p->max_path_length < 1 || p->max_path_length > 16) return fail(RB2_EINVAL, "max_path_length must be in [1, 16]");
     if (p->connections < 1 || p->connections > rb2dev::kMaxConnections) return fail(RB2_EINVAL, "connections must be in [1, 8]");
-    if (it->scene->has_delta)
-        return fail(RB2_ENOTSUP, "BDPT connects through non-specular materials only (a material has a mirror or glass "
-                                 "layer); use the path tracer for this scene");
     cudaStream_t s = (cudaStream_t)stream;
     const uint64_t npix = (uint64_t)cam->width * cam->height;
     if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");

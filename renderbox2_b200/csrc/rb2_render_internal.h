@@ -22,7 +22,6 @@ struct rb2_scene_dev {
     uint32_t* d_lights = nullptr;  // emissive triangle ids
     rb2dev::MaterialDev* d_mats = nullptr;  // layered materials (null: one Lambertian layer = albedo)
     bool layered = false;                   // some non-emitter material is not a single Lambertian layer
-    bool has_delta = false;                 // some non-emitter material has a mirror or glass layer
     uint32_t nv = 0, ntri = 0, n_mat = 0, n_lights = 0;
     uint64_t bytes = 0;
 };
