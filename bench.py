@@ -1,7 +1,7 @@
 """Benchmark: incoherent ray-query throughput on one B200 (config 4 workload).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl rb2|reference]
-                  [--rays-per-scene R] [--scenes S] [--workload trace|ao|pt|bdpt]
+                  [--rays-per-scene R] [--scenes S] [--workload trace|ao|pt|bdpt|raycast]
 
 One step = every scene's ray batch traced once: 64 heightfield scenes with
 log-uniform 1k..2M triangles, 1M incoherent diffuse-bounce rays per scene,
@@ -377,7 +377,8 @@ def run_workload(args, rank, local_rank):
     r = integrator(args.workload, keep=keep)
     if rank == 0:
         names = {"ao": "config 1: ambient occlusion", "pt": "config 2: wavefront path tracing",
-                 "bdpt": "config 3: BDPT with light-vertex cache"}
+                 "bdpt": "config 3: BDPT with light-vertex cache",
+                 "raycast": "config-2 scene, camera and spp: ray casting (primary rays, primitive-id shading)"}
         line = {"metric": "samples/s and Mrays/s", "workload": names[args.workload], **r}
         if world_of_env() == 1:
             base, counts = integrator_cpu_baseline(args.workload, keep)
@@ -415,6 +416,29 @@ def integrator_cpu_baseline(kind, keep):
         dt = time.perf_counter() - t0
         samples = xy.shape[0] * c["ao_samples"]
         crop = f"full frame {W}x{H}, {c['ao_samples']} AO rays per pixel"
+    elif kind == "raycast":
+        gx, gy = 128, 72
+        sx, sy = W // gx, H // gy
+        spp = c["spp"]
+        ii, jj = np.meshgrid(np.arange(gx) * sx + sx // 2, np.arange(gy) * sy + sy // 2)
+        rng = np.random.Generator(np.random.PCG64(5))
+        base = np.stack([ii.ravel(), jj.ravel()], 1)
+        xy = (np.tile(base, (spp, 1)) + rng.uniform(0, 1, (base.shape[0] * spp, 2))).astype(np.float32)
+        rays = oracle.ref_camera_rays(keep["eye"], keep["lookat"], c["up"], W, H, c["fov"], xy)
+        nodes, woop, tri = bvh.get_node_buffer(), bvh.get_tri_woop_buffer(), bvh.get_tri_index_buffer()
+        t0 = time.perf_counter()
+        hits, cnt = oracle.trace(nodes, woop, tri, rays, counts=True)
+        oracle.raycast_shade(hits["prim"], 0, scene.vertices, scene.indices, scene.material_ids, scene.albedo,
+                             scene.emission)
+        dt = time.perf_counter() - t0
+        oracle.counts_reset(False)
+        samples = base.shape[0] * spp
+        crop = f"{gx}x{gy} pixels on a stride-{sx}x{sy} grid over the {W}x{H} frame at {spp} spp"
+        counts = {"camera": {"rays": int(rays.shape[0]), "nodes": int(cnt["nodes"].sum()),
+                             "tris": int(cnt["tris"].sum()), "leafterms": int(cnt["leafterms"].sum())}}
+        return ({"value": round(samples / dt, 1), "unit": "samples/s", "cores": cores, "kind": "port",
+                 "sample": f"{crop}: {samples:,} samples in {dt:.1f}s, CPU traversal (oracle) and ray-cast "
+                           f"shading, OpenMP over {cores} threads"}, counts)
     else:
         gx, gy = 128, 72
         sx, sy = W // gx, H // gy
@@ -467,6 +491,8 @@ def integrator_roofline(kind, r, counts):
         npix = r["width"] * r["height"]
         hit_frac = counts["shadow"]["rays"] / max(1, counts["camera"]["rays"] * (r["samples"] // npix))
         gpu = {"camera": npix, "shadow": r["samples"] * hit_frac}
+    elif kind == "raycast":
+        gpu = {"camera": st["primary_rays"]}
     else:
         gpu = {"camera": st["primary_rays"], "extension": st["extension_rays"], "shadow": st["shadow_rays"],
                "connection": st["connection_rays"], "light": st["light_rays"]}
@@ -621,7 +647,7 @@ def main():
     ap.add_argument("--e2e-chunk", type=int, default=1 << 20, help="rays per chunk of the pipelined host path")
     ap.add_argument("--e2e-depth", type=int, default=4, help="streams of the pipelined host path")
     ap.add_argument("--serve-jobs", type=int, default=300, help="config-5 jobs in the serving measurement (0: skip)")
-    ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt"], default="trace",
+    ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt", "raycast"], default="trace",
                     help="trace: the headline config-4 line; ao/pt/bdpt: configs 1-3 at full size")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -182,7 +182,7 @@ int rb2_integrator_set_launch(rb2_integrator* it, const rb2_launch_config* cfg);
  * waves mean larger traversal launches (less time in launch tails) and more
  * device memory.  Unfiltered images do not depend on the wave size. */
 int rb2_integrator_set_wave(rb2_integrator* it, uint64_t paths);
-/* Film filter of the path tracer and BDPT (default RB2_FILTER_NONE); NULL resets. */
+/* Film filter of the path tracer, BDPT and ray casting (default RB2_FILTER_NONE); NULL resets. */
 int rb2_integrator_set_filter(rb2_integrator* it, const rb2_filter* f);
 
 /* Ambient occlusion (AmbientOcclusionIntegratorParams, core/params.h:126-131;
@@ -250,6 +250,36 @@ typedef struct {
     uint64_t seed;
 } rb2_bdpt_params;
 int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_params* p, float* d_rgb, void* stream);
+
+/* Ray casting (RayCastIntegratorParams / RayCastShade, core/params.h:139-151;
+ * IntegratorRayCast::compute and kernel_ray_cast_update,
+ * integrators/integrator_raycast.cu:27-113): spp jittered camera samples per
+ * pixel (the path tracer's sample positions for the same seed), one
+ * closest-hit traversal, one colour per sample from its hit:
+ *   PRIMITIVE_ID  the reference's 15-entry palette at (primitive id mod 15);
+ *   MATERIAL_ID   the colour of the hit material's first layer (Lambertian,
+ *                 mirror, glass, microfacet R; the emission of an emitter;
+ *                 black for Oren-Nayar, which the reference does not handle);
+ *   NORMALS       the shading normal, which is the unflipped geometric normal
+ *                 normalize(cross(v1 - v0, v2 - v0)) for these scenes;
+ *   UVS           black (the reference leaves this mode empty);
+ *   UNIFORM       1 on a hit.
+ * Misses are black.  d_rgb[3*pixel] = mean over the samples, or the filtered
+ * value when a film filter is set (rb2_integrator_set_filter). */
+enum {
+    RB2_RAYCAST_SHADE_PRIMITIVE_ID = 0,
+    RB2_RAYCAST_SHADE_MATERIAL_ID = 1,
+    RB2_RAYCAST_SHADE_NORMALS = 2,
+    RB2_RAYCAST_SHADE_UVS = 3,
+    RB2_RAYCAST_SHADE_UNIFORM = 4
+};
+typedef struct {
+    uint32_t spp;
+    uint32_t shade;   /* RB2_RAYCAST_SHADE_* */
+    uint64_t seed;
+} rb2_raycast_params;
+int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_raycast_params* p, float* d_rgb,
+                       void* stream);
 
 /* Statistics of the last render on this integrator (rays traced per kind);
  * trace_ms = GPU time of its traversal launches (CUDA events around each),

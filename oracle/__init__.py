@@ -436,3 +436,91 @@ def bdpt(bvh_buffers, vertices, indices, tri_mat, albedo, emission, lights, cam_
 
 
 C_ = C
+
+
+# ---- ray casting ---------------------------------------------------------------------
+# kernel_ray_cast_update's colour table (integrators/integrator_raycast.cu:49-63).
+RAYCAST_PALETTE = np.array([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0], [0.0, 1.0, 1.0], [1.0, 0.0, 1.0],
+                            [1.0, 1.0, 0.0], [0.1, 0.1, 0.1], [0.5, 0.5, 0.5], [1.0, 1.0, 1.0], [0.0, 0.25, 0.5],
+                            [1.0, 0.5, 0.0], [0.5, 0.25, 0.0], [0.2, 0.9, 1.0], [0.7, 0.3, 0.1],
+                            [0.34, 0.89, 0.45]], np.float32)
+_LAYER_OREN_NAYAR = 1
+
+
+def raycast_shade(prim, mode, vertices, indices, tri_mat, albedo, emission, materials=None):
+    """Colour per camera sample of the reference's ray-cast integrator
+    (kernel_ray_cast_update, integrators/integrator_raycast.cu:37-131) from
+    closest-hit primitive ids (-1 = miss), float32 (n, 3); misses are black:
+
+    mode 0 (:65-71): the palette at prim mod 15;
+    mode 1 (:72-109): the first layer's colour of the hit material (the
+        emission of an emitter; black for Oren-Nayar, which has no branch
+        there), with `materials` a material_descs array or None (one
+        Lambertian layer = albedo per material);
+    mode 2 (:110-116): the shading normal, here the unflipped geometric
+        normal normalize(cross(v1 - v0, v2 - v0)) (float64, rounded);
+    mode 3 (:117-120): black (the branch is empty);
+    mode 4 (:121-124): one on a hit."""
+    prim = np.asarray(prim).astype(np.int64).reshape(-1)
+    hit = prim >= 0
+    out = np.zeros((prim.size, 3), np.float32)
+    p = prim[hit]
+    if mode == 0:
+        out[hit] = RAYCAST_PALETTE[p % 15]
+    elif mode == 1:
+        m = np.asarray(tri_mat, np.int64)[p]
+        em = np.asarray(emission, np.float32).reshape(-1, 3)
+        col = np.asarray(albedo, np.float32).reshape(-1, 3).copy()
+        if materials is not None:
+            arr = materials_array(materials)
+            for k in range(arr.shape[0]):
+                lay = arr[k]["layer"][0]
+                if arr[k]["n_layers"] >= 1:
+                    col[k] = 0.0 if lay["type"] == _LAYER_OREN_NAYAR else lay["color"]
+        emitter = (em > 0).any(axis=1)
+        col[emitter] = em[emitter]
+        out[hit] = col[m]
+    elif mode == 2:
+        v = np.asarray(vertices, np.float64).reshape(-1, 3)
+        t = np.asarray(indices, np.int64).reshape(-1, 3)[p]
+        n = np.cross(v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 0]])
+        out[hit] = (n / np.linalg.norm(n, axis=1, keepdims=True)).astype(np.float32)
+    elif mode == 4:
+        out[hit] = 1.0
+    return out
+
+
+def _splitmix64(z):
+    z = (z + np.uint64(0x9E3779B97F4A7C15)) & np.uint64(0xFFFFFFFFFFFFFFFF)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def keyed_u01_f32(seed, key, dim):
+    """The integrators' keyed draw in [0, 1) as float32 (24 bits), restated so
+    that tests can rebuild the device's sample positions: splitmix64 of
+    (key * 0x100000001B3 + dim), xor seed, splitmix64 again, then the PCG32
+    xorshift-and-rotate output permutation; the top 24 of its 32 bits give the
+    value.  `key` is an integer array."""
+    with np.errstate(over="ignore"):
+        key = np.asarray(key, np.uint64)
+        s = _splitmix64(np.uint64(seed) ^ _splitmix64(key * np.uint64(0x100000001B3) + np.uint64(dim)))
+        xs = (((s >> np.uint64(18)) ^ s) >> np.uint64(27)) & np.uint64(0xFFFFFFFF)
+        rot = s >> np.uint64(59)
+        r = ((xs >> rot) | (xs << ((np.uint64(32) - rot) & np.uint64(31)))) & np.uint64(0xFFFFFFFF)
+    return (r >> np.uint64(8)).astype(np.float32) * np.float32(1.0 / 16777216.0)
+
+
+def jittered_raster(width, height, spp, seed, sample0=0):
+    """Raster positions of the integrators' camera samples, sample-major
+    (index = s * pixels + pixel): x = pixel % width + u(key, 0), y = pixel /
+    width + u(key, 1), key = (sample0 + s) * pixels + pixel, float32 sums."""
+    npix = width * height
+    pix = np.tile(np.arange(npix, dtype=np.uint64), spp)
+    s = np.repeat(np.arange(spp, dtype=np.uint64), npix) + np.uint64(sample0)
+    key = s * np.uint64(npix) + pix
+    jx, jy = keyed_u01_f32(seed, key, 0), keyed_u01_f32(seed, key, 1)
+    x = (pix % np.uint64(width)).astype(np.float32) + jx
+    y = (pix // np.uint64(width)).astype(np.float32) + jy
+    return np.stack([x, y], 1)

@@ -100,6 +100,10 @@ class BdptParams(C.Structure):
                 ("connections", C.c_uint32), ("rr_start", C.c_uint32), ("rr_prob", C.c_float), ("seed", C.c_uint64)]
 
 
+class RayCastParams(C.Structure):
+    _fields_ = [("spp", C.c_uint32), ("shade", C.c_uint32), ("seed", C.c_uint64)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("primary_rays", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("connection_rays", C.c_uint64), ("light_rays", C.c_uint64), ("lvc_vertices", C.c_uint64),
@@ -178,6 +182,7 @@ SIGNATURES = {
     "rb2_integrator_stats": (C.c_int, [P, C.POINTER(RenderStats), P]),
     "rb2_render_ao": (C.c_int, [P, C.POINTER(Camera), C.POINTER(AoParams), P, P]),
     "rb2_render_pt": (C.c_int, [P, C.POINTER(Camera), C.POINTER(PtParams), P, P]),
+    "rb2_render_raycast": (C.c_int, [P, C.POINTER(Camera), C.POINTER(RayCastParams), P, P]),
     "rb2_render_bdpt": (C.c_int, [P, C.POINTER(Camera), C.POINTER(BdptParams), P, P]),
     "rb2_camera_init": (C.c_int, [C.POINTER(Camera), P, P, P, U32, U32, C.c_float]),
     "rb2_camera_rays": (C.c_int, [C.POINTER(Camera), U32, U64, I32, P, P]),

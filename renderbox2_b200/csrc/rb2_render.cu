@@ -454,6 +454,51 @@ __global__ void k_pt_accumulate(const float4* L, uint32_t npix, uint32_t per_pix
     }
 }
 
+// ---- Ray casting (integrators/integrator_raycast.cu:27-113) ---------------------------
+// The reference's palette for primitive ids (its entries, in its order; the
+// names in its comments do not all match the values).
+__constant__ float4 kRayCastPalette[15] = {
+    {1.0f, 0.0f, 0.0f, 0.0f},   {0.0f, 1.0f, 0.0f, 0.0f},  {0.0f, 0.0f, 1.0f, 0.0f}, {0.0f, 1.0f, 1.0f, 0.0f},
+    {1.0f, 0.0f, 1.0f, 0.0f},   {1.0f, 1.0f, 0.0f, 0.0f},  {0.1f, 0.1f, 0.1f, 0.0f}, {0.5f, 0.5f, 0.5f, 0.0f},
+    {1.0f, 1.0f, 1.0f, 0.0f},   {0.0f, 0.25f, 0.5f, 0.0f}, {1.0f, 0.5f, 0.0f, 0.0f}, {0.5f, 0.25f, 0.0f, 0.0f},
+    {0.2f, 0.9f, 1.0f, 0.0f},   {0.7f, 0.3f, 0.1f, 0.0f},  {0.34f, 0.89f, 0.45f, 0.0f}};
+
+// One colour per camera sample from its closest hit (kernel_ray_cast_update):
+// mode is an RB2_RAYCAST_SHADE_* value; misses stay black in every mode.
+__global__ void k_rc_shade(SceneView sc, uint32_t paths, uint32_t mode, const int4* hits, float4* L,
+                           WaveCountersDev* wc)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) wc->stats[0] += paths;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < paths; p += gridDim.x * blockDim.x) {
+        const int h = hits[p].x;
+        float3 c = f3(0.0f, 0.0f, 0.0f);
+        if (h >= 0) {
+            if (mode == RB2_RAYCAST_SHADE_PRIMITIVE_ID) {
+                c = xyz(kRayCastPalette[(uint32_t)h % 15u]);
+            } else if (mode == RB2_RAYCAST_SHADE_MATERIAL_ID) {
+                // First layer's colour; an emitter shows its emission.
+                const uint32_t m = sc.tris[h].w;
+                const float4 E = sc.emission[m];
+                if (E.x > 0.0f || E.y > 0.0f || E.z > 0.0f) {
+                    c = xyz(E);
+                } else if (sc.mats && !(sc.mats[m].flags & kMatPlainLambertian)) {
+                    const LayerDev& l = sc.mats[m].layer[0];
+                    if (layer_kind(l) != kOrenNayar) c = xyz(l.q0);
+                } else {
+                    c = xyz(sc.albedo[m]);
+                }
+            } else if (mode == RB2_RAYCAST_SHADE_NORMALS) {
+                const uint4 tri = sc.tris[h];
+                const float3 v0 = xyz(sc.verts[tri.x]), v1 = xyz(sc.verts[tri.y]), v2 = xyz(sc.verts[tri.z]);
+                c = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
+            } else if (mode == RB2_RAYCAST_SHADE_UNIFORM) {
+                c = f3(1.0f, 1.0f, 1.0f);
+            }
+        }
+        L[p] = make_float4(c.x, c.y, c.z, 0.0f);
+    }
+}
+
 // ---- BDPT with a light-vertex cache -----------------------------------------------
 constexpr uint32_t kMaxConnections = 8;
 constexpr uint64_t kLightSalt = 0xA24BAED4963EE407ull;
@@ -1371,6 +1416,71 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
         rb2dev::k_pt_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp,
                                                                       d_rgb);
     RB2_CUDA(cudaGetLastError(), "PT finalize");
+    return RB2_OK;
+}
+
+int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_raycast_params* p, float* d_rgb,
+                       void* stream)
+{
+    if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
+    it->ev_used = 0;
+    if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
+    if (p->shade > RB2_RAYCAST_SHADE_UNIFORM) return fail(RB2_EINVAL, "shade must be an RB2_RAYCAST_SHADE_* value");
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t npix = (uint64_t)cam->width * cam->height;
+    if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");
+    const uint64_t P = pt_paths_in_flight(npix, p->spp, 0, it->wave_paths ? it->wave_paths : kRenderWavePaths);
+    const uint32_t spw = (uint32_t)(P / npix);
+    PathState& ps = it->ps;
+    int rc;
+    if ((rc = ensure_path_state(ps, P))) return rc;
+    if ((rc = grow(it->d_accum, it->cap_accum, npix))) return rc;
+    const bool filtered = it->filter.kind != RB2_FILTER_NONE;
+    rb2dev::FilmArgs fa{};
+    if (filtered) {
+        if ((rc = grow(it->d_film_xy, it->cap_film_xy, P))) return rc;
+        if ((rc = film_args(it->filter, cam->width, cam->height, fa))) return rc;
+    }
+    if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
+    RB2_CUDA(cudaMemsetAsync(it->d_accum, 0, npix * 16, s), "accumulator reset");
+    RB2_CUDA(cudaMemsetAsync(it->d_wave, 0, sizeof(WaveCounters), s), "counter reset");
+    rb2dev::CamArgs ca;
+    std::memcpy(ca.r2c, cam->raster_to_camera, sizeof(ca.r2c));
+    std::memcpy(ca.c2w, cam->camera_to_world, sizeof(ca.c2w));
+    ca.width = cam->width; ca.height = cam->height; ca.spp = 1; ca.jitter = 1; ca.seed = p->seed;
+    const rb2_scene_dev* sd = it->scene;
+    rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights, sd->d_mats};
+    const DeviceBvhView bv = device_bvh(it->tracer, true);
+    WaveCounters* wc = it->d_wave;
+    const unsigned g = grid_for(P, it->sms);
+    for (uint32_t s0 = 0; s0 < p->spp; s0 += spw) {
+        const uint32_t cur_spw = std::min(spw, p->spp - s0);
+        const uint32_t paths = (uint32_t)(npix * cur_spw);
+        // Camera samples (kernel_generate_perspective_camera_samples), then the
+        // closest-hit trace (CudaTracer::trace with any_hit = false).
+        rb2dev::k_pt_camera<<<g, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, paths, s0, ps.ray, ps.T, ps.L, ps.q[0], wc,
+                                              filtered ? it->d_film_xy : nullptr);
+        RB2_CUDA(cudaGetLastError(), "ray-cast camera");
+        rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, 1u);
+        rb2dev::QueueSource prim{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop), bv.triidx,
+                                 ps.q[0], &wc->n_ext[0], ps.ray, &wc->head_ext, rb2dev::kClosest,
+                                 ps.hit, nullptr, nullptr};
+        if ((rc = launch_persistent(prim, paths, it, bv, s))) return rc;
+        rb2dev::k_rc_shade<<<g, 256, 0, s>>>(sv, paths, p->shade, ps.hit, ps.L, wc);
+        RB2_CUDA(cudaGetLastError(), "ray-cast shade");
+        if (filtered)
+            rb2dev::k_film_gather<<<grid_for(npix, it->sms), 256, 0, s>>>(
+                fa, rb2dev::ArrayPos{it->d_film_xy, (uint32_t)npix}, ps.L, cur_spw, it->d_accum, nullptr);
+        else
+            rb2dev::k_pt_accumulate<<<grid_for(npix, it->sms), 256, 0, s>>>(ps.L, (uint32_t)npix, cur_spw, it->d_accum);
+        RB2_CUDA(cudaGetLastError(), "ray-cast accumulate");
+    }
+    if (filtered)
+        rb2dev::k_film_resolve<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_accum, (uint32_t)npix, d_rgb);
+    else
+        rb2dev::k_pt_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp,
+                                                                      d_rgb);
+    RB2_CUDA(cudaGetLastError(), "ray-cast finalize");
     return RB2_OK;
 }
 

@@ -10,7 +10,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._native import AoParams, BdptParams, DevScene, IsectBuffer, PtParams, RenderStats, check, lib
+from ._native import AoParams, BdptParams, DevScene, IsectBuffer, PtParams, RayCastParams, RenderStats, check, lib
 from ._native import BsdfLayer as _BsdfLayer
 from ._native import Filter as _Filter
 from ._native import MaterialDesc as _MaterialDesc
@@ -233,6 +233,18 @@ class BidirectionalPathIntegratorLvcParams:
     seed: int = 13
 
 
+# RayCastShade (core/params.h:139-146), by the names the reference's integrator
+# file uses (config/configuration.cpp:222-250; "uvs" has no name there).
+RAYCAST_SHADES = {"primitive_id": 0, "material_id": 1, "normals": 2, "uvs": 3, "uniform": 4}
+
+
+@dataclass
+class RayCastIntegratorParams:
+    shade: str = "primitive_id"     # primitive_id | material_id | normals | uvs | uniform
+    spp: int = 1
+    seed: int = 5
+
+
 class Integrator:
     """Binds a tracer and a device scene; owns the wavefront scratch."""
 
@@ -256,7 +268,7 @@ class Integrator:
         check(lib().rb2_integrator_set_timing(self._it, 1 if on else 0))
 
     def set_filter(self, f: "Filter | None"):
-        """Film filter of render_pt / render_bdpt (None: per-pixel mean)."""
+        """Film filter of render_pt / render_bdpt / render_raycast (None: per-pixel mean)."""
         if f is None:
             check(lib().rb2_integrator_set_filter(self._it, None))
         else:
@@ -296,6 +308,17 @@ class Integrator:
         p = BdptParams(params.spp, params.max_path_length, params.num_light_paths, params.connections,
                        params.rr_start, params.rr_prob, params.seed)
         check(lib().rb2_render_bdpt(self._it, C.byref(camera.c), C.byref(p), _ptr(out), _stream_handle(stream)))
+        return out
+
+    def render_raycast(self, camera, params: RayCastIntegratorParams, out=None, stream=None):
+        """IntegratorRayCast::render: (w*h, 3) colours, mean over params.spp samples."""
+        import torch
+        n = camera.width * camera.height
+        if out is None:
+            out = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+        shade = RAYCAST_SHADES[params.shade] if isinstance(params.shade, str) else int(params.shade)
+        p = RayCastParams(params.spp, shade, params.seed)
+        check(lib().rb2_render_raycast(self._it, C.byref(camera.c), C.byref(p), _ptr(out), _stream_handle(stream)))
         return out
 
     def stats(self, stream=None) -> dict:

@@ -24,6 +24,8 @@ def _event_ms(fn, stream, reps=1):
 
 def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order: int | None = None):
     """Config 1 (AO), 2 (PT) or 3 (BDPT) at full size: samples/s and Mrays/s.
+    "raycast": the config-2 scene, camera and spp through the ray-cast
+    integrator (primary rays only, primitive-id shading).
     `keep` (optional dict) receives the scene, BVH and config used.  The
     traversal layout is `node_order`, or (None) the faster of the binary BFS
     and the compressed 8-wide layout on one timed frame each."""
@@ -32,14 +34,14 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
     import renderbox2_b200 as rb
     from renderbox2_b200 import configs
     from renderbox2_b200.render import (AmbientOcclusionIntegratorParams, BidirectionalPathIntegratorLvcParams,
-                                        DeviceScene, Integrator, PathIntegratorParams)
+                                        DeviceScene, Integrator, PathIntegratorParams, RayCastIntegratorParams)
     t0 = time.time()
     if kind == "ao":
         c = configs.CONFIG1
         scene = rb.heightfield_scene(seed=c["seed"], grid_n=c["grid_n"], amplitude=c["amplitude"],
                                      n_boxes=c["n_boxes"], box_min=c["box_min"], box_max=c["box_max"])
     else:
-        c = configs.CONFIG2 if kind == "pt" else configs.CONFIG3
+        c = configs.CONFIG2 if kind in ("pt", "raycast") else configs.CONFIG3
         scene = rb.RoomScene(seed=c["seed"], n_boxes=c["n_boxes"], n_spheres=c["n_spheres"],
                              sphere_subdiv=c["sphere_subdiv"], rmin=c["rmin"], rmax=c["rmax"],
                              n_lights=c["n_lights"], emission=c["emission"], room_size=c["room_size"])
@@ -65,6 +67,11 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
                                      rr_prob=c["rr_prob"], seed=1)
             out = torch.empty((npix, 3), dtype=torch.float32, device="cuda")
             run = lambda: it.render_pt(cam, p, out=out, stream=stream)  # noqa: E731
+            samples = npix * c["spp"]
+        elif kind == "raycast":
+            p = RayCastIntegratorParams("primitive_id", spp=c["spp"], seed=1)
+            out = torch.empty((npix, 3), dtype=torch.float32, device="cuda")
+            run = lambda: it.render_raycast(cam, p, out=out, stream=stream)  # noqa: E731
             samples = npix * c["spp"]
         else:
             p = BidirectionalPathIntegratorLvcParams(spp=c["spp"], max_path_length=c["max_path_length"],

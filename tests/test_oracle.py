@@ -227,3 +227,39 @@ def test_material_functions_match_reference_bsdfs(orc):
         keep = ok & ~quirk
         np.testing.assert_allclose(ours[keep], ref[keep], rtol=2e-3, atol=2e-5, err_msg=f"sample, material {k}")
         assert (ours[quirk, 3:6] == 0).all()
+
+
+def test_raycast_shade_rules(orc):
+    """The restatement of kernel_ray_cast_update (integrators/integrator_raycast.cu:
+    65-124): misses black in every mode, the palette wraps at 15, the uv mode
+    is empty, a material's colour is its first layer's (the emission for an
+    emitter, black for Oren-Nayar), normals are unit geometric normals."""
+    from renderbox2_b200.render import BsdfLayer as B, material_descs
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 1], [2, 0, 1]], np.float32)
+    idx = np.array([[0, 1, 2], [0, 2, 3], [3, 4, 5], [1, 4, 5]], np.uint32)
+    tri_mat = np.array([0, 1, 2, 3], np.uint32)
+    albedo = np.array([[0.1, 0.2, 0.3], [0.4, 0.5, 0.6], [0.7, 0.8, 0.9], [0.2, 0.2, 0.2]], np.float32)
+    emission = np.zeros((4, 3), np.float32)
+    emission[3] = (5.0, 6.0, 7.0)
+    mats = material_descs([[B("lambertian", (0.1, 0.2, 0.3))], [B("orennayar", (0.5, 0.5, 0.5), sigma_deg=20.0)],
+                           [B("mirror", (0.9, 0.8, 0.7)), B("lambertian", (0.3, 0.3, 0.3))], []])
+    prim = np.array([-1, 0, 1, 2, 3], np.int64)
+    args = (v, idx, tri_mat, albedo, emission)
+    for mode in range(5):
+        assert not orc.raycast_shade(prim[:1], mode, *args, mats).any()
+    # The palette mode reads no geometry: ids past the triangle count only index the palette.
+    ids = np.array([0, 14, 15, 16, 29, 30])
+    assert np.array_equal(orc.raycast_shade(ids, 0, *args), orc.RAYCAST_PALETTE[[0, 14, 0, 1, 14, 0]])
+    assert not orc.raycast_shade(prim, 3, *args, mats).any()
+    mat = orc.raycast_shade(np.array([0, 1, 2, 3]), 1, *args, mats)
+    np.testing.assert_array_equal(mat, np.array([[0.1, 0.2, 0.3], [0, 0, 0], [0.9, 0.8, 0.7], [5, 6, 7]], np.float32))
+    plain = orc.raycast_shade(np.array([0, 1, 2]), 1, *args)
+    np.testing.assert_array_equal(plain, albedo[:3])
+    nrm = orc.raycast_shade(np.array([0, 1, 2, 3]), 2, *args)
+    np.testing.assert_allclose(np.linalg.norm(nrm, axis=1), 1.0, rtol=1e-6)
+    np.testing.assert_allclose(nrm[0], (0, 0, 1))
+    assert np.array_equal(orc.raycast_shade(np.array([-1, 2]), 4, *args), np.array([[0, 0, 0], [1, 1, 1]], np.float32))
+    # The sample positions stay inside their pixels and are sample-major.
+    xy = orc.jittered_raster(7, 3, 2, 11)
+    base = np.tile(np.stack([np.arange(21) % 7, np.arange(21) // 7], 1), (2, 1))
+    assert ((xy - base >= 0) & (xy - base < 1)).all()
