@@ -646,7 +646,8 @@ def main():
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--e2e-chunk", type=int, default=1 << 20, help="rays per chunk of the pipelined host path")
     ap.add_argument("--e2e-depth", type=int, default=4, help="streams of the pipelined host path")
-    ap.add_argument("--serve-jobs", type=int, default=300, help="config-5 jobs in the serving measurement (0: skip)")
+    ap.add_argument("--serve-jobs", type=int, default=10000,
+                    help="config-5 jobs in the serving measurement (0: skip)")
     ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt", "raycast"], default="trace",
                     help="trace: the headline config-4 line; ao/pt/bdpt: configs 1-3 at full size")
     args = ap.parse_args()

@@ -129,12 +129,64 @@ class Server:
         return [res[i] for i in range(n)], {k: getattr(st, k) for k, _ in ServerStats._fields_}
 
 
-class JobList:
-    """Jobs plus the pinned host buffers they read and write."""
+class SharedBuffers:
+    """Pinned host memory shared by the jobs of a long run, so that thousands
+    of jobs need neither per-job inputs nor per-job outputs: per pool BVH one
+    set of `rays_per_bvh` incoherent surface rays, which ray jobs read slices
+    of, and a circular output arena that jobs take their output bytes from in
+    issue order.  Output bytes are handed out again only after `arena_bytes`
+    of later jobs' outputs, so as long as the jobs in flight at once write far
+    less than the arena, no two running jobs share bytes; a later job
+    overwrites an earlier one's output, so such runs are for timing."""
 
-    def __init__(self):
+    def __init__(self, pool: Pool, rays_per_bvh: int = 4 << 20, arena_bytes: int = 4 << 30, seed: int = 17):
+        import torch
+        self.rays_per_bvh = int(rays_per_bvh)
+        self.rays = [torch.from_numpy(surface_rays(sc, seed=seed + k, n=self.rays_per_bvh)[0]).pin_memory()
+                     for k, sc in enumerate(pool.scenes)]
+        self.arena = torch.empty(int(arena_bytes), dtype=torch.uint8).pin_memory()
+        self._pos = 0
+
+    def take(self, nbytes: int) -> int:
+        nbytes = (int(nbytes) + 255) & ~255
+        if nbytes > self.arena.numel():
+            raise ValueError("output larger than the arena")
+        if self._pos + nbytes > self.arena.numel():
+            self._pos = 0
+        ptr = self.arena.data_ptr() + self._pos
+        self._pos += nbytes
+        return ptr
+
+
+def _out_bytes(j) -> int:
+    if j.kind == 1:
+        return j.tile * j.tile * 12
+    return j.n_rays * (1 if j.mode == 2 else 16)
+
+
+class JobList:
+    """Jobs plus the pinned host buffers they read and write (their own, or
+    slices of a SharedBuffers)."""
+
+    def __init__(self, shared: SharedBuffers | None = None):
         self.jobs, self.inputs, self.outputs = [], [], []
+        self.shared = shared
         self._arr = None
+
+    def add_rays_shared(self, bvh: int, offset: int, n: int, mode: int, arrival: float = 0.0):
+        """A ray job reading rays [offset, offset + n) of the shared set of `bvh`."""
+        sh = self.shared
+        if offset < 0 or offset + n > sh.rays_per_bvh:
+            raise ValueError("slice outside the shared ray set")
+        j = Job()
+        j.kind, j.bvh, j.arrival_s, j.n_rays, j.mode = 0, bvh, arrival, n, mode
+        j.h_rays = sh.rays[bvh].data_ptr() + 32 * offset
+        j.h_out = sh.take(_out_bytes(j))
+        self.jobs.append(j)
+        self.inputs.append(None)
+        self.outputs.append(None)
+        self._arr = None
+        return len(self.jobs) - 1
 
     def add_rays(self, bvh: int, rays: np.ndarray, mode: int, arrival: float = 0.0):
         import torch
@@ -153,12 +205,16 @@ class JobList:
     def add_tile(self, bvh: int, tile: int, spp: int, seed: int, eye, lookat, up=(0.0, 1.0, 0.0), fov=60.0,
                  max_depth=8, rr_start=3, rr_prob=0.95, arrival: float = 0.0):
         import torch
-        out = torch.empty((tile * tile, 3), dtype=torch.float32).pin_memory()
         j = Job()
         j.kind, j.bvh, j.arrival_s, j.tile, j.spp = 1, bvh, arrival, tile, spp
         j.max_depth, j.rr_start, j.rr_prob, j.seed, j.fov_deg = max_depth, rr_start, rr_prob, seed, fov
         j.eye[:], j.lookat[:], j.up[:] = list(eye), list(lookat), list(up)
-        j.h_out = out.data_ptr()
+        if self.shared is not None:
+            out = None
+            j.h_out = self.shared.take(_out_bytes(j))
+        else:
+            out = torch.empty((tile * tile, 3), dtype=torch.float32).pin_memory()
+            j.h_out = out.data_ptr()
         self.jobs.append(j)
         self.inputs.append(None)
         self.outputs.append(out)
@@ -168,12 +224,16 @@ class JobList:
     def subset(self, idx, arrival: float = 0.0) -> "JobList":
         """A job list sharing inputs with this one, with fresh outputs."""
         import torch
-        out = JobList()
+        out = JobList(self.shared)
         for i in idx:
             j = Job.from_buffer_copy(self.jobs[i])
             j.arrival_s = arrival
-            o = torch.empty_like(self.outputs[i]).pin_memory()
-            j.h_out = o.data_ptr()
+            if self.outputs[i] is None:
+                o = None
+                j.h_out = self.shared.take(_out_bytes(j))
+            else:
+                o = torch.empty_like(self.outputs[i]).pin_memory()
+                j.h_out = o.data_ptr()
             out.jobs.append(j)
             out.inputs.append(self.inputs[i])
             out.outputs.append(o)
@@ -196,12 +256,18 @@ class JobList:
 
 
 def config5_jobs(pool: Pool, n_jobs: int, seed: int = 5, tile_fraction=0.7, tile_min=64, tile_max=1024,
-                 spp_choices=(1, 4, 16, 64), rays_min=64 * 1024, rays_max=4 * 1024 * 1024) -> JobList:
+                 spp_choices=(1, 4, 16, 64), rays_min=64 * 1024, rays_max=4 * 1024 * 1024,
+                 shared: SharedBuffers | None = None) -> JobList:
     """The config-5 mix: tile renders (square side uniform in [tile_min,
     tile_max], spp from spp_choices, depth 8) and incoherent ray batches
-    (log-uniform size, half closest-hit, half occlusion)."""
+    (log-uniform size, half closest-hit, half occlusion).  With `shared`, ray
+    jobs read a slice of their BVH's shared ray set (the draw that seeds a
+    job's own rays otherwise picks the slice) and outputs come from its arena:
+    the same jobs, sizes and BVHs without per-job host buffers."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    jl = JobList()
+    jl = JobList(shared)
+    if shared is not None and rays_max > shared.rays_per_bvh:
+        raise ValueError("rays_max exceeds the shared ray sets")
     for k in range(n_jobs):
         b = int(rng.integers(0, len(pool.tracers)))
         if rng.uniform() < tile_fraction:
@@ -212,8 +278,12 @@ def config5_jobs(pool: Pool, n_jobs: int, seed: int = 5, tile_fraction=0.7, tile
                         lookat=(-ex, 0.0, ez), fov=60.0)
         else:
             n = int(np.exp(rng.uniform(np.log(rays_min), np.log(rays_max))))
-            rays, _ = surface_rays(pool.scenes[b], seed=int(rng.integers(1 << 31)), n=n)
-            jl.add_rays(b, rays, mode=0 if rng.uniform() < 0.5 else 2)
+            draw = int(rng.integers(1 << 31))
+            if shared is not None:
+                jl.add_rays_shared(b, draw % (shared.rays_per_bvh - n + 1), n, mode=0 if rng.uniform() < 0.5 else 2)
+            else:
+                rays, _ = surface_rays(pool.scenes[b], seed=draw, n=n)
+                jl.add_rays(b, rays, mode=0 if rng.uniform() < 0.5 else 2)
     return jl
 
 

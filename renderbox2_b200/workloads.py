@@ -108,34 +108,43 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
             "layout_probe_ms": {str(k): round(v, 3) for k, v in probe.items()}}
 
 
-def serving(n_jobs: int = 300, n_bvh: int = 32, seed: int = 5, slots: int = 8):
-    """Config 5, scaled to n_jobs: pool of n_bvh lit heightfields (1k..4M
-    triangles, log-uniform), 70 % tile renders / 30 % ray batches.  The
-    arrival rate is the throughput of the plain path (one job at a time)
-    on a burst of the same jobs, i.e. the rate that saturates it; both paths
-    then serve the same Poisson arrival sequence.  `capacity` compares both
-    paths on the burst itself (every job queued at t = 0)."""
+def serving(n_jobs: int = 10000, n_bvh: int = 32, seed: int = 5, slots: int = 8, burst_jobs: int = 2000,
+            shared: bool | None = None):
+    """Config 5: pool of n_bvh lit heightfields (1k..4M triangles,
+    log-uniform), n_jobs jobs, 70 % tile renders / 30 % ray batches.  The
+    arrival rate is the throughput of the plain path (one job at a time) on a
+    burst of the first `burst_jobs` jobs, i.e. the rate that saturates it;
+    both paths then serve the same Poisson arrival sequence of all n_jobs.
+    `capacity` compares both paths on that burst (every job queued at t = 0).
+    `shared` (default: more than 1000 jobs) takes ray-job inputs from one
+    pinned ray set per BVH and outputs from a circular pinned arena
+    (serve.SharedBuffers) instead of per-job host buffers."""
     from renderbox2_b200 import configs
-    from renderbox2_b200.serve import Server, build_pool, config5_jobs, pool_triangle_counts, poisson_arrivals
+    from renderbox2_b200.serve import (Server, SharedBuffers, build_pool, config5_jobs, pool_triangle_counts,
+                                       poisson_arrivals)
     c = configs.CONFIG5
     t0 = time.time()
     counts = pool_triangle_counts(n_bvh, c["tri_min"], c["tri_max"], seed)
     pool = build_pool(counts, seed=seed)
-    jobs = config5_jobs(pool, n_jobs, seed=seed)
+    use_shared = n_jobs > 1000 if shared is None else shared
+    sh = SharedBuffers(pool, rays_per_bvh=c["rays_max"]) if use_shared else None
+    jobs = config5_jobs(pool, n_jobs, seed=seed, shared=sh)
     setup_s = time.time() - t0
     cont = Server(pool, slots=slots, fifo=False)
     plain = Server(pool, fifo=True)
     # warm-up: a few jobs through both
     cont.run(jobs.subset(range(min(8, n_jobs))))
     plain.run(jobs.subset(range(min(8, n_jobs))))
-    _, burst = plain.run(jobs.subset(range(n_jobs)))
-    _, cburst = cont.run(jobs.subset(range(n_jobs)))
-    rate = n_jobs / burst["wall_s"]
+    nb = min(burst_jobs, n_jobs)
+    _, burst = plain.run(jobs.subset(range(nb)))
+    _, cburst = cont.run(jobs.subset(range(nb)))
+    rate = nb / burst["wall_s"]
     arr = poisson_arrivals(n_jobs, rate, seed=seed + 1)
     _, s_plain = plain.run(jobs.with_arrivals(arr))
     _, s_cont = cont.run(jobs.with_arrivals(arr))
     keep = ("p50_s", "p99_s", "mean_s", "mrays_per_s", "wall_s", "max_concurrent")
-    return {"jobs": n_jobs, "bvhs": n_bvh, "pool_triangles": int(sum(counts)),
+    return {"jobs": n_jobs, "burst_jobs": nb, "host_buffers": "shared ray sets + output arena" if use_shared
+            else "per job", "bvhs": n_bvh, "pool_triangles": int(sum(counts)),
             "arrival_rate_jobs_per_s": round(rate, 2), "setup_s": round(setup_s, 1),
             "resident_gb": round(s_cont["resident_bytes"] / 1e9, 2),
             "continuous": {k: round(s_cont[k], 5) for k in keep},

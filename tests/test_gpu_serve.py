@@ -92,3 +92,42 @@ def test_admission_by_hbm_footprint(pool, cuda):
     res2, st2 = srv.run(jobs.with_arrivals(arr))
     assert all(r.latency_s > 0 and r.admit_s >= a - 1e-6 for r, a in zip(res2, arr))
     assert st2["p99_s"] >= st2["p50_s"] > 0
+
+
+def test_shared_buffer_jobs_equal_direct_traces(pool, cuda):
+    """config5_jobs over serve.SharedBuffers (the host buffers of the long
+    serving runs): ray jobs read slices of one pinned ray set per BVH and every
+    job writes into the circular output arena.  In a run too short to wrap the
+    arena, each ray job's output equals a direct trace of its slice, and the
+    continuous and the one-at-a-time servers write identical outputs."""
+    from renderbox2_b200.serve import Server, SharedBuffers, _out_bytes, config5_jobs
+    torch = cuda
+    sh = SharedBuffers(pool, rays_per_bvh=256 * 1024, arena_bytes=1 << 30, seed=23)
+    n = 24
+    jobs = config5_jobs(pool, n, seed=11, tile_min=32, tile_max=96, spp_choices=(1, 2), rays_min=16 * 1024,
+                        rays_max=256 * 1024, shared=sh)
+    a, b = jobs.subset(range(n)), jobs.subset(range(n))
+    assert 3 * sum(_out_bytes(j) + 256 for j in jobs.jobs) < sh.arena.numel()   # no wrap in this test
+    base = sh.arena.data_ptr()
+
+    def out(jl, i):
+        j = jl.jobs[i]
+        o = j.h_out - base
+        return sh.arena[o:o + _out_bytes(j)].clone()
+
+    ra, _ = Server(pool, slots=4, max_tile=128, max_rays=256 * 1024).run(a)
+    rf, sf = Server(pool, fifo=True, max_tile=128, max_rays=256 * 1024).run(b)
+    assert all(r.status == 0 for r in ra) and all(r.status == 0 for r in rf)
+    assert sf["max_concurrent"] == 1
+    n_ray = 0
+    for i, j in enumerate(a.jobs):
+        assert torch.equal(out(a, i), out(b, i)), f"job {i} differs between the servers"
+        if j.kind == 0:
+            n_ray += 1
+            off = (j.h_rays - sh.rays[j.bvh].data_ptr()) // 32
+            d = sh.rays[j.bvh][off:off + j.n_rays].cuda()
+            if j.mode == 0:
+                assert torch.equal(out(a, i).view(torch.int32).view(-1, 4), pool.tracers[j.bvh].trace(d).cpu())
+            else:
+                assert torch.equal(out(a, i), pool.tracers[j.bvh].trace_occlusion(d).cpu())
+    assert 0 < n_ray < n
