@@ -224,8 +224,8 @@ __global__ void k_pt_camera(CamArgs cam, uint64_t seed, uint32_t npix, uint32_t 
         if (xy_out) xy_out[p] = make_float2(sx, sy);
         rays[2 * (size_t)p] = o;
         rays[2 * (size_t)p + 1] = d;
-        T[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-        L[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (T) T[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);  // null: no path state (ray casting)
+        if (L) L[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         q0[p] = p;
     }
 }
@@ -463,39 +463,61 @@ __constant__ float4 kRayCastPalette[15] = {
     {1.0f, 1.0f, 1.0f, 0.0f},   {0.0f, 0.25f, 0.5f, 0.0f}, {1.0f, 0.5f, 0.0f, 0.0f}, {0.5f, 0.25f, 0.0f, 0.0f},
     {0.2f, 0.9f, 1.0f, 0.0f},   {0.7f, 0.3f, 0.1f, 0.0f},  {0.34f, 0.89f, 0.45f, 0.0f}};
 
-// One colour per camera sample from its closest hit (kernel_ray_cast_update):
+// The colour of one camera sample from its closest hit (kernel_ray_cast_update):
 // mode is an RB2_RAYCAST_SHADE_* value; misses stay black in every mode.
+__device__ __forceinline__ float3 rc_colour(const SceneView& sc, int h, uint32_t mode)
+{
+    float3 c = f3(0.0f, 0.0f, 0.0f);
+    if (h < 0) return c;
+    if (mode == RB2_RAYCAST_SHADE_PRIMITIVE_ID) {
+        c = xyz(kRayCastPalette[(uint32_t)h % 15u]);
+    } else if (mode == RB2_RAYCAST_SHADE_MATERIAL_ID) {
+        // First layer's colour; an emitter shows its emission.
+        const uint32_t m = sc.tris[h].w;
+        const float4 E = sc.emission[m];
+        if (E.x > 0.0f || E.y > 0.0f || E.z > 0.0f) {
+            c = xyz(E);
+        } else if (sc.mats && !(sc.mats[m].flags & kMatPlainLambertian)) {
+            const LayerDev& l = sc.mats[m].layer[0];
+            if (layer_kind(l) != kOrenNayar) c = xyz(l.q0);
+        } else {
+            c = xyz(sc.albedo[m]);
+        }
+    } else if (mode == RB2_RAYCAST_SHADE_NORMALS) {
+        const uint4 tri = sc.tris[h];
+        const float3 v0 = xyz(sc.verts[tri.x]), v1 = xyz(sc.verts[tri.y]), v2 = xyz(sc.verts[tri.z]);
+        c = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
+    } else if (mode == RB2_RAYCAST_SHADE_UNIFORM) {
+        c = f3(1.0f, 1.0f, 1.0f);
+    }
+    return c;
+}
+
+// Per-sample colours into L (the film gather reads them with the sample positions).
 __global__ void k_rc_shade(SceneView sc, uint32_t paths, uint32_t mode, const int4* hits, float4* L,
                            WaveCountersDev* wc)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) wc->stats[0] += paths;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < paths; p += gridDim.x * blockDim.x) {
-        const int h = hits[p].x;
-        float3 c = f3(0.0f, 0.0f, 0.0f);
-        if (h >= 0) {
-            if (mode == RB2_RAYCAST_SHADE_PRIMITIVE_ID) {
-                c = xyz(kRayCastPalette[(uint32_t)h % 15u]);
-            } else if (mode == RB2_RAYCAST_SHADE_MATERIAL_ID) {
-                // First layer's colour; an emitter shows its emission.
-                const uint32_t m = sc.tris[h].w;
-                const float4 E = sc.emission[m];
-                if (E.x > 0.0f || E.y > 0.0f || E.z > 0.0f) {
-                    c = xyz(E);
-                } else if (sc.mats && !(sc.mats[m].flags & kMatPlainLambertian)) {
-                    const LayerDev& l = sc.mats[m].layer[0];
-                    if (layer_kind(l) != kOrenNayar) c = xyz(l.q0);
-                } else {
-                    c = xyz(sc.albedo[m]);
-                }
-            } else if (mode == RB2_RAYCAST_SHADE_NORMALS) {
-                const uint4 tri = sc.tris[h];
-                const float3 v0 = xyz(sc.verts[tri.x]), v1 = xyz(sc.verts[tri.y]), v2 = xyz(sc.verts[tri.z]);
-                c = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
-            } else if (mode == RB2_RAYCAST_SHADE_UNIFORM) {
-                c = f3(1.0f, 1.0f, 1.0f);
-            }
-        }
+        const float3 c = rc_colour(sc, hits[p].x, mode);
         L[p] = make_float4(c.x, c.y, c.z, 0.0f);
+    }
+}
+
+// Unfiltered: shade a pixel's samples of the wave in sample order and add them
+// to its accumulator (the sums k_rc_shade + k_pt_accumulate form, without the
+// per-sample colour buffer).
+__global__ void k_rc_shade_accumulate(SceneView sc, uint32_t npix, uint32_t per_pixel, uint32_t mode,
+                                      const int4* hits, float4* accum, WaveCountersDev* wc)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) wc->stats[0] += (unsigned long long)npix * per_pixel;
+    for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < npix; pix += gridDim.x * blockDim.x) {
+        float4 a = accum[pix];
+        for (uint32_t j = 0; j < per_pixel; j++) {
+            const float3 c = rc_colour(sc, hits[(size_t)j * npix + pix].x, mode);
+            a.x += c.x; a.y += c.y; a.z += c.z;
+        }
+        accum[pix] = a;
     }
 }
 
@@ -1458,22 +1480,23 @@ int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_rayc
         const uint32_t paths = (uint32_t)(npix * cur_spw);
         // Camera samples (kernel_generate_perspective_camera_samples), then the
         // closest-hit trace (CudaTracer::trace with any_hit = false).
-        rb2dev::k_pt_camera<<<g, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, paths, s0, ps.ray, ps.T, ps.L, ps.q[0], wc,
-                                              filtered ? it->d_film_xy : nullptr);
+        rb2dev::k_pt_camera<<<g, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, paths, s0, ps.ray, nullptr, nullptr, ps.q[0],
+                                              wc, filtered ? it->d_film_xy : nullptr);
         RB2_CUDA(cudaGetLastError(), "ray-cast camera");
         rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, 1u);
         rb2dev::QueueSource prim{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop), bv.triidx,
                                  ps.q[0], &wc->n_ext[0], ps.ray, &wc->head_ext, rb2dev::kClosest,
                                  ps.hit, nullptr, nullptr};
         if ((rc = launch_persistent(prim, paths, it, bv, s))) return rc;
-        rb2dev::k_rc_shade<<<g, 256, 0, s>>>(sv, paths, p->shade, ps.hit, ps.L, wc);
-        RB2_CUDA(cudaGetLastError(), "ray-cast shade");
-        if (filtered)
+        if (filtered) {
+            rb2dev::k_rc_shade<<<g, 256, 0, s>>>(sv, paths, p->shade, ps.hit, ps.L, wc);
             rb2dev::k_film_gather<<<grid_for(npix, it->sms), 256, 0, s>>>(
                 fa, rb2dev::ArrayPos{it->d_film_xy, (uint32_t)npix}, ps.L, cur_spw, it->d_accum, nullptr);
-        else
-            rb2dev::k_pt_accumulate<<<grid_for(npix, it->sms), 256, 0, s>>>(ps.L, (uint32_t)npix, cur_spw, it->d_accum);
-        RB2_CUDA(cudaGetLastError(), "ray-cast accumulate");
+        } else {
+            rb2dev::k_rc_shade_accumulate<<<grid_for(npix, it->sms), 256, 0, s>>>(sv, (uint32_t)npix, cur_spw, p->shade,
+                                                                                 ps.hit, it->d_accum, wc);
+        }
+        RB2_CUDA(cudaGetLastError(), "ray-cast shade");
     }
     if (filtered)
         rb2dev::k_film_resolve<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_accum, (uint32_t)npix, d_rgb);
