@@ -240,6 +240,19 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
  * symmetric, and a glass transmission sampled on a light subpath takes the
  * adjoint factor (eta of the outgoing side / eta of the incoming side)^6 times
  * the camera-side factor.  d_rgb[3*pixel] = mean radiance over spp iterations. */
+/* The reference's BidirectionalPathIntegratorLvcParams (core/params.h:108-120)
+ * map as follows: m_num_light_paths -> num_light_paths;
+ * m_num_cam_path_connections (sample_N) -> connections; m_cam_path_rrstart and
+ * m_light_path_rrstart -> rr_start, one value for both subpaths (the
+ * reference's own integrator file gives both the same value);
+ * m_cam_path_rrprob -> rr_prob; m_num_cam_path_max_depth and
+ * m_num_light_path_max_depth -> max_path_length, one cap on the whole path
+ * (light subpaths keep at most max_path_length - 2 surface vertices).  No
+ * field replaces m_num_prep_paths: the cache is sized exactly by a prefix scan,
+ * so no preparation pass runs.  m_num_cam_path_sample_connections (sample_M)
+ * is read by the reference's configuration code but used by none of its
+ * kernels.  m_mode (sk, mk, sort) has no counterpart: the three reference
+ * kernels compute one estimator, which this wavefront implementation runs. */
 typedef struct {
     uint32_t spp;
     uint32_t max_path_length;   /* segments, camera to light (config 3: 6) */
