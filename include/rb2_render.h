@@ -206,7 +206,9 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
  * balance heuristic, Russian roulette from bounce rr_start with continue
  * probability min(rr_prob, luminance(throughput)) and division by it.
  * Vertices 0..max_depth get NEE; extension rays are traced from vertices
- * below max_depth.  d_rgb[3*pixel] = mean radiance over spp jittered samples. */
+ * below max_depth.  d_rgb[3*pixel] = mean radiance over spp jittered samples.
+ * The reference's m_use_max_depth has no counterpart: its configuration code
+ * reads it and none of its kernels use it, so max_depth always applies. */
 typedef struct {
     uint32_t spp;
     uint32_t max_depth;
