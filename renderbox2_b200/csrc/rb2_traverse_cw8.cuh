@@ -87,6 +87,7 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
     L.hitIndex = -1;
     uint32_t ng_base = 0, ng_bits = 0, tg_base = 0, tg_bits = 0, tg_mask = 0;
     uint32_t tg2_base = 0, tg2_bits = 0, tg2_mask = 0;  // a second pending triangle group
+    uint32_t oct_inv = 0;  // 7 xor the ray's direction octant (set when a ray is fetched)
     bool has_ray = false, retired = false;
 
     // Tables shared by the block: s_perm[o][m] moves bit s of an 8-bit slot
@@ -131,6 +132,8 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                     ng_bits = 0x80000000u;   // with an empty inner-child mask
                     tg_bits = 0;
                     tg2_bits = 0;
+                    oct_inv = 7u ^ ((__float_as_uint(L.idx) >> 31) | ((__float_as_uint(L.idy) >> 31) << 1) |
+                                    ((__float_as_uint(L.idz) >> 31) << 2));
                     has_ray = true;
                 }
             }
@@ -148,8 +151,6 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                         ng_base = stack[sp].x;
                         ng_bits = stack[sp].y;
                     }
-                    const uint32_t oct_inv = 7u ^ ((__float_as_uint(L.idx) >> 31) | ((__float_as_uint(L.idy) >> 31) << 1) |
-                                                   ((__float_as_uint(L.idz) >> 31) << 2));
                     const uint32_t k = 31u - (uint32_t)__clz(ng_bits);
                     ng_bits &= ~(1u << k);
                     const uint32_t slot = (k - 24u) ^ oct_inv;
