@@ -298,11 +298,11 @@ def run_rb2(args, rank, world, local_rank):
     # 8 scenes x 500k triangles with 4.19M incoherent rays, half closest hit /
     # half occlusion, measured against 7961.2 MB of algorithmic bytes: 618.5 MB
     # for the binary layout (profiles/k_trace_jobs_batched_8x500k_full.md) and
-    # 444.4 MB for the compressed 8-wide layout
+    # 445.7 MB for the compressed 8-wide layout
     # (profiles/k_trace_jobs_cw8_batched_8x500k_full.md); scaled to this launch
     # by algorithmic bytes.
     cw8 = tuned is not None and tuned.get("node_order") == 3
-    traffic = alg_per_launch * ((444.4 if cw8 else 618.5) / 7961.2)
+    traffic = alg_per_launch * ((445.7 if cw8 else 618.5) / 7961.2)
     layout_name = {0: "binary DFS", 1: "binary BFS", 2: "4-wide", 3: "compressed 8-wide"}.get(
         (tuned or {}).get("node_order", 0), "binary DFS")
 
