@@ -117,7 +117,7 @@ template <int BLOCK, int REGS, class Src, int LAYOUT>
 __global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK)
     k_persistent(Src src, uint32_t fetch_threshold, unsigned int* status)
 {
-    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8(src, fetch_threshold, status);
+    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8<Src, true>(src, fetch_threshold, status);
     else persistent_trace(src, fetch_threshold, status);
 }
 

@@ -76,7 +76,12 @@ __device__ __forceinline__ bool cw8_triangle(Lane& L, int triAddr)
     return true;
 }
 
-template <class Source>
+// kOodSlab: form a node's slab offsets from the ray's precomputed o * idir
+// (one FMA per axis) instead of (plane - o) * idir.  The boxes' margin covers
+// the rounding of either form.  The integrators' kernels take it (fewer
+// instructions, no added spills); in the batched job kernel it adds spills
+// and costs more than it saves, so that kernel keeps the subtraction.
+template <class Source, bool kOodSlab = false>
 __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch_threshold, unsigned int* status)
 {
     const unsigned lane = threadIdx.x & 31u;
@@ -181,9 +186,16 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                         const float sy = __fmul_rn(__uint_as_float(((ew >> 8) & 0xFFu) << 23), L.idy);
                         const float sz = __fmul_rn(__uint_as_float(((ew >> 16) & 0xFFu) << 23), L.idz);
                         // Slab offsets less 1024 cells (planes arrive as 1024 + q).
-                        const float ax = __fmaf_rn(-1024.0f, sx, __fmul_rn(__fsub_rn(h0.x, L.ox), L.idx));
-                        const float ay = __fmaf_rn(-1024.0f, sy, __fmul_rn(__fsub_rn(h0.y, L.oy), L.idy));
-                        const float az = __fmaf_rn(-1024.0f, sz, __fmul_rn(__fsub_rn(h0.z, L.oz), L.idz));
+                        float ax, ay, az;
+                        if constexpr (kOodSlab) {
+                            ax = __fmaf_rn(-1024.0f, sx, __fmaf_rn(h0.x, L.idx, -L.oodx));
+                            ay = __fmaf_rn(-1024.0f, sy, __fmaf_rn(h0.y, L.idy, -L.oody));
+                            az = __fmaf_rn(-1024.0f, sz, __fmaf_rn(h0.z, L.idz, -L.oodz));
+                        } else {
+                            ax = __fmaf_rn(-1024.0f, sx, __fmul_rn(__fsub_rn(h0.x, L.ox), L.idx));
+                            ay = __fmaf_rn(-1024.0f, sy, __fmul_rn(__fsub_rn(h0.y, L.oy), L.idy));
+                            az = __fmaf_rn(-1024.0f, sz, __fmul_rn(__fsub_rn(h0.z, L.oz), L.idz));
+                        }
                         // Near and far plane words per axis (the high plane is near for a
                         // negative direction), children 0-3 in the first word, 4-7 in the second.
                         const bool rx = L.idx < 0.0f, ry = L.idy < 0.0f, rz = L.idz < 0.0f;
