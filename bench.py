@@ -1,7 +1,8 @@
 """Benchmark: incoherent ray-query throughput on one B200 (config 4 workload).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl rb2|reference]
-                  [--rays-per-scene R] [--scenes S] [--workload trace|ao|pt|bdpt|raycast]
+                  [--rays-per-scene R] [--scenes S]
+                  [--workload trace|ao|pt|bdpt|raycast|profile]
 
 One step = every scene's ray batch traced once: 64 heightfield scenes with
 log-uniform 1k..2M triangles, 1M incoherent diffuse-bounce rays per scene,
@@ -9,13 +10,23 @@ log-uniform 1k..2M triangles, 1M incoherent diffuse-bounce rays per scene,
 when the timed region starts; L2 is flushed (256 MB write) between timed
 steps.  `e2e` repeats the step through the host-buffer C-ABI call
 (rb2_trace_host_jobs: pinned host rays in, hits / occlusion bytes out, the
-copies pipelined with traversal over several streams), copies included.  Under torchrun each rank runs the same
-workload on its own GPU (replicas, no collective); `value` = all ranks' rays
-/ max-over-ranks time.
+copies pipelined with traversal over several streams), copies included.
+After timing, 4096 rays per scene and mode of the timed launch's outputs
+(device and end-to-end) are checked against the CPU oracle on the same BVH
+buffers; any mismatch makes the run exit non-zero.  The default line also
+carries the configs 1-3 frame times (AO, path tracing, BDPT) and the serving
+measurement (config 5).  Under torchrun each rank runs the same workload on
+its own GPU (replicas, no collective); `value` = all ranks' rays /
+max-over-ranks time.
 
---impl reference times the CPU restatement of the reference traversal (the
-reference has no host traversal of its own) on all host cores over a bounded
-sample of the same workload.
+--impl reference times the reference's own CPU path on the host cores: its
+SBVH builder (compiled from the reference sources) builds the smaller scenes
+of the same workload, and the CPU restatement of its traversal (the
+reference has no host traversal) traces each scene's full ray batch.  That
+process loads no part of this library.
+
+--workload profile runs one batched launch configuration over a small case
+repeatedly (for ncu captures; see --profile-* options).
 """
 from __future__ import annotations
 
@@ -25,6 +36,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -65,29 +77,81 @@ def build_workload(n_scenes: int, rays_per_scene: int, seed_base: int = 4):
     return scenes, build_s
 
 
-def oracle_bytes_sample(scenes, per_scene: int, nthreads: int = 0):
-    """Canonical single-lane visit counts of the oracle on a sample of each
-    scene's rays -> mean algorithmic bytes per ray, per mode and scene."""
+def sample_index(n: int, per: int) -> np.ndarray:
+    """Evenly spread sample of `per` indices out of n (all when n <= per)."""
+    return np.linspace(0, n - 1, min(per, n)).astype(np.int64) if n else np.zeros(0, np.int64)
+
+
+def oracle_sample(scenes, per_scene: int, nthreads: int = 0):
+    """The oracle on an evenly spread sample of each scene's closest-hit and
+    any-hit rays: hit records (for the parity check of the timed launch) and
+    canonical single-lane visit counts (for the algorithmic bytes).  Returns
+    one dict per scene: mode -> {idx, hits, bytes_per_ray, nodes, tris}."""
     import oracle
     out = []
-    t_cpu = 0.0
-    n_cpu = 0
     for s in scenes:
         nodes, woop, tri = s["bvh"].buffers_view()
         res = {}
         for mode, sl in (("ch", slice(0, s["n_ch"])), ("ah", slice(s["n_ch"], None))):
             r = s["rays"][sl]
-            idx = np.linspace(0, r.shape[0] - 1, min(per_scene, r.shape[0])).astype(np.int64)
-            t0 = time.perf_counter()
-            _, cnt = oracle.trace(nodes, woop, tri, r[idx], any_hit=(mode == "ah"), counts=True, nthreads=nthreads)
-            t_cpu += time.perf_counter() - t0
-            n_cpu += idx.size
+            idx = sample_index(r.shape[0], per_scene)
+            hits, cnt = oracle.trace(nodes, woop, tri, r[idx], any_hit=(mode == "ah"), counts=True,
+                                     nthreads=nthreads)
             out_b = 16 if mode == "ch" else 1
             bpr = 32 + 64 * cnt["nodes"].astype(np.float64) + 48 * cnt["tris"] + 16 * cnt["leafterms"] + out_b
-            res[mode] = dict(bytes_per_ray=float(bpr.mean()), nodes=float(cnt["nodes"].mean()),
-                             tris=float(cnt["tris"].mean()))
+            res[mode] = dict(idx=idx, hits=hits, bytes_per_ray=float(bpr.mean()) if idx.size else 0.0,
+                             nodes=float(cnt["nodes"].mean()) if idx.size else 0.0,
+                             tris=float(cnt["tris"].mean()) if idx.size else 0.0)
         out.append(res)
-    return out, (n_cpu / t_cpu / 1e6 if t_cpu > 0 else 0.0), n_cpu, t_cpu
+    return out
+
+
+def parity_check(scenes, samples, got_ch, got_occ, count_ties: bool = True):
+    """Closest hits: prim, t, u and v bits equal to the oracle's, except at a
+    confirmed tie (both triangles accept the ray at the same t: the layouts
+    that test triangles in another order may report the other one, the
+    reference's rule being tmin < t < hitT, kepler_dynamic_fetch.h:264).
+    Occlusion bytes equal to the oracle's any-hit decision.  `got_ch[k]` /
+    `got_occ[k]`: the GPU's records at samples[k]["ch"/"ah"]["idx"].  Also
+    counts the sampled closest-hit rays on which a tie exists (oracle, BVH
+    walk)."""
+    import oracle
+    n = mism = divergent = ties = 0
+    first = None
+    for k, (s, smp) in enumerate(zip(scenes, samples)):
+        nodes, woop, tri = s["bvh"].buffers_view()
+        want = smp["ch"]["hits"]
+        got = np.asarray(got_ch[k])
+        rays = s["rays"][: s["n_ch"]][smp["ch"]["idx"]]
+        n += want.shape[0]
+        if want.shape[0]:
+            g = got.view(np.uint32)
+            ok = (got[:, 0] == want["prim"]) & (g[:, 1] == want["t"].view(np.uint32)) & \
+                (g[:, 2] == want["u"].view(np.uint32)) & (g[:, 3] == want["v"].view(np.uint32))
+            bad = np.nonzero(~ok)[0]
+            slots = oracle.woop_slots_of(woop, tri) if bad.size else {}
+            for b in bad:
+                if got[b, 0] != want["prim"][b] and g[b, 1] == want["t"].view(np.uint32)[b] and \
+                        oracle.is_tie(woop, tri, slots, rays[b], got[b, 0], want["prim"][b]):
+                    divergent += 1
+                else:
+                    mism += 1
+                    if first is None:
+                        first = {"scene": k, "mode": "closest", "ray": int(smp["ch"]["idx"][b]),
+                                 "gpu": [int(x) for x in got[b]], "oracle_prim": int(want["prim"][b])}
+            if count_ties:
+                ties += int((oracle.tie_count(woop, tri, rays, want, nodes=nodes) >= 2).sum())
+        want_o = smp["ah"]["hits"]["prim"] >= 0
+        got_o = np.asarray(got_occ[k]).astype(bool)
+        n += want_o.shape[0]
+        bad_o = np.nonzero(got_o != want_o)[0]
+        mism += int(bad_o.size)
+        if bad_o.size and first is None:
+            first = {"scene": k, "mode": "occlusion", "ray": int(smp["ah"]["idx"][bad_o[0]])}
+    out = {"rays": int(n), "mismatches": int(mism), "ties": int(ties), "tie_divergent": int(divergent)}
+    if first is not None:
+        out["first_mismatch"] = first
+    return out
 
 
 # ------------------------------------------------------------------------------ clocks
@@ -99,11 +163,10 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self.path = Path(tempfile.mkdtemp(prefix="rb2_clocks_")) / "clocks.csv"
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -137,6 +200,43 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- GPU arm
+L2_BYTES = 126 * 1024 * 1024
+
+# DRAM bytes per algorithmic byte of the batched traversal kernel, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on a capture
+# small enough for the profiler: the first 8 scenes of this workload (triangle
+# counts and seeds as here) with 524,288 rays each, the tuned launch shape,
+# measured against the launch's algorithmic bytes.  Keyed by node order.
+DRAM_PER_ALG_BYTE = {
+    3: (445.7e6 / 7961.2e6, "8 scenes x 500k triangles, 4.19M rays, compressed 8-wide layout"),
+    1: (618.5e6 / 7961.2e6, "8 scenes x 500k triangles, 4.19M rays, binary BFS layout"),
+}
+
+
+def l2_copy_gbs(dev, stream, mbytes: int = 32, reps: int = 200) -> float:
+    """Achieved L2 bandwidth: a device-to-device copy of an `mbytes` MB
+    buffer into another (both resident in the 126 MB L2 after the first
+    pass), repeated; read + write bytes over CUDA-event time, best of 3."""
+    import torch
+    n = mbytes * 1024 * 1024 // 4
+    a = torch.ones(n, dtype=torch.float32, device=dev)
+    b = torch.empty_like(a)
+    best = 0.0
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            for _ in range(5):
+                b.copy_(a)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                b.copy_(a)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            best = max(best, 2.0 * a.numel() * 4 * reps / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del a, b
+    return best
+
+
 def run_rb2(args, rank, world, local_rank):
     import torch
 
@@ -155,6 +255,10 @@ def run_rb2(args, rank, world, local_rank):
     bvh_bytes = sum(t.device_bytes() for t in tracers)
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # Parity sample: the same evenly spread rays the oracle traces below.
+    idx_ch = [torch.from_numpy(sample_index(s["n_ch"], args.parity_rays)).to(dev) for s in scenes]
+    idx_ah = [torch.from_numpy(sample_index(s["rays"].shape[0] - s["n_ch"], args.parity_rays)).to(dev)
+              for s in scenes]
 
     def ev():
         return torch.cuda.Event(enable_timing=True)
@@ -177,10 +281,11 @@ def run_rb2(args, rank, world, local_rank):
                     pev[k][1][1].record(stream)
 
     # ---- batched path: one persistent launch over all 2 x scenes jobs, graph-replayed.
-    jobs = []
+    jobs, ch_jobs = [], []
     for k, s in enumerate(scenes):
         jobs.append((tracers[k], d_rays[k][: s["n_ch"]], rb.MODE_CLOSEST, d_hits[k], None))
         jobs.append((tracers[k], d_rays[k][s["n_ch"]:], rb.MODE_OCCLUSION, d_occ[k], None))
+        ch_jobs.append(jobs[-2])
     batch = rb.TraceBatch(jobs)
 
     def timed(step_fn, steps, per_step_events=None):
@@ -200,23 +305,34 @@ def run_rb2(args, rank, world, local_rank):
                 per_step_events()
         return ms
 
-    ch_ms, ah_ms = np.zeros(len(scenes)), np.zeros(len(scenes))
+    def plain_timed():
+        ch_ms, ah_ms = np.zeros(len(scenes)), np.zeros(len(scenes))
 
-    def collect_plain():
-        for k in range(len(scenes)):
-            ch_ms[k] += pev[k][0][0].elapsed_time(pev[k][0][1])
-            ah_ms[k] += pev[k][1][0].elapsed_time(pev[k][1][1])
+        def collect():
+            for k in range(len(scenes)):
+                ch_ms[k] += pev[k][0][0].elapsed_time(pev[k][0][1])
+                ah_ms[k] += pev[k][1][0].elapsed_time(pev[k][1][1])
+
+        for _ in range(args.warmup):
+            plain_step(False)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        ms = timed(lambda: plain_step(True), args.steps, collect)
+        return ms, ch_ms, ah_ms
+
+    def gather_outputs():
+        return ([d_hits[k][idx_ch[k]].cpu().numpy() for k in range(len(scenes))],
+                [d_occ[k][idx_ah[k]].cpu().numpy() for k in range(len(scenes))])
 
     # The plain path is timed first, with the tracers' defaults (the reference's
     # DFS Compact2 layout, default launch shape), before the autotuner changes
     # any tracer's layout; then the batched launch is tuned (untimed), captured
-    # and timed.  Clocks are sampled across both timed regions.
-    for _ in range(args.warmup):
-        plain_step(False)
-    torch.cuda.synchronize(dev)
-    barrier(world)
+    # and timed; then a batch of the closest-hit jobs alone; then the plain
+    # path again with the autotuned layout and launch shape, which separates
+    # the gain of batching from the gain of the layout.  Clocks are sampled
+    # across all timed regions.
     with ClockSampler(local_rank) as clk:
-        plain_ms = timed(lambda: plain_step(True), args.steps, collect_plain)
+        plain_ms, ch_ms, ah_ms = plain_timed()
         tuned, tuned_ms = batch.autotune(stream=stream, reps=5)
         batch.capture(stream)
         for _ in range(args.warmup):
@@ -224,12 +340,30 @@ def run_rb2(args, rank, world, local_rank):
         torch.cuda.synchronize(dev)
         barrier(world)
         batch_ms = timed(lambda: batch.launch(stream), args.steps)
+        got_ch, got_occ = gather_outputs()  # outputs of the last timed launch
+        batch_status = batch.status(stream)
+        ch_batch = rb.TraceBatch(ch_jobs)
+        ch_batch.set_config(**tuned)
+        ch_batch.capture(stream)
+        for _ in range(args.warmup):
+            ch_batch.launch(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        ch_batch_ms = timed(lambda: ch_batch.launch(stream), args.steps)
+        ch_batch_status = ch_batch.status(stream)
+        for t in tracers:  # the batch already switched every tracer to the tuned layout
+            t.set_launch(ctas_per_sm=tuned["ctas_per_sm"], fetch_threshold=tuned["fetch_threshold"],
+                         block_threads=tuned["block_threads"], regs=tuned["regs"])
+        same_ms, same_ch_ms, same_ah_ms = plain_timed()
     clocks = clk.summary()
-    plain_rate, plain_total = whole_job_rate(total_rays * args.steps, sum(plain_ms), world, dev)
+    plain_rate, _ = whole_job_rate(total_rays * args.steps, sum(plain_ms), world, dev)
     batch_rate, batch_total = whole_job_rate(total_rays * args.steps, sum(batch_ms), world, dev)
+    ch_batch_rate, _ = whole_job_rate(n_ch_total * args.steps, sum(ch_batch_ms), world, dev)
+    same_rate, _ = whole_job_rate(total_rays * args.steps, sum(same_ms), world, dev)
     for t in tracers:
         assert t.status() == 0, "device status word set"
-    assert batch.status() == 0, "batch status word set"
+    assert batch_status == 0 and ch_batch_status == 0, "batch status word set"
+    del ch_batch
 
     # ---- e2e through the host-buffer C-ABI calls (pinned host memory, copies in the timed region).
     # Headline: rb2_trace_host_jobs, chunks cycling through several streams so
@@ -281,47 +415,65 @@ def run_rb2(args, rank, world, local_rank):
     e2e_steps = max(1, min(args.steps, 5))
     e2e_single_steps = max(1, min(args.steps, 2))
     e2e_rate, _ = whole_job_rate(total_rays * e2e_steps, device_ms(e2e_step, e2e_steps), world, dev)
+    e2e_ch = [h_hits[k].numpy()[sample_index(s["n_ch"], args.parity_rays)] for k, s in enumerate(scenes)]
+    e2e_occ = [h_occ[k].numpy()[sample_index(s["rays"].shape[0] - s["n_ch"], args.parity_rays)]
+               for k, s in enumerate(scenes)]
     e2e_single_rate, _ = whole_job_rate(total_rays * e2e_single_steps, device_ms(e2e_single_step, e2e_single_steps),
                                         world, dev)
+    l2_gbs = l2_copy_gbs(dev, stream)
+
+    # ---- parity of the timed launch and of the end-to-end outputs against the oracle.
+    samples = oracle_sample(scenes, args.parity_rays)
+    parity = parity_check(scenes, samples, got_ch, got_occ)
+    parity_e2e = parity_check(scenes, samples, e2e_ch, e2e_occ, count_ties=False)
+    parity["e2e_mismatches"] = parity_e2e["mismatches"]
+    parity["e2e_tie_divergent"] = parity_e2e["tie_divergent"]
+    parity["checked"] = (f"{args.parity_rays} closest-hit + {args.parity_rays} any-hit rays per scene, evenly "
+                         "spread: the last timed batched launch and the e2e host outputs against the CPU oracle "
+                         "on the same BVH buffers (prim/t/u/v bits; occlusion bytes); ties = sampled closest-hit "
+                         "rays that 2+ triangles accept at the same t")
 
     # ---- roofline: dominant kernel = the batched traversal launch (one per step).
-    bytes_info, _, _, _ = oracle_bytes_sample(scenes, 4096)
-    ch_bytes = sum(bi["ch"]["bytes_per_ray"] * s["n_ch"] for bi, s in zip(bytes_info, scenes))
-    ah_bytes = sum(bi["ah"]["bytes_per_ray"] * (s["rays"].shape[0] - s["n_ch"]) for bi, s in zip(bytes_info, scenes))
+    ch_bytes = sum(sm["ch"]["bytes_per_ray"] * s["n_ch"] for sm, s in zip(samples, scenes))
+    ah_bytes = sum(sm["ah"]["bytes_per_ray"] * (s["rays"].shape[0] - s["n_ch"]) for sm, s in zip(samples, scenes))
+    node_visits = sum(sm["ch"]["nodes"] * s["n_ch"] + sm["ah"]["nodes"] * (s["rays"].shape[0] - s["n_ch"])
+                      for sm, s in zip(samples, scenes))
+    tri_tests = sum(sm["ch"]["tris"] * s["n_ch"] + sm["ah"]["tris"] * (s["rays"].shape[0] - s["n_ch"])
+                    for sm, s in zip(samples, scenes))
     launch_s = batch_total / 1e3 / args.steps
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
     alg_per_launch = ch_bytes + ah_bytes
     achieved = alg_per_launch / launch_s / 1e9
-    # DRAM traffic per launch: the ncu capture of the same batched kernel on
-    # 8 scenes x 500k triangles with 4.19M incoherent rays, half closest hit /
-    # half occlusion, measured against 7961.2 MB of algorithmic bytes: 618.5 MB
-    # for the binary layout (profiles/k_trace_jobs_batched_8x500k_full.md) and
-    # 445.7 MB for the compressed 8-wide layout
-    # (profiles/k_trace_jobs_cw8_batched_8x500k_full.md); scaled to this launch
-    # by algorithmic bytes.
-    cw8 = tuned is not None and tuned.get("node_order") == 3
-    traffic = alg_per_launch * ((445.7 if cw8 else 618.5) / 7961.2)
-    layout_name = {0: "binary DFS", 1: "binary BFS", 2: "4-wide", 3: "compressed 8-wide"}.get(
-        (tuned or {}).get("node_order", 0), "binary DFS")
+    order = (tuned or {}).get("node_order", 0)
+    ratio, ratio_src = DRAM_PER_ALG_BYTE.get(order, DRAM_PER_ALG_BYTE[1])
+    traffic = alg_per_launch * ratio
+    layout_name = {0: "binary DFS", 1: "binary BFS", 2: "4-wide", 3: "compressed 8-wide"}.get(order, "binary DFS")
 
     cpu_baseline = builder = None
     if rank == 0 and world == 1:
-        cpu_baseline = cpu_baseline_run(scenes, args.cpu_sample_s)
+        cpu_baseline = cpu_baseline_run(scenes, args.cpu_sample_s, args.ref_max_tris, args.ref_budget_tris)
         if args.cpu_sample_s > 0:
             builder = build_baseline(scenes)
 
     # ---- config 5: served jobs (continuous batching) vs plain one-at-a-time launches.
     serving = None
+    del batch
+    batch = None
     if args.serve_jobs > 0:
-        del batch
-        batch = None
         from renderbox2_b200.workloads import serving as serving_run
         serving = serving_run(n_jobs=args.serve_jobs)
 
+    # ---- configs 1-3: one frame each at full size (trace-stage roofline vs L2 or HBM).
+    integrators = {}
+    if args.integrators:
+        for kind in ("ao", "pt", "bdpt"):
+            integrators[kind] = integrator_summary(kind, l2_gbs, hbm_peak, with_cpu=(rank == 0 and world == 1))
+
     value = batch_rate / 1e6
     plain_value = plain_rate / 1e6
+    same_value = same_rate / 1e6
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(batch_total / args.steps, 4), "higher_is_better": True,
@@ -334,25 +486,47 @@ def run_rb2(args, rank, world, local_rank):
             "rays_per_step": int(total_rays), "l2": "flushed (256 MB write) between timed steps",
             "bvh_device_bytes": int(bvh_bytes), "build_s_host": round(build_s, 2), "parallelism": "replicas",
         },
+        "parity": parity,
         "plain_launches_mrays": round(plain_value, 2),
         "batched_over_plain": round(value / plain_value, 3),
         "plain_closest_hit_mrays": round(world * n_ch_total * args.steps / (ch_ms.sum() / 1e3) / 1e6, 2),
         "plain_any_hit_mrays": round(world * (total_rays - n_ch_total) * args.steps / (ah_ms.sum() / 1e3) / 1e6, 2),
+        "plain_same_layout_mrays": round(same_value, 2),
+        "plain_same_layout_closest_hit_mrays": round(world * n_ch_total * args.steps / (same_ch_ms.sum() / 1e3) / 1e6,
+                                                     2),
+        "batched_over_plain_same_layout": round(value / same_value, 3),
+        "batched_closest_hit_mrays": round(ch_batch_rate / 1e6, 2),
+        "batched_closest_hit_over_plain_same_layout": round(
+            ch_batch_rate / 1e6 / (world * n_ch_total * args.steps / (same_ch_ms.sum() / 1e3) / 1e6), 3),
+        "plain_note": "plain = 2 launches per scene (closest-hit half, any-hit half); default = the reference's DFS "
+                      "layout and the default launch shape; same_layout = the autotuned layout and launch shape",
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(achieved / hbm_peak, 4), "traffic": round(traffic),
                      "kernel": f"k_trace_jobs<BLOCK, REGS, LAYOUT> (batched, 1 launch/step, {layout_name} nodes)",
                      "peak_source": peak_src,
                      "alg_bytes_per_launch": round(alg_per_launch),
                      "alg_bytes_per_ray": round(alg_per_launch / total_rays, 1),
-                     "traffic_source": "scaled from ncu dram bytes of the 8 x 500k-triangle batched capture"},
+                     "traffic_source": f"ncu DRAM bytes per algorithmic byte of a capture ({ratio_src}) x this "
+                                       "launch's algorithmic bytes",
+                     "dram_gbs": round(traffic / launch_s / 1e9, 1),
+                     "dram_frac": round(traffic / launch_s / 1e9 / hbm_peak, 4),
+                     "l2_copy_gbs": round(l2_gbs, 1),
+                     "alg_frac_of_l2": round(achieved / l2_gbs, 4),
+                     "node_visits_per_s": round(node_visits / launch_s, 0),
+                     "box_tests_per_s": round(2 * node_visits / launch_s, 0),
+                     "tri_tests_per_s": round(tri_tests / launch_s, 0),
+                     "tests_note": "canonical single-lane counts of the oracle on the binary tree (inner-node "
+                                   "fetches, 2 box tests each; Woop triangle tests), per second of the batched "
+                                   "launch"},
         "e2e": {"value": round(e2e_rate / 1e6, 2), "unit": "Mrays/s",
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                 "path": f"rb2_trace_host_jobs over the 128 jobs (pinned host buffers, chunks of {args.e2e_chunk} "
                         f"rays through {args.e2e_depth} streams, copies in the timed region, CUDA events)",
                 "single_call_mrays": round(e2e_single_rate / 1e6, 2),
                 "single_call_path": "one blocking rb2_trace_host per job, 16-byte hits for every ray"},
-        "gpu_launches": args.steps * (1 + 2 * len(scenes)),
-        "gpu_launches_note": "timed region: batched steps (1 traversal launch each) + plain steps (2 per scene)",
+        "gpu_launches": args.steps * (2 + 4 * len(scenes)),
+        "gpu_launches_note": "timed region: batched steps (1 traversal launch each), closest-hit batch steps "
+                             "(1 each), plain steps with default and with tuned layout (2 per scene each)",
         "clocks": clocks,
     }
     if cpu_baseline is not None:
@@ -361,10 +535,38 @@ def run_rb2(args, rank, world, local_rank):
         line["build_baseline"] = builder
     if serving is not None:
         line["serving"] = serving
+    if integrators:
+        line["integrators"] = integrators
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del batch
     torch.cuda.synchronize(dev)
+    if parity["mismatches"] or parity["e2e_mismatches"]:
+        log(f"PARITY FAILURE: {parity}")
+        sys.exit(3)
+
+
+def integrator_summary(kind, l2_gbs, hbm_gbs, with_cpu=True):
+    """One full-size frame of config 1 (AO), 2 (PT) or 3 (BDPT): frame time,
+    samples/s, Mrays/s, the trace stage's roofline (against the measured L2
+    copy bandwidth when the binary BVH fits the 126 MB L2, else HBM) and the
+    FP64 CPU integrator on a small sample of the same frame."""
+    from renderbox2_b200.workloads import integrator
+    keep = {}
+    r = integrator(kind, keep=keep)
+    c = keep["bvh"].counts()
+    bvh_bytes = int(c.n_nodes_u4 * 16 + c.n_woop_u4 * 16 + c.n_triidx * 4)
+    out = {"ms_per_frame": r["ms"], "samples_per_s": r["samples_per_s"], "mrays_per_s": r["mrays_per_s"],
+           "triangles": r["triangles"], "resolution": [r["width"], r["height"]], "node_order": r["node_order"],
+           "binary_bvh_bytes": bvh_bytes}
+    base, counts = integrator_cpu_baseline(kind, keep)
+    if with_cpu:
+        out["cpu_baseline"] = base
+    if counts is not None:
+        l2_resident = bvh_bytes <= L2_BYTES
+        roof = integrator_roofline(kind, r, counts, l2_gbs if l2_resident else hbm_gbs,
+                                   "measured L2 copy (binary BVH fits L2)" if l2_resident else "MEASURED_PEAKS hbm_gbs")
+        out["roofline"] = roof
+    return out
 
 
 def run_workload(args, rank, local_rank):
@@ -385,7 +587,15 @@ def run_workload(args, rank, local_rank):
             if args.cpu_sample_s > 0:
                 line["cpu_baseline"] = base
             if counts is not None:
-                line["roofline"] = integrator_roofline(args.workload, r, counts)
+                c = keep["bvh"].counts()
+                bvh_bytes = int(c.n_nodes_u4 * 16 + c.n_woop_u4 * 16 + c.n_triidx * 4)
+                if bvh_bytes <= L2_BYTES:
+                    import torch
+                    dev = torch.device("cuda", local_rank)
+                    peak, src = l2_copy_gbs(dev, torch.cuda.Stream(device=dev)), "measured L2 copy (binary BVH fits L2)"
+                else:
+                    peak, src = _hbm_peak()[0], "MEASURED_PEAKS hbm_gbs"
+                line["roofline"] = integrator_roofline(args.workload, r, counts, peak, src)
         print(json.dumps(line), flush=True)
 
 
@@ -471,13 +681,19 @@ def integrator_cpu_baseline(kind, keep):
                        f"OpenMP over {cores} threads"}, counts)
 
 
-def integrator_roofline(kind, r, counts):
+def _hbm_peak():
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    if "hbm_gbs" in peaks:
+        return peaks["hbm_gbs"], "MEASURED_PEAKS.json hbm_gbs (measured)"
+    return 6650.0, "fallback 6650 GB/s"
+
+
+def integrator_roofline(kind, r, counts, peak, peak_src):
     """Trace-stage roofline of configs 1-3: algorithmic bytes of the frame's
     rays (GPU ray counts per type x the oracle's mean bytes per ray of that
     type, from its own rays of the same distributions) / the GPU time of the
-    traversal launches (CUDA events around each)."""
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    hbm = peaks.get("hbm_gbs", 6650.0)
+    traversal launches (CUDA events around each), against `peak` (the
+    measured L2 copy bandwidth when the BVH fits L2, else HBM)."""
     out_b = {"camera": 16, "extension": 16, "light": 16, "shadow": 1, "connection": 1}
 
     def bpr(t):
@@ -501,16 +717,18 @@ def integrator_roofline(kind, r, counts):
     if trace_s <= 0:
         return None
     ach = alg / trace_s / 1e9
-    return {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
-            "traffic": None, "alg_bytes_per_frame": round(alg), "trace_ms": round(st["trace_ms"], 3),
-            "bytes_per_ray": {t: round(bpr(t), 1) for t in gpu},
-            "note": "peak = measured HBM copy; the BVHs of configs 1 and 2 fit the 126 MB L2, so the traversal "
-                    "there is L2-bound and frac can exceed what HBM alone would allow"}
+    return {"bound": "hbm", "achieved": round(ach, 1), "peak": round(peak, 1), "unit": "GB/s",
+            "frac": round(ach / peak, 4), "peak_source": peak_src, "traffic": None,
+            "alg_bytes_per_frame": round(alg), "trace_ms": round(st["trace_ms"], 3),
+            "bytes_per_ray": {t: round(bpr(t), 1) for t in gpu}}
 
 
-def cpu_baseline_run(scenes, budget_s: float):
+def cpu_baseline_run(scenes, budget_s: float, ref_max_tris: int, ref_budget_tris: int):
     """Oracle traversal on all host cores over a bounded sample: equal share of
-    each scene's closest-hit and any-hit rays, sized to ~budget_s seconds."""
+    each scene's closest-hit and any-hit rays, sized to ~budget_s seconds.
+    Also times the oracle over this library's trees for the scene subset the
+    reference arm builds with the reference's builder (its full rays), so the
+    two CPU figures can be compared on the same scenes and rays."""
     import oracle
     cores = os.cpu_count() or 1
     # Calibrate on a small sample, then size the measured sample to the budget.
@@ -522,14 +740,23 @@ def cpu_baseline_run(scenes, budget_s: float):
         if dt > 0.5:
             break
         per *= 4
-    rate = n / dt
     per = int(max(256, min(scenes[0]["rays"].shape[0] // 2, per * budget_s / max(dt, 1e-3))))
     t0 = time.perf_counter()
     n = trace_sample(oracle, scenes, per)
     dt = time.perf_counter() - t0
-    return {"value": round(n / dt / 1e6, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
-            "sample": f"{per} closest-hit + {per} any-hit rays from each of {len(scenes)} scenes "
-                      f"({n:,} rays, {dt:.1f}s), oracle C restatement, OpenMP over {cores} threads"}
+    out = {"value": round(n / dt / 1e6, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
+           "sample": f"{per} closest-hit + {per} any-hit rays from each of {len(scenes)} scenes "
+                     f"({n:,} rays, {dt:.1f}s), oracle C restatement, OpenMP over {cores} threads"}
+    sub = reference_subset([s["tris"] for s in scenes], ref_max_tris, ref_budget_tris)
+    if sub and budget_s > 0:
+        t0 = time.perf_counter()
+        n = trace_sample(oracle, [scenes[k] for k in sub], 1 << 40)
+        dt = time.perf_counter() - t0
+        out["reference_subset"] = {"value": round(n / dt / 1e6, 3), "scenes": len(sub),
+                                   "triangles": int(sum(scenes[k]["tris"] for k in sub)), "rays": n,
+                                   "note": "the oracle over this library's trees of the scenes the reference arm "
+                                           "builds with the reference builder, every ray of each"}
+    return out
 
 
 def build_baseline(scenes, budget_tris: int = 30_000):
@@ -577,36 +804,176 @@ def trace_sample(oracle, scenes, per):
 
 
 # ------------------------------------------------------------------- reference arm
+def _load_configs():
+    """renderbox2_b200/configs.py loaded by file path, so the reference
+    process never imports the package (nor loads its library)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_rb2_configs", ROOT / "renderbox2_b200" / "configs.py")
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def reference_subset(tris, max_tris: int, budget_tris: int) -> list[int]:
+    """Scenes the reference's single-threaded builder can build within the
+    run: smallest first, each at most max_tris triangles, budget_tris in all.
+    Returns scene indices in workload order."""
+    pick, tot = [], 0
+    for k in sorted(range(len(tris)), key=lambda k: tris[k]):
+        if tris[k] > max_tris or tot + tris[k] > budget_tris:
+            break
+        pick.append(k)
+        tot += tris[k]
+    return sorted(pick)
+
+
+def _ref_build_worker(item):
+    """One scene through the reference's SBVH builder + Compact2 packer
+    (compiled from its sources), in a worker process."""
+    k, v, i = item
+    import oracle
+    t0 = time.perf_counter()
+    r = oracle.ref_build(v, i)
+    return k, r["nodes"], r["woop"], r["triidx"], time.perf_counter() - t0
+
+
 def run_reference(args, rank, world):
+    """The reference's CPU path on the host cores: the scenes of the batching
+    workload that its builder can build in the run (reference_subset), built
+    by that builder (one process per scene, all cores), then every ray of
+    each built scene (the workload's 1M rays: closest-hit half and any-hit
+    half, one call each) traced by the CPU restatement of its traversal on
+    all cores.  Scenes and rays come from the oracle's copy of the workload
+    generator; no part of this library is loaded."""
     if rank != 0:
         return
-    scenes, _ = build_workload(args.scenes, args.rays_per_scene)
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
     import oracle
     cores = os.cpu_count() or 1
-    per = max(256, args.ref_rays_per_scene)
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "reference builder (oracle/_ref) not built"}),
+              flush=True)
+        return
+    cfgs = _load_configs()
+    c4 = cfgs.CONFIG4
+    counts = cfgs.config4_triangle_counts(dict(c4, n_scenes=64))[: args.scenes]
+    sub = reference_subset(counts, args.ref_max_tris, args.ref_budget_tris)
+    t0 = time.time()
+    scenes = []
+    for k in sub:
+        v, i = oracle.gen_heightfield_for_triangles(4000 + k, counts[k])
+        rays, flags = oracle.gen_surface_rays(v, i, 4500 + k, args.rays_per_scene, c4["offset_scale"],
+                                              c4["anyhit_fraction"])
+        order = np.argsort(flags, kind="stable")
+        scenes.append(dict(k=k, v=v, i=i, rays=np.ascontiguousarray(rays[order]), n_ch=int((flags == 0).sum()),
+                           tris=int(i.shape[0])))
+    gen_s = time.time() - t0
+    t0 = time.time()
+    work = sorted(range(len(scenes)), key=lambda j: -scenes[j]["tris"])
+    build_cpu = 0.0
+    with cf.ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context("spawn")) as ex:
+        for j, nodes, woop, tri, dt in ex.map(_ref_build_worker, [(j, scenes[j]["v"], scenes[j]["i"]) for j in work]):
+            scenes[j].update(nodes=nodes, woop=woop, tri=tri)
+            build_cpu += dt
+    build_wall = time.time() - t0
+    log(f"reference arm: {len(scenes)} scenes, {sum(s['tris'] for s in scenes):,} triangles; generation "
+        f"{gen_s:.1f}s, reference SBVH build {build_wall:.1f}s wall ({build_cpu:.1f}s over {cores} processes)")
+
+    def step():
+        n = 0
+        for s in scenes:
+            ch, ah = s["rays"][: s["n_ch"]], s["rays"][s["n_ch"]:]
+            oracle.trace(s["nodes"], s["woop"], s["tri"], ch, any_hit=False)
+            oracle.trace(s["nodes"], s["woop"], s["tri"], ah, any_hit=True)
+            n += ch.shape[0] + ah.shape[0]
+        return n
+
     for _ in range(args.warmup):
-        trace_sample(oracle, scenes, min(per, 256))
+        step()
     times, n = [], 0
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        n = trace_sample(oracle, scenes, per)
+        n = step()
         times.append(time.perf_counter() - t0)
     tot = sum(times)
     value = n * args.steps / tot / 1e6
-    sample = (f"{per} closest-hit + {per} any-hit rays from each of {len(scenes)} scenes per step "
-              f"({n:,} rays), CPU restatement of the reference traversal (the reference has no host "
-              f"traversal), OpenMP over {cores} threads")
+    tris = sum(s["tris"] for s in scenes)
+    sample = (f"{len(scenes)} of the {len(counts)} scenes ({tris:,} triangles; every scene of at most "
+              f"{args.ref_max_tris:,} triangles, {args.ref_budget_tris:,} in all) built by the reference SBVH "
+              f"builder; all {args.rays_per_scene:,} rays of each per step ({n:,} rays), traced by the CPU "
+              f"restatement of the reference traversal (the reference has no host traversal), OpenMP over "
+              f"{cores} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot / args.steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "config 4: 64 heightfield scenes, log-uniform 1k..2M triangles, incoherent "
-                               "diffuse-bounce rays, 50% closest-hit / 50% any-hit", "parallelism": "host cores"},
-        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
+        "config": {"workload": "config 4: 64 heightfield scenes, log-uniform 1k..2M triangles, 1M incoherent "
+                               "diffuse-bounce rays per scene, 50% closest-hit / 50% any-hit; the scenes the "
+                               "reference builder builds within the run", "parallelism": "host cores",
+                   "scenes": len(scenes), "triangles": tris, "rays_per_step": n},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": cores, "kind": "reference",
                          "sample": sample},
+        "build": {"reference_sbvh_wall_s": round(build_wall, 2), "reference_sbvh_cpu_s": round(build_cpu, 2),
+                  "processes": cores, "triangles": tris},
         "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------- profile case
+def run_profile(args, local_rank):
+    """A small, repeatable case of the batched traversal for ncu captures:
+    either the first --scenes scenes of the batching workload (its triangle
+    counts and seeds) with --rays-per-scene rays each, or (with
+    --profile-equal-tris T) --scenes heightfields of T/scenes triangles each
+    (seeds 300+k, rays 400+k); half closest-hit / half occlusion jobs; one
+    launch configuration; --launches launches, CUDA-event timed.  Prints the
+    launch times and the algorithmic bytes per launch (oracle visit counts)."""
+    import torch
+
+    import renderbox2_b200 as rb
+    torch.cuda.set_device(local_rank)
+    if args.profile_equal_tris:
+        per = max(1000, args.profile_equal_tris // args.scenes)
+        scenes = []
+        for k in range(args.scenes):
+            sc = rb.heightfield_for_triangles(seed=300 + k, n_tris=per)
+            rays, _ = rb.surface_rays(sc, seed=400 + k, n=args.rays_per_scene)
+            scenes.append(dict(scene=sc, bvh=rb.BVH(sc), rays=rays, n_ch=args.rays_per_scene // 2,
+                               tris=sc.num_triangles))
+    else:
+        scenes, _ = build_workload(args.scenes, args.rays_per_scene)
+    keep, jobs = [], []
+    for s in scenes:
+        tr = rb.CudaTracer(s["bvh"])
+        d = torch.from_numpy(s["rays"]).cuda()
+        out_h = torch.empty((s["n_ch"], 4), dtype=torch.int32, device="cuda")
+        out_o = torch.empty((s["rays"].shape[0] - s["n_ch"],), dtype=torch.uint8, device="cuda")
+        jobs += [(tr, d[: s["n_ch"]], rb.MODE_CLOSEST, out_h, None), (tr, d[s["n_ch"]:], rb.MODE_OCCLUSION, out_o, None)]
+        keep.append((tr, d, out_h, out_o))
+    batch = rb.TraceBatch(jobs)
+    batch.set_config(block_threads=args.profile_block, regs=args.profile_regs, node_order=args.profile_order,
+                     fetch_threshold=args.profile_threshold, ctas_per_sm=args.profile_ctas, chunk=args.profile_chunk)
+    ms = []
+    for _ in range(args.launches):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.launch()
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    assert batch.status() == 0
+    res = {"scenes": len(scenes), "triangles": int(sum(s["tris"] for s in scenes)),
+           "rays": int(sum(s["rays"].shape[0] for s in scenes)), "launch_ms": ms, "config": batch.config()}
+    if not args.no_oracle:
+        smp = oracle_sample(scenes, args.parity_rays)
+        alg = sum(sm["ch"]["bytes_per_ray"] * s["n_ch"] + sm["ah"]["bytes_per_ray"] * (s["rays"].shape[0] - s["n_ch"])
+                  for sm, s in zip(smp, scenes))
+        best = min(ms[1:] if len(ms) > 1 else ms)
+        res.update(alg_bytes_per_launch=alg, achieved_gbs_best=alg / (best / 1e3) / 1e9)
+    print(json.dumps(res), flush=True)
 
 
 # ----------------------------------------------------------------------- dist glue
@@ -642,14 +1009,32 @@ def main():
     ap.add_argument("--impl", choices=["rb2", "reference"], default="rb2")
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--rays-per-scene", type=int, default=1 << 20)
-    ap.add_argument("--ref-rays-per-scene", type=int, default=2048)
+    ap.add_argument("--parity-rays", type=int, default=4096,
+                    help="rays per scene and mode checked against the oracle after timing")
+    ap.add_argument("--ref-max-tris", type=int, default=150_000,
+                    help="reference arm: largest scene its builder builds")
+    ap.add_argument("--ref-budget-tris", type=int, default=2_000_000,
+                    help="reference arm: triangles built in all")
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--e2e-chunk", type=int, default=1 << 20, help="rays per chunk of the pipelined host path")
     ap.add_argument("--e2e-depth", type=int, default=4, help="streams of the pipelined host path")
     ap.add_argument("--serve-jobs", type=int, default=10000,
                     help="config-5 jobs in the serving measurement (0: skip)")
-    ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt", "raycast"], default="trace",
-                    help="trace: the headline config-4 line; ao/pt/bdpt: configs 1-3 at full size")
+    ap.add_argument("--no-integrators", dest="integrators", action="store_false",
+                    help="leave configs 1-3 out of the default line")
+    ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt", "raycast", "profile"], default="trace",
+                    help="trace: the headline config-4 line; ao/pt/bdpt/raycast: one integrator config at full "
+                         "size; profile: a small batched case for ncu")
+    ap.add_argument("--launches", type=int, default=3, help="profile: launches")
+    ap.add_argument("--no-oracle", action="store_true", help="profile: skip the algorithmic-byte count")
+    ap.add_argument("--profile-equal-tris", type=int, default=0,
+                    help="profile: equal heightfields of this many triangles in all instead of workload scenes")
+    ap.add_argument("--profile-block", type=int, default=256)
+    ap.add_argument("--profile-regs", type=int, default=64)
+    ap.add_argument("--profile-order", type=int, default=3)
+    ap.add_argument("--profile-threshold", type=int, default=28)
+    ap.add_argument("--profile-ctas", type=int, default=0)
+    ap.add_argument("--profile-chunk", type=int, default=1)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -666,6 +1051,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload == "profile":
+            run_profile(args, local_rank)
         elif args.workload != "trace":
             run_workload(args, rank, local_rank)
         else:

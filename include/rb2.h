@@ -28,7 +28,7 @@ typedef enum {
     RB2_ECUDA = 3,       /* CUDA runtime error */
     RB2_EIO = 4,         /* file could not be read or written */
     RB2_EFORMAT = 5,     /* corrupt or unsupported BVH / cache contents */
-    RB2_ETIMEOUT = 6,    /* a bounded device wait ran out */
+    RB2_ETIMEOUT = 6,    /* a bounded wait ran out (device wait, or a served job's deadline) */
     RB2_EDEVICE = 7,     /* device-side check failed (status word set) */
     RB2_ENOTSUP = 8      /* feature not available on this device / build */
 } rb2_status;
@@ -269,6 +269,17 @@ int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream);
  * `reps` launches each), applies and returns the fastest. */
 int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best, double* best_ms);
 
+/* ------------------------------------------------------- fault injection --
+ * Host-side hooks for tests of the error paths; no GPU fault is involved.
+ * Every device allocation of the library goes through one wrapper.
+ * rb2_debug_fail_alloc(k): the k-th device allocation from this call on
+ * fails as cudaMalloc would when memory is exhausted (the entry point that
+ * made it returns RB2_ENOMEM and frees what it had allocated); 0 disarms.
+ * rb2_debug_alloc_count: successful allocations since load and allocations
+ * not yet freed (for leak checks around create / destroy pairs). */
+int rb2_debug_fail_alloc(uint64_t k);
+int rb2_debug_alloc_count(uint64_t* total, int64_t* live);
+
 /* --------------------------------------------------- allocation-free batch --
  * No counterpart in the reference.  For callers that cannot let a library
  * allocate device memory: hosts that own all device memory through their own
@@ -306,6 +317,13 @@ typedef struct {
 } rb2_noalloc_job;
 
 int rb2_trace_batch_noalloc(const rb2_noalloc_job* jobs, uint32_t n_jobs, void* stream);
+/* Guard bits of the last rb2_trace_batch_noalloc call that traced any ray on
+ * the current device (0 = clean; bit 0 = a ray whose traversal stack would
+ * have overflowed, as a corrupt or over-deep tree can cause, was reported as
+ * a miss).  Copies the word from the shared array into *status on `stream`
+ * and synchronises that stream; allocates nothing.  Issue it on the stream
+ * of the trace call it checks, under the same one-stream rule. */
+int rb2_trace_batch_noalloc_status(uint32_t* status, void* stream);
 
 #ifdef __cplusplus
 }

@@ -49,11 +49,17 @@ typedef struct {
 } rb2_job_result;
 
 typedef struct {
-    uint32_t slots;         /* concurrent execution slots (streams); 0 = 8 */
+    uint32_t slots;         /* concurrent execution slots (streams); 0 = 8, at most 256 (RB2_EINVAL above:
+                               a tracer hands out 256 per-launch queue heads) */
     uint32_t fifo;          /* 1: one job at a time, arrival order, one slot */
     uint64_t hbm_budget;    /* bytes of job working set admitted at once; 0 = 8 GiB */
     uint32_t max_tile;      /* largest tile side (slot state is sized for it); 0 = 1024 */
-    uint32_t reserved;
+    uint32_t job_timeout_ms;/* per-job deadline from admission; 0 = none.  A job still running at its
+                               deadline gets status RB2_ETIMEOUT (latency = time to the deadline check)
+                               and the loop goes on admitting and retiring other jobs; its slot and
+                               budget share come back once its work has left the slot's stream, and
+                               its output is unspecified.  rb2_server_run returns only after every
+                               slot is idle, timed-out jobs included. */
     uint64_t max_rays;      /* largest ray job (slot staging); 0 = 4M */
 } rb2_server_config;
 
@@ -74,11 +80,18 @@ typedef struct rb2_server rb2_server;
 int rb2_server_create(rb2_tracer* const* tracers, rb2_scene_dev* const* scenes, uint32_t n_bvh,
                       const rb2_server_config* cfg, rb2_server** out);
 int rb2_server_destroy(rb2_server* s);
-/* Runs the request loop until every job completed; results[i] belongs to jobs[i]. */
+/* Runs the request loop until every job completed or timed out; results[i]
+ * belongs to jobs[i].  Returns the first failing job's status (RB2_OK when
+ * every job succeeded). */
 int rb2_server_run(rb2_server* s, const rb2_job* jobs, uint32_t n_jobs, rb2_job_result* results,
                    rb2_server_stats* stats);
 /* Device working set a job reserves against the HBM budget. */
 uint64_t rb2_job_footprint(const rb2_job* job);
+
+/* Fault injection on the host, for tests of the deadline: the next job the
+ * loop enqueues waits behind a host function (cudaLaunchHostFunc) that
+ * sleeps `ms` milliseconds on its slot's stream.  No GPU fault is involved. */
+int rb2_debug_stall_next_job(uint32_t ms);
 
 #ifdef __cplusplus
 }

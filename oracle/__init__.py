@@ -19,7 +19,6 @@ compiled code and against fixtures in tests/golden/ generated from it.
 from __future__ import annotations
 
 import ctypes as C
-import os
 import subprocess
 from pathlib import Path
 
@@ -28,7 +27,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 REF_SO = HERE / "_ref" / "librb2ref.so"
 ORACLE_SO = HERE / "liboracle.so"
-REF_SRC = Path(os.environ.get("RB2_REF_SRC", "/root/reference/renderbox2/src"))
+
+# The reference checkout is located by oracle/Makefile (override: RB2_REF_SRC).
 
 _ref = None
 _orc = None
@@ -53,10 +53,8 @@ COUNT_DTYPE = np.dtype([("nodes", np.uint32), ("tris", np.uint32), ("leafterms",
 
 def build(ref: bool = True) -> None:
     """Builds liboracle.so, and librb2ref.so when the reference sources exist."""
-    targets = ["oracle"]
-    if ref and REF_SRC.exists():
-        targets.append("ref")
-    subprocess.run(["make", "-s", "-C", str(HERE), *targets, f"REF_SRC={REF_SRC}"], check=True)
+    targets = ["oracle"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
 
 
 def have_ref() -> bool:
@@ -98,6 +96,20 @@ def orc_lib():
         L.rb2o_woop_test.restype = C.c_int
         L.rb2o_bruteforce.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
         L.rb2o_bruteforce.restype = None
+        L.rb2o_tie_count_brute.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                           C.c_void_p, C.c_int]
+        L.rb2o_tie_count_brute.restype = None
+        L.rb2o_tie_count.argtypes = [C.c_void_p] * 4 + [C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]
+        L.rb2o_tie_count.restype = None
+        L.rb2o_gen_heightfield_counts.argtypes = [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
+                                                  C.POINTER(C.c_uint32)]
+        L.rb2o_gen_heightfield_counts.restype = C.c_int
+        L.rb2o_gen_heightfield.argtypes = [C.c_uint64, C.c_uint32, C.c_float, C.c_uint32, C.c_float, C.c_float,
+                                           C.c_void_p, C.c_void_p]
+        L.rb2o_gen_heightfield.restype = C.c_int
+        L.rb2o_gen_surface_rays.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64,
+                                            C.c_float, C.c_float, C.c_void_p, C.c_void_p]
+        L.rb2o_gen_surface_rays.restype = C.c_int
         _orc = L
     return _orc
 
@@ -276,6 +288,62 @@ def bruteforce(woop, triidx, rays, nthreads=0):
     orc_lib().rb2o_bruteforce(_p(woop), _p(triidx), woop.reshape(-1, 4).shape[0], _p(rays), rays.shape[0],
                               _p(hits), int(nthreads))
     return hits
+
+
+def tie_count(woop, triidx, rays, hits, nodes=None, nthreads=0) -> np.ndarray:
+    """Per ray, how many distinct triangles accept it at exactly its
+    closest-hit t (hits from `trace`): >= 2 marks a tie at a shared edge or
+    vertex.  Without `nodes` every Woop slot is tested (exact, for small
+    scenes); with the node buffer the BVH is walked with a slack around t
+    (for statistics on large scenes)."""
+    woop = np.ascontiguousarray(woop, np.uint32)
+    triidx = np.ascontiguousarray(triidx, np.uint32)
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    hits = np.ascontiguousarray(hits, HIT_DTYPE)
+    out = np.zeros(rays.shape[0], np.uint32)
+    if nodes is None:
+        orc_lib().rb2o_tie_count_brute(_p(woop), _p(triidx), woop.reshape(-1, 4).shape[0], _p(rays), rays.shape[0],
+                                       _p(hits), _p(out), int(nthreads))
+    else:
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        orc_lib().rb2o_tie_count(_p(nodes), _p(woop), _p(triidx), _p(rays), rays.shape[0], _p(hits), _p(out),
+                                 int(nthreads))
+    return out
+
+
+def gen_heightfield(seed: int, grid_n: int, amplitude: float = 0.2, n_boxes: int = 64, box_min: float = 0.02,
+                    box_max: float = 0.1):
+    """The synthetic heightfield scene (oracle copy of the product generator):
+    (vertices (nv, 3) float32, indices (nt, 3) uint32)."""
+    nv, nt = C.c_uint32(), C.c_uint32()
+    if orc_lib().rb2o_gen_heightfield_counts(grid_n, n_boxes, C.byref(nv), C.byref(nt)):
+        raise ValueError("bad heightfield size")
+    v = np.empty((nv.value, 3), np.float32)
+    i = np.empty((nt.value, 3), np.uint32)
+    if orc_lib().rb2o_gen_heightfield(seed, grid_n, amplitude, n_boxes, box_min, box_max, _p(v), _p(i)):
+        raise RuntimeError("heightfield generation failed")
+    return v, i
+
+
+def gen_heightfield_for_triangles(seed: int, n_tris: int, n_boxes: int = 64):
+    """Heightfield with a grid sized to about n_tris triangles (grid n =
+    round(sqrt((T - 12 boxes) / 2)), the batching workload's rule)."""
+    n = max(1, int(round(np.sqrt(max(2, n_tris - 12 * n_boxes) / 2.0))))
+    return gen_heightfield(seed, n, n_boxes=n_boxes)
+
+
+def gen_surface_rays(vertices, indices, seed: int, n: int, offset_scale: float = 1e-4,
+                     anyhit_fraction: float = 0.5):
+    """Incoherent diffuse-bounce rays from the scene's surfaces (oracle copy
+    of the product generator): (rays (n, 8) float32, flags (n,) uint8)."""
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+    i = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
+    rays = np.empty((n, 8), np.float32)
+    flags = np.empty((n,), np.uint8)
+    if orc_lib().rb2o_gen_surface_rays(_p(v), v.shape[0], _p(i), i.shape[0], seed, n, offset_scale,
+                                       anyhit_fraction, _p(rays), _p(flags)):
+        raise ValueError("bad ray-generation arguments")
+    return rays, flags
 
 
 def woop_slots_of(woop, triidx):

@@ -31,6 +31,7 @@
  */
 #include "rb2_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -349,6 +350,107 @@ void rb2o_bruteforce(const uint32_t* woop, const uint32_t* triidx, uint32_t n_wo
         } else {
             out[i].prim = -1; out[i].t = rays[8 * i + 7]; out[i].u = 0.0f; out[i].v = 0.0f;
         }
+    }
+    (void)nthreads;
+}
+
+/* Distinct triangle ids among `ids[0..n)`; appends `id` when new. */
+static inline void add_distinct(uint32_t* ids, uint32_t* n, uint32_t cap, uint32_t id)
+{
+    for (uint32_t k = 0; k < *n; k++)
+        if (ids[k] == id) return;
+    if (*n < cap) ids[(*n)++] = id;
+}
+
+#define RB2O_TIE_CAP 64
+
+void rb2o_tie_count_brute(const uint32_t* woop, const uint32_t* triidx, uint32_t n_woop_u4, const float* rays,
+                          uint32_t n, const rb2o_hit* hits, uint32_t* out, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        out[i] = 0;
+        if (hits[i].prim < 0) continue;
+        ray_setup s;
+        setup_ray(rays + 8 * i, &s);
+        const float t = hits[i].t;
+        uint32_t ids[RB2O_TIE_CAP], nid = 0;
+        for (uint32_t slot = 0; slot < n_woop_u4;) {
+            const uint32_t* w = woop + 4 * (size_t)slot;
+            if (w[0] == 0x80000000u) { slot += 1; continue; }
+            float wf[12];
+            for (int k = 0; k < 12; k++) wf[k] = as_f(w[k]);
+            float tuv[3];
+            if (woop_accept(&s, wf, FLT_MAX, tuv) && tuv[0] == t) add_distinct(ids, &nid, RB2O_TIE_CAP, triidx[slot]);
+            slot += 3;
+        }
+        out[i] = nid;
+    }
+    (void)nthreads;
+}
+
+void rb2o_tie_count(const uint32_t* nodes, const uint32_t* woop, const uint32_t* triidx, const float* rays,
+                    uint32_t n, const rb2o_hit* hits, uint32_t* out, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        out[i] = 0;
+        if (hits[i].prim < 0) continue;
+        ray_setup s;
+        setup_ray(rays + 8 * i, &s);
+        const float t = hits[i].t;
+        /* Visit every node whose box the ray enters before t plus a slack
+         * that covers the slab test's rounding (boxes whose face holds the
+         * hit point stay in), and never shrink the interval. */
+        const float omax = fmaxf(fabsf(s.ox), fmaxf(fabsf(s.oy), fabsf(s.oz)));
+        const float tcut = t + fabsf(t) * 1.0e-3f + (omax + 1.0f) * 1.0e-5f;
+        uint32_t ids[RB2O_TIE_CAP], nid = 0;
+        int32_t stack[4 * RB2O_STACK];
+        int sp = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            int32_t a = stack[--sp];
+            if (a < 0) {
+                for (int32_t triAddr = ~a;; triAddr += 3) {
+                    const uint32_t* w = woop + 4 * (size_t)triAddr;
+                    if (w[0] == 0x80000000u) break;
+                    float wf[12];
+                    for (int k = 0; k < 12; k++) wf[k] = as_f(w[k]);
+                    float tuv[3];
+                    if (woop_accept(&s, wf, FLT_MAX, tuv) && tuv[0] == t)
+                        add_distinct(ids, &nid, RB2O_TIE_CAP, triidx[triAddr]);
+                }
+                continue;
+            }
+            const uint32_t* nd = nodes + 4 * (size_t)a;
+            const float lo0[3] = {as_f(nd[0]), as_f(nd[2]), as_f(nd[8])};
+            const float hi0[3] = {as_f(nd[1]), as_f(nd[3]), as_f(nd[9])};
+            const float lo1[3] = {as_f(nd[4]), as_f(nd[6]), as_f(nd[10])};
+            const float hi1[3] = {as_f(nd[5]), as_f(nd[7]), as_f(nd[11])};
+            const float id3[3] = {s.idx, s.idy, s.idz}, ood3[3] = {s.oodx, s.oody, s.oodz};
+            const int32_t ch[2] = {(int32_t)nd[12], (int32_t)nd[13]};
+            for (int c = 0; c < 2; c++) {
+                const float* lo = c ? lo1 : lo0;
+                const float* hi = c ? hi1 : hi0;
+                float e[3], x[3];
+                for (int k = 0; k < 3; k++) {
+                    float p = fmaf(lo[k], id3[k], -ood3[k]), q = fmaf(hi[k], id3[k], -ood3[k]);
+                    e[k] = fminf(p, q);
+                    x[k] = fmaxf(p, q);
+                }
+                float cmin = fmaxf(fmaxf(e[0], e[1]), fmaxf(e[2], s.tmin));
+                float cmax = fminf(fminf(x[0], x[1]), fminf(x[2], tcut));
+                if (cmax >= cmin * (cmin > 0.0f ? 1.0f - 1.0e-5f : 1.0f + 1.0e-5f) && sp < 4 * RB2O_STACK)
+                    stack[sp++] = ch[c];
+            }
+        }
+        out[i] = nid;
     }
     (void)nthreads;
 }

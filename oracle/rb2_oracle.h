@@ -40,6 +40,25 @@ int rb2o_woop_test(const uint32_t* woop12, const float* ray8, float tmax, float*
 void rb2o_bruteforce(const uint32_t* woop, const uint32_t* triidx, uint32_t n_woop_u4,
                      const float* rays, uint32_t n, rb2o_hit* out, int nthreads);
 
+/* Tie count per ray: the number of distinct triangles whose Woop test
+ * accepts the ray at exactly its closest-hit t (hits[i].t; 0 for misses).
+ * A ray through a shared edge or vertex of triangles that agree on t counts
+ * 2 or more.  _brute tests every Woop slot (exact; small scenes); the other
+ * walks the BVH with the t interval widened by a slack that keeps boxes whose
+ * face holds the hit point, so it is meant for statistics on large scenes. */
+void rb2o_tie_count_brute(const uint32_t* woop, const uint32_t* triidx, uint32_t n_woop_u4, const float* rays,
+                          uint32_t n, const rb2o_hit* hits, uint32_t* out, int nthreads);
+void rb2o_tie_count(const uint32_t* nodes, const uint32_t* woop, const uint32_t* triidx, const float* rays,
+                    uint32_t n, const rb2o_hit* hits, uint32_t* out, int nthreads);
+
+/* The synthetic heightfield workload (oracle copy of the product generator;
+ * rb2_oracle_gen.c).  Return 0 on success. */
+int rb2o_gen_heightfield_counts(uint32_t grid_n, uint32_t n_boxes, uint32_t* nv, uint32_t* ntri);
+int rb2o_gen_heightfield(uint64_t seed, uint32_t grid_n, float amplitude, uint32_t n_boxes, float box_min,
+                         float box_max, float* v, uint32_t* idx);
+int rb2o_gen_surface_rays(const float* v_xyz, uint32_t nv, const uint32_t* idx3, uint32_t ntri, uint64_t seed,
+                          uint64_t n_rays, float offset_scale, float anyhit_fraction, float* rays, uint8_t* flags);
+
 /* Intersection record of a closest hit, as the reference's bulk kernel fills
  * IntersectionBuffer (accelerators/sbvh/kepler_dynamic_fetch.h:313-355),
  * in IEEE single precision with no contraction:

@@ -236,8 +236,10 @@ class CudaTracer:
         check(lib().rb2_tracer_device_bytes(self._t, C.byref(v)))
         return v.value
 
-    def set_launch(self, ctas_per_sm=0, fetch_threshold=0):
-        cfg = LaunchConfig(0, ctas_per_sm, fetch_threshold, 0)
+    def set_launch(self, ctas_per_sm=0, fetch_threshold=0, block_threads=0, regs=0):
+        """Launch shape of this tracer's bulk traversals (rb2_launch_config;
+        0 = the tuned default for each field)."""
+        cfg = LaunchConfig(block_threads, ctas_per_sm, fetch_threshold, regs)
         check(lib().rb2_tracer_set_launch(self._t, C.byref(cfg)))
 
     def set_node_order(self, order: int):

@@ -1,6 +1,7 @@
 // Film: filtered, deterministic image reconstruction (rb2_film_develop, the
 // integrators' filtered accumulation) and the PFM image writer.
 #include "rb2.h"
+#include "rb2_devmem.h"
 #include "rb2_film.cuh"
 #include "rb2_internal.h"
 #include "rb2_render.h"
@@ -38,7 +39,7 @@ using namespace rb2;
 
 namespace {
 
-int cuda_fail(cudaError_t e, const char* what) { return fail(RB2_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)); }
+int cuda_fail(cudaError_t e, const char* what) { return fail(rb2::cuda_status(e), std::string(what) + ": " + cudaGetErrorString(e)); }
 
 unsigned film_grid(uint64_t npix)
 {

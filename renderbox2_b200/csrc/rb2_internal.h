@@ -140,6 +140,9 @@ DeviceBvhView device_bvh(const rb2_tracer* t, bool allow_cw8 = false);
 int validate_filter(const rb2_filter* f);
 
 // A zeroed-before-use queue head of the tracer's ring (one per launch in flight).
+// The ring holds kTracerQueueSlots heads, so at most that many launches of one
+// tracer may be in flight at once.
+constexpr uint32_t kTracerQueueSlots = 256;
 unsigned long long* tracer_queue_counter(rb2_tracer* t);
 
 inline uint32_t f2u(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }

@@ -6,6 +6,7 @@
 // (accelerators/sbvh/kepler_dynamic_fetch.h:313-355), so hit records never
 // make a round trip through HBM before the record is built.
 #include "rb2.h"
+#include "rb2_devmem.h"
 #include "rb2_device.cuh"
 #include "rb2_internal.h"
 #include "rb2_render.h"
@@ -111,7 +112,7 @@ using namespace rb2;
 
 namespace {
 
-int cuda_fail(cudaError_t e, const char* what) { return fail(RB2_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)); }
+int cuda_fail(cudaError_t e, const char* what) { return fail(rb2::cuda_status(e), std::string(what) + ": " + cudaGetErrorString(e)); }
 
 #define RB2_CUDA(call, what)                               \
     do {                                                   \

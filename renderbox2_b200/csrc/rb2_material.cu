@@ -1,6 +1,7 @@
 // Layered materials: host packing (rb2_scene_set_materials) and the device
 // query entry used by the tests (rb2_material_query).
 #include "rb2.h"
+#include "rb2_devmem.h"
 #include "rb2_internal.h"
 #include "rb2_material.cuh"
 #include "rb2_render.h"
@@ -46,7 +47,7 @@ using namespace rb2;
 
 namespace {
 
-int cuda_fail(cudaError_t e, const char* what) { return fail(RB2_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)); }
+int cuda_fail(cudaError_t e, const char* what) { return fail(rb2::cuda_status(e), std::string(what) + ": " + cudaGetErrorString(e)); }
 
 // One layer in the device packing; Oren-Nayar A, B as the scene reader
 // computes them (io/customfilereader.cpp:128-136).
@@ -113,16 +114,16 @@ int rb2_scene_set_materials(rb2_scene_dev* s, const rb2_material_desc* materials
         layered |= !plain;
     }
     rb2dev::MaterialDev* dm = nullptr;
-    if ((e = cudaMalloc(&dm, mats.size() * sizeof(rb2dev::MaterialDev))) != cudaSuccess)
+    if ((e = rb2::dev_malloc(&dm, mats.size() * sizeof(rb2dev::MaterialDev))) != cudaSuccess)
         return fail(RB2_ENOMEM, std::string("material table: ") + cudaGetErrorString(e));
     if ((e = cudaMemcpy(dm, mats.data(), mats.size() * sizeof(rb2dev::MaterialDev), cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(s->d_albedo, alb.data(), s->n_mat * sizeof(float4), cudaMemcpyHostToDevice)) != cudaSuccess) {
-        cudaFree(dm);
+        rb2::dev_free(dm);
         return cuda_fail(e, "material upload");
     }
     if (s->d_mats) {
         s->bytes -= (uint64_t)s->n_mat * sizeof(rb2dev::MaterialDev);
-        cudaFree(s->d_mats);
+        rb2::dev_free(s->d_mats);
     }
     s->d_mats = dm;
     s->layered = layered;

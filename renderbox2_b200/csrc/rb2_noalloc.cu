@@ -158,3 +158,27 @@ extern "C" int rb2_trace_batch_noalloc(const rb2_noalloc_job* jobs, uint32_t n_j
     if (e != cudaSuccess) return rb2::fail(RB2_ECUDA, std::string("trace launch: ") + cudaGetErrorString(e));
     return RB2_OK;
 }
+
+// Status of the last rb2_trace_batch_noalloc call on the current device: the
+// guard bits its kernel set (bit 0: a ray's traversal stack would have
+// overflowed, so that ray was reported as a miss).  The word is copied into
+// the caller's host variable on `stream` and the stream is synchronised; no
+// memory is allocated.  Same one-stream rule as the trace call: a query
+// issued while another call's kernel is in flight on a different stream reads
+// an unspecified value.
+extern "C" int rb2_trace_batch_noalloc_status(uint32_t* status, void* stream)
+{
+    if (!status) return rb2::fail(RB2_EINVAL, "rb2_trace_batch_noalloc_status: null status pointer");
+    DeviceSetup dev;
+    int rc = setup_current_device(dev);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const char* base = reinterpret_cast<const char*>(dev.scratch);
+    unsigned int word = 0;
+    cudaError_t e = cudaMemcpyAsync(&word, base + offsetof(NoAllocScratch, status), sizeof(word),
+                                    cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return rb2::fail(RB2_ECUDA, std::string("status read: ") + cudaGetErrorString(e));
+    *status = word;
+    return RB2_OK;
+}

@@ -6,6 +6,7 @@
 // kernel's fetch() from path state and consumed in finish(), so secondary-ray
 // buffers never round-trip through HBM.
 #include "rb2.h"
+#include "rb2_devmem.h"
 #include "rb2_internal.h"
 #include "rb2_render.h"
 #include "rb2_camera.cuh"
@@ -25,7 +26,7 @@ using namespace rb2;
 
 namespace {
 
-int cuda_fail(cudaError_t e, const char* what) { return fail(RB2_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)); }
+int cuda_fail(cudaError_t e, const char* what) { return fail(rb2::cuda_status(e), std::string(what) + ": " + cudaGetErrorString(e)); }
 
 #define RB2_CUDA(call, what)                               \
     do {                                                   \
@@ -37,10 +38,10 @@ template <class T>
 int grow(T*& p, uint64_t& cap, uint64_t n)
 {
     if (n <= cap) return RB2_OK;
-    cudaFree(p);
+    rb2::dev_free(p);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc(&p, sizeof(T) * std::max<uint64_t>(n, 1));
+    cudaError_t e = rb2::dev_malloc(&p, sizeof(T) * std::max<uint64_t>(n, 1));
     if (e != cudaSuccess) return fail(RB2_ENOMEM, std::string("integrator scratch: ") + cudaGetErrorString(e));
     cap = n;
     return RB2_OK;
@@ -1118,15 +1119,15 @@ namespace rb2 {
 int ensure_path_state(PathState& ps, uint64_t P)
 {
     if (P <= ps.cap) return RB2_OK;
-    cudaFree(ps.T); cudaFree(ps.L); cudaFree(ps.ray); cudaFree(ps.hit); cudaFree(ps.sray); cudaFree(ps.sc);
-    cudaFree(ps.q[0]); cudaFree(ps.q[1]); cudaFree(ps.qs);
+    rb2::dev_free(ps.T); rb2::dev_free(ps.L); rb2::dev_free(ps.ray); rb2::dev_free(ps.hit); rb2::dev_free(ps.sray); rb2::dev_free(ps.sc);
+    rb2::dev_free(ps.q[0]); rb2::dev_free(ps.q[1]); rb2::dev_free(ps.qs);
     ps = PathState();
     cudaError_t e;
-    if ((e = cudaMalloc(&ps.T, P * 16)) != cudaSuccess || (e = cudaMalloc(&ps.L, P * 16)) != cudaSuccess ||
-        (e = cudaMalloc(&ps.ray, P * 32)) != cudaSuccess || (e = cudaMalloc(&ps.hit, P * 16)) != cudaSuccess ||
-        (e = cudaMalloc(&ps.sray, P * 32)) != cudaSuccess || (e = cudaMalloc(&ps.sc, P * 16)) != cudaSuccess ||
-        (e = cudaMalloc(&ps.q[0], P * 4)) != cudaSuccess || (e = cudaMalloc(&ps.q[1], P * 4)) != cudaSuccess ||
-        (e = cudaMalloc(&ps.qs, P * 4)) != cudaSuccess)
+    if ((e = rb2::dev_malloc(&ps.T, P * 16)) != cudaSuccess || (e = rb2::dev_malloc(&ps.L, P * 16)) != cudaSuccess ||
+        (e = rb2::dev_malloc(&ps.ray, P * 32)) != cudaSuccess || (e = rb2::dev_malloc(&ps.hit, P * 16)) != cudaSuccess ||
+        (e = rb2::dev_malloc(&ps.sray, P * 32)) != cudaSuccess || (e = rb2::dev_malloc(&ps.sc, P * 16)) != cudaSuccess ||
+        (e = rb2::dev_malloc(&ps.q[0], P * 4)) != cudaSuccess || (e = rb2::dev_malloc(&ps.q[1], P * 4)) != cudaSuccess ||
+        (e = rb2::dev_malloc(&ps.qs, P * 4)) != cudaSuccess)
         return fail(RB2_ENOMEM, std::string("path state: ") + cudaGetErrorString(e));
     ps.cap = P;
     return RB2_OK;
@@ -1135,36 +1136,36 @@ int ensure_path_state(PathState& ps, uint64_t P)
 int ensure_bdpt_state(BdptState& bd, uint64_t n_paths, uint64_t n_slots, uint64_t n_conn)
 {
     cudaError_t e = cudaSuccess;
-    if (!bd.lvc_off && (e = cudaMalloc(&bd.lvc_off, (kMaxBdptWave + 1) * sizeof(uint32_t))) != cudaSuccess)
+    if (!bd.lvc_off && (e = rb2::dev_malloc(&bd.lvc_off, (kMaxBdptWave + 1) * sizeof(uint32_t))) != cudaSuccess)
         return fail(RB2_ENOMEM, std::string("cache offsets: ") + cudaGetErrorString(e));
     if (n_paths > bd.cap_paths) {
-        for (void* p : {(void*)bd.lray, (void*)bd.lbeta, (void*)bd.lhit, (void*)bd.lq[0], (void*)bd.lq[1]}) cudaFree(p);
+        for (void* p : {(void*)bd.lray, (void*)bd.lbeta, (void*)bd.lhit, (void*)bd.lq[0], (void*)bd.lq[1]}) rb2::dev_free(p);
         bd.lray = bd.lbeta = nullptr; bd.lhit = nullptr; bd.lq[0] = bd.lq[1] = nullptr; bd.cap_paths = 0;
-        if ((e = cudaMalloc(&bd.lray, n_paths * 32)) != cudaSuccess || (e = cudaMalloc(&bd.lbeta, n_paths * 16)) != cudaSuccess ||
-            (e = cudaMalloc(&bd.lhit, n_paths * 16)) != cudaSuccess || (e = cudaMalloc(&bd.lq[0], n_paths * 4)) != cudaSuccess ||
-            (e = cudaMalloc(&bd.lq[1], n_paths * 4)) != cudaSuccess)
+        if ((e = rb2::dev_malloc(&bd.lray, n_paths * 32)) != cudaSuccess || (e = rb2::dev_malloc(&bd.lbeta, n_paths * 16)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&bd.lhit, n_paths * 16)) != cudaSuccess || (e = rb2::dev_malloc(&bd.lq[0], n_paths * 4)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&bd.lq[1], n_paths * 4)) != cudaSuccess)
             return fail(RB2_ENOMEM, std::string("light paths: ") + cudaGetErrorString(e));
         bd.cap_paths = n_paths;
     }
     if (n_slots > bd.cap_slots) {
         for (void* p : {(void*)bd.s_pos, (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_wi, (void*)bd.s_valid,
                         (void*)bd.d_slot, (void*)bd.block_sums})
-            cudaFree(p);
+            rb2::dev_free(p);
         bd.s_pos = bd.s_nrm = bd.s_beta = bd.s_wi = nullptr;
         bd.s_valid = nullptr; bd.d_slot = nullptr; bd.block_sums = nullptr; bd.cap_slots = 0;
         const uint64_t nb = (n_slots + rb2dev::kScanChunk - 1) / rb2dev::kScanChunk;
-        if ((e = cudaMalloc(&bd.s_pos, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.s_nrm, n_slots * 16)) != cudaSuccess ||
-            (e = cudaMalloc(&bd.s_beta, n_slots * 16)) != cudaSuccess || (e = cudaMalloc(&bd.s_valid, n_slots)) != cudaSuccess ||
-            (e = cudaMalloc(&bd.d_slot, n_slots * 4)) != cudaSuccess || (e = cudaMalloc(&bd.s_wi, n_slots * 16)) != cudaSuccess ||
-            (e = cudaMalloc(&bd.block_sums, nb * 4)) != cudaSuccess)
+        if ((e = rb2::dev_malloc(&bd.s_pos, n_slots * 16)) != cudaSuccess || (e = rb2::dev_malloc(&bd.s_nrm, n_slots * 16)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&bd.s_beta, n_slots * 16)) != cudaSuccess || (e = rb2::dev_malloc(&bd.s_valid, n_slots)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&bd.d_slot, n_slots * 4)) != cudaSuccess || (e = rb2::dev_malloc(&bd.s_wi, n_slots * 16)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&bd.block_sums, nb * 4)) != cudaSuccess)
             return fail(RB2_ENOMEM, std::string("light vertex cache: ") + cudaGetErrorString(e));
         bd.cap_slots = n_slots;
     }
     if (n_conn > bd.cap_conn) {
-        for (void* p : {(void*)bd.cray, (void*)bd.cc, (void*)bd.cq}) cudaFree(p);
+        for (void* p : {(void*)bd.cray, (void*)bd.cc, (void*)bd.cq}) rb2::dev_free(p);
         bd.cray = bd.cc = nullptr; bd.cq = nullptr; bd.cap_conn = 0;
-        if ((e = cudaMalloc(&bd.cray, n_conn * 32)) != cudaSuccess || (e = cudaMalloc(&bd.cc, n_conn * 16)) != cudaSuccess ||
-            (e = cudaMalloc(&bd.cq, n_conn * 4)) != cudaSuccess)
+        if ((e = rb2::dev_malloc(&bd.cray, n_conn * 32)) != cudaSuccess || (e = rb2::dev_malloc(&bd.cc, n_conn * 16)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&bd.cq, n_conn * 4)) != cudaSuccess)
             return fail(RB2_ENOMEM, std::string("connection rays: ") + cudaGetErrorString(e));
         bd.cap_conn = n_conn;
     }
@@ -1184,7 +1185,7 @@ int integrator_reserve_pt(rb2_integrator* it, uint64_t paths, uint64_t npix)
     int rc;
     if ((rc = ensure_path_state(it->ps, paths))) return rc;
     if ((rc = grow(it->d_accum, it->cap_accum, npix))) return rc;
-    if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
+    if (!it->d_wave) RB2_CUDA(rb2::dev_malloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
     return RB2_OK;
 }
 
@@ -1224,12 +1225,12 @@ int rb2_scene_create(const float* v_xyz, uint32_t nv, const uint32_t* idx3, uint
     s->nv = nv; s->ntri = ntri; s->n_mat = nm; s->n_lights = (uint32_t)lights.size();
     if (lights.empty()) lights.push_back(0);
     cudaError_t e;
-    if ((e = cudaMalloc(&s->d_verts, v.size() * sizeof(float4))) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_tris, t.size() * sizeof(uint4))) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_albedo, nm * sizeof(float4))) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_emission, nm * sizeof(float4))) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_lights, lights.size() * sizeof(uint32_t))) != cudaSuccess) {
-        cudaFree(s->d_verts); cudaFree(s->d_tris); cudaFree(s->d_albedo); cudaFree(s->d_emission); cudaFree(s->d_lights);
+    if ((e = rb2::dev_malloc(&s->d_verts, v.size() * sizeof(float4))) != cudaSuccess ||
+        (e = rb2::dev_malloc(&s->d_tris, t.size() * sizeof(uint4))) != cudaSuccess ||
+        (e = rb2::dev_malloc(&s->d_albedo, nm * sizeof(float4))) != cudaSuccess ||
+        (e = rb2::dev_malloc(&s->d_emission, nm * sizeof(float4))) != cudaSuccess ||
+        (e = rb2::dev_malloc(&s->d_lights, lights.size() * sizeof(uint32_t))) != cudaSuccess) {
+        rb2::dev_free(s->d_verts); rb2::dev_free(s->d_tris); rb2::dev_free(s->d_albedo); rb2::dev_free(s->d_emission); rb2::dev_free(s->d_lights);
         return fail(RB2_ENOMEM, std::string("scene allocation: ") + cudaGetErrorString(e));
     }
     RB2_CUDA(cudaMemcpy(s->d_verts, v.data(), v.size() * sizeof(float4), cudaMemcpyHostToDevice), "scene upload");
@@ -1245,8 +1246,8 @@ int rb2_scene_create(const float* v_xyz, uint32_t nv, const uint32_t* idx3, uint
 int rb2_scene_destroy(rb2_scene_dev* s)
 {
     if (!s) return RB2_OK;
-    cudaFree(s->d_verts); cudaFree(s->d_tris); cudaFree(s->d_albedo); cudaFree(s->d_emission); cudaFree(s->d_lights);
-    cudaFree(s->d_mats);
+    rb2::dev_free(s->d_verts); rb2::dev_free(s->d_tris); rb2::dev_free(s->d_albedo); rb2::dev_free(s->d_emission); rb2::dev_free(s->d_lights);
+    rb2::dev_free(s->d_mats);
     delete s;
     return RB2_OK;
 }
@@ -1268,7 +1269,7 @@ int rb2_integrator_create(rb2_tracer* tracer, const rb2_scene_dev* scene, rb2_in
     int dev = 0;
     RB2_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
     RB2_CUDA(cudaDeviceGetAttribute(&it->sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    RB2_CUDA(cudaMalloc(&it->d_counters, 16 * sizeof(unsigned long long)), "integrator counters");
+    RB2_CUDA(rb2::dev_malloc(&it->d_counters, 16 * sizeof(unsigned long long)), "integrator counters");
     *out = it.release();
     return RB2_OK;
 }
@@ -1276,18 +1277,18 @@ int rb2_integrator_create(rb2_tracer* tracer, const rb2_scene_dev* scene, rb2_in
 int rb2_integrator_destroy(rb2_integrator* it)
 {
     if (!it) return RB2_OK;
-    cudaFree(it->d_rays); cudaFree(it->d_hits); cudaFree(it->d_count); cudaFree(it->d_counters);
-    cudaFree(it->d_accum); cudaFree(it->d_wave); cudaFree(it->d_film_xy);
+    rb2::dev_free(it->d_rays); rb2::dev_free(it->d_hits); rb2::dev_free(it->d_count); rb2::dev_free(it->d_counters);
+    rb2::dev_free(it->d_accum); rb2::dev_free(it->d_wave); rb2::dev_free(it->d_film_xy);
     for (cudaEvent_t e : it->ev) cudaEventDestroy(e);
     PathState& ps = it->ps;
-    cudaFree(ps.T); cudaFree(ps.L); cudaFree(ps.ray); cudaFree(ps.hit); cudaFree(ps.sray); cudaFree(ps.sc);
-    cudaFree(ps.q[0]); cudaFree(ps.q[1]); cudaFree(ps.qs);
+    rb2::dev_free(ps.T); rb2::dev_free(ps.L); rb2::dev_free(ps.ray); rb2::dev_free(ps.hit); rb2::dev_free(ps.sray); rb2::dev_free(ps.sc);
+    rb2::dev_free(ps.q[0]); rb2::dev_free(ps.q[1]); rb2::dev_free(ps.qs);
     BdptState& bd = it->bd;
     for (void* p : {(void*)bd.lray, (void*)bd.lbeta, (void*)bd.lhit, (void*)bd.lq[0], (void*)bd.lq[1], (void*)bd.s_pos,
                     (void*)bd.s_nrm, (void*)bd.s_beta, (void*)bd.s_wi, (void*)bd.s_valid, (void*)bd.d_slot,
                     (void*)bd.block_sums, (void*)bd.cray,
                     (void*)bd.cc, (void*)bd.cq, (void*)bd.lvc_off})
-        cudaFree(p);
+        rb2::dev_free(p);
     delete it;
     return RB2_OK;
 }
@@ -1388,7 +1389,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
         if ((rc = grow(it->d_film_xy, it->cap_film_xy, P))) return rc;
         if ((rc = film_args(it->filter, cam->width, cam->height, fa))) return rc;
     }
-    if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
+    if (!it->d_wave) RB2_CUDA(rb2::dev_malloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
     RB2_CUDA(cudaMemsetAsync(it->d_accum, 0, npix * 16, s), "accumulator reset");
     RB2_CUDA(cudaMemsetAsync(it->d_wave, 0, sizeof(WaveCounters), s), "counter reset");
 
@@ -1463,7 +1464,7 @@ int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_rayc
         if ((rc = grow(it->d_film_xy, it->cap_film_xy, P))) return rc;
         if ((rc = film_args(it->filter, cam->width, cam->height, fa))) return rc;
     }
-    if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
+    if (!it->d_wave) RB2_CUDA(rb2::dev_malloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
     RB2_CUDA(cudaMemsetAsync(it->d_accum, 0, npix * 16, s), "accumulator reset");
     RB2_CUDA(cudaMemsetAsync(it->d_wave, 0, sizeof(WaveCounters), s), "counter reset");
     rb2dev::CamArgs ca;
@@ -1542,7 +1543,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
         if ((rc = grow(it->d_film_xy, it->cap_film_xy, npix * Wv))) return rc;
         if ((rc = film_args(it->filter, cam->width, cam->height, fa))) return rc;
     }
-    if (!it->d_wave) RB2_CUDA(cudaMalloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
+    if (!it->d_wave) RB2_CUDA(rb2::dev_malloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
     RB2_CUDA(cudaMemsetAsync(it->d_accum, 0, npix * 16, s), "accumulator reset");
     RB2_CUDA(cudaMemsetAsync(it->d_wave, 0, sizeof(WaveCounters), s), "counter reset");
 

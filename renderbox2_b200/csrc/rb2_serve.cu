@@ -8,6 +8,7 @@
 // kernels on its slot's stream, and retires jobs by polling their completion
 // events; kernels of different slots run concurrently on the GPU.
 #include "rb2.h"
+#include "rb2_devmem.h"
 #include "rb2_internal.h"
 #include "rb2_render.h"
 #include "rb2_render_internal.h"
@@ -16,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <numeric>
@@ -33,10 +35,22 @@ struct Slot {
     float4* d_rays = nullptr;
     int4* d_out = nullptr;   // rb2_hit or uint8 occlusion
     float* d_img = nullptr;
-    int job = -1;
+    int job = -1;           // job running on the slot, -1 = none
+    bool draining = false;  // a timed-out job's work is still on the stream
+    double deadline = 0.0;  // loop time after which the running job times out
+    uint64_t footprint = 0; // bytes the slot holds against the HBM budget
 };
 
 uint64_t out_bytes_per_ray(uint32_t mode) { return mode == RB2_MODE_OCCLUSION ? 1 : 16; }
+
+// Host-side fault injection (rb2_debug_stall_next_job): the next enqueued job
+// waits behind a host function that sleeps this many milliseconds.
+std::atomic<uint32_t> g_stall_next_ms{0};
+
+void CUDART_CB sleep_host_fn(void* ms)
+{
+    std::this_thread::sleep_for(std::chrono::milliseconds((uintptr_t)ms));
+}
 
 }  // namespace
 
@@ -64,9 +78,9 @@ extern "C" int rb2_server_destroy(rb2_server* s)
     for (Slot& sl : s->slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
         rb2_integrator_destroy(sl.it);
-        cudaFree(sl.d_rays);
-        cudaFree(sl.d_out);
-        cudaFree(sl.d_img);
+        rb2::dev_free(sl.d_rays);
+        rb2::dev_free(sl.d_out);
+        rb2::dev_free(sl.d_img);
         if (sl.done) cudaEventDestroy(sl.done);
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }
@@ -91,6 +105,11 @@ extern "C" int rb2_server_create(rb2_tracer* const* tracers, rb2_scene_dev* cons
     if (!c.hbm_budget) c.hbm_budget = 8ull << 30;
     if (!c.max_tile) c.max_tile = 1024;
     if (!c.max_rays) c.max_rays = 4ull << 20;
+    // Ray jobs take their queue head from the tracer's ring of per-launch
+    // counters; more slots than ring entries could hand two concurrent
+    // launches the same head.
+    if (c.slots > kTracerQueueSlots)
+        return fail(RB2_EINVAL, "at most " + std::to_string(kTracerQueueSlots) + " server slots");
     if (c.max_rays > 0xFFFFFFFFull) return fail(RB2_EINVAL, "max_rays must fit 32 bits");
     const uint64_t max_npix = (uint64_t)c.max_tile * c.max_tile;
     // Path state for the largest tile at up to 64 spp in flight (larger spp
@@ -108,9 +127,9 @@ extern "C" int rb2_server_create(rb2_tracer* const* tracers, rb2_scene_dev* cons
         cudaError_t e;
         if ((e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaMalloc(&sl.d_rays, c.max_rays * 32)) != cudaSuccess ||
-            (e = cudaMalloc(&sl.d_out, c.max_rays * 16)) != cudaSuccess ||
-            (e = cudaMalloc(&sl.d_img, max_npix * 12)) != cudaSuccess) {
+            (e = rb2::dev_malloc(&sl.d_rays, c.max_rays * 32)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&sl.d_out, c.max_rays * 16)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&sl.d_img, max_npix * 12)) != cudaSuccess) {
             rb2_server_destroy(s.release());
             return fail(RB2_ENOMEM, std::string("server slot: ") + cudaGetErrorString(e));
         }
@@ -134,6 +153,10 @@ int enqueue(rb2_server* s, Slot& sl, const rb2_job& j)
 {
     cudaStream_t st = sl.stream;
     if (j.bvh >= s->tracers.size()) return fail(RB2_EINVAL, "job names a BVH outside the pool");
+    if (const uint32_t ms = g_stall_next_ms.exchange(0)) {
+        cudaError_t e = cudaLaunchHostFunc(st, sleep_host_fn, (void*)(uintptr_t)ms);
+        if (e != cudaSuccess) return fail(RB2_ECUDA, std::string("stall injection: ") + cudaGetErrorString(e));
+    }
     if (j.kind == RB2_JOB_RAYS) {
         if (j.n_rays > s->cfg.max_rays || (j.n_rays && (!j.h_rays || !j.h_out)) || j.mode > RB2_MODE_OCCLUSION)
             return fail(RB2_EINVAL, "bad ray job");
@@ -182,7 +205,12 @@ extern "C" int rb2_server_run(rb2_server* s, const rb2_job* jobs, uint32_t n_job
                               rb2_server_stats* stats)
 {
     if (!s || (n_jobs && (!jobs || !results))) return fail(RB2_EINVAL, "null argument");
-    for (Slot& sl : s->slots) sl.job = -1;
+    for (Slot& sl : s->slots) {
+        sl.job = -1;
+        sl.draining = false;
+        sl.footprint = 0;
+    }
+    const double timeout_s = s->cfg.job_timeout_ms ? s->cfg.job_timeout_ms * 1e-3 : 0.0;
     std::vector<uint32_t> order(n_jobs);
     std::iota(order.begin(), order.end(), 0u);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return jobs[a].arrival_s < jobs[b].arrival_s; });
@@ -194,12 +222,37 @@ extern "C" int rb2_server_run(rb2_server* s, const rb2_job* jobs, uint32_t n_job
     int first_error = RB2_OK;
     while (done < n_jobs) {
         bool progress = false;
-        // Retire finished jobs.
+        // Retire finished jobs; time out jobs past their deadline.
         for (uint32_t k = 0; k < s->slots.size(); k++) {
             Slot& sl = s->slots[k];
+            if (sl.draining) {
+                // The timed-out job's work has left the stream: the slot and
+                // its share of the budget are free again.
+                if (cudaEventQuery(sl.done) == cudaErrorNotReady) continue;
+                sl.draining = false;
+                admitted -= sl.footprint;
+                sl.footprint = 0;
+                progress = true;
+                continue;
+            }
             if (sl.job < 0) continue;
             const cudaError_t q = cudaEventQuery(sl.done);
-            if (q == cudaErrorNotReady) continue;
+            if (q == cudaErrorNotReady) {
+                if (timeout_s > 0.0 && now() > sl.deadline) {
+                    rb2_job_result& r = results[sl.job];
+                    r.end_s = now();
+                    r.latency_s = r.end_s - jobs[sl.job].arrival_s;
+                    r.status = fail(RB2_ETIMEOUT, "job " + std::to_string(sl.job) + " passed its " +
+                                                      std::to_string(s->cfg.job_timeout_ms) + " ms deadline");
+                    if (!first_error) first_error = r.status;
+                    sl.job = -1;
+                    sl.draining = true;
+                    active--;
+                    done++;
+                    progress = true;
+                }
+                continue;
+            }
             rb2_job_result& r = results[sl.job];
             const rb2_job& j = jobs[sl.job];
             r.end_s = now();
@@ -215,7 +268,8 @@ extern "C" int rb2_server_run(rb2_server* s, const rb2_job* jobs, uint32_t n_job
                 if (rb2_integrator_stats(sl.it, &rs, sl.stream) == RB2_OK)
                     r.rays = rs.primary_rays + rs.extension_rays + rs.shadow_rays;
             }
-            admitted -= r.footprint_bytes;
+            admitted -= sl.footprint;
+            sl.footprint = 0;
             sl.job = -1;
             active--;
             done++;
@@ -230,7 +284,7 @@ extern "C" int rb2_server_run(rb2_server* s, const rb2_job* jobs, uint32_t n_job
             Slot* free_slot = nullptr;
             uint32_t slot_idx = 0;
             for (uint32_t k = 0; k < s->slots.size(); k++)
-                if (s->slots[k].job < 0) { free_slot = &s->slots[k]; slot_idx = k; break; }
+                if (s->slots[k].job < 0 && !s->slots[k].draining) { free_slot = &s->slots[k]; slot_idx = k; break; }
             if (!free_slot) break;  // wait for a slot
             rb2_job_result& r = results[ji];
             r.admit_s = t;
@@ -249,6 +303,8 @@ extern "C" int rb2_server_run(rb2_server* s, const rb2_job* jobs, uint32_t n_job
             }
             cudaEventRecord(free_slot->done, free_slot->stream);
             free_slot->job = (int)ji;
+            free_slot->deadline = t + timeout_s;
+            free_slot->footprint = fp;
             admitted += fp;
             peak = std::max(peak, admitted);
             active++;
@@ -260,6 +316,13 @@ extern "C" int rb2_server_run(rb2_server* s, const rb2_job* jobs, uint32_t n_job
             if (active == 0 && wait > 2e-4) std::this_thread::sleep_for(std::chrono::duration<double>(wait - 1e-4));
             else std::this_thread::yield();
         }
+    }
+    // Timed-out jobs may still be writing their outputs: return only once
+    // every slot's stream is idle.
+    for (Slot& sl : s->slots) {
+        if (sl.draining) cudaEventSynchronize(sl.done);
+        sl.draining = false;
+        sl.footprint = 0;
     }
     const double wall = now();
     if (stats) {
@@ -285,4 +348,10 @@ extern "C" int rb2_server_run(rb2_server* s, const rb2_job* jobs, uint32_t n_job
         stats->resident_bytes = s->resident;
     }
     return first_error;
+}
+
+extern "C" int rb2_debug_stall_next_job(uint32_t ms)
+{
+    g_stall_next_ms.store(ms);
+    return RB2_OK;
 }

@@ -11,6 +11,7 @@
 // g_warpCounter made trace() non-reentrant, kepler_dynamic_fetch.h:65), and a
 // stack guard that records a status bit instead of writing out of bounds.
 #include "rb2.h"
+#include "rb2_devmem.h"
 #include "rb2_internal.h"
 #include "rb2_render.h"
 #include "rb2_sources.cuh"
@@ -65,12 +66,12 @@ using namespace rb2;
 
 namespace {
 
-constexpr uint32_t kSlots = 256;
+constexpr uint32_t kSlots = kTracerQueueSlots;
 constexpr uint32_t kDefaultBlock = 128;
 
 int cuda_fail(cudaError_t e, const char* what)
 {
-    return fail(RB2_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return fail(rb2::cuda_status(e), std::string(what) + ": " + cudaGetErrorString(e));
 }
 
 #define RB2_CUDA(call, what)                                \
@@ -350,15 +351,15 @@ int upload_cw8(rb2_tracer* t)
     float4 *dn = nullptr, *dw = nullptr;
     uint32_t* di = nullptr;
     cudaError_t e;
-    if ((e = cudaMalloc(&dn, nb)) != cudaSuccess || (e = cudaMalloc(&dw, wb)) != cudaSuccess ||
-        (e = cudaMalloc(&di, ib)) != cudaSuccess) {
-        cudaFree(dn); cudaFree(dw); cudaFree(di);
+    if ((e = rb2::dev_malloc(&dn, nb)) != cudaSuccess || (e = rb2::dev_malloc(&dw, wb)) != cudaSuccess ||
+        (e = rb2::dev_malloc(&di, ib)) != cudaSuccess) {
+        rb2::dev_free(dn); rb2::dev_free(dw); rb2::dev_free(di);
         return fail(RB2_ENOMEM, std::string("compressed 8-wide layout: ") + cudaGetErrorString(e));
     }
     if ((e = cudaMemcpy(dn, cw.nodes.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(dw, cw.woop.data(), cw.woop.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(di, tri3.data(), ib, cudaMemcpyHostToDevice)) != cudaSuccess) {
-        cudaFree(dn); cudaFree(dw); cudaFree(di);
+        rb2::dev_free(dn); rb2::dev_free(dw); rb2::dev_free(di);
         return cuda_fail(e, "compressed 8-wide upload");
     }
     t->d_cw_nodes = dn;
@@ -392,13 +393,13 @@ int rb2_tracer_create(const rb2_host_bvh* bvh, rb2_tracer** out)
     // three rows before testing the first for the terminator.
     const size_t nb = h.nodes.size() * 4, wb = (h.woop.size() + 8) * 4, ib = h.triidx.size() * 4 + 16;
     auto cleanup = [&]() {
-        cudaFree(t->d_nodes); cudaFree(t->d_woop); cudaFree(t->d_triidx); cudaFree(t->d_counters); cudaFree(t->d_status);
+        rb2::dev_free(t->d_nodes); rb2::dev_free(t->d_woop); rb2::dev_free(t->d_triidx); rb2::dev_free(t->d_counters); rb2::dev_free(t->d_status);
     };
     cudaError_t e;
-    if ((e = cudaMalloc(&t->d_nodes, nb)) != cudaSuccess || (e = cudaMalloc(&t->d_woop, wb)) != cudaSuccess ||
-        (e = cudaMalloc(&t->d_triidx, ib)) != cudaSuccess ||
-        (e = cudaMalloc(&t->d_counters, kSlots * sizeof(unsigned long long))) != cudaSuccess ||
-        (e = cudaMalloc(&t->d_status, sizeof(unsigned int))) != cudaSuccess) {
+    if ((e = rb2::dev_malloc(&t->d_nodes, nb)) != cudaSuccess || (e = rb2::dev_malloc(&t->d_woop, wb)) != cudaSuccess ||
+        (e = rb2::dev_malloc(&t->d_triidx, ib)) != cudaSuccess ||
+        (e = rb2::dev_malloc(&t->d_counters, kSlots * sizeof(unsigned long long))) != cudaSuccess ||
+        (e = rb2::dev_malloc(&t->d_status, sizeof(unsigned int))) != cudaSuccess) {
         cleanup();
         return fail(RB2_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
     }
@@ -420,18 +421,18 @@ int rb2_tracer_create(const rb2_host_bvh* bvh, rb2_tracer** out)
 int rb2_tracer_destroy(rb2_tracer* t)
 {
     if (!t) return RB2_OK;
-    cudaFree(t->d_nodes);
-    cudaFree(t->d_woop);
-    cudaFree(t->d_triidx);
-    cudaFree(t->d_counters);
-    cudaFree(t->d_status);
-    cudaFree(t->d_rays);
-    cudaFree(t->d_hits);
-    cudaFree(t->d_mask);
-    cudaFree(t->d_wide);
-    cudaFree(t->d_cw_nodes);
-    cudaFree(t->d_cw_woop);
-    cudaFree(t->d_cw_triidx);
+    rb2::dev_free(t->d_nodes);
+    rb2::dev_free(t->d_woop);
+    rb2::dev_free(t->d_triidx);
+    rb2::dev_free(t->d_counters);
+    rb2::dev_free(t->d_status);
+    rb2::dev_free(t->d_rays);
+    rb2::dev_free(t->d_hits);
+    rb2::dev_free(t->d_mask);
+    rb2::dev_free(t->d_wide);
+    rb2::dev_free(t->d_cw_nodes);
+    rb2::dev_free(t->d_cw_woop);
+    rb2::dev_free(t->d_cw_triidx);
     delete t;
     return RB2_OK;
 }
@@ -469,9 +470,9 @@ int rb2_tracer_set_node_order(rb2_tracer* t, uint32_t order)
             if (3u * depth + 2u > (uint32_t)rb2dev::kStackSizeWide)
                 return fail(RB2_ENOTSUP, "tree too deep for the 4-wide layout's stack");
             float4* d = nullptr;
-            RB2_CUDA(cudaMalloc(&d, wide.size() * 4), "wide node allocation");
+            RB2_CUDA(rb2::dev_malloc(&d, wide.size() * 4), "wide node allocation");
             if (cudaMemcpy(d, wide.data(), wide.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
-                cudaFree(d);
+                rb2::dev_free(d);
                 return fail(RB2_ECUDA, "wide node upload");
             }
             t->d_wide = d;
@@ -531,13 +532,13 @@ int rb2_trace_host(rb2_tracer* t, const float* h_rays, uint32_t n, int any_hit, 
     std::unique_lock<std::mutex> g(t->mu);
     if (n > t->scratch_cap) {
         RB2_CUDA(cudaStreamSynchronize(s), "stream sync");
-        cudaFree(t->d_rays); cudaFree(t->d_hits); cudaFree(t->d_mask);
+        rb2::dev_free(t->d_rays); rb2::dev_free(t->d_hits); rb2::dev_free(t->d_mask);
         t->d_rays = nullptr; t->d_hits = nullptr; t->d_mask = nullptr;
         t->scratch_cap = 0;
         cudaError_t e;
-        if ((e = cudaMalloc(&t->d_rays, (size_t)n * 32)) != cudaSuccess ||
-            (e = cudaMalloc(&t->d_hits, (size_t)n * 16)) != cudaSuccess ||
-            (e = cudaMalloc(&t->d_mask, (size_t)n)) != cudaSuccess)
+        if ((e = rb2::dev_malloc(&t->d_rays, (size_t)n * 32)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&t->d_hits, (size_t)n * 16)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&t->d_mask, (size_t)n)) != cudaSuccess)
             return fail(RB2_ENOMEM, std::string("scratch allocation: ") + cudaGetErrorString(e));
         t->scratch_cap = n;
     }
@@ -672,11 +673,11 @@ int rb2_batch_create(const rb2_trace_job* jobs, uint32_t n_jobs, rb2_batch** out
     int rc = occupancy(b->occ);
     if (rc) return rc;
     cudaError_t e;
-    if ((e = cudaMalloc(&b->d_jobs, sizeof(rb2dev::JobDesc) * std::max<uint32_t>(1, n_jobs))) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_start, sizeof(unsigned long long) * (n_jobs + 1))) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_counter, sizeof(unsigned long long))) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_status, sizeof(unsigned int))) != cudaSuccess) {
-        cudaFree(b->d_jobs); cudaFree(b->d_start); cudaFree(b->d_counter); cudaFree(b->d_status);
+    if ((e = rb2::dev_malloc(&b->d_jobs, sizeof(rb2dev::JobDesc) * std::max<uint32_t>(1, n_jobs))) != cudaSuccess ||
+        (e = rb2::dev_malloc(&b->d_start, sizeof(unsigned long long) * (n_jobs + 1))) != cudaSuccess ||
+        (e = rb2::dev_malloc(&b->d_counter, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = rb2::dev_malloc(&b->d_status, sizeof(unsigned int))) != cudaSuccess) {
+        rb2::dev_free(b->d_jobs); rb2::dev_free(b->d_start); rb2::dev_free(b->d_counter); rb2::dev_free(b->d_status);
         return fail(RB2_ENOMEM, std::string("batch allocation: ") + cudaGetErrorString(e));
     }
     if (n_jobs) RB2_CUDA(cudaMemcpy(b->d_jobs, descs.data(), sizeof(rb2dev::JobDesc) * n_jobs, cudaMemcpyHostToDevice), "job upload");
@@ -690,10 +691,10 @@ int rb2_batch_destroy(rb2_batch* b)
 {
     if (!b) return RB2_OK;
     b->drop_graph();
-    cudaFree(b->d_jobs);
-    cudaFree(b->d_start);
-    cudaFree(b->d_counter);
-    cudaFree(b->d_status);
+    rb2::dev_free(b->d_jobs);
+    rb2::dev_free(b->d_start);
+    rb2::dev_free(b->d_counter);
+    rb2::dev_free(b->d_status);
     delete b;
     return RB2_OK;
 }
@@ -783,10 +784,10 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     RB2_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev), "L2 size");
     const size_t flush_bytes = std::max<size_t>(2 * (size_t)l2, 1 << 20);
     void* flush = nullptr;
-    if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) flush = nullptr;  // tune warm if memory is short
+    if (rb2::dev_malloc(&flush, flush_bytes) != cudaSuccess) flush = nullptr;  // tune warm if memory is short
     struct FlushFree {
         void* p;
-        ~FlushFree() { if (p) cudaFree(p); }
+        ~FlushFree() { if (p) rb2::dev_free(p); }
     } flush_guard{flush};
     auto time_cfg = [&](const rb2_batch_config& c, double& ms) -> int {
         int rc = rb2_batch_set_config(b, &c);
@@ -965,9 +966,9 @@ int rb2_pipeline_destroy(rb2_pipeline* p)
     if (!p) return RB2_OK;
     for (auto& s : p->slots) {
         if (s.stream) cudaStreamSynchronize(s.stream);
-        cudaFree(s.d_rays);
-        cudaFree(s.d_out);
-        cudaFree(s.d_mask);
+        rb2::dev_free(s.d_rays);
+        rb2::dev_free(s.d_out);
+        rb2::dev_free(s.d_mask);
         if (s.done) cudaEventDestroy(s.done);
         if (s.stream) cudaStreamDestroy(s.stream);
     }
@@ -992,9 +993,9 @@ int rb2_pipeline_create(uint64_t chunk_rays, uint32_t depth, rb2_pipeline** out)
         cudaError_t e;
         if ((e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaMalloc(&s.d_rays, chunk_rays * 32)) != cudaSuccess ||
-            (e = cudaMalloc(&s.d_out, chunk_rays * 16)) != cudaSuccess ||
-            (e = cudaMalloc(&s.d_mask, chunk_rays)) != cudaSuccess) {
+            (e = rb2::dev_malloc(&s.d_rays, chunk_rays * 32)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&s.d_out, chunk_rays * 16)) != cudaSuccess ||
+            (e = rb2::dev_malloc(&s.d_mask, chunk_rays)) != cudaSuccess) {
             rb2_pipeline_destroy(p.release());
             return fail(RB2_ENOMEM, std::string("pipeline staging: ") + cudaGetErrorString(e));
         }

@@ -31,7 +31,7 @@ class JobResult(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("fifo", C.c_uint32), ("hbm_budget", C.c_uint64), ("max_tile", C.c_uint32),
-                ("reserved", C.c_uint32), ("max_rays", C.c_uint64)]
+                ("job_timeout_ms", C.c_uint32), ("max_rays", C.c_uint64)]
 
 
 class ServerStats(C.Structure):
@@ -105,13 +105,14 @@ def pool_triangle_counts(n: int, lo: float, hi: float, seed: int) -> list[int]:
 
 
 class Server:
-    def __init__(self, pool: Pool, slots=8, fifo=False, hbm_budget=8 << 30, max_tile=1024, max_rays=4 << 20):
+    def __init__(self, pool: Pool, slots=8, fifo=False, hbm_budget=8 << 30, max_tile=1024, max_rays=4 << 20,
+                 job_timeout_ms=0):
         L = _lib()
         self.pool = pool
         n = len(pool.tracers)
         self._tr = (C.c_void_p * n)(*[t.handle.value for t in pool.tracers])
         self._sc = (C.c_void_p * n)(*[d.handle.value for d in pool.dscenes])
-        cfg = ServerConfig(slots, 1 if fifo else 0, hbm_budget, max_tile, 0, max_rays)
+        cfg = ServerConfig(slots, 1 if fifo else 0, hbm_budget, max_tile, job_timeout_ms, max_rays)
         self._s = C.c_void_p()
         check(L.rb2_server_create(self._tr, self._sc, n, C.byref(cfg), C.byref(self._s)))
 
@@ -121,11 +122,16 @@ class Server:
             _lib().rb2_server_destroy(s)
             self._s = C.c_void_p()
 
-    def run(self, jobs: "JobList"):
+    def run(self, jobs: "JobList", raise_on_error: bool = True):
+        """Serves the jobs; returns (per-job results, run stats).  With
+        raise_on_error=False a failing or timed-out job does not raise: its
+        status is in its result."""
         n = len(jobs.jobs)
         res = (JobResult * max(1, n))()
         st = ServerStats()
-        check(_lib().rb2_server_run(self._s, jobs.array, n, res, C.byref(st)))
+        rc = _lib().rb2_server_run(self._s, jobs.array, n, res, C.byref(st))
+        if raise_on_error:
+            check(rc)
         return [res[i] for i in range(n)], {k: getattr(st, k) for k, _ in ServerStats._fields_}
 
 

@@ -131,3 +131,44 @@ def test_shared_buffer_jobs_equal_direct_traces(pool, cuda):
             else:
                 assert torch.equal(out(a, i), pool.tracers[j.bvh].trace_occlusion(d).cpu())
     assert 0 < n_ray < n
+
+
+def test_job_deadline_times_out_one_job_and_the_loop_goes_on(pool, cuda, rb):
+    """A served job whose stream is held up past its deadline (a host function
+    that sleeps on the slot's stream, injected on the host) gets RB2_ETIMEOUT;
+    the other jobs, admitted on the other slots meanwhile, complete with the
+    same outputs as direct traces, and the run returns only after the stalled
+    slot has drained."""
+    import ctypes as C
+
+    from renderbox2_b200.serve import JobList, Server
+    L = rb.lib()
+    L.rb2_debug_stall_next_job.argtypes = [C.c_uint32]
+    jl = JobList()
+    keep = []
+    for k in range(10):
+        rays, _ = rb.surface_rays(pool.scenes[k % 3], seed=700 + k, n=20_000)
+        rays[::2, 4:7] *= -1.0
+        jl.add_rays(k % 3, rays, mode=0, arrival=0.0 if k == 0 else 0.02 + 0.01 * k)
+        keep.append(rays)
+    srv = Server(pool, slots=3, max_tile=64, max_rays=64 * 1024, job_timeout_ms=300)
+    assert L.rb2_debug_stall_next_job(1500) == 0
+    res, st = srv.run(jl, raise_on_error=False)
+    assert res[0].status == 6, "the stalled job must report RB2_ETIMEOUT"
+    assert 0.25 < res[0].latency_s < 1.2, res[0].latency_s
+    assert st["wall_s"] >= 1.4, "the run must wait for the stalled slot to drain"
+    for k in range(1, 10):
+        assert res[k].status == 0, (k, res[k].status)
+        direct = pool.tracers[k % 3].trace(cuda.from_numpy(keep[k]).cuda()).cpu()
+        assert cuda.equal(jl.outputs[k], direct), f"job {k}"
+    # the server is usable afterwards, with no stall
+    res2, _ = srv.run(jl.subset(range(3)))
+    assert all(r.status == 0 for r in res2)
+
+
+def test_server_rejects_more_slots_than_queue_heads(pool, cuda, rb):
+    from renderbox2_b200._native import Rb2Error
+    from renderbox2_b200.serve import Server
+    with pytest.raises(Rb2Error) as e:
+        Server(pool, slots=257, max_tile=64, max_rays=64 * 1024)
+    assert e.value.code == 1 and "256" in str(e.value)

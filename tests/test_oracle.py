@@ -263,3 +263,48 @@ def test_raycast_shade_rules(orc):
     xy = orc.jittered_raster(7, 3, 2, 11)
     base = np.tile(np.stack([np.arange(21) % 7, np.arange(21) // 7], 1), (2, 1))
     assert ((xy - base >= 0) & (xy - base < 1)).all()
+
+
+@pytest.mark.parametrize("seed,tris", [(4000, 1_000), (4017, 40_000), (4040, 300_000)])
+def test_oracle_workload_generator_equals_product_generator(rb, orc, seed, tris):
+    """The CPU reference arm builds the batching workload without the product
+    library; its generator must give the product's scenes and rays bit for bit."""
+    sc = rb.heightfield_for_triangles(seed=seed, n_tris=tris)
+    v, i = orc.gen_heightfield_for_triangles(seed, tris)
+    assert np.array_equal(v.view(np.uint32), sc.vertices.view(np.uint32))
+    assert np.array_equal(i, sc.indices)
+    r1, f1 = rb.surface_rays(sc, seed=seed + 500, n=150_000)
+    r2, f2 = orc.gen_surface_rays(v, i, seed + 500, 150_000)
+    assert np.array_equal(r1.view(np.uint32), r2.view(np.uint32))
+    assert np.array_equal(f1, f2)
+
+
+def test_tie_scene_produces_ties_on_both_trees(rb, orc):
+    """Rays through shared edges and vertices of dyadic geometry: most are
+    accepted by 2-6 triangles at the same t; the traversal's pick is one of
+    them; the BVH-walking tie count never exceeds the exhaustive one."""
+    from tie_scene import tie_rays, tie_scene
+    scene = tie_scene(rb)
+    rays, kinds = tie_rays()
+    bvh = rb.BVH(scene)  # buffers_view() borrows the BVH's memory: keep it alive
+    trees = [bvh.buffers_view()]
+    if orc.have_ref():
+        r = orc.ref_build(scene.vertices, scene.indices)
+        trees.append((r["nodes"], r["woop"], r["triidx"]))
+    for nodes, woop, tri in trees:
+        h = orc.trace(nodes, woop, tri, rays)
+        assert (h["prim"] >= 0).all()
+        exact = orc.tie_count(woop, tri, rays, h)
+        walked = orc.tie_count(woop, tri, rays, h, nodes=nodes)
+        assert (exact >= 1).all(), "the reported triangle must accept at its own t"
+        assert (walked <= exact).all()
+        assert (exact >= 2).mean() > 0.5
+        for k in ("vertex", "edge", "diagonal", "box_edge", "box_corner"):
+            assert (exact[kinds == k] >= 2).any(), k
+        # The exhaustive search agrees with the traversal on t, except where
+        # an axis-parallel ray runs exactly in a box's boundary plane: the
+        # slab test (zero direction replaced by +-2^-80) culls that box, as
+        # the reference's traversal does, so the traversal's t is larger.
+        bf = orc.bruteforce(woop, tri, rays)
+        assert (h["t"] >= bf["t"]).all()
+        assert (h["t"] == bf["t"]).mean() > 0.99

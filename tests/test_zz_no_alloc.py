@@ -6,9 +6,11 @@ must not appear).
 The caller owns every buffer: here the BVH, rays and outputs live in torch
 tensors allocated by the test, and the library uses only its fixed
 file-scope scratch array.  Results must equal the regular batched entry point
-(rb2_batch_create / rb2_batch_launch) bit for bit, on two calls in a row
-(the scratch array keeps the previous call's contents, so the second call
-checks that it is cleared correctly).  Collected last on purpose."""
+(rb2_batch_create / rb2_batch_launch) bit for bit and the CPU oracle, on two
+calls in a row (the scratch array keeps the previous call's contents, so the
+second call checks that it is cleared correctly), and the guard-bit query
+(rb2_trace_batch_noalloc_status) must read 0 after each.  Collected last on
+purpose."""
 import ctypes as C
 
 import numpy as np
@@ -30,6 +32,16 @@ def _bind(rb):
     return fn
 
 
+def _status(rb, stream):
+    """Guard bits of the last call, read through rb2_trace_batch_noalloc_status."""
+    fn = rb.lib().rb2_trace_batch_noalloc_status
+    fn.argtypes = [C.POINTER(C.c_uint32), C.c_void_p]
+    fn.restype = C.c_int
+    word = C.c_uint32(0xFFFFFFFF)
+    assert fn(C.byref(word), stream) == 0, rb.lib().rb2_last_error()
+    return word.value
+
+
 def _caller_owned_bvh(torch, bvh):
     """Uploads a BVH into tensors the caller owns (Woop rows + 2 spare uint4)."""
     nodes, woop, tri = bvh.buffers_view()
@@ -47,12 +59,12 @@ def _out_like(torch, n, mode):
     return torch.full((n, 4), 9, dtype=torch.int32, device="cuda")
 
 
-def test_noalloc_matches_batched_entry_point_twice(rb, cuda):
+def test_noalloc_matches_batched_entry_point_twice(rb, orc, cuda):
     torch = cuda
     fn = _bind(rb)
     specs = [(3_000, 40_000, rb.MODE_CLOSEST), (80_000, 100_000, rb.MODE_OCCLUSION), (500, 7, rb.MODE_ANY),
              (20_000, 65_536, rb.MODE_CLOSEST)]
-    keep, ref_jobs, ref_outs = [], [], []
+    keep, ref_jobs, ref_outs, host_rays = [], [], [], []
     na = (NoAllocJob * len(specs))()
     for k, (tris, n, mode) in enumerate(specs):
         sc = rb.heightfield_for_triangles(seed=600 + k, n_tris=tris, n_boxes=4)
@@ -61,6 +73,7 @@ def test_noalloc_matches_batched_entry_point_twice(rb, cuda):
         r, _ = rb.surface_rays(sc, seed=650 + k, n=n)
         r[::2, 4:7] *= -1.0
         d_rays = torch.from_numpy(r).cuda()
+        host_rays.append(r)
         ref_out = _out_like(torch, n, mode)
         ref_jobs.append((tr, d_rays, mode, ref_out, None))
         ref_outs.append(ref_out)
@@ -85,9 +98,22 @@ def test_noalloc_matches_batched_entry_point_twice(rb, cuda):
             na[k].d_out = o.data_ptr()
         rc = fn(na, len(specs), stream)
         assert rc == 0, rb.lib().rb2_last_error()
+        assert _status(rb, stream) == 0, "guard bits set by a no-alloc call"
         torch.cuda.synchronize()
         for k, (o, ref) in enumerate(zip(outs, ref_outs)):
             assert torch.equal(o, ref), f"call {call}, job {k} differs from rb2_batch_launch"
+        # and directly against the CPU oracle on the same buffers
+        for k, ((tris, n, mode), o) in enumerate(zip(specs, outs)):
+            nodes, woop, tri = keep[k][0].buffers_view()
+            want = orc.trace(nodes, woop, tri, host_rays[k], any_hit=(mode != rb.MODE_CLOSEST))
+            got = o.cpu().numpy()
+            if mode == rb.MODE_OCCLUSION:
+                assert np.array_equal(got.astype(bool), want["prim"] >= 0), f"call {call}, job {k}"
+            elif mode == rb.MODE_ANY:
+                assert np.array_equal(got[:, 0] >= 0, want["prim"] >= 0), f"call {call}, job {k}"
+            else:
+                assert np.array_equal(got[:, 0], want["prim"]), f"call {call}, job {k}"
+                assert np.array_equal(got[:, 1].view(np.uint32), want["t"].view(np.uint32)), f"call {call}, job {k}"
     # closest-hit job sanity: real hits were produced
     assert (ref_outs[0][:, 0] >= 0).float().mean().item() > 0.3
 
