@@ -185,6 +185,27 @@ int rb2_integrator_set_wave(rb2_integrator* it, uint64_t paths);
 /* Film filter of the path tracer, BDPT and ray casting (default RB2_FILTER_NONE); NULL resets. */
 int rb2_integrator_set_filter(rb2_integrator* it, const rb2_filter* f);
 
+/* Reference-compatibility switches (the `compat` fields below).  By default
+ * the integrators correct four behaviours of the reference; each switch
+ * reproduces one of them instead, so an image can be compared with what the
+ * reference's own kernels would produce (in expectation: the random numbers
+ * come from this library's generator, not thrust's).
+ *  RB2_COMPAT_AO_DIRECTION  AO rays along X cos(phi) sin(theta) + Y sin(phi)
+ *      sin(theta) + Z cos(phi), phi = 2 pi u1, theta = acos(sqrt(1 - u2)),
+ *      about the unflipped geometric normal with the reference's choice of
+ *      X and Y (core/montecarlo.cu:133-151): neither unit length nor
+ *      cosine-distributed; tmax stays `radius` in units of that direction.
+ *      Where X is undefined (a normal along +z or -z, whose cross product
+ *      with the chosen axis vanishes) the reference's ray is NaN and never
+ *      hits: the sample counts as unoccluded.
+ *  RB2_COMPAT_RR_DIVISOR  Russian roulette from bounce rr_start + 1, and
+ *      survivors divided by 1 - q instead of q (integrator_path.cu:232-244);
+ *      needs rr_prob < 1.
+ *  RB2_COMPAT_NEE_RESEED  next-event estimation draws the same light choice
+ *      and point at every vertex of a path (the reference re-seeds its NEE
+ *      generator each bounce, integrator_path.cu:113). */
+enum { RB2_COMPAT_AO_DIRECTION = 1u << 0, RB2_COMPAT_RR_DIVISOR = 1u << 1, RB2_COMPAT_NEE_RESEED = 1u << 2 };
+
 /* Ambient occlusion (AmbientOcclusionIntegratorParams, core/params.h:126-131;
  * integrators/integrator_ao.cu:42-110): one primary ray per pixel centre,
  * `samples` any-hit rays per hit from the hit point (tmin = 1e-3 t, tmax =
@@ -194,6 +215,8 @@ typedef struct {
     uint32_t samples;
     float radius;
     uint64_t seed;
+    uint32_t compat;         /* RB2_COMPAT_AO_DIRECTION or 0 */
+    uint32_t reserved;
 } rb2_ao_params;
 int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params* p, float* d_ao, void* stream);
 
@@ -216,7 +239,7 @@ typedef struct {
     float rr_prob;
     uint64_t seed;
     uint32_t spp_per_wave;   /* samples per pixel in flight at once (0 = auto) */
-    uint32_t reserved;
+    uint32_t compat;         /* RB2_COMPAT_RR_DIVISOR | RB2_COMPAT_NEE_RESEED, or 0 */
 } rb2_pt_params;
 int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, float* d_rgb, void* stream);
 
@@ -265,6 +288,67 @@ typedef struct {
     uint64_t seed;
 } rb2_bdpt_params;
 int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_params* p, float* d_rgb, void* stream);
+
+/* The reference's full BidirectionalPathIntegratorLvcParams (core/params.h:108-120,
+ * read from its integrator file by config/configuration.cpp:251-300), plus
+ * the estimator choice.
+ *
+ * RB2_BDPT_ESTIMATOR_UNBIASED: the estimator of rb2_render_bdpt above, with
+ *   max_path_length the whole-path cap, light_path_rrstart and
+ *   cam_path_rrstart the bounces from which each subpath plays Russian
+ *   roulette (continue probability min(cam_path_rrprob, luminance)), and the
+ *   two max-depth fields unused (the whole-path cap bounds both subpaths).
+ * RB2_BDPT_ESTIMATOR_REFERENCE: the reference's own estimator
+ *   (integrators/integrator_bdpt_lvc_sk.cu:47-514), field for field:
+ *   - a preparation pass of num_prep_paths light subpaths sizes the cache at
+ *     ceil(1.1 * mean stored vertices per path * num_light_paths) vertices;
+ *     a light subpath stops storing once the cache is full (the cache keeps
+ *     the first vertices in (path, depth) order);
+ *   - light subpaths start as DiffuseAreaLight::Le does (core/lights.cu:63-69):
+ *     a direction drawn uniformly from the hemisphere about world +z and
+ *     negated, contribution Le / pdf with no factor for the choice of
+ *     emissive triangle; they store every surface vertex they hit and play
+ *     roulette at every bounce with continue probability
+ *     min(1, luminance(f |cos| / pdf)), and stop when their contribution is
+ *     black.  The reference never caps their length; here they keep at most
+ *     num_light_path_max_depth vertices (its integrator file: 8), which bounds
+ *     the cache;
+ *   - camera vertices 0..num_cam_path_max_depth add emission (first vertex or
+ *     after a specular bounce, full weight), next-event estimation at full
+ *     weight with the same draws at every vertex (the reference re-seeds each
+ *     bounce), and num_cam_path_connections connections to uniformly chosen
+ *     cached vertices, each weighted 1 / ((bounce + 1) + depth of the cached
+ *     vertex) with no cache-size factor;
+ *   - camera Russian roulette from bounce cam_path_rrstart + 1 with continue
+ *     probability min(cam_path_rrprob, luminance) and survivors divided by
+ *     1 - that probability (needs cam_path_rrprob < 1);
+ *   - light_path_rrstart and num_cam_path_sample_connections are accepted and,
+ *     as in the reference's kernels, not used; mode (sk, mk, sort) selects
+ *     among three kernel organisations of one estimator there, and this
+ *     wavefront implementation runs that estimator for each.
+ *   The light point of a subpath starts 1e-4 off the light (the reference's
+ *   ray starts on it and can hit its own light at a rounding-level t). */
+enum { RB2_BDPT_ESTIMATOR_UNBIASED = 0, RB2_BDPT_ESTIMATOR_REFERENCE = 1 };
+enum { RB2_BDPT_MODE_SK = 0, RB2_BDPT_MODE_MK = 1, RB2_BDPT_MODE_SORT = 2 };
+typedef struct {
+    uint32_t spp;                              /* iterations (one camera sample per pixel each) */
+    uint32_t num_prep_paths;                   /* m_num_prep_paths (reference estimator; 0 = no cap) */
+    uint32_t num_light_paths;                  /* m_num_light_paths per iteration (0 = one per pixel) */
+    uint32_t num_light_path_max_depth;         /* m_num_light_path_max_depth (reference estimator) */
+    uint32_t light_path_rrstart;               /* m_light_path_rrstart */
+    uint32_t num_cam_path_max_depth;           /* m_num_cam_path_max_depth (reference estimator) */
+    uint32_t cam_path_rrstart;                 /* m_cam_path_rrstart */
+    float cam_path_rrprob;                     /* m_cam_path_rrprob */
+    uint32_t num_cam_path_sample_connections;  /* m_num_cam_path_sample_connections (sample_M) */
+    uint32_t num_cam_path_connections;         /* m_num_cam_path_connections (sample_N), 1..8 */
+    uint32_t mode;                             /* m_mode: RB2_BDPT_MODE_* */
+    uint32_t estimator;                        /* RB2_BDPT_ESTIMATOR_* */
+    uint32_t max_path_length;                  /* unbiased estimator: segments camera to light, 1..16 */
+    uint32_t reserved;
+    uint64_t seed;
+} rb2_bdpt_lvc_params;
+int rb2_render_bdpt_lvc(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_lvc_params* p, float* d_rgb,
+                        void* stream);
 
 /* Ray casting (RayCastIntegratorParams / RayCastShade, core/params.h:139-151;
  * IntegratorRayCast::compute and kernel_ray_cast_update,

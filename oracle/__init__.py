@@ -346,6 +346,52 @@ def gen_surface_rays(vertices, indices, seed: int, n: int, offset_scale: float =
     return rays, flags
 
 
+def ao_ref_dir(normal, u1, u2):
+    """The reference's AO direction formula (oracle restatement, double);
+    None where the reference's direction is NaN."""
+    L = orc_lib()
+    L.rb2o_ao_ref_dir.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_void_p]
+    L.rb2o_ao_ref_dir.restype = C.c_int
+    n = np.ascontiguousarray(normal, np.float64)
+    out = np.zeros(3, np.float64)
+    return out if L.rb2o_ao_ref_dir(_p(n), float(u1), float(u2), _p(out)) else None
+
+
+def light_le_ref(light_normal, area, u3, u4):
+    """DiffuseAreaLight::Le's direction and Le / pdf factor (oracle restatement)."""
+    L = orc_lib()
+    L.rb2o_light_le_ref.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p,
+                                    C.POINTER(C.c_double)]
+    L.rb2o_light_le_ref.restype = None
+    n = np.ascontiguousarray(light_normal, np.float64)
+    d = np.zeros(3, np.float64)
+    k = C.c_double()
+    L.rb2o_light_le_ref(_p(n), float(area), float(u3), float(u4), _p(d), C.byref(k))
+    return d, k.value
+
+
+def ref_ao_direction(normal, u1, u2):
+    """The reference's compiled cosine_sample_hemisphere_normal (float)."""
+    L = ref_lib()
+    L.rb2ref_ao_direction.argtypes = [C.c_float, C.c_float, C.c_void_p, C.c_void_p]
+    L.rb2ref_ao_direction.restype = C.c_int
+    n = np.ascontiguousarray(normal, np.float32)
+    out = np.zeros(3, np.float32)
+    L.rb2ref_ao_direction(float(u1), float(u2), _p(n), _p(out))
+    return out
+
+
+def ref_light_le(v0, v1, v2, emit, u5):
+    """The reference's compiled DiffuseAreaLight::Le: (point, direction, pdf, L)."""
+    L = ref_lib()
+    L.rb2ref_light_le.argtypes = [C.c_void_p] * 9
+    L.rb2ref_light_le.restype = C.c_int
+    a = [np.ascontiguousarray(x, np.float32) for x in (v0, v1, v2, emit, u5)]
+    pt, d, pdf, Lo = np.zeros(3, np.float32), np.zeros(3, np.float32), np.zeros(1, np.float32), np.zeros(3, np.float32)
+    L.rb2ref_light_le(*[_p(x) for x in a], _p(pt), _p(d), _p(pdf), _p(Lo))
+    return pt, d, float(pdf[0]), Lo
+
+
 def woop_slots_of(woop, triidx):
     """Map from triangle id to its first Woop slot (for tie checks)."""
     w = np.asarray(woop, np.uint32).reshape(-1, 4)
@@ -451,11 +497,12 @@ def _bvh_struct(nodes, woop, triidx):
     return _Bvh(*[_p(k) for k in keep]), keep
 
 
-def ao(bvh_buffers, vertices, indices, prim_rays, samples, radius, seed=1, nthreads=0):
-    """FP64 ambient occlusion per primary ray (see rb2_oracle.h)."""
+def ao(bvh_buffers, vertices, indices, prim_rays, samples, radius, seed=1, nthreads=0, compat=0):
+    """FP64 ambient occlusion per primary ray (see rb2_oracle.h); compat=1:
+    the reference's AO direction formula."""
     L = orc_lib()
     L.rb2o_ao.argtypes = [C.POINTER(_Bvh), C.POINTER(_Scene), C.c_void_p, C.c_uint32, C.c_uint32, C.c_float,
-                          C.c_uint64, C.c_void_p, C.c_int]
+                          C.c_uint64, C.c_uint32, C.c_void_p, C.c_int]
     L.rb2o_ao.restype = None
     n_tri = np.asarray(indices).reshape(-1, 3).shape[0]
     s, ks = _scene_struct(vertices, indices, np.zeros(n_tri, np.uint32), np.zeros((1, 3), np.float32),
@@ -463,23 +510,25 @@ def ao(bvh_buffers, vertices, indices, prim_rays, samples, radius, seed=1, nthre
     b, kb = _bvh_struct(*bvh_buffers)
     r = np.ascontiguousarray(prim_rays, np.float32).reshape(-1, 8)
     out = np.empty(r.shape[0], np.float64)
-    L.rb2o_ao(C.byref(b), C.byref(s), _p(r), r.shape[0], samples, radius, seed, _p(out), nthreads)
+    L.rb2o_ao(C.byref(b), C.byref(s), _p(r), r.shape[0], samples, radius, seed, compat, _p(out), nthreads)
     return out
 
 
 def pt(bvh_buffers, vertices, indices, tri_mat, albedo, emission, lights, rays, max_depth, rr_start, rr_prob,
-       seed=1, nthreads=0, materials=None):
+       seed=1, nthreads=0, materials=None, compat=0):
     """One FP64 path-traced sample per camera ray; returns (n, 3) radiance.
-    `materials` (optional): layered material descriptions per material."""
+    `materials` (optional): layered material descriptions per material.
+    compat: 2 = the reference's roulette divisor, 4 = its NEE re-seeding."""
     L = orc_lib()
     L.rb2o_pt.argtypes = [C.POINTER(_Bvh), C.POINTER(_Scene), C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
-                          C.c_float, C.c_uint64, C.c_void_p, C.c_int]
+                          C.c_float, C.c_uint64, C.c_uint32, C.c_void_p, C.c_int]
     L.rb2o_pt.restype = None
     s, ks = _scene_struct(vertices, indices, tri_mat, albedo, emission, lights, materials)
     b, kb = _bvh_struct(*bvh_buffers)
     r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
     out = np.empty((r.shape[0], 3), np.float64)
-    L.rb2o_pt(C.byref(b), C.byref(s), _p(r), r.shape[0], max_depth, rr_start, rr_prob, seed, _p(out), nthreads)
+    L.rb2o_pt(C.byref(b), C.byref(s), _p(r), r.shape[0], max_depth, rr_start, rr_prob, seed, compat, _p(out),
+              nthreads)
     return out
 
 
@@ -504,6 +553,32 @@ def bdpt(bvh_buffers, vertices, indices, tri_mat, albedo, emission, lights, cam_
 
 
 C_ = C
+
+
+class _BdptRefParams(C.Structure):
+    _fields_ = [("n_prep", C.c_uint32), ("n_light_paths", C.c_uint32), ("light_max_depth", C.c_uint32),
+                ("cam_max_depth", C.c_uint32), ("cam_rrstart", C.c_uint32), ("connections", C.c_uint32),
+                ("cam_rrprob", C.c_float)]
+
+
+def bdpt_ref(bvh_buffers, vertices, indices, tri_mat, albedo, emission, lights, cam_rays, n_cam, n_iter,
+             n_prep, n_light_paths, light_max_depth, cam_max_depth, cam_rrstart, cam_rrprob, connections, seed=1,
+             nthreads=0, materials=None):
+    """FP64 restatement of the reference's own BDPT estimator
+    (integrators/integrator_bdpt_lvc_sk.cu; see rb2_oracle.h): mean radiance
+    per camera pixel over n_iter iterations (cam_rays iteration-major)."""
+    L = orc_lib()
+    L.rb2o_bdpt_ref.argtypes = [C.POINTER(_Bvh), C.POINTER(_Scene), C.c_void_p, C.c_uint32, C.c_uint32,
+                                C.POINTER(_BdptRefParams), C.c_uint64, C.c_void_p, C.c_int]
+    L.rb2o_bdpt_ref.restype = None
+    s, ks = _scene_struct(vertices, indices, tri_mat, albedo, emission, lights, materials)
+    b, kb = _bvh_struct(*bvh_buffers)
+    r = np.ascontiguousarray(cam_rays, np.float32).reshape(-1, 8)
+    assert r.shape[0] == n_cam * n_iter
+    p = _BdptRefParams(n_prep, n_light_paths, light_max_depth, cam_max_depth, cam_rrstart, connections, cam_rrprob)
+    out = np.empty((n_cam, 3), np.float64)
+    L.rb2o_bdpt_ref(C.byref(b), C.byref(s), _p(r), n_cam, n_iter, C.byref(p), seed, _p(out), nthreads)
+    return out
 
 
 # ---- ray casting ---------------------------------------------------------------------

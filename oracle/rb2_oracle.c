@@ -584,8 +584,42 @@ static inline int occluded_t(const rb2o_bvh* b, const float* r8, int type)
 }
 #define occluded(b, r8) occluded_t((b), (r8), RB2O_RAY_SHADOW)
 
+/* The reference's AO direction (core/montecarlo.cu:133-151) about n:
+ * returns 0 when its X axis is undefined (n along the axis its signed
+ * comparisons pick), where the reference's direction is NaN. */
+int rb2o_ao_ref_dir(const double* n3, double u1, double u2, double* out3)
+{
+    d3 ng = D3(n3[0], n3[1], n3[2]);
+    d3 perp = D3(0, 0, 1);
+    if (ng.x < ng.y && ng.x < ng.z) perp = D3(1, 0, 0);
+    else if (ng.y < ng.x && ng.y < ng.z) perp = D3(0, 1, 0);
+    d3 cx = dcross(ng, perp);
+    if (!(ddot(cx, cx) > 0.0)) return 0;
+    d3 X = dnorm(cx), Y = dnorm(dcross(ng, X));
+    double phi = 2.0 * RB2O_PI * u1, theta = acos(sqrt(1.0 - u2));
+    d3 w = dadd(dadd(dmul(X, cos(phi) * sin(theta)), dmul(Y, sin(phi) * sin(theta))), dmul(ng, cos(phi)));
+    out3[0] = w.x; out3[1] = w.y; out3[2] = w.z;
+    return 1;
+}
+
+/* DiffuseAreaLight::Le's direction and contribution factor (core/lights.cu:63-69):
+ * direction uniform over the hemisphere about world +z (z = u3, phi = 2 pi u4),
+ * negated when its dot product with the light normal ln is nonzero; the
+ * contribution Le / pdf is Le x k, k = area 2 pi cos for cos = ln . dir > 0,
+ * else 0. */
+void rb2o_light_le_ref(const double* ln3, double area, double u3, double u4, double* dir3, double* k)
+{
+    d3 ln = D3(ln3[0], ln3[1], ln3[2]);
+    double hr = sqrt(u3 < 1.0 ? 1.0 - u3 * u3 : 0.0), phi = 2.0 * RB2O_PI * u4;
+    d3 dir = D3(hr * cos(phi), hr * sin(phi), u3);
+    if (ddot(dir, ln) != 0.0) dir = dmul(dir, -1.0);
+    double c = ddot(ln, dir);
+    dir3[0] = dir.x; dir3[1] = dir.y; dir3[2] = dir.z;
+    *k = c > 0.0 ? area * 2.0 * RB2O_PI * c : 0.0;
+}
+
 void rb2o_ao(const rb2o_bvh* b, const rb2o_scene* s, const float* prim_rays, uint32_t n, uint32_t samples,
-             float radius, uint64_t seed, double* out, int nthreads)
+             float radius, uint64_t seed, uint32_t compat, double* out, int nthreads)
 {
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
@@ -600,8 +634,27 @@ void rb2o_ao(const rb2o_bvh* b, const rb2o_scene* s, const float* prim_rays, uin
         d3 v0 = vtx(s, t[0]), v1 = vtx(s, t[1]), v2 = vtx(s, t[2]);
         d3 ng = dnorm(dcross(dsub(v1, v0), dsub(v2, v0)));
         d3 d = D3(r[4], r[5], r[6]);
-        if (ddot(ng, d) > 0.0) ng = dmul(ng, -1.0);
         d3 pos = dadd(D3(r[0], r[1], r[2]), dmul(d, h.t));
+        if (compat & 1u) {
+            /* The reference's direction formula about the unflipped normal. */
+            const double n3[3] = {ng.x, ng.y, ng.z};
+            uint64_t open = 0;
+            for (uint32_t k = 0; k < samples; k++) {
+                uint64_t key = (uint64_t)i * samples + k;
+                double w3[3];
+                if (!rb2o_ao_ref_dir(n3, u01(seed, key, 0), u01(seed, key, 1), w3)) {
+                    open++;  /* the reference's direction is NaN: no hit */
+                    continue;
+                }
+                d3 w = D3(w3[0], w3[1], w3[2]);
+                float r8[8];
+                mkray(r8, pos, 1.0e-3 * (double)h.t, w, radius);
+                if (!occluded(b, r8)) open++;
+            }
+            out[i] = (double)open / (double)samples;
+            continue;
+        }
+        if (ddot(ng, d) > 0.0) ng = dmul(ng, -1.0);
         d3 fx, fy;
         frame(ng, &fx, &fy);
         uint64_t open = 0;
@@ -841,8 +894,23 @@ static int has_nondelta(const rb2o_material* m)
     return 0;
 }
 
+/* Russian roulette after the BSDF sample at bounce bnc: from bounce rr_start
+ * dividing survivors by q, or (compat bit 2) from rr_start + 1 dividing by
+ * 1 - q (integrator_path.cu:232-244).  Returns 0 when the path ends. */
+static int rr_step(double* T, uint32_t bnc, uint32_t rr_start, float rr_prob, uint32_t compat, double u)
+{
+    const int ref = (compat & 2u) != 0;
+    if (ref ? bnc <= rr_start : bnc < rr_start) return 1;
+    double lum = 0.212671 * T[0] + 0.715160 * T[1] + 0.072169 * T[2];
+    double q = lum < rr_prob ? lum : rr_prob;
+    if (!(u < q)) return 0;
+    double div = ref ? 1.0 - q : q;
+    for (int c = 0; c < 3; c++) T[c] /= div;
+    return 1;
+}
+
 void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t n, uint32_t max_depth,
-             uint32_t rr_start, float rr_prob, uint64_t seed, double* out_rgb, int nthreads)
+             uint32_t rr_start, float rr_prob, uint64_t seed, uint32_t compat, double* out_rgb, int nthreads)
 {
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
@@ -879,6 +947,9 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
                 break;
             }
             uint64_t key = (uint64_t)i * 64 + bnc;
+            /* NEE draws: this vertex's, or (compat bit 4) the first vertex's at every
+             * vertex, as the reference re-seeds its NEE generator (integrator_path.cu:113). */
+            uint64_t nkey = (compat & 4u) ? (uint64_t)i * 64 : key;
             if (s->materials && !plain_lambertian(&s->materials[m])) {
                 /* Layered material: NEE with material_f / material_pdf (skipped for
                  * purely specular materials), continuation by material_sample_f;
@@ -887,12 +958,12 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
                 frame3 fr = frame_z(ng);
                 d3 wo_l = fr_local(&fr, wo);
                 if (s->n_lights && has_nondelta(mt)) {
-                    uint32_t j = (uint32_t)(u01(seed, key, 0) * s->n_lights);
+                    uint32_t j = (uint32_t)(u01(seed, nkey, 0) * s->n_lights);
                     if (j >= s->n_lights) j = s->n_lights - 1;
                     const uint32_t lt = s->lights[j];
                     const uint32_t* lv = s->tris + 3 * (size_t)lt;
                     d3 l0 = vtx(s, lv[0]), l1 = vtx(s, lv[1]), l2 = vtx(s, lv[2]);
-                    double su = sqrt(u01(seed, key, 1)), u2 = u01(seed, key, 2);
+                    double su = sqrt(u01(seed, nkey, 1)), u2 = u01(seed, nkey, 2);
                     double b0 = 1.0 - su, b1 = u2 * su;
                     d3 lp = dadd(dadd(dmul(l0, b0), dmul(l1, b1)), dmul(l2, 1.0 - b0 - b1));
                     d3 ln = dnorm(dcross(dsub(l1, l0), dsub(l2, l0)));
@@ -929,24 +1000,19 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
                 double k = fabs(ddot(wi, ng)) / pdf;
                 T[0] *= f.x * k; T[1] *= f.y * k; T[2] *= f.z * k;
                 pdf_prev = spec ? -1.0 : pdf;
-                if (bnc >= rr_start) {
-                    double lum = 0.212671 * T[0] + 0.715160 * T[1] + 0.072169 * T[2];
-                    double q = lum < rr_prob ? lum : rr_prob;
-                    if (!(u01(seed, key, 5) < q)) break;
-                    for (int c2 = 0; c2 < 3; c2++) T[c2] /= q;
-                }
+                if (!rr_step(T, bnc, rr_start, rr_prob, compat, u01(seed, key, 5))) break;
                 mkray(ray, pos, eps, wi, 3.402823466e+38);
                 continue;
             }
             d3 nrm = ddot(ng, wo) < 0.0 ? dmul(ng, -1.0) : ng;
             const float* A = s->albedo + 3 * (size_t)m;
             if (s->n_lights) {
-                uint32_t j = (uint32_t)(u01(seed, key, 0) * s->n_lights);
+                uint32_t j = (uint32_t)(u01(seed, nkey, 0) * s->n_lights);
                 if (j >= s->n_lights) j = s->n_lights - 1;
                 const uint32_t lt = s->lights[j];
                 const uint32_t* lv = s->tris + 3 * (size_t)lt;
                 d3 l0 = vtx(s, lv[0]), l1 = vtx(s, lv[1]), l2 = vtx(s, lv[2]);
-                double su = sqrt(u01(seed, key, 1)), u2 = u01(seed, key, 2);
+                double su = sqrt(u01(seed, nkey, 1)), u2 = u01(seed, nkey, 2);
                 double b0 = 1.0 - su, b1 = u2 * su;
                 d3 lp = dadd(dadd(dmul(l0, b0), dmul(l1, b1)), dmul(l2, 1.0 - b0 - b1));
                 d3 ln = dnorm(dcross(dsub(l1, l0), dsub(l2, l0)));
@@ -975,12 +1041,7 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
             for (int c = 0; c < 3; c++) T[c] *= A[c];
             pdf_prev = pdf;
             if (T[0] <= 0.0 && T[1] <= 0.0 && T[2] <= 0.0) break;
-            if (bnc >= rr_start) {
-                double lum = 0.212671 * T[0] + 0.715160 * T[1] + 0.072169 * T[2];
-                double q = lum < rr_prob ? lum : rr_prob;
-                if (!(u01(seed, key, 5) < q)) break;
-                for (int c = 0; c < 3; c++) T[c] /= q;
-            }
+            if (!rr_step(T, bnc, rr_start, rr_prob, compat, u01(seed, key, 5))) break;
             mkray(ray, pos, eps, wi, 3.402823466e+38);
         }
         for (int c = 0; c < 3; c++) out_rgb[3 * i + c] = L[c];
@@ -1289,6 +1350,316 @@ void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, ui
     }
     free(sparse);
     free(valid);
+    free(dense);
+    (void)nthreads;
+}
+
+/* ---- the reference's BDPT estimator (see rb2_oracle.h) ----------------------------- */
+typedef struct { d3 pos, nrm, beta, wi, ng; uint32_t depth, mat; } ref_vertex;
+
+/* One light subpath of the reference estimator; stores its vertices in
+ * out[0 .. return value).  Keys: light salt, `key`. */
+static uint32_t ref_light_path(const rb2o_bvh* b, const rb2o_scene* s, uint64_t ls, uint64_t key, uint32_t Dl,
+                               ref_vertex* out)
+{
+    uint32_t j = (uint32_t)(u01(ls, key, 0) * s->n_lights);
+    if (j >= s->n_lights) j = s->n_lights - 1;
+    const uint32_t lt = s->lights[j];
+    const uint32_t* lv = s->tris + 3 * (size_t)lt;
+    d3 l0 = vtx(s, lv[0]), l1 = vtx(s, lv[1]), l2 = vtx(s, lv[2]);
+    double su = sqrt(u01(ls, key, 1)), u2 = u01(ls, key, 2);
+    double b0 = 1.0 - su, b1 = u2 * su;
+    d3 y0 = dadd(dadd(dmul(l0, b0), dmul(l1, b1)), dmul(l2, 1.0 - b0 - b1));
+    d3 ln = dnorm(dcross(dsub(l1, l0), dsub(l2, l0)));
+    /* DiffuseAreaLight::Le: uniform over the hemisphere about world +z, negated
+     * when its dot product with the light normal is nonzero; Le / pdf with
+     * pdf = (1 / area) (1 / 2 pi) / |cos|, Le only toward the front. */
+    const double ln3[3] = {ln.x, ln.y, ln.z};
+    double dir3[3], kk;
+    /* compute_area (core/primitives.h:273-276) is 0.5 for every triangle. */
+    rb2o_light_le_ref(ln3, 0.5, u01(ls, key, 3), u01(ls, key, 4), dir3, &kk);
+    d3 dir = D3(dir3[0], dir3[1], dir3[2]);
+    const float* Le = s->emission + 3 * (size_t)s->tri_mat[lt];
+    double beta[3] = {Le[0] * kk, Le[1] * kk, Le[2] * kk};
+    float ray[8];
+    mkray(ray, y0, 1.0e-4, dir, 3.402823466e+38);
+    uint32_t nv = 0;
+    for (uint32_t d = 1; d <= Dl; d++) {
+        rb2o_hit h;
+        trace_ct(b, ray, 0, &h, RB2O_RAY_LIGHT);
+        if (h.prim < 0) break;
+        const uint32_t* t = s->tris + 3 * (size_t)h.prim;
+        const uint32_t m = s->tri_mat[h.prim];
+        const float* E = s->emission + 3 * (size_t)m;
+        const int emitter = E[0] > 0.0f || E[1] > 0.0f || E[2] > 0.0f;
+        d3 v0 = vtx(s, t[0]), v1 = vtx(s, t[1]), v2 = vtx(s, t[2]);
+        d3 ng = dnorm(dcross(dsub(v1, v0), dsub(v2, v0)));
+        d3 dd = D3(ray[4], ray[5], ray[6]);
+        d3 wo = dmul(dd, -1.0);
+        d3 nrm = ddot(ng, wo) < 0.0 ? dmul(ng, -1.0) : ng;
+        d3 pos = dadd(D3(ray[0], ray[1], ray[2]), dmul(dd, h.t));
+        ref_vertex* V = &out[nv++];
+        V->pos = pos; V->nrm = nrm; V->wi = wo; V->ng = ng; V->depth = d; V->mat = m;
+        V->beta = emitter ? D3(0, 0, 0) : D3(beta[0], beta[1], beta[2]);
+        if (emitter || d >= Dl) break;
+        double fac[3];
+        d3 wn;
+        if (s->materials && !plain_lambertian(&s->materials[m])) {
+            double pdf;
+            int spec;
+            d3 f = mat_sample(&s->materials[m], ng, wo, u01(ls, key, 8 + 8 * d), u01(ls, key, 9 + 8 * d),
+                              u01(ls, key, 11 + 8 * d), &wn, &pdf, &spec, NULL);
+            if (!(pdf > 0.0) || !(f.x > 0.0 || f.y > 0.0 || f.z > 0.0)) break;
+            double k = fabs(ddot(wn, ng)) / pdf;
+            fac[0] = f.x * k; fac[1] = f.y * k; fac[2] = f.z * k;
+        } else {
+            d3 fx, fy;
+            frame(nrm, &fx, &fy);
+            d3 lc = cos_hemi(u01(ls, key, 8 + 8 * d), u01(ls, key, 9 + 8 * d));
+            if (!(lc.z > 0.0)) break;
+            wn = dnorm(dadd(dadd(dmul(fx, lc.x), dmul(fy, lc.y)), dmul(nrm, lc.z)));
+            const float* A = s->albedo + 3 * (size_t)m;
+            fac[0] = A[0]; fac[1] = A[1]; fac[2] = A[2];
+        }
+        double lum = 0.212671 * fac[0] + 0.715160 * fac[1] + 0.072169 * fac[2];
+        double q = lum < 1.0 ? lum : 1.0;
+        if (!(q > 0.0 && u01(ls, key, 10 + 8 * d) < q)) break;
+        for (int cc = 0; cc < 3; cc++) beta[cc] *= fac[cc] / q;
+        if (!(beta[0] > 0.0 || beta[1] > 0.0 || beta[2] > 0.0)) break;
+        mkray(ray, pos, 1.0e-3 * (double)h.t, wn, 3.402823466e+38);
+    }
+    return nv;
+}
+
+void rb2o_bdpt_ref(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, uint32_t n_cam, uint32_t n_iter,
+                   const rb2o_bdpt_ref_params* p, uint64_t seed, double* out_rgb, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#endif
+    const uint32_t Dl = p->light_max_depth, NL = p->n_light_paths, C = p->connections;
+    const uint32_t Kc = p->cam_max_depth + 1;
+    const double inv_nl = s->n_lights ? 1.0 / (double)s->n_lights : 0.0;
+    const uint64_t ls = seed ^ 0xA24BAED4963EE407ull;
+    ref_vertex* sparse = (ref_vertex*)calloc((size_t)NL * Dl, sizeof(ref_vertex));
+    uint32_t* nvert = (uint32_t*)calloc(NL, sizeof(uint32_t));
+    ref_vertex* dense = (ref_vertex*)calloc((size_t)NL * Dl, sizeof(ref_vertex));
+    for (size_t i = 0; i < (size_t)n_cam * 3; i++) out_rgb[i] = 0.0;
+    /* Preparation pass: mean stored vertices per light subpath -> cache capacity. */
+    uint64_t cap = (uint64_t)-1;
+    if (p->n_prep > 0 && s->n_lights) {
+        uint64_t total = 0;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nthreads)
+#endif
+        {
+            ref_vertex* tmp = (ref_vertex*)calloc(Dl, sizeof(ref_vertex));
+            uint64_t part = 0;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 64)
+#endif
+            for (int64_t q = 0; q < (int64_t)p->n_prep; q++)
+                part += ref_light_path(b, s, ls ^ 0x5EED5EED5EED5EEDull, (uint64_t)q, Dl, tmp);
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+            total += part;
+            free(tmp);
+        }
+        float avg = (float)total / (float)p->n_prep;
+        cap = (uint64_t)ceilf(1.1f * avg * (float)NL);
+    }
+    for (uint32_t it = 0; it < n_iter; it++) {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+#endif
+        for (int64_t q = 0; q < (int64_t)NL; q++)
+            nvert[q] = s->n_lights ? ref_light_path(b, s, ls, (uint64_t)it * NL + (uint64_t)q, Dl, sparse + (size_t)q * Dl)
+                                   : 0u;
+        uint64_t M = 0;
+        for (uint32_t q = 0; q < NL; q++)
+            for (uint32_t k = 0; k < nvert[q]; k++)
+                if (M < cap) dense[M++] = sparse[(size_t)q * Dl + k];
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+#endif
+        for (int64_t ci = 0; ci < (int64_t)n_cam; ci++) {
+            double L[3] = {0, 0, 0}, T[3] = {1, 1, 1};
+            int prev_spec = 1; /* the camera counts as specular */
+            float ray[8];
+            for (int k = 0; k < 8; k++) ray[k] = cam_rays[8 * ((size_t)it * n_cam + ci) + k];
+            const uint64_t key = (uint64_t)it * n_cam + (uint64_t)ci;
+            for (uint32_t i = 1; i <= Kc; i++) {
+                rb2o_hit h;
+                trace_ct(b, ray, 0, &h, i == 1 ? RB2O_RAY_CAMERA : RB2O_RAY_EXTENSION);
+                if (h.prim < 0) break;
+                const uint32_t* t = s->tris + 3 * (size_t)h.prim;
+                const uint32_t m = s->tri_mat[h.prim];
+                d3 v0 = vtx(s, t[0]), v1 = vtx(s, t[1]), v2 = vtx(s, t[2]);
+                d3 ng = dnorm(dcross(dsub(v1, v0), dsub(v2, v0)));
+                d3 dd = D3(ray[4], ray[5], ray[6]);
+                d3 wo = dmul(dd, -1.0);
+                d3 pos = dadd(D3(ray[0], ray[1], ray[2]), dmul(dd, h.t));
+                const double eps = 1.0e-3 * (double)h.t;
+                const float* E = s->emission + 3 * (size_t)m;
+                if (E[0] > 0.0f || E[1] > 0.0f || E[2] > 0.0f) {
+                    if (prev_spec && ddot(ng, wo) > 0.0)
+                        for (int c = 0; c < 3; c++) L[c] += T[c] * E[c];
+                    break;
+                }
+                d3 nrm = ddot(ng, wo) < 0.0 ? dmul(ng, -1.0) : ng;
+                const float* A = s->albedo + 3 * (size_t)m;
+                const rb2o_material* mc = (s->materials && !plain_lambertian(&s->materials[m])) ? &s->materials[m] : NULL;
+                frame3 frc = frame_z(ng);
+                d3 wo_l = fr_local(&frc, wo);
+                uint64_t vkey = key * 64 + i;
+                uint64_t nkey = key * 64 + 1; /* NEE: the first vertex's draws at every vertex */
+                if (s->n_lights) {
+                    /* compute_direct_lighting (integrator_bdpt_lvc_sk.cu:233-327): a light
+                     * sample and a BSDF sample toward one uniformly chosen emissive
+                     * triangle j, balance-heuristic weights from the reference's pdfs
+                     * (triangle area 0.5, no 1 / n_lights), the sum times n_lights. */
+                    const double nl = (double)s->n_lights;
+                    uint32_t j = (uint32_t)(u01(seed, nkey, 0) * s->n_lights);
+                    if (j >= s->n_lights) j = s->n_lights - 1;
+                    const uint32_t lt = s->lights[j];
+                    const uint32_t* lv = s->tris + 3 * (size_t)lt;
+                    d3 l0 = vtx(s, lv[0]), l1 = vtx(s, lv[1]), l2 = vtx(s, lv[2]);
+                    d3 ln = dnorm(dcross(dsub(l1, l0), dsub(l2, l0)));
+                    const float* Le = s->emission + 3 * (size_t)s->tri_mat[lt];
+                    double su = sqrt(u01(seed, nkey, 1)), u2 = u01(seed, nkey, 2);
+                    double b0 = 1.0 - su, b1 = u2 * su;
+                    d3 lp = dadd(dadd(dmul(l0, b0), dmul(l1, b1)), dmul(l2, 1.0 - b0 - b1));
+                    d3 dv = dsub(lp, pos);
+                    double dist2 = ddot(dv, dv), dist = sqrt(dist2);
+                    d3 wi = dmul(dv, 1.0 / dist);
+                    double cos_l = -ddot(ln, wi), cos_s = ddot(nrm, wi);
+                    d3 f = D3(0, 0, 0);
+                    double pdf_b = 0.0;
+                    if (mc) {
+                        d3 wi_l = fr_local(&frc, wi);
+                        f = mat_f(mc, ng, wo, wi, wo_l, wi_l);
+                        pdf_b = mat_pdf(mc, wo_l, wi_l);
+                    } else if (cos_s > 0.0) {
+                        f = dmul(D3(A[0], A[1], A[2]), 1.0 / RB2O_PI);
+                        pdf_b = cos_s / RB2O_PI;
+                    }
+                    if (cos_l > 0.0 && dist > 0.0 && (f.x > 0.0 || f.y > 0.0 || f.z > 0.0)) {
+                        double pdf_l = dist2 / (0.5 * cos_l);
+                        float sr[8];
+                        mkray(sr, pos, eps, wi, dist * (1.0 - 1.0e-3));
+                        if (!occluded(b, sr)) {
+                            double k = fabs(cos_s) * (pdf_l / (pdf_l + pdf_b)) / pdf_l * nl;
+                            L[0] += T[0] * f.x * Le[0] * k;
+                            L[1] += T[1] * f.y * Le[1] * k;
+                            L[2] += T[2] * f.z * Le[2] * k;
+                        }
+                    }
+                    /* BSDF half: counts when the sampled ray's closest hit is triangle j. */
+                    d3 wb = D3(0, 0, 0), fb = D3(0, 0, 0);
+                    double pb = 0.0;
+                    if (mc) {
+                        int spec;
+                        fb = mat_sample(mc, ng, wo, u01(seed, key, 8000), u01(seed, key, 8001), u01(seed, key, 8002),
+                                        &wb, &pb, &spec, NULL);
+                        if (spec) pb = 0.0;
+                    } else {
+                        d3 fx, fy;
+                        frame(nrm, &fx, &fy);
+                        d3 lc = cos_hemi(u01(seed, key, 8000), u01(seed, key, 8001));
+                        if (lc.z > 0.0) {
+                            wb = dnorm(dadd(dadd(dmul(fx, lc.x), dmul(fy, lc.y)), dmul(nrm, lc.z)));
+                            fb = dmul(D3(A[0], A[1], A[2]), 1.0 / RB2O_PI);
+                            pb = lc.z / RB2O_PI;
+                        }
+                    }
+                    if (pb > 0.0 && (fb.x > 0.0 || fb.y > 0.0 || fb.z > 0.0)) {
+                        /* sample_triangle_pdf: Moller-Trumbore of the ray against j. */
+                        d3 e1 = dsub(l1, l0), e2 = dsub(l2, l0), pv = dcross(wb, e2);
+                        double det = ddot(e1, pv);
+                        if (!(det < 1.0e-6 && det > -1.0e-6)) {
+                            d3 tv = dsub(pos, l0);
+                            double uu = ddot(tv, pv) / det;
+                            d3 qv = dcross(tv, e1);
+                            double vv = ddot(wb, qv) / det, th = ddot(e2, qv) / det;
+                            double cth = -ddot(ln, wb);
+                            if (uu >= 0.0 && uu <= 1.0 && vv >= 0.0 && uu + vv <= 1.0 && th > eps && cth > 0.0) {
+                                double pdf_l = th * th / (0.5 * cth);
+                                float br[8];
+                                mkray(br, pos, eps, wb, 3.402823466e+38);
+                                rb2o_hit bh;
+                                trace_ct(b, br, 0, &bh, RB2O_RAY_CONNECTION);
+                                if (bh.prim == (int32_t)lt) {
+                                    double k = fabs(ddot(wb, nrm)) * (pb / (pb + pdf_l)) / pb * nl;
+                                    L[0] += T[0] * fb.x * Le[0] * k;
+                                    L[1] += T[1] * fb.y * Le[1] * k;
+                                    L[2] += T[2] * fb.z * Le[2] * k;
+                                }
+                            }
+                        }
+                    }
+                }
+                for (uint32_t cidx = 0; M > 0 && cidx < C; cidx++) {
+                    uint64_t v = (uint64_t)(u01(seed, vkey, 16 + cidx) * (double)M);
+                    if (v >= M) v = M - 1;
+                    const ref_vertex* V = &dense[v];
+                    d3 dv = dsub(V->pos, pos);
+                    double dist2 = ddot(dv, dv), dist = sqrt(dist2);
+                    if (!(dist > 0.0)) continue;
+                    d3 dir = dmul(dv, 1.0 / dist);
+                    double cos_c = ddot(nrm, dir), cos_v = -ddot(V->nrm, dir);
+                    const rb2o_material* mv =
+                        (s->materials && !plain_lambertian(&s->materials[V->mat])) ? &s->materials[V->mat] : NULL;
+                    d3 fc = mc ? mat_f(mc, ng, wo, dir, wo_l, fr_local(&frc, dir))
+                               : (cos_c > 0.0 ? dmul(D3(A[0], A[1], A[2]), 1.0 / RB2O_PI) : D3(0, 0, 0));
+                    d3 fv;
+                    if (mv) {
+                        /* material_f(cached material, wo = toward the previous light
+                         * vertex, wi = toward the camera vertex) */
+                        frame3 frv = frame_z(V->ng);
+                        d3 wiv = dmul(dir, -1.0);
+                        fv = mat_f(mv, V->ng, V->wi, wiv, fr_local(&frv, V->wi), fr_local(&frv, wiv));
+                    } else {
+                        const float* Av = s->albedo + 3 * (size_t)V->mat;
+                        fv = cos_v > 0.0 ? dmul(D3(Av[0], Av[1], Av[2]), 1.0 / RB2O_PI) : D3(0, 0, 0);
+                    }
+                    double g = fabs(cos_c) * fabs(cos_v) / dist2 / ((double)i + (double)V->depth);
+                    double cv[3] = {T[0] * fc.x * fv.x * V->beta.x * g, T[1] * fc.y * fv.y * V->beta.y * g,
+                                    T[2] * fc.z * fv.z * V->beta.z * g};
+                    if (!(cv[0] > 0.0 || cv[1] > 0.0 || cv[2] > 0.0)) continue;
+                    float cr[8];
+                    mkray(cr, pos, eps, dir, dist * (1.0 - 1.0e-3));
+                    if (occluded_t(b, cr, RB2O_RAY_CONNECTION)) continue;
+                    for (int c = 0; c < 3; c++) L[c] += cv[c];
+                }
+                if (i >= Kc) break;
+                d3 wn;
+                int spec = 0;
+                if (mc) {
+                    double pdf;
+                    d3 f = mat_sample(mc, ng, wo, u01(seed, vkey, 3), u01(seed, vkey, 4), u01(seed, vkey, 6), &wn, &pdf,
+                                      &spec, NULL);
+                    if (!(pdf > 0.0) || !(f.x > 0.0 || f.y > 0.0 || f.z > 0.0)) break;
+                    double k = fabs(ddot(wn, ng)) / pdf;
+                    T[0] *= f.x * k; T[1] *= f.y * k; T[2] *= f.z * k;
+                } else {
+                    d3 fx, fy;
+                    frame(nrm, &fx, &fy);
+                    d3 lc = cos_hemi(u01(seed, vkey, 3), u01(seed, vkey, 4));
+                    if (!(lc.z > 0.0)) break;
+                    wn = dnorm(dadd(dadd(dmul(fx, lc.x), dmul(fy, lc.y)), dmul(nrm, lc.z)));
+                    for (int c = 0; c < 3; c++) T[c] *= A[c];
+                }
+                if (!(T[0] > 0.0 || T[1] > 0.0 || T[2] > 0.0)) break;
+                if (!rr_step(T, i - 1, p->cam_rrstart, p->cam_rrprob, 2u, u01(seed, vkey, 5))) break;
+                prev_spec = spec;
+                mkray(ray, pos, eps, wn, 3.402823466e+38);
+            }
+            for (int c = 0; c < 3; c++) out_rgb[3 * ci + c] += L[c] / (double)n_iter;
+        }
+    }
+    free(sparse);
+    free(nvert);
     free(dense);
     (void)nthreads;
 }

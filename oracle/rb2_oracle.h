@@ -154,15 +154,26 @@ void rb2o_counts_read(uint64_t* out);
 
 /* Ambient occlusion (integrators/integrator_ao.cu:51-84): per primary ray, the
  * unoccluded fraction of `samples` cosine-distributed rays about the
- * viewer-facing geometric normal, tmin 1e-3 t, tmax radius; 0 on a miss. */
+ * viewer-facing geometric normal, tmin 1e-3 t, tmax radius; 0 on a miss.
+ * compat bit 1: the reference's direction formula about the unflipped normal
+ * (core/montecarlo.cu:133-151; a sample whose X axis is undefined is open). */
 void rb2o_ao(const rb2o_bvh* b, const rb2o_scene* s, const float* prim_rays, uint32_t n, uint32_t samples,
-             float radius, uint64_t seed, double* out, int nthreads);
+             float radius, uint64_t seed, uint32_t compat, double* out, int nthreads);
+/* The two reference formulas the compatibility modes restate, in double (pinned
+ * against the reference's compiled functions by the CPU tests):
+ * rb2o_ao_ref_dir: the AO direction about n3 (0 where the reference's is NaN);
+ * rb2o_light_le_ref: DiffuseAreaLight::Le's direction and Le / pdf factor. */
+int rb2o_ao_ref_dir(const double* n3, double u1, double u2, double* out3);
+void rb2o_light_le_ref(const double* ln3, double area, double u3, double u4, double* dir3, double* k);
 
 /* One path-traced sample per camera ray (integrators/integrator_path.cu:56-260
  * with unbiased Russian roulette): NEE to a uniformly chosen emissive triangle
- * and BSDF sampling combined by the balance heuristic; out_rgb: 3 per ray. */
+ * and BSDF sampling combined by the balance heuristic; out_rgb: 3 per ray.
+ * compat bit 2: roulette from bounce rr_start + 1 dividing survivors by 1 - q
+ * (integrator_path.cu:232-244); bit 4: the same NEE draws at every vertex
+ * (integrator_path.cu:113). */
 void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t n, uint32_t max_depth,
-             uint32_t rr_start, float rr_prob, uint64_t seed, double* out_rgb, int nthreads);
+             uint32_t rr_start, float rr_prob, uint64_t seed, uint32_t compat, double* out_rgb, int nthreads);
 
 /* BDPT with a light-vertex cache (integrators/integrator_bdpt_lvc_sk.cu:47-514,
  * with uniform 1/k weights over all k strategies of a k-segment path and the
@@ -173,6 +184,26 @@ void rb2o_pt(const rb2o_bvh* b, const rb2o_scene* s, const float* rays, uint32_t
 void rb2o_bdpt(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, uint32_t n_cam, uint32_t n_iter,
                uint32_t n_light_paths, uint32_t K, uint32_t C, uint32_t rr_start, float rr_prob, uint64_t seed,
                double* out_rgb, int nthreads);
+
+/* The reference's own BDPT estimator (integrators/integrator_bdpt_lvc_sk.cu:47-514),
+ * restated in FP64 with counter-keyed draws: a preparation pass of n_prep
+ * light subpaths sizes the cache at ceil(1.1 * mean stored vertices *
+ * n_light_paths) (single precision, :466-470; n_prep 0: no cap); light
+ * subpaths start as DiffuseAreaLight::Le (core/lights.cu:63-69: direction
+ * uniform about world +z, negated, contribution Le / pdf without the triangle
+ * choice), store every surface vertex (emitters with zero contribution, then
+ * stop), play roulette min(1, luminance) at every bounce and stop when black,
+ * keeping at most light_max_depth vertices; camera vertices 0..cam_max_depth
+ * add emission (first vertex or after a specular bounce), NEE at full weight
+ * with the first vertex's draws at every vertex, and `connections`
+ * connections to uniform cached vertices weighted 1 / ((bounce + 1) + depth);
+ * camera roulette from bounce cam_rrstart + 1 divides survivors by 1 - q. */
+typedef struct {
+    uint32_t n_prep, n_light_paths, light_max_depth, cam_max_depth, cam_rrstart, connections;
+    float cam_rrprob;
+} rb2o_bdpt_ref_params;
+void rb2o_bdpt_ref(const rb2o_bvh* b, const rb2o_scene* s, const float* cam_rays, uint32_t n_cam, uint32_t n_iter,
+                   const rb2o_bdpt_ref_params* p, uint64_t seed, double* out_rgb, int nthreads);
 
 /* PCG32 (O'Neill 2014, pcg32_srandom_r / pcg32_random_r), the generator the
  * product uses for every seeded stream. */

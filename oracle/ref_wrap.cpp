@@ -15,6 +15,8 @@
 #include <core/bsdf.h>
 #include <core/util.h>
 #include <core/camera.h>
+#include <core/lights.h>
+#include <core/montecarlo.h>
 #include <core/material.h>
 #include <core/mesh.h>
 #include <core/primitives.h>
@@ -317,6 +319,36 @@ int rb2ref_material(const rb2ref_layer* layers, uint32_t n_layers, int sample, c
         out[0] = f.x; out[1] = f.y; out[2] = f.z;
         out[3] = material_pdf(mb, 0, wo, wi, frame, fl);
     }
+    return 0;
+}
+
+// cosine_sample_hemisphere_normal (core/montecarlo.cu:133-151), the
+// reference's AO direction about `normal`.
+int rb2ref_ao_direction(float u1, float u2, const float* normal, float* dir_out)
+{
+    float3 n = make_float3(normal[0], normal[1], normal[2]);
+    float3 d = cosine_sample_hemisphere_normal(u1, u2, n);
+    dir_out[0] = d.x; dir_out[1] = d.y; dir_out[2] = d.z;
+    return 0;
+}
+
+// DiffuseAreaLight(v0, v1, v2, emit).Le(...) (core/lights.cu:63-69): writes
+// the light point, the direction, the pdf and the returned radiance.
+int rb2ref_light_le(const float* v0, const float* v1, const float* v2, const float* emit, const float* u5,
+                    float* pt_out, float* dir_out, float* pdf_out, float* L_out)
+{
+    DiffuseAreaLight l(make_float3(v0[0], v0[1], v0[2]), make_float3(v1[0], v1[1], v1[2]),
+                       make_float3(v2[0], v2[1], v2[2]), make_float3(emit[0], emit[1], emit[2]));
+    LightSample sample;
+    sample.m_u0 = u5[0];
+    sample.m_u1 = u5[1];
+    float3 pt, dir;
+    float pdf = 0.0f;
+    float3 L = l.Le(sample, make_float2(u5[2], u5[3]), pt, dir, pdf);
+    pt_out[0] = pt.x; pt_out[1] = pt.y; pt_out[2] = pt.z;
+    dir_out[0] = dir.x; dir_out[1] = dir.y; dir_out[2] = dir.z;
+    *pdf_out = pdf;
+    L_out[0] = L.x; L_out[1] = L.y; L_out[2] = L.z;
     return 0;
 }
 

@@ -87,17 +87,29 @@ class BatchConfig(C.Structure):
 
 
 class AoParams(C.Structure):
-    _fields_ = [("samples", C.c_uint32), ("radius", C.c_float), ("seed", C.c_uint64)]
+    _fields_ = [("samples", C.c_uint32), ("radius", C.c_float), ("seed", C.c_uint64), ("compat", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class PtParams(C.Structure):
     _fields_ = [("spp", C.c_uint32), ("max_depth", C.c_uint32), ("rr_start", C.c_uint32), ("rr_prob", C.c_float),
-                ("seed", C.c_uint64), ("spp_per_wave", C.c_uint32), ("reserved", C.c_uint32)]
+                ("seed", C.c_uint64), ("spp_per_wave", C.c_uint32), ("compat", C.c_uint32)]
 
 
 class BdptParams(C.Structure):
     _fields_ = [("spp", C.c_uint32), ("max_path_length", C.c_uint32), ("num_light_paths", C.c_uint32),
                 ("connections", C.c_uint32), ("rr_start", C.c_uint32), ("rr_prob", C.c_float), ("seed", C.c_uint64)]
+
+
+class BdptLvcParams(C.Structure):
+    """rb2_bdpt_lvc_params: the reference's BidirectionalPathIntegratorLvcParams
+    (core/params.h:108-120) plus the estimator choice."""
+    _fields_ = [("spp", C.c_uint32), ("num_prep_paths", C.c_uint32), ("num_light_paths", C.c_uint32),
+                ("num_light_path_max_depth", C.c_uint32), ("light_path_rrstart", C.c_uint32),
+                ("num_cam_path_max_depth", C.c_uint32), ("cam_path_rrstart", C.c_uint32),
+                ("cam_path_rrprob", C.c_float), ("num_cam_path_sample_connections", C.c_uint32),
+                ("num_cam_path_connections", C.c_uint32), ("mode", C.c_uint32), ("estimator", C.c_uint32),
+                ("max_path_length", C.c_uint32), ("reserved", C.c_uint32), ("seed", C.c_uint64)]
 
 
 class RayCastParams(C.Structure):
@@ -184,6 +196,7 @@ SIGNATURES = {
     "rb2_render_pt": (C.c_int, [P, C.POINTER(Camera), C.POINTER(PtParams), P, P]),
     "rb2_render_raycast": (C.c_int, [P, C.POINTER(Camera), C.POINTER(RayCastParams), P, P]),
     "rb2_render_bdpt": (C.c_int, [P, C.POINTER(Camera), C.POINTER(BdptParams), P, P]),
+    "rb2_render_bdpt_lvc": (C.c_int, [P, C.POINTER(Camera), C.POINTER(BdptLvcParams), P, P]),
     "rb2_camera_init": (C.c_int, [C.POINTER(Camera), P, P, P, U32, U32, C.c_float]),
     "rb2_camera_rays": (C.c_int, [C.POINTER(Camera), U32, U64, I32, P, P]),
     "rb2_camera_rays_at": (C.c_int, [C.POINTER(Camera), P, U32, P, P]),

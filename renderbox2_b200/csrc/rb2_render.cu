@@ -75,6 +75,7 @@ struct AoSource {
     uint32_t samples;
     float radius;
     uint64_t seed;
+    uint32_t compat;   // RB2_COMPAT_AO_DIRECTION: the reference's direction formula
 
     __device__ __forceinline__ void claim(unsigned count, unsigned long long& b1, unsigned& n1, unsigned long long& b2)
     {
@@ -95,9 +96,31 @@ struct AoSource {
         const uint4 tri = tris[h.x];
         const float3 v0 = xyz(verts[tri.x]), v1 = xyz(verts[tri.y]), v2 = xyz(verts[tri.z]);
         float3 ng = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
-        if (dot3(ng, xyz(d4)) > 0.0f) ng = mul(ng, -1.0f);
-        const Frame fr = frame_from_z(ng);
-        const float3 dir = to_world(fr, cosine_hemisphere(rng_u01(seed, slot, 0), rng_u01(seed, slot, 1)));
+        float3 dir;
+        if (compat & RB2_COMPAT_AO_DIRECTION) {
+            // cosine_sample_hemisphere_normal (core/montecarlo.cu:133-151) about the
+            // unflipped normal; X from the cross product with the axis picked by
+            // signed component comparisons.
+            const float u1 = rng_u01(seed, slot, 0), u2 = rng_u01(seed, slot, 1);
+            const float phi = 6.283185307179586f * u1, theta = acosf(sqrtf(1.0f - u2));
+            float3 perp = f3(0.0f, 0.0f, 1.0f);
+            if (ng.x < ng.y && ng.x < ng.z) perp = f3(1.0f, 0.0f, 0.0f);
+            else if (ng.y < ng.x && ng.y < ng.z) perp = f3(0.0f, 1.0f, 0.0f);
+            const float3 cx = cross3(ng, perp);
+            const float lx2 = dot3(cx, cx);
+            if (!(lx2 > 0.0f)) {  // the reference's X is NaN there: its ray never hits
+                atomicAdd(&counts[pix], 1u);
+                return -1;
+            }
+            const float3 X = mul(cx, 1.0f / sqrtf(lx2));
+            const float3 Y = normalize3(cross3(ng, X));
+            const float st = sinf(theta), cp = cosf(phi), sp = sinf(phi);
+            dir = add(add(mul(X, cp * st), mul(Y, sp * st)), mul(ng, cp));
+        } else {
+            if (dot3(ng, xyz(d4)) > 0.0f) ng = mul(ng, -1.0f);
+            const Frame fr = frame_from_z(ng);
+            dir = to_world(fr, cosine_hemisphere(rng_u01(seed, slot, 0), rng_u01(seed, slot, 1)));
+        }
         L.nodes = nodes;
         L.woop = woop;
         L.set_tag(kOcclusion, 0);
@@ -254,21 +277,37 @@ __device__ __forceinline__ float tri_area(float3 v0, float3 v1, float3 v2)
 // specular materials), then material_sample_f for the continuation.  T.w
 // carries the sampled pdf for the emission MIS weight, -1 after a specular
 // bounce (full weight, as integrator_path.cu:94 counts emission after one).
+// Russian roulette of a camera path after the BSDF sample at vertex b: from
+// b = rr_start with division by q, or (RB2_COMPAT_RR_DIVISOR) from
+// b = rr_start + 1 with division by 1 - q (integrator_path.cu:232-244).
+__device__ __forceinline__ bool roulette(float4& Tp, uint32_t b, uint32_t rr_start, float rr_prob, uint32_t compat,
+                                         float u)
+{
+    const bool ref = (compat & RB2_COMPAT_RR_DIVISOR) != 0;
+    if (ref ? b <= rr_start : b < rr_start) return true;
+    const float q = fminf(rr_prob, luminance(xyz(Tp)));
+    if (!(u < q)) return false;
+    const float inv = ref ? 1.0f / (1.0f - q) : 1.0f / q;
+    Tp.x *= inv; Tp.y *= inv; Tp.z *= inv;
+    return true;
+}
+
 __device__ __forceinline__ void shade_layered(const SceneView& sc, const MaterialDev& m, uint64_t seed, uint64_t key,
                                               uint32_t b, uint32_t max_depth, uint32_t rr_start, float rr_prob,
-                                              float inv_nl, float3 pos, float eps, float3 ng, float3 wo, float4& Tp,
-                                              bool& shadow, float4& so, float4& sd, float4& scv, bool& cont,
-                                              float4& new_o, float4& new_d)
+                                              uint32_t compat, float inv_nl, float3 pos, float eps, float3 ng,
+                                              float3 wo, float4& Tp, bool& shadow, float4& so, float4& sd,
+                                              float4& scv, bool& cont, float4& new_o, float4& new_d)
 {
     const Frame fr = frame_from_z(ng);
     const float3 wo_l = to_local(fr, wo);
+    const uint32_t bn = (compat & RB2_COMPAT_NEE_RESEED) ? 0u : b;  // NEE draws of this vertex
     if (sc.n_lights && (m.flags & kMatHasNonDelta)) {
-        uint32_t j = (uint32_t)(rng_u01(seed, key, vdim(b, kDimLight)) * (float)sc.n_lights);
+        uint32_t j = (uint32_t)(rng_u01(seed, key, vdim(bn, kDimLight)) * (float)sc.n_lights);
         j = min(j, sc.n_lights - 1);
         const uint4 lt = sc.tris[sc.lights[j]];
         const float3 l0 = xyz(sc.verts[lt.x]), l1 = xyz(sc.verts[lt.y]), l2 = xyz(sc.verts[lt.z]);
-        const float3 lp = sample_triangle(l0, l1, l2, rng_u01(seed, key, vdim(b, kDimLightU)),
-                                          rng_u01(seed, key, vdim(b, kDimLightV)));
+        const float3 lp = sample_triangle(l0, l1, l2, rng_u01(seed, key, vdim(bn, kDimLightU)),
+                                          rng_u01(seed, key, vdim(bn, kDimLightV)));
         const float3 ln = normalize3(cross3(sub(l1, l0), sub(l2, l0)));
         const float3 dv = sub(lp, pos);
         const float dist2 = dot3(dv, dv);
@@ -303,11 +342,7 @@ __device__ __forceinline__ void shade_layered(const SceneView& sc, const Materia
     Tp.x *= f.x * k; Tp.y *= f.y * k; Tp.z *= f.z * k;
     Tp.w = spec ? -1.0f : pdf;
     cont = isfinite(Tp.x) && isfinite(Tp.y) && isfinite(Tp.z) && (Tp.x > 0.0f || Tp.y > 0.0f || Tp.z > 0.0f);
-    if (cont && b >= rr_start) {
-        const float q = fminf(rr_prob, luminance(xyz(Tp)));
-        if (!(rng_u01(seed, key, vdim(b, kDimRR)) < q)) cont = false;
-        else { Tp.x /= q; Tp.y /= q; Tp.z /= q; }
-    }
+    if (cont) cont = roulette(Tp, b, rr_start, rr_prob, compat, rng_u01(seed, key, vdim(b, kDimRR)));
     if (cont) {
         new_o = make_float4(pos.x, pos.y, pos.z, eps);
         new_d = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
@@ -315,7 +350,8 @@ __device__ __forceinline__ void shade_layered(const SceneView& sc, const Materia
 }
 
 __global__ void k_pt_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t sample0, uint32_t b, uint32_t max_depth,
-                           uint32_t rr_start, float rr_prob, const uint32_t* q_in, uint32_t* q_out, float4* rays,
+                           uint32_t rr_start, float rr_prob, uint32_t compat, const uint32_t* q_in, uint32_t* q_out,
+                           float4* rays,
                            const int4* hits, float4* T, float4* L, float4* srays, float4* sc_out, uint32_t* qs,
                            WaveCountersDev* wc, uint32_t cur)
 {
@@ -359,20 +395,21 @@ __global__ void k_pt_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t 
                     }
                     // Emitters end the path (integrator_path.cu:94-107).
                 } else if (sc.mats != nullptr && !(sc.mats[tri.w].flags & kMatPlainLambertian)) {
-                    shade_layered(sc, sc.mats[tri.w], seed, key, b, max_depth, rr_start, rr_prob, inv_nl, pos, eps, ng,
-                                  wo, Tp, shadow, so, sd, scv, cont, new_o, new_d);
+                    shade_layered(sc, sc.mats[tri.w], seed, key, b, max_depth, rr_start, rr_prob, compat, inv_nl, pos,
+                                  eps, ng, wo, Tp, shadow, so, sd, scv, cont, new_o, new_d);
                     if (cont) T[path] = Tp;
                 } else {
                     const float3 nrm = dot3(ng, wo) < 0.0f ? mul(ng, -1.0f) : ng;
                     const float4 A = sc.albedo[tri.w];
                     // Next-event estimation to one uniformly chosen emissive triangle.
                     if (sc.n_lights) {
-                        uint32_t j = (uint32_t)(rng_u01(seed, key, vdim(b, kDimLight)) * (float)sc.n_lights);
+                        const uint32_t bn = (compat & RB2_COMPAT_NEE_RESEED) ? 0u : b;
+                        uint32_t j = (uint32_t)(rng_u01(seed, key, vdim(bn, kDimLight)) * (float)sc.n_lights);
                         j = min(j, sc.n_lights - 1);
                         const uint4 lt = sc.tris[sc.lights[j]];
                         const float3 l0 = xyz(sc.verts[lt.x]), l1 = xyz(sc.verts[lt.y]), l2 = xyz(sc.verts[lt.z]);
-                        const float3 lp = sample_triangle(l0, l1, l2, rng_u01(seed, key, vdim(b, kDimLightU)),
-                                                          rng_u01(seed, key, vdim(b, kDimLightV)));
+                        const float3 lp = sample_triangle(l0, l1, l2, rng_u01(seed, key, vdim(bn, kDimLightU)),
+                                                          rng_u01(seed, key, vdim(bn, kDimLightV)));
                         const float3 ln = normalize3(cross3(sub(l1, l0), sub(l2, l0)));
                         const float3 dv = sub(lp, pos);
                         const float dist2 = dot3(dv, dv);
@@ -402,13 +439,9 @@ __global__ void k_pt_shade(SceneView sc, uint64_t seed, uint32_t npix, uint32_t 
                             const float3 wi = normalize3(to_world(frame_from_z(nrm), loc));
                             Tp.x *= A.x; Tp.y *= A.y; Tp.z *= A.z; Tp.w = pdf;
                             cont = Tp.x > 0.0f || Tp.y > 0.0f || Tp.z > 0.0f;
-                            if (cont && b >= rr_start) {
-                                // Unbiased Russian roulette (the reference divides by 1 - q,
-                                // integrator_path.cu:232-244).
-                                const float q = fminf(rr_prob, luminance(xyz(Tp)));
-                                if (!(rng_u01(seed, key, vdim(b, kDimRR)) < q)) cont = false;
-                                else { Tp.x /= q; Tp.y /= q; Tp.z /= q; }
-                            }
+                            // Unbiased Russian roulette unless RB2_COMPAT_RR_DIVISOR asks for
+                            // the reference's division by 1 - q (integrator_path.cu:232-244).
+                            if (cont) cont = roulette(Tp, b, rr_start, rr_prob, compat, rng_u01(seed, key, vdim(b, kDimRR)));
                             if (cont) {
                                 T[path] = Tp;
                                 new_o = make_float4(pos.x, pos.y, pos.z, eps);
@@ -1018,6 +1051,408 @@ __global__ void k_bd_cam_shade(SceneView sc, uint64_t seed, uint32_t npix, uint3
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&wc->stats[i == 1 ? 0 : 1], (unsigned long long)n);
 }
 
+// ---- BDPT: the reference's own estimator (integrators/integrator_bdpt_lvc_sk.cu) ---------
+// Same wavefront stages and buffers as above; only the estimator differs
+// (rb2_bdpt_lvc_params, RB2_BDPT_ESTIMATOR_REFERENCE).
+
+// The reference's triangle area (compute_area, core/primitives.h:273-276) is
+// 0.5 * length(compute_normal(...)), and compute_normal is normalized: every
+// triangle's area is 0.5 in its light pdfs.
+constexpr float kRefTriArea = 0.5f;
+// Random dimensions of the BSDF half of the reference estimator's NEE (the
+// same at every vertex, as its re-seeded NEE generator draws them).
+constexpr uint32_t kDimNeeBsdf = 8000;
+
+// intersect_ray_triangle (core/primitives.cu:51-70): Moller-Trumbore without a
+// distance check, determinant threshold 1e-6; returns t.
+__device__ __forceinline__ bool ref_intersect(float3 o, float3 d, float3 v0, float3 v1, float3 v2, float& t)
+{
+    const float3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+    const float3 pv = cross3(d, e2);
+    const float det = dot3(e1, pv);
+    if (det < 1.0e-6f && det > -1.0e-6f) return false;
+    const float inv = 1.0f / det;
+    const float3 tv = sub(o, v0);
+    const float u = dot3(tv, pv) * inv;
+    if (u < 0.0f || u > 1.0f) return false;
+    const float3 qv = cross3(tv, e1);
+    const float v = dot3(d, qv) * inv;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    t = dot3(e2, qv) * inv;
+    return true;
+}
+
+// Light subpath start as DiffuseAreaLight::Le computes it (core/lights.cu:63-69,
+// integrator_bdpt_lvc_sk.cu:61-83): uniform emissive triangle, uniform point,
+// a direction uniform over the hemisphere about world +z (uniform_sample_hemisphere,
+// core/montecarlo.cu:115-122) negated whenever its dot product with the light
+// normal is nonzero; contribution Le / pdf, pdf = (1 / area) (1 / 2 pi) / |cos|,
+// Le only toward the light's front, no factor for the triangle choice.
+__global__ void k_bd_light_init_ref(SceneView sc, uint64_t seed, uint64_t key0, uint32_t n_paths, float4* lray,
+                                    float4* lbeta, uint32_t* lq0, WaveCountersDev* wc)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) wc->n_ext[0] = sc.n_lights ? n_paths : 0u;
+    if (!sc.n_lights) return;
+    const uint64_t ls = seed ^ kLightSalt;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
+        const uint64_t key = key0 + p;
+        uint32_t j = min((uint32_t)(rng_u01(ls, key, 0) * (float)sc.n_lights), sc.n_lights - 1);
+        const uint4 lt = sc.tris[sc.lights[j]];
+        const float3 l0 = xyz(sc.verts[lt.x]), l1 = xyz(sc.verts[lt.y]), l2 = xyz(sc.verts[lt.z]);
+        const float3 y0 = sample_triangle(l0, l1, l2, rng_u01(ls, key, 1), rng_u01(ls, key, 2));
+        const float3 ln = normalize3(cross3(sub(l1, l0), sub(l2, l0)));
+        const float hz = rng_u01(ls, key, 3);
+        const float hr = sqrtf(fmaxf(0.0f, 1.0f - hz * hz)), phi = 6.283185307179586f * rng_u01(ls, key, 4);
+        float3 dir = f3(hr * cosf(phi), hr * sinf(phi), hz);
+        if (dot3(dir, ln) != 0.0f) dir = mul(dir, -1.0f);
+        const float c = dot3(ln, dir);
+        const float4 Le = sc.emission[lt.w];
+        // pdf uses compute_area, which is 0.5 for every triangle (core/primitives.h:273-276:
+        // half the length of the already normalized normal).
+        const float k = c > 0.0f ? kRefTriArea * 6.283185307179586f * c : 0.0f;
+        lbeta[p] = make_float4(Le.x * k, Le.y * k, Le.z * k, 0.0f);
+        lray[2 * (size_t)p] = make_float4(y0.x, y0.y, y0.z, kLightRayTmin);
+        lray[2 * (size_t)p + 1] = make_float4(dir.x, dir.y, dir.z, 3.402823466e+38f);
+        lq0[p] = p;
+    }
+}
+
+// Light vertex d (integrator_bdpt_lvc_sk.cu:93-166): every surface hit is
+// stored, whatever its material and contribution (an emitter's BSDF is black:
+// it is stored with zero contribution and ends the subpath); the subpath goes
+// on with the sampled f |cos| / pdf and Russian roulette at every bounce,
+// continue probability min(1, luminance), until its contribution is black.
+__global__ void k_bd_light_shade_ref(SceneView sc, uint64_t seed, uint64_t key0, uint32_t d, uint32_t Dl,
+                                     const uint32_t* q_in, uint32_t* q_out, float4* lray, const int4* lhit,
+                                     float4* lbeta, float4* s_pos, float4* s_nrm, float4* s_beta, float4* s_wi,
+                                     uint8_t* s_valid, WaveCountersDev* wc, uint32_t cur)
+{
+    const uint32_t n = wc->n_ext[cur];
+    const uint64_t ls = seed ^ kLightSalt;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        bool cont = false;
+        uint32_t path = 0;
+        float4 no, nd;
+        if (i < n) {
+            path = q_in[i];
+            const int4 h = lhit[path];
+            if (h.x >= 0) {
+                const float4 o4 = lray[2 * (size_t)path], d4 = lray[2 * (size_t)path + 1];
+                const float t = __int_as_float(h.y);
+                const float3 dd = xyz(d4);
+                const float3 pos = f3(fmaf(dd.x, t, o4.x), fmaf(dd.y, t, o4.y), fmaf(dd.z, t, o4.z));
+                const uint4 tri = sc.tris[h.x];
+                const float4 E = sc.emission[tri.w];
+                const bool emitter = E.x > 0.0f || E.y > 0.0f || E.z > 0.0f;
+                const float3 v0 = xyz(sc.verts[tri.x]), v1 = xyz(sc.verts[tri.y]), v2 = xyz(sc.verts[tri.z]);
+                const float3 ng = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
+                const float3 wo = mul(dd, -1.0f);
+                const float3 nrm = dot3(ng, wo) < 0.0f ? mul(ng, -1.0f) : ng;
+                float4 beta = lbeta[path];
+                const size_t slot = (size_t)path * Dl + (d - 1);
+                s_pos[slot] = make_float4(pos.x, pos.y, pos.z, (float)(d + 1));
+                s_nrm[slot] = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(tri.w));
+                s_beta[slot] = emitter ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : make_float4(beta.x, beta.y, beta.z, 0.0f);
+                s_valid[slot] = 1;
+                if (s_wi) s_wi[slot] = make_float4(wo.x, wo.y, wo.z, dot3(ng, nrm) < 0.0f ? -1.0f : 1.0f);
+                if (!emitter && d < Dl) {
+                    const uint64_t key = key0 + path;
+                    const MaterialDev* lm = layered_material(sc, tri.w);
+                    float3 fac = f3(0.0f, 0.0f, 0.0f), wi = f3(0.0f, 0.0f, 0.0f);
+                    bool ok = false;
+                    if (lm) {
+                        float pdf, eta_io;
+                        bool spec;
+                        const float3 f = material_sample(*lm, frame_from_z(ng), ng, wo, rng_u01(ls, key, 8 + 8 * d),
+                                                         rng_u01(ls, key, 9 + 8 * d), rng_u01(ls, key, 11 + 8 * d), wi,
+                                                         pdf, spec, &eta_io);
+                        if (pdf > 0.0f && (f.x > 0.0f || f.y > 0.0f || f.z > 0.0f)) {
+                            const float k = fabsf(dot3(wi, ng)) / pdf;
+                            fac = f3(f.x * k, f.y * k, f.z * k);
+                            ok = isfinite(fac.x) && isfinite(fac.y) && isfinite(fac.z);
+                        }
+                    } else {
+                        const float3 loc = cosine_hemisphere(rng_u01(ls, key, 8 + 8 * d), rng_u01(ls, key, 9 + 8 * d));
+                        if (loc.z > 0.0f) {
+                            wi = normalize3(to_world(frame_from_z(nrm), loc));
+                            fac = xyz(sc.albedo[tri.w]);
+                            ok = true;
+                        }
+                    }
+                    if (ok) {
+                        const float q = fminf(1.0f, luminance(fac));
+                        cont = q > 0.0f && rng_u01(ls, key, 10 + 8 * d) < q;
+                        if (cont) {
+                            beta.x *= fac.x / q; beta.y *= fac.y / q; beta.z *= fac.z / q;
+                            cont = beta.x > 0.0f || beta.y > 0.0f || beta.z > 0.0f;
+                        }
+                        if (cont) {
+                            lbeta[path] = beta;
+                            no = make_float4(pos.x, pos.y, pos.z, 1.0e-3f * t);
+                            nd = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
+                        }
+                    }
+                }
+            }
+        }
+        const uint32_t slot_out = warp_append(&wc->n_ext[cur ^ 1u], cont);
+        if (cont) {
+            lray[2 * (size_t)path] = no;
+            lray[2 * (size_t)path + 1] = nd;
+            q_out[slot_out] = path;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&wc->stats[4], (unsigned long long)n);
+}
+
+// Camera vertex i = bounce + 1 (integrator_bdpt_lvc_sk.cu:186-434): emission
+// on the first vertex or after a specular bounce (full weight, ends the path),
+// next-event estimation at full weight with the draws of the first vertex at
+// every vertex (the reference re-seeds its NEE generator each bounce), C
+// connections to uniformly chosen cached vertices of this iteration, each
+// weighted 1 / (i + depth of the cached vertex) with no cache-size factor,
+// then the BSDF continuation and Russian roulette from bounce rr_start + 1
+// dividing survivors by 1 - q.  The first `lvc_cap` cached vertices of the
+// iteration (in (path, depth) order) are the cache.
+__global__ void k_bd_cam_shade_ref(SceneView sc, uint64_t seed, uint32_t npix, uint32_t it0, uint32_t i, uint32_t Kc,
+                                   uint32_t C, uint32_t Cs, uint32_t rr_start, float rr_prob, uint32_t lvc_cap,
+                                   const uint32_t* q_in,
+                                   uint32_t* q_out, float4* rays, const int4* hits, float4* T, float4* L, float4* srays,
+                                   float4* sc_out, uint32_t* qs, float4* cray, float4* cc, uint32_t* cq,
+                                   const float4* lvc_pos, const float4* lvc_nrm, const float4* lvc_beta,
+                                   const float4* lvc_wi, const uint32_t* lvc_slot, const uint32_t* lvc_off,
+                                   WaveCountersDev* wc, uint32_t cur)
+{
+    const uint32_t n = wc->n_ext[cur];
+    const float inv_nl = sc.n_lights ? 1.0f / (float)sc.n_lights : 0.0f;
+    const uint32_t b = i - 1;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t qi = base + threadIdx.x;
+        bool cont = false, shadow = false;
+        // Slots 0..C-1: cache connections; slot C: the BSDF half of NEE (an
+        // occlusion segment to the light point it hits, same reduction).
+        bool conn[kMaxConnections + 1];
+        float4 cro[kMaxConnections + 1], crd[kMaxConnections + 1];
+        for (uint32_t c = 0; c <= kMaxConnections; c++) conn[c] = false;
+        uint32_t path = 0;
+        float4 new_o, new_d, so, sd, scv;
+        if (qi < n) {
+            path = q_in[qi];
+            for (uint32_t c = 0; c < Cs; c++) cc[(size_t)path * Cs + c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const int4 h = hits[path];
+            if (h.x >= 0) {
+                const uint64_t key = (uint64_t)it0 * npix + path;
+                const uint32_t li = path / npix;
+                const uint32_t vbase = lvc_off[li], M = min(lvc_off[li + 1] - vbase, lvc_cap);
+                const float4 o4 = rays[2 * (size_t)path], d4 = rays[2 * (size_t)path + 1];
+                const float t = __int_as_float(h.y);
+                const float3 d = xyz(d4);
+                const float3 pos = f3(fmaf(d.x, t, o4.x), fmaf(d.y, t, o4.y), fmaf(d.z, t, o4.z));
+                const float eps = 1.0e-3f * t;
+                const uint4 tri = sc.tris[h.x];
+                const float3 v0 = xyz(sc.verts[tri.x]), v1 = xyz(sc.verts[tri.y]), v2 = xyz(sc.verts[tri.z]);
+                const float3 ng = normalize3(cross3(sub(v1, v0), sub(v2, v0)));
+                const float3 wo = mul(d, -1.0f);
+                float4 Tp = T[path];
+                const uint32_t cst = __float_as_uint(Tp.w);
+                const float4 E = sc.emission[tri.w];
+                if (E.x > 0.0f || E.y > 0.0f || E.z > 0.0f) {
+                    // The camera counts as a specular vertex, so this covers bounce 0 too.
+                    if (!bd_nonspec(cst) && dot3(ng, wo) > 0.0f) {
+                        float4 Lp = L[path];
+                        Lp.x += Tp.x * E.x; Lp.y += Tp.y * E.y; Lp.z += Tp.z * E.z;
+                        L[path] = Lp;
+                    }
+                } else {
+                    const float3 nrm = dot3(ng, wo) < 0.0f ? mul(ng, -1.0f) : ng;
+                    const float4 A = sc.albedo[tri.w];
+                    const MaterialDev* mc = layered_material(sc, tri.w);
+                    const Frame frc = frame_from_z(ng);
+                    const float3 wo_l = to_local(frc, wo);
+                    if (sc.n_lights) {
+                        // compute_direct_lighting's two halves for one uniformly chosen
+                        // emissive triangle j (integrator_bdpt_lvc_sk.cu:233-327): a light
+                        // sample and a BSDF sample, balance-heuristic weights from the
+                        // reference's pdfs (area 0.5, no 1/n_lights), the sum times n_lights.
+                        const float nl = (float)sc.n_lights;
+                        uint32_t j = min((uint32_t)(rng_u01(seed, key, vdim(0, kDimLight)) * nl), sc.n_lights - 1);
+                        const uint4 lt = sc.tris[sc.lights[j]];
+                        const float3 l0 = xyz(sc.verts[lt.x]), l1 = xyz(sc.verts[lt.y]), l2 = xyz(sc.verts[lt.z]);
+                        const float3 ln = normalize3(cross3(sub(l1, l0), sub(l2, l0)));
+                        const float4 Le = sc.emission[lt.w];
+                        {
+                            const float3 lp = sample_triangle(l0, l1, l2, rng_u01(seed, key, vdim(0, kDimLightU)),
+                                                              rng_u01(seed, key, vdim(0, kDimLightV)));
+                            const float3 dv = sub(lp, pos);
+                            const float dist2 = dot3(dv, dv), dist = sqrtf(dist2);
+                            const float3 wi = mul(dv, 1.0f / dist);
+                            const float cos_l = -dot3(ln, wi), cos_s = dot3(nrm, wi);
+                            float3 f = f3(0.0f, 0.0f, 0.0f);
+                            float pdf_b = 0.0f;
+                            if (mc) {
+                                const float3 wi_l = to_local(frc, wi);
+                                f = material_f(*mc, ng, wo, wi, wo_l, wi_l);
+                                pdf_b = material_pdf(*mc, wo_l, wi_l);
+                            } else if (cos_s > 0.0f) {
+                                f = f3(A.x * kInvPi, A.y * kInvPi, A.z * kInvPi);
+                                pdf_b = cos_s * kInvPi;
+                            }
+                            if (cos_l > 0.0f && dist > 0.0f && (f.x > 0.0f || f.y > 0.0f || f.z > 0.0f)) {
+                                const float pdf_l = dist2 / (kRefTriArea * cos_l);
+                                const float k = fabsf(cos_s) * (pdf_l / (pdf_l + pdf_b)) / pdf_l * nl;
+                                scv = make_float4(Tp.x * f.x * Le.x * k, Tp.y * f.y * Le.y * k, Tp.z * f.z * Le.z * k,
+                                                  0.0f);
+                                so = make_float4(pos.x, pos.y, pos.z, eps);
+                                sd = make_float4(wi.x, wi.y, wi.z, dist * (1.0f - 1.0e-3f));
+                                shadow = scv.x > 0.0f || scv.y > 0.0f || scv.z > 0.0f;
+                            }
+                        }
+                        {
+                            float3 wi = f3(0.0f, 0.0f, 0.0f), f = f3(0.0f, 0.0f, 0.0f);
+                            float pdf_b = 0.0f;
+                            if (mc) {
+                                bool spec;
+                                f = material_sample(*mc, frc, ng, wo, rng_u01(seed, key, kDimNeeBsdf),
+                                                    rng_u01(seed, key, kDimNeeBsdf + 1),
+                                                    rng_u01(seed, key, kDimNeeBsdf + 2), wi, pdf_b, spec);
+                                if (spec) pdf_b = 0.0f;  // the reference samples the non-specular layers here
+                            } else {
+                                const float3 loc = cosine_hemisphere(rng_u01(seed, key, kDimNeeBsdf),
+                                                                     rng_u01(seed, key, kDimNeeBsdf + 1));
+                                if (loc.z > 0.0f) {
+                                    wi = normalize3(to_world(frame_from_z(nrm), loc));
+                                    f = f3(A.x * kInvPi, A.y * kInvPi, A.z * kInvPi);
+                                    pdf_b = loc.z * kInvPi;
+                                }
+                            }
+                            float th;
+                            if (pdf_b > 0.0f && (f.x > 0.0f || f.y > 0.0f || f.z > 0.0f) &&
+                                ref_intersect(pos, wi, l0, l1, l2, th) && th > eps) {
+                                const float cth = dot3(ln, mul(wi, -1.0f));   // L(-wi): front side only
+                                const float pdf_l = th * th / (kRefTriArea * fabsf(cth));
+                                const float k = (cth > 0.0f ? 1.0f : 0.0f) * fabsf(dot3(wi, nrm)) *
+                                                (pdf_b / (pdf_b + pdf_l)) / pdf_b * nl;
+                                const float4 cv = make_float4(Tp.x * f.x * Le.x * k, Tp.y * f.y * Le.y * k,
+                                                              Tp.z * f.z * Le.z * k, 0.0f);
+                                if (cv.x > 0.0f || cv.y > 0.0f || cv.z > 0.0f) {
+                                    // The reference counts it when the BSDF ray's closest hit is
+                                    // triangle j: the segment up to it must be unoccluded.
+                                    cc[(size_t)path * Cs + C] = cv;
+                                    cro[C] = make_float4(pos.x, pos.y, pos.z, eps);
+                                    crd[C] = make_float4(wi.x, wi.y, wi.z, th * (1.0f - 1.0e-3f));
+                                    conn[C] = true;
+                                }
+                            }
+                        }
+                    }
+                    if (M > 0) {
+                        for (uint32_t c = 0; c < C; c++) {
+                            const uint32_t v = lvc_slot[vbase + min((uint32_t)(rng_u01(seed, key, vdim(b, 6) +
+                                                                                         520u * (c + 1)) * (float)M),
+                                                                    M - 1)];
+                            const float4 vp4 = lvc_pos[v];
+                            const float depth = vp4.w - 1.0f;  // the reference's m_depth: 1 at the first hit
+                            const float4 vn4 = lvc_nrm[v];
+                            const float3 dv = sub(xyz(vp4), pos);
+                            const float dist2 = dot3(dv, dv), dist = sqrtf(dist2);
+                            if (!(dist > 0.0f)) continue;
+                            const float3 dir = mul(dv, 1.0f / dist);
+                            const float cos_c = dot3(nrm, dir), cos_v = -dot3(xyz(vn4), dir);
+                            const uint32_t vmat = __float_as_uint(vn4.w);
+                            const MaterialDev* mv = lvc_wi ? layered_material(sc, vmat) : nullptr;
+                            const float4 Av = sc.albedo[vmat];
+                            const float4 bv = lvc_beta[v];
+                            float3 fc = f3(0.0f, 0.0f, 0.0f), fv = f3(0.0f, 0.0f, 0.0f);
+                            if (mc) fc = material_f(*mc, ng, wo, dir, wo_l, to_local(frc, dir));
+                            else if (cos_c > 0.0f) fc = f3(A.x * kInvPi, A.y * kInvPi, A.z * kInvPi);
+                            if (mv) {
+                                // material_f(lvc material, wo = toward the previous light vertex,
+                                // wi = toward the camera vertex), as the reference orders them.
+                                const float4 w4 = lvc_wi[v];
+                                const float3 ngv = mul(xyz(vn4), w4.w), wov = xyz(w4), wiv = mul(dir, -1.0f);
+                                const Frame frv = frame_from_z(ngv);
+                                fv = material_f(*mv, ngv, wov, wiv, to_local(frv, wov), to_local(frv, wiv));
+                            } else if (cos_v > 0.0f) {
+                                fv = f3(Av.x * kInvPi, Av.y * kInvPi, Av.z * kInvPi);
+                            }
+                            const float g = fabsf(cos_c) * fabsf(cos_v) / dist2 / ((float)i + depth);
+                            const float4 cv = make_float4(Tp.x * fc.x * fv.x * bv.x * g, Tp.y * fc.y * fv.y * bv.y * g,
+                                                          Tp.z * fc.z * fv.z * bv.z * g, 0.0f);
+                            if (!(cv.x > 0.0f || cv.y > 0.0f || cv.z > 0.0f)) continue;
+                            cc[(size_t)path * Cs + c] = cv;
+                            cro[c] = make_float4(pos.x, pos.y, pos.z, eps);
+                            crd[c] = make_float4(dir.x, dir.y, dir.z, dist * (1.0f - 1.0e-3f));
+                            conn[c] = true;
+                        }
+                    }
+                    if (i < Kc) {
+                        float3 wi = f3(0.0f, 0.0f, 0.0f);
+                        bool ok = false, spec = false;
+                        if (mc) {
+                            float pdf;
+                            const float3 f = material_sample(*mc, frc, ng, wo, rng_u01(seed, key, vdim(b, kDimBsdfU)),
+                                                             rng_u01(seed, key, vdim(b, kDimBsdfV)),
+                                                             rng_u01(seed, key, vdim(b, kDimBsdfC)), wi, pdf, spec);
+                            if (pdf > 0.0f && (f.x > 0.0f || f.y > 0.0f || f.z > 0.0f)) {
+                                const float k = fabsf(dot3(wi, ng)) / pdf;
+                                Tp.x *= f.x * k; Tp.y *= f.y * k; Tp.z *= f.z * k;
+                                ok = true;
+                            }
+                        } else {
+                            const float3 loc = cosine_hemisphere(rng_u01(seed, key, vdim(b, kDimBsdfU)),
+                                                                 rng_u01(seed, key, vdim(b, kDimBsdfV)));
+                            if (loc.z > 0.0f) {
+                                wi = normalize3(to_world(frame_from_z(nrm), loc));
+                                Tp.x *= A.x; Tp.y *= A.y; Tp.z *= A.z;
+                                ok = true;
+                            }
+                        }
+                        if (ok) {
+                            Tp.w = __uint_as_float(bd_advance(cst, !spec));
+                            cont = isfinite(Tp.x) && isfinite(Tp.y) && isfinite(Tp.z) &&
+                                   (Tp.x > 0.0f || Tp.y > 0.0f || Tp.z > 0.0f);
+                            if (cont && b > rr_start) {
+                                const float q = fminf(rr_prob, luminance(xyz(Tp)));
+                                if (!(rng_u01(seed, key, vdim(b, kDimRR)) < q)) cont = false;
+                                else { const float inv = 1.0f / (1.0f - q); Tp.x *= inv; Tp.y *= inv; Tp.z *= inv; }
+                            }
+                            if (cont) {
+                                T[path] = Tp;
+                                new_o = make_float4(pos.x, pos.y, pos.z, eps);
+                                new_d = make_float4(wi.x, wi.y, wi.z, 3.402823466e+38f);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        const uint32_t s_slot = warp_append(&wc->n_shadow, shadow);
+        if (shadow) {
+            srays[2 * (size_t)path] = so;
+            srays[2 * (size_t)path + 1] = sd;
+            sc_out[path] = scv;
+            qs[s_slot] = path;
+        }
+        for (uint32_t c = 0; c < Cs; c++) {
+            const uint32_t c_slot = warp_append(&wc->n_conn, conn[c]);
+            if (conn[c]) {
+                const size_t cs = (size_t)path * Cs + c;
+                cray[2 * cs] = cro[c];
+                cray[2 * cs + 1] = crd[c];
+                cq[c_slot] = (uint32_t)cs;
+            }
+        }
+        const uint32_t e_slot = warp_append(&wc->n_ext[cur ^ 1u], cont);
+        if (cont) {
+            rays[2 * (size_t)path] = new_o;
+            rays[2 * (size_t)path + 1] = new_d;
+            q_out[e_slot] = path;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&wc->stats[i == 1 ? 0 : 1], (unsigned long long)n);
+}
+
 __global__ void k_bd_stats(WaveCountersDev* wc)
 {
     wc->stats[2] += wc->n_shadow;
@@ -1318,6 +1753,7 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
     if (!it || !cam || !p || !d_ao) return fail(RB2_EINVAL, "null argument");
     it->ev_used = 0;
     if (p->samples == 0 || !(p->radius > 0.0f)) return fail(RB2_EINVAL, "AO needs samples > 0 and radius > 0");
+    if (p->compat & ~(uint32_t)RB2_COMPAT_AO_DIRECTION) return fail(RB2_EINVAL, "AO compat flags: RB2_COMPAT_AO_DIRECTION only");
     cudaStream_t s = (cudaStream_t)stream;
     const uint64_t npix = (uint64_t)cam->width * cam->height;
     if (npix > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image too large");
@@ -1360,6 +1796,7 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
     src.samples = p->samples;
     src.radius = p->radius;
     src.seed = p->seed;
+    src.compat = p->compat;
     if ((rc = launch_persistent(src, src.n_slots, it, bv, s))) return rc;
     // 4. AO = unoccluded fraction (misses contribute 0, integrator_ao.cu:56-84).
     rb2dev::k_ao_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_hits, it->d_count, (uint32_t)npix, p->samples, d_ao);
@@ -1373,6 +1810,10 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
     it->ev_used = 0;
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
     if (p->max_depth > 64) return fail(RB2_EINVAL, "max_depth must be <= 64");
+    if (p->compat & ~(uint32_t)(RB2_COMPAT_RR_DIVISOR | RB2_COMPAT_NEE_RESEED))
+        return fail(RB2_EINVAL, "PT compat flags: RB2_COMPAT_RR_DIVISOR and RB2_COMPAT_NEE_RESEED only");
+    if ((p->compat & RB2_COMPAT_RR_DIVISOR) && !(p->rr_prob < 1.0f))
+        return fail(RB2_EINVAL, "RB2_COMPAT_RR_DIVISOR divides by 1 - q: rr_prob must be < 1");
     cudaStream_t s = (cudaStream_t)stream;
     const uint64_t npix = (uint64_t)cam->width * cam->height;
     if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");
@@ -1416,8 +1857,8 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
                                     ps.hit, nullptr, nullptr};
             if ((rc = launch_persistent(ext, paths, it, bv, s))) return rc;
             rb2dev::k_pt_shade<<<g, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, s0, b, p->max_depth, p->rr_start, p->rr_prob,
-                                                ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L, ps.sray, ps.sc,
-                                                ps.qs, wc, cur);
+                                                p->compat, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L,
+                                                ps.sray, ps.sc, ps.qs, wc, cur);
             RB2_CUDA(cudaGetLastError(), "PT shade");
             rb2dev::k_pt_stats_shadow<<<1, 1, 0, s>>>(wc);
             rb2dev::QueueSource shadow{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop),
@@ -1511,31 +1952,75 @@ int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_rayc
 int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_params* p, float* d_rgb, void* stream)
 {
     if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
+    rb2_bdpt_lvc_params q{};
+    q.spp = p->spp;
+    q.num_light_paths = p->num_light_paths;
+    q.light_path_rrstart = p->rr_start;
+    q.cam_path_rrstart = p->rr_start;
+    q.cam_path_rrprob = p->rr_prob;
+    q.num_cam_path_connections = p->connections;
+    q.estimator = RB2_BDPT_ESTIMATOR_UNBIASED;
+    q.max_path_length = p->max_path_length;
+    q.seed = p->seed;
+    return rb2_render_bdpt_lvc(it, cam, &q, d_rgb, stream);
+}
+
+int rb2_render_bdpt_lvc(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_lvc_params* p, float* d_rgb,
+                        void* stream)
+{
+    if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
     it->ev_used = 0;
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
-    if (p->max_path_length < 1 || p->max_path_length > 16) return fail(RB2_EINVAL, "max_path_length must be in [1, 16]");
-    if (p->connections < 1 || p->connections > rb2dev::kMaxConnections) return fail(RB2_EINVAL, "connections must be in [1, 8]");
+    if (p->estimator > RB2_BDPT_ESTIMATOR_REFERENCE) return fail(RB2_EINVAL, "unknown BDPT estimator");
+    if (p->mode > RB2_BDPT_MODE_SORT) return fail(RB2_EINVAL, "unknown BDPT mode (sk, mk, sort)");
+    const bool ref = p->estimator == RB2_BDPT_ESTIMATOR_REFERENCE;
+    if (!ref && (p->max_path_length < 1 || p->max_path_length > 16))
+        return fail(RB2_EINVAL, "max_path_length must be in [1, 16]");
+    if (ref && (p->num_light_path_max_depth < 1 || p->num_light_path_max_depth > 16))
+        return fail(RB2_EINVAL, "num_light_path_max_depth must be in [1, 16] (it bounds the light-vertex cache)");
+    if (ref && p->num_cam_path_max_depth > 63) return fail(RB2_EINVAL, "num_cam_path_max_depth must be <= 63");
+    if (ref && !(p->cam_path_rrprob < 1.0f))
+        return fail(RB2_EINVAL, "the reference estimator divides by 1 - q: cam_path_rrprob must be < 1");
+    if (p->num_cam_path_connections < 1 || p->num_cam_path_connections > rb2dev::kMaxConnections)
+        return fail(RB2_EINVAL, "num_cam_path_connections must be in [1, 8]");
     cudaStream_t s = (cudaStream_t)stream;
     const uint64_t npix = (uint64_t)cam->width * cam->height;
     if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");
-    const uint32_t K = p->max_path_length, C = p->connections;
-    const uint32_t Dl = K >= 2 ? K - 2 : 0;  // cached light vertices y1..y_{K-2} suffice for k <= K
+    // K: camera vertices of a path (unbiased: the whole-path cap in segments,
+    // which also bounds the camera subpath; reference: bounces 0..max depth).
+    const uint32_t K = ref ? p->num_cam_path_max_depth + 1 : p->max_path_length;
+    const uint32_t C = p->num_cam_path_connections;
+    // Connection-ray slots per camera vertex (the reference estimator adds the
+    // BSDF half of its NEE as one more occlusion segment).
+    const uint32_t Cs = ref ? C + 1 : C;
+    // Cached light vertices per subpath: y1..y_{K-2} suffice for paths of at most
+    // K segments; the reference estimator keeps up to num_light_path_max_depth.
+    const uint32_t Dl = ref ? p->num_light_path_max_depth : (K >= 2 ? K - 2 : 0);
     const uint64_t NL = p->num_light_paths ? p->num_light_paths : npix;
+    const uint32_t rr_light = p->light_path_rrstart, rr_cam = p->cam_path_rrstart;
+    const float rr_prob = p->cam_path_rrprob;
     // Iterations per wave: as many as fit the wave budget in camera and light
     // paths, spread evenly over the waves, with every wave index 32-bit.
     const uint64_t per_iter = NL * std::max<uint32_t>(Dl, 1);   // cache slots of one iteration
     if (per_iter > 0xFFFFFFFFull) return fail(RB2_EINVAL, "num_light_paths x cached depth must fit 32-bit slot indices");
     const uint64_t budget = it->wave_paths ? it->wave_paths : kBdptWavePaths;
     uint64_t wmax = std::max<uint64_t>(1, budget / std::max(npix, NL));
-    wmax = std::min<uint64_t>({wmax, (uint64_t)p->spp, (uint64_t)kMaxBdptWave, 0xFFFFFFFFull / (npix * C),
+    wmax = std::min<uint64_t>({wmax, (uint64_t)p->spp, (uint64_t)kMaxBdptWave, 0xFFFFFFFFull / (npix * Cs),
                                0xFFFFFFFFull / per_iter});
     wmax = std::max<uint64_t>(wmax, 1);
     const uint32_t n_waves = (uint32_t)((p->spp + wmax - 1) / wmax);
     const uint32_t Wv = (p->spp + n_waves - 1) / n_waves;
     const uint64_t n_slots = per_iter * Wv;
+    // The reference estimator's preparation pass traces num_prep_paths light
+    // subpaths through the same buffers (integrator_bdpt_lvc_sk.cu:447-470).
+    const uint64_t n_prep = ref ? p->num_prep_paths : 0;
+    if (n_prep * std::max<uint32_t>(Dl, 1) > 0xFFFFFFFFull)
+        return fail(RB2_EINVAL, "num_prep_paths x cached depth must fit 32-bit slot indices");
     int rc;
     if ((rc = ensure_path_state(it->ps, npix * Wv))) return rc;
-    if ((rc = ensure_bdpt_state(it->bd, NL * Wv, n_slots, npix * Wv * C))) return rc;
+    if ((rc = ensure_bdpt_state(it->bd, std::max<uint64_t>(NL * Wv, n_prep),
+                                std::max<uint64_t>(n_slots, n_prep * std::max<uint32_t>(Dl, 1)), npix * Wv * Cs)))
+        return rc;
     if ((rc = grow(it->d_accum, it->cap_accum, npix))) return rc;
     const bool filtered = it->filter.kind != RB2_FILTER_NONE;
     rb2dev::FilmArgs fa{};
@@ -1561,31 +2046,66 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
     BdptState& bd = it->bd;
     // Light-vertex directions are cached only when a layered material needs them.
     float4* s_wi = it->scene->layered ? bd.s_wi : nullptr;
+    // Light subpaths of a wave (or of the preparation pass) into the sparse cache.
+    auto light_pass = [&](uint64_t key0, uint64_t n_light) -> int {
+        const unsigned gl = grid_for(n_light, it->sms);
+        RB2_CUDA(cudaMemsetAsync(bd.s_valid, 0, n_light * std::max<uint32_t>(Dl, 1), s), "cache reset");
+        if (ref)
+            rb2dev::k_bd_light_init_ref<<<gl, 256, 0, s>>>(sv, p->seed, key0, (uint32_t)n_light, bd.lray, bd.lbeta,
+                                                           bd.lq[0], wc);
+        else
+            rb2dev::k_bd_light_init<<<gl, 256, 0, s>>>(sv, p->seed, key0, (uint32_t)n_light, bd.lray, bd.lbeta,
+                                                       bd.lq[0], wc);
+        RB2_CUDA(cudaGetLastError(), "BDPT light init");
+        uint32_t lc = 0;
+        for (uint32_t d = 1; d <= Dl; d++) {
+            rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, lc ^ 1u);
+            rb2dev::QueueSource lsrc{bn, bw, bv.triidx, bd.lq[lc], &wc->n_ext[lc], bd.lray, &wc->head_ext,
+                                     rb2dev::kClosest, bd.lhit, nullptr, nullptr};
+            int r = launch_persistent(lsrc, n_light, it, bv, s);
+            if (r) return r;
+            if (ref)
+                rb2dev::k_bd_light_shade_ref<<<gl, 256, 0, s>>>(sv, p->seed, key0, d, Dl, bd.lq[lc], bd.lq[lc ^ 1u],
+                                                                bd.lray, bd.lhit, bd.lbeta, bd.s_pos, bd.s_nrm,
+                                                                bd.s_beta, s_wi, bd.s_valid, wc, lc);
+            else
+                rb2dev::k_bd_light_shade<<<gl, 256, 0, s>>>(sv, p->seed, key0, d, Dl, rr_light, rr_prob, bd.lq[lc],
+                                                            bd.lq[lc ^ 1u], bd.lray, bd.lhit, bd.lbeta, bd.s_pos,
+                                                            bd.s_nrm, bd.s_beta, s_wi, bd.s_valid, wc, lc);
+            RB2_CUDA(cudaGetLastError(), "BDPT light shade");
+            lc ^= 1u;
+        }
+        return RB2_OK;
+    };
+    // Cache capacity of one iteration (reference estimator): 1.1 x the mean
+    // number of vertices a preparation subpath stored x num_light_paths, in
+    // single precision as the reference computes it (integrator_bdpt_lvc_sk.cu:466-470).
+    uint32_t lvc_cap = 0xFFFFFFFFu;
+    if (n_prep > 0) {
+        if ((rc = light_pass((uint64_t)p->spp * NL, n_prep))) return rc;
+        const uint64_t prep_slots = n_prep * Dl;
+        const uint64_t n_chunks = (prep_slots + rb2dev::kScanChunk - 1) / rb2dev::kScanChunk;
+        rb2dev::k_lvc_count<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(bd.s_valid, prep_slots, bd.block_sums);
+        rb2dev::k_lvc_scan_top<<<1, 1024, 0, s>>>(bd.block_sums, (uint32_t)n_chunks, wc);
+        RB2_CUDA(cudaGetLastError(), "preparation count");
+        uint32_t total = 0;
+        RB2_CUDA(cudaMemcpyAsync(&total, &wc->lvc_count, sizeof(total), cudaMemcpyDeviceToHost, s), "preparation read");
+        RB2_CUDA(cudaStreamSynchronize(s), "preparation sync");
+        const float avg = (float)total / (float)n_prep;
+        const float cap = std::ceil(1.1f * avg * (float)NL);
+        lvc_cap = cap >= 4294967295.0f ? 0xFFFFFFFFu : (uint32_t)cap;
+    }
     for (uint32_t it0 = 0; it0 < p->spp; it0 += Wv) {
         // Wave of w iterations: light path l is path l % NL of iteration it0 + l / NL,
         // camera path c is pixel c % npix of iteration it0 + c / npix.  The random
         // keys are those of the iterations run one at a time.
         const uint32_t w = std::min(Wv, p->spp - it0);
         const uint64_t n_light = NL * w, n_cam = npix * w, wave_slots = per_iter * w;
-        const unsigned gl = grid_for(n_light, it->sms), gc = grid_for(n_cam, it->sms), gp = grid_for(npix, it->sms);
+        const unsigned gc = grid_for(n_cam, it->sms), gp = grid_for(npix, it->sms);
         const uint64_t n_chunks = (wave_slots + rb2dev::kScanChunk - 1) / rb2dev::kScanChunk;
         // ---- light pass: subpaths into the sparse cache, then compaction.
-        RB2_CUDA(cudaMemsetAsync(bd.s_valid, 0, wave_slots, s), "cache reset");
-        rb2dev::k_bd_light_init<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)it0 * NL, (uint32_t)n_light, bd.lray,
-                                                   bd.lbeta, bd.lq[0], wc);
-        RB2_CUDA(cudaGetLastError(), "BDPT light init");
+        if ((rc = light_pass((uint64_t)it0 * NL, n_light))) return rc;
         uint32_t cur = 0;
-        for (uint32_t d = 1; d <= Dl; d++) {
-            rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
-            rb2dev::QueueSource lsrc{bn, bw, bv.triidx, bd.lq[cur], &wc->n_ext[cur], bd.lray, &wc->head_ext,
-                                     rb2dev::kClosest, bd.lhit, nullptr, nullptr};
-            if ((rc = launch_persistent(lsrc, n_light, it, bv, s))) return rc;
-            rb2dev::k_bd_light_shade<<<gl, 256, 0, s>>>(sv, p->seed, (uint64_t)it0 * NL, d, Dl, p->rr_start, p->rr_prob,
-                                                        bd.lq[cur], bd.lq[cur ^ 1u], bd.lray, bd.lhit, bd.lbeta, bd.s_pos,
-                                                        bd.s_nrm, bd.s_beta, s_wi, bd.s_valid, wc, cur);
-            RB2_CUDA(cudaGetLastError(), "BDPT light shade");
-            cur ^= 1u;
-        }
         rb2dev::k_lvc_count<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(bd.s_valid, wave_slots, bd.block_sums);
         rb2dev::k_lvc_scan_top<<<1, 1024, 0, s>>>(bd.block_sums, (uint32_t)n_chunks, wc);
         rb2dev::k_lvc_scatter<<<(unsigned)n_chunks, rb2dev::kScanThreads, 0, s>>>(
@@ -1603,10 +2123,17 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             rb2dev::QueueSource ext{bn, bw, bv.triidx, ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext,
                                     rb2dev::kClosest, ps.hit, nullptr, nullptr};
             if ((rc = launch_persistent(ext, n_cam, it, bv, s))) return rc;
-            rb2dev::k_bd_cam_shade<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, it0, i, K, C, p->rr_start, p->rr_prob,
-                                                      (float)NL, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L,
-                                                      ps.sray, ps.sc, ps.qs, bd.cray, bd.cc, bd.cq, bd.s_pos, bd.s_nrm,
-                                                      bd.s_beta, s_wi, bd.d_slot, bd.lvc_off, wc, cur);
+            if (ref)
+                rb2dev::k_bd_cam_shade_ref<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, it0, i, K, C, Cs, rr_cam,
+                                                              rr_prob, lvc_cap, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T,
+                                                              ps.L, ps.sray, ps.sc, ps.qs, bd.cray, bd.cc, bd.cq,
+                                                              bd.s_pos, bd.s_nrm, bd.s_beta, s_wi, bd.d_slot,
+                                                              bd.lvc_off, wc, cur);
+            else
+                rb2dev::k_bd_cam_shade<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, it0, i, K, C, rr_cam, rr_prob,
+                                                          (float)NL, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T,
+                                                          ps.L, ps.sray, ps.sc, ps.qs, bd.cray, bd.cc, bd.cq, bd.s_pos,
+                                                          bd.s_nrm, bd.s_beta, s_wi, bd.d_slot, bd.lvc_off, wc, cur);
             RB2_CUDA(cudaGetLastError(), "BDPT camera shade");
             rb2dev::k_bd_stats<<<1, 1, 0, s>>>(wc);
             rb2dev::QueueSource nee{bn, bw, bv.triidx, ps.qs, &wc->n_shadow, ps.sray, &wc->head_shadow,
@@ -1614,8 +2141,8 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
             if ((rc = launch_persistent(nee, n_cam, it, bv, s))) return rc;
             rb2dev::QueueSource con{bn, bw, bv.triidx, bd.cq, &wc->n_conn, bd.cray, &wc->head_conn,
                                     rb2dev::kOcclusion, nullptr, nullptr, bd.cc};
-            if ((rc = launch_persistent(con, n_cam * C, it, bv, s))) return rc;
-            rb2dev::k_bd_conn_reduce<<<gc, 256, 0, s>>>(ps.q[cur], wc, cur, C, bd.cc, ps.L);
+            if ((rc = launch_persistent(con, n_cam * Cs, it, bv, s))) return rc;
+            rb2dev::k_bd_conn_reduce<<<gc, 256, 0, s>>>(ps.q[cur], wc, cur, Cs, bd.cc, ps.L);
             RB2_CUDA(cudaGetLastError(), "BDPT connection reduce");
             cur ^= 1u;
         }

@@ -10,7 +10,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._native import AoParams, BdptParams, DevScene, IsectBuffer, PtParams, RayCastParams, RenderStats, check, lib
+from ._native import AoParams, BdptLvcParams, DevScene, IsectBuffer, PtParams, RayCastParams, RenderStats, check, lib
 from ._native import BsdfLayer as _BsdfLayer
 from ._native import Filter as _Filter
 from ._native import MaterialDesc as _MaterialDesc
@@ -205,11 +205,17 @@ def write_pfm(path: str, rgb: np.ndarray, width: int, height: int) -> None:
     check(lib().rb2_image_write_pfm(str(path).encode(), _ptr(rgb), width, height))
 
 
+# Reference-compatibility switches (rb2_render.h): each reproduces one
+# behaviour of the reference that the integrators otherwise correct.
+COMPAT_AO_DIRECTION, COMPAT_RR_DIVISOR, COMPAT_NEE_RESEED = 1, 2, 4
+
+
 @dataclass
 class AmbientOcclusionIntegratorParams:
     samples: int = 16
     radius: float = 0.1
     seed: int = 7
+    compat: int = 0                 # COMPAT_AO_DIRECTION: the reference's AO direction formula
 
 
 @dataclass
@@ -220,10 +226,22 @@ class PathIntegratorParams:
     rr_prob: float = 0.95
     seed: int = 11
     spp_per_wave: int = 0
+    compat: int = 0                 # COMPAT_RR_DIVISOR | COMPAT_NEE_RESEED
+
+
+BDPT_MODES = {"sk": 0, "mk": 1, "sort": 2}
+BDPT_ESTIMATORS = {"unbiased": 0, "reference": 1}
 
 
 @dataclass
 class BidirectionalPathIntegratorLvcParams:
+    """The reference's BidirectionalPathIntegratorLvcParams (core/params.h:108-120)
+    with its integrator file's names, plus `estimator`: "unbiased" (this
+    library's estimator; max_path_length caps the whole path) or "reference"
+    (the reference's own estimator: preparation pass, 1 / ((bounce + 1) +
+    depth) connection weights, separate light / camera depths; see
+    rb2_render.h).  rr_start / rr_prob give both subpaths' Russian roulette
+    unless light_path_rrstart / cam_path_rrstart / cam_path_rrprob are set."""
     spp: int = 16
     max_path_length: int = 6
     num_light_paths: int = 0        # 0: one light subpath per pixel per iteration
@@ -231,6 +249,24 @@ class BidirectionalPathIntegratorLvcParams:
     rr_start: int = 3
     rr_prob: float = 0.95
     seed: int = 13
+    estimator: str = "unbiased"
+    num_prep_paths: int = 10000
+    num_light_path_max_depth: int = 8
+    light_path_rrstart: int | None = None
+    num_cam_path_max_depth: int = 8
+    cam_path_rrstart: int | None = None
+    cam_path_rrprob: float | None = None
+    num_cam_path_sample_connections: int = 10
+    mode: str = "sk"
+
+    def c_struct(self) -> BdptLvcParams:
+        return BdptLvcParams(
+            self.spp, self.num_prep_paths, self.num_light_paths, self.num_light_path_max_depth,
+            self.rr_start if self.light_path_rrstart is None else self.light_path_rrstart,
+            self.num_cam_path_max_depth, self.rr_start if self.cam_path_rrstart is None else self.cam_path_rrstart,
+            self.rr_prob if self.cam_path_rrprob is None else self.cam_path_rrprob,
+            self.num_cam_path_sample_connections, self.connections, BDPT_MODES[self.mode],
+            BDPT_ESTIMATORS[self.estimator], self.max_path_length, 0, self.seed)
 
 
 # RayCastShade (core/params.h:139-146), by the names the reference's integrator
@@ -286,7 +322,7 @@ class Integrator:
         n = camera.width * camera.height
         if out is None:
             out = torch.empty((n,), dtype=torch.float32, device="cuda")
-        p = AoParams(params.samples, params.radius, params.seed)
+        p = AoParams(params.samples, params.radius, params.seed, params.compat, 0)
         check(lib().rb2_render_ao(self._it, C.byref(camera.c), C.byref(p), _ptr(out), _stream_handle(stream)))
         return out
 
@@ -296,7 +332,7 @@ class Integrator:
         if out is None:
             out = torch.empty((n, 3), dtype=torch.float32, device="cuda")
         p = PtParams(params.spp, params.max_depth, params.rr_start, params.rr_prob, params.seed,
-                     params.spp_per_wave, 0)
+                     params.spp_per_wave, params.compat)
         check(lib().rb2_render_pt(self._it, C.byref(camera.c), C.byref(p), _ptr(out), _stream_handle(stream)))
         return out
 
@@ -305,9 +341,8 @@ class Integrator:
         n = camera.width * camera.height
         if out is None:
             out = torch.empty((n, 3), dtype=torch.float32, device="cuda")
-        p = BdptParams(params.spp, params.max_path_length, params.num_light_paths, params.connections,
-                       params.rr_start, params.rr_prob, params.seed)
-        check(lib().rb2_render_bdpt(self._it, C.byref(camera.c), C.byref(p), _ptr(out), _stream_handle(stream)))
+        p = params.c_struct()
+        check(lib().rb2_render_bdpt_lvc(self._it, C.byref(camera.c), C.byref(p), _ptr(out), _stream_handle(stream)))
         return out
 
     def render_raycast(self, camera, params: RayCastIntegratorParams, out=None, stream=None):

@@ -308,3 +308,43 @@ def test_tie_scene_produces_ties_on_both_trees(rb, orc):
         bf = orc.bruteforce(woop, tri, rays)
         assert (h["t"] >= bf["t"]).all()
         assert (h["t"] == bf["t"]).mean() > 0.99
+
+
+def test_compat_formulas_pinned_to_the_reference(orc):
+    """The two reference formulas the compatibility modes restate, against the
+    reference's compiled functions: the AO direction of
+    cosine_sample_hemisphere_normal (core/montecarlo.cu:133-151; NaN exactly
+    where the oracle reports it undefined) and DiffuseAreaLight::Le's
+    direction and Le / pdf (core/lights.cu:63-69)."""
+    if not orc.have_ref():
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.Generator(np.random.PCG64(8))
+    normals = list(rng.normal(size=(200, 3))) + [np.array(v, float) for v in
+                                                 ((0, 1, 0), (0, -1, 0), (1, 0, 0), (-1, 0, 0), (0, 0, 1), (0, 0, -1))]
+    undefined = 0
+    for n in normals:
+        n = np.asarray(n, np.float32)
+        n = (n / np.sqrt(np.dot(n, n))).astype(np.float32)
+        for u1, u2 in rng.uniform(0, 1, size=(8, 2)).astype(np.float32):
+            ref = orc.ref_ao_direction(n, u1, u2)
+            got = orc.ao_ref_dir(n.astype(np.float64), float(u1), float(u2))
+            if got is None:
+                undefined += 1
+                assert np.isnan(ref).any()
+            else:
+                assert np.allclose(got, ref, atol=2e-6), (n, u1, u2, got, ref)
+    assert undefined > 0  # normals along +-z have no X axis there
+    v0, v1, v2 = np.array([0.2, 1.0, 0.1]), np.array([0.6, 1.0, 0.1]), np.array([0.2, 1.0, 0.5])
+    emit = np.array([10.0, 10.0, 10.0])
+    ln = np.cross(v1 - v0, v2 - v0)
+    area = 0.5 * np.linalg.norm(ln)
+    ln = ln / np.linalg.norm(ln)
+    lit = 0
+    for u in rng.uniform(0, 1, size=(400, 4)).astype(np.float32):
+        _, d_ref, pdf, L = orc.ref_light_le(v0, v1, v2, emit, u)
+        d, k = orc.light_le_ref(ln, area, float(u[2]), float(u[3]))
+        assert np.allclose(d, d_ref, atol=2e-6)
+        contrib = L[0] / pdf if pdf > 0 else 0.0
+        assert np.isclose(emit[0] * k, contrib, rtol=1e-5, atol=1e-6), (u, k, L, pdf)
+        lit += k > 0
+    assert 0 < lit < 400  # only directions toward the light's front carry Le
