@@ -315,7 +315,8 @@ def test_compat_formulas_pinned_to_the_reference(orc):
     reference's compiled functions: the AO direction of
     cosine_sample_hemisphere_normal (core/montecarlo.cu:133-151; NaN exactly
     where the oracle reports it undefined) and DiffuseAreaLight::Le's
-    direction and Le / pdf (core/lights.cu:63-69)."""
+    direction and Le / pdf (core/lights.cu:63-69), whose pdf uses the
+    reference's triangle area of 0.5."""
     if not orc.have_ref():
         pytest.skip("oracle/_ref not built")
     rng = np.random.Generator(np.random.PCG64(8))
@@ -339,10 +340,13 @@ def test_compat_formulas_pinned_to_the_reference(orc):
     ln = np.cross(v1 - v0, v2 - v0)
     area = 0.5 * np.linalg.norm(ln)
     ln = ln / np.linalg.norm(ln)
+    # The reference's compute_area (core/primitives.h:273-276) halves the length
+    # of the already normalized normal: every triangle has area 0.5 in its pdfs.
+    assert abs(area - 0.08) < 1e-12
     lit = 0
     for u in rng.uniform(0, 1, size=(400, 4)).astype(np.float32):
         _, d_ref, pdf, L = orc.ref_light_le(v0, v1, v2, emit, u)
-        d, k = orc.light_le_ref(ln, area, float(u[2]), float(u[3]))
+        d, k = orc.light_le_ref(ln, 0.5, float(u[2]), float(u[3]))
         assert np.allclose(d, d_ref, atol=2e-6)
         contrib = L[0] / pdf if pdf > 0 else 0.0
         assert np.isclose(emit[0] * k, contrib, rtol=1e-5, atol=1e-6), (u, k, L, pdf)
