@@ -109,22 +109,30 @@ def _bdpt_reference_params(spp, seed, **kw):
 
 
 def test_bdpt_reference_estimator_converges_to_host(rb, orc, cuda):
+    """In a room 5 units on a side, where the light's triangles have area 0.5,
+    the reference's triangle-area quirk (every area 0.5) is neutral and the
+    estimator's variance is moderate.  (In the unit room its light-sample pdf
+    is 25x too small and its light subpaths carry 25x their power, so its
+    connections are heavy-tailed: two 2048-iteration host images differ by
+    7 % RMSE there, against 1.4 % here.)"""
     from renderbox2_b200.configs import CONFIG2 as C2
     from renderbox2_b200.render import BidirectionalPathIntegratorLvcParams, DeviceScene, Integrator
-    room = _room(rb)
+    rs = 5.0
+    room = rb.RoomScene(seed=2, n_boxes=10, n_spheres=60, sphere_subdiv=2, n_lights=1, emission=10.0, room_size=rs)
     bvh = rb.BVH(room)
+    eye, look = [x * rs for x in C2["eye"]], [x * rs for x in C2["lookat"]]
     W, H = 96, 54
     ii, jj, pix = _grid(W, H, 3)
     n_iter = 2048
     rng = np.random.Generator(np.random.PCG64(41))
     base = np.tile(np.stack([ii.ravel(), jj.ravel()], 1), (n_iter, 1))
     xy = (base + rng.uniform(0, 1, size=base.shape)).astype(np.float32)
-    rays = orc.ref_camera_rays(C2["eye"], C2["lookat"], C2["up"], W, H, C2["fov"], xy)
+    rays = orc.ref_camera_rays(eye, look, C2["up"], W, H, C2["fov"], xy)
     ref = orc.bdpt_ref(bvh.buffers_view(), room.vertices, room.indices, room.material_ids, room.albedo,
                        room.emission, room.light_ids_to_primitive_ids, rays, pix.size, n_iter, 10000, 2048, 8, 8, 4,
                        0.3, 1, seed=43)
     it = Integrator(rb.CudaTracer(bvh), DeviceScene(room))
-    cam = rb.PerspectiveCamera(C2["eye"], C2["lookat"], C2["up"], (W, H), C2["fov"])
+    cam = rb.PerspectiveCamera(eye, look, C2["up"], (W, H), C2["fov"])
     spps, errs = [16, 64, 256], []
     for spp in spps:
         g = it.render_bdpt(cam, _bdpt_reference_params(spp, 47)).cpu().numpy()[pix].astype(np.float64)
@@ -135,12 +143,17 @@ def test_bdpt_reference_estimator_converges_to_host(rb, orc, cuda):
     assert st["connection_rays"] > 0 and st["light_rays"] > 0 and st["lvc_vertices"] > 0
     assert errs[1] <= 0.8
     assert -0.65 <= _slope(spps, errs) <= -0.35
-    # The reference's weights are not the unbiased ones: the converged means differ.
-    ref_mean = it.render_bdpt(cam, _bdpt_reference_params(512, 53)).cpu().numpy().mean()
-    unb_mean = it.render_bdpt(cam, BidirectionalPathIntegratorLvcParams(spp=512, max_path_length=9, connections=1,
-                                                                        num_light_paths=2048, seed=53)).cpu().numpy().mean()
-    print("BDPT means reference / unbiased", ref_mean, unb_mean)
-    assert abs(ref_mean - unb_mean) / unb_mean > 0.03
+    # The reference's estimator is not the unbiased one: in the unit room, where
+    # the lights' triangles have area 0.02, its 0.5-area quirk makes the
+    # converged image many times brighter.
+    room1 = _room(rb)
+    it1 = Integrator(rb.CudaTracer(rb.BVH(room1)), DeviceScene(room1))
+    cam1 = rb.PerspectiveCamera(C2["eye"], C2["lookat"], C2["up"], (W, H), C2["fov"])
+    ref_mean = it1.render_bdpt(cam1, _bdpt_reference_params(256, 53)).cpu().numpy().mean()
+    unb_mean = it1.render_bdpt(cam1, BidirectionalPathIntegratorLvcParams(spp=256, max_path_length=9, connections=1,
+                                                                          num_light_paths=2048, seed=53)).cpu().numpy().mean()
+    print("BDPT unit-room means reference / unbiased", ref_mean, unb_mean)
+    assert ref_mean > 5.0 * unb_mean
 
 
 def test_bdpt_reference_params_struct(rb, cuda):
