@@ -26,9 +26,12 @@
 //   [16..17] qlo.z[8]  [18..19] qhi.z[8]
 // Quantized boxes contain the binary boxes plus a margin of 2^-16 x the
 // scene's largest coordinate (several times the rounding error of either slab
-// test for rays that start inside the scene's coordinate range), so a box the binary traversal enters is entered
-// here too despite the different rounding of the two slab tests; closest hits
-// therefore equal the binary traversal's except for exact ties in t.
+// test for rays that start inside the scene's coordinate range) plus 2^-14 of
+// the parent node's extent (the plane decode's offset rounding), so a box the
+// binary traversal enters is entered here too despite the different rounding
+// of the two slab tests; closest hits therefore equal the binary traversal's
+// except for exact ties in t (and for axis-parallel rays that run exactly in a
+// binary box's boundary plane, which the binary slab test culls).
 #include <algorithm>
 #include <cmath>
 
@@ -289,13 +292,17 @@ void Collapser::emit(std::vector<Item> items, uint32_t level, std::vector<Pendin
             if (slot_of_entry[c.e] < 0 && entry_of_slot[c.s] < 0) { slot_of_entry[c.e] = c.s; entry_of_slot[c.s] = c.e; }
         }
     }
-    // Quantization grid.
+    // Quantization grid.  Each child box is widened by the scene margin and by
+    // 2^-14 of this node's extent per axis: the traversal decodes a plane as
+    // the float 32768 + q and folds 32768 cells into its slab offset, whose
+    // rounding is at most about 1/512 of a cell (2^-17 of the node).
     float p[3];
     int ex[3];
-    double scale[3];
+    double scale[3], wid[3];
     for (int a = 0; a < 3; a++) {
-        p[a] = round_down(ulo[a] - margin);
-        const double ext = (uhi[a] + margin) - (double)p[a];
+        wid[a] = std::max(0.0, uhi[a] - ulo[a]) * 0x1p-14;
+        p[a] = round_down(ulo[a] - margin - wid[a]);
+        const double ext = (uhi[a] + margin + wid[a]) - (double)p[a];
         int e = -126;
         if (ext > 0.0) {
             e = (int)std::ceil(std::log2(ext / 255.0));
@@ -322,8 +329,8 @@ void Collapser::emit(std::vector<Item> items, uint32_t level, std::vector<Pendin
         const Slot& sl = entries[e];
         const Item& it = items[sl.item];
         for (int a = 0; a < 3 && box_valid(it); a++) {
-            const double lo = std::floor(((it.lo[a] - margin) - (double)p[a]) / scale[a]);
-            const double hi = std::ceil(((it.hi[a] + margin) - (double)p[a]) / scale[a]);
+            const double lo = std::floor(((it.lo[a] - margin - wid[a]) - (double)p[a]) / scale[a]);
+            const double hi = std::ceil(((it.hi[a] + margin + wid[a]) - (double)p[a]) / scale[a]);
             qlo[a][s] = (uint8_t)std::max(0.0, std::min(255.0, lo));
             qhi[a][s] = (uint8_t)std::max(0.0, std::min(255.0, hi));
         }

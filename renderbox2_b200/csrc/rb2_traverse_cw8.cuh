@@ -17,8 +17,6 @@
 // exact ties in t.
 #pragma once
 
-#include <cuda_fp16.h>
-
 #include "rb2_traverse.cuh"
 
 namespace rb2dev {
@@ -28,14 +26,19 @@ namespace rb2dev {
 constexpr int kStackSizeCw8 = 72;
 constexpr uint32_t kCw8NodeWords = 20;
 
-// Two quantized planes (bytes 2h and 2h + 1 of w) as floats 1024 + q: each
-// byte becomes the mantissa of a half-precision 1024 (0x64xx), converted
-// exactly.  The 1024 is folded into the per-node slab offset.
+// Two quantized planes (bytes 2h and 2h + 1 of w) as floats 32768 + q: each
+// byte is moved into bits 8-15 of the float 32768 (0x47000000), whose unit in
+// the last place there is 1, so one byte permute yields the plane exactly.
+// The 32768 cells are folded into the per-node slab offset (the layout widens
+// every box by 2^-14 of its node for that offset's rounding).
+constexpr float kCw8PlaneBias = 32768.0f;
+__device__ __forceinline__ float cw8_plane(uint32_t w, int b)
+{
+    return __uint_as_float(__byte_perm(w, 0x47000000u, 0x7504u | ((uint32_t)b << 4)));
+}
 __device__ __forceinline__ float2 cw8_planes(uint32_t w, int h)
 {
-    const uint32_t p = __byte_perm(w, 0x6464u, h ? 0x4342u : 0x4140u);
-    const __half2 v = *reinterpret_cast<const __half2*>(&p);
-    return __half22float2(v);
+    return make_float2(cw8_plane(w, 2 * h), cw8_plane(w, 2 * h + 1));
 }
 
 // Two IEEE single-precision FMAs in one paired instruction (sm_100 f32x2).
@@ -185,16 +188,16 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
                         const float sx = __fmul_rn(__uint_as_float((ew & 0xFFu) << 23), L.idx);
                         const float sy = __fmul_rn(__uint_as_float(((ew >> 8) & 0xFFu) << 23), L.idy);
                         const float sz = __fmul_rn(__uint_as_float(((ew >> 16) & 0xFFu) << 23), L.idz);
-                        // Slab offsets less 1024 cells (planes arrive as 1024 + q).
+                        // Slab offsets less the plane bias (planes arrive as 32768 + q cells).
                         float ax, ay, az;
                         if constexpr (kOodSlab) {
-                            ax = __fmaf_rn(-1024.0f, sx, __fmaf_rn(h0.x, L.idx, -L.oodx));
-                            ay = __fmaf_rn(-1024.0f, sy, __fmaf_rn(h0.y, L.idy, -L.oody));
-                            az = __fmaf_rn(-1024.0f, sz, __fmaf_rn(h0.z, L.idz, -L.oodz));
+                            ax = __fmaf_rn(-kCw8PlaneBias, sx, __fmaf_rn(h0.x, L.idx, -L.oodx));
+                            ay = __fmaf_rn(-kCw8PlaneBias, sy, __fmaf_rn(h0.y, L.idy, -L.oody));
+                            az = __fmaf_rn(-kCw8PlaneBias, sz, __fmaf_rn(h0.z, L.idz, -L.oodz));
                         } else {
-                            ax = __fmaf_rn(-1024.0f, sx, __fmul_rn(__fsub_rn(h0.x, L.ox), L.idx));
-                            ay = __fmaf_rn(-1024.0f, sy, __fmul_rn(__fsub_rn(h0.y, L.oy), L.idy));
-                            az = __fmaf_rn(-1024.0f, sz, __fmul_rn(__fsub_rn(h0.z, L.oz), L.idz));
+                            ax = __fmaf_rn(-kCw8PlaneBias, sx, __fmul_rn(__fsub_rn(h0.x, L.ox), L.idx));
+                            ay = __fmaf_rn(-kCw8PlaneBias, sy, __fmul_rn(__fsub_rn(h0.y, L.oy), L.idy));
+                            az = __fmaf_rn(-kCw8PlaneBias, sz, __fmul_rn(__fsub_rn(h0.z, L.oz), L.idz));
                         }
                         // Near and far plane words per axis (the high plane is near for a
                         // negative direction), children 0-3 in the first word, 4-7 in the second.
