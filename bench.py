@@ -209,12 +209,14 @@ class ClockSampler:
 L2_BYTES = 126 * 1024 * 1024
 
 # DRAM bytes per algorithmic byte of the batched traversal kernel, from ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on a capture
-# small enough for the profiler: the first 8 scenes of this workload (triangle
-# counts and seeds as here) with 524,288 rays each, the tuned launch shape,
-# measured against the launch's algorithmic bytes.  Keyed by node order.
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on captures
+# small enough for the profiler, measured against the launch's algorithmic
+# bytes.  Keyed by node order: the compressed 8-wide kernel on the first 8
+# scenes of this workload (its triangle counts and seeds, 524,288 rays each,
+# block 256, 64 registers); the binary kernel on 8 heightfields of 500k
+# triangles with 524,288 rays each.
 DRAM_PER_ALG_BYTE = {
-    3: (445.7e6 / 7961.2e6, "8 scenes x 500k triangles, 4.19M rays, compressed 8-wide layout"),
+    3: (403.0e6 / 7023.9e6, "first 8 scenes of this workload, 4.19M rays, compressed 8-wide layout"),
     1: (618.5e6 / 7961.2e6, "8 scenes x 500k triangles, 4.19M rays, binary BFS layout"),
 }
 
