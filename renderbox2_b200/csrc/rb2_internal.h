@@ -145,6 +145,14 @@ int validate_filter(const rb2_filter* f);
 constexpr uint32_t kTracerQueueSlots = 256;
 unsigned long long* tracer_queue_counter(rb2_tracer* t);
 
+// Whether rays from origin o keep the compressed 8-wide traversal exact (its
+// boxes' margin covers slab rounding for origins within 128 x the scene's
+// largest coordinate); integrators trace camera rays from farther away through
+// the binary buffer.
+bool cw8_origin_ok(const rb2_tracer* t, const float* o);
+// Bulk trace through the binary buffer whatever the tracer's node order.
+int trace_binary(rb2_tracer* t, const float* d_rays, uint64_t n, int any_hit, void* d_out, void* stream);
+
 inline uint32_t f2u(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
 inline float u2f(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
 

@@ -1771,7 +1771,11 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
         }
         RB2_CUDA(cudaEventRecord(it->ev[it->ev_used], s), "timing event");
     }
-    if ((rc = rb2_trace(it->tracer, reinterpret_cast<const float*>(it->d_rays), (uint32_t)npix, 0, nullptr,
+    // Camera rays from beyond the compressed layout's origin bound go through the binary buffer.
+    if (!cw8_origin_ok(it->tracer, cam->eye)) {
+        if ((rc = trace_binary(it->tracer, reinterpret_cast<const float*>(it->d_rays), npix, 0, it->d_hits, s)))
+            return rc;
+    } else if ((rc = rb2_trace(it->tracer, reinterpret_cast<const float*>(it->d_rays), (uint32_t)npix, 0, nullptr,
                         reinterpret_cast<rb2_hit*>(it->d_hits), stream)))
         return rc;
     if (it->timing) {
@@ -1841,6 +1845,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
     const rb2_scene_dev* sd = it->scene;
     rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights, sd->d_mats};
     const DeviceBvhView bv = device_bvh(it->tracer, true);
+    const DeviceBvhView bv_cam = device_bvh(it->tracer, cw8_origin_ok(it->tracer, cam->eye));
     WaveCounters* wc = it->d_wave;
     const unsigned g = grid_for(P, it->sms);
     for (uint32_t s0 = 0; s0 < p->spp; s0 += spw) {
@@ -1852,10 +1857,11 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
         uint32_t cur = 0;
         for (uint32_t b = 0; b <= p->max_depth; b++) {
             rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
-            rb2dev::QueueSource ext{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop), bv.triidx,
+            const DeviceBvhView& bx = b == 0 ? bv_cam : bv;  // camera rays: see cw8_origin_ok
+            rb2dev::QueueSource ext{static_cast<const float4*>(bx.nodes), static_cast<const float4*>(bx.woop), bx.triidx,
                                     ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext, rb2dev::kClosest,
                                     ps.hit, nullptr, nullptr};
-            if ((rc = launch_persistent(ext, paths, it, bv, s))) return rc;
+            if ((rc = launch_persistent(ext, paths, it, bx, s))) return rc;
             rb2dev::k_pt_shade<<<g, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, s0, b, p->max_depth, p->rr_start, p->rr_prob,
                                                 p->compat, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T, ps.L,
                                                 ps.sray, ps.sc, ps.qs, wc, cur);
@@ -1915,6 +1921,7 @@ int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_rayc
     const rb2_scene_dev* sd = it->scene;
     rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights, sd->d_mats};
     const DeviceBvhView bv = device_bvh(it->tracer, true);
+    const DeviceBvhView bv_cam = device_bvh(it->tracer, cw8_origin_ok(it->tracer, cam->eye));
     WaveCounters* wc = it->d_wave;
     const unsigned g = grid_for(P, it->sms);
     for (uint32_t s0 = 0; s0 < p->spp; s0 += spw) {
@@ -1926,10 +1933,10 @@ int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_rayc
                                               wc, filtered ? it->d_film_xy : nullptr);
         RB2_CUDA(cudaGetLastError(), "ray-cast camera");
         rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, 1u);
-        rb2dev::QueueSource prim{static_cast<const float4*>(bv.nodes), static_cast<const float4*>(bv.woop), bv.triidx,
-                                 ps.q[0], &wc->n_ext[0], ps.ray, &wc->head_ext, rb2dev::kClosest,
+        rb2dev::QueueSource prim{static_cast<const float4*>(bv_cam.nodes), static_cast<const float4*>(bv_cam.woop),
+                                 bv_cam.triidx, ps.q[0], &wc->n_ext[0], ps.ray, &wc->head_ext, rb2dev::kClosest,
                                  ps.hit, nullptr, nullptr};
-        if ((rc = launch_persistent(prim, paths, it, bv, s))) return rc;
+        if ((rc = launch_persistent(prim, paths, it, bv_cam, s))) return rc;
         if (filtered) {
             rb2dev::k_rc_shade<<<g, 256, 0, s>>>(sv, paths, p->shade, ps.hit, ps.L, wc);
             rb2dev::k_film_gather<<<grid_for(npix, it->sms), 256, 0, s>>>(
@@ -2039,6 +2046,7 @@ int rb2_render_bdpt_lvc(rb2_integrator* it, const rb2_camera* cam, const rb2_bdp
     const rb2_scene_dev* sd = it->scene;
     rb2dev::SceneView sv{sd->d_verts, sd->d_tris, sd->d_albedo, sd->d_emission, sd->d_lights, sd->n_lights, sd->d_mats};
     const DeviceBvhView bv = device_bvh(it->tracer, true);
+    const DeviceBvhView bv_cam = device_bvh(it->tracer, cw8_origin_ok(it->tracer, cam->eye));
     const float4* bn = static_cast<const float4*>(bv.nodes);
     const float4* bw = static_cast<const float4*>(bv.woop);
     WaveCounters* wc = it->d_wave;
@@ -2120,9 +2128,11 @@ int rb2_render_bdpt_lvc(rb2_integrator* it, const rb2_camera* cam, const rb2_bdp
         cur = 0;
         for (uint32_t i = 1; i <= K; i++) {
             rb2dev::k_pt_bounce_reset<<<1, 1, 0, s>>>(wc, cur ^ 1u);
-            rb2dev::QueueSource ext{bn, bw, bv.triidx, ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext,
-                                    rb2dev::kClosest, ps.hit, nullptr, nullptr};
-            if ((rc = launch_persistent(ext, n_cam, it, bv, s))) return rc;
+            const DeviceBvhView& bx = i == 1 ? bv_cam : bv;  // camera rays: see cw8_origin_ok
+            rb2dev::QueueSource ext{static_cast<const float4*>(bx.nodes), static_cast<const float4*>(bx.woop), bx.triidx,
+                                    ps.q[cur], &wc->n_ext[cur], ps.ray, &wc->head_ext, rb2dev::kClosest, ps.hit,
+                                    nullptr, nullptr};
+            if ((rc = launch_persistent(ext, n_cam, it, bx, s))) return rc;
             if (ref)
                 rb2dev::k_bd_cam_shade_ref<<<gc, 256, 0, s>>>(sv, p->seed, (uint32_t)npix, it0, i, K, C, Cs, rr_cam,
                                                               rr_prob, lvc_cap, ps.q[cur], ps.q[cur ^ 1u], ps.ray, ps.hit, ps.T,

@@ -284,6 +284,10 @@ struct rb2_tracer {
     uint8_t* d_mask = nullptr;
     uint64_t scratch_cap = 0;
     uint64_t device_bytes = 0;
+    // Ray origins up to this distance per axis keep the compressed 8-wide
+    // traversal conservative: 128 x the scene's largest coordinate (its boxes'
+    // margin covers slab rounding of about |origin| x 2^-24).
+    float cw8_origin_bound = 3.402823466e+38f;
     std::mutex mu;
 
     unsigned long long* next_counter()
@@ -311,7 +315,7 @@ rb2dev::JobDesc job_of(const rb2_tracer* t, const float* rays, uint64_t n, uint3
 }
 
 int trace_single(rb2_tracer* t, const float* d_rays, uint64_t n, uint32_t mode, const uint8_t* d_mask, void* d_out,
-                 cudaStream_t s)
+                 cudaStream_t s, bool binary = false)
 {
     if (n == 0) return RB2_OK;
     unsigned long long* counter = t->next_counter();
@@ -319,14 +323,20 @@ int trace_single(rb2_tracer* t, const float* d_rays, uint64_t n, uint32_t mode, 
     rb2dev::KernelArgs a{};
     a.jobs = nullptr;
     a.start = nullptr;
+    const uint32_t order = binary ? t->binary_order : t->node_order;
     a.inline_job = job_of(t, d_rays, n, mode, d_mask, d_out);
+    if (binary && t->node_order != t->binary_order) {
+        a.inline_job.nodes = t->d_nodes;
+        a.inline_job.woop = t->d_woop;
+        a.inline_job.triidx = t->d_triidx;
+    }
     a.n_jobs = 1;
     a.fetch_threshold = t->cfg.fetch_threshold ? t->cfg.fetch_threshold : 20u;
     a.chunk = 1;
     a.counter = counter;
     a.status = t->d_status;
     const uint32_t block = t->cfg.block_threads ? t->cfg.block_threads : kDefaultBlock;
-    return launch_jobs(a, n, block, t->cfg.ctas_per_sm, t->cfg.regs, layout_of(t->node_order), t->occ, s);
+    return launch_jobs(a, n, block, t->cfg.ctas_per_sm, t->cfg.regs, layout_of(order), t->occ, s);
 }
 
 bool valid_regs(uint32_t r) { return r == 0 || r == 64 || r == 48 || r == 40; }
@@ -389,6 +399,11 @@ int rb2_tracer_create(const rb2_host_bvh* bvh, rb2_tracer** out)
     t->n_nodes_u4 = h.nodes.size() / 4;
     t->n_woop_u4 = h.woop.size() / 4;
     t->host_nodes = h.nodes;
+    {
+        float m = 0.0f;
+        for (int k = 0; k < 12 && (size_t)k < h.nodes.size(); k++) m = std::max(m, std::fabs(u2f(h.nodes[k])));
+        t->cw8_origin_bound = 128.0f * std::max(m, 1e-30f);
+    }
     // Two spare uint4 after the Woop buffer: the kernel fetches a triangle's
     // three rows before testing the first for the terminator.
     const size_t nb = h.nodes.size() * 4, wb = (h.woop.size() + 8) * 4, ib = h.triidx.size() * 4 + 16;
@@ -931,6 +946,18 @@ DeviceBvhView device_bvh(const rb2_tracer* t, bool allow_cw8)
 }
 
 unsigned long long* tracer_queue_counter(rb2_tracer* t) { return t->next_counter(); }
+
+bool cw8_origin_ok(const rb2_tracer* t, const float* o)
+{
+    const float b = t->cw8_origin_bound;
+    return std::fabs(o[0]) <= b && std::fabs(o[1]) <= b && std::fabs(o[2]) <= b;
+}
+
+int trace_binary(rb2_tracer* t, const float* d_rays, uint64_t n, int any_hit, void* d_out, void* stream)
+{
+    return trace_single(t, d_rays, n, any_hit ? rb2dev::kAny : rb2dev::kClosest, nullptr, d_out,
+                        (cudaStream_t)stream, true);
+}
 }  // namespace rb2
 
 extern "C" int rb2_tracer_dev_bvh(const rb2_tracer* t, rb2_dev_bvh* out)
