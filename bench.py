@@ -471,7 +471,7 @@ def run_rb2(args, rank, world, local_rank):
     batch = None
     if args.serve_jobs > 0:
         from renderbox2_b200.workloads import serving as serving_run
-        serving = serving_run(n_jobs=args.serve_jobs)
+        serving = serving_run(n_jobs=args.serve_jobs, slots=args.serve_slots)
 
     # ---- configs 1-3: one frame each at full size (trace-stage roofline vs L2 or HBM).
     integrators = {}
@@ -963,7 +963,8 @@ def run_profile(args, local_rank):
         keep.append((tr, d, out_h, out_o))
     batch = rb.TraceBatch(jobs)
     batch.set_config(block_threads=args.profile_block, regs=args.profile_regs, node_order=args.profile_order,
-                     fetch_threshold=args.profile_threshold, ctas_per_sm=args.profile_ctas, chunk=args.profile_chunk)
+                     fetch_threshold=args.profile_threshold, ctas_per_sm=args.profile_ctas, chunk=args.profile_chunk,
+                     reorder=args.profile_reorder)
     ms = []
     for _ in range(args.launches):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1028,11 +1029,14 @@ def main():
     ap.add_argument("--e2e-depth", type=int, default=4, help="streams of the pipelined host path")
     ap.add_argument("--serve-jobs", type=int, default=10000,
                     help="config-5 jobs in the serving measurement (0: skip)")
+    ap.add_argument("--serve-slots", type=int, default=8, help="concurrent slots of the continuous server")
     ap.add_argument("--no-integrators", dest="integrators", action="store_false",
                     help="leave configs 1-3 out of the default line")
-    ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt", "raycast", "profile"], default="trace",
+    ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt", "raycast", "profile", "serve-curve"],
+                    default="trace",
                     help="trace: the headline config-4 line; ao/pt/bdpt/raycast: one integrator config at full "
-                         "size; profile: a small batched case for ncu")
+                         "size; profile: a small batched case for ncu; serve-curve: config-5 latency against "
+                         "offered load")
     ap.add_argument("--launches", type=int, default=3, help="profile: launches")
     ap.add_argument("--no-oracle", action="store_true", help="profile: skip the algorithmic-byte count")
     ap.add_argument("--profile-equal-tris", type=int, default=0,
@@ -1043,6 +1047,7 @@ def main():
     ap.add_argument("--profile-threshold", type=int, default=28)
     ap.add_argument("--profile-ctas", type=int, default=0)
     ap.add_argument("--profile-chunk", type=int, default=1)
+    ap.add_argument("--profile-reorder", type=int, default=0, help="profile: ray reordering bits per axis (0 off)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -1061,6 +1066,14 @@ def main():
             run_reference(args, rank, world)
         elif args.workload == "profile":
             run_profile(args, local_rank)
+        elif args.workload == "serve-curve":
+            import torch
+
+            from renderbox2_b200.workloads import serving_curve
+            torch.cuda.set_device(local_rank)
+            r = serving_curve(n_jobs=args.serve_jobs if args.serve_jobs != 10000 else 3000, slots=args.serve_slots)
+            if rank == 0:
+                print(json.dumps({"metric": "served-job latency against offered load (config 5)", **r}), flush=True)
         elif args.workload != "trace":
             run_workload(args, rank, local_rank)
         else:

@@ -248,6 +248,12 @@ typedef struct {
     uint32_t node_order;      /* RB2_NODE_ORDER_*; applied to every tracer in the batch */
     uint32_t regs;            /* register budget of the kernel variant: 64, 48 or 40 (0 = 64);
                                  lower budgets keep more warps resident and spill a little to L1 */
+    uint32_t reorder;         /* ray reordering before the traversal: 0 off, or k in 3..5: each job's
+                                 rays are visited in the order of (direction octant, k-bit-per-axis
+                                 Morton code of the origin within its scene's box), so a warp's rays
+                                 start near each other and head the same way; records still go to
+                                 each ray's own index, and every ray's result is unchanged */
+    uint32_t reserved;
 } rb2_batch_config;
 
 typedef struct rb2_batch rb2_batch;
@@ -265,8 +271,9 @@ int rb2_batch_launch(rb2_batch* b, void* stream);
 int rb2_batch_capture(rb2_batch* b, void* stream);
 int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream);
 /* Times candidate configs (coordinate descent over node order, block shape x
- * register budget, CTAs per SM, fetch threshold and queue chunk; median of
- * `reps` launches each), applies and returns the fastest. */
+ * register budget, CTAs per SM, fetch threshold and queue chunk, without and
+ * with ray reordering; median of `reps` launches each), applies and returns
+ * the fastest. */
 int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best, double* best_ms);
 
 /* ------------------------------------------------------- fault injection --

@@ -37,6 +37,7 @@ struct KernelArgs {
     uint32_t pad;
     unsigned long long* counter;         // queue head (zeroed before the launch)
     unsigned int* status;                // guard bits
+    const uint32_t* perm;                // nullable: queue slot -> ray slot (ray reordering)
 };
 
 struct JobSource {
@@ -47,6 +48,7 @@ struct JobSource {
     unsigned long long* counter;
     uint32_t chunk;
     unsigned long long* rem;             // per-warp private [cur, end) in shared memory
+    const uint32_t* perm;                // nullable: the order in which ray slots are visited
 
     __device__ __forceinline__ void claim(unsigned count, unsigned long long& b1, unsigned& n1,
                                           unsigned long long& b2)
@@ -84,6 +86,7 @@ struct JobSource {
     __device__ __forceinline__ int fetch(unsigned long long slot, Lane& L) const
     {
         if (slot >= total) return 0;
+        if (perm != nullptr) slot = __ldg(perm + slot);  // a permutation of [0, total), job ranges kept
         const uint32_t j = find_job(slot);
         const JobDesc& d = jobs[j];
         const uint64_t r = slot - start[j];
@@ -151,6 +154,7 @@ __global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK) k_trace_jobs(co
     src.counter = a.counter;
     src.chunk = a.chunk;
     src.rem = s_rem;
+    src.perm = a.perm;
     if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8<JobSource>(src, a.fetch_threshold, a.status);
     else persistent_trace<JobSource, LAYOUT == kLayoutWide4>(src, a.fetch_threshold, a.status);
 }

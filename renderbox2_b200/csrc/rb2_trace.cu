@@ -16,6 +16,7 @@
 #include "rb2_render.h"
 #include "rb2_sources.cuh"
 #include "rb2_camera.cuh"
+#include "rb2_reorder.cuh"
 
 #include <cuda_runtime.h>
 
@@ -594,6 +595,14 @@ struct rb2_batch {
     Occupancy occ;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // ray reordering (cfg.reorder): per-job scene boxes, bucket counters, scan
+    // scratch and the visiting order, allocated when first enabled
+    float4* d_boxes = nullptr;
+    uint32_t* d_hist = nullptr;
+    uint32_t* d_chunk_sums = nullptr;
+    uint32_t* d_perm = nullptr;
+    uint32_t* d_keys = nullptr;
+    uint64_t hist_cap = 0, chunk_cap = 0;
 
     void drop_graph()
     {
@@ -610,6 +619,22 @@ int batch_enqueue(rb2_batch* b, cudaStream_t s)
 {
     RB2_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), s), "queue reset");
     rb2dev::KernelArgs a{};
+    if (b->cfg.reorder) {
+        rb2::ReorderArgs r{};
+        r.jobs = b->d_jobs;
+        r.start = b->d_start;
+        r.boxes = b->d_boxes;
+        r.n_jobs = (uint32_t)b->jobs.size();
+        r.bits = b->cfg.reorder;
+        r.total = b->total;
+        r.hist = b->d_hist;
+        r.chunk_sums = b->d_chunk_sums;
+        r.perm = b->d_perm;
+        r.keys = b->d_keys;
+        r.sms = b->occ.sms;
+        RB2_CUDA(rb2::reorder_enqueue(r, s), "ray reordering");
+        a.perm = b->d_perm;
+    }
     a.jobs = b->d_jobs;
     a.start = b->d_start;
     a.n_jobs = (uint32_t)b->jobs.size();
@@ -628,6 +653,63 @@ int batch_check_layout(const rb2_batch* b)
     for (const rb2_tracer* t : b->unique_tracers)
         if (layout_of(t->node_order) != layout_of(b->cfg.node_order))
             return fail(RB2_EINVAL, "a tracer's node layout changed since rb2_batch_set_config; set it again");
+    return RB2_OK;
+}
+
+// Buffers of ray reordering at `bits` per axis: each job's scene box (the union
+// of the root's child boxes) as lo and 1 / extent, counters, scan scratch
+// each ray's key and the visiting order.
+int batch_prepare_reorder(rb2_batch* b, uint32_t bits)
+{
+    if (bits == 0) return RB2_OK;
+    if (bits < 3 || bits > 5) return fail(RB2_EINVAL, "reorder must be 0 or 3..5 bits per axis");
+    if (b->total >= 0xFFFFFFFFull) return fail(RB2_EINVAL, "ray reordering needs fewer than 2^32 rays per batch");
+    const uint32_t n = (uint32_t)b->jobs.size();
+    const uint64_t buckets = rb2::reorder_buckets(n, bits), chunks = rb2::reorder_chunks(buckets);
+    if (chunks > 0xFFFFFFFFull) return fail(RB2_EINVAL, "too many reordering buckets");
+    cudaError_t e = cudaSuccess;
+    if (!b->d_boxes) {
+        std::vector<float4> boxes(2 * (size_t)std::max<uint32_t>(n, 1));
+        for (uint32_t i = 0; i < n; i++) {
+            const std::vector<uint32_t>& h = b->jobs[i].tracer->host_nodes;
+            float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+            if (h.size() >= 12) {
+                const int lo_w[2][3] = {{0, 2, 8}, {4, 6, 10}}, hi_w[2][3] = {{1, 3, 9}, {5, 7, 11}};
+                for (int a = 0; a < 3; a++) {
+                    lo[a] = std::min(u2f(h[lo_w[0][a]]), u2f(h[lo_w[1][a]]));
+                    hi[a] = std::max(u2f(h[hi_w[0][a]]), u2f(h[hi_w[1][a]]));
+                }
+            }
+            float sc[3];
+            for (int a = 0; a < 3; a++) sc[a] = 1.0f / std::max(hi[a] - lo[a], 1e-30f);
+            boxes[2 * i] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+            boxes[2 * i + 1] = make_float4(sc[0], sc[1], sc[2], 0.0f);
+        }
+        if ((e = rb2::dev_malloc(&b->d_boxes, sizeof(float4) * boxes.size())) != cudaSuccess)
+            return fail(RB2_ENOMEM, std::string("reordering boxes: ") + cudaGetErrorString(e));
+        RB2_CUDA(cudaMemcpy(b->d_boxes, boxes.data(), sizeof(float4) * boxes.size(), cudaMemcpyHostToDevice),
+                 "reordering boxes");
+    }
+    if (!b->d_perm && (e = rb2::dev_malloc(&b->d_perm, sizeof(uint32_t) * std::max<uint64_t>(b->total, 1))) != cudaSuccess)
+        return fail(RB2_ENOMEM, std::string("reordering order: ") + cudaGetErrorString(e));
+    if (!b->d_keys && (e = rb2::dev_malloc(&b->d_keys, sizeof(uint32_t) * std::max<uint64_t>(b->total, 1))) != cudaSuccess)
+        return fail(RB2_ENOMEM, std::string("reordering keys: ") + cudaGetErrorString(e));
+    if (buckets > b->hist_cap) {
+        rb2::dev_free(b->d_hist);
+        b->d_hist = nullptr;
+        b->hist_cap = 0;
+        if ((e = rb2::dev_malloc(&b->d_hist, sizeof(uint32_t) * buckets)) != cudaSuccess)
+            return fail(RB2_ENOMEM, std::string("reordering counters: ") + cudaGetErrorString(e));
+        b->hist_cap = buckets;
+    }
+    if (chunks > b->chunk_cap) {
+        rb2::dev_free(b->d_chunk_sums);
+        b->d_chunk_sums = nullptr;
+        b->chunk_cap = 0;
+        if ((e = rb2::dev_malloc(&b->d_chunk_sums, sizeof(uint32_t) * chunks)) != cudaSuccess)
+            return fail(RB2_ENOMEM, std::string("reordering scan: ") + cudaGetErrorString(e));
+        b->chunk_cap = chunks;
+    }
     return RB2_OK;
 }
 
@@ -710,6 +792,11 @@ int rb2_batch_destroy(rb2_batch* b)
     rb2::dev_free(b->d_start);
     rb2::dev_free(b->d_counter);
     rb2::dev_free(b->d_status);
+    rb2::dev_free(b->d_boxes);
+    rb2::dev_free(b->d_hist);
+    rb2::dev_free(b->d_chunk_sums);
+    rb2::dev_free(b->d_perm);
+    rb2::dev_free(b->d_keys);
     delete b;
     return RB2_OK;
 }
@@ -722,6 +809,7 @@ int rb2_batch_set_config(rb2_batch* b, const rb2_batch_config* cfg)
     if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
     if (cfg->node_order > RB2_NODE_ORDER_CW8) return fail(RB2_EINVAL, "unknown node order");
     if (!valid_regs(cfg->regs)) return fail(RB2_ENOTSUP, "regs must be 64, 48 or 40");
+    if (int rc0 = batch_prepare_reorder(b, cfg->reorder)) return rc0;
     b->drop_graph();
     for (rb2_tracer* t : b->unique_tracers) {
         int rc = rb2_tracer_set_node_order(t, cfg->node_order);
@@ -823,15 +911,6 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
         ms = t[reps / 2];
         return RB2_OK;
     };
-    rb2_batch_config best{};
-    best.block_threads = kDefaultBlock;
-    best.fetch_threshold = 20;
-    best.chunk = 1;
-    best.node_order = RB2_NODE_ORDER_DFS;
-    best.regs = 64;
-    double best_ms = 0;
-    int rc = time_cfg(best, best_ms);
-    if (rc) return rc;
     const uint32_t orders[] = {RB2_NODE_ORDER_DFS, RB2_NODE_ORDER_BFS, RB2_NODE_ORDER_WIDE4, RB2_NODE_ORDER_CW8};
     const uint32_t blocks[] = {64, 128, 256};
     const uint32_t regs[] = {64, 48, 40};
@@ -864,37 +943,66 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
         }
         return RB2_OK;
     };
-    // Each layout gets its own shape search (the layouts favour different
-    // register budgets and thresholds); the winner gets a second pass and the
-    // queue chunk.
-    std::vector<rb2_batch_config> per_layout;
-    for (uint32_t o : orders) {
-        rb2_batch_config c = best;
-        c.node_order = o;
-        double ms;
-        if ((rc = time_cfg(c, ms))) return rc;
-        if ((rc = tune_shape(c, ms))) return rc;
-        per_layout.push_back(c);
-        if (ms < best_ms) { best = c; best_ms = ms; }
-    }
-    if ((rc = tune_shape(best, best_ms))) return rc;
-    for (uint32_t ch : chunks) {
-        rb2_batch_config c = best; c.chunk = ch; double ms;
-        if ((rc = time_cfg(c, ms))) return rc;
-        if (ms < best_ms) { best = c; best_ms = ms; }
-    }
-    // Last look at the layouts, each with its own tuned shape, re-timed
-    // together with the incumbent so drift between searches cannot decide it.
-    {
+    // The whole search at one reordering setting: each layout gets its own
+    // shape search (the layouts favour different register budgets and
+    // thresholds); the winner gets a second pass and the queue chunk; then a
+    // last look at the layouts, each with its own tuned shape, re-timed with
+    // the incumbent so drift between searches cannot decide it.
+    auto search = [&](uint32_t reorder, rb2_batch_config& best, double& best_ms) -> int {
+        int rc2;
+        best = rb2_batch_config{};
+        best.block_threads = kDefaultBlock;
+        best.fetch_threshold = 20;
+        best.chunk = 1;
+        best.node_order = RB2_NODE_ORDER_DFS;
+        best.regs = 64;
+        best.reorder = reorder;
+        if ((rc2 = time_cfg(best, best_ms))) return rc2;
+        std::vector<rb2_batch_config> per_layout;
+        for (uint32_t o : orders) {
+            rb2_batch_config c = best;
+            c.node_order = o;
+            double ms;
+            if ((rc2 = time_cfg(c, ms))) return rc2;
+            if ((rc2 = tune_shape(c, ms))) return rc2;
+            per_layout.push_back(c);
+            if (ms < best_ms) { best = c; best_ms = ms; }
+        }
+        if ((rc2 = tune_shape(best, best_ms))) return rc2;
+        for (uint32_t ch : chunks) {
+            rb2_batch_config c = best; c.chunk = ch; double ms;
+            if ((rc2 = time_cfg(c, ms))) return rc2;
+            if (ms < best_ms) { best = c; best_ms = ms; }
+        }
         double inc_ms;
-        if ((rc = time_cfg(best, inc_ms))) return rc;
+        if ((rc2 = time_cfg(best, inc_ms))) return rc2;
         best_ms = inc_ms;
         for (const rb2_batch_config& c : per_layout) {
             if (c.node_order == best.node_order) continue;
             double ms;
-            if ((rc = time_cfg(c, ms))) return rc;
+            if ((rc2 = time_cfg(c, ms))) return rc2;
             if (ms < best_ms) { best = c; best_ms = ms; }
         }
+        return RB2_OK;
+    };
+    rb2_batch_config best{}, best_r{};
+    double best_ms = 0, best_r_ms = 0;
+    int rc = search(0, best, best_ms);
+    if (rc) return rc;
+    // Ray reordering (when the batch's rays fit its 32-bit visiting order):
+    // the search again with 4 bits per axis, then the other widths on its winner.
+    if (b->total < 0xFFFFFFFFull) {
+        if ((rc = search(4, best_r, best_r_ms))) return rc;
+        for (uint32_t bits : {3u, 5u}) {
+            rb2_batch_config c = best_r; c.reorder = bits; double ms;
+            if ((rc = time_cfg(c, ms))) return rc;
+            if (ms < best_r_ms) { best_r = c; best_r_ms = ms; }
+        }
+        double ms0;
+        if ((rc = time_cfg(best, ms0))) return rc;
+        if ((rc = time_cfg(best_r, best_r_ms))) return rc;
+        best_ms = ms0;
+        if (best_r_ms < best_ms) { best = best_r; best_ms = best_r_ms; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

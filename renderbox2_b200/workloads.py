@@ -155,3 +155,42 @@ def serving(n_jobs: int = 10000, n_bvh: int = 32, seed: int = 5, slots: int = 8,
                          "continuous_mrays_per_s": round(cburst["mrays_per_s"], 1),
                          "plain_fifo_mrays_per_s": round(burst["mrays_per_s"], 1),
                          "ratio": round(cburst["mrays_per_s"] / max(burst["mrays_per_s"], 1e-9), 3)}}
+
+
+def serving_curve(n_jobs: int = 3000, n_bvh: int = 32, seed: int = 5, slots: int = 8,
+                  loads=(0.5, 0.8, 1.0, 1.2), burst_jobs: int = 1000):
+    """Latency against offered load for config 5: the continuous server's
+    burst capacity (jobs per second with every job queued at t = 0) sets the
+    unit of load; each point serves the same n_jobs with Poisson arrivals at
+    load x that rate, through the continuous server and the one-at-a-time
+    FIFO server.  Returns the capacity and one record per load."""
+    from renderbox2_b200 import configs
+    from renderbox2_b200.serve import (Server, SharedBuffers, build_pool, config5_jobs, pool_triangle_counts,
+                                       poisson_arrivals)
+    c = configs.CONFIG5
+    counts = pool_triangle_counts(n_bvh, c["tri_min"], c["tri_max"], seed)
+    pool = build_pool(counts, seed=seed)
+    sh = SharedBuffers(pool, rays_per_bvh=c["rays_max"])
+    jobs = config5_jobs(pool, n_jobs, seed=seed, shared=sh)
+    cont = Server(pool, slots=slots, fifo=False)
+    plain = Server(pool, fifo=True)
+    cont.run(jobs.subset(range(min(8, n_jobs))))
+    plain.run(jobs.subset(range(min(8, n_jobs))))
+    nb = min(burst_jobs, n_jobs)
+    _, cb = cont.run(jobs.subset(range(nb)))
+    _, pb = plain.run(jobs.subset(range(nb)))
+    cap = nb / cb["wall_s"]
+    out = {"jobs": n_jobs, "slots": slots, "continuous_capacity_jobs_per_s": round(cap, 2),
+           "plain_capacity_jobs_per_s": round(nb / pb["wall_s"], 2),
+           "capacity_ratio_mrays": round(cb["mrays_per_s"] / max(pb["mrays_per_s"], 1e-9), 3), "points": []}
+    for k, load in enumerate(loads):
+        arr = poisson_arrivals(n_jobs, load * cap, seed=seed + 10 + k)
+        _, sc = cont.run(jobs.with_arrivals(arr))
+        _, sp = plain.run(jobs.with_arrivals(arr))
+        out["points"].append({
+            "load": load, "arrival_rate_jobs_per_s": round(load * cap, 2),
+            "continuous": {"p50_s": round(sc["p50_s"], 5), "p99_s": round(sc["p99_s"], 5),
+                           "mrays_per_s": round(sc["mrays_per_s"], 1)},
+            "plain_fifo": {"p50_s": round(sp["p50_s"], 5), "p99_s": round(sp["p99_s"], 5),
+                           "mrays_per_s": round(sp["mrays_per_s"], 1)}})
+    return out

@@ -85,6 +85,9 @@ def test_batch_equals_plain_launches(rb, orc, cuda):
     dict(regs=40, block_threads=64, chunk=2), dict(node_order=2), dict(node_order=2, regs=48, block_threads=256),
     dict(node_order=2, regs=40, chunk=4), dict(node_order=3), dict(node_order=3, regs=48, block_threads=256),
     dict(node_order=3, regs=40, chunk=4, fetch_threshold=8),
+    dict(reorder=3), dict(reorder=4, chunk=4), dict(reorder=5, node_order=1, regs=48, block_threads=256),
+    dict(reorder=4, node_order=2), dict(reorder=4, node_order=3, regs=48, block_threads=256, fetch_threshold=16),
+    dict(reorder=5, node_order=3, regs=40, chunk=2),
 ])
 def test_batch_configs_give_identical_results(rb, orc, cuda, cfg):
     scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
@@ -239,3 +242,52 @@ def test_cw8_layout_on_rooms(rb, orc, cuda):
         want = orc.trace(nodes, woop, tri, r)
         ties, bad, first = compare_closest(orc, b, {k: want[k] for k in ("prim", "t", "u", "v")}, woop, tri, r)
         assert bad == 0, f"seed {seed}, ray {first}"
+
+
+def test_ray_reordering_keeps_every_ray(rb, orc, cuda):
+    """Ray reordering visits each job's rays in (octant, Morton code of the
+    origin) order: with stencil masks, origins far outside the scene box,
+    empty and one-ray jobs and a job spanning two scenes' worth of rays, every
+    record still lands at its own ray's index and equals the plain launch's,
+    for 3, 4 and 5 bits per axis and after graph capture; widths outside 3..5
+    are refused."""
+    scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
+    # job 0 gets a stencil and a block of rays whose origins sit far outside the box
+    sc, bvh, r = scenes[0]
+    far = r.copy()
+    far[:5000, 0:3] += np.float32(50.0)
+    far[5000:6000, 0:3] -= np.float32(1e4)
+    d_far = cuda.from_numpy(far).cuda()
+    mask = cuda.from_numpy((np.arange(far.shape[0]) % 5 != 2).astype(np.uint8)).cuda()
+    out_m = cuda.full((far.shape[0], 4), 7, dtype=cuda.int32, device="cuda")
+    ref_m = tracers[0].trace(d_far, stencil=mask).clone()
+    jobs = jobs + [(tracers[0], d_far, rb.MODE_CLOSEST, out_m, mask)]
+    outs = outs + [out_m]
+    plain = plain + [ref_m]
+    batch = rb.TraceBatch(jobs)
+    for bits in (3, 4, 5):
+        batch.set_config(reorder=bits)
+        for o in outs:
+            o.fill_(7)
+        batch.launch()
+        _check(outs, plain, cuda)
+        assert batch.status() == 0
+    s = cuda.cuda.Stream()
+    batch.capture(s)
+    for _ in range(2):
+        for o in outs:
+            o.fill_(7)
+        cuda.cuda.synchronize()
+        batch.launch(s)
+        s.synchronize()
+        _check(outs, plain, cuda)
+    for bad in (1, 2, 6):
+        with pytest.raises(rb.Rb2Error, match="reorder"):
+            batch.set_config(reorder=bad)
+    # the masked job equals the oracle on its active rays
+    nodes, woop, tri = bvh.buffers_view()
+    act = mask.cpu().numpy() != 0
+    want = orc.trace(nodes, woop, tri, far[act])
+    got = out_m.cpu().numpy()[act]
+    assert np.array_equal(got[:, 0], want["prim"])
+    assert np.array_equal(got[:, 1].view(np.uint32), want["t"].view(np.uint32))
