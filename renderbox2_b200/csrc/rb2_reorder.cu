@@ -5,9 +5,10 @@
 
 namespace {
 
-constexpr uint32_t kChunk = 2048;      // counters per scan chunk
-constexpr uint32_t kThreads = 256;     // threads per scan block (8 counters each)
-constexpr uint32_t kSmemJobs = 1024;   // job prefixes staged in shared memory up to this many jobs
+constexpr uint32_t kChunk = 2048;        // counters per scan chunk
+constexpr uint32_t kThreads = 256;       // threads per scan block (8 counters each)
+constexpr uint32_t kSmemJobs = 1024;     // job prefixes staged in shared memory up to this many jobs
+constexpr uint32_t kTileThreads = 1024;  // threads per tile CTA of the tiled form
 
 __device__ __forceinline__ uint32_t quantize(float x, float lo, float inv_extent, float cells, uint32_t qmax)
 {
@@ -35,8 +36,88 @@ __device__ __forceinline__ uint32_t key_of(const rb2::ReorderArgs& a, uint32_t j
     return (oct << (3 * k)) | m;
 }
 
-// Stage 1 (kScatter false): each ray's key, kept in `keys`, and the bucket
-// counts.  Stage 3 (true): each ray takes the next position of its bucket,
+// ---------------------------------------------------------------- tiled form
+
+// Step 1: the tile's keys and its shared-memory histogram, stored as row t of cnt.
+__global__ void __launch_bounds__(kTileThreads) k_tile_count(const rb2::ReorderArgs a)
+{
+    extern __shared__ uint32_t s_h[];
+    const uint32_t nb = 1u << (3 + 3 * a.bits);
+    for (uint32_t t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+        for (uint32_t i = threadIdx.x; i < nb; i += kTileThreads) s_h[i] = 0u;
+        __syncthreads();
+        const rb2::ReorderTile tl = a.tiles[t];
+        const uint64_t s0 = a.start[tl.job];
+        // Two rays per thread per pass, so each thread has both loads in flight.
+        for (uint32_t s = tl.begin + threadIdx.x; s < tl.end; s += 2 * kTileThreads) {
+            const uint32_t s2 = s + kTileThreads;
+            const uint32_t k1 = key_of(a, tl.job, s - s0);
+            const uint32_t k2 = s2 < tl.end ? key_of(a, tl.job, s2 - s0) : 0u;
+            a.keys[s] = k1;
+            atomicAdd(&s_h[k1], 1u);
+            if (s2 < tl.end) {
+                a.keys[s2] = k2;
+                atomicAdd(&s_h[k2], 1u);
+            }
+        }
+        __syncthreads();
+        uint32_t* row = a.cnt + (uint64_t)t * nb;
+        for (uint32_t i = threadIdx.x; i < nb; i += kTileThreads) row[i] = s_h[i];
+        __syncthreads();
+    }
+}
+
+// Step 2: per (job, bucket), an exclusive scan down the job's tiles, in place;
+// the bucket's total goes to tot = a.hist.
+__global__ void k_tile_columns(const rb2::ReorderArgs a)
+{
+    constexpr uint32_t kRows = 8;  // rows loaded together, so their loads overlap
+    const uint32_t nb = 1u << (3 + 3 * a.bits);
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    uint32_t* __restrict__ cnt = a.cnt;
+    for (uint32_t j = blockIdx.y; j < a.n_jobs; j += gridDim.y) {
+        const uint32_t t0 = a.job_tile0[j], t1 = a.job_tile0[j + 1];
+        uint32_t run = 0;
+        for (uint32_t t = t0; t < t1; t += kRows) {
+            const uint32_t m = t1 - t < kRows ? t1 - t : kRows;
+            uint32_t c[kRows];
+#pragma unroll
+            for (uint32_t i = 0; i < kRows; i++) c[i] = i < m ? cnt[(uint64_t)(t + i) * nb + b] : 0u;
+#pragma unroll
+            for (uint32_t i = 0; i < kRows; i++) {
+                if (i < m) cnt[(uint64_t)(t + i) * nb + b] = run;
+                run += c[i];
+            }
+        }
+        a.hist[(uint64_t)j * nb + b] = run;
+    }
+}
+
+// Step 4: the tile's first position in every bucket (bucket start + the
+// tile's offset inside it) in shared memory; each ray takes the next one.
+__global__ void __launch_bounds__(kTileThreads) k_tile_scatter(const rb2::ReorderArgs a)
+{
+    extern __shared__ uint32_t s_off[];
+    const uint32_t nb = 1u << (3 + 3 * a.bits);
+    for (uint32_t t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+        const rb2::ReorderTile tl = a.tiles[t];
+        const uint32_t* row = a.cnt + (uint64_t)t * nb;
+        const uint32_t* base = a.hist + (uint64_t)tl.job * nb;
+        for (uint32_t i = threadIdx.x; i < nb; i += kTileThreads) s_off[i] = base[i] + row[i];
+        __syncthreads();
+        for (uint32_t s = tl.begin + threadIdx.x; s < tl.end; s += kTileThreads) {
+            const uint32_t pos = atomicAdd(&s_off[a.keys[s]], 1u);
+            a.perm[pos] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ global form (k = 5)
+
+// Step 1 (kScatter false): each ray's key, kept in `keys`, and the bucket
+// counts.  Step 3 (true): each ray takes the next position of its bucket,
 // whose counter holds the bucket's start after the scan, and records its
 // slot there.  Buckets are job-major: (job << (3 + 3k)) | key.
 template <bool kScatter>
@@ -68,8 +149,10 @@ __global__ void k_reorder(const rb2::ReorderArgs a)
     }
 }
 
-// Stage 2: exclusive scan of the counters, in place (chunk sums, a scan of the
-// sums in one block, then each chunk's own scan plus its offset).
+// ------------------------------------------------------------------- the scan
+
+// Exclusive scan of the counters, in place (chunk sums, a scan of the sums in
+// one block, then each chunk's own scan plus its offset).
 __global__ void k_chunk_sums(const uint32_t* v, uint64_t n, uint32_t* sums)
 {
     __shared__ uint32_t s_warp[kThreads / 32];
@@ -142,23 +225,48 @@ __global__ void k_chunk_scan(uint32_t* v, uint64_t n, const uint32_t* sums)
     }
 }
 
+cudaError_t scan_enqueue(uint32_t* v, uint64_t n, uint32_t* sums, cudaStream_t s)
+{
+    const uint64_t chunks = rb2::reorder_chunks(n);
+    k_chunk_sums<<<(unsigned)chunks, kThreads, 0, s>>>(v, n, sums);
+    k_sums_scan<<<1, 1024, 0, s>>>(sums, (uint32_t)chunks);
+    k_chunk_scan<<<(unsigned)chunks, kThreads, 0, s>>>(v, n, sums);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 namespace rb2 {
+
+cudaError_t reorder_init()
+{
+    const int smem = (int)(sizeof(uint32_t) << (3 + 3 * kReorderTiledMaxBits));
+    cudaError_t e = cudaFuncSetAttribute(k_tile_count, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_tile_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return e;
+}
 
 cudaError_t reorder_enqueue(const ReorderArgs& a, cudaStream_t s)
 {
     if (a.total == 0) return cudaSuccess;
     const uint64_t buckets = reorder_buckets(a.n_jobs, a.bits);
-    const uint64_t chunks = reorder_chunks(buckets);
+    if (a.bits <= kReorderTiledMaxBits) {
+        const uint32_t nb = (uint32_t)reorder_job_buckets(a.bits);
+        const size_t smem = sizeof(uint32_t) * nb;
+        k_tile_count<<<a.n_tiles, kTileThreads, smem, s>>>(a);
+        const dim3 cols((nb + 255) / 256, std::min<uint32_t>(a.n_jobs, 65535u));
+        k_tile_columns<<<cols, 256, 0, s>>>(a);
+        cudaError_t e = scan_enqueue(a.hist, buckets, a.chunk_sums, s);
+        if (e != cudaSuccess) return e;
+        k_tile_scatter<<<a.n_tiles, kTileThreads, smem, s>>>(a);
+        return cudaGetLastError();
+    }
     cudaError_t e = cudaMemsetAsync(a.hist, 0, buckets * sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
     const size_t smem = a.n_jobs <= kSmemJobs ? (a.n_jobs + 1) * sizeof(unsigned long long) : 0;
     const unsigned grid = (unsigned)std::min<uint64_t>((a.total + 255) / 256, (uint64_t)std::max(a.sms, 1) * 8);
     k_reorder<false><<<grid, 256, smem, s>>>(a);
-    k_chunk_sums<<<(unsigned)chunks, kThreads, 0, s>>>(a.hist, buckets, a.chunk_sums);
-    k_sums_scan<<<1, 1024, 0, s>>>(a.chunk_sums, (uint32_t)chunks);
-    k_chunk_scan<<<(unsigned)chunks, kThreads, 0, s>>>(a.hist, buckets, a.chunk_sums);
+    if ((e = scan_enqueue(a.hist, buckets, a.chunk_sums, s)) != cudaSuccess) return e;
     k_reorder<true><<<grid, 256, smem, s>>>(a);
     return cudaGetLastError();
 }

@@ -603,6 +603,13 @@ struct rb2_batch {
     uint32_t* d_perm = nullptr;
     uint32_t* d_keys = nullptr;
     uint64_t hist_cap = 0, chunk_cap = 0;
+    // tiled form of the sort (reorder <= 4): tile table, first tile of each
+    // job, per-tile bucket counters
+    rb2::ReorderTile* d_tiles = nullptr;
+    uint32_t* d_job_tile0 = nullptr;
+    uint32_t* d_cnt = nullptr;
+    uint32_t n_tiles = 0;
+    uint64_t cnt_cap = 0;
 
     void drop_graph()
     {
@@ -631,6 +638,10 @@ int batch_enqueue(rb2_batch* b, cudaStream_t s)
         r.chunk_sums = b->d_chunk_sums;
         r.perm = b->d_perm;
         r.keys = b->d_keys;
+        r.tiles = b->d_tiles;
+        r.job_tile0 = b->d_job_tile0;
+        r.cnt = b->d_cnt;
+        r.n_tiles = b->n_tiles;
         r.sms = b->occ.sms;
         RB2_CUDA(rb2::reorder_enqueue(r, s), "ray reordering");
         a.perm = b->d_perm;
@@ -709,6 +720,45 @@ int batch_prepare_reorder(rb2_batch* b, uint32_t bits)
         if ((e = rb2::dev_malloc(&b->d_chunk_sums, sizeof(uint32_t) * chunks)) != cudaSuccess)
             return fail(RB2_ENOMEM, std::string("reordering scan: ") + cudaGetErrorString(e));
         b->chunk_cap = chunks;
+    }
+    if (bits <= rb2::kReorderTiledMaxBits) {
+        RB2_CUDA(rb2::reorder_init(), "reordering shared memory");
+        if (!b->d_tiles) {
+            // Tiles of at most reorder_tile_rays() rays that never cross a job.
+            const uint32_t per = rb2::reorder_tile_rays(b->total, b->occ.sms);
+            std::vector<rb2::ReorderTile> tiles;
+            std::vector<uint32_t> tile0(n + 1, 0);
+            uint64_t at = 0;
+            for (uint32_t i = 0; i < n; i++) {
+                tile0[i] = (uint32_t)tiles.size();
+                const uint64_t end = at + b->jobs[i].n;
+                for (uint64_t t = at; t < end; t += per)
+                    tiles.push_back(rb2::ReorderTile{i, (uint32_t)t, (uint32_t)std::min<uint64_t>(end, t + per), 0u});
+                at = end;
+            }
+            tile0[n] = (uint32_t)tiles.size();
+            if ((e = rb2::dev_malloc(&b->d_tiles, sizeof(rb2::ReorderTile) * std::max<size_t>(tiles.size(), 1))) != cudaSuccess ||
+                (e = rb2::dev_malloc(&b->d_job_tile0, sizeof(uint32_t) * (n + 1))) != cudaSuccess) {
+                rb2::dev_free(b->d_tiles);
+                b->d_tiles = nullptr;
+                return fail(RB2_ENOMEM, std::string("reordering tiles: ") + cudaGetErrorString(e));
+            }
+            if (!tiles.empty())
+                RB2_CUDA(cudaMemcpy(b->d_tiles, tiles.data(), sizeof(rb2::ReorderTile) * tiles.size(),
+                                    cudaMemcpyHostToDevice), "reordering tiles");
+            RB2_CUDA(cudaMemcpy(b->d_job_tile0, tile0.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice),
+                     "reordering tiles");
+            b->n_tiles = (uint32_t)tiles.size();
+        }
+        const uint64_t cnt = (uint64_t)b->n_tiles * rb2::reorder_job_buckets(bits);
+        if (cnt > b->cnt_cap) {
+            rb2::dev_free(b->d_cnt);
+            b->d_cnt = nullptr;
+            b->cnt_cap = 0;
+            if ((e = rb2::dev_malloc(&b->d_cnt, sizeof(uint32_t) * cnt)) != cudaSuccess)
+                return fail(RB2_ENOMEM, std::string("reordering tile counters: ") + cudaGetErrorString(e));
+            b->cnt_cap = cnt;
+        }
     }
     return RB2_OK;
 }
@@ -797,6 +847,9 @@ int rb2_batch_destroy(rb2_batch* b)
     rb2::dev_free(b->d_chunk_sums);
     rb2::dev_free(b->d_perm);
     rb2::dev_free(b->d_keys);
+    rb2::dev_free(b->d_tiles);
+    rb2::dev_free(b->d_job_tile0);
+    rb2::dev_free(b->d_cnt);
     delete b;
     return RB2_OK;
 }
