@@ -209,15 +209,16 @@ class ClockSampler:
 L2_BYTES = 126 * 1024 * 1024
 
 # DRAM bytes per algorithmic byte of the batched traversal kernel, from ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on captures
-# small enough for the profiler, measured against the launch's algorithmic
-# bytes.  Keyed by node order: the compressed 8-wide kernel on the first 8
-# scenes of this workload (its triangle counts and seeds, 524,288 rays each,
-# block 256, 64 registers); the binary kernel on 8 heightfields of 500k
-# triangles with 524,288 rays each.
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on a case small
+# enough for the profiler: the first 8 scenes of this workload (its triangle
+# counts and seeds, 524,288 rays each, 7,023.9 MB of algorithmic bytes), block
+# 256.  Keyed by (node order, ray reordering on): the compressed 8-wide kernel
+# at 64 registers on rays in their own order; the binary BFS kernel at 48
+# registers on rays reordered at 5 bits per axis.
 DRAM_PER_ALG_BYTE = {
-    3: (403.0e6 / 7023.9e6, "first 8 scenes of this workload, 4.19M rays, compressed 8-wide layout"),
-    1: (618.5e6 / 7961.2e6, "8 scenes x 500k triangles, 4.19M rays, binary BFS layout"),
+    (3, False): (403.0e6 / 7023.9e6, "first 8 scenes of this workload, 4.19M rays, compressed 8-wide layout"),
+    (1, True): (595.1e6 / 7023.9e6, "first 8 scenes of this workload, 4.19M rays, binary BFS layout, rays "
+                                    "reordered"),
 }
 
 
@@ -455,9 +456,17 @@ def run_rb2(args, rank, world, local_rank):
     alg_per_launch = ch_bytes + ah_bytes
     achieved = alg_per_launch / launch_s / 1e9
     order = (tuned or {}).get("node_order", 0)
-    ratio, ratio_src = DRAM_PER_ALG_BYTE.get(order, DRAM_PER_ALG_BYTE[1])
+    sorted_rays = bool((tuned or {}).get("reorder", 0))
+    key = (order, sorted_rays)
+    if key not in DRAM_PER_ALG_BYTE:  # the capture of the nearest variant: same ray order, binary or compressed
+        key = (3, False) if order == 3 or not sorted_rays else (1, True)
+    ratio, ratio_src = DRAM_PER_ALG_BYTE[key]
     traffic = alg_per_launch * ratio
     layout_name = {0: "binary DFS", 1: "binary BFS", 2: "4-wide", 3: "compressed 8-wide"}.get(order, "binary DFS")
+    # kernels of the ray-reordering sort per batched launch: one pass (count, columns, 3 scan, scatter) at
+    # 3-4 bits per axis, two passes at 5-6
+    reorder_bits = (tuned or {}).get("reorder", 0)
+    sort_launches = 0 if not reorder_bits else (6 if reorder_bits <= 4 else 12)
 
     cpu_baseline = builder = None
     if rank == 0 and world == 1:
@@ -510,7 +519,9 @@ def run_rb2(args, rank, world, local_rank):
                       "layout and the default launch shape; same_layout = the autotuned layout and launch shape",
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(achieved / hbm_peak, 4), "traffic": round(traffic),
-                     "kernel": f"k_trace_jobs<BLOCK, REGS, LAYOUT> (batched, 1 launch/step, {layout_name} nodes)",
+                     "kernel": f"k_trace_jobs<BLOCK, REGS, LAYOUT> (batched, 1 launch/step, {layout_name} nodes)"
+                               + (f"; the step time includes the {sort_launches} ray-reordering launches before it"
+                                  if sort_launches else ""),
                      "peak_source": peak_src,
                      "alg_bytes_per_launch": round(alg_per_launch),
                      "alg_bytes_per_ray": round(alg_per_launch / total_rays, 1),
@@ -532,9 +543,10 @@ def run_rb2(args, rank, world, local_rank):
                         f"rays through {args.e2e_depth} streams, copies in the timed region, CUDA events)",
                 "single_call_mrays": round(e2e_single_rate / 1e6, 2),
                 "single_call_path": "one blocking rb2_trace_host per job, 16-byte hits for every ray"},
-        "gpu_launches": args.steps * (2 + 4 * len(scenes)),
-        "gpu_launches_note": "timed region: batched steps (1 traversal launch each), closest-hit batch steps "
-                             "(1 each), plain steps with default and with tuned layout (2 per scene each)",
+        "gpu_launches": args.steps * (2 * (1 + sort_launches) + 4 * len(scenes)),
+        "gpu_launches_note": f"timed region: batched steps (1 traversal launch each, after {sort_launches} "
+                             "ray-reordering launches), closest-hit batch steps (the same), plain steps with "
+                             "default and with tuned layout (2 per scene each)",
         "clocks": clocks,
     }
     if cpu_baseline is not None:
@@ -1029,7 +1041,7 @@ def main():
     ap.add_argument("--e2e-depth", type=int, default=4, help="streams of the pipelined host path")
     ap.add_argument("--serve-jobs", type=int, default=10000,
                     help="config-5 jobs in the serving measurement (0: skip)")
-    ap.add_argument("--serve-slots", type=int, default=8, help="concurrent slots of the continuous server")
+    ap.add_argument("--serve-slots", type=int, default=32, help="concurrent slots of the continuous server")
     ap.add_argument("--no-integrators", dest="integrators", action="store_false",
                     help="leave configs 1-3 out of the default line")
     ap.add_argument("--workload", choices=["trace", "ao", "pt", "bdpt", "raycast", "profile", "serve-curve"],

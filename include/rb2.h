@@ -248,7 +248,7 @@ typedef struct {
     uint32_t node_order;      /* RB2_NODE_ORDER_*; applied to every tracer in the batch */
     uint32_t regs;            /* register budget of the kernel variant: 64, 48 or 40 (0 = 64);
                                  lower budgets keep more warps resident and spill a little to L1 */
-    uint32_t reorder;         /* ray reordering before the traversal: 0 off, or k in 3..5: each job's
+    uint32_t reorder;         /* ray reordering before the traversal: 0 off, or k in 3..6: each job's
                                  rays are visited in the order of (direction octant, k-bit-per-axis
                                  Morton code of the origin within its scene's box), so a warp's rays
                                  start near each other and head the same way; records still go to

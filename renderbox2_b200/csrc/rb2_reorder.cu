@@ -7,8 +7,13 @@ namespace {
 
 constexpr uint32_t kChunk = 2048;        // counters per scan chunk
 constexpr uint32_t kThreads = 256;       // threads per scan block (8 counters each)
-constexpr uint32_t kSmemJobs = 1024;     // job prefixes staged in shared memory up to this many jobs
-constexpr uint32_t kTileThreads = 1024;  // threads per tile CTA of the tiled form
+constexpr uint32_t kTileThreads = 1024;  // threads per tile CTA
+constexpr uint32_t kWarpAggMax = 64;     // histograms this small aggregate each warp's equal digits
+
+// Passes of the sort: the whole key (k <= 4), or the low then the high digit (k = 5, 6).
+enum Pass : int { kWhole = 0, kLow = 1, kHigh = 2 };
+
+__device__ __forceinline__ uint32_t low_bits(uint32_t k) { return 3 * k - 12; }
 
 __device__ __forceinline__ uint32_t quantize(float x, float lo, float inv_extent, float cells, uint32_t qmax)
 {
@@ -36,29 +41,61 @@ __device__ __forceinline__ uint32_t key_of(const rb2::ReorderArgs& a, uint32_t j
     return (oct << (3 * k)) | m;
 }
 
-// ---------------------------------------------------------------- tiled form
+template <int P>
+__device__ __forceinline__ uint32_t digit_of(uint32_t key, uint32_t k)
+{
+    if constexpr (P == kWhole) return key;
+    else if constexpr (P == kLow) return key & ((1u << low_bits(k)) - 1u);
+    else return key >> low_bits(k);
+}
 
-// Step 1: the tile's keys and its shared-memory histogram, stored as row t of cnt.
-__global__ void __launch_bounds__(kTileThreads) k_tile_count(const rb2::ReorderArgs a)
+// Adds one to counter[digit] for every valid lane and returns each lane's
+// previous value plus its rank among the warp's lanes of the same digit (the
+// full warp calls this together).  Small histograms aggregate equal digits in
+// the warp first, so one lane per digit touches shared memory.
+__device__ __forceinline__ uint32_t take(uint32_t* counter, uint32_t digit, bool valid, bool aggregate)
+{
+    if (!aggregate) return valid ? atomicAdd(&counter[digit], 1u) : 0u;
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t tag = valid ? digit : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, tag);
+    const unsigned leader = __ffs(peers) - 1u;
+    uint32_t base = 0;
+    if (valid && lane == leader) base = atomicAdd(&counter[digit], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    return base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+}
+
+// Step 1: the tile's digits counted in shared memory, stored as row t of cnt.
+// The first pass computes each ray's key from the ray and keeps it in keys.
+template <int P>
+__global__ void __launch_bounds__(kTileThreads) k_tile_count(const rb2::ReorderArgs a, uint32_t nb)
 {
     extern __shared__ uint32_t s_h[];
-    const uint32_t nb = 1u << (3 + 3 * a.bits);
+    const bool agg = nb <= kWarpAggMax;
+    const uint32_t warp0 = (threadIdx.x & ~31u), lane = threadIdx.x & 31u;
     for (uint32_t t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
         for (uint32_t i = threadIdx.x; i < nb; i += kTileThreads) s_h[i] = 0u;
         __syncthreads();
         const rb2::ReorderTile tl = a.tiles[t];
         const uint64_t s0 = a.start[tl.job];
-        // Two rays per thread per pass, so each thread has both loads in flight.
-        for (uint32_t s = tl.begin + threadIdx.x; s < tl.end; s += 2 * kTileThreads) {
-            const uint32_t s2 = s + kTileThreads;
-            const uint32_t k1 = key_of(a, tl.job, s - s0);
-            const uint32_t k2 = s2 < tl.end ? key_of(a, tl.job, s2 - s0) : 0u;
-            a.keys[s] = k1;
-            atomicAdd(&s_h[k1], 1u);
-            if (s2 < tl.end) {
-                a.keys[s2] = k2;
-                atomicAdd(&s_h[k2], 1u);
+        // Whole warps step together (the aggregation needs every lane); two
+        // entries per lane per step keep two loads in flight.
+        for (uint32_t w = tl.begin + warp0; w < tl.end; w += 2 * kTileThreads) {
+            const uint32_t s1 = w + lane, s2 = w + kTileThreads + lane;
+            const bool v1 = s1 < tl.end, v2 = s2 < tl.end;
+            uint32_t k1 = 0, k2 = 0;
+            if constexpr (P == kHigh) {
+                if (v1) k1 = a.pairs[s1].x;
+                if (v2) k2 = a.pairs[s2].x;
+            } else {
+                if (v1) k1 = key_of(a, tl.job, s1 - s0);
+                if (v2) k2 = key_of(a, tl.job, s2 - s0);
+                if (v1) a.keys[s1] = k1;
+                if (v2) a.keys[s2] = k2;
             }
+            take(s_h, digit_of<P>(k1, a.bits), v1, agg);
+            if (__any_sync(0xFFFFFFFFu, v2)) take(s_h, digit_of<P>(k2, a.bits), v2, agg);
         }
         __syncthreads();
         uint32_t* row = a.cnt + (uint64_t)t * nb;
@@ -68,11 +105,10 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_count(const rb2::ReorderA
 }
 
 // Step 2: per (job, bucket), an exclusive scan down the job's tiles, in place;
-// the bucket's total goes to tot = a.hist.
-__global__ void k_tile_columns(const rb2::ReorderArgs a)
+// the bucket's total goes to tot.
+__global__ void k_tile_columns(const rb2::ReorderArgs a, uint32_t nb)
 {
     constexpr uint32_t kRows = 8;  // rows loaded together, so their loads overlap
-    const uint32_t nb = 1u << (3 + 3 * a.bits);
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
     uint32_t* __restrict__ cnt = a.cnt;
@@ -90,62 +126,44 @@ __global__ void k_tile_columns(const rb2::ReorderArgs a)
                 run += c[i];
             }
         }
-        a.hist[(uint64_t)j * nb + b] = run;
+        a.tot[(uint64_t)j * nb + b] = run;
     }
 }
 
 // Step 4: the tile's first position in every bucket (bucket start + the
-// tile's offset inside it) in shared memory; each ray takes the next one.
-__global__ void __launch_bounds__(kTileThreads) k_tile_scatter(const rb2::ReorderArgs a)
+// tile's offset inside it) in shared memory; each entry takes the next one.
+template <int P>
+__global__ void __launch_bounds__(kTileThreads) k_tile_scatter(const rb2::ReorderArgs a, uint32_t nb)
 {
     extern __shared__ uint32_t s_off[];
-    const uint32_t nb = 1u << (3 + 3 * a.bits);
+    const bool agg = nb <= kWarpAggMax;
+    const uint32_t warp0 = (threadIdx.x & ~31u), lane = threadIdx.x & 31u;
     for (uint32_t t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
         const rb2::ReorderTile tl = a.tiles[t];
         const uint32_t* row = a.cnt + (uint64_t)t * nb;
-        const uint32_t* base = a.hist + (uint64_t)tl.job * nb;
+        const uint32_t* base = a.tot + (uint64_t)tl.job * nb;
         for (uint32_t i = threadIdx.x; i < nb; i += kTileThreads) s_off[i] = base[i] + row[i];
         __syncthreads();
-        for (uint32_t s = tl.begin + threadIdx.x; s < tl.end; s += kTileThreads) {
-            const uint32_t pos = atomicAdd(&s_off[a.keys[s]], 1u);
-            a.perm[pos] = s;
+        for (uint32_t w = tl.begin + warp0; w < tl.end; w += kTileThreads) {
+            const uint32_t s = w + lane;
+            const bool v = s < tl.end;
+            uint32_t key = 0, slot = s;
+            if constexpr (P == kHigh) {
+                if (v) {
+                    const uint2 pr = a.pairs[s];
+                    key = pr.x;
+                    slot = pr.y;
+                }
+            } else {
+                if (v) key = a.keys[s];
+            }
+            const uint32_t pos = take(s_off, digit_of<P>(key, a.bits), v, agg);
+            if (v) {
+                if constexpr (P == kLow) a.pairs[pos] = make_uint2(key, slot);
+                else a.perm[pos] = slot;
+            }
         }
         __syncthreads();
-    }
-}
-
-// ------------------------------------------------------------ global form (k = 5)
-
-// Step 1 (kScatter false): each ray's key, kept in `keys`, and the bucket
-// counts.  Step 3 (true): each ray takes the next position of its bucket,
-// whose counter holds the bucket's start after the scan, and records its
-// slot there.  Buckets are job-major: (job << (3 + 3k)) | key.
-template <bool kScatter>
-__global__ void k_reorder(const rb2::ReorderArgs a)
-{
-    extern __shared__ unsigned long long s_start[];
-    const bool staged = a.n_jobs <= kSmemJobs;
-    if (staged)
-        for (uint32_t i = threadIdx.x; i <= a.n_jobs; i += blockDim.x) s_start[i] = a.start[i];
-    __syncthreads();
-    const unsigned long long* st = staged ? s_start : a.start;
-    const uint32_t shift = 3 + 3 * a.bits;
-    for (uint64_t slot = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; slot < a.total;
-         slot += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t lo = 0, hi = a.n_jobs;  // st[lo] <= slot < st[hi]
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (st[mid] <= slot) lo = mid; else hi = mid;
-        }
-        if constexpr (kScatter) {
-            const uint64_t b = ((uint64_t)lo << shift) | a.keys[slot];
-            const uint32_t pos = atomicAdd(&a.hist[b], 1u);
-            a.perm[pos] = (uint32_t)slot;
-        } else {
-            const uint32_t key = key_of(a, lo, slot - st[lo]);
-            a.keys[slot] = key;
-            atomicAdd(&a.hist[((uint64_t)lo << shift) | key], 1u);
-        }
     }
 }
 
@@ -240,35 +258,40 @@ namespace rb2 {
 
 cudaError_t reorder_init()
 {
-    const int smem = (int)(sizeof(uint32_t) << (3 + 3 * kReorderTiledMaxBits));
-    cudaError_t e = cudaFuncSetAttribute(k_tile_count, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_tile_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int smem = (int)(sizeof(uint32_t) << kReorderHighBits);
+    cudaError_t e = cudaSuccess;
+    const void* fns[] = {(const void*)k_tile_count<kWhole>, (const void*)k_tile_count<kLow>,
+                         (const void*)k_tile_count<kHigh>, (const void*)k_tile_scatter<kWhole>,
+                         (const void*)k_tile_scatter<kLow>, (const void*)k_tile_scatter<kHigh>};
+    for (const void* f : fns)
+        if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) break;
     return e;
 }
 
+namespace {
+
+template <int P>
+cudaError_t pass_enqueue(const ReorderArgs& a, uint32_t nb, cudaStream_t s)
+{
+    const size_t smem = sizeof(uint32_t) * nb;
+    k_tile_count<P><<<a.n_tiles, kTileThreads, smem, s>>>(a, nb);
+    const dim3 cols((nb + 255) / 256, std::min<uint32_t>(a.n_jobs, 65535u));
+    k_tile_columns<<<cols, 256, 0, s>>>(a, nb);
+    cudaError_t e = scan_enqueue(a.tot, (uint64_t)a.n_jobs * nb, a.chunk_sums, s);
+    if (e != cudaSuccess) return e;
+    k_tile_scatter<P><<<a.n_tiles, kTileThreads, smem, s>>>(a, nb);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
 cudaError_t reorder_enqueue(const ReorderArgs& a, cudaStream_t s)
 {
-    if (a.total == 0) return cudaSuccess;
-    const uint64_t buckets = reorder_buckets(a.n_jobs, a.bits);
-    if (a.bits <= kReorderTiledMaxBits) {
-        const uint32_t nb = (uint32_t)reorder_job_buckets(a.bits);
-        const size_t smem = sizeof(uint32_t) * nb;
-        k_tile_count<<<a.n_tiles, kTileThreads, smem, s>>>(a);
-        const dim3 cols((nb + 255) / 256, std::min<uint32_t>(a.n_jobs, 65535u));
-        k_tile_columns<<<cols, 256, 0, s>>>(a);
-        cudaError_t e = scan_enqueue(a.hist, buckets, a.chunk_sums, s);
-        if (e != cudaSuccess) return e;
-        k_tile_scatter<<<a.n_tiles, kTileThreads, smem, s>>>(a);
-        return cudaGetLastError();
-    }
-    cudaError_t e = cudaMemsetAsync(a.hist, 0, buckets * sizeof(uint32_t), s);
+    if (a.total == 0 || a.n_tiles == 0) return cudaSuccess;
+    if (a.bits <= kReorderOnePassMaxBits) return pass_enqueue<kWhole>(a, 1u << (3 + 3 * a.bits), s);
+    cudaError_t e = pass_enqueue<kLow>(a, 1u << (3 * a.bits - 12), s);
     if (e != cudaSuccess) return e;
-    const size_t smem = a.n_jobs <= kSmemJobs ? (a.n_jobs + 1) * sizeof(unsigned long long) : 0;
-    const unsigned grid = (unsigned)std::min<uint64_t>((a.total + 255) / 256, (uint64_t)std::max(a.sms, 1) * 8);
-    k_reorder<false><<<grid, 256, smem, s>>>(a);
-    if ((e = scan_enqueue(a.hist, buckets, a.chunk_sums, s)) != cudaSuccess) return e;
-    k_reorder<true><<<grid, 256, smem, s>>>(a);
-    return cudaGetLastError();
+    return pass_enqueue<kHigh>(a, 1u << kReorderHighBits, s);
 }
 
 }  // namespace rb2

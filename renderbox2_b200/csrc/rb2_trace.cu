@@ -595,21 +595,21 @@ struct rb2_batch {
     Occupancy occ;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    // ray reordering (cfg.reorder): per-job scene boxes, bucket counters, scan
-    // scratch and the visiting order, allocated when first enabled
+    // ray reordering (cfg.reorder), allocated when first enabled: per-job
+    // scene boxes, the tile table and first tile of each job, per-tile
+    // counters, per-job bucket totals, scan scratch, each ray's key, the
+    // (key, slot) pairs between the two passes of a wide key, the visiting order
     float4* d_boxes = nullptr;
-    uint32_t* d_hist = nullptr;
-    uint32_t* d_chunk_sums = nullptr;
-    uint32_t* d_perm = nullptr;
-    uint32_t* d_keys = nullptr;
-    uint64_t hist_cap = 0, chunk_cap = 0;
-    // tiled form of the sort (reorder <= 4): tile table, first tile of each
-    // job, per-tile bucket counters
     rb2::ReorderTile* d_tiles = nullptr;
     uint32_t* d_job_tile0 = nullptr;
     uint32_t* d_cnt = nullptr;
+    uint32_t* d_tot = nullptr;
+    uint32_t* d_chunk_sums = nullptr;
+    uint32_t* d_keys = nullptr;
+    uint2* d_pairs = nullptr;
+    uint32_t* d_perm = nullptr;
     uint32_t n_tiles = 0;
-    uint64_t cnt_cap = 0;
+    uint64_t cnt_cap = 0, tot_cap = 0, chunk_cap = 0;
 
     void drop_graph()
     {
@@ -634,15 +634,15 @@ int batch_enqueue(rb2_batch* b, cudaStream_t s)
         r.n_jobs = (uint32_t)b->jobs.size();
         r.bits = b->cfg.reorder;
         r.total = b->total;
-        r.hist = b->d_hist;
-        r.chunk_sums = b->d_chunk_sums;
-        r.perm = b->d_perm;
-        r.keys = b->d_keys;
         r.tiles = b->d_tiles;
         r.job_tile0 = b->d_job_tile0;
         r.cnt = b->d_cnt;
+        r.tot = b->d_tot;
+        r.chunk_sums = b->d_chunk_sums;
+        r.keys = b->d_keys;
+        r.pairs = b->d_pairs;
+        r.perm = b->d_perm;
         r.n_tiles = b->n_tiles;
-        r.sms = b->occ.sms;
         RB2_CUDA(rb2::reorder_enqueue(r, s), "ray reordering");
         a.perm = b->d_perm;
     }
@@ -667,17 +667,30 @@ int batch_check_layout(const rb2_batch* b)
     return RB2_OK;
 }
 
+// (Re)allocates *p for at least `n` entries when its capacity `cap` is smaller.
+template <typename T>
+cudaError_t grow(T** p, uint64_t& cap, uint64_t n)
+{
+    if (n <= cap && *p) return cudaSuccess;
+    rb2::dev_free(*p);
+    *p = nullptr;
+    cap = 0;
+    const cudaError_t e = rb2::dev_malloc(p, sizeof(T) * std::max<uint64_t>(n, 1));
+    if (e == cudaSuccess) cap = n;
+    return e;
+}
+
 // Buffers of ray reordering at `bits` per axis: each job's scene box (the union
-// of the root's child boxes) as lo and 1 / extent, counters, scan scratch
-// each ray's key and the visiting order.
+// of the root's child boxes) as lo and 1 / extent, the tile table, counters,
+// totals, scan scratch, keys, pairs (two-pass widths) and the visiting order.
 int batch_prepare_reorder(rb2_batch* b, uint32_t bits)
 {
     if (bits == 0) return RB2_OK;
-    if (bits < 3 || bits > 5) return fail(RB2_EINVAL, "reorder must be 0 or 3..5 bits per axis");
+    if (bits < rb2::kReorderMinBits || bits > rb2::kReorderMaxBits)
+        return fail(RB2_EINVAL, "reorder must be 0 or 3..6 bits per axis");
     if (b->total >= 0xFFFFFFFFull) return fail(RB2_EINVAL, "ray reordering needs fewer than 2^32 rays per batch");
     const uint32_t n = (uint32_t)b->jobs.size();
-    const uint64_t buckets = rb2::reorder_buckets(n, bits), chunks = rb2::reorder_chunks(buckets);
-    if (chunks > 0xFFFFFFFFull) return fail(RB2_EINVAL, "too many reordering buckets");
+    RB2_CUDA(rb2::reorder_init(), "reordering shared memory");
     cudaError_t e = cudaSuccess;
     if (!b->d_boxes) {
         std::vector<float4> boxes(2 * (size_t)std::max<uint32_t>(n, 1));
@@ -685,6 +698,7 @@ int batch_prepare_reorder(rb2_batch* b, uint32_t bits)
             const std::vector<uint32_t>& h = b->jobs[i].tracer->host_nodes;
             float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
             if (h.size() >= 12) {
+                // Compact2 root: child 0's box in words 0-3 (x, y) and 8-9 (z), child 1's in 4-7 and 10-11.
                 const int lo_w[2][3] = {{0, 2, 8}, {4, 6, 10}}, hi_w[2][3] = {{1, 3, 9}, {5, 7, 11}};
                 for (int a = 0; a < 3; a++) {
                     lo[a] = std::min(u2f(h[lo_w[0][a]]), u2f(h[lo_w[1][a]]));
@@ -701,65 +715,42 @@ int batch_prepare_reorder(rb2_batch* b, uint32_t bits)
         RB2_CUDA(cudaMemcpy(b->d_boxes, boxes.data(), sizeof(float4) * boxes.size(), cudaMemcpyHostToDevice),
                  "reordering boxes");
     }
-    if (!b->d_perm && (e = rb2::dev_malloc(&b->d_perm, sizeof(uint32_t) * std::max<uint64_t>(b->total, 1))) != cudaSuccess)
-        return fail(RB2_ENOMEM, std::string("reordering order: ") + cudaGetErrorString(e));
-    if (!b->d_keys && (e = rb2::dev_malloc(&b->d_keys, sizeof(uint32_t) * std::max<uint64_t>(b->total, 1))) != cudaSuccess)
-        return fail(RB2_ENOMEM, std::string("reordering keys: ") + cudaGetErrorString(e));
-    if (buckets > b->hist_cap) {
-        rb2::dev_free(b->d_hist);
-        b->d_hist = nullptr;
-        b->hist_cap = 0;
-        if ((e = rb2::dev_malloc(&b->d_hist, sizeof(uint32_t) * buckets)) != cudaSuccess)
-            return fail(RB2_ENOMEM, std::string("reordering counters: ") + cudaGetErrorString(e));
-        b->hist_cap = buckets;
-    }
-    if (chunks > b->chunk_cap) {
-        rb2::dev_free(b->d_chunk_sums);
-        b->d_chunk_sums = nullptr;
-        b->chunk_cap = 0;
-        if ((e = rb2::dev_malloc(&b->d_chunk_sums, sizeof(uint32_t) * chunks)) != cudaSuccess)
-            return fail(RB2_ENOMEM, std::string("reordering scan: ") + cudaGetErrorString(e));
-        b->chunk_cap = chunks;
-    }
-    if (bits <= rb2::kReorderTiledMaxBits) {
-        RB2_CUDA(rb2::reorder_init(), "reordering shared memory");
-        if (!b->d_tiles) {
-            // Tiles of at most reorder_tile_rays() rays that never cross a job.
-            const uint32_t per = rb2::reorder_tile_rays(b->total, b->occ.sms);
-            std::vector<rb2::ReorderTile> tiles;
-            std::vector<uint32_t> tile0(n + 1, 0);
-            uint64_t at = 0;
-            for (uint32_t i = 0; i < n; i++) {
-                tile0[i] = (uint32_t)tiles.size();
-                const uint64_t end = at + b->jobs[i].n;
-                for (uint64_t t = at; t < end; t += per)
-                    tiles.push_back(rb2::ReorderTile{i, (uint32_t)t, (uint32_t)std::min<uint64_t>(end, t + per), 0u});
-                at = end;
-            }
-            tile0[n] = (uint32_t)tiles.size();
-            if ((e = rb2::dev_malloc(&b->d_tiles, sizeof(rb2::ReorderTile) * std::max<size_t>(tiles.size(), 1))) != cudaSuccess ||
-                (e = rb2::dev_malloc(&b->d_job_tile0, sizeof(uint32_t) * (n + 1))) != cudaSuccess) {
-                rb2::dev_free(b->d_tiles);
-                b->d_tiles = nullptr;
-                return fail(RB2_ENOMEM, std::string("reordering tiles: ") + cudaGetErrorString(e));
-            }
-            if (!tiles.empty())
-                RB2_CUDA(cudaMemcpy(b->d_tiles, tiles.data(), sizeof(rb2::ReorderTile) * tiles.size(),
-                                    cudaMemcpyHostToDevice), "reordering tiles");
-            RB2_CUDA(cudaMemcpy(b->d_job_tile0, tile0.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice),
-                     "reordering tiles");
-            b->n_tiles = (uint32_t)tiles.size();
+    if (!b->d_tiles) {
+        // Tiles of at most reorder_tile_rays() rays that never cross a job.
+        const uint32_t per = rb2::reorder_tile_rays(b->total, b->occ.sms);
+        std::vector<rb2::ReorderTile> tiles;
+        std::vector<uint32_t> tile0(n + 1, 0);
+        uint64_t at = 0;
+        for (uint32_t i = 0; i < n; i++) {
+            tile0[i] = (uint32_t)tiles.size();
+            const uint64_t end = at + b->jobs[i].n;
+            for (uint64_t t = at; t < end; t += per)
+                tiles.push_back(rb2::ReorderTile{i, (uint32_t)t, (uint32_t)std::min<uint64_t>(end, t + per), 0u});
+            at = end;
         }
-        const uint64_t cnt = (uint64_t)b->n_tiles * rb2::reorder_job_buckets(bits);
-        if (cnt > b->cnt_cap) {
-            rb2::dev_free(b->d_cnt);
-            b->d_cnt = nullptr;
-            b->cnt_cap = 0;
-            if ((e = rb2::dev_malloc(&b->d_cnt, sizeof(uint32_t) * cnt)) != cudaSuccess)
-                return fail(RB2_ENOMEM, std::string("reordering tile counters: ") + cudaGetErrorString(e));
-            b->cnt_cap = cnt;
-        }
+        tile0[n] = (uint32_t)tiles.size();
+        if ((e = rb2::dev_malloc(&b->d_job_tile0, sizeof(uint32_t) * (n + 1))) != cudaSuccess)
+            return fail(RB2_ENOMEM, std::string("reordering tiles: ") + cudaGetErrorString(e));
+        if ((e = rb2::dev_malloc(&b->d_tiles, sizeof(rb2::ReorderTile) * std::max<size_t>(tiles.size(), 1))) !=
+            cudaSuccess)
+            return fail(RB2_ENOMEM, std::string("reordering tiles: ") + cudaGetErrorString(e));
+        if (!tiles.empty())
+            RB2_CUDA(cudaMemcpy(b->d_tiles, tiles.data(), sizeof(rb2::ReorderTile) * tiles.size(),
+                                cudaMemcpyHostToDevice), "reordering tiles");
+        RB2_CUDA(cudaMemcpy(b->d_job_tile0, tile0.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice),
+                 "reordering tiles");
+        b->n_tiles = (uint32_t)tiles.size();
     }
+    const uint64_t nb = rb2::reorder_max_buckets(bits), tot = (uint64_t)n * nb;
+    uint64_t perm_cap = b->d_perm ? b->total : 0, keys_cap = b->d_keys ? b->total : 0;
+    uint64_t pairs_cap = b->d_pairs ? b->total : 0;
+    if ((e = grow(&b->d_cnt, b->cnt_cap, (uint64_t)b->n_tiles * nb)) != cudaSuccess ||
+        (e = grow(&b->d_tot, b->tot_cap, tot)) != cudaSuccess ||
+        (e = grow(&b->d_chunk_sums, b->chunk_cap, rb2::reorder_chunks(tot))) != cudaSuccess ||
+        (e = grow(&b->d_keys, keys_cap, b->total)) != cudaSuccess ||
+        (e = grow(&b->d_perm, perm_cap, b->total)) != cudaSuccess ||
+        (bits > rb2::kReorderOnePassMaxBits && (e = grow(&b->d_pairs, pairs_cap, b->total)) != cudaSuccess))
+        return fail(RB2_ENOMEM, std::string("ray reordering buffers: ") + cudaGetErrorString(e));
     return RB2_OK;
 }
 
@@ -843,13 +834,14 @@ int rb2_batch_destroy(rb2_batch* b)
     rb2::dev_free(b->d_counter);
     rb2::dev_free(b->d_status);
     rb2::dev_free(b->d_boxes);
-    rb2::dev_free(b->d_hist);
-    rb2::dev_free(b->d_chunk_sums);
-    rb2::dev_free(b->d_perm);
-    rb2::dev_free(b->d_keys);
     rb2::dev_free(b->d_tiles);
     rb2::dev_free(b->d_job_tile0);
     rb2::dev_free(b->d_cnt);
+    rb2::dev_free(b->d_tot);
+    rb2::dev_free(b->d_chunk_sums);
+    rb2::dev_free(b->d_keys);
+    rb2::dev_free(b->d_pairs);
+    rb2::dev_free(b->d_perm);
     delete b;
     return RB2_OK;
 }
@@ -1046,7 +1038,7 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     // the search again with 4 bits per axis, then the other widths on its winner.
     if (b->total < 0xFFFFFFFFull) {
         if ((rc = search(4, best_r, best_r_ms))) return rc;
-        for (uint32_t bits : {3u, 5u}) {
+        for (uint32_t bits : {3u, 5u, 6u}) {
             rb2_batch_config c = best_r; c.reorder = bits; double ms;
             if ((rc = time_cfg(c, ms))) return rc;
             if (ms < best_r_ms) { best_r = c; best_r_ms = ms; }

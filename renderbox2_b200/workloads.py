@@ -108,14 +108,16 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
             "layout_probe_ms": {str(k): round(v, 3) for k, v in probe.items()}}
 
 
-def serving(n_jobs: int = 10000, n_bvh: int = 32, seed: int = 5, slots: int = 8, burst_jobs: int = 2000,
-            shared: bool | None = None):
+def serving(n_jobs: int = 10000, n_bvh: int = 32, seed: int = 5, slots: int = 32, burst_jobs: int = 2000,
+            shared: bool | None = None, hbm_budget: int = 48 << 30):
     """Config 5: pool of n_bvh lit heightfields (1k..4M triangles,
     log-uniform), n_jobs jobs, 70 % tile renders / 30 % ray batches.  The
     arrival rate is the throughput of the plain path (one job at a time) on a
     burst of the first `burst_jobs` jobs, i.e. the rate that saturates it;
     both paths then serve the same Poisson arrival sequence of all n_jobs.
     `capacity` compares both paths on that burst (every job queued at t = 0).
+    The continuous server runs `slots` concurrent jobs whose admitted
+    working sets stay within `hbm_budget` bytes.
     `shared` (default: more than 1000 jobs) takes ray-job inputs from one
     pinned ray set per BVH and outputs from a circular pinned arena
     (serve.SharedBuffers) instead of per-job host buffers."""
@@ -130,7 +132,7 @@ def serving(n_jobs: int = 10000, n_bvh: int = 32, seed: int = 5, slots: int = 8,
     sh = SharedBuffers(pool, rays_per_bvh=c["rays_max"]) if use_shared else None
     jobs = config5_jobs(pool, n_jobs, seed=seed, shared=sh)
     setup_s = time.time() - t0
-    cont = Server(pool, slots=slots, fifo=False)
+    cont = Server(pool, slots=slots, fifo=False, hbm_budget=hbm_budget)
     plain = Server(pool, fifo=True)
     # warm-up: a few jobs through both
     cont.run(jobs.subset(range(min(8, n_jobs))))
@@ -143,7 +145,8 @@ def serving(n_jobs: int = 10000, n_bvh: int = 32, seed: int = 5, slots: int = 8,
     _, s_plain = plain.run(jobs.with_arrivals(arr))
     _, s_cont = cont.run(jobs.with_arrivals(arr))
     keep = ("p50_s", "p99_s", "mean_s", "mrays_per_s", "wall_s", "max_concurrent")
-    return {"jobs": n_jobs, "burst_jobs": nb, "host_buffers": "shared ray sets + output arena" if use_shared
+    return {"jobs": n_jobs, "burst_jobs": nb, "slots": slots, "hbm_budget_gb": hbm_budget >> 30,
+            "host_buffers": "shared ray sets + output arena" if use_shared
             else "per job", "bvhs": n_bvh, "pool_triangles": int(sum(counts)),
             "arrival_rate_jobs_per_s": round(rate, 2), "setup_s": round(setup_s, 1),
             "resident_gb": round(s_cont["resident_bytes"] / 1e9, 2),
@@ -157,8 +160,8 @@ def serving(n_jobs: int = 10000, n_bvh: int = 32, seed: int = 5, slots: int = 8,
                          "ratio": round(cburst["mrays_per_s"] / max(burst["mrays_per_s"], 1e-9), 3)}}
 
 
-def serving_curve(n_jobs: int = 3000, n_bvh: int = 32, seed: int = 5, slots: int = 8,
-                  loads=(0.5, 0.8, 1.0, 1.2), burst_jobs: int = 1000):
+def serving_curve(n_jobs: int = 3000, n_bvh: int = 32, seed: int = 5, slots: int = 32,
+                  loads=(0.5, 0.8, 1.0, 1.2), burst_jobs: int = 1000, hbm_budget: int = 48 << 30):
     """Latency against offered load for config 5: the continuous server's
     burst capacity (jobs per second with every job queued at t = 0) sets the
     unit of load; each point serves the same n_jobs with Poisson arrivals at
@@ -172,7 +175,7 @@ def serving_curve(n_jobs: int = 3000, n_bvh: int = 32, seed: int = 5, slots: int
     pool = build_pool(counts, seed=seed)
     sh = SharedBuffers(pool, rays_per_bvh=c["rays_max"])
     jobs = config5_jobs(pool, n_jobs, seed=seed, shared=sh)
-    cont = Server(pool, slots=slots, fifo=False)
+    cont = Server(pool, slots=slots, fifo=False, hbm_budget=hbm_budget)
     plain = Server(pool, fifo=True)
     cont.run(jobs.subset(range(min(8, n_jobs))))
     plain.run(jobs.subset(range(min(8, n_jobs))))

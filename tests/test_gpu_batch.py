@@ -87,7 +87,7 @@ def test_batch_equals_plain_launches(rb, orc, cuda):
     dict(node_order=3, regs=40, chunk=4, fetch_threshold=8),
     dict(reorder=3), dict(reorder=4, chunk=4), dict(reorder=5, node_order=1, regs=48, block_threads=256),
     dict(reorder=4, node_order=2), dict(reorder=4, node_order=3, regs=48, block_threads=256, fetch_threshold=16),
-    dict(reorder=5, node_order=3, regs=40, chunk=2),
+    dict(reorder=5, node_order=3, regs=40, chunk=2), dict(reorder=6), dict(reorder=6, node_order=3, regs=48),
 ])
 def test_batch_configs_give_identical_results(rb, orc, cuda, cfg):
     scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
@@ -249,8 +249,8 @@ def test_ray_reordering_keeps_every_ray(rb, orc, cuda):
     origin) order: with stencil masks, origins far outside the scene box,
     empty and one-ray jobs and a job spanning two scenes' worth of rays, every
     record still lands at its own ray's index and equals the plain launch's,
-    for 3, 4 and 5 bits per axis and after graph capture; widths outside 3..5
-    are refused."""
+    for 3 to 6 bits per axis (one- and two-pass sorts) and after graph
+    capture; widths outside 3..6 are refused."""
     scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
     # job 0 gets a stencil and a block of rays whose origins sit far outside the box
     sc, bvh, r = scenes[0]
@@ -265,7 +265,7 @@ def test_ray_reordering_keeps_every_ray(rb, orc, cuda):
     outs = outs + [out_m]
     plain = plain + [ref_m]
     batch = rb.TraceBatch(jobs)
-    for bits in (3, 4, 5):
+    for bits in (3, 4, 5, 6):
         batch.set_config(reorder=bits)
         for o in outs:
             o.fill_(7)
@@ -281,7 +281,7 @@ def test_ray_reordering_keeps_every_ray(rb, orc, cuda):
         batch.launch(s)
         s.synchronize()
         _check(outs, plain, cuda)
-    for bad in (1, 2, 6):
+    for bad in (1, 2, 7):
         with pytest.raises(rb.Rb2Error, match="reorder"):
             batch.set_config(reorder=bad)
     # the masked job equals the oracle on its active rays
