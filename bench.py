@@ -342,7 +342,11 @@ def run_rb2(args, rank, world, local_rank):
     # across all timed regions.
     with ClockSampler(local_rank) as clk:
         plain_ms, ch_ms, ah_ms = plain_timed()
-        tuned, tuned_ms = batch.autotune(stream=stream, reps=5)
+        if args.batch_config:
+            batch.set_config(**json.loads(args.batch_config))
+            tuned, tuned_ms = batch.config(), None
+        else:
+            tuned, tuned_ms = batch.autotune(stream=stream, reps=5)
         batch.capture(stream)
         for _ in range(args.warmup):
             batch.launch(stream)
@@ -351,6 +355,18 @@ def run_rb2(args, rank, world, local_rank):
         batch_ms = timed(lambda: batch.launch(stream), args.steps)
         got_ch, got_occ = gather_outputs()  # outputs of the last timed launch
         batch_status = batch.status(stream)
+        # The same launch without ray reordering (the plain launches have none).
+        unsorted_ms = None
+        if tuned.get("reorder", 0):
+            batch.set_config(**dict(tuned, reorder=0))
+            batch.capture(stream)
+            for _ in range(args.warmup):
+                batch.launch(stream)
+            torch.cuda.synchronize(dev)
+            barrier(world)
+            unsorted_ms = timed(lambda: batch.launch(stream), args.steps)
+            batch_status |= batch.status(stream)
+            batch.set_config(**tuned)
         ch_batch = rb.TraceBatch(ch_jobs)
         ch_batch.set_config(**tuned)
         ch_batch.capture(stream)
@@ -369,6 +385,8 @@ def run_rb2(args, rank, world, local_rank):
     batch_rate, batch_total = whole_job_rate(total_rays * args.steps, sum(batch_ms), world, dev)
     ch_batch_rate, _ = whole_job_rate(n_ch_total * args.steps, sum(ch_batch_ms), world, dev)
     same_rate, _ = whole_job_rate(total_rays * args.steps, sum(same_ms), world, dev)
+    unsorted_rate = (whole_job_rate(total_rays * args.steps, sum(unsorted_ms), world, dev)[0]
+                     if unsorted_ms is not None else None)
     for t in tracers:
         assert t.status() == 0, "device status word set"
     assert batch_status == 0 and ch_batch_status == 0, "batch status word set"
@@ -498,7 +516,8 @@ def run_rb2(args, rank, world, local_rank):
         "config": {
             "workload": "config 4: 64 heightfield scenes, log-uniform 1k..2M triangles, 1M incoherent "
                         "diffuse-bounce rays per scene, 50% closest-hit / 50% any-hit (occlusion)",
-            "mode": "batched: one persistent graph-replayed launch over 128 jobs (autotuned)",
+            "mode": "batched: one persistent graph-replayed launch over 128 jobs "
+                    + ("(configuration given on the command line)" if args.batch_config else "(autotuned)"),
             "autotuned": tuned, "scenes": len(scenes), "triangles": int(sum(s["tris"] for s in scenes)),
             "rays_per_step": int(total_rays), "l2": "flushed (256 MB write) between timed steps",
             "bvh_device_bytes": int(bvh_bytes), "build_s_host": round(build_s, 2), "parallelism": "replicas",
@@ -515,8 +534,11 @@ def run_rb2(args, rank, world, local_rank):
         "batched_closest_hit_mrays": round(ch_batch_rate / 1e6, 2),
         "batched_closest_hit_over_plain_same_layout": round(
             ch_batch_rate / 1e6 / (world * n_ch_total * args.steps / (same_ch_ms.sum() / 1e3) / 1e6), 3),
+        "batched_without_reorder_mrays": round(unsorted_rate / 1e6, 2) if unsorted_rate else None,
         "plain_note": "plain = 2 launches per scene (closest-hit half, any-hit half); default = the reference's DFS "
-                      "layout and the default launch shape; same_layout = the autotuned layout and launch shape",
+                      "layout and the default launch shape; same_layout = the autotuned layout and launch shape "
+                      "(plain launches have no ray reordering; batched_without_reorder = the batched launch with "
+                      "the tuned shape and reordering off)",
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(achieved / hbm_peak, 4), "traffic": round(traffic),
                      "kernel": f"k_trace_jobs<BLOCK, REGS, LAYOUT> (batched, 1 launch/step, {layout_name} nodes)"
@@ -543,10 +565,11 @@ def run_rb2(args, rank, world, local_rank):
                         f"rays through {args.e2e_depth} streams, copies in the timed region, CUDA events)",
                 "single_call_mrays": round(e2e_single_rate / 1e6, 2),
                 "single_call_path": "one blocking rb2_trace_host per job, 16-byte hits for every ray"},
-        "gpu_launches": args.steps * (2 * (1 + sort_launches) + 4 * len(scenes)),
+        "gpu_launches": args.steps * (2 * (1 + sort_launches) + (1 if sort_launches else 0) + 4 * len(scenes)),
         "gpu_launches_note": f"timed region: batched steps (1 traversal launch each, after {sort_launches} "
-                             "ray-reordering launches), closest-hit batch steps (the same), plain steps with "
-                             "default and with tuned layout (2 per scene each)",
+                             "ray-reordering launches), closest-hit batch steps (the same), batched steps without "
+                             "reordering (1 each, when reordering is on), plain steps with default and with tuned "
+                             "layout (2 per scene each)",
         "clocks": clocks,
     }
     if cpu_baseline is not None:
@@ -1060,6 +1083,9 @@ def main():
     ap.add_argument("--profile-ctas", type=int, default=0)
     ap.add_argument("--profile-chunk", type=int, default=1)
     ap.add_argument("--profile-reorder", type=int, default=0, help="profile: ray reordering bits per axis (0 off)")
+    ap.add_argument("--batch-config", default="",
+                    help="trace: a JSON rb2_batch_config for the batched launch instead of the autotuner's pick "
+                         "(for repeatable profiles)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

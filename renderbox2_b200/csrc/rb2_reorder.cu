@@ -23,6 +23,18 @@ __device__ __forceinline__ uint32_t quantize(float x, float lo, float inv_extent
     return q >= (float)qmax ? qmax : (uint32_t)q;
 }
 
+// Bits 0..9 of x moved to bits 0, 3, 6, ..., 27 (the usual magic-number
+// interleave), so three spread coordinates OR into a Morton code.
+__device__ __forceinline__ uint32_t spread3(uint32_t x)
+{
+    x &= 0x3FFu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
 // Key of a ray within its job: (direction octant, Morton code of the origin,
 // k bits per axis), 3 + 3k bits.
 __device__ __forceinline__ uint32_t key_of(const rb2::ReorderArgs& a, uint32_t j, uint64_t r)
@@ -34,9 +46,7 @@ __device__ __forceinline__ uint32_t key_of(const rb2::ReorderArgs& a, uint32_t j
     const float cells = (float)(1u << k);
     const uint32_t qx = quantize(o.x, lo.x, sc.x, cells, qmax), qy = quantize(o.y, lo.y, sc.y, cells, qmax),
                    qz = quantize(o.z, lo.z, sc.z, cells, qmax);
-    uint32_t m = 0;
-    for (uint32_t b = 0; b < k; b++)
-        m |= (((qx >> b) & 1u) << (3 * b)) | (((qy >> b) & 1u) << (3 * b + 1)) | (((qz >> b) & 1u) << (3 * b + 2));
+    const uint32_t m = spread3(qx) | (spread3(qy) << 1) | (spread3(qz) << 2);
     const uint32_t oct = (dd.x < 0.0f ? 1u : 0u) | (dd.y < 0.0f ? 2u : 0u) | (dd.z < 0.0f ? 4u : 0u);
     return (oct << (3 * k)) | m;
 }
@@ -69,7 +79,7 @@ __device__ __forceinline__ uint32_t take(uint32_t* counter, uint32_t digit, bool
 // Step 1: the tile's digits counted in shared memory, stored as row t of cnt.
 // The first pass computes each ray's key from the ray and keeps it in keys.
 template <int P>
-__global__ void __launch_bounds__(kTileThreads) k_tile_count(const rb2::ReorderArgs a, uint32_t nb)
+__global__ void __launch_bounds__(kTileThreads, 2) k_tile_count(const rb2::ReorderArgs a, uint32_t nb)
 {
     extern __shared__ uint32_t s_h[];
     const bool agg = nb <= kWarpAggMax;

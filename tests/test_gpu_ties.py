@@ -101,9 +101,11 @@ def test_ties_follow_the_reference_rule(rb, orc, cuda, tree, order):
           f"GPU chose the other triangle of a confirmed tie on {divergent}; reference-culled rays {culled}")
 
 
-@pytest.mark.parametrize("order", [0, 3])
-def test_ties_in_the_batched_launch(rb, orc, cuda, order):
-    """The job-table launch (closest hit + occlusion jobs) on the tie rays."""
+@pytest.mark.parametrize("order,reorder", [(0, 0), (3, 0), (1, 4), (0, 5)])
+def test_ties_in_the_batched_launch(rb, orc, cuda, order, reorder):
+    """The job-table launch (closest hit + occlusion jobs) on the tie rays,
+    with and without ray reordering (which changes only which rays share a
+    warp, so the binary layouts stay bit-identical at every tie)."""
     torch = cuda
     scene, bvh = _setup(rb, orc, "rb2")
     nodes, woop, tri = bvh.buffers_view()
@@ -114,10 +116,10 @@ def test_ties_in_the_batched_launch(rb, orc, cuda, order):
     out_h = torch.full((rays.shape[0], 4), 7, dtype=torch.int32, device="cuda")
     out_o = torch.full((rays.shape[0],), 7, dtype=torch.uint8, device="cuda")
     batch = rb.TraceBatch([(tr, d, rb.MODE_CLOSEST, out_h, None), (tr, d, rb.MODE_OCCLUSION, out_o, None)])
-    batch.set_config(node_order=order)
+    batch.set_config(node_order=order, reorder=reorder)
     batch.launch()
     got = out_h.cpu().numpy()
-    if order == 0:
+    if order in (0, 1):
         assert np.array_equal(got[:, 0], want["prim"])
         assert np.array_equal(got[:, 1].view(np.uint32), want["t"].view(np.uint32))
         assert np.array_equal(out_o.cpu().numpy().astype(bool), want["prim"] >= 0)
