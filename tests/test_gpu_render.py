@@ -100,32 +100,6 @@ def test_pt_is_deterministic(rb, cuda):
     assert cuda.equal(a, b)
 
 
-@pytest.mark.parametrize("order", [0, 3])
-def test_pt_queue_reordering_keeps_the_image(rb, cuda, order):
-    """Sorting the extension and shadow queues before each trace changes only
-    which paths share a warp: the image is bit-identical at 3 and 4 bits per
-    axis, in the binary and the compressed 8-wide layout, over several waves
-    (queues of different lengths), and widths outside 3..4 are refused."""
-    from renderbox2_b200.configs import CONFIG2 as C2
-    from renderbox2_b200.render import DeviceScene, Integrator, PathIntegratorParams
-    room = _room(rb, n_spheres=40)
-    tr = rb.CudaTracer(rb.BVH(room))
-    tr.set_node_order(order)
-    it = Integrator(tr, DeviceScene(room))
-    cam = rb.PerspectiveCamera(C2["eye"], C2["lookat"], C2["up"], (96, 54), C2["fov"])
-    p = PathIntegratorParams(spp=8, seed=5, spp_per_wave=3, max_depth=6)
-    ref = it.render_pt(cam, p).clone()
-    for bits in (3, 4):
-        it.set_reorder(bits)
-        assert cuda.equal(it.render_pt(cam, p), ref), bits
-    assert tr.status() == 0
-    for bad in (1, 5):
-        with pytest.raises(rb.Rb2Error, match="reorder"):
-            it.set_reorder(bad)
-    it.set_reorder(0)
-    assert cuda.equal(it.render_pt(cam, p), ref)
-
-
 def _bdpt_setup(rb, orc, W=96, H=54, step=3, n_iter=2048, n_light=2048):
     from renderbox2_b200.configs import CONFIG2 as C2
     room = _room(rb)
