@@ -53,9 +53,14 @@ def log(*a):
 
 
 # ----------------------------------------------------------------------------- workload
-def build_workload(n_scenes: int, rays_per_scene: int, seed_base: int = 4):
+def build_workload(n_scenes: int, rays_per_scene: int, seed_base: int = 4, tri_cost: float | None = None):
+    """The batching workload's scenes (config 4), built with the benchmark SAH
+    costs (configs.BUILD; `tri_cost` overrides the triangle cost)."""
     import renderbox2_b200 as rb
-    from renderbox2_b200.configs import CONFIG4, config4_triangle_counts
+    from renderbox2_b200.accel import Platform
+    from renderbox2_b200.configs import BUILD, CONFIG4, config4_triangle_counts
+    platform = Platform(sah_node_cost=BUILD["sah_node_cost"],
+                        sah_triangle_cost=BUILD["sah_triangle_cost"] if tri_cost is None else tri_cost)
     counts = config4_triangle_counts(dict(CONFIG4, n_scenes=64))[:n_scenes]
     scenes = []
     t0 = time.time()
@@ -63,7 +68,7 @@ def build_workload(n_scenes: int, rays_per_scene: int, seed_base: int = 4):
     for k, tris in enumerate(counts):
         sc = rb.heightfield_for_triangles(seed=seed_base * 1000 + k, n_tris=tris)
         tb = time.time()
-        bvh = rb.BVH(sc)
+        bvh = rb.BVH(sc, platform=platform)
         build_s += time.time() - tb
         rays, flags = rb.surface_rays(sc, seed=seed_base * 1000 + 500 + k, n=rays_per_scene,
                                       offset_scale=CONFIG4["offset_scale"],
@@ -213,12 +218,16 @@ L2_BYTES = 126 * 1024 * 1024
 # enough for the profiler: the first 8 scenes of this workload (its triangle
 # counts and seeds, 524,288 rays each, 7,023.9 MB of algorithmic bytes), block
 # 256.  Keyed by (node order, ray reordering on): the compressed 8-wide kernel
-# at 64 registers on rays in their own order; the binary BFS kernel at 48
-# registers on rays reordered at 5 bits per axis.
+# at 64 registers on rays in their own order (reference SAH costs); the binary
+# BFS kernel at 48 registers on rays reordered at 5 bits per axis (reference
+# costs); the compressed kernel at 64 registers on rays reordered at 4 bits
+# per axis (benchmark costs, 6,944.2 MB algorithmic).
 DRAM_PER_ALG_BYTE = {
     (3, False): (403.0e6 / 7023.9e6, "first 8 scenes of this workload, 4.19M rays, compressed 8-wide layout"),
     (1, True): (595.1e6 / 7023.9e6, "first 8 scenes of this workload, 4.19M rays, binary BFS layout, rays "
                                     "reordered"),
+    (3, True): (423.9e6 / 6944.2e6, "first 8 scenes of this workload, 4.19M rays, compressed 8-wide layout, "
+                                    "rays reordered"),
 }
 
 
@@ -252,7 +261,7 @@ def run_rb2(args, rank, world, local_rank):
     import renderbox2_b200 as rb
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    scenes, build_s = build_workload(args.scenes, args.rays_per_scene)
+    scenes, build_s = build_workload(args.scenes, args.rays_per_scene, tri_cost=args.sah_triangle_cost)
     total_rays = sum(s["rays"].shape[0] for s in scenes)
     n_ch_total = sum(s["n_ch"] for s in scenes)
     tracers, d_rays, d_hits, d_occ = [], [], [], []
@@ -521,6 +530,10 @@ def run_rb2(args, rank, world, local_rank):
             "autotuned": tuned, "scenes": len(scenes), "triangles": int(sum(s["tris"] for s in scenes)),
             "rays_per_step": int(total_rays), "l2": "flushed (256 MB write) between timed steps",
             "bvh_device_bytes": int(bvh_bytes), "build_s_host": round(build_s, 2), "parallelism": "replicas",
+            "bvh_build": {"sah_node_cost": _load_configs().BUILD["sah_node_cost"],
+                          "sah_triangle_cost": (args.sah_triangle_cost if args.sah_triangle_cost is not None
+                                                else _load_configs().BUILD["sah_triangle_cost"]),
+                          "note": "this library's SBVH builder; the reference's Platform costs are 1 and 1"},
         },
         "parity": parity,
         "plain_launches_mrays": round(plain_value, 2),
@@ -987,7 +1000,7 @@ def run_profile(args, local_rank):
             scenes.append(dict(scene=sc, bvh=rb.BVH(sc), rays=rays, n_ch=args.rays_per_scene // 2,
                                tris=sc.num_triangles))
     else:
-        scenes, _ = build_workload(args.scenes, args.rays_per_scene)
+        scenes, _ = build_workload(args.scenes, args.rays_per_scene, tri_cost=args.sah_triangle_cost)
     keep, jobs = [], []
     for s in scenes:
         tr = rb.CudaTracer(s["bvh"])
@@ -1083,6 +1096,9 @@ def main():
     ap.add_argument("--profile-ctas", type=int, default=0)
     ap.add_argument("--profile-chunk", type=int, default=1)
     ap.add_argument("--profile-reorder", type=int, default=0, help="profile: ray reordering bits per axis (0 off)")
+    ap.add_argument("--sah-triangle-cost", type=float, default=None,
+                    help="trace/profile: SAH triangle cost of the workload's builds (default: configs.BUILD; the "
+                         "reference's is 1)")
     ap.add_argument("--batch-config", default="",
                     help="trace: a JSON rb2_batch_config for the batched launch instead of the autotuner's pick "
                          "(for repeatable profiles)")

@@ -28,7 +28,8 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
     integrator (primary rays only, primitive-id shading).
     `keep` (optional dict) receives the scene, BVH and config used.  The
     traversal layout is `node_order`, or (None) the faster of the binary BFS
-    and the compressed 8-wide layout on one timed frame each."""
+    and the compressed 8-wide layout on one timed frame each.  The BVH is
+    built with the benchmark SAH costs (configs.BUILD)."""
     import torch
 
     import renderbox2_b200 as rb
@@ -45,7 +46,9 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
         scene = rb.RoomScene(seed=c["seed"], n_boxes=c["n_boxes"], n_spheres=c["n_spheres"],
                              sphere_subdiv=c["sphere_subdiv"], rmin=c["rmin"], rmax=c["rmax"],
                              n_lights=c["n_lights"], emission=c["emission"], room_size=c["room_size"])
-    bvh = rb.BVH(scene)
+    from renderbox2_b200.accel import Platform
+    bvh = rb.BVH(scene, platform=Platform(sah_node_cost=configs.BUILD["sah_node_cost"],
+                                          sah_triangle_cost=configs.BUILD["sah_triangle_cost"]))
     build_s = time.time() - t0
     tracer = rb.CudaTracer(bvh)
     it = Integrator(tracer, DeviceScene(scene))
@@ -103,6 +106,7 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
     return {"workload": kind, "triangles": scene.num_triangles, "width": c["width"], "height": c["height"],
             "samples": int(samples), "ms": round(ms, 3), "samples_per_s": round(samples / (ms / 1e3), 1),
             "mrays_per_s": round(rays / (ms / 1e3) / 1e6, 2), "rays": int(rays), "build_s": round(build_s, 2),
+            "sah_triangle_cost": configs.BUILD["sah_triangle_cost"],
             "stats": st, "image_mean": float(out.float().mean().item()),
             "node_order": {0: "dfs", 1: "bfs", 2: "wide4", 3: "cw8"}[tracer.node_order()],
             "layout_probe_ms": {str(k): round(v, 3) for k, v in probe.items()}}
