@@ -2,13 +2,15 @@
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl rb2|reference]
                   [--rays-per-scene R] [--scenes S]
-                  [--workload trace|ao|pt|bdpt|raycast|profile]
+                  [--workload trace|ao|pt|bdpt|raycast|profile|serve-curve]
 
 One step = every scene's ray batch traced once: 64 heightfield scenes with
-log-uniform 1k..2M triangles, 1M incoherent diffuse-bounce rays per scene,
-50 % closest-hit and 50 % any-hit (occlusion).  Inputs are resident in HBM
-when the timed region starts; L2 is flushed (256 MB write) between timed
-steps.  `e2e` repeats the step through the host-buffer C-ABI call
+log-uniform 1k..2M triangles (built with the benchmark SAH costs,
+configs.BUILD), 1M incoherent diffuse-bounce rays per scene, 50 % closest-hit
+and 50 % any-hit (occlusion), in one batched launch whose configuration the
+autotuner picks (node layout, launch shape, ray reordering; the reordering
+sort runs inside the step).  Inputs are resident in HBM when the timed region
+starts; L2 is flushed (256 MB write) between timed steps.  `e2e` repeats the step through the host-buffer C-ABI call
 (rb2_trace_host_jobs: pinned host rays in, hits / occlusion bytes out, the
 copies pipelined with traversal over several streams), copies included.
 After timing, 4096 rays per scene and mode of the timed launch's outputs
@@ -26,7 +28,10 @@ reference has no host traversal) traces each scene's full ray batch.  That
 process loads no part of this library.
 
 --workload profile runs one batched launch configuration over a small case
-repeatedly (for ncu captures; see --profile-* options).
+repeatedly (for ncu captures; see --profile-* options); --batch-config fixes
+the headline's batch configuration instead of autotuning it (for repeatable
+launch lists); --workload serve-curve measures config-5 latency against
+offered load.
 """
 from __future__ import annotations
 
