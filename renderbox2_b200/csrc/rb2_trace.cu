@@ -680,6 +680,19 @@ cudaError_t grow(T** p, uint64_t& cap, uint64_t n)
     return e;
 }
 
+// Whether the sort's counters at `bits` per axis stay proportionate to the
+// batch: (tiles + jobs) x buckets counters, at most two per ray plus 16M.  A
+// batch of many tiny jobs would need far more counters than it has rays (and
+// gains nothing from sorting a few rays per job).
+bool reorder_fits(const rb2_batch* b, uint32_t bits)
+{
+    const uint64_t per = rb2::reorder_tile_rays(b->total, b->occ.sms);
+    uint64_t tiles = 0;
+    for (const rb2_trace_job& j : b->jobs) tiles += (j.n + per - 1) / per;
+    const uint64_t counters = (tiles + b->jobs.size()) * (uint64_t)rb2::reorder_max_buckets(bits);
+    return counters <= 2 * b->total + (16ull << 20);
+}
+
 // Buffers of ray reordering at `bits` per axis: each job's scene box (the union
 // of the root's child boxes) as lo and 1 / extent, the tile table, counters,
 // totals, scan scratch, keys, pairs (two-pass widths) and the visiting order.
@@ -689,6 +702,10 @@ int batch_prepare_reorder(rb2_batch* b, uint32_t bits)
     if (bits < rb2::kReorderMinBits || bits > rb2::kReorderMaxBits)
         return fail(RB2_EINVAL, "reorder must be 0 or 3..6 bits per axis");
     if (b->total >= 0xFFFFFFFFull) return fail(RB2_EINVAL, "ray reordering needs fewer than 2^32 rays per batch");
+    if (!reorder_fits(b, bits))
+        return fail(RB2_ENOTSUP, "ray reordering at " + std::to_string(bits) +
+                                     " bits per axis needs more bucket counters than this batch has rays "
+                                     "(many small jobs); use fewer bits or none");
     const uint32_t n = (uint32_t)b->jobs.size();
     RB2_CUDA(rb2::reorder_init(), "reordering shared memory");
     cudaError_t e = cudaSuccess;
@@ -922,7 +939,12 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     if (!b) return fail(RB2_EINVAL, "null argument");
     cudaStream_t s = (cudaStream_t)stream;
     if (reps == 0) reps = 3;
-    cudaEvent_t e0, e1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    struct EventFree {
+        cudaEvent_t* a;
+        cudaEvent_t* b;
+        ~EventFree() { if (*a) cudaEventDestroy(*a); if (*b) cudaEventDestroy(*b); }
+    } event_guard{&e0, &e1};
     RB2_CUDA(cudaEventCreate(&e0), "event");
     RB2_CUDA(cudaEventCreate(&e1), "event");
     // Each timed launch starts with a cold L2 (a write of twice its size,
@@ -1034,11 +1056,13 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     double best_ms = 0, best_r_ms = 0;
     int rc = search(0, best, best_ms);
     if (rc) return rc;
-    // Ray reordering (when the batch's rays fit its 32-bit visiting order):
-    // the search again with 4 bits per axis, then the other widths on its winner.
-    if (b->total < 0xFFFFFFFFull) {
+    // Ray reordering (when the batch's rays fit its 32-bit visiting order and
+    // its sort counters stay proportionate): the search again with 4 bits per
+    // axis, then the other widths on its winner.
+    if (b->total < 0xFFFFFFFFull && reorder_fits(b, 4)) {
         if ((rc = search(4, best_r, best_r_ms))) return rc;
         for (uint32_t bits : {3u, 5u, 6u}) {
+            if (!reorder_fits(b, bits)) continue;
             rb2_batch_config c = best_r; c.reorder = bits; double ms;
             if ((rc = time_cfg(c, ms))) return rc;
             if (ms < best_r_ms) { best_r = c; best_r_ms = ms; }
@@ -1049,8 +1073,6 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
         best_ms = ms0;
         if (best_r_ms < best_ms) { best = best_r; best_ms = best_r_ms; }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     rc = rb2_batch_set_config(b, &best);
     if (rc) return rc;
     if (best_out) *best_out = best;

@@ -291,3 +291,31 @@ def test_ray_reordering_keeps_every_ray(rb, orc, cuda):
     got = out_m.cpu().numpy()[act]
     assert np.array_equal(got[:, 0], want["prim"])
     assert np.array_equal(got[:, 1].view(np.uint32), want["t"].view(np.uint32))
+
+
+def test_ray_reordering_refused_for_many_tiny_jobs(rb, cuda):
+    """A batch of 3,000 jobs of 5 rays each would need far more sort counters
+    than it has rays: every reordering width is refused with a clear error,
+    the autotuner leaves reordering off, and the launch still equals the
+    plain trace."""
+    sc = rb.heightfield_for_triangles(seed=77, n_tris=2_000)
+    tr = rb.CudaTracer(rb.BVH(sc))
+    r, _ = rb.surface_rays(sc, seed=78, n=15_000)
+    d = cuda.from_numpy(r).cuda()
+    out = cuda.full((r.shape[0], 4), 7, dtype=cuda.int32, device="cuda")
+    jobs = [(tr, d[5 * k: 5 * k + 5], rb.MODE_CLOSEST, out[5 * k: 5 * k + 5], None) for k in range(3000)]
+    batch = rb.TraceBatch(jobs)
+    for bits in (3, 4, 5, 6):
+        with pytest.raises(rb.Rb2Error, match="reordering"):
+            batch.set_config(reorder=bits)
+    best, ms = batch.autotune(reps=1)
+    assert best["reorder"] == 0 and ms > 0
+    out.fill_(7)
+    batch.launch()
+    cuda.cuda.synchronize()
+    ref = tr.trace(d)
+    if best["node_order"] in (2, 3):
+        assert cuda.equal(out[:, 0] >= 0, ref[:, 0] >= 0)
+    else:
+        assert cuda.equal(out, ref)
+    assert batch.status() == 0
