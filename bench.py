@@ -518,7 +518,8 @@ def run_rb2(args, rank, world, local_rank):
     integrators = {}
     if args.integrators:
         for kind in ("ao", "pt", "bdpt"):
-            integrators[kind] = integrator_summary(kind, l2_gbs, hbm_peak, with_cpu=(rank == 0 and world == 1))
+            integrators[kind] = integrator_summary(kind, l2_gbs, hbm_peak, with_cpu=(rank == 0 and world == 1),
+                                                   tri_cost=args.sah_triangle_cost)
 
     value = batch_rate / 1e6
     plain_value = plain_rate / 1e6
@@ -606,14 +607,14 @@ def run_rb2(args, rank, world, local_rank):
         sys.exit(3)
 
 
-def integrator_summary(kind, l2_gbs, hbm_gbs, with_cpu=True):
+def integrator_summary(kind, l2_gbs, hbm_gbs, with_cpu=True, tri_cost=None):
     """One full-size frame of config 1 (AO), 2 (PT) or 3 (BDPT): frame time,
     samples/s, Mrays/s, the trace stage's roofline (against the measured L2
     copy bandwidth when the binary BVH fits the 126 MB L2, else HBM) and the
     FP64 CPU integrator on a small sample of the same frame."""
     from renderbox2_b200.workloads import integrator
     keep = {}
-    r = integrator(kind, keep=keep)
+    r = integrator(kind, keep=keep, tri_cost=tri_cost)
     c = keep["bvh"].counts()
     bvh_bytes = int(c.n_nodes_u4 * 16 + c.n_woop_u4 * 16 + c.n_triidx * 4)
     out = {"ms_per_frame": r["ms"], "samples_per_s": r["samples_per_s"], "mrays_per_s": r["mrays_per_s"],
@@ -637,7 +638,7 @@ def run_workload(args, rank, local_rank):
     from renderbox2_b200.workloads import integrator
     torch.cuda.set_device(local_rank)
     keep = {}
-    r = integrator(args.workload, keep=keep)
+    r = integrator(args.workload, keep=keep, tri_cost=args.sah_triangle_cost)
     if rank == 0:
         names = {"ao": "config 1: ambient occlusion", "pt": "config 2: wavefront path tracing",
                  "bdpt": "config 3: BDPT with light-vertex cache",
@@ -1102,7 +1103,7 @@ def main():
     ap.add_argument("--profile-chunk", type=int, default=1)
     ap.add_argument("--profile-reorder", type=int, default=0, help="profile: ray reordering bits per axis (0 off)")
     ap.add_argument("--sah-triangle-cost", type=float, default=None,
-                    help="trace/profile: SAH triangle cost of the workload's builds (default: configs.BUILD; the "
+                    help="SAH triangle cost of the workloads' builds (configs 1-4; default: configs.BUILD; the "
                          "reference's is 1)")
     ap.add_argument("--batch-config", default="",
                     help="trace: a JSON rb2_batch_config for the batched launch instead of the autotuner's pick "

@@ -22,14 +22,16 @@ def _event_ms(fn, stream, reps=1):
     return e0.elapsed_time(e1) / reps
 
 
-def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order: int | None = None):
+def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order: int | None = None,
+               tri_cost: float | None = None):
     """Config 1 (AO), 2 (PT) or 3 (BDPT) at full size: samples/s and Mrays/s.
     "raycast": the config-2 scene, camera and spp through the ray-cast
     integrator (primary rays only, primitive-id shading).
     `keep` (optional dict) receives the scene, BVH and config used.  The
     traversal layout is `node_order`, or (None) the faster of the binary BFS
     and the compressed 8-wide layout on one timed frame each.  The BVH is
-    built with the benchmark SAH costs (configs.BUILD)."""
+    built with the benchmark SAH costs (configs.BUILD; `tri_cost` overrides
+    the triangle cost)."""
     import torch
 
     import renderbox2_b200 as rb
@@ -47,8 +49,8 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
                              sphere_subdiv=c["sphere_subdiv"], rmin=c["rmin"], rmax=c["rmax"],
                              n_lights=c["n_lights"], emission=c["emission"], room_size=c["room_size"])
     from renderbox2_b200.accel import Platform
-    bvh = rb.BVH(scene, platform=Platform(sah_node_cost=configs.BUILD["sah_node_cost"],
-                                          sah_triangle_cost=configs.BUILD["sah_triangle_cost"]))
+    tri_cost = configs.BUILD["sah_triangle_cost"] if tri_cost is None else tri_cost
+    bvh = rb.BVH(scene, platform=Platform(sah_node_cost=configs.BUILD["sah_node_cost"], sah_triangle_cost=tri_cost))
     build_s = time.time() - t0
     tracer = rb.CudaTracer(bvh)
     it = Integrator(tracer, DeviceScene(scene))
@@ -106,7 +108,7 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
     return {"workload": kind, "triangles": scene.num_triangles, "width": c["width"], "height": c["height"],
             "samples": int(samples), "ms": round(ms, 3), "samples_per_s": round(samples / (ms / 1e3), 1),
             "mrays_per_s": round(rays / (ms / 1e3) / 1e6, 2), "rays": int(rays), "build_s": round(build_s, 2),
-            "sah_triangle_cost": configs.BUILD["sah_triangle_cost"],
+            "sah_triangle_cost": tri_cost,
             "stats": st, "image_mean": float(out.float().mean().item()),
             "node_order": {0: "dfs", 1: "bfs", 2: "wide4", 3: "cw8"}[tracer.node_order()],
             "layout_probe_ms": {str(k): round(v, 3) for k, v in probe.items()}}
