@@ -59,10 +59,11 @@ __device__ __forceinline__ uint32_t digit_of(uint32_t key, uint32_t k)
     else return key >> low_bits(k);
 }
 
-// Adds one to counter[digit] for every valid lane and returns each lane's
-// previous value plus its rank among the warp's lanes of the same digit (the
-// full warp calls this together).  Small histograms aggregate equal digits in
-// the warp first, so one lane per digit touches shared memory.
+// Adds one to counter[digit] for every valid lane and returns a distinct
+// previous value to each (the full warp calls this together; invalid lanes
+// get an unused value).  Small histograms aggregate equal digits in the warp
+// first: one lane per digit adds the group's size, and each lane takes the
+// group's base plus its rank among the group's lanes, in lane order.
 __device__ __forceinline__ uint32_t take(uint32_t* counter, uint32_t digit, bool valid, bool aggregate)
 {
     if (!aggregate) return valid ? atomicAdd(&counter[digit], 1u) : 0u;
