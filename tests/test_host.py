@@ -89,6 +89,26 @@ def test_builder_deterministic_across_thread_counts(rb):
     assert np.array_equal(b1.get_tri_woop_buffer(), b8.get_tri_woop_buffer())
 
 
+def test_benchmark_build_costs_make_smaller_leaves_with_the_same_hits(rb, orc):
+    """The benchmark workloads build with SAH triangle cost 2
+    (configs.BUILD) instead of the reference's 1: leaves hold fewer triangle
+    references, the tree stays valid, and the closest hit distance of every
+    ray equals the exhaustive search's on both trees."""
+    from renderbox2_b200.configs import BUILD
+    s = rb.heightfield_for_triangles(seed=31, n_tris=20_000, n_boxes=16)
+    ref = rb.BVH(s)
+    gpu = rb.BVH(s, platform=rb.Platform(sah_node_cost=BUILD["sah_node_cost"],
+                                          sah_triangle_cost=BUILD["sah_triangle_cost"]))
+    assert BUILD["sah_triangle_cost"] > 1.0
+    per_leaf = [b.stats()["n_tri_refs"] / b.stats()["n_leaves"] for b in (ref, gpu)]
+    assert per_leaf[1] < per_leaf[0], per_leaf
+    rays, _ = rb.surface_rays(s, seed=32, n=20_000)
+    for b in (ref, gpu):
+        h = orc.trace(b.get_node_buffer(), b.get_tri_woop_buffer(), b.get_tri_index_buffer(), rays)
+        bf = orc.bruteforce(b.get_tri_woop_buffer(), b.get_tri_index_buffer(), rays)
+        assert np.array_equal(h["t"].view(np.uint32), bf["t"].view(np.uint32))
+
+
 def test_spatial_splits_duplicate_long_triangles(rb, orc):
     # Long thin diagonal triangles overlap heavily: the SBVH should split some.
     rng = np.random.Generator(np.random.PCG64(3))
