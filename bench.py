@@ -809,6 +809,17 @@ def cpu_baseline_run(scenes, budget_s: float, ref_max_tris: int, ref_budget_tris
     out = {"value": round(n / dt / 1e6, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
            "sample": f"{per} closest-hit + {per} any-hit rays from each of {len(scenes)} scenes "
                      f"({n:,} rays, {dt:.1f}s), oracle C restatement, OpenMP over {cores} threads"}
+    if budget_s > 0:
+        # One thread on a sample sized to about a tenth of the budget (assuming
+        # the all-core rate divides evenly over the cores).
+        per1 = int(n / dt / cores * budget_s / 10 / (2 * len(scenes)))
+        per1 = max(64, min(per1, per))
+        t0 = time.perf_counter()
+        n1 = trace_sample(oracle, scenes, per1, nthreads=1)
+        dt1 = time.perf_counter() - t0
+        out["single_thread"] = {"value": round(n1 / dt1 / 1e6, 3), "unit": "Mrays/s",
+                                "sample": f"{per1} closest-hit + {per1} any-hit rays from each scene ({n1:,} rays, "
+                                          f"{dt1:.1f}s), one thread"}
     sub = reference_subset([s["tris"] for s in scenes], ref_max_tris, ref_budget_tris)
     if sub and budget_s > 0:
         t0 = time.perf_counter()
@@ -853,14 +864,16 @@ def build_baseline(scenes, budget_tris: int = 30_000):
     return out
 
 
-def trace_sample(oracle, scenes, per):
+def trace_sample(oracle, scenes, per, nthreads: int = 0):
+    """The oracle over `per` closest-hit and `per` any-hit rays of each scene
+    (nthreads 0: all host threads); returns the rays traced."""
     n = 0
     for s in scenes:
         nodes, woop, tri = s["bvh"].buffers_view()
         ch = s["rays"][: min(per, s["n_ch"])]
         ah = s["rays"][s["n_ch"]: s["n_ch"] + per]
-        oracle.trace(nodes, woop, tri, ch, any_hit=False)
-        oracle.trace(nodes, woop, tri, ah, any_hit=True)
+        oracle.trace(nodes, woop, tri, ch, any_hit=False, nthreads=nthreads)
+        oracle.trace(nodes, woop, tri, ah, any_hit=True, nthreads=nthreads)
         n += ch.shape[0] + ah.shape[0]
     return n
 
