@@ -785,6 +785,17 @@ def integrator_roofline(kind, r, counts, peak, peak_src):
             "bytes_per_ray": {t: round(bpr(t), 1) for t in gpu}}
 
 
+def host_cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the CPU legs' records."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline_run(scenes, budget_s: float, ref_max_tris: int, ref_budget_tris: int):
     """Oracle traversal on all host cores over a bounded sample: equal share of
     each scene's closest-hit and any-hit rays, sized to ~budget_s seconds.
@@ -807,6 +818,7 @@ def cpu_baseline_run(scenes, budget_s: float, ref_max_tris: int, ref_budget_tris
     n = trace_sample(oracle, scenes, per)
     dt = time.perf_counter() - t0
     out = {"value": round(n / dt / 1e6, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
+           "cpu": host_cpu_model(),
            "sample": f"{per} closest-hit + {per} any-hit rays from each of {len(scenes)} scenes "
                      f"({n:,} rays, {dt:.1f}s), oracle C restatement, OpenMP over {cores} threads"}
     if budget_s > 0:
@@ -989,7 +1001,7 @@ def run_reference(args, rank, world):
                                "reference builder builds within the run", "parallelism": "host cores",
                    "scenes": len(scenes), "triangles": tris, "rays_per_step": n},
         "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": cores, "kind": "reference",
-                         "sample": sample},
+                         "cpu": host_cpu_model(), "sample": sample},
         "build": {"reference_sbvh_wall_s": round(build_wall, 2), "reference_sbvh_cpu_s": round(build_cpu, 2),
                   "processes": cores, "triangles": tris},
         "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
