@@ -510,13 +510,16 @@ def run_rb2(args, rank, world, local_rank):
     serving = None
     del batch
     batch = None
-    if args.serve_jobs > 0:
+    # Serving and configs 1-3 are one-GPU measurements: under torchrun only
+    # rank 0 runs them (its line reports them), so N ranks do not pin N times
+    # the serving buffers on the host.
+    if args.serve_jobs > 0 and rank == 0:
         from renderbox2_b200.workloads import serving as serving_run
         serving = serving_run(n_jobs=args.serve_jobs, slots=args.serve_slots)
 
     # ---- configs 1-3: one frame each at full size (trace-stage roofline vs L2 or HBM).
     integrators = {}
-    if args.integrators:
+    if args.integrators and rank == 0:
         for kind in ("ao", "pt", "bdpt"):
             integrators[kind] = integrator_summary(kind, l2_gbs, hbm_peak, with_cpu=(rank == 0 and world == 1),
                                                    tri_cost=args.sah_triangle_cost)
