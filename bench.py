@@ -58,11 +58,13 @@ def log(*a):
 
 
 # ----------------------------------------------------------------------------- workload
-def build_workload(n_scenes: int, rays_per_scene: int, seed_base: int = 4, tri_cost: float | None = None):
+def build_workload(n_scenes: int, rays_per_scene: int, seed_base: int = 4, tri_cost: float | None = None,
+                   threads: int = 0):
     """The batching workload's scenes (config 4), built with the benchmark SAH
-    costs (configs.BUILD; `tri_cost` overrides the triangle cost)."""
+    costs (configs.BUILD; `tri_cost` overrides the triangle cost) on `threads`
+    host threads (0: all)."""
     import renderbox2_b200 as rb
-    from renderbox2_b200.accel import Platform
+    from renderbox2_b200.accel import BuildParams, Platform
     from renderbox2_b200.configs import BUILD, CONFIG4, config4_triangle_counts
     platform = Platform(sah_node_cost=BUILD["sah_node_cost"],
                         sah_triangle_cost=BUILD["sah_triangle_cost"] if tri_cost is None else tri_cost)
@@ -73,7 +75,7 @@ def build_workload(n_scenes: int, rays_per_scene: int, seed_base: int = 4, tri_c
     for k, tris in enumerate(counts):
         sc = rb.heightfield_for_triangles(seed=seed_base * 1000 + k, n_tris=tris)
         tb = time.time()
-        bvh = rb.BVH(sc, platform=platform)
+        bvh = rb.BVH(sc, platform=platform, params=BuildParams(num_threads=threads))
         build_s += time.time() - tb
         rays, flags = rb.surface_rays(sc, seed=seed_base * 1000 + 500 + k, n=rays_per_scene,
                                       offset_scale=CONFIG4["offset_scale"],
@@ -266,7 +268,10 @@ def run_rb2(args, rank, world, local_rank):
     import renderbox2_b200 as rb
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    scenes, build_s = build_workload(args.scenes, args.rays_per_scene, tri_cost=args.sah_triangle_cost)
+    # Ranks on one host share its cores for the builds.
+    threads = max(1, (os.cpu_count() or 1) // world) if world > 1 else 0
+    scenes, build_s = build_workload(args.scenes, args.rays_per_scene, tri_cost=args.sah_triangle_cost,
+                                     threads=threads)
     total_rays = sum(s["rays"].shape[0] for s in scenes)
     n_ch_total = sum(s["n_ch"] for s in scenes)
     tracers, d_rays, d_hits, d_occ = [], [], [], []
