@@ -218,19 +218,19 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- GPU arm
-L2_BYTES = 126 * 1024 * 1024
-
 # DRAM bytes per algorithmic byte of the batched traversal kernel, from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on a case small
 # enough for the profiler: the first 8 scenes of this workload (its triangle
 # counts and seeds, 524,288 rays each, 7,023.9 MB of algorithmic bytes), block
 # 256.  Keyed by (node order, ray reordering on): the compressed 8-wide kernel
-# at 64 registers on rays in their own order (reference SAH costs); the binary
-# BFS kernel at 48 registers on rays reordered at 5 bits per axis (reference
-# costs); the compressed kernel at 64 registers on rays reordered at 4 bits
-# per axis (benchmark costs, 6,944.2 MB algorithmic).
+# at 64 registers on rays in their own order with node-phase threshold 12
+# (benchmark SAH costs, 6,944.2 MB algorithmic); the binary BFS kernel at 48
+# registers on rays reordered at 5 bits per axis (reference costs, node-phase
+# threshold 1); the compressed kernel at 64 registers on rays reordered at 4
+# bits per axis (benchmark costs, node-phase threshold 1).
 DRAM_PER_ALG_BYTE = {
-    (3, False): (403.0e6 / 7023.9e6, "first 8 scenes of this workload, 4.19M rays, compressed 8-wide layout"),
+    (3, False): (392.0e6 / 6944.2e6, "first 8 scenes of this workload, 4.19M rays, compressed 8-wide layout, "
+                                     "node-phase threshold 12"),
     (1, True): (595.1e6 / 7023.9e6, "first 8 scenes of this workload, 4.19M rays, binary BFS layout, rays "
                                     "reordered"),
     (3, True): (423.9e6 / 6944.2e6, "first 8 scenes of this workload, 4.19M rays, compressed 8-wide layout, "
@@ -526,7 +526,7 @@ def run_rb2(args, rank, world, local_rank):
     integrators = {}
     if args.integrators and rank == 0:
         for kind in ("ao", "pt", "bdpt"):
-            integrators[kind] = integrator_summary(kind, l2_gbs, hbm_peak, with_cpu=(rank == 0 and world == 1),
+            integrators[kind] = integrator_summary(kind, l2_gbs, with_cpu=(rank == 0 and world == 1),
                                                    tri_cost=args.sah_triangle_cost)
 
     value = batch_rate / 1e6
@@ -566,20 +566,24 @@ def run_rb2(args, rank, world, local_rank):
                       "layout and the default launch shape; same_layout = the autotuned layout and launch shape "
                       "(plain launches have no ray reordering; batched_without_reorder = the batched launch with "
                       "the tuned shape and reordering off)",
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved / hbm_peak, 4), "traffic": round(traffic),
+        "roofline": {"bound": "l2", "achieved": round(achieved, 1), "peak": round(l2_gbs, 1), "unit": "GB/s",
+                     "frac": round(achieved / l2_gbs, 4), "traffic": round(traffic),
                      "kernel": f"k_trace_jobs<BLOCK, REGS, LAYOUT> (batched, 1 launch/step, {layout_name} nodes)"
                                + (f"; the step time includes the {sort_launches} ray-reordering launches before it"
                                   if sort_launches else ""),
-                     "peak_source": peak_src,
+                     "peak_source": "L2 copy bandwidth measured in this run (a 32 MB buffer copied repeatedly, "
+                                    "CUDA events)",
+                     "bound_note": "DRAM serves about 6 % of the algorithmic bytes (traffic below; L1 and L2 hit "
+                                   "the rest), so the L2 is the memory level those bytes are bound by; the "
+                                   "kernel itself is issue-bound (ncu: ALU pipe and issue slots, not memory)",
+                     "hbm_peak": hbm_peak, "hbm_peak_source": peak_src,
+                     "alg_frac_of_hbm": round(achieved / hbm_peak, 4),
                      "alg_bytes_per_launch": round(alg_per_launch),
                      "alg_bytes_per_ray": round(alg_per_launch / total_rays, 1),
                      "traffic_source": f"ncu DRAM bytes per algorithmic byte of a capture ({ratio_src}) x this "
                                        "launch's algorithmic bytes",
                      "dram_gbs": round(traffic / launch_s / 1e9, 1),
                      "dram_frac": round(traffic / launch_s / 1e9 / hbm_peak, 4),
-                     "l2_copy_gbs": round(l2_gbs, 1),
-                     "alg_frac_of_l2": round(achieved / l2_gbs, 4),
                      "node_visits_per_s": round(node_visits / launch_s, 0),
                      "box_tests_per_s": round(2 * node_visits / launch_s, 0),
                      "tri_tests_per_s": round(tri_tests / launch_s, 0),
@@ -615,11 +619,11 @@ def run_rb2(args, rank, world, local_rank):
         sys.exit(3)
 
 
-def integrator_summary(kind, l2_gbs, hbm_gbs, with_cpu=True, tri_cost=None):
+def integrator_summary(kind, l2_gbs, with_cpu=True, tri_cost=None):
     """One full-size frame of config 1 (AO), 2 (PT) or 3 (BDPT): frame time,
-    samples/s, Mrays/s, the trace stage's roofline (against the measured L2
-    copy bandwidth when the binary BVH fits the 126 MB L2, else HBM) and the
-    FP64 CPU integrator on a small sample of the same frame."""
+    samples/s, Mrays/s, the trace stage's roofline (against the L2 copy
+    bandwidth measured in the run) and the FP64 CPU integrator on a small
+    sample of the same frame."""
     from renderbox2_b200.workloads import integrator
     keep = {}
     r = integrator(kind, keep=keep, tri_cost=tri_cost)
@@ -632,10 +636,7 @@ def integrator_summary(kind, l2_gbs, hbm_gbs, with_cpu=True, tri_cost=None):
     if with_cpu:
         out["cpu_baseline"] = base
     if counts is not None:
-        l2_resident = bvh_bytes <= L2_BYTES
-        roof = integrator_roofline(kind, r, counts, l2_gbs if l2_resident else hbm_gbs,
-                                   "measured L2 copy (binary BVH fits L2)" if l2_resident else "MEASURED_PEAKS hbm_gbs")
-        out["roofline"] = roof
+        out["roofline"] = integrator_roofline(kind, r, counts, l2_gbs, "L2 copy bandwidth measured in this run")
     return out
 
 
@@ -646,7 +647,7 @@ def run_workload(args, rank, local_rank):
     from renderbox2_b200.workloads import integrator
     torch.cuda.set_device(local_rank)
     keep = {}
-    r = integrator(args.workload, keep=keep, tri_cost=args.sah_triangle_cost)
+    r = integrator(args.workload, keep=keep, tri_cost=args.sah_triangle_cost, node_threshold=args.node_threshold)
     if rank == 0:
         names = {"ao": "config 1: ambient occlusion", "pt": "config 2: wavefront path tracing",
                  "bdpt": "config 3: BDPT with light-vertex cache",
@@ -657,15 +658,10 @@ def run_workload(args, rank, local_rank):
             if args.cpu_sample_s > 0:
                 line["cpu_baseline"] = base
             if counts is not None:
-                c = keep["bvh"].counts()
-                bvh_bytes = int(c.n_nodes_u4 * 16 + c.n_woop_u4 * 16 + c.n_triidx * 4)
-                if bvh_bytes <= L2_BYTES:
-                    import torch
-                    dev = torch.device("cuda", local_rank)
-                    peak, src = l2_copy_gbs(dev, torch.cuda.Stream(device=dev)), "measured L2 copy (binary BVH fits L2)"
-                else:
-                    peak, src = _hbm_peak()[0], "MEASURED_PEAKS hbm_gbs"
-                line["roofline"] = integrator_roofline(args.workload, r, counts, peak, src)
+                dev = torch.device("cuda", local_rank)
+                peak = l2_copy_gbs(dev, torch.cuda.Stream(device=dev))
+                line["roofline"] = integrator_roofline(args.workload, r, counts, peak,
+                                                       "L2 copy bandwidth measured in this run")
         print(json.dumps(line), flush=True)
 
 
@@ -762,8 +758,11 @@ def integrator_roofline(kind, r, counts, peak, peak_src):
     """Trace-stage roofline of configs 1-3: algorithmic bytes of the frame's
     rays (GPU ray counts per type x the oracle's mean bytes per ray of that
     type, from its own rays of the same distributions) / the GPU time of the
-    traversal launches (CUDA events around each), against `peak` (the
-    measured L2 copy bandwidth when the BVH fits L2, else HBM)."""
+    traversal launches (CUDA events around each), against `peak`: the L2
+    copy bandwidth measured in the run, since L1 and L2 serve nearly all of a
+    traversal's algorithmic bytes (ncu on the batching workload, whose BVHs
+    are 21x the L2: DRAM moves about 6 % of them); the fraction of HBM is
+    reported beside it."""
     out_b = {"camera": 16, "extension": 16, "light": 16, "shadow": 1, "connection": 1}
 
     def bpr(t):
@@ -787,8 +786,10 @@ def integrator_roofline(kind, r, counts, peak, peak_src):
     if trace_s <= 0:
         return None
     ach = alg / trace_s / 1e9
-    out = {"bound": "l2" if "L2" in peak_src else "hbm", "achieved": round(ach, 1), "peak": round(peak, 1),
+    hbm, _ = _hbm_peak()
+    out = {"bound": "l2", "achieved": round(ach, 1), "peak": round(peak, 1),
            "unit": "GB/s", "frac": round(ach / peak, 4), "peak_source": peak_src, "traffic": None,
+           "alg_frac_of_hbm": round(ach / hbm, 4),
            "alg_bytes_per_frame": round(alg), "trace_ms": round(st["trace_ms"], 3),
            "bytes_per_ray": {t: round(bpr(t), 1) for t in gpu}}
     if kind == "raycast":
@@ -1055,7 +1056,7 @@ def run_profile(args, local_rank):
     batch = rb.TraceBatch(jobs)
     batch.set_config(block_threads=args.profile_block, regs=args.profile_regs, node_order=args.profile_order,
                      fetch_threshold=args.profile_threshold, ctas_per_sm=args.profile_ctas, chunk=args.profile_chunk,
-                     reorder=args.profile_reorder)
+                     reorder=args.profile_reorder, node_threshold=args.profile_node_threshold)
     ms = []
     for _ in range(args.launches):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1136,12 +1137,15 @@ def main():
     ap.add_argument("--profile-regs", type=int, default=64)
     ap.add_argument("--profile-order", type=int, default=3)
     ap.add_argument("--profile-threshold", type=int, default=28)
+    ap.add_argument("--profile-node-threshold", type=int, default=0, help="profile: node-phase threshold (0: default)")
     ap.add_argument("--profile-ctas", type=int, default=0)
     ap.add_argument("--profile-chunk", type=int, default=1)
     ap.add_argument("--profile-reorder", type=int, default=0, help="profile: ray reordering bits per axis (0 off)")
     ap.add_argument("--sah-triangle-cost", type=float, default=None,
                     help="SAH triangle cost of the workloads' builds (configs 1-4; default: configs.BUILD; the "
                          "reference's is 1)")
+    ap.add_argument("--node-threshold", type=int, default=0,
+                    help="ao/pt/bdpt/raycast: the traversal's node-phase threshold (0: the layout's default)")
     ap.add_argument("--batch-config", default="",
                     help="trace: a JSON rb2_batch_config for the batched launch instead of the autotuner's pick "
                          "(for repeatable profiles)")

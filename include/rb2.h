@@ -121,6 +121,10 @@ typedef struct {
     uint32_t ctas_per_sm;       /* resident CTAs per SM (0 = occupancy maximum) */
     uint32_t fetch_threshold;   /* refill a warp when fewer lanes stay busy (reference: 20) */
     uint32_t regs;              /* register budget of the kernel variant: 64, 48 or 40 (0 = 64) */
+    uint32_t node_threshold;    /* end a warp's node phase, and test the triangles its lanes hold,
+                                   once fewer than this many lanes still traverse nodes (1..32;
+                                   1 = only when none does, the reference's while-while; 0 = the
+                                   layout's tuned default); results do not depend on it */
 } rb2_launch_config;
 
 /* Node layout of the bulk traversals: the reference's Compact2 buffer in its
@@ -253,7 +257,7 @@ typedef struct {
                                  Morton code of the origin within its scene's box), so a warp's rays
                                  start near each other and head the same way; records still go to
                                  each ray's own index, and every ray's result is unchanged */
-    uint32_t reserved;
+    uint32_t node_threshold;  /* as rb2_launch_config.node_threshold (0 = the layout's default) */
 } rb2_batch_config;
 
 typedef struct rb2_batch rb2_batch;

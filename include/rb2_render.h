@@ -170,10 +170,11 @@ int rb2_integrator_create(rb2_tracer* tracer, const rb2_scene_dev* scene, rb2_in
 int rb2_integrator_destroy(rb2_integrator* it);
 int rb2_integrator_device_bytes(const rb2_integrator* it, uint64_t* bytes);
 /* Launch shape of the integrator's persistent traversals: block_threads 128
- * or 256, regs 64 or 48, fetch_threshold (zero fields: 128, 24 and a register
- * budget of 48 for the binary layout, 64 for the compressed 8-wide layout,
- * the fastest shapes measured on configs 1-3; ctas_per_sm is ignored).
- * Images do not depend on the shape. */
+ * or 256, regs 64 or 48, fetch_threshold, node_threshold (zero fields: 128,
+ * 24, a register budget of 48 for the binary layout and 64 for the compressed
+ * 8-wide layout, a node-phase threshold of 8 for the binary layout and 16 for
+ * the compressed one: the fastest shapes measured on configs 1-3;
+ * ctas_per_sm is ignored).  Images do not depend on the shape. */
 int rb2_integrator_set_launch(rb2_integrator* it, const rb2_launch_config* cfg);
 /* Paths in flight per wave (0 = defaults: 32M paths for the path tracer,
  * 8M camera paths for BDPT).  The path tracer runs as many samples per pixel

@@ -38,7 +38,7 @@ class Cw8Counts(C.Structure):
 
 class LaunchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("ctas_per_sm", C.c_uint32),
-                ("fetch_threshold", C.c_uint32), ("regs", C.c_uint32)]
+                ("fetch_threshold", C.c_uint32), ("regs", C.c_uint32), ("node_threshold", C.c_uint32)]
 
 
 class TraceJob(C.Structure):
@@ -84,7 +84,7 @@ class Filter(C.Structure):
 class BatchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("fetch_threshold", C.c_uint32),
                 ("chunk", C.c_uint32), ("node_order", C.c_uint32), ("regs", C.c_uint32), ("reorder", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("node_threshold", C.c_uint32)]
 
 
 class AoParams(C.Structure):

@@ -236,10 +236,10 @@ class CudaTracer:
         check(lib().rb2_tracer_device_bytes(self._t, C.byref(v)))
         return v.value
 
-    def set_launch(self, ctas_per_sm=0, fetch_threshold=0, block_threads=0, regs=0):
+    def set_launch(self, ctas_per_sm=0, fetch_threshold=0, block_threads=0, regs=0, node_threshold=0):
         """Launch shape of this tracer's bulk traversals (rb2_launch_config;
         0 = the tuned default for each field)."""
-        cfg = LaunchConfig(block_threads, ctas_per_sm, fetch_threshold, regs)
+        cfg = LaunchConfig(block_threads, ctas_per_sm, fetch_threshold, regs, node_threshold)
         check(lib().rb2_tracer_set_launch(self._t, C.byref(cfg)))
 
     def set_node_order(self, order: int):
@@ -353,7 +353,7 @@ class TraceBatch:
         from ._native import BatchConfig
         c = BatchConfig()
         check(lib().rb2_batch_get_config(self._b, C.byref(c)))
-        return {k: getattr(c, k) for k, _ in BatchConfig._fields_ if k != "reserved"}
+        return {k: getattr(c, k) for k, _ in BatchConfig._fields_}
 
     def set_config(self, **kw):
         from ._native import BatchConfig
@@ -374,7 +374,7 @@ class TraceBatch:
         c = BatchConfig()
         ms = C.c_double()
         check(lib().rb2_batch_autotune(self._b, _stream_handle(stream), reps, C.byref(c), C.byref(ms)))
-        return {k: getattr(c, k) for k, _ in BatchConfig._fields_ if k != "reserved"}, ms.value
+        return {k: getattr(c, k) for k, _ in BatchConfig._fields_}, ms.value
 
     def status(self, stream=None) -> int:
         v = C.c_uint32()

@@ -84,11 +84,12 @@ struct IsectSource {
 // LAYOUT: binary Compact2 or compressed 8-wide nodes (the tracer's layout).
 template <int BLOCK, int LAYOUT>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
-    k_trace_isect(const __grid_constant__ IsectSource src, uint32_t fetch_threshold, unsigned int* status)
+    k_trace_isect(const __grid_constant__ IsectSource src, uint32_t fetch_threshold, uint32_t node_threshold,
+                  unsigned int* status)
 {
     IsectSource s = src;
-    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8(s, fetch_threshold, status);
-    else persistent_trace(s, fetch_threshold, status);
+    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8(s, fetch_threshold, node_threshold, status);
+    else persistent_trace(s, fetch_threshold, node_threshold, status);
 }
 
 __global__ void k_trace_per_thread(rb2_dev_bvh bvh, const float4* rays, const uint8_t* mask, uint32_t n, int any_hit,
@@ -172,7 +173,8 @@ int rb2_trace_isect(rb2_tracer* t, const rb2_scene_dev* scene, const float* d_ra
     RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0), "occupancy");
     uint64_t blocks = (uint64_t)sms * (uint64_t)std::max(1, per_sm);
     blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, ((uint64_t)n + 127) / 128));
-    kern<<<(unsigned)blocks, 128, 0, s>>>(src, 20u, bv.status);
+    kern<<<(unsigned)blocks, 128, 0, s>>>(
+        src, 20u, rb2dev::default_node_threshold(bv.cw8 ? rb2dev::kLayoutCw8 : rb2dev::kLayoutBinary), bv.status);
     RB2_CUDA(cudaGetLastError(), "isect launch");
     return RB2_OK;
 }

@@ -147,6 +147,7 @@ extern "C" int rb2_trace_batch_noalloc(const rb2_noalloc_job* jobs, uint32_t n_j
     a.start = reinterpret_cast<const unsigned long long*>(base + offsetof(NoAllocScratch, start));
     a.n_jobs = n_jobs;
     a.fetch_threshold = 20;
+    a.node_threshold = rb2dev::default_node_threshold(rb2dev::kLayoutBinary);
     a.chunk = 1;
     a.counter = reinterpret_cast<unsigned long long*>(base + offsetof(NoAllocScratch, counter));
     a.status = reinterpret_cast<unsigned int*>(base + offsetof(NoAllocScratch, status));

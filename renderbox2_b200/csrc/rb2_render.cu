@@ -139,10 +139,10 @@ struct AoSource {
 // SM, 48: 40 warps), binary Compact2 or compressed 8-wide layout.
 template <int BLOCK, int REGS, class Src, int LAYOUT>
 __global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK)
-    k_persistent(Src src, uint32_t fetch_threshold, unsigned int* status)
+    k_persistent(Src src, uint32_t fetch_threshold, uint32_t node_threshold, unsigned int* status)
 {
-    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8<Src, true>(src, fetch_threshold, status);
-    else persistent_trace(src, fetch_threshold, status);
+    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8<Src, true>(src, fetch_threshold, node_threshold, status);
+    else persistent_trace(src, fetch_threshold, node_threshold, status);
 }
 
 __global__ void k_ao_finalize(const int4* hits, const uint32_t* counts, uint32_t npix, uint32_t samples, float* out)
@@ -1491,8 +1491,8 @@ __global__ void k_pt_finalize(const float4* accum, uint32_t npix, float inv_spp,
 namespace {
 
 template <int B, int R, int LAYOUT, class Src>
-int launch_persistent_variant(const Src& src, uint64_t work, int sms, uint32_t threshold, unsigned int* status,
-                              cudaStream_t s)
+int launch_persistent_variant(const Src& src, uint64_t work, int sms, uint32_t threshold, uint32_t node_threshold,
+                              unsigned int* status, cudaStream_t s)
 {
     int per_sm = 0;
     RB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb2dev::k_persistent<B, R, Src, LAYOUT>, B, 0),
@@ -1500,7 +1500,7 @@ int launch_persistent_variant(const Src& src, uint64_t work, int sms, uint32_t t
     uint64_t blocks = (uint64_t)sms * (uint64_t)std::max(1, per_sm);
     blocks = std::min<uint64_t>(blocks, (work + B - 1) / B);
     blocks = std::max<uint64_t>(blocks, 1);
-    rb2dev::k_persistent<B, R, Src, LAYOUT><<<(unsigned)blocks, B, 0, s>>>(src, threshold, status);
+    rb2dev::k_persistent<B, R, Src, LAYOUT><<<(unsigned)blocks, B, 0, s>>>(src, threshold, node_threshold, status);
     RB2_CUDA(cudaGetLastError(), "persistent launch");
     return RB2_OK;
 }
@@ -1509,12 +1509,17 @@ template <int LAYOUT, class Src>
 int launch_persistent_shape(const Src& src, uint64_t work, const rb2_integrator* it, unsigned int* status, cudaStream_t s)
 {
     const uint32_t th = it->tr_threshold;
+    // Node-phase threshold: on the config-2/3 rooms 16 was the fastest for the
+    // compressed layout (path tracer 307.5 ms vs 309.2 at 12 and 366.3 at 1;
+    // BDPT 83.1 vs 86.5 and 104.3 ms); the binary layout keeps its default.
+    const uint32_t nt = it->tr_node_threshold ? it->tr_node_threshold
+                                              : (LAYOUT == rb2dev::kLayoutCw8 ? 16u : rb2dev::default_node_threshold(LAYOUT));
     const uint32_t regs = it->tr_regs ? it->tr_regs : (LAYOUT == rb2dev::kLayoutCw8 ? 64u : 48u);
     if (it->tr_block == 256)
-        return regs == 48 ? launch_persistent_variant<256, 48, LAYOUT>(src, work, it->sms, th, status, s)
-                                 : launch_persistent_variant<256, 64, LAYOUT>(src, work, it->sms, th, status, s);
-    return regs == 48 ? launch_persistent_variant<128, 48, LAYOUT>(src, work, it->sms, th, status, s)
-                             : launch_persistent_variant<128, 64, LAYOUT>(src, work, it->sms, th, status, s);
+        return regs == 48 ? launch_persistent_variant<256, 48, LAYOUT>(src, work, it->sms, th, nt, status, s)
+                                 : launch_persistent_variant<256, 64, LAYOUT>(src, work, it->sms, th, nt, status, s);
+    return regs == 48 ? launch_persistent_variant<128, 48, LAYOUT>(src, work, it->sms, th, nt, status, s)
+                             : launch_persistent_variant<128, 64, LAYOUT>(src, work, it->sms, th, nt, status, s);
 }
 
 template <class Src>
@@ -1735,9 +1740,11 @@ int rb2_integrator_set_launch(rb2_integrator* it, const rb2_launch_config* cfg)
         return fail(RB2_ENOTSUP, "integrator traversal block_threads must be 128 or 256");
     if (cfg->regs && cfg->regs != 64 && cfg->regs != 48) return fail(RB2_ENOTSUP, "integrator regs must be 64 or 48");
     if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
+    if (cfg->node_threshold > 32) return fail(RB2_EINVAL, "node_threshold must be <= 32");
     it->tr_block = cfg->block_threads ? cfg->block_threads : 128;
     it->tr_regs = cfg->regs;
     it->tr_threshold = cfg->fetch_threshold ? cfg->fetch_threshold : 24;
+    it->tr_node_threshold = cfg->node_threshold;
     return RB2_OK;
 }
 

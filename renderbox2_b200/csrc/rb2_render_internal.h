@@ -83,6 +83,7 @@ struct rb2_integrator {
     int sms = 0;
     // launch shape of the integrator's traversal kernels (rb2_integrator_set_launch)
     uint32_t tr_block = 128, tr_regs = 0, tr_threshold = 24;   // tr_regs 0: 48 binary, 64 compressed 8-wide
+    uint32_t tr_node_threshold = 0;                             // 0: the layout's default
     // paths in flight per wave (rb2_integrator_set_wave; 0: the defaults below)
     uint64_t wave_paths = 0;
     // traversal timing (rb2_integrator_set_timing): an event pair per launch

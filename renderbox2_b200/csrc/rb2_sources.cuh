@@ -34,7 +34,7 @@ struct KernelArgs {
     uint32_t n_jobs;
     uint32_t fetch_threshold;            // refill a warp when fewer lanes stay busy
     uint32_t chunk;                      // warp reserves chunk*32 slots per atomic (<= 1: exact)
-    uint32_t pad;
+    uint32_t node_threshold;             // end a node phase below this many lanes (persistent_trace*)
     unsigned long long* counter;         // queue head (zeroed before the launch)
     unsigned int* status;                // guard bits
     const uint32_t* perm;                // nullable: queue slot -> ray slot (ray reordering)
@@ -155,8 +155,8 @@ __global__ void __launch_bounds__(BLOCK, (65536 / REGS) / BLOCK) k_trace_jobs(co
     src.chunk = a.chunk;
     src.rem = s_rem;
     src.perm = a.perm;
-    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8<JobSource>(src, a.fetch_threshold, a.status);
-    else persistent_trace<JobSource, LAYOUT == kLayoutWide4>(src, a.fetch_threshold, a.status);
+    if constexpr (LAYOUT == kLayoutCw8) persistent_trace_cw8<JobSource>(src, a.fetch_threshold, a.node_threshold, a.status);
+    else persistent_trace<JobSource, LAYOUT == kLayoutWide4>(src, a.fetch_threshold, a.node_threshold, a.status);
 }
 
 }  // namespace rb2dev

@@ -333,6 +333,7 @@ int trace_single(rb2_tracer* t, const float* d_rays, uint64_t n, uint32_t mode, 
     }
     a.n_jobs = 1;
     a.fetch_threshold = t->cfg.fetch_threshold ? t->cfg.fetch_threshold : 20u;
+    a.node_threshold = t->cfg.node_threshold ? t->cfg.node_threshold : rb2dev::default_node_threshold(layout_of(order));
     a.chunk = 1;
     a.counter = counter;
     a.status = t->d_status;
@@ -459,6 +460,7 @@ int rb2_tracer_set_launch(rb2_tracer* t, const rb2_launch_config* cfg)
     if (cfg->block_threads && cfg->block_threads != 64 && cfg->block_threads != 128 && cfg->block_threads != 256)
         return fail(RB2_ENOTSUP, "block_threads must be 64, 128 or 256");
     if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
+    if (cfg->node_threshold > 32) return fail(RB2_EINVAL, "node_threshold must be <= 32");
     if (!valid_regs(cfg->regs)) return fail(RB2_ENOTSUP, "regs must be 64, 48 or 40");
     t->cfg = *cfg;
     return RB2_OK;
@@ -650,6 +652,8 @@ int batch_enqueue(rb2_batch* b, cudaStream_t s)
     a.start = b->d_start;
     a.n_jobs = (uint32_t)b->jobs.size();
     a.fetch_threshold = b->cfg.fetch_threshold ? b->cfg.fetch_threshold : 20u;
+    a.node_threshold =
+        b->cfg.node_threshold ? b->cfg.node_threshold : rb2dev::default_node_threshold(layout_of(b->cfg.node_order));
     a.chunk = b->cfg.chunk ? b->cfg.chunk : 1u;
     a.counter = b->d_counter;
     a.status = b->d_status;
@@ -869,6 +873,7 @@ int rb2_batch_set_config(rb2_batch* b, const rb2_batch_config* cfg)
     if (cfg->block_threads && cfg->block_threads != 64 && cfg->block_threads != 128 && cfg->block_threads != 256)
         return fail(RB2_ENOTSUP, "block_threads must be 64, 128 or 256");
     if (cfg->fetch_threshold > 32) return fail(RB2_EINVAL, "fetch_threshold must be <= 32");
+    if (cfg->node_threshold > 32) return fail(RB2_EINVAL, "node_threshold must be <= 32");
     if (cfg->node_order > RB2_NODE_ORDER_CW8) return fail(RB2_EINVAL, "unknown node order");
     if (!valid_regs(cfg->regs)) return fail(RB2_ENOTSUP, "regs must be 64, 48 or 40");
     if (int rc0 = batch_prepare_reorder(b, cfg->reorder)) return rc0;
@@ -982,9 +987,11 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
     const uint32_t blocks[] = {64, 128, 256};
     const uint32_t regs[] = {64, 48, 40};
     const uint32_t thresholds[] = {8, 16, 20, 24, 28};
+    const uint32_t node_thresholds[] = {1, 4, 8, 12, 16, 20};
     const uint32_t chunks[] = {1, 2, 4, 8};
     // One coordinate-descent pass over the launch shape of a fixed layout:
-    // block x register budget jointly, then resident CTAs, then the threshold.
+    // block x register budget jointly, then the node-phase threshold, then
+    // resident CTAs, then the fetch threshold.
     auto tune_shape = [&](rb2_batch_config& cur, double& cur_ms) -> int {
         int rc2;
         for (uint32_t bl : blocks) {
@@ -995,6 +1002,11 @@ int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_conf
                 if ((rc2 = time_cfg(c, ms))) return rc2;
                 if (ms < cur_ms) { cur = c; cur_ms = ms; }
             }
+        }
+        for (uint32_t nt : node_thresholds) {
+            rb2_batch_config c = cur; c.node_threshold = nt; double ms;
+            if ((rc2 = time_cfg(c, ms))) return rc2;
+            if (ms < cur_ms) { cur = c; cur_ms = ms; }
         }
         const int maxc =
             std::max(1, b->occ.per_sm[block_index(cur.block_threads)][regs_index(cur.regs)][layout_of(cur.node_order)]);

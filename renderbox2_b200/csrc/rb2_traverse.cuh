@@ -40,6 +40,14 @@ enum Mode : uint32_t { kClosest = 0, kAny = 1, kOcclusion = 2 };
 // Node layouts of the traversal kernel variants.
 enum Layout : int { kLayoutBinary = 0, kLayoutWide4 = 1, kLayoutCw8 = 2 };
 
+// Node-phase threshold of persistent_trace / persistent_trace_cw8 for a launch
+// configuration that leaves it 0: the fastest measured on the batching
+// workload for each layout.
+__host__ __device__ constexpr uint32_t default_node_threshold(int layout)
+{
+    return layout == kLayoutCw8 ? 12u : 8u;
+}
+
 constexpr uint32_t kJobMask = 0x3FFFFFFFu;          // job index bits of Lane::tag
 constexpr uint64_t kMaxJobRays = 0xFFFFFFFFull;     // rays per job (Lane::ray is 32-bit)
 
@@ -140,8 +148,12 @@ __device__ __forceinline__ void cswap(float& ka, int& ca, float& kb, int& cb)
     }
 }
 
+// node_threshold: the node phase also ends, so that postponed leaves are
+// tested, once fewer than this many lanes still traverse nodes while some lane
+// holds a leaf (0 or 1: only when no lane is left searching for one).
 template <class Source, bool WIDE = false>
-__device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_threshold, unsigned int* status)
+__device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_threshold, uint32_t node_threshold,
+                                                 unsigned int* status)
 {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -287,6 +299,10 @@ __device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_thr
                     }
                 }
                 if (!__any_sync(kFull, in && L.leafAddr >= 0)) break;
+                if ((unsigned)__popc(__ballot_sync(kFull, has_ray && (unsigned)L.nodeAddr < (unsigned)kSentinel)) <
+                        node_threshold &&
+                    __any_sync(kFull, has_ray && L.leafAddr < 0))
+                    break;
             }
 
             // Postponed leaves.

@@ -9,7 +9,8 @@
 // yields an 8-bit mask of hit slots; two table lookups turn it into both
 // groups (instead of the paper's per-child meta-byte decoding).  The warp walks nodes
 // until every busy lane holds triangles (the counterpart of the binary
-// kernel's postponed leaf), then tests triangles, then refills lanes from the
+// kernel's postponed leaf) or too few lanes still want nodes, then tests
+// triangles, then refills lanes from the
 // ray source as the binary kernel does (same RaySource policy, same dynamic
 // fetch).  Triangles are the binary layout's Woop rows with the same test
 // arithmetic, so an accepted hit has the same t, u, v bits; boxes are
@@ -84,8 +85,16 @@ __device__ __forceinline__ bool cw8_triangle(Lane& L, int triAddr)
 // the rounding of either form.  The integrators' kernels take it (fewer
 // instructions, no added spills); in the batched job kernel it adds spills
 // and costs more than it saves, so that kernel keeps the subtraction.
+//
+// node_threshold: a node phase also ends, so that pending triangle groups are
+// tested, once fewer than this many lanes still want nodes while some lane
+// holds triangles (0 or 1: only when no lane wants nodes).  Testing triangles
+// earlier shortens the lanes' hit distances sooner and keeps more lanes busy
+// in the node phases; a lane's own order of node visits and triangle tests is
+// unchanged, so results do not depend on it.
 template <class Source, bool kOodSlab = false>
-__device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch_threshold, unsigned int* status)
+__device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch_threshold, uint32_t node_threshold,
+                                                     unsigned int* status)
 {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -152,7 +161,9 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
             // ---- nodes, until every busy lane holds triangles or is done.
             for (;;) {
                 const bool in = has_ray && tg2_bits == 0 && (ng_bits > 0x00FFFFFFu || sp > 0);
-                if (!__any_sync(kFull, in)) break;
+                const unsigned inm = __ballot_sync(kFull, in);
+                if (inm == 0) break;
+                if ((unsigned)__popc(inm) < node_threshold && __any_sync(kFull, has_ray && tg_bits != 0)) break;
                 if (in) {
                     if (ng_bits <= 0x00FFFFFFu) {
                         --sp;

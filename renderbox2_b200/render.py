@@ -289,10 +289,10 @@ class Integrator:
         self._it = C.c_void_p()
         check(lib().rb2_integrator_create(tracer.handle, scene.handle, C.byref(self._it)))
 
-    def set_launch(self, block_threads: int = 0, regs: int = 0, fetch_threshold: int = 0):
+    def set_launch(self, block_threads: int = 0, regs: int = 0, fetch_threshold: int = 0, node_threshold: int = 0):
         """Launch shape of the integrator's traversal kernels (0 = default)."""
         from ._native import LaunchConfig
-        c = LaunchConfig(block_threads, 0, fetch_threshold, regs)
+        c = LaunchConfig(block_threads, 0, fetch_threshold, regs, node_threshold)
         check(lib().rb2_integrator_set_launch(self._it, C.byref(c)))
 
     def set_wave(self, paths: int = 0):

@@ -23,7 +23,7 @@ def _event_ms(fn, stream, reps=1):
 
 
 def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order: int | None = None,
-               tri_cost: float | None = None):
+               tri_cost: float | None = None, node_threshold: int = 0):
     """Config 1 (AO), 2 (PT) or 3 (BDPT) at full size: samples/s and Mrays/s.
     "raycast": the config-2 scene, camera and spp through the ray-cast
     integrator (primary rays only, primitive-id shading).
@@ -31,7 +31,8 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
     traversal layout is `node_order`, or (None) the faster of the binary BFS
     and the compressed 8-wide layout on one timed frame each.  The BVH is
     built with the benchmark SAH costs (configs.BUILD; `tri_cost` overrides
-    the triangle cost)."""
+    the triangle cost).  `node_threshold` sets the traversal's node-phase
+    threshold (rb2_launch_config.node_threshold; 0: the layout's default)."""
     import torch
 
     import renderbox2_b200 as rb
@@ -55,6 +56,8 @@ def integrator(kind: str, warmup: int = 1, keep: dict | None = None, node_order:
     tracer = rb.CudaTracer(bvh)
     it = Integrator(tracer, DeviceScene(scene))
     it.set_timing(True)  # traversal launches bracketed by CUDA events (stats "trace_ms")
+    if node_threshold:
+        it.set_launch(node_threshold=node_threshold)
     scale = c.get("room_size", 1.0)
     eye = [x * scale for x in c["eye"]]
     look = [x * scale for x in c["lookat"]]

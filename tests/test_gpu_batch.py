@@ -88,6 +88,9 @@ def test_batch_equals_plain_launches(rb, orc, cuda):
     dict(reorder=3), dict(reorder=4, chunk=4), dict(reorder=5, node_order=1, regs=48, block_threads=256),
     dict(reorder=4, node_order=2), dict(reorder=4, node_order=3, regs=48, block_threads=256, fetch_threshold=16),
     dict(reorder=5, node_order=3, regs=40, chunk=2), dict(reorder=6), dict(reorder=6, node_order=3, regs=48),
+    dict(node_threshold=1), dict(node_order=1, node_threshold=8, reorder=4), dict(node_order=2, node_threshold=16),
+    dict(node_order=3, node_threshold=1), dict(node_order=3, node_threshold=32, block_threads=64),
+    dict(node_order=3, node_threshold=4, reorder=4, fetch_threshold=28),
 ])
 def test_batch_configs_give_identical_results(rb, orc, cuda, cfg):
     scenes, tracers, jobs, outs, plain = _setup(rb, cuda)
