@@ -795,6 +795,9 @@ def integrator_roofline(kind, r, counts, peak, peak_src):
     if kind == "raycast":
         out["note"] = ("coherent camera rays: neighbouring lanes fetch the same nodes, which the L1 serves, so the "
                        "fraction can exceed 1; neither L2 nor HBM bounds this trace")
+    elif kind == "pt":
+        out["note"] = ("camera and extension rays leave neighbouring pixels' points in pixel order, so the L1 serves "
+                       "part of the node fetches and the fraction of the L2 copy can exceed 1")
     return out
 
 
