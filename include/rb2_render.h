@@ -243,6 +243,21 @@ typedef struct {
     uint32_t compat;         /* RB2_COMPAT_RR_DIVISOR | RB2_COMPAT_NEE_RESEED, or 0 */
 } rb2_pt_params;
 int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, float* d_rgb, void* stream);
+/* Progressive path tracing: the checkpoint / resume form of rb2_render_pt for
+ * long renders (the reference renders a whole frame at once and keeps no
+ * render state, renderers/samplerrenderer.cu:182-196, MODE_PROGRESSIVE not
+ * implemented in renderers/samplerrenderer.cpp:103-106).  Adds samples
+ * [first_sample, first_sample + p->spp) of every pixel to the caller's running
+ * sums d_sum (4 floats per pixel, 16-byte aligned: r, g, b sums, and the
+ * filter weight sum when a film filter is set), zeroed by the caller before
+ * the first call, and, when d_rgb is not NULL, writes the image over all
+ * first_sample + p->spp samples summed so far.  A render can stop after any
+ * call and resume later from a copy of d_sum and its sample count.  Without a
+ * film filter, splitting the samples over calls gives the same bits as one
+ * rb2_render_pt call of the total spp with the same seed; with one, the same
+ * samples summed in another order (equal within float rounding). */
+int rb2_render_pt_progressive(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, uint32_t first_sample,
+                              float* d_sum, float* d_rgb, void* stream);
 
 /* Bidirectional path tracing with a light-vertex cache
  * (BidirectionalPathIntegratorLvcParams, core/params.h:103-118;

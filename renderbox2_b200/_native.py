@@ -195,6 +195,7 @@ SIGNATURES = {
     "rb2_integrator_stats": (C.c_int, [P, C.POINTER(RenderStats), P]),
     "rb2_render_ao": (C.c_int, [P, C.POINTER(Camera), C.POINTER(AoParams), P, P]),
     "rb2_render_pt": (C.c_int, [P, C.POINTER(Camera), C.POINTER(PtParams), P, P]),
+    "rb2_render_pt_progressive": (C.c_int, [P, C.POINTER(Camera), C.POINTER(PtParams), C.c_uint32, P, P, P]),
     "rb2_render_raycast": (C.c_int, [P, C.POINTER(Camera), C.POINTER(RayCastParams), P, P]),
     "rb2_render_bdpt": (C.c_int, [P, C.POINTER(Camera), C.POINTER(BdptParams), P, P]),
     "rb2_render_bdpt_lvc": (C.c_int, [P, C.POINTER(Camera), C.POINTER(BdptLvcParams), P, P]),

@@ -1815,9 +1815,18 @@ int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params
     return RB2_OK;
 }
 
-int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, float* d_rgb, void* stream)
+namespace {
+
+// The path tracer over samples [first_sample, first_sample + spp) of every
+// pixel, added to `accum` (per pixel: r, g, b sums, and the filter weight sum
+// in w when a film filter is set), which is zeroed first when `reset`; then,
+// when d_rgb is given, the mean over the first_sample + spp samples summed so
+// far.  Every random number is keyed by the sample's global index and the sums
+// run in sample order, so unfiltered sums do not depend on how the samples are
+// split into calls or waves.
+int render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, uint32_t first_sample, float4* accum,
+              bool reset, float* d_rgb, void* stream)
 {
-    if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
     it->ev_used = 0;
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
     if (p->max_depth > 64) return fail(RB2_EINVAL, "max_depth must be <= 64");
@@ -1827,14 +1836,15 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
         return fail(RB2_EINVAL, "RB2_COMPAT_RR_DIVISOR divides by 1 - q: rr_prob must be < 1");
     cudaStream_t s = (cudaStream_t)stream;
     const uint64_t npix = (uint64_t)cam->width * cam->height;
-    if (npix == 0 || npix * p->spp > 0xFFFFFFFFull) return fail(RB2_EINVAL, "image x spp must fit 32-bit sample keys");
+    const uint64_t end_sample = (uint64_t)first_sample + p->spp;
+    if (npix == 0 || npix * end_sample > 0xFFFFFFFFull)
+        return fail(RB2_EINVAL, "image x (first sample + spp) must fit 32-bit sample keys");
     // Samples per pixel in flight: about 8M paths per wave by default.
     const uint64_t P = pt_paths_in_flight(npix, p->spp, p->spp_per_wave, it->wave_paths ? it->wave_paths : kRenderWavePaths);
     const uint32_t spw = (uint32_t)(P / npix);
     PathState& ps = it->ps;
     int rc;
     if ((rc = ensure_path_state(ps, P))) return rc;
-    if ((rc = grow(it->d_accum, it->cap_accum, npix))) return rc;
     const bool filtered = it->filter.kind != RB2_FILTER_NONE;
     rb2dev::FilmArgs fa{};
     if (filtered) {
@@ -1842,7 +1852,7 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
         if ((rc = film_args(it->filter, cam->width, cam->height, fa))) return rc;
     }
     if (!it->d_wave) RB2_CUDA(rb2::dev_malloc(&it->d_wave, sizeof(WaveCounters)), "wave counters");
-    RB2_CUDA(cudaMemsetAsync(it->d_accum, 0, npix * 16, s), "accumulator reset");
+    if (reset) RB2_CUDA(cudaMemsetAsync(accum, 0, npix * 16, s), "accumulator reset");
     RB2_CUDA(cudaMemsetAsync(it->d_wave, 0, sizeof(WaveCounters), s), "counter reset");
 
     rb2dev::CamArgs ca;
@@ -1855,8 +1865,8 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
     const DeviceBvhView bv_cam = device_bvh(it->tracer, cw8_origin_ok(it->tracer, cam->eye));
     WaveCounters* wc = it->d_wave;
     const unsigned g = grid_for(P, it->sms);
-    for (uint32_t s0 = 0; s0 < p->spp; s0 += spw) {
-        const uint32_t cur_spw = std::min(spw, p->spp - s0);
+    for (uint32_t s0 = first_sample; s0 < (uint32_t)end_sample; s0 += spw) {
+        const uint32_t cur_spw = std::min(spw, (uint32_t)end_sample - s0);
         const uint32_t paths = (uint32_t)(npix * cur_spw);
         rb2dev::k_pt_camera<<<g, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, paths, s0, ps.ray, ps.T, ps.L, ps.q[0], wc,
                                               filtered ? it->d_film_xy : nullptr);
@@ -1882,18 +1892,39 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
         }
         if (filtered)
             rb2dev::k_film_gather<<<grid_for(npix, it->sms), 256, 0, s>>>(
-                fa, rb2dev::ArrayPos{it->d_film_xy, (uint32_t)npix}, ps.L, cur_spw, it->d_accum, nullptr);
+                fa, rb2dev::ArrayPos{it->d_film_xy, (uint32_t)npix}, ps.L, cur_spw, accum, nullptr);
         else
-            rb2dev::k_pt_accumulate<<<grid_for(npix, it->sms), 256, 0, s>>>(ps.L, (uint32_t)npix, cur_spw, it->d_accum);
+            rb2dev::k_pt_accumulate<<<grid_for(npix, it->sms), 256, 0, s>>>(ps.L, (uint32_t)npix, cur_spw, accum);
         RB2_CUDA(cudaGetLastError(), "PT accumulate");
     }
+    if (!d_rgb) return RB2_OK;
     if (filtered)
-        rb2dev::k_film_resolve<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_accum, (uint32_t)npix, d_rgb);
+        rb2dev::k_film_resolve<<<grid_for(npix, it->sms), 256, 0, s>>>(accum, (uint32_t)npix, d_rgb);
     else
-        rb2dev::k_pt_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(it->d_accum, (uint32_t)npix, 1.0f / (float)p->spp,
-                                                                      d_rgb);
+        rb2dev::k_pt_finalize<<<grid_for(npix, it->sms), 256, 0, s>>>(accum, (uint32_t)npix,
+                                                                      1.0f / (float)end_sample, d_rgb);
     RB2_CUDA(cudaGetLastError(), "PT finalize");
     return RB2_OK;
+}
+
+}  // namespace
+
+int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, float* d_rgb, void* stream)
+{
+    if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
+    const uint64_t npix = (uint64_t)cam->width * cam->height;
+    if (npix && npix <= 0xFFFFFFFFull) {
+        if (int rc = grow(it->d_accum, it->cap_accum, npix)) return rc;
+    }
+    return render_pt(it, cam, p, 0, it->d_accum, true, d_rgb, stream);
+}
+
+int rb2_render_pt_progressive(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, uint32_t first_sample,
+                              float* d_sum, float* d_rgb, void* stream)
+{
+    if (!it || !cam || !p || !d_sum) return fail(RB2_EINVAL, "null argument");
+    if ((uintptr_t)d_sum & 15u) return fail(RB2_EINVAL, "d_sum must be 16-byte aligned");
+    return render_pt(it, cam, p, first_sample, reinterpret_cast<float4*>(d_sum), false, d_rgb, stream);
 }
 
 int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_raycast_params* p, float* d_rgb,

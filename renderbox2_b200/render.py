@@ -336,6 +336,26 @@ class Integrator:
         check(lib().rb2_render_pt(self._it, C.byref(camera.c), C.byref(p), _ptr(out), _stream_handle(stream)))
         return out
 
+    def render_pt_progressive(self, camera, params: PathIntegratorParams, first_sample: int, sums, out=None,
+                              stream=None):
+        """Adds samples [first_sample, first_sample + params.spp) of every
+        pixel to `sums` (a float32 CUDA tensor of 4 values per pixel, zeroed
+        before the first call) and returns the image over all samples summed
+        so far in `out` (allocated when None).  Unfiltered, any split of the
+        samples over calls gives the same image as one render_pt call of the
+        total spp (rb2_render_pt_progressive)."""
+        import torch
+        n = camera.width * camera.height
+        if sums.numel() != 4 * n or sums.dtype != torch.float32 or not sums.is_cuda or not sums.is_contiguous():
+            raise ValueError("sums must be a contiguous float32 CUDA tensor of 4 values per pixel")
+        if out is None:
+            out = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+        p = PtParams(params.spp, params.max_depth, params.rr_start, params.rr_prob, params.seed,
+                     params.spp_per_wave, params.compat)
+        check(lib().rb2_render_pt_progressive(self._it, C.byref(camera.c), C.byref(p), int(first_sample), _ptr(sums),
+                                              _ptr(out), _stream_handle(stream)))
+        return out
+
     def render_bdpt(self, camera, params: BidirectionalPathIntegratorLvcParams, out=None, stream=None):
         import torch
         n = camera.width * camera.height

@@ -255,3 +255,36 @@ def test_far_camera_on_the_compressed_layout(rb, cuda):
         print(name, "differing pixels", diff)
         assert diff <= 2e-3, name
     tr.set_node_order(rb.NODE_ORDER_DFS)
+
+
+def test_pt_progressive_resume_matches_one_render(rb, cuda):
+    """Progressive path tracing: 20 + 20 + 24 samples added to running sums
+    (with a host round trip of the sums between calls, as a checkpoint would
+    do) give the same bits as one 64-sample render with the same seed; with a
+    Gaussian film filter the same samples agree within float rounding."""
+    import torch
+
+    from renderbox2_b200.configs import CONFIG2 as C2
+    from renderbox2_b200.render import DeviceScene, Filter, Integrator, PathIntegratorParams
+    room = _room(rb, n_spheres=20)
+    it = Integrator(rb.CudaTracer(rb.BVH(room)), DeviceScene(room))
+    W, H = 64, 36
+    cam = rb.PerspectiveCamera(C2["eye"], C2["lookat"], C2["up"], (W, H), C2["fov"])
+    for filt in (None, Filter("gaussian", 2.0, 2.0, 2.0)):
+        it.set_filter(filt)
+        whole = it.render_pt(cam, PathIntegratorParams(spp=64, max_depth=5, seed=9, spp_per_wave=16)).clone()
+        sums = torch.zeros((W * H * 4,), dtype=torch.float32, device="cuda")
+        first = 0
+        for spp in (20, 20, 24):
+            img = it.render_pt_progressive(cam, PathIntegratorParams(spp=spp, max_depth=5, seed=9), first, sums)
+            first += spp
+            sums = sums.cpu().cuda()  # checkpoint: the state leaves the device and comes back
+        torch.cuda.synchronize()
+        if filt is None:
+            assert cuda.equal(img, whole)
+        else:
+            assert torch.allclose(img, whole, rtol=1e-5, atol=1e-7)
+    it.set_filter(None)
+    with pytest.raises(rb.Rb2Error):
+        it.render_pt_progressive(cam, PathIntegratorParams(spp=4), 0,
+                                 torch.zeros((W * H * 4 + 1,), dtype=torch.float32, device="cuda")[1:])
