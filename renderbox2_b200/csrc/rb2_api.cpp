@@ -55,6 +55,7 @@ int rb2_build_params_default(rb2_build_params* p)
 int rb2_bvh_build(const float* v_xyz, uint32_t nv, const uint32_t* idx3, uint32_t ntri, const rb2_build_params* params,
                   rb2_host_bvh** out)
 {
+    rb2::Range nvtx_range("rb2_bvh_build");
     if (!out) return fail(RB2_EINVAL, "null output handle");
     *out = nullptr;
     if ((ntri && (!v_xyz || !idx3)) || (nv && !v_xyz)) return fail(RB2_EINVAL, "null geometry");

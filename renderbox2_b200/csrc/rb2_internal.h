@@ -4,6 +4,8 @@
 #include "rb2.h"
 #include "rb2_render.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
@@ -152,6 +154,16 @@ unsigned long long* tracer_queue_counter(rb2_tracer* t);
 bool cw8_origin_ok(const rb2_tracer* t, const float* o);
 // Bulk trace through the binary buffer whatever the tracer's node order.
 int trace_binary(rb2_tracer* t, const float* d_rays, uint64_t n, int any_hit, void* d_out, void* stream);
+
+// A named profiler range over one host-side stage of the library (NVTX, header
+// only: without a profiler attached, such as `ncu --nvtx`, it costs a branch).
+// Ranges nest with scope; the names are the C-ABI entry points.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
 
 inline uint32_t f2u(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
 inline float u2f(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }

@@ -140,6 +140,7 @@ int rb2_scene_dev_view(const rb2_scene_dev* s, rb2_dev_scene* out)
 int rb2_trace_isect(rb2_tracer* t, const rb2_scene_dev* scene, const float* d_rays, uint32_t n, int any_hit,
                     const uint8_t* d_mask, const rb2_isect_buffer* out, void* stream)
 {
+    rb2::Range nvtx_range("rb2_trace_isect");
     if (!t || !scene || !out || (n && !d_rays)) return fail(RB2_EINVAL, "null argument");
     if (misaligned(d_rays, 16)) return fail(RB2_EINVAL, "rays must be 16-byte aligned");
     if (out->uv && misaligned(out->uv, 8)) return fail(RB2_EINVAL, "uv must be 8-byte aligned");

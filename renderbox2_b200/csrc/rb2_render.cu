@@ -1757,6 +1757,7 @@ int rb2_integrator_device_bytes(const rb2_integrator* it, uint64_t* bytes)
 
 int rb2_render_ao(rb2_integrator* it, const rb2_camera* cam, const rb2_ao_params* p, float* d_ao, void* stream)
 {
+    rb2::Range nvtx_range("rb2_render_ao");
     if (!it || !cam || !p || !d_ao) return fail(RB2_EINVAL, "null argument");
     it->ev_used = 0;
     if (p->samples == 0 || !(p->radius > 0.0f)) return fail(RB2_EINVAL, "AO needs samples > 0 and radius > 0");
@@ -1827,6 +1828,7 @@ namespace {
 int render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p, uint32_t first_sample, float4* accum,
               bool reset, float* d_rgb, void* stream)
 {
+    rb2::Range nvtx_range("rb2_render_pt");
     it->ev_used = 0;
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
     if (p->max_depth > 64) return fail(RB2_EINVAL, "max_depth must be <= 64");
@@ -1930,6 +1932,7 @@ int rb2_render_pt_progressive(rb2_integrator* it, const rb2_camera* cam, const r
 int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_raycast_params* p, float* d_rgb,
                        void* stream)
 {
+    rb2::Range nvtx_range("rb2_render_raycast");
     if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
     it->ev_used = 0;
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");
@@ -1996,6 +1999,7 @@ int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_rayc
 
 int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_params* p, float* d_rgb, void* stream)
 {
+    rb2::Range nvtx_range("rb2_render_bdpt");
     if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
     rb2_bdpt_lvc_params q{};
     q.spp = p->spp;
@@ -2013,6 +2017,7 @@ int rb2_render_bdpt(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_pa
 int rb2_render_bdpt_lvc(rb2_integrator* it, const rb2_camera* cam, const rb2_bdpt_lvc_params* p, float* d_rgb,
                         void* stream)
 {
+    rb2::Range nvtx_range("rb2_render_bdpt_lvc");
     if (!it || !cam || !p || !d_rgb) return fail(RB2_EINVAL, "null argument");
     it->ev_used = 0;
     if (p->spp == 0) return fail(RB2_EINVAL, "spp must be > 0");

@@ -204,6 +204,7 @@ double percentile(std::vector<double> v, double q)
 extern "C" int rb2_server_run(rb2_server* s, const rb2_job* jobs, uint32_t n_jobs, rb2_job_result* results,
                               rb2_server_stats* stats)
 {
+    rb2::Range nvtx_range("rb2_server_run");
     if (!s || (n_jobs && (!jobs || !results))) return fail(RB2_EINVAL, "null argument");
     for (Slot& sl : s->slots) {
         sl.job = -1;

@@ -387,6 +387,7 @@ extern "C" {
 
 int rb2_tracer_create(const rb2_host_bvh* bvh, rb2_tracer** out)
 {
+    rb2::Range nvtx_range("rb2_tracer_create");
     if (!bvh || !out) return fail(RB2_EINVAL, "null argument");
     *out = nullptr;
     const HostBvh& h = host_of(bvh);
@@ -528,6 +529,7 @@ int rb2_tracer_device_bytes(const rb2_tracer* t, uint64_t* bytes)
 int rb2_trace(rb2_tracer* t, const float* d_rays, uint32_t n, int any_hit, const uint8_t* d_mask, rb2_hit* d_hits,
               void* stream)
 {
+    rb2::Range nvtx_range("rb2_trace");
     if (!t || (n && (!d_rays || !d_hits))) return fail(RB2_EINVAL, "null argument");
     if (((uintptr_t)d_rays | (uintptr_t)d_hits) & 15u) return fail(RB2_EINVAL, "rays and hits must be 16-byte aligned");
     return trace_single(t, d_rays, n, any_hit ? rb2dev::kAny : rb2dev::kClosest, d_mask, d_hits, (cudaStream_t)stream);
@@ -536,6 +538,7 @@ int rb2_trace(rb2_tracer* t, const float* d_rays, uint32_t n, int any_hit, const
 int rb2_trace_occlusion(rb2_tracer* t, const float* d_rays, uint32_t n, const uint8_t* d_mask, uint8_t* d_occluded,
                         void* stream)
 {
+    rb2::Range nvtx_range("rb2_trace_occlusion");
     if (!t || (n && (!d_rays || !d_occluded))) return fail(RB2_EINVAL, "null argument");
     if ((uintptr_t)d_rays & 15u) return fail(RB2_EINVAL, "rays must be 16-byte aligned");
     return trace_single(t, d_rays, n, rb2dev::kOcclusion, d_mask, d_occluded, (cudaStream_t)stream);
@@ -544,6 +547,7 @@ int rb2_trace_occlusion(rb2_tracer* t, const float* d_rays, uint32_t n, const ui
 int rb2_trace_host(rb2_tracer* t, const float* h_rays, uint32_t n, int any_hit, const uint8_t* h_mask, rb2_hit* h_hits,
                    void* stream)
 {
+    rb2::Range nvtx_range("rb2_trace_host");
     if (!t || (n && (!h_rays || !h_hits))) return fail(RB2_EINVAL, "null argument");
     if (n == 0) return RB2_OK;
     cudaStream_t s = (cudaStream_t)stream;
@@ -912,6 +916,7 @@ int rb2_batch_capture(rb2_batch* b, void* stream)
 
 int rb2_batch_launch(rb2_batch* b, void* stream)
 {
+    rb2::Range nvtx_range("rb2_batch_launch");
     if (!b) return fail(RB2_EINVAL, "null argument");
     cudaStream_t s = (cudaStream_t)stream;
     if (b->total == 0) return RB2_OK;
@@ -941,6 +946,7 @@ int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream)
 // the fastest kept.
 int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best_out, double* best_ms_out)
 {
+    rb2::Range nvtx_range("rb2_batch_autotune");
     if (!b) return fail(RB2_EINVAL, "null argument");
     cudaStream_t s = (cudaStream_t)stream;
     if (reps == 0) reps = 3;
@@ -1220,6 +1226,7 @@ int rb2_pipeline_create(uint64_t chunk_rays, uint32_t depth, rb2_pipeline** out)
 
 int rb2_trace_host_jobs(rb2_pipeline* p, const rb2_host_job* jobs, uint32_t n_jobs, void* stream)
 {
+    rb2::Range nvtx_range("rb2_trace_host_jobs");
     if (!p || (n_jobs && !jobs)) return fail(RB2_EINVAL, "null argument");
     const cudaStream_t caller = (cudaStream_t)stream;
     for (uint32_t i = 0; i < n_jobs; i++) {
