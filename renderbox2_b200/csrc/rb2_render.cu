@@ -1867,7 +1867,10 @@ int render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p,
     const DeviceBvhView bv_cam = device_bvh(it->tracer, cw8_origin_ok(it->tracer, cam->eye));
     WaveCounters* wc = it->d_wave;
     const unsigned g = grid_for(P, it->sms);
-    for (uint32_t s0 = first_sample; s0 < (uint32_t)end_sample; s0 += spw) {
+    // (The step stops at the end instead of stepping past it, so a count of
+    // samples near 2^32 cannot wrap the counter.)
+    for (uint32_t s0 = first_sample; s0 < (uint32_t)end_sample;
+         s0 = (uint32_t)end_sample - s0 > spw ? s0 + spw : (uint32_t)end_sample) {
         const uint32_t cur_spw = std::min(spw, (uint32_t)end_sample - s0);
         const uint32_t paths = (uint32_t)(npix * cur_spw);
         rb2dev::k_pt_camera<<<g, 256, 0, s>>>(ca, p->seed, (uint32_t)npix, paths, s0, ps.ray, ps.T, ps.L, ps.q[0], wc,
@@ -1965,7 +1968,7 @@ int rb2_render_raycast(rb2_integrator* it, const rb2_camera* cam, const rb2_rayc
     const DeviceBvhView bv_cam = device_bvh(it->tracer, cw8_origin_ok(it->tracer, cam->eye));
     WaveCounters* wc = it->d_wave;
     const unsigned g = grid_for(P, it->sms);
-    for (uint32_t s0 = 0; s0 < p->spp; s0 += spw) {
+    for (uint32_t s0 = 0; s0 < p->spp; s0 = p->spp - s0 > spw ? s0 + spw : p->spp) {
         const uint32_t cur_spw = std::min(spw, p->spp - s0);
         const uint32_t paths = (uint32_t)(npix * cur_spw);
         // Camera samples (kernel_generate_perspective_camera_samples), then the
@@ -2146,7 +2149,7 @@ int rb2_render_bdpt_lvc(rb2_integrator* it, const rb2_camera* cam, const rb2_bdp
         const float cap = std::ceil(1.1f * avg * (float)NL);
         lvc_cap = cap >= 4294967295.0f ? 0xFFFFFFFFu : (uint32_t)cap;
     }
-    for (uint32_t it0 = 0; it0 < p->spp; it0 += Wv) {
+    for (uint32_t it0 = 0; it0 < p->spp; it0 = p->spp - it0 > Wv ? it0 + Wv : p->spp) {
         // Wave of w iterations: light path l is path l % NL of iteration it0 + l / NL,
         // camera path c is pixel c % npix of iteration it0 + c / npix.  The random
         // keys are those of the iterations run one at a time.
