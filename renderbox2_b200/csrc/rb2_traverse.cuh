@@ -195,7 +195,8 @@ __device__ __forceinline__ void persistent_trace(Source& src, uint32_t fetch_thr
 
         // ---- traversal until too few lanes are busy.
         while (__any_sync(kFull, has_ray)) {
-            // Inner nodes until every busy lane has postponed a leaf.
+            // Inner nodes until every busy lane has postponed a leaf, or fewer
+            // than node_threshold lanes still traverse while some lane holds one.
             for (;;) {
                 const bool in = has_ray && (unsigned)L.nodeAddr < (unsigned)kSentinel;
                 if (!__any_sync(kFull, in)) break;

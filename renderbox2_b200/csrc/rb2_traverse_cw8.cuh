@@ -158,7 +158,9 @@ __device__ __forceinline__ void persistent_trace_cw8(Source& src, uint32_t fetch
         if (__all_sync(kFull, retired)) break;
 
         while (__any_sync(kFull, has_ray)) {
-            // ---- nodes, until every busy lane holds triangles or is done.
+            // ---- nodes, until every busy lane holds triangles or is done, or
+            //      fewer than node_threshold lanes want nodes while some lane
+            //      holds triangles.
             for (;;) {
                 const bool in = has_ray && tg2_bits == 0 && (ng_bits > 0x00FFFFFFu || sp > 0);
                 const unsigned inm = __ballot_sync(kFull, in);
