@@ -8,8 +8,8 @@ One step = every scene's ray batch traced once: 64 heightfield scenes with
 log-uniform 1k..2M triangles (built with the benchmark SAH costs,
 configs.BUILD), 1M incoherent diffuse-bounce rays per scene, 50 % closest-hit
 and 50 % any-hit (occlusion), in one batched launch whose configuration the
-autotuner picks (node layout, launch shape, ray reordering; the reordering
-sort runs inside the step).  Inputs are resident in HBM when the timed region
+autotuner picks (node layout, launch shape, fetch and node-phase thresholds,
+ray reordering; a reordering sort, when picked, runs inside the step).  Inputs are resident in HBM when the timed region
 starts; L2 is flushed (256 MB write) between timed steps.  `e2e` repeats the step through the host-buffer C-ABI call
 (rb2_trace_host_jobs: pinned host rays in, hits / occlusion bytes out, the
 copies pipelined with traversal over several streams), copies included.
@@ -28,7 +28,9 @@ reference has no host traversal) traces each scene's full ray batch.  That
 process loads no part of this library.
 
 --workload profile runs one batched launch configuration over a small case
-repeatedly (for ncu captures; see --profile-* options); --batch-config fixes
+repeatedly (for ncu captures; see --profile-* options); --node-threshold sets
+the integrators' node-phase threshold in the ao/pt/bdpt/raycast lines;
+--batch-config fixes
 the headline's batch configuration instead of autotuning it (for repeatable
 launch lists); --workload serve-curve measures config-5 latency against
 offered load.
