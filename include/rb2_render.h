@@ -251,8 +251,10 @@ int rb2_render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params
  * sums d_sum (4 floats per pixel, 16-byte aligned: r, g, b sums, and the
  * filter weight sum when a film filter is set), zeroed by the caller before
  * the first call, and, when d_rgb is not NULL, writes the image over all
- * first_sample + p->spp samples summed so far.  A render can stop after any
- * call and resume later from a copy of d_sum and its sample count.  Without a
+ * first_sample + p->spp samples summed so far.  Every call of one render
+ * uses the same camera, seed, path parameters and film filter; only spp and
+ * first_sample change.  A render can stop after any call and resume later
+ * from a copy of d_sum and its sample count.  Without a
  * film filter, splitting the samples over calls gives the same bits as one
  * rb2_render_pt call of the total spp with the same seed; with one, the same
  * samples summed in another order (equal within float rounding). */

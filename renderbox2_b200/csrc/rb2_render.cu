@@ -1841,7 +1841,7 @@ int render_pt(rb2_integrator* it, const rb2_camera* cam, const rb2_pt_params* p,
     const uint64_t end_sample = (uint64_t)first_sample + p->spp;
     if (npix == 0 || npix * end_sample > 0xFFFFFFFFull)
         return fail(RB2_EINVAL, "image x (first sample + spp) must fit 32-bit sample keys");
-    // Samples per pixel in flight: about 8M paths per wave by default.
+    // Samples per pixel in flight: up to kRenderWavePaths paths per wave by default.
     const uint64_t P = pt_paths_in_flight(npix, p->spp, p->spp_per_wave, it->wave_paths ? it->wave_paths : kRenderWavePaths);
     const uint32_t spw = (uint32_t)(P / npix);
     PathState& ps = it->ps;
