@@ -275,9 +275,9 @@ int rb2_batch_launch(rb2_batch* b, void* stream);
 int rb2_batch_capture(rb2_batch* b, void* stream);
 int rb2_batch_status(rb2_batch* b, uint32_t* status, void* stream);
 /* Times candidate configs (coordinate descent over node order, block shape x
- * register budget, CTAs per SM, fetch threshold and queue chunk, without and
- * with ray reordering; median of `reps` launches each), applies and returns
- * the fastest. */
+ * register budget, node-phase threshold, CTAs per SM, fetch threshold and
+ * queue chunk, without and with ray reordering; median of `reps` launches
+ * each), applies and returns the fastest. */
 int rb2_batch_autotune(rb2_batch* b, void* stream, uint32_t reps, rb2_batch_config* best, double* best_ms);
 
 /* ------------------------------------------------------- fault injection --
